@@ -1,0 +1,749 @@
+/*
+ * kifmm_oracle.c -- CPU restatement of the reference's adaptive 2D KIFMM.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the oracle: the checker that the
+ * tests, the smoke check and the CPU-baseline leg of bench.py compare the
+ * CUDA path against.  Nothing in the product links or calls it.
+ *
+ * It restates, step for step, the algorithm of dbstein/pykifmm2d's live FMM
+ * (pykifmm2d/class_fmm.py:166-402 over pykifmm2d/tree.py:460-590):
+ *   - tree build by level splitting with the same in-place 4-way partition,
+ *     the same colleague tagging, level restriction and X-list fake leaves;
+ *   - operator precompute (E2C LU, M2MC, M2LS, CM2LS) per level;
+ *   - upward pass (M2M + P2M + LU solve), downward pass (L2L + M2L GEMMs +
+ *     scatter), local expansions, L2P and P2P evaluation.
+ * Loops the reference runs under numba.prange run under OpenMP here.
+ *
+ * The modified-Helmholtz K0 used here is computed independently of any
+ * table: the power series of K0 for x < 2 and the trapezoidal rule on the
+ * integral K0(x) = int_0^inf exp(-x cosh t) dt (DLMF 10.32.9) for x >= 2.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <omp.h>
+
+#define ORK_MAXLEV 64
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+/* ------------------------------------------------------------------ kernels */
+static double ork_k0(double x)
+{
+    if (x < 0) return NAN;
+    if (x == 0) return INFINITY;
+    if (x < 2.0) {
+        /* K0(x) = -(ln(x/2)+gamma) I0(x) + sum_{k>=1} H_k (x^2/4)^k/(k!)^2 */
+        const double g = 0.57721566490153286060651209;
+        double q = 0.25 * x * x, term = 1.0, i0 = 1.0, s = 0.0, hk = 0.0;
+        for (int k = 1; k < 40; k++) {
+            term *= q / ((double)k * (double)k);
+            hk += 1.0 / k;
+            i0 += term;
+            s += hk * term;
+            if (term < 1e-18) break;
+        }
+        return -(log(0.5 * x) + g) * i0 + s;
+    }
+    /* trapezoidal rule, exponentially convergent for this analytic integrand */
+    /* step small enough for the Gaussian-like peak of width ~ 1/sqrt(x) */
+    const double h = fmin(0.125, 0.5 / sqrt(x));
+    double acc = 0.5; /* f(0) / 2 with f(t) = exp(-x (cosh t - 1)) */
+    for (int j = 1; j < 4000; j++) {
+        double f = exp(-x * (cosh(j * h) - 1.0));
+        acc += f;
+        if (f < 1e-19) break;
+    }
+    return exp(-x) * h * acc;
+}
+
+typedef struct { int kind; double k; } OKern;
+
+/* G(s -> t): Laplace -log(r^2)/(4 pi); modified Helmholtz K0(k r)/(2 pi).
+ * The reference plug-ins: examples/laplace2.py:31-36, modified_helmholtz.py:38-43. */
+static inline double ork_eval(OKern kn, double sx, double sy, double tx, double ty)
+{
+    double dx = tx - sx, dy = ty - sy;
+    double r2 = dx * dx + dy * dy;
+    if (kn.kind == 0) return -0.25 / M_PI * log(r2);
+    return ork_k0(kn.k * sqrt(r2)) / (2.0 * M_PI);
+}
+
+/* ------------------------------------------------------------------- levels */
+typedef struct {
+    int64_t n;
+    double width, half;
+    double *xmin, *ymin, *xmid, *ymid;
+    int64_t *bot, *top, *parent, *children;
+    uint8_t *leaf, *fake, *xlist, *cu;
+    int64_t *coll;           /* n x 9, -1 padded */
+    int64_t *depth, ndepth;  /* ndepth lags n after X-list fake nodes */
+    int64_t n_alloc, n_sib;
+    int64_t *pdi, *tdi;      /* parent_density_ind [n/4], this_density_ind [n] */
+} OLevel;
+
+typedef struct {
+    int64_t N, ppl;
+    double *x, *y;
+    int64_t *ordv;
+    double rmin, rmax;
+    int L;
+    OLevel lv[ORK_MAXLEV];
+} OTree;
+
+static void *xrealloc(void *p, size_t sz) { void *q = realloc(p, sz ? sz : 1); if (!q) abort(); return q; }
+
+static void level_basic(OLevel *v)
+{
+    v->xmid = xrealloc(v->xmid, v->n * sizeof(double));
+    v->ymid = xrealloc(v->ymid, v->n * sizeof(double));
+    for (int64_t i = 0; i < v->n; i++) {
+        v->xmid[i] = v->xmin[i] + v->half;
+        v->ymid[i] = v->ymin[i] + v->half;
+    }
+}
+
+/* Level.__init__ (tree.py:318-338) and Level.add_nodes (tree.py:384-395) */
+static void level_append(OLevel *v, int64_t m, const double *xmin, const double *ymin,
+                         const int64_t *bot, const int64_t *top, const int64_t *par, int xl)
+{
+    int64_t n0 = v->n, n = n0 + m;
+    v->xmin = xrealloc(v->xmin, n * sizeof(double));
+    v->ymin = xrealloc(v->ymin, n * sizeof(double));
+    v->bot = xrealloc(v->bot, n * sizeof(int64_t));
+    v->top = xrealloc(v->top, n * sizeof(int64_t));
+    v->parent = xrealloc(v->parent, n * sizeof(int64_t));
+    v->children = xrealloc(v->children, n * sizeof(int64_t));
+    v->leaf = xrealloc(v->leaf, n);
+    v->fake = xrealloc(v->fake, n);
+    for (int64_t i = 0; i < m; i++) {
+        v->xmin[n0 + i] = xmin[i];
+        v->ymin[n0 + i] = ymin[i];
+        v->bot[n0 + i] = bot[i];
+        v->top[n0 + i] = top[i];
+        v->parent[n0 + i] = par[i];
+        v->children[n0 + i] = -1;
+        v->leaf[n0 + i] = xl ? 0 : 1;
+        v->fake[n0 + i] = xl ? 1 : 0;
+    }
+    v->n = n;
+    level_basic(v);
+}
+
+/* classify + get_inds + get_target + reorder_inplace (tree.py:14-126):
+ * class = 2*(x > midx) + (y > midy); in-place cycle placement. */
+static void reorder_inplace(double *x, double *y, int64_t *ordv, int64_t n,
+                            double midx, double midy, int64_t nns[4])
+{
+    int8_t *cl = malloc(n ? n : 1);
+    int64_t ns[4] = {0, 0, 0, 0}, inds[4];
+    for (int64_t i = 0; i < n; i++) {
+        int c = 2 * (x[i] > midx) + (y[i] > midy);
+        cl[i] = (int8_t)c;
+        ns[c]++;
+    }
+    inds[0] = 0;
+    for (int i = 0; i < 3; i++) inds[i + 1] = inds[i] + ns[i];
+    for (int i = 0; i < 4; i++) nns[i] = inds[i];
+    for (int64_t i = 0; i < n; i++) {
+        int target = i < nns[1] ? 0 : i < nns[2] ? 1 : i < nns[3] ? 2 : 3;
+        for (;;) {
+            int cli = cl[i];
+            int64_t icli = inds[cli];
+            if (cli != target) {
+                int8_t tc = cl[i]; cl[i] = cl[icli]; cl[icli] = tc;
+                double td = x[i]; x[i] = x[icli]; x[icli] = td;
+                td = y[i]; y[i] = y[icli]; y[icli] = td;
+                int64_t to = ordv[i]; ordv[i] = ordv[icli]; ordv[icli] = to;
+                inds[cli]++;
+                if (cl[icli] == target) break;
+            } else {
+                inds[target]++;
+                break;
+            }
+        }
+    }
+    free(cl);
+}
+
+/* divide_and_reorder (tree.py:128-190) followed by appending the children to
+ * the next level (get_new_level tree.py:229-258 / split_bad_leaves :296-311). */
+static void divide_into(OTree *t, int l, const uint8_t *tosplit, int xl)
+{
+    OLevel *v = &t->lv[l], *d = &t->lv[l + 1];
+    int64_t nsplit = 0;
+    int64_t *ids = malloc((v->n ? v->n : 1) * sizeof(int64_t));
+    for (int64_t i = 0; i < v->n; i++) { ids[i] = nsplit; if (tosplit[i]) nsplit++; }
+    int64_t m = 4 * nsplit;
+    double *xmin = malloc((m ? m : 1) * sizeof(double)), *ymin = malloc((m ? m : 1) * sizeof(double));
+    int64_t *bot = malloc((m ? m : 1) * sizeof(int64_t)), *top = malloc((m ? m : 1) * sizeof(int64_t));
+    int64_t *par = malloc((m ? m : 1) * sizeof(int64_t));
+    int64_t start = d->n;
+    double hw = v->half;
+#pragma omp parallel for schedule(dynamic, 16)
+    for (int64_t i = 0; i < v->n; i++) {
+        if (!tosplit[i]) continue;
+        int64_t s = ids[i], bi = v->bot[i], ti = v->top[i], nns[4];
+        reorder_inplace(t->x + bi, t->y + bi, t->ordv + bi, ti - bi, v->xmid[i], v->ymid[i], nns);
+        xmin[4 * s + 0] = v->xmid[i] - hw; xmin[4 * s + 1] = v->xmid[i] - hw;
+        xmin[4 * s + 2] = v->xmid[i];      xmin[4 * s + 3] = v->xmid[i];
+        ymin[4 * s + 0] = v->ymid[i] - hw; ymin[4 * s + 1] = v->ymid[i];
+        ymin[4 * s + 2] = v->ymid[i] - hw; ymin[4 * s + 3] = v->ymid[i];
+        for (int j = 0; j < 4; j++) bot[4 * s + j] = bi + nns[j];
+        top[4 * s + 0] = bi + nns[1]; top[4 * s + 1] = bi + nns[2];
+        top[4 * s + 2] = bi + nns[3]; top[4 * s + 3] = ti;
+        if (!xl) v->leaf[i] = 0;
+        for (int j = 0; j < 4; j++) par[4 * s + j] = i;
+        v->children[i] = start + 4 * s;
+    }
+    d->width = v->half;
+    d->half = 0.5 * d->width;
+    level_append(d, m, xmin, ymin, bot, top, par, xl);
+    free(ids); free(xmin); free(ymin); free(bot); free(top); free(par);
+}
+
+/* Level.tag_colleagues (tree.py:349-375): direct O(n^2) below 100 nodes
+ * (numba_tag_colleagues :260-272), otherwise via the parent's colleagues'
+ * children (numba_loop_colleagues :274-294). */
+static void tag_colleagues(OTree *t, int l)
+{
+    OLevel *v = &t->lv[l];
+    v->coll = xrealloc(v->coll, (v->n ? v->n : 1) * 9 * sizeof(int64_t));
+    for (int64_t i = 0; i < 9 * v->n; i++) v->coll[i] = -1;
+    double dist = 1.5 * v->width, dist2 = dist * dist;
+    if (v->n < 100) {
+#pragma omp parallel for
+        for (int64_t i = 0; i < v->n; i++) {
+            int it = 0;
+            for (int64_t j = 0; j < v->n; j++) {
+                double dx = v->xmid[i] - v->xmid[j], dy = v->ymid[i] - v->ymid[j];
+                if (dx * dx + dy * dy < dist2) v->coll[9 * i + it++] = j;
+            }
+        }
+        return;
+    }
+    OLevel *a = &t->lv[l - 1];
+#pragma omp parallel for
+    for (int64_t i = 0; i < v->n; i++) {
+        int it = 0;
+        int64_t pi = v->parent[i];
+        for (int j = 0; j < 9; j++) {
+            int64_t pij = a->coll[9 * pi + j];
+            if (pij < 0 || a->children[pij] < 0) continue;
+            for (int k = 0; k < 4; k++) {
+                int64_t c = a->children[pij] + k;
+                double dx = v->xmid[i] - v->xmid[c], dy = v->ymid[i] - v->ymid[c];
+                if (dx * dx + dy * dy < dist2) v->coll[9 * i + it++] = c;
+            }
+        }
+    }
+}
+
+/* gather_depths (tree.py:582-585) with numba_get_depths (:423-430) */
+static void gather_depths(OTree *t)
+{
+    for (int l = t->L - 1; l >= 0; l--) {
+        OLevel *v = &t->lv[l];
+        v->depth = xrealloc(v->depth, (v->n ? v->n : 1) * sizeof(int64_t));
+        v->ndepth = v->n;
+        for (int64_t i = 0; i < v->n; i++) v->depth[i] = 0;
+        if (l == t->L - 1) continue;
+        OLevel *d = &t->lv[l + 1];
+        for (int64_t i = 0; i < v->n; i++) {
+            if (v->leaf[i]) continue;
+            int64_t c = v->children[i], mx = d->depth[c];
+            for (int k = 1; k < 4; k++) if (d->depth[c + k] > mx) mx = d->depth[c + k];
+            v->depth[i] = mx + 1;
+        }
+    }
+}
+
+void ork_tree_free(OTree *t)
+{
+    if (!t) return;
+    for (int l = 0; l < ORK_MAXLEV; l++) {
+        OLevel *v = &t->lv[l];
+        free(v->xmin); free(v->ymin); free(v->xmid); free(v->ymid);
+        free(v->bot); free(v->top); free(v->parent); free(v->children);
+        free(v->leaf); free(v->fake); free(v->xlist); free(v->cu);
+        free(v->coll); free(v->depth); free(v->pdi); free(v->tdi);
+    }
+    free(t->x); free(t->y); free(t->ordv);
+    free(t);
+}
+
+/* Tree.__init__ (tree.py:464-522).  fix_bbox = 0 keeps the reference's root
+ * box [floor(min(xmin, ymin)), ceil(max(xmax, ymin))] (tree.py:475-484). */
+int ork_tree_build(const double *x, const double *y, int64_t N, int64_t ppl, int fix_bbox, OTree **out)
+{
+    if (N <= 0 || ppl <= 0) return 1;
+    OTree *t = calloc(1, sizeof(OTree));
+    t->N = N; t->ppl = ppl;
+    t->x = malloc(N * sizeof(double)); t->y = malloc(N * sizeof(double));
+    t->ordv = malloc(N * sizeof(int64_t));
+    memcpy(t->x, x, N * sizeof(double)); memcpy(t->y, y, N * sizeof(double));
+    double xmn = x[0], xmx = x[0], ymn = y[0], ymx = y[0];
+    for (int64_t i = 0; i < N; i++) {
+        if (!isfinite(x[i]) || !isfinite(y[i])) { ork_tree_free(t); return 2; }
+        if (x[i] < xmn) xmn = x[i];
+        if (x[i] > xmx) xmx = x[i];
+        if (y[i] < ymn) ymn = y[i];
+        if (y[i] > ymx) ymx = y[i];
+        t->ordv[i] = i;
+    }
+    double ytop = fix_bbox ? ymx : ymn;
+    t->rmin = floor(xmn < ymn ? xmn : ymn);
+    t->rmax = ceil(xmx > ytop ? xmx : ytop);
+    OLevel *v0 = &t->lv[0];
+    v0->width = t->rmax - t->rmin;
+    v0->half = 0.5 * v0->width;
+    double r = t->rmin; int64_t b = 0, tp = N, p = -1;
+    level_append(v0, 1, &r, &r, &b, &tp, &p, 0);
+    t->L = 1;
+    if (N > ppl) {
+        for (;;) {
+            OLevel *v = &t->lv[t->L - 1];
+            uint8_t *ts = malloc(v->n);
+            int64_t cnt = 0;
+            for (int64_t i = 0; i < v->n; i++) { ts[i] = (v->top[i] - v->bot[i]) > ppl; cnt += ts[i]; }
+            if (t->L >= ORK_MAXLEV - 1) { free(ts); ork_tree_free(t); return 3; }
+            divide_into(t, t->L - 1, ts, 0);
+            free(ts);
+            t->L++;
+            OLevel *d = &t->lv[t->L - 1];
+            int more = 0;
+            for (int64_t i = 0; i < d->n; i++) if (d->top[i] - d->bot[i] > ppl) { more = 1; break; }
+            if (!more) break;
+        }
+    }
+    for (int l = 0; l < t->L; l++) tag_colleagues(t, l);
+    gather_depths(t);
+    /* level_restrict (tree.py:533-545) with numba_get_bads (:432-444) */
+    int64_t newn = 1;
+    while (newn > 0) {
+        newn = 0;
+        for (int l = 1; l < t->L - 2; l++) {
+            OLevel *v = &t->lv[l];
+            uint8_t *bads = calloc(v->n ? v->n : 1, 1);
+            int64_t nb = 0;
+            for (int64_t i = 0; i < v->n; i++) {
+                if (!v->leaf[i]) continue;
+                for (int j = 0; j < 9; j++) {
+                    int64_t cj = v->coll[9 * i + j];
+                    if (cj < 0) continue;
+                    int64_t dd = v->depth[i] - v->depth[cj];
+                    if (dd > 1 || dd < -1) { bads[i] = 1; }
+                }
+                nb += bads[i];
+            }
+            divide_into(t, l, bads, 0);
+            tag_colleagues(t, l + 1);
+            gather_depths(t);
+            free(bads);
+            newn += nb;
+        }
+    }
+    /* split_Xlist (tree.py:546-576) with numba_get_Xlist (:446-458) */
+    for (int l = 0; l < t->L; l++) {
+        OLevel *v = &t->lv[l];
+        v->xlist = xrealloc(v->xlist, v->n ? v->n : 1);
+        memset(v->xlist, 0, v->n);
+        if (l > 0 && l < t->L - 1) {
+            int64_t nd = v->ndepth, nx = 0;
+            for (int64_t i = 0; i < nd; i++) {
+                if (!v->leaf[i]) continue;
+                for (int j = 0; j < 9; j++) {
+                    int64_t cj = v->coll[9 * i + j];
+                    if (cj >= 0 && cj < nd && v->depth[i] - v->depth[cj] < 0) v->xlist[i] = 1;
+                }
+                nx += v->xlist[i];
+            }
+            if (nx > 0) {
+                divide_into(t, l, v->xlist, 1);
+                tag_colleagues(t, l + 1);
+            }
+        }
+        if (l > 0) {
+            v->cu = xrealloc(v->cu, v->n);
+            v->pdi = xrealloc(v->pdi, (v->n / 4 ? v->n / 4 : 1) * sizeof(int64_t));
+            v->tdi = xrealloc(v->tdi, v->n * sizeof(int64_t));
+            for (int64_t i = 0; i < v->n; i++)
+                v->cu[i] = ((v->leaf[i] && !v->xlist[i]) || v->fake[i]) && (v->top[i] > v->bot[i]);
+            int64_t ns = 0, na = 0;
+            for (int64_t g = 0; g < v->n / 4; g++) {
+                int has = 0;
+                for (int k = 0; k < 4; k++) has |= v->top[4 * g + k] > v->bot[4 * g + k];
+                v->pdi[g] = has ? ns++ : -1;
+                for (int k = 0; k < 4; k++) v->tdi[4 * g + k] = has ? na++ : -1;
+            }
+            v->n_sib = ns;
+            v->n_alloc = na;
+        }
+    }
+    *out = t;
+    return 0;
+}
+
+int ork_tree_levels(const OTree *t) { return t->L; }
+
+int64_t ork_tree_num_nodes(const OTree *t)
+{
+    int64_t s = 0;
+    for (int l = 0; l < t->L; l++) s += t->lv[l].n;
+    return s;
+}
+
+/* Canonical export: per node (level, ix, iy, leaf, fake_leaf, Xlist, ns) with
+ * ix = (xmin - root) / width (exact on the dyadic grid). */
+void ork_tree_export(const OTree *t, int64_t *nodes, double *root)
+{
+    int64_t r = 0;
+    for (int l = 0; l < t->L; l++) {
+        const OLevel *v = &t->lv[l];
+        for (int64_t i = 0; i < v->n; i++, r++) {
+            nodes[7 * r + 0] = l;
+            nodes[7 * r + 1] = (int64_t)llround((v->xmin[i] - t->rmin) / v->width);
+            nodes[7 * r + 2] = (int64_t)llround((v->ymin[i] - t->rmin) / v->width);
+            nodes[7 * r + 3] = v->leaf[i];
+            nodes[7 * r + 4] = v->fake[i];
+            nodes[7 * r + 5] = v->xlist ? v->xlist[i] : 0;
+            nodes[7 * r + 6] = v->top[i] - v->bot[i];
+        }
+    }
+    root[0] = t->rmin;
+    root[1] = t->rmax;
+}
+
+/* locate_points (tree.py:703-727): descend with strict '>' until a leaf. */
+static void locate1(const OTree *t, double x, double y, int *ind, int64_t *loc)
+{
+    int l = 0;
+    int64_t i = 0;
+    while (!t->lv[l].leaf[i]) {
+        int64_t c = t->lv[l].children[i];
+        if (x > t->lv[l].xmid[i]) c += 2;
+        if (y > t->lv[l].ymid[i]) c += 1;
+        i = c;
+        l++;
+    }
+    *ind = l;
+    *loc = i;
+}
+
+void ork_locate(const OTree *t, const double *x, const double *y, int64_t n, int64_t *out)
+{
+#pragma omp parallel for
+    for (int64_t p = 0; p < n; p++) {
+        int l; int64_t i;
+        locate1(t, x[p], y[p], &l, &i);
+        const OLevel *v = &t->lv[l];
+        out[3 * p + 0] = l;
+        out[3 * p + 1] = (int64_t)llround((v->xmin[i] - t->rmin) / v->width);
+        out[3 * p + 2] = (int64_t)llround((v->ymin[i] - t->rmin) / v->width);
+    }
+}
+
+/* ---------------------------------------------------------------- dense LA */
+/* LU with partial pivoting (the getrf step of scipy.linalg.lu_factor) */
+static void lu_factor(double *a, int n, int *piv)
+{
+    for (int k = 0; k < n; k++) {
+        int p = k;
+        double mx = fabs(a[k * n + k]);
+        for (int i = k + 1; i < n; i++) if (fabs(a[i * n + k]) > mx) { mx = fabs(a[i * n + k]); p = i; }
+        piv[k] = p;
+        if (p != k) for (int j = 0; j < n; j++) { double tmp = a[k * n + j]; a[k * n + j] = a[p * n + j]; a[p * n + j] = tmp; }
+        double d = a[k * n + k];
+        for (int i = k + 1; i < n; i++) {
+            double f = a[i * n + k] / d;
+            a[i * n + k] = f;
+            for (int j = k + 1; j < n; j++) a[i * n + j] -= f * a[k * n + j];
+        }
+    }
+}
+
+/* getrs for one right-hand side, in place */
+static void lu_solve(const double *lu, const int *piv, int n, double *b)
+{
+    for (int k = 0; k < n; k++) if (piv[k] != k) { double tmp = b[k]; b[k] = b[piv[k]]; b[piv[k]] = tmp; }
+    for (int i = 0; i < n; i++) { double s = b[i]; for (int j = 0; j < i; j++) s -= lu[i * n + j] * b[j]; b[i] = s; }
+    for (int i = n - 1; i >= 0; i--) { double s = b[i]; for (int j = i + 1; j < n; j++) s -= lu[i * n + j] * b[j]; b[i] = s / lu[i * n + i]; }
+}
+
+/* ----------------------------------------------------------------- the FMM */
+typedef struct {
+    OTree *t;
+    OKern kn;
+    int Q;                   /* Nequiv */
+    double *sx[ORK_MAXLEV], *sy[ORK_MAXLEV], *lx[ORK_MAXLEV], *ly[ORK_MAXLEV];
+    double *e2c[ORK_MAXLEV]; int *piv[ORK_MAXLEV];
+    double *m2mc[ORK_MAXLEV];            /* Q x 4Q */
+    double *cm2l[ORK_MAXLEV];            /* 9 blocks of 4Q x 4Q (centre unused) */
+    double *chk[ORK_MAXLEV], *eqd[ORK_MAXLEV], *ls[ORK_MAXLEV], *le[ORK_MAXLEV];
+    double *tau_o;
+} OFMM;
+
+/* out[j, i] = G(s_i -> t_j)  (Get_Kernel_Functions.KF, class_fmm.py:116-122) */
+static void kf(OKern kn, const double *sx, const double *sy, int ns, const double *tx, const double *ty, int nt, double *out)
+{
+    for (int j = 0; j < nt; j++)
+        for (int i = 0; i < ns; i++) out[j * ns + i] = ork_eval(kn, sx[i], sy[i], tx[j], ty[j]);
+}
+
+void ork_fmm_free(OFMM *f)
+{
+    if (!f) return;
+    for (int l = 0; l < ORK_MAXLEV; l++) {
+        free(f->sx[l]); free(f->sy[l]); free(f->lx[l]); free(f->ly[l]);
+        free(f->e2c[l]); free(f->piv[l]); free(f->m2mc[l]); free(f->cm2l[l]);
+        free(f->chk[l]); free(f->eqd[l]); free(f->ls[l]); free(f->le[l]);
+    }
+    free(f->tau_o);
+    free(f);
+}
+
+/* FMM.precompute (class_fmm.py:182-298) */
+int ork_fmm_create(OTree *t, int kind, double k, int Q, OFMM **out)
+{
+    if (Q <= 0 || Q > 256) return 1;
+    OFMM *f = calloc(1, sizeof(OFMM));
+    f->t = t; f->kn.kind = kind; f->kn.k = k; f->Q = Q;
+    int L = t->L;
+    double dd = 0.01;
+    for (int l = 0; l < L; l++) {
+        double w = t->lv[l].width;
+        double r1 = 0.5 * w * (sqrt(2.0) + dd), r2 = 0.5 * w * (4.0 - sqrt(2.0) - 2 * dd);
+        f->sx[l] = malloc(Q * sizeof(double)); f->sy[l] = malloc(Q * sizeof(double));
+        f->lx[l] = malloc(Q * sizeof(double)); f->ly[l] = malloc(Q * sizeof(double));
+        double step = 2.0 * M_PI / Q;
+        for (int q = 0; q < Q; q++) {
+            double th = q * step;
+            f->sx[l][q] = r1 * cos(th); f->sy[l][q] = r1 * sin(th);
+            f->lx[l][q] = r2 * cos(th); f->ly[l][q] = r2 * sin(th);
+        }
+        f->e2c[l] = malloc((size_t)Q * Q * sizeof(double));
+        f->piv[l] = malloc(Q * sizeof(int));
+        kf(f->kn, f->sx[l], f->sy[l], Q, f->lx[l], f->ly[l], Q, f->e2c[l]);
+        lu_factor(f->e2c[l], Q, f->piv[l]);
+    }
+    double *cx = malloc(4 * Q * sizeof(double)), *cy = malloc(4 * Q * sizeof(double));
+    for (int l = 0; l + 1 < L; l++) {
+        double hw = 0.5 * t->lv[l + 1].width;
+        for (int q = 0; q < Q; q++) {
+            cx[q] = f->sx[l + 1][q] - hw;         cy[q] = f->sy[l + 1][q] - hw;
+            cx[Q + q] = f->sx[l + 1][q] - hw;     cy[Q + q] = f->sy[l + 1][q] + hw;
+            cx[2 * Q + q] = f->sx[l + 1][q] + hw; cy[2 * Q + q] = f->sy[l + 1][q] - hw;
+            cx[3 * Q + q] = f->sx[l + 1][q] + hw; cy[3 * Q + q] = f->sy[l + 1][q] + hw;
+        }
+        f->m2mc[l] = malloc((size_t)Q * 4 * Q * sizeof(double));
+        kf(f->kn, cx, cy, 4 * Q, f->lx[l], f->ly[l], Q, f->m2mc[l]);
+    }
+    free(cx); free(cy);
+    double *m2l = malloc((size_t)49 * Q * Q * sizeof(double));
+    double *shx = malloc(Q * sizeof(double)), *shy = malloc(Q * sizeof(double));
+    for (int l = 1; l < L; l++) {
+        double w = t->lv[l].width;
+        for (int ix = 0; ix < 7; ix++)
+            for (int iy = 0; iy < 7; iy++) {
+                if (ix >= 2 && ix <= 4 && iy >= 2 && iy <= 4) continue;
+                for (int q = 0; q < Q; q++) { shx[q] = f->sx[l][q] + (ix - 3) * w; shy[q] = f->sy[l][q] + (iy - 3) * w; }
+                kf(f->kn, shx, shy, Q, f->sx[l], f->sy[l], Q, m2l + (size_t)(ix * 7 + iy) * Q * Q);
+            }
+        int Q4 = 4 * Q;
+        f->cm2l[l] = calloc((size_t)9 * Q4 * Q4, sizeof(double));
+        for (int kx = 0; kx < 3; kx++)
+            for (int ky = 0; ky < 3; ky++) {
+                if (kx == 1 && ky == 1) continue;
+                double *C = f->cm2l[l] + (size_t)(kx * 3 + ky) * Q4 * Q4;
+                for (int ii = 0; ii < 2; ii++)
+                    for (int jj = 0; jj < 2; jj++) {
+                        int shx0 = 2 * (kx - 1) - ii + 3, shy0 = 2 * (ky - 1) - jj + 3, base = 2 * ii + jj;
+                        for (int iii = 0; iii < 2; iii++)
+                            for (int jjj = 0; jjj < 2; jjj++) {
+                                int fx = shx0 + iii, fy = shy0 + jjj, bb = 2 * iii + jjj;
+                                int near = fx >= 2 && fx <= 4 && fy >= 2 && fy <= 4;
+                                for (int a = 0; a < Q; a++)
+                                    for (int c = 0; c < Q; c++)
+                                        C[(size_t)(base * Q + a) * Q4 + bb * Q + c] =
+                                            near ? 0.0 : m2l[(size_t)(fx * 7 + fy) * Q * Q + a * Q + c];
+                            }
+                    }
+            }
+    }
+    free(m2l); free(shx); free(shy);
+    for (int l = 1; l < L; l++) {
+        OLevel *v = &t->lv[l];
+        f->chk[l] = calloc((size_t)(v->n_alloc ? v->n_alloc : 1) * Q, sizeof(double));
+        f->eqd[l] = calloc((size_t)(v->n_alloc ? v->n_alloc : 1) * Q, sizeof(double));
+        f->ls[l] = calloc((size_t)(v->n ? v->n : 1) * Q, sizeof(double));
+        f->le[l] = calloc((size_t)(v->n ? v->n : 1) * Q, sizeof(double));
+    }
+    f->tau_o = malloc(t->N * sizeof(double));
+    *out = f;
+    return 0;
+}
+
+static int isgn(double v) { return (v > 0) - (v < 0); }
+
+/* FMM.build_expansions (class_fmm.py:299-352), on freshly zeroed workspaces */
+int ork_fmm_apply(OFMM *f, const double *tau)
+{
+    OTree *t = f->t;
+    int L = t->L, Q = f->Q, Q4 = 4 * Q;
+    for (int64_t i = 0; i < t->N; i++) f->tau_o[i] = tau[t->ordv[i]];
+    for (int l = 1; l < L; l++) {
+        memset(f->chk[l], 0, (size_t)t->lv[l].n_alloc * Q * sizeof(double));
+        memset(f->ls[l], 0, (size_t)t->lv[l].n * Q * sizeof(double));
+    }
+    /* upward pass */
+    for (int l = L - 1; l >= 1; l--) {
+        OLevel *v = &t->lv[l];
+        double *ucs = f->chk[l];
+        if (l != L - 1) {
+            OLevel *a = &t->lv[l + 1];
+            const double *M = f->m2mc[l];
+            /* temp1 = (M2MC @ RSEQD.T).T, then numba_distribute (:11-15) */
+#pragma omp parallel for
+            for (int64_t g = 0; g < a->n / 4; g++) {
+                int64_t di = a->pdi[g];
+                if (di < 0) continue;
+                const double *rs = f->eqd[l + 1] + (size_t)di * Q4;
+                double *dst = ucs + (size_t)v->tdi[a->parent[4 * g]] * Q;
+                for (int r = 0; r < Q; r++) {
+                    double s = 0;
+                    for (int c = 0; c < Q4; c++) s += M[r * Q4 + c] * rs[c];
+                    dst[r] = s;
+                }
+            }
+        }
+        /* numba_upwards_pass (class_fmm.py:57-71) */
+#pragma omp parallel for schedule(dynamic, 8)
+        for (int64_t i = 0; i < v->n; i++) {
+            if (!v->cu[i] || v->tdi[i] < 0) continue;
+            double *u = ucs + (size_t)v->tdi[i] * Q;
+            for (int64_t s = v->bot[i]; s < v->top[i]; s++)
+                for (int q = 0; q < Q; q++)
+                    u[q] += ork_eval(f->kn, t->x[s], t->y[s], f->lx[l][q] + v->xmid[i], f->ly[l][q] + v->ymid[i]) * f->tau_o[s];
+        }
+#pragma omp parallel for
+        for (int64_t i = 0; i < v->n_alloc; i++) {
+            memcpy(f->eqd[l] + (size_t)i * Q, ucs + (size_t)i * Q, Q * sizeof(double));
+            lu_solve(f->e2c[l], f->piv[l], Q, f->eqd[l] + (size_t)i * Q);
+        }
+    }
+    /* downward pass 1 */
+    for (int l = 1; l < L - 1; l++) {
+        OLevel *v = &t->lv[l], *d = &t->lv[l + 1];
+        const double *M = f->m2mc[l];
+#pragma omp parallel for
+        for (int64_t i = 0; i < v->n; i++) {
+            int doit = (!v->leaf[i] || v->xlist[i]) && !v->fake[i];
+            if (!doit) continue;
+            double le[256], o;
+            memcpy(le, f->ls[l] + (size_t)i * Q, Q * sizeof(double));
+            lu_solve(f->e2c[l], f->piv[l], Q, le);
+            for (int c = 0; c < Q4; c++) {
+                o = 0;
+                for (int r = 0; r < Q; r++) o += M[r * Q4 + c] * le[r];
+                f->ls[l + 1][(size_t)v->children[i] * Q + c] = o;
+            }
+        }
+        /* M2Ms[d] = CM2L[l+1][d] @ RSEQD.T (class_fmm.py:336-341) */
+        int64_t G = d->n_sib;
+        double *M2Ms = malloc((size_t)9 * Q4 * (G ? G : 1) * sizeof(double));
+        const double *CM = f->cm2l[l + 1];
+#pragma omp parallel for collapse(2)
+        for (int dir = 0; dir < 9; dir++)
+            for (int64_t g = 0; g < G; g++) {
+                if (dir == 4) continue;
+                const double *C = CM + (size_t)dir * Q4 * Q4;
+                const double *rs = f->eqd[l + 1] + (size_t)g * Q4;
+                double *o = M2Ms + ((size_t)dir * G + g) * Q4;
+                for (int r = 0; r < Q4; r++) {
+                    double s = 0;
+                    for (int c = 0; c < Q4; c++) s += C[(size_t)r * Q4 + c] * rs[c];
+                    o[r] = s;
+                }
+            }
+        /* numba_add_interactions (class_fmm.py:17-33); ci4 = trunc(children/4) */
+#pragma omp parallel for
+        for (int64_t i = 0; i < v->n; i++) {
+            int doit = (!v->leaf[i] || v->xlist[i]) && !v->fake[i];
+            if (!doit) continue;
+            int64_t dii = v->children[i] / 4;
+            for (int j = 0; j < 9; j++) {
+                int64_t ci = v->coll[9 * i + j];
+                if (ci < 0 || ci == i) continue;
+                int xd = isgn(v->xmid[ci] - v->xmid[i]), yd = isgn(v->ymid[ci] - v->ymid[i]);
+                int64_t di = d->pdi[v->children[ci] / 4];
+                if (di < 0) continue;
+                const double *src = M2Ms + ((size_t)((xd + 1) * 3 + (yd + 1)) * G + di) * Q4;
+                for (int k = 0; k < 4; k++)
+                    for (int q = 0; q < Q; q++) f->ls[l + 1][(size_t)(4 * dii + k) * Q + q] += src[k * Q + q];
+            }
+        }
+        free(M2Ms);
+    }
+    /* downward pass 2a */
+    for (int l = 1; l < L; l++) {
+        OLevel *v = &t->lv[l];
+#pragma omp parallel for
+        for (int64_t i = 0; i < v->n; i++) {
+            memcpy(f->le[l] + (size_t)i * Q, f->ls[l] + (size_t)i * Q, Q * sizeof(double));
+            lu_solve(f->e2c[l], f->piv[l], Q, f->le[l] + (size_t)i * Q);
+        }
+    }
+    return 0;
+}
+
+/* FMM.evaluate_to_points (class_fmm.py:379-399): L2P (:73-88) then P2P (:90-111) */
+int ork_fmm_eval(const OFMM *f, const double *x, const double *y, int64_t n, int check, double *pot)
+{
+    const OTree *t = f->t;
+    int Q = f->Q;
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t p = 0; p < n; p++) {
+        int l; int64_t i;
+        double px = x[p], py = y[p];
+        locate1(t, px, py, &l, &i);
+        const OLevel *v = &t->lv[l];
+        double acc = 0.0;
+        if (l > 0) {
+            double tx = px - v->xmid[i], ty = py - v->ymid[i];
+            const double *e = f->le[l] + (size_t)i * Q;
+            for (int q = 0; q < Q; q++) acc += ork_eval(f->kn, f->lx[l][q], f->ly[l][q], tx, ty) * e[q];
+        }
+        for (int j = 0; j < 9; j++) {
+            int64_t ci = v->coll[9 * i + j];
+            if (ci < 0) continue;
+            for (int64_t s = v->bot[ci]; s < v->top[ci]; s++) {
+                if (check && px - t->x[s] == 0 && py - t->y[s] == 0) continue;
+                acc += ork_eval(f->kn, t->x[s], t->y[s], px, py) * f->tau_o[s];
+            }
+        }
+        pot[p] = acc;
+    }
+    return 0;
+}
+
+/* The reference's KAS (class_fmm.py:134-143) for selected targets: FP64
+ * direct sum over all sources, skipping only the pair i == j. */
+void ork_direct(int kind, double k, const double *x, const double *y, const double *tau, int64_t n,
+                const int64_t *tgt, int64_t nt, double *out)
+{
+    OKern kn = {kind, k};
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int64_t a = 0; a < nt; a++) {
+        int64_t j = tgt[a];
+        double s = 0.0;
+        for (int64_t i = 0; i < n; i++)
+            if (i != j) s += ork_eval(kn, x[i], y[i], x[j], y[j]) * tau[i];
+        out[a] = s;
+    }
+}
+
+double ork_k0_value(double x) { return ork_k0(x); }
+void ork_set_threads(int n) { if (n > 0) omp_set_num_threads(n); }
+int ork_max_threads(void) { return omp_get_max_threads(); }

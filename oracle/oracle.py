@@ -1,0 +1,154 @@
+"""ctypes wrapper of the C oracle (``kifmm_oracle.c``).
+
+TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()``
+and the CPU-baseline leg of ``bench.py`` as the checker.  The product
+(``pykifmm2d_b200``) never imports it.
+
+The oracle restates the reference's ``class_fmm.FMM`` pipeline
+(pykifmm2d/class_fmm.py:166-402 over pykifmm2d/tree.py:460-727) in C with
+OpenMP; ``OracleFMM`` mirrors the reference's method names.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "libkifmm_oracle.so")
+_lib = None
+
+_d = ctypes.POINTER(ctypes.c_double)
+_i64 = ctypes.POINTER(ctypes.c_int64)
+_vp = ctypes.c_void_p
+
+
+def build():
+    """Compile the oracle library in place (gcc + OpenMP)."""
+    subprocess.check_call(["make", "-s", "-C", _HERE])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        src = os.path.join(_HERE, "kifmm_oracle.c")
+        if not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(src):
+            build()
+        L = ctypes.CDLL(_LIB)
+        L.ork_tree_build.argtypes = [_d, _d, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.POINTER(_vp)]
+        L.ork_tree_build.restype = ctypes.c_int
+        L.ork_tree_levels.argtypes = [_vp]
+        L.ork_tree_levels.restype = ctypes.c_int
+        L.ork_tree_num_nodes.argtypes = [_vp]
+        L.ork_tree_num_nodes.restype = ctypes.c_int64
+        L.ork_tree_export.argtypes = [_vp, _i64, _d]
+        L.ork_locate.argtypes = [_vp, _d, _d, ctypes.c_int64, _i64]
+        L.ork_tree_free.argtypes = [_vp]
+        L.ork_fmm_create.argtypes = [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(_vp)]
+        L.ork_fmm_create.restype = ctypes.c_int
+        L.ork_fmm_apply.argtypes = [_vp, _d]
+        L.ork_fmm_eval.argtypes = [_vp, _d, _d, ctypes.c_int64, ctypes.c_int, _d]
+        L.ork_fmm_free.argtypes = [_vp]
+        L.ork_direct.argtypes = [ctypes.c_int, ctypes.c_double, _d, _d, _d, ctypes.c_int64, _i64, ctypes.c_int64, _d]
+        L.ork_k0_value.argtypes = [ctypes.c_double]
+        L.ork_k0_value.restype = ctypes.c_double
+        L.ork_set_threads.argtypes = [ctypes.c_int]
+        L.ork_max_threads.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a, t=_d):
+    return a.ctypes.data_as(t)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def set_threads(n):
+    lib().ork_set_threads(int(n))
+
+
+def max_threads():
+    return lib().ork_max_threads()
+
+
+def k0(x):
+    return np.array([lib().ork_k0_value(float(v)) for v in np.ravel(x)])
+
+
+class OracleTree:
+    """Tree(x, y, ppl) of the reference (tree.py:464-522)."""
+
+    def __init__(self, x, y, ppl, fix_bbox=False):
+        self.x = _f64(x)
+        self.y = _f64(y)
+        h = _vp()
+        rc = lib().ork_tree_build(_p(self.x), _p(self.y), self.x.size, int(ppl), int(fix_bbox), ctypes.byref(h))
+        if rc:
+            raise ValueError(f"oracle tree build failed (code {rc})")
+        self.h = h
+        self.levels = lib().ork_tree_levels(h)
+
+    def export(self):
+        n = lib().ork_tree_num_nodes(self.h)
+        nodes = np.zeros((n, 7), dtype=np.int64)
+        root = np.zeros(2)
+        lib().ork_tree_export(self.h, _p(nodes, _i64), _p(root))
+        order = np.lexsort((nodes[:, 2], nodes[:, 1], nodes[:, 0]))
+        return nodes[order], root
+
+    def locate(self, x, y):
+        x = _f64(x)
+        y = _f64(y)
+        out = np.zeros((x.size, 3), dtype=np.int64)
+        lib().ork_locate(self.h, _p(x), _p(y), x.size, _p(out, _i64))
+        return out
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().ork_tree_free(self.h)
+            self.h = None
+
+
+KERNEL_LAPLACE = 0
+KERNEL_K0 = 1
+
+
+class OracleFMM:
+    """Mirror of the reference's FMM (class_fmm.py:166-402) on the C oracle."""
+
+    def __init__(self, x, y, kernel=KERNEL_LAPLACE, k=0.0, Nequiv=48, Ncutoff=50, fix_bbox=False):
+        self.tree = OracleTree(x, y, Ncutoff, fix_bbox)
+        h = _vp()
+        rc = lib().ork_fmm_create(self.tree.h, int(kernel), float(k), int(Nequiv), ctypes.byref(h))
+        if rc:
+            raise ValueError(f"oracle precompute failed (code {rc})")
+        self.h = h
+
+    def build_expansions(self, tau):
+        self.tau = _f64(tau)
+        lib().ork_fmm_apply(self.h, _p(self.tau))
+
+    def evaluate_to_points(self, x, y, check_self=False):
+        x = _f64(x)
+        y = _f64(y)
+        pot = np.zeros(x.size)
+        lib().ork_fmm_eval(self.h, _p(x), _p(y), x.size, int(bool(check_self)), _p(pot))
+        return pot
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().ork_fmm_free(self.h)
+            self.h = None
+
+
+def direct(x, y, tau, targets, kernel=KERNEL_LAPLACE, k=0.0):
+    """FP64 direct sum at selected targets, skipping only i == j (the KAS of
+    class_fmm.py:134-143)."""
+    x, y, tau = _f64(x), _f64(y), _f64(tau)
+    t = np.ascontiguousarray(targets, dtype=np.int64)
+    out = np.zeros(t.size)
+    lib().ork_direct(int(kernel), float(k), _p(x), _p(y), _p(tau), x.size, _p(t, _i64), t.size, _p(out))
+    return out
