@@ -1,0 +1,464 @@
+#!/usr/bin/env python
+"""Headline benchmark: adaptive Laplace KIFMM throughput at N = 1M.
+
+Workload (default --config c2): 1,000,000 points from a mixture of 16
+isotropic Gaussians (sigma log-uniform in [1e-3, 1e-1], centres uniform in
+[-1, 1]^2) plus 20 % of the points on the unit circle, charges N(0, 1),
+Nequiv = 32, Ncutoff = 64, Laplace kernel, seeded synthetic data.
+
+A step is the whole FMM on one point set, as the reference's FMM class runs it:
+build_tree + precompute + build_expansions(tau) + evaluate_to_points(x, y, True).
+`value` is Mpts/s with the inputs already in HBM (device pointers through the
+C ABI); `e2e` is the same step through the public Python API with pinned host
+buffers, host->device and device->host copies inside the timed region.
+The relative error max|u - u_ref| / max|u_ref| is measured against an FP64
+direct sum at 4,096 seeded sample targets.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+Under torchrun every rank runs an independent replica (the FMM does not shard);
+value = all points processed / max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "Laplace FMM Mpts/s at N=1M, mixed vs plain at 1e-7 rel err; p50/p99 latency"
+L2_FLUSH_BYTES = 256 << 20
+
+
+# ------------------------------------------------------------ generators
+def gen_uniform(n, seed):
+    rng = np.random.default_rng(seed)
+    return rng.uniform(-1, 1, n), rng.uniform(-1, 1, n), rng.standard_normal(n)
+
+
+def gen_mixture(n, seed):
+    rng = np.random.default_rng(seed)
+    nc = int(0.2 * n)
+    ng = n - nc
+    th = rng.uniform(0, 2 * np.pi, nc)
+    cx = rng.uniform(-1, 1, 16)
+    cy = rng.uniform(-1, 1, 16)
+    sig = 10 ** rng.uniform(-3, -1, 16)
+    lab = rng.integers(0, 16, ng)
+    x = np.concatenate([cx[lab] + sig[lab] * rng.standard_normal(ng), np.cos(th)])
+    y = np.concatenate([cy[lab] + sig[lab] * rng.standard_normal(ng), np.sin(th)])
+    return x, y, rng.standard_normal(n)
+
+
+def gen_annulus(n, seed):
+    rng = np.random.default_rng(seed)
+    r = np.sqrt(rng.uniform(0.25, 1, n))
+    th = rng.uniform(0, 2 * np.pi, n)
+    return r * np.cos(th), r * np.sin(th), rng.uniform(-1, 1, n)
+
+
+CONFIGS = {
+    "c1": dict(desc="uniform [-1,1]^2, N=20k, Nequiv 24, Ncutoff 64", gen=gen_uniform, n=20_000, neq=24, cut=64,
+               kernel=0, k=0.0),
+    "c2": dict(desc="Gaussian mixture + 20% unit circle, N=1M, Nequiv 32, Ncutoff 64", gen=gen_mixture,
+               n=1_000_000, neq=32, cut=64, kernel=0, k=0.0),
+    "c3": dict(desc="uniform [-1,1]^2, N=4M, Nequiv 32, Ncutoff 64", gen=gen_uniform, n=4_000_000, neq=32, cut=64,
+               kernel=0, k=0.0),
+    "c4": dict(desc="annulus 0.5<r<1, N=2M, K0 k=10, Nequiv 40, Ncutoff 48", gen=gen_annulus, n=2_000_000, neq=40,
+               cut=48, kernel=1, k=10.0),
+}
+
+
+def kernel_obj(cfg):
+    import pykifmm2d_b200 as P
+    return P.LaplaceKernel() if cfg["kernel"] == 0 else P.ModifiedHelmholtzKernel(cfg["k"])
+
+
+def make_fmm(cfg, x, y, precision, stream=None):
+    import pykifmm2d_b200 as P
+    kern = kernel_obj(cfg)
+    return P.FMM(x, y, P.Get_Kernel_Functions(kern), P.prepare_numba_functions_on_the_fly(kern), cfg["neq"],
+                 cfg["cut"], precision=precision, stream=stream)
+
+
+def sample_targets(n):
+    return np.random.default_rng(123).choice(n, min(n, 4096), replace=False)
+
+
+# --------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            p = [v.strip() for v in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx.append(float(p[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ------------------------------------------------------------- our arm
+def flush_l2(torch, buf):
+    buf.zero_()
+
+
+def time_full_steps(torch, cfg, xd, yd, td, precision, steps, warmup, flush, profile=False):
+    """Full pipeline on device-resident inputs; returns per-step ms (CUDA events)."""
+    from pykifmm2d_b200 import _lib as B
+    stream = torch.cuda.current_stream()
+    f = make_fmm(cfg, xd, yd, precision, stream=stream.cuda_stream)
+    out = torch.empty_like(xd)
+    lib = B.load()
+    times = []
+    launches = 0
+    phase = np.zeros(len(B.PHASES))
+    for it in range(warmup + steps):
+        timed = it >= warmup
+        flush_l2(torch, flush)
+        if timed and profile:
+            lib.kifmm_set_profiling(f._plan, 1)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        l0 = lib.kifmm_launch_count()
+        a.record(stream)
+        f.build_tree()
+        f.precompute()
+        f.build_expansions(td)
+        f.evaluate_to_points(xd, yd, True, out=out)
+        b.record(stream)
+        torch.cuda.synchronize()
+        if timed:
+            times.append(a.elapsed_time(b))
+            launches += lib.kifmm_launch_count() - l0
+            if profile:
+                ms = np.zeros(len(B.PHASES))
+                lib.kifmm_get_phase_times(f._plan, ms.ctypes.data, None, 1)
+                lib.kifmm_set_profiling(f._plan, 0)
+                phase += ms
+    return times, launches, phase / max(steps, 1), f, out
+
+
+def time_apply_steps(torch, f, xd, yd, td, steps, warmup, flush):
+    stream = torch.cuda.current_stream()
+    out = torch.empty_like(xd)
+    times = []
+    for it in range(warmup + steps):
+        flush_l2(torch, flush)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        f.build_expansions(td)
+        f.evaluate_to_points(xd, yd, True, out=out)
+        b.record(stream)
+        torch.cuda.synchronize()
+        if it >= warmup:
+            times.append(a.elapsed_time(b))
+    return times
+
+
+def time_e2e(torch, cfg, x, y, tau, precision, steps, warmup):
+    """Through the public API with pinned host buffers (copies in the timed region)."""
+    xp = torch.from_numpy(x).pin_memory()
+    yp = torch.from_numpy(y).pin_memory()
+    tp = torch.from_numpy(tau).pin_memory()
+    outp = torch.empty(x.size, dtype=torch.float64).pin_memory()
+    times = []
+    for it in range(warmup + steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        f = make_fmm(cfg, xp, yp, precision)
+        f.build_tree()
+        f.precompute()
+        f.build_expansions(tp)
+        f.evaluate_to_points(xp, yp, True, out=outp)
+        t1 = time.perf_counter()
+        del f
+        if it >= warmup:
+            times.append((t1 - t0) * 1e3)
+    return times, outp.numpy().copy()
+
+
+def rel_err(pot, ref, idx):
+    return float(np.abs(pot[idx] - ref).max() / np.abs(ref).max())
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            d = json.load(fh)
+        return d, "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+def p2p_flops_per_pair(kernel):
+    # Laplace: 2 sub, 2 mul/fma for r^2, 1 lg2, 1 fma = 8 flops per pair (SURVEY-style count)
+    return 8.0 if kernel == 0 else 40.0
+
+
+def run_ours(args, cfg, rank, world, dist):
+    import torch
+    from pykifmm2d_b200 import _lib as B
+    dev = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(dev)
+    x, y, tau = cfg["gen"](cfg["n"], 0)
+    n = x.size
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.from_numpy(y).cuda()
+    td = torch.from_numpy(tau).cuda()
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    precision = args.precision
+    lib = B.load()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    barrier()
+    with ClockSampler(dev) as clk:
+        times, launches, phase, f, out = time_full_steps(torch, cfg, xd, yd, td, precision, args.steps, args.warmup,
+                                                         flush, profile=True)
+    barrier()
+    clocks = clk.summary()
+    tot = float(sum(times))
+    if dist is not None:
+        t = torch.tensor([tot], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        tot = float(t.item())
+    ms_step = tot / len(times)
+    value = world * n / (ms_step * 1e-3) / 1e6
+    info = f.tree_info()
+    res = {}
+    if rank == 0:
+        # accuracy against the FP64 direct sum on the GPU (KAS)
+        idx = sample_targets(n)
+        import pykifmm2d_b200 as P
+        KF, KA, KAS = P.Get_Kernel_Functions(kernel_obj(cfg))
+        ref = np.zeros(idx.size)
+        KAS(x, y, tau, ref, targets=idx)
+        pot = out.cpu().numpy()
+        res["err"] = rel_err(pot, ref, idx)
+        # apply-only (tree and operators reused, repeated densities)
+        at = time_apply_steps(torch, f, xd, yd, td, max(3, args.steps // 2), 2, flush)
+        res["apply_ms"] = statistics.mean(at)
+        # plain FP64 form for the mixed-vs-plain comparison
+        if precision != "fp64":
+            pt, _, _, fp, outp = time_full_steps(torch, cfg, xd, yd, td, "fp64", max(3, args.steps // 2), 2, flush)
+            res["plain_ms"] = statistics.mean(pt)
+            res["plain_err"] = rel_err(outp.cpu().numpy(), ref, idx)
+            res["plain_apply_ms"] = statistics.mean(time_apply_steps(torch, fp, xd, yd, td, 3, 1, flush))
+            del fp
+        else:
+            res["plain_ms"], res["plain_err"], res["plain_apply_ms"] = ms_step, res["err"], res["apply_ms"]
+        e2e_t, e2e_pot = time_e2e(torch, cfg, x, y, tau, precision, max(3, args.steps // 2), 2)
+        res["e2e_ms"] = statistics.mean(e2e_t)
+        res["e2e_err"] = rel_err(e2e_pot, ref, idx)
+    if rank != 0:
+        return None
+    pk, pk_src = peaks()
+    # roofline of the dominant phase
+    names = B.PHASES
+    dom = int(np.argmax(phase[[0, 2, 3, 4, 5, 6]]))
+    dom = [0, 2, 3, 4, 5, 6][dom]
+    roof = None
+    if names[dom] == "leaf":
+        pairs = info.n_p2p_pairs
+        flops = pairs * p2p_flops_per_pair(cfg["kernel"]) + n * cfg["neq"] * (p2p_flops_per_pair(cfg["kernel"]) + 2)
+        fp32_peak = 148 * 128 * 2 * pk.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+        fp64_peak = fp32_peak / 2
+        peak = fp32_peak if precision == "mixed" else fp64_peak
+        ach = flops / (phase[dom] * 1e-3) / 1e12
+        roof = {"kernel": "k_leaf_eval (L2P+P2P)", "bound": "fp32" if precision == "mixed" else "fp64",
+                "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
+                "peak_source": f"nominal SIMT peak at sm_max_mhz of MEASURED_PEAKS.json ({pk_src})",
+                "work": f"{pairs:.4g} P2P pairs x {p2p_flops_per_pair(cfg['kernel'])} flops + L2P"}
+    elif names[dom] == "tree":
+        byts = 52.0 * n
+        ach = byts / (phase[1] * 1e-3) / 1e9 if phase[1] > 0 else 0.0
+        roof = {"kernel": "radix sort (Morton keys)", "bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"],
+                "unit": "GB/s", "frac": ach / pk["hbm_gbs"], "traffic": None, "peak_source": pk_src}
+    else:
+        roof = {"kernel": names[dom], "bound": "tensor" if names[dom] == "m2l" else "hbm", "achieved": None,
+                "peak": None, "unit": None, "frac": None, "traffic": None}
+    line = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "Mpts/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_step,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if precision == "fp64" else "f32+f64",
+        "data": "synthetic (seeded generator, seed 0)",
+        "config": {"workload": cfg["desc"], "n_points": n, "kernel": "laplace" if cfg["kernel"] == 0 else "k0",
+                   "nequiv": cfg["neq"], "ncutoff": cfg["cut"], "precision": precision,
+                   "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) before every timed step",
+                   "step": "build_tree + precompute + build_expansions + evaluate_to_points(check_self)"},
+        "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99))},
+        "rel_err": res["err"],
+        "plain_fp64": {"ms_per_step": res["plain_ms"], "mpts_s": n / (res["plain_ms"] * 1e-3) / 1e6,
+                       "rel_err": res["plain_err"], "apply_ms": res["plain_apply_ms"]},
+        "apply_only": {"ms": res["apply_ms"], "mpts_s": n / (res["apply_ms"] * 1e-3) / 1e6},
+        "phases_ms": {nm: float(v) for nm, v in zip(names, phase)},
+        "tree": {"levels": info.levels, "nodes": info.n_nodes, "leaves": info.n_leaves, "outside_root": info.n_outside,
+                 "p2p_pairs": info.n_p2p_pairs},
+        "roofline": roof,
+        "e2e": {"value": n / (res["e2e_ms"] * 1e-3) / 1e6, "unit": "Mpts/s",
+                "h2d_bytes_per_step": 3 * 8 * n, "d2h_bytes_per_step": 8 * n, "ms_per_step": res["e2e_ms"],
+                "rel_err": res["e2e_err"]},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cfg, x, y, tau, repeats=3)
+    return line
+
+
+# ------------------------------------------------------- CPU baseline
+def cpu_baseline(cfg, x, y, tau, repeats=3, threads=None):
+    """The oracle (C restatement of the reference, OpenMP) on the host cores."""
+    from oracle import oracle as O
+    nthr = threads or os.cpu_count()
+    O.set_threads(nthr)
+    ts = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        f = O.OracleFMM(x, y, cfg["kernel"], cfg["k"], cfg["neq"], cfg["cut"])
+        f.build_expansions(tau)
+        f.evaluate_to_points(x, y, True)
+        ts.append(time.perf_counter() - t0)
+        del f
+    med = statistics.median(ts)
+    cpu = ""
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                cpu = line.split(":", 1)[1].strip()
+                break
+    except Exception:
+        pass
+    return {"value": x.size / med / 1e6, "unit": "Mpts/s", "cores": nthr, "kind": "port",
+            "sample": f"full workload ({x.size} points), median of {repeats} runs, {med:.2f} s each; CPU: {cpu}"}
+
+
+def run_reference(args, cfg):
+    x, y, tau = cfg["gen"](cfg["n"], 0)
+    from oracle import oracle as O
+    nthr = os.cpu_count()
+    O.set_threads(nthr)
+    ts = []
+    for it in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        f = O.OracleFMM(x, y, cfg["kernel"], cfg["k"], cfg["neq"], cfg["cut"])
+        f.build_expansions(tau)
+        f.evaluate_to_points(x, y, True)
+        dt = time.perf_counter() - t0
+        del f
+        if it >= args.warmup:
+            ts.append(dt)
+    ms = 1e3 * statistics.mean(ts)
+    v = x.size / (ms * 1e-3) / 1e6
+    return {
+        "metric": METRIC, "value": v, "unit": "Mpts/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded generator, seed 0)", "impl": "reference",
+        "config": {"workload": cfg["desc"], "n_points": x.size, "precision": "fp64",
+                   "step": "build_tree + precompute + build_expansions + evaluate_to_points(check_self)"},
+        "latency_ms": {"p50": float(np.percentile(ts, 50)) * 1e3, "p99": float(np.percentile(ts, 99)) * 1e3},
+        "cpu_baseline": {"value": v, "unit": "Mpts/s", "cores": nthr, "kind": "port",
+                         "sample": f"full workload ({x.size} points) per step; the reference is pure Python + "
+                                   "numba, so its algorithm runs as the C/OpenMP restatement in oracle/"},
+        "e2e": {"value": v, "unit": "Mpts/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    cfg = CONFIGS[args.config]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args, cfg)), flush=True)
+        return 0
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        line = run_ours(args, cfg, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,203 @@
+/*
+ * kifmm2d.h -- C ABI of the B200-native 2D kernel-independent FMM.
+ *
+ * The library (pykifmm2d_b200/libkifmm2d.so) replaces the hot path behind the
+ * reference's Python class `FMM` (dbstein/pykifmm2d, pykifmm2d/class_fmm.py)
+ * with hand-written sm_100a CUDA kernels.  Each entry point below names the
+ * reference interface it replaces.  The Python layer pykifmm2d_b200 binds
+ * these symbols with ctypes; other hosts can bind them the same way.
+ *
+ * Conventions
+ *   - Every call returns a kifmm_status; nothing aborts or traps.  The text of
+ *     the last error of the calling thread is kifmm_last_error().
+ *   - `mem` says where a caller buffer lives: KIFMM_MEM_HOST (ordinary or
+ *     pinned host memory; the call returns once the data is consumed or
+ *     written) or KIFMM_MEM_DEVICE (device pointers on the plan's device;
+ *     work is ordered on the plan's stream and the call may return before
+ *     it finishes -- use kifmm_synchronize or the stream).
+ *   - A plan owns its device memory.  The caller owns its input and output
+ *     buffers.  One plan is used from one host thread at a time.
+ */
+#ifndef KIFMM2D_H
+#define KIFMM2D_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    KIFMM_OK = 0,
+    KIFMM_ERR_ARG = 1,        /* invalid argument (null pointer, bad size, NaN input, ...) */
+    KIFMM_ERR_CUDA = 2,       /* a CUDA runtime call failed */
+    KIFMM_ERR_NOMEM = 3,      /* device allocation failed */
+    KIFMM_ERR_DEPTH = 4,      /* tree would need more than KIFMM_MAX_LEVELS levels */
+    KIFMM_ERR_STATE = 5,      /* call out of order (e.g. apply before build_tree) */
+    KIFMM_ERR_RANGE = 6,      /* coordinates out of the exactly representable range */
+    KIFMM_ERR_UNSUPPORTED = 7 /* option not supported by this build */
+} kifmm_status;
+
+enum { KIFMM_MEM_HOST = 0, KIFMM_MEM_DEVICE = 1 };
+
+/* Opaque plan: tree, operators and workspaces of one FMM object. */
+typedef struct kifmm_plan kifmm_plan;
+
+/* Kernel plug-ins.  The reference takes a numba scalar function
+ * Kernel_Eval(sx, sy, tx, ty) (class_fmm.py:55, :115); the two it ships and
+ * benchmarks are the Laplace log kernel (examples/laplace2.py:31-36) and the
+ * modified Helmholtz kernel K0(k r)/(2 pi) (examples/modified_helmholtz.py:38-43). */
+enum { KIFMM_KERNEL_LAPLACE = 0, KIFMM_KERNEL_MOD_HELMHOLTZ = 1 };
+typedef struct kifmm_kernel {
+    int32_t kind;     /* KIFMM_KERNEL_* */
+    int32_t reserved;
+    double k;         /* modified Helmholtz parameter (unused for Laplace) */
+} kifmm_kernel;
+
+/* Arithmetic of the evaluation passes. */
+enum {
+    KIFMM_PREC_FP64 = 0,  /* every pass in FP64 ("plain") */
+    KIFMM_PREC_MIXED = 1  /* FP32 near field and P2M/L2P, compensated M2L */
+};
+/* M2L form used with KIFMM_PREC_MIXED. */
+enum {
+    KIFMM_M2L_AUTO = 0,
+    KIFMM_M2L_FP32 = 1,       /* FP32 FFMA tiles on the CUDA cores */
+    KIFMM_M2L_BF16X3 = 2,     /* tcgen05 kind::f16, bf16 hi/lo, 3 products, FP32 accumulate */
+    KIFMM_M2L_FP16X3 = 3,     /* tcgen05 kind::f16, fp16 hi/lo with scaling, 3 products */
+    KIFMM_M2L_FP64 = 4        /* FP64 tiles (as in KIFMM_PREC_FP64) */
+};
+
+typedef struct kifmm_options {
+    int32_t precision;  /* KIFMM_PREC_* (default FP64) */
+    int32_t m2l;        /* KIFMM_M2L_* (default AUTO) */
+    int32_t fix_bbox;   /* 0 (default): the reference's root box
+                           [floor(min(xmin,ymin)), ceil(max(xmax,ymin))] (tree.py:475-484);
+                           1: use ymax, so every point lies inside the root box */
+    int32_t radii;      /* 0 (default): the reference's circles r1=(sqrt2+0.01)w/2,
+                           r2=(4-sqrt2-0.02)w/2 (class_fmm.py:35-45); 1: 1.5 and 2.5 half-widths */
+    int32_t device;     /* CUDA device ordinal */
+    int32_t reserved;
+    void *stream;       /* cudaStream_t to order work on; NULL: the plan creates its own */
+} kifmm_options;
+
+#define KIFMM_MAX_LEVELS 30
+
+typedef struct kifmm_tree_info {
+    int64_t n_points;
+    int32_t levels;          /* number of levels (reference Tree.levels) */
+    int32_t reserved;
+    int64_t n_nodes;         /* all nodes, fake leaves included */
+    int64_t n_leaves;        /* real leaves (reference Level.leaf summed) */
+    int64_t n_fake;          /* fake leaves made by X-list splits */
+    int64_t n_xlist;         /* X-list leaves */
+    int64_t n_outside;       /* points outside the root box (reference bbox quirk) */
+    double root_min, root_max;
+    int64_t n_p2p_pairs;     /* sum over target leaves of n_t * (points in its colleagues) */
+    int64_t n_p2m_points;    /* source points entering P2M */
+    int64_t n_m2l_pairs;     /* V-list (target box, source box) pairs */
+    int64_t n_m2l_groups;    /* (target sibling group, parent direction) blocks with a source group */
+    int64_t nodes_per_level[KIFMM_MAX_LEVELS];
+} kifmm_tree_info;
+
+/* Fill *o with the defaults listed above. */
+void kifmm_default_options(kifmm_options *o);
+
+/* FMM.__init__(x, y, kernel_functions, numba_functions, Nequiv, Ncutoff)
+ * (class_fmm.py:167-176): a plan for one kernel, Nequiv equivalent/check
+ * points per box and leaf cutoff Ncutoff.  No device work yet. */
+int kifmm_plan_create(const kifmm_kernel *kernel, int32_t nequiv, int32_t ncutoff,
+                      const kifmm_options *opts, kifmm_plan **plan_out);
+
+/* FMM.build_tree() -> Tree(x, y, Ncutoff) (class_fmm.py:177-181, tree.py:464-522):
+ * Morton keys, radix sort, leaf split, level restriction, X-list fake leaves,
+ * colleague lists.  Points are copied; the caller keeps x, y. */
+int kifmm_build_tree(kifmm_plan *plan, const double *x, const double *y, int64_t n, int32_t mem);
+
+/* FMM.precompute() (class_fmm.py:182-298): per-level translation operators
+ * in FP64 on the device, with the check-to-equivalent inverses composed in. */
+int kifmm_precompute(kifmm_plan *plan);
+
+/* FMM.build_expansions(tau) (class_fmm.py:299-352): P2M, M2M, M2L, L2L.
+ * Every call starts from zeroed workspaces (a repeated apply is exact). */
+int kifmm_build_expansions(kifmm_plan *plan, const double *tau, int32_t mem);
+
+/* FMM.evaluate_to_points(x, y, check_self) at the plan's own source points
+ * (class_fmm.py:379-399 with x, y the sources): L2P + P2P.  pot[n] is in
+ * the caller's point order.  check_self skips pairs with equal coordinates
+ * (class_fmm.py:107). */
+int kifmm_evaluate_to_sources(kifmm_plan *plan, double *pot, int32_t check_self, int32_t mem);
+
+/* FMM.evaluate_to_points(x, y, check_self) at arbitrary targets
+ * (class_fmm.py:379-399): locate (tree.py:703-727), L2P, P2P. */
+int kifmm_evaluate_to_points(kifmm_plan *plan, const double *x, const double *y, int64_t n,
+                             int32_t check_self, double *pot, int32_t mem);
+
+/* Wait for all work queued on the plan's stream. */
+int kifmm_synchronize(kifmm_plan *plan);
+
+/* Tree statistics (reference Tree.levels, Level.n_node, ...). */
+int kifmm_get_tree_info(kifmm_plan *plan, kifmm_tree_info *info);
+
+/* Canonical tree for parity checks: nodes[n_nodes][7] = (level, ix, iy,
+ * leaf, fake_leaf, Xlist, ns) with ix = (xmin - root_min)/width, in the same
+ * meaning as the reference's Level arrays (tree.py:313-420); point_leaf[n][3]
+ * = (level, ix, iy) of the leaf holding each point (tree.py:703-727).
+ * Host buffers; either may be NULL. */
+int kifmm_export_tree(kifmm_plan *plan, int64_t *nodes, int64_t *point_leaf);
+
+/* Release the plan and its device memory. */
+int kifmm_plan_destroy(kifmm_plan *plan);
+
+/* Text of the calling thread's last error ("" if none). */
+const char *kifmm_last_error(void);
+
+/* Get_Kernel_Functions(...).KAS (class_fmm.py:134-143), restricted to chosen
+ * targets: FP64 direct sum out[a] = sum_{i != t_a} G(s_i -> s_{t_a}) tau_i.
+ * The O(N^2) oracle of the error metric, on the GPU. */
+int kifmm_direct_sum(const kifmm_kernel *kernel, const double *x, const double *y,
+                     const double *tau, int64_t n, const int64_t *targets, int64_t nt,
+                     double *out, int32_t mem, int32_t device);
+
+/* Get_Kernel_Functions(...).KF (class_fmm.py:116-122) / Kernel_Form
+ * (:147-164): out[j*ns + i] = G(s_i -> t_j), FP64. */
+int kifmm_kernel_matrix(const kifmm_kernel *kernel, const double *sx, const double *sy, int64_t ns,
+                        const double *tx, const double *ty, int64_t nt, double *out,
+                        int32_t mem, int32_t device);
+
+/* Get_Kernel_Functions(...).KA (class_fmm.py:124-132): out[j] =
+ * sum_i G(s_i -> t_j) tau_i, FP64. */
+int kifmm_kernel_apply(const kifmm_kernel *kernel, const double *sx, const double *sy, int64_t ns,
+                       const double *tx, const double *ty, int64_t nt, const double *tau,
+                       double *out, int32_t mem, int32_t device);
+
+/* Phase timers (no counterpart in the reference, which prints wall-clock
+ * phase times when verbose, class_fmm.py:178-181,297-298,320-352).  When
+ * enabled, CUDA events on the plan's stream bracket each phase and the device
+ * milliseconds accumulate per phase id (KIFMM_PHASE_*). */
+enum {
+    KIFMM_PHASE_TREE = 0,      /* whole build_tree */
+    KIFMM_PHASE_SORT = 1,      /* Morton radix sort of the points (inside TREE) */
+    KIFMM_PHASE_PRECOMPUTE = 2,
+    KIFMM_PHASE_P2M = 3,
+    KIFMM_PHASE_M2M = 4,
+    KIFMM_PHASE_M2L = 5,       /* M2L + L2L, all levels */
+    KIFMM_PHASE_LEAF = 6,      /* L2P + P2P at the sources */
+    KIFMM_PHASE_TARGETS = 7,   /* locate + L2P + P2P at separate targets */
+    KIFMM_PHASE_COUNT = 8
+};
+int kifmm_set_profiling(kifmm_plan *plan, int32_t on);
+/* ms[KIFMM_PHASE_COUNT] and launches[KIFMM_PHASE_COUNT] (either may be NULL);
+ * reset != 0 clears the accumulators after reading. */
+int kifmm_get_phase_times(kifmm_plan *plan, double *ms, int64_t *launches, int32_t reset);
+
+/* Number of kernels this library has launched in the process so far. */
+int64_t kifmm_launch_count(void);
+
+/* Library version (major*10000 + minor*100 + patch). */
+int kifmm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* KIFMM2D_H */

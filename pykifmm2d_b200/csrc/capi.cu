@@ -1,0 +1,392 @@
+// capi.cu -- the extern "C" entry points declared in include/kifmm2d.h.
+#include <cstring>
+#include <new>
+
+#include "kifmm_internal.cuh"
+
+namespace kifmm {
+
+static thread_local std::string g_last_error;
+std::atomic<long long> g_launch_count{0};
+thread_local cudaStream_t g_stream = nullptr;
+
+// Keep up to this many bytes of freed blocks cached in the device's default
+// memory pool, so that plans created per point set reuse memory instead of
+// returning it to the driver.
+static const uint64_t kPoolKeepBytes = 8ull << 30;
+static bool g_pool_ready[64] = {};
+static void prepare_pool(int device) {
+    if (device < 0 || device >= 64 || g_pool_ready[device]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = kPoolKeepBytes;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    g_pool_ready[device] = true;
+}
+
+PhaseScope::PhaseScope(kifmm_plan *p, int phase) : P(p), id(phase) {
+    if (!P->profiling) return;
+    l0 = g_launch_count.load();
+    if (cudaEventCreate(&a) == cudaSuccess) cudaEventRecord(a, P->stream);
+    else a = nullptr;
+}
+
+PhaseScope::~PhaseScope() {
+    if (!a) return;
+    cudaEvent_t b = nullptr;
+    if (cudaEventCreate(&b) == cudaSuccess && cudaEventRecord(b, P->stream) == cudaSuccess) {
+        P->pending.push_back(PendingPhase{id, a, b, g_launch_count.load() - l0});
+    } else {
+        cudaEventDestroy(a);
+        if (b) cudaEventDestroy(b);
+    }
+}
+
+static void resolve_phases(kifmm_plan *P) {
+    if (P->pending.empty()) return;
+    KIFMM_CUDA(cudaStreamSynchronize(P->stream));
+    for (auto &ph : P->pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, ph.a, ph.b) == cudaSuccess) P->phase_ms[ph.id] += ms;
+        P->phase_launches[ph.id] += ph.launches;
+        cudaEventDestroy(ph.a);
+        cudaEventDestroy(ph.b);
+    }
+    P->pending.clear();
+}
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+
+template <class F>
+static int guarded(F &&f) {
+    try {
+        g_last_error.clear();
+        f();
+        return KIFMM_OK;
+    } catch (const Fail &e) {
+        return e.code;
+    } catch (const std::bad_alloc &) {
+        set_error("host allocation failed");
+        return KIFMM_ERR_NOMEM;
+    } catch (...) {
+        set_error("unexpected C++ exception");
+        return KIFMM_ERR_CUDA;
+    }
+}
+
+static void use_device(kifmm_plan *P) {
+    KIFMM_CUDA(cudaSetDevice(P->device));
+    g_stream = P->stream;
+}
+
+static void copy_in(kifmm_plan *P, DBuf<double> &dst, const double *src, int64_t n, int mem) {
+    KIFMM_REQUIRE(src || n == 0, KIFMM_ERR_ARG, "null input pointer");
+    KIFMM_REQUIRE(mem == KIFMM_MEM_HOST || mem == KIFMM_MEM_DEVICE, KIFMM_ERR_ARG, "bad mem flag");
+    dst.alloc(n);
+    if (n)
+        KIFMM_CUDA(cudaMemcpyAsync(dst.p, src, n * sizeof(double),
+                                   mem == KIFMM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                                   P->stream));
+}
+
+static void copy_out(kifmm_plan *P, double *dst, const double *src, int64_t n, int mem) {
+    KIFMM_REQUIRE(dst || n == 0, KIFMM_ERR_ARG, "null output pointer");
+    if (n)
+        KIFMM_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double),
+                                   mem == KIFMM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                                   P->stream));
+    if (mem == KIFMM_MEM_HOST) KIFMM_CUDA(cudaStreamSynchronize(P->stream));
+}
+
+static void check_kernel(const kifmm_kernel *k) {
+    KIFMM_REQUIRE(k, KIFMM_ERR_ARG, "null kernel descriptor");
+    KIFMM_REQUIRE(k->kind == KIFMM_KERNEL_LAPLACE || k->kind == KIFMM_KERNEL_MOD_HELMHOLTZ, KIFMM_ERR_ARG,
+                  "unknown kernel kind");
+    KIFMM_REQUIRE(k->kind != KIFMM_KERNEL_MOD_HELMHOLTZ || k->k > 0, KIFMM_ERR_ARG,
+                  "modified Helmholtz needs k > 0");
+}
+
+// Stand-alone kernel-function calls (KF/KA/KAS) run on a temporary stream.
+struct TempCtx {
+    kifmm_plan P;
+    explicit TempCtx(int device) {
+        P.device = device;
+        KIFMM_CUDA(cudaSetDevice(device));
+        KIFMM_CUDA(cudaStreamCreateWithFlags(&P.stream, cudaStreamNonBlocking));
+        P.own_stream = true;
+        g_stream = P.stream;
+    }
+    ~TempCtx() {
+        if (P.stream) cudaStreamDestroy(P.stream);
+    }
+};
+
+}  // namespace kifmm
+
+using namespace kifmm;
+
+extern "C" {
+
+void kifmm_default_options(kifmm_options *o) {
+    if (!o) return;
+    memset(o, 0, sizeof(*o));
+    o->precision = KIFMM_PREC_FP64;
+    o->m2l = KIFMM_M2L_AUTO;
+}
+
+int kifmm_plan_create(const kifmm_kernel *kernel, int32_t nequiv, int32_t ncutoff, const kifmm_options *opts,
+                      kifmm_plan **plan_out) {
+    return guarded([&] {
+        KIFMM_REQUIRE(plan_out, KIFMM_ERR_ARG, "null plan_out");
+        *plan_out = nullptr;
+        check_kernel(kernel);
+        KIFMM_REQUIRE(nequiv >= 4 && nequiv <= 64, KIFMM_ERR_ARG, "Nequiv must be in [4, 64]");
+        KIFMM_REQUIRE(ncutoff >= 1, KIFMM_ERR_ARG, "Ncutoff must be >= 1");
+        kifmm_options o;
+        kifmm_default_options(&o);
+        if (opts) o = *opts;
+        KIFMM_REQUIRE(o.precision == KIFMM_PREC_FP64 || o.precision == KIFMM_PREC_MIXED, KIFMM_ERR_ARG,
+                      "unknown precision");
+        KIFMM_REQUIRE(o.m2l >= KIFMM_M2L_AUTO && o.m2l <= KIFMM_M2L_FP64, KIFMM_ERR_ARG, "unknown M2L form");
+        KIFMM_REQUIRE(o.radii == 0 || o.radii == 1, KIFMM_ERR_ARG, "unknown radii preset");
+        kifmm_plan *P = new kifmm_plan();
+        P->kern = *kernel;
+        P->Q = nequiv;
+        P->ppl = ncutoff;
+        P->opt = o;
+        P->device = o.device;
+        try {
+            KIFMM_CUDA(cudaSetDevice(P->device));
+            int sms = 0;
+            KIFMM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device));
+            P->num_sms = sms > 0 ? sms : 148;
+            prepare_pool(P->device);
+            if (o.stream) {
+                P->stream = (cudaStream_t)o.stream;
+            } else {
+                KIFMM_CUDA(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking));
+                P->own_stream = true;
+            }
+        } catch (...) {
+            delete P;
+            throw;
+        }
+        *plan_out = P;
+    });
+}
+
+int kifmm_build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int32_t mem) {
+    return guarded([&] {
+        KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
+        KIFMM_REQUIRE(mem == KIFMM_MEM_HOST || mem == KIFMM_MEM_DEVICE, KIFMM_ERR_ARG, "bad mem flag");
+        use_device(P);
+        PhaseScope ph(P, KIFMM_PHASE_TREE);
+        build_tree(P, x, y, n, mem);
+    });
+}
+
+int kifmm_precompute(kifmm_plan *P) {
+    return guarded([&] {
+        KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
+        use_device(P);
+        PhaseScope ph(P, KIFMM_PHASE_PRECOMPUTE);
+        build_operators(P);
+    });
+}
+
+int kifmm_build_expansions(kifmm_plan *P, const double *tau, int32_t mem) {
+    return guarded([&] {
+        KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
+        KIFMM_REQUIRE(P->have_ops, KIFMM_ERR_STATE, "build_expansions: call precompute first");
+        use_device(P);
+        P->have_expansions = false;
+        copy_in(P, P->tau, tau, P->N, mem);
+        run_upward_downward(P);
+        P->have_expansions = true;
+    });
+}
+
+int kifmm_evaluate_to_sources(kifmm_plan *P, double *pot, int32_t check_self, int32_t mem) {
+    return guarded([&] {
+        KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
+        KIFMM_REQUIRE(P->have_expansions, KIFMM_ERR_STATE, "evaluate: call build_expansions first");
+        KIFMM_REQUIRE(mem == KIFMM_MEM_HOST || mem == KIFMM_MEM_DEVICE, KIFMM_ERR_ARG, "bad mem flag");
+        use_device(P);
+        run_eval_sources(P, check_self != 0);
+        copy_out(P, pot, P->pot_out.p, P->N, mem);
+    });
+}
+
+int kifmm_evaluate_to_points(kifmm_plan *P, const double *x, const double *y, int64_t n, int32_t check_self,
+                             double *pot, int32_t mem) {
+    return guarded([&] {
+        KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
+        KIFMM_REQUIRE(P->have_expansions, KIFMM_ERR_STATE, "evaluate: call build_expansions first");
+        KIFMM_REQUIRE(n >= 0, KIFMM_ERR_ARG, "negative target count");
+        use_device(P);
+        if (n == 0) return;
+        copy_in(P, P->tx, x, n, mem);
+        copy_in(P, P->ty, y, n, mem);
+        P->tpot.alloc(n);
+        {
+            PhaseScope ph(P, KIFMM_PHASE_TARGETS);
+            run_eval_targets(P, P->tx.p, P->ty.p, n, check_self != 0, P->tpot.p);
+        }
+        copy_out(P, pot, P->tpot.p, n, mem);
+    });
+}
+
+int kifmm_synchronize(kifmm_plan *P) {
+    return guarded([&] {
+        KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
+        use_device(P);
+        KIFMM_CUDA(cudaStreamSynchronize(P->stream));
+    });
+}
+
+int kifmm_get_tree_info(kifmm_plan *P, kifmm_tree_info *info) {
+    return guarded([&] {
+        KIFMM_REQUIRE(P && info, KIFMM_ERR_ARG, "null argument");
+        KIFMM_REQUIRE(P->have_tree, KIFMM_ERR_STATE, "tree_info: no tree");
+        memset(info, 0, sizeof(*info));
+        info->n_points = P->N;
+        info->levels = P->L;
+        info->n_nodes = P->n_nodes;
+        info->n_leaves = P->n_leaves;
+        info->n_fake = P->n_fake;
+        info->n_xlist = P->n_xlist;
+        info->n_outside = P->n_outside;
+        info->root_min = P->root_min;
+        info->root_max = P->root_max;
+        info->n_p2p_pairs = P->n_p2p_pairs;
+        info->n_p2m_points = P->n_p2m_points;
+        info->n_m2l_pairs = P->n_m2l_pairs;
+        info->n_m2l_groups = P->n_m2l_groups;
+        for (int l = 0; l < P->L && l < KIFMM_MAX_LEVELS; l++) info->nodes_per_level[l] = P->lv[l].n;
+    });
+}
+
+int kifmm_export_tree(kifmm_plan *P, int64_t *nodes, int64_t *point_leaf) {
+    return guarded([&] {
+        KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
+        use_device(P);
+        export_tree(P, nodes, point_leaf);
+    });
+}
+
+int kifmm_plan_destroy(kifmm_plan *P) {
+    return guarded([&] {
+        if (!P) return;
+        cudaSetDevice(P->device);
+        g_stream = P->stream;
+        for (auto &ph : P->pending) { cudaEventDestroy(ph.a); cudaEventDestroy(ph.b); }
+        P->pending.clear();
+        cudaStream_t s = P->stream;
+        bool own = P->own_stream;
+        delete P;  // buffers are freed stream-ordered on s
+        if (s) cudaStreamSynchronize(s);
+        if (own && s) cudaStreamDestroy(s);
+    });
+}
+
+const char *kifmm_last_error(void) { return g_last_error.c_str(); }
+
+int kifmm_direct_sum(const kifmm_kernel *kernel, const double *x, const double *y, const double *tau, int64_t n,
+                     const int64_t *targets, int64_t nt, double *out, int32_t mem, int32_t device) {
+    return guarded([&] {
+        check_kernel(kernel);
+        KIFMM_REQUIRE(n > 0 && nt >= 0, KIFMM_ERR_ARG, "bad sizes");
+        TempCtx C(device);
+        kifmm_plan *P = &C.P;
+        DBuf<double> dx, dy, dt, dout;
+        DBuf<int64_t> dtg;
+        const double *px = x, *py = y, *pt = tau;
+        const int64_t *ptg = targets;
+        double *po = out;
+        if (mem == KIFMM_MEM_HOST) {
+            KIFMM_REQUIRE(targets || nt == 0, KIFMM_ERR_ARG, "null targets");
+            for (int64_t a = 0; a < nt; a++)
+                KIFMM_REQUIRE(targets[a] >= 0 && targets[a] < n, KIFMM_ERR_ARG, "target index out of range");
+            copy_in(P, dx, x, n, mem); copy_in(P, dy, y, n, mem); copy_in(P, dt, tau, n, mem);
+            dtg.alloc(nt);
+            KIFMM_CUDA(cudaMemcpyAsync(dtg.p, targets, nt * sizeof(int64_t), cudaMemcpyHostToDevice, P->stream));
+            dout.alloc(nt);
+            px = dx.p; py = dy.p; pt = dt.p; ptg = dtg.p; po = dout.p;
+        }
+        direct_sum_device(*kernel, px, py, pt, n, ptg, nt, po, P->stream);
+        if (mem == KIFMM_MEM_HOST) copy_out(P, out, dout.p, nt, mem);
+        KIFMM_CUDA(cudaStreamSynchronize(P->stream));
+    });
+}
+
+int kifmm_kernel_matrix(const kifmm_kernel *kernel, const double *sx, const double *sy, int64_t ns, const double *tx,
+                        const double *ty, int64_t nt, double *out, int32_t mem, int32_t device) {
+    return guarded([&] {
+        check_kernel(kernel);
+        KIFMM_REQUIRE(ns >= 0 && nt >= 0, KIFMM_ERR_ARG, "bad sizes");
+        TempCtx C(device);
+        kifmm_plan *P = &C.P;
+        DBuf<double> a, b, c, d, o;
+        const double *psx = sx, *psy = sy, *ptx = tx, *pty = ty;
+        double *po = out;
+        if (mem == KIFMM_MEM_HOST) {
+            copy_in(P, a, sx, ns, mem); copy_in(P, b, sy, ns, mem); copy_in(P, c, tx, nt, mem); copy_in(P, d, ty, nt, mem);
+            o.alloc(ns * nt);
+            psx = a.p; psy = b.p; ptx = c.p; pty = d.p; po = o.p;
+        }
+        kernel_matrix_device(*kernel, psx, psy, ns, ptx, pty, nt, po, P->stream);
+        if (mem == KIFMM_MEM_HOST) copy_out(P, out, o.p, ns * nt, mem);
+        KIFMM_CUDA(cudaStreamSynchronize(P->stream));
+    });
+}
+
+int kifmm_kernel_apply(const kifmm_kernel *kernel, const double *sx, const double *sy, int64_t ns, const double *tx,
+                       const double *ty, int64_t nt, const double *tau, double *out, int32_t mem, int32_t device) {
+    return guarded([&] {
+        check_kernel(kernel);
+        KIFMM_REQUIRE(ns >= 0 && nt >= 0, KIFMM_ERR_ARG, "bad sizes");
+        TempCtx C(device);
+        kifmm_plan *P = &C.P;
+        DBuf<double> a, b, c, d, t, o;
+        const double *psx = sx, *psy = sy, *ptx = tx, *pty = ty, *pt = tau;
+        double *po = out;
+        if (mem == KIFMM_MEM_HOST) {
+            copy_in(P, a, sx, ns, mem); copy_in(P, b, sy, ns, mem); copy_in(P, c, tx, nt, mem);
+            copy_in(P, d, ty, nt, mem); copy_in(P, t, tau, ns, mem);
+            o.alloc(nt);
+            psx = a.p; psy = b.p; ptx = c.p; pty = d.p; pt = t.p; po = o.p;
+        }
+        kernel_apply_device(*kernel, psx, psy, ns, ptx, pty, nt, pt, po, P->stream);
+        if (mem == KIFMM_MEM_HOST) copy_out(P, out, o.p, nt, mem);
+        KIFMM_CUDA(cudaStreamSynchronize(P->stream));
+    });
+}
+
+int kifmm_set_profiling(kifmm_plan *P, int32_t on) {
+    return guarded([&] {
+        KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
+        use_device(P);
+        resolve_phases(P);
+        P->profiling = on != 0;
+    });
+}
+
+int kifmm_get_phase_times(kifmm_plan *P, double *ms, int64_t *launches, int32_t reset) {
+    return guarded([&] {
+        KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
+        use_device(P);
+        resolve_phases(P);
+        for (int i = 0; i < KIFMM_PHASE_COUNT; i++) {
+            if (ms) ms[i] = P->phase_ms[i];
+            if (launches) launches[i] = P->phase_launches[i];
+            if (reset) { P->phase_ms[i] = 0; P->phase_launches[i] = 0; }
+        }
+    });
+}
+
+int64_t kifmm_launch_count(void) { return g_launch_count.load(); }
+
+int kifmm_version(void) { return 100; }
+
+}  // extern "C"

@@ -1,0 +1,319 @@
+// kifmm_internal.cuh -- shared definitions of the sm_100a KIFMM library.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <atomic>
+#include <string>
+#include <vector>
+
+#include "../../include/kifmm2d.h"
+
+// ----------------------------------------------------------------- errors
+namespace kifmm {
+
+void set_error(const std::string &msg);
+
+struct Fail {
+    int code;
+};
+
+#define KIFMM_CUDA(call)                                                            \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess) {                                                    \
+            kifmm::set_error(std::string(#call) + ": " + cudaGetErrorString(e_));  \
+            throw kifmm::Fail{e_ == cudaErrorMemoryAllocation ? KIFMM_ERR_NOMEM     \
+                                                              : KIFMM_ERR_CUDA};    \
+        }                                                                           \
+    } while (0)
+
+#define KIFMM_REQUIRE(cond, code, msg)          \
+    do {                                        \
+        if (!(cond)) {                          \
+            kifmm::set_error(msg);              \
+            throw kifmm::Fail{code};            \
+        }                                       \
+    } while (0)
+
+// Kernels launched by this library in the process (kifmm_launch_count).
+extern std::atomic<long long> g_launch_count;
+
+// Launch check: configuration errors surface at once, faults at the next sync.
+#define KIFMM_LAUNCHED()                                                  \
+    do {                                                                  \
+        kifmm::g_launch_count.fetch_add(1, std::memory_order_relaxed);    \
+        KIFMM_CUDA(cudaGetLastError());                                   \
+    } while (0)
+
+// ---------------------------------------------------------- device buffers
+// Stream on which the current entry point orders its work; device buffers
+// are allocated and freed stream-ordered on it (cudaMallocAsync from the
+// device's default pool, which keeps freed blocks cached, see capi.cu).
+extern thread_local cudaStream_t g_stream;
+
+// A device allocation owned by a plan (freed by the plan's destructor).
+template <class T>
+struct DBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    cudaStream_t s = nullptr;
+    void alloc(size_t count) {
+        if (count <= n && p) return;
+        release();
+        void *q = nullptr;
+        KIFMM_CUDA(cudaMallocAsync(&q, (count ? count : 1) * sizeof(T), g_stream));
+        p = (T *)q;
+        n = count;
+        s = g_stream;
+    }
+    void release() {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+        n = 0;
+    }
+    ~DBuf() { release(); }
+    DBuf() = default;
+    DBuf(const DBuf &) = delete;
+    DBuf &operator=(const DBuf &) = delete;
+};
+
+// ---------------------------------------------------------- tree constants
+// Points are keyed on a 2^D x 2^D grid over the root box; a level-l cell key
+// is the top 2l bits of the 2D-bit Morton key (child order (hx, hy) -> 2hx+hy,
+// the reference's (lo-x,lo-y), (lo-x,hi-y), (hi-x,lo-y), (hi-x,hi-y), tree.py:170-185).
+constexpr int KEY_DEPTH = 29;
+constexpr int MAX_LEVELS = KIFMM_MAX_LEVELS;  // levels 0..29
+// Split/X-list cell entries: (level << 57) | (cell key << 1) | is_xlist
+constexpr int ENT_LEVEL_SHIFT = 57;
+constexpr uint64_t ENT_EMPTY = ~0ull;
+
+enum NodeFlags : uint8_t {
+    NF_SPLIT = 1,   // real node that has real children (reference: not leaf, not fake)
+    NF_XLIST = 2,   // real leaf split into fake children (reference Level.Xlist)
+    NF_FAKE = 4,    // fake leaf (reference Level.fake_leaf)
+};
+
+struct LevelInfo {
+    int64_t off;    // first global node index of the level
+    int64_t n;      // nodes on the level
+    int64_t eoff;   // first entry (split/X-list cell) of the level in the sorted list
+    int64_t ne;     // entries on the level
+    double width;
+};
+
+// Per-level geometry passed by value to kernels.
+struct LevelTable {
+    int L;
+    int64_t off[MAX_LEVELS + 1];
+    int64_t eoff[MAX_LEVELS + 1];
+    int64_t ne[MAX_LEVELS + 1];
+};
+
+// Operator block of one level (device pointers into Plan::ops).
+struct LevelOps {
+    double *inv;    // [Q x Q]      check -> equivalent (E2C^-1)
+    double *m2m;    // [Q x 4Q]     u_up(parent) = m2m . u_up(children)   (M2MC . Inv_{l+1})
+    double *l2lT;   // [Q x 4Q]     transposed: u_down(children) = l2lT^T . u_down(parent)
+    double *m2lT;   // [8][4Q x 4Q] transposed directional M2L blocks (CM2L . Inv)
+    double *large;  // [2Q]         check-circle offsets (x then y)
+    double *small;  // [2Q]         equivalent-circle offsets
+};
+
+struct PendingPhase {
+    int id;
+    cudaEvent_t a, b;
+    long long launches;
+};
+
+}  // namespace kifmm
+
+// --------------------------------------------------------------- the plan
+struct kifmm_plan {
+    // configuration
+    kifmm_kernel kern{};
+    int Q = 0;            // Nequiv
+    int ppl = 0;          // Ncutoff
+    kifmm_options opt{};
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int device = 0;
+    int num_sms = 148;
+
+    // points
+    int64_t N = 0;
+    double root_min = 0, root_max = 0, W = 0;
+    int64_t n_outside = 0;
+    kifmm::DBuf<double> x, y;        // caller order
+    kifmm::DBuf<double> xs, ys;      // Morton order
+    kifmm::DBuf<uint64_t> pkey;      // sorted point keys
+    kifmm::DBuf<int32_t> perm;       // sorted position -> caller index
+
+    // tree
+    bool have_tree = false;
+    int L = 0;
+    kifmm::LevelInfo lv[kifmm::MAX_LEVELS + 1]{};
+    kifmm::LevelTable lt{};
+    int64_t n_nodes = 0, n_ent = 0;
+    kifmm::DBuf<uint64_t> ent;       // sorted entries
+    kifmm::DBuf<int32_t> ent_node;   // entry -> node
+    kifmm::DBuf<uint64_t> nkey;      // node cell key
+    kifmm::DBuf<int8_t> nlev;        // node level
+    kifmm::DBuf<uint8_t> nflag;      // NodeFlags
+    kifmm::DBuf<int32_t> nbot, ntop; // point range (Morton order)
+    kifmm::DBuf<int32_t> nparent, nchild, nent;  // parent, first child, own entry
+    kifmm::DBuf<int32_t> ncoll;      // [n_nodes][9] colleagues by direction (dx+1)*3+(dy+1)
+    kifmm::DBuf<int32_t> leaf_list, p2m_list;
+    int64_t n_leaf_list = 0, n_p2m_list = 0;
+    int64_t n_leaves = 0, n_fake = 0, n_xlist = 0;
+    int64_t n_p2p_pairs = 0, n_p2m_points = 0, n_m2l_pairs = 0, n_m2l_groups = 0;
+
+    // operators
+    bool have_ops = false;
+    kifmm::DBuf<double> ops, ops_tmp;
+    kifmm::LevelOps lops[kifmm::MAX_LEVELS + 1]{};
+    kifmm::DBuf<float> ops_f;        // FP32 copies for the mixed passes
+    kifmm::DBuf<uint16_t> ops_h;     // split half-precision M2L operators
+    size_t ops_stride = 0;           // doubles per level block
+
+    // workspaces
+    kifmm::DBuf<double> tau, taus, pots, pot_out, tx, ty, tpot;
+    kifmm::DBuf<double> uup, udown;
+    kifmm::DBuf<float> uup_f, udown_f;
+    bool have_expansions = false;
+
+    // scratch for the tree build
+    kifmm::DBuf<uint64_t> key2, hash, list;
+    kifmm::DBuf<int32_t> perm2;
+    kifmm::DBuf<uint32_t> sort_hist;
+    kifmm::DBuf<unsigned long long> scal;  // small device scalars
+    kifmm::DBuf<int64_t> misc;
+
+    // phase timers (kifmm_set_profiling)
+    bool profiling = false;
+    double phase_ms[KIFMM_PHASE_COUNT] = {};
+    int64_t phase_launches[KIFMM_PHASE_COUNT] = {};
+    std::vector<kifmm::PendingPhase> pending;
+};
+
+namespace kifmm {
+// Brackets one phase with CUDA events on the plan's stream when profiling.
+struct PhaseScope {
+    kifmm_plan *P;
+    int id;
+    cudaEvent_t a = nullptr;
+    long long l0 = 0;
+    PhaseScope(kifmm_plan *p, int phase);
+    ~PhaseScope();
+};
+}  // namespace kifmm
+
+// ------------------------------------------------------- kernel functions
+namespace kifmm {
+
+#include "k0_tables.h"
+
+__device__ __forceinline__ double k0_d(double x) {
+    if (x <= 2.0) {
+        double t = x * x, a = K0_I0_D[K0_I0_D_N - 1], b = K0_P_D[K0_P_D_N - 1];
+#pragma unroll
+        for (int i = K0_I0_D_N - 2; i >= 0; i--) a = fma(a, t, K0_I0_D[i]);
+#pragma unroll
+        for (int i = K0_P_D_N - 2; i >= 0; i--) b = fma(b, t, K0_P_D[i]);
+        return b - log(0.5 * x) * a;
+    }
+    double u = 4.0 / x - 1.0, b0 = 0.0, b1 = 0.0, b2;
+#pragma unroll
+    for (int i = K0_CHEB_D_N - 1; i >= 1; i--) {
+        b2 = b1;
+        b1 = b0;
+        b0 = fma(2.0 * u, b1, K0_CHEB_D[i] - b2);
+    }
+    double f = fma(u, b0, K0_CHEB_D[0] - b1);
+    return exp(-x) * rsqrt(x) * f;
+}
+
+__device__ __forceinline__ float k0_f(float x) {
+    if (x <= 2.0f) {
+        float t = x * x, a = K0_I0_F[K0_I0_F_N - 1], b = K0_P_F[K0_P_F_N - 1];
+#pragma unroll
+        for (int i = K0_I0_F_N - 2; i >= 0; i--) a = fmaf(a, t, K0_I0_F[i]);
+#pragma unroll
+        for (int i = K0_P_F_N - 2; i >= 0; i--) b = fmaf(b, t, K0_P_F[i]);
+        return b - logf(0.5f * x) * a;
+    }
+    float u = 4.0f / x - 1.0f, b0 = 0.0f, b1 = 0.0f, b2;
+#pragma unroll
+    for (int i = K0_CHEB_F_N - 1; i >= 1; i--) {
+        b2 = b1;
+        b1 = b0;
+        b0 = fmaf(2.0f * u, b1, K0_CHEB_F[i] - b2);
+    }
+    float f = fmaf(u, b0, K0_CHEB_F[0] - b1);
+    return expf(-x) * rsqrtf(x) * f;
+}
+
+// G(r^2) for the plug-in kernels, FP64: Laplace -log(r^2)/(4 pi), modified
+// Helmholtz K0(k r)/(2 pi).
+__device__ __forceinline__ double green_d(int kind, double k, double r2) {
+    if (kind == KIFMM_KERNEL_LAPLACE) return -0.07957747154594767 * log(r2);
+    return 0.15915494309189535 * k0_d(k * sqrt(r2));
+}
+__device__ __forceinline__ float green_f(int kind, float k, float r2) {
+    if (kind == KIFMM_KERNEL_LAPLACE) return -0.0795774715f * __logf(r2);
+    return 0.159154943f * k0_f(k * sqrtf(r2));
+}
+
+// Morton helpers (interleave with the x bit above the y bit)
+__host__ __device__ __forceinline__ uint64_t spread2(uint64_t v) {
+    v &= 0x00000000FFFFFFFFull;
+    v = (v | (v << 16)) & 0x0000FFFF0000FFFFull;
+    v = (v | (v << 8)) & 0x00FF00FF00FF00FFull;
+    v = (v | (v << 4)) & 0x0F0F0F0F0F0F0F0Full;
+    v = (v | (v << 2)) & 0x3333333333333333ull;
+    v = (v | (v << 1)) & 0x5555555555555555ull;
+    return v;
+}
+__host__ __device__ __forceinline__ uint64_t compact2(uint64_t v) {
+    v &= 0x5555555555555555ull;
+    v = (v | (v >> 1)) & 0x3333333333333333ull;
+    v = (v | (v >> 2)) & 0x0F0F0F0F0F0F0F0Full;
+    v = (v | (v >> 4)) & 0x00FF00FF00FF00FFull;
+    v = (v | (v >> 8)) & 0x0000FFFF0000FFFFull;
+    v = (v | (v >> 16)) & 0x00000000FFFFFFFFull;
+    return v;
+}
+__host__ __device__ __forceinline__ uint64_t morton(uint64_t ix, uint64_t iy) {
+    return (spread2(ix) << 1) | spread2(iy);
+}
+
+// ------------------------------------------------------ host-side helpers
+inline unsigned grid_for(int64_t n, int block, int cap = 1 << 20) {
+    int64_t g = (n + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (unsigned)g;
+}
+
+// tree.cu
+void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int mem);
+void export_tree(kifmm_plan *P, int64_t *nodes, int64_t *point_leaf);
+// operators.cu
+void build_operators(kifmm_plan *P);
+// passes.cu
+void run_upward_downward(kifmm_plan *P);
+void run_eval_sources(kifmm_plan *P, int check_self);
+void run_eval_targets(kifmm_plan *P, const double *tx, const double *ty, int64_t n, int check_self, double *pot);
+void direct_sum_device(const kifmm_kernel &k, const double *x, const double *y, const double *tau, int64_t n,
+                       const int64_t *tg, int64_t nt, double *out, cudaStream_t s);
+void kernel_matrix_device(const kifmm_kernel &k, const double *sx, const double *sy, int64_t ns,
+                          const double *tx, const double *ty, int64_t nt, double *out, cudaStream_t s);
+void kernel_apply_device(const kifmm_kernel &k, const double *sx, const double *sy, int64_t ns,
+                         const double *tx, const double *ty, int64_t nt, const double *tau, double *out,
+                         cudaStream_t s);
+// radix_sort.cu
+void radix_sort_pairs(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_tmp, int64_t n, int bits,
+                      kifmm_plan *P);
+void radix_sort_keys(uint64_t *key, uint64_t *key_tmp, int64_t n, int bits, kifmm_plan *P);
+
+}  // namespace kifmm

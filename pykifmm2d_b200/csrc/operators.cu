@@ -1,0 +1,264 @@
+// operators.cu -- per-level translation operators, built in FP64 on the GPU.
+//
+// Reference: FMM.precompute (pykifmm2d/class_fmm.py:182-298).
+//   equivalent circle r1 = (sqrt2 + 0.01) w/2, check circle r2 = (4 - sqrt2 - 0.02) w/2,
+//   Q points at theta_q = 2 pi q / Q (get_level_information, :35-45, :192);
+//   E2C_l = G(small -> large)  (:213-217, LU-factored there; inverted here);
+//   M2MC_l = G(children's small circles -> parent's large circle)  (:219-235);
+//   M2LS_l[o] = G(small + o w -> small), o in [-3,3]^2 minus the 3x3 block (:237-250);
+//   CM2LS_l[d] = the 4Q x 4Q child-to-child blocks for parent direction d (:252-285).
+// The passes keep check potentials (u) rather than equivalent densities, so
+// the inverse is composed into every operator:
+//   M2M:  u_up(parent)   = sum_q (M2MC_l[:, q] Inv_{l+1}) u_up(child q)
+//   L2L:  u_down(child q) = (M2MC_l[:, q])^T Inv_l u_down(parent)
+//   M2L:  u_down(children of p) += (CM2LS_l[d] blockdiag(Inv_l)) u_up(children of p + d)
+//   L2P:  equivalent density Inv_l u_down, evaluated on the check circle.
+// Operators are stored column-major (element (r, c) at c * rows + r) so that
+// threads owning consecutive rows read consecutive addresses.
+#include <cmath>
+
+#include "kifmm_internal.cuh"
+
+namespace kifmm {
+
+struct OpsArgs {
+    int L, Q, kind;
+    double k;
+    double W;
+    double rf1, rf2;
+    size_t stride;          // doubles per level block
+    double *ops;            // level blocks
+    double *m2ls;           // temp [L][49][Q][Q] (row-major r, t)
+    double *m2mc;           // temp [L][Q][4Q] (row-major)
+    double *poff;           // temp [L][49][Q][Q] = M2LS . Inv (row-major)
+};
+
+// level block layout (offsets in doubles)
+__host__ __device__ inline size_t off_inv(int) { return 0; }
+__host__ __device__ inline size_t off_m2m(int Q) { return (size_t)Q * Q; }
+__host__ __device__ inline size_t off_l2l(int Q) { return (size_t)5 * Q * Q; }
+__host__ __device__ inline size_t off_m2l(int Q) { return (size_t)9 * Q * Q; }
+__host__ __device__ inline size_t off_large(int Q) { return (size_t)153 * Q * Q; }
+__host__ __device__ inline size_t off_small(int Q) { return (size_t)153 * Q * Q + 2 * Q; }
+__host__ __device__ inline size_t ops_stride(int Q) { return ((size_t)153 * Q * Q + 4 * Q + 31) & ~(size_t)31; }
+
+__device__ __forceinline__ double lvl_width(const OpsArgs &A, int l) { return ldexp(A.W, -l); }
+
+__global__ void k_ops_surfaces(OpsArgs A) {
+    int l = blockIdx.x, q = threadIdx.x;
+    if (l >= A.L || q >= A.Q) return;
+    double w = lvl_width(A, l);
+    double r1 = 0.5 * w * A.rf1, r2 = 0.5 * w * A.rf2;
+    double th = q * (2.0 * 3.141592653589793 / A.Q);
+    double c = cos(th), s = sin(th);
+    double *b = A.ops + (size_t)l * A.stride;
+    b[off_large(A.Q) + q] = r2 * c;
+    b[off_large(A.Q) + A.Q + q] = r2 * s;
+    b[off_small(A.Q) + q] = r1 * c;
+    b[off_small(A.Q) + A.Q + q] = r1 * s;
+}
+
+__device__ __forceinline__ double gval(const OpsArgs &A, double sx, double sy, double tx, double ty) {
+    double dx = tx - sx, dy = ty - sy;
+    return green_d(A.kind, A.k, dx * dx + dy * dy);
+}
+
+// Gauss-Jordan with partial pivoting on [E2C | I] for one level per block.
+__global__ void k_ops_inverse(OpsArgs A) {
+    extern __shared__ double sm[];
+    const int Q = A.Q, Q2 = 2 * Q, l = blockIdx.x;
+    if (l < 1 || l >= A.L) return;
+    double *a = sm;                 // Q x 2Q
+    double *fac = sm + Q * Q2;      // Q
+    __shared__ int piv;
+    const double *b = A.ops + (size_t)l * A.stride;
+    const double *lx = b + off_large(Q), *ly = lx + Q, *sx = b + off_small(Q), *sy = sx + Q;
+    for (int e = threadIdx.x; e < Q * Q2; e += blockDim.x) {
+        int r = e / Q2, c = e % Q2;
+        a[e] = c < Q ? gval(A, sx[c], sy[c], lx[r], ly[r]) : (c - Q == r ? 1.0 : 0.0);
+    }
+    __syncthreads();
+    for (int k = 0; k < Q; k++) {
+        if (threadIdx.x < 32) {
+            double best = -1.0;
+            int bi = k;
+            for (int i = k + threadIdx.x; i < Q; i += 32) {
+                double v = fabs(a[i * Q2 + k]);
+                if (v > best) { best = v; bi = i; }
+            }
+            for (int o = 16; o; o >>= 1) {
+                double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+            }
+            if (threadIdx.x == 0) piv = bi;
+        }
+        __syncthreads();
+        int p = piv;
+        if (p != k)
+            for (int c = threadIdx.x; c < Q2; c += blockDim.x) {
+                double t = a[k * Q2 + c]; a[k * Q2 + c] = a[p * Q2 + c]; a[p * Q2 + c] = t;
+            }
+        __syncthreads();
+        double pv = a[k * Q2 + k];
+        for (int i = threadIdx.x; i < Q; i += blockDim.x) fac[i] = a[i * Q2 + k];
+        __syncthreads();
+        for (int c = threadIdx.x; c < Q2; c += blockDim.x) a[k * Q2 + c] /= pv;
+        __syncthreads();
+        for (int e = threadIdx.x; e < Q * Q2; e += blockDim.x) {
+            int r = e / Q2, c = e % Q2;
+            if (r != k) a[e] -= fac[r] * a[k * Q2 + c];
+        }
+        __syncthreads();
+    }
+    double *inv = A.ops + (size_t)l * A.stride + off_inv(Q);  // row-major
+    for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) inv[e] = a[(e / Q) * Q2 + Q + e % Q];
+}
+
+// kernel matrices: M2LS (far offsets) and M2MC, one block per (level, slot)
+__global__ void k_ops_kmats(OpsArgs A) {
+    const int Q = A.Q, l = blockIdx.x, slot = blockIdx.y;  // slot 0..48: M2LS offset, 49: M2MC
+    if (l < 1 || l >= A.L) return;
+    const double *b = A.ops + (size_t)l * A.stride;
+    const double *sx = b + off_small(Q), *sy = sx + Q, *lx = b + off_large(Q), *ly = lx + Q;
+    double w = lvl_width(A, l);
+    if (slot < 49) {
+        int ox = slot / 7 - 3, oy = slot % 7 - 3;
+        if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1) return;
+        double *m = A.m2ls + ((size_t)l * 49 + slot) * Q * Q;
+        for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) {
+            int r = e / Q, t = e % Q;
+            m[e] = gval(A, sx[t] + ox * w, sy[t] + oy * w, sx[r], sy[r]);
+        }
+    } else {
+        if (l + 1 >= A.L) return;
+        const double *b1 = A.ops + (size_t)(l + 1) * A.stride;
+        const double *cx = b1 + off_small(Q), *cy = cx + Q;
+        double hw = 0.5 * lvl_width(A, l + 1);
+        double *m = A.m2mc + (size_t)l * Q * 4 * Q;
+        for (int e = threadIdx.x; e < Q * 4 * Q; e += blockDim.x) {
+            int r = e / (4 * Q), c = e % (4 * Q), qc = c / Q, t = c % Q;
+            double ox = (qc >= 2) ? hw : -hw, oy = (qc & 1) ? hw : -hw;
+            m[e] = gval(A, cx[t] + ox, cy[t] + oy, lx[r], ly[r]);
+        }
+    }
+}
+
+// P_o = M2LS_o . Inv_l (far offsets), M2M and L2L compositions
+__global__ void k_ops_compose(OpsArgs A) {
+    const int Q = A.Q, l = blockIdx.x, slot = blockIdx.y;  // 0..48 offsets, 49 M2M, 50 L2L
+    if (l < 1 || l >= A.L) return;
+    double *b = A.ops + (size_t)l * A.stride;
+    const double *inv = b + off_inv(Q);
+    if (slot < 49) {
+        int ox = slot / 7 - 3, oy = slot % 7 - 3;
+        if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1) return;
+        const double *m = A.m2ls + ((size_t)l * 49 + slot) * Q * Q;
+        double *p = A.poff + ((size_t)l * 49 + slot) * Q * Q;
+        for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) {
+            int r = e / Q, c = e % Q;
+            double s = 0;
+            for (int t = 0; t < Q; t++) s = fma(m[r * Q + t], inv[t * Q + c], s);
+            p[e] = s;
+        }
+    } else if (slot == 49) {
+        if (l + 1 >= A.L) return;
+        const double *inv1 = A.ops + (size_t)(l + 1) * A.stride + off_inv(Q);
+        const double *m = A.m2mc + (size_t)l * Q * 4 * Q;
+        double *o = b + off_m2m(Q);  // [4Q cols][Q rows]
+        for (int e = threadIdx.x; e < Q * 4 * Q; e += blockDim.x) {
+            int r = e / (4 * Q), c = e % (4 * Q), qc = c / Q, cc = c % Q;
+            double s = 0;
+            for (int t = 0; t < Q; t++) s = fma(m[r * 4 * Q + qc * Q + t], inv1[t * Q + cc], s);
+            o[(size_t)c * Q + r] = s;
+        }
+    } else {
+        if (l + 1 >= A.L) return;
+        const double *m = A.m2mc + (size_t)l * Q * 4 * Q;
+        double *o = b + off_l2l(Q);  // [Q cols][4Q rows]
+        for (int e = threadIdx.x; e < 4 * Q * Q; e += blockDim.x) {
+            int r = e / Q, c = e % Q;  // r in 4Q (child block q = r / Q), c in Q
+            double s = 0;
+            for (int t = 0; t < Q; t++) s = fma(m[t * 4 * Q + r], inv[t * Q + c], s);
+            o[(size_t)c * 4 * Q + r] = s;
+        }
+    }
+}
+
+// directional M2L blocks: for parent direction d = (dx+1)*3 + (dy+1), target
+// child a = 2ii+jj and source child b = 2iii+jjj sit at offset
+// 2(dx,dy) - (ii,jj) + (iii,jjj) (class_fmm.py:263-283); near offsets are zero.
+__global__ void k_ops_assemble(OpsArgs A) {
+    const int Q = A.Q, Q4 = 4 * Q, l = blockIdx.x, d = blockIdx.y;
+    if (l < 1 || l >= A.L || d == 4) return;
+    int dx = d / 3 - 1, dy = d % 3 - 1;
+    double *o = A.ops + (size_t)l * A.stride + off_m2l(Q) + (size_t)d * Q4 * Q4;
+    for (int e = threadIdx.x; e < Q4 * Q4; e += blockDim.x) {
+        int c = e / Q4, r = e % Q4;       // column-major element (r, c)
+        int ta = r / Q, rr = r % Q, sb = c / Q, cc = c % Q;
+        int ox = 2 * dx - (ta >> 1) + (sb >> 1), oy = 2 * dy - (ta & 1) + (sb & 1);
+        double v = 0.0;
+        if (!(ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1)) {
+            int slot = (ox + 3) * 7 + (oy + 3);
+            v = A.poff[((size_t)l * 49 + slot) * Q * Q + rr * Q + cc];
+        }
+        o[e] = v;
+    }
+}
+
+__global__ void k_to_float(const double *__restrict__ a, float *__restrict__ b, size_t n) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+void build_operators(kifmm_plan *P) {
+    KIFMM_REQUIRE(P->have_tree, KIFMM_ERR_STATE, "precompute: build_tree first");
+    const int L = P->L, Q = P->Q;
+    cudaStream_t s = P->stream;
+    OpsArgs A{};
+    A.L = L; A.Q = Q; A.kind = P->kern.kind; A.k = P->kern.k; A.W = P->W;
+    if (P->opt.radii == 1) { A.rf1 = 1.5; A.rf2 = 2.5; }
+    else { A.rf1 = std::sqrt(2.0) + 0.01; A.rf2 = 4.0 - std::sqrt(2.0) - 2 * 0.01; }
+    A.stride = ops_stride(Q);
+    P->ops_stride = A.stride;
+    P->ops.alloc(A.stride * (size_t)L);
+    KIFMM_CUDA(cudaMemsetAsync(P->ops.p, 0, A.stride * (size_t)L * sizeof(double), s));
+    A.ops = P->ops.p;
+    DBuf<double> &tmp = P->ops_tmp;
+    size_t n49 = (size_t)L * 49 * Q * Q;
+    tmp.alloc(2 * n49 + (size_t)L * 4 * Q * Q);
+    A.m2ls = tmp.p;
+    A.poff = tmp.p + n49;
+    A.m2mc = tmp.p + 2 * n49;
+    for (int l = 0; l < L; l++) {
+        double *b = P->ops.p + (size_t)l * A.stride;
+        P->lops[l].inv = b + off_inv(Q);
+        P->lops[l].m2m = b + off_m2m(Q);
+        P->lops[l].l2lT = b + off_l2l(Q);
+        P->lops[l].m2lT = b + off_m2l(Q);
+        P->lops[l].large = b + off_large(Q);
+        P->lops[l].small = b + off_small(Q);
+    }
+    if (L >= 2) {
+        k_ops_surfaces<<<L, Q, 0, s>>>(A);
+        KIFMM_LAUNCHED();
+        size_t smem = (size_t)Q * 2 * Q * sizeof(double) + Q * sizeof(double);
+        KIFMM_CUDA(cudaFuncSetAttribute(k_ops_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_ops_inverse<<<L, 256, smem, s>>>(A);
+        KIFMM_LAUNCHED();
+        k_ops_kmats<<<dim3(L, 50), 256, 0, s>>>(A);
+        KIFMM_LAUNCHED();
+        k_ops_compose<<<dim3(L, 51), 256, 0, s>>>(A);
+        KIFMM_LAUNCHED();
+        k_ops_assemble<<<dim3(L, 9), 256, 0, s>>>(A);
+        KIFMM_LAUNCHED();
+    }
+    if (P->opt.precision == KIFMM_PREC_MIXED) {
+        P->ops_f.alloc(A.stride * (size_t)L);
+        k_to_float<<<grid_for(A.stride * L, 256, 4096), 256, 0, s>>>(P->ops.p, P->ops_f.p, A.stride * (size_t)L);
+        KIFMM_LAUNCHED();
+    }
+    P->have_ops = true;
+}
+
+}  // namespace kifmm

@@ -1,0 +1,151 @@
+// radix_sort.cu -- stable LSD radix sort of 64-bit keys (optionally with int32
+// payloads) for the Morton-key tree build.
+//
+// Each pass sorts one 8-bit digit in three kernels:
+//   1. per-tile digit histograms (tile = 256 threads x 16 keys),
+//   2. one exclusive scan over the digit-major histogram table,
+//   3. a stable scatter: inside a tile, each warp ranks its 512 keys in order
+//      with __match_any_sync, warps are combined by a per-digit prefix in
+//      shared memory, and the tile's base comes from the scanned table.
+#include "kifmm_internal.cuh"
+
+namespace kifmm {
+
+constexpr int RS_THREADS = 256;
+constexpr int RS_ITEMS = 16;
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
+constexpr int RS_WARPS = RS_THREADS / 32;
+
+__global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const uint64_t *__restrict__ key, int64_t n, int shift,
+                                                         uint32_t *__restrict__ hist, int nblocks) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    int64_t base = (int64_t)blockIdx.x * RS_TILE;
+#pragma unroll 4
+    for (int i = 0; i < RS_ITEMS; i++) {
+        int64_t idx = base + i * RS_THREADS + threadIdx.x;
+        if (idx < n) atomicAdd(&h[(key[idx] >> shift) & 255], 1u);
+    }
+    __syncthreads();
+    hist[(size_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
+}
+
+// exclusive scan of `total` counters by one block of 1024 threads
+__global__ void __launch_bounds__(1024) k_rs_scan(uint32_t *__restrict__ hist, int64_t total) {
+    __shared__ uint32_t part[1024];
+    int64_t chunk = (total + 1023) / 1024;
+    int64_t b = threadIdx.x * chunk, e = b + chunk < total ? b + chunk : total;
+    uint32_t s = 0;
+    for (int64_t i = b; i < e; i++) s += hist[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t run = part[threadIdx.x] - s;
+    for (int64_t i = b; i < e; i++) {
+        uint32_t v = hist[i];
+        hist[i] = run;
+        run += v;
+    }
+}
+
+template <bool PAIRS>
+__global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t *__restrict__ key, const int32_t *__restrict__ val,
+                                                            uint64_t *__restrict__ okey, int32_t *__restrict__ oval,
+                                                            int64_t n, int shift, const uint32_t *__restrict__ hist,
+                                                            int nblocks) {
+    __shared__ uint32_t wcnt[RS_WARPS][256];
+    __shared__ uint32_t base[256];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int d = threadIdx.x; d < 256 * RS_WARPS; d += RS_THREADS) (&wcnt[0][0])[d] = 0;
+    base[threadIdx.x] = hist[(size_t)threadIdx.x * nblocks + blockIdx.x];
+    __syncthreads();
+    const int64_t t0 = (int64_t)blockIdx.x * RS_TILE + (int64_t)w * (RS_ITEMS * 32);
+    uint64_t k[RS_ITEMS];
+    int32_t v[RS_ITEMS];
+    uint32_t rank[RS_ITEMS];
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int r = 0; r < RS_ITEMS; r++) {
+        int64_t idx = t0 + r * 32 + lane;
+        bool ok = idx < n;
+        k[r] = ok ? key[idx] : 0;
+        if (PAIRS) v[r] = ok ? val[idx] : 0;
+        uint32_t d = ok ? (uint32_t)((k[r] >> shift) & 255) : 256u;
+        unsigned peers = __match_any_sync(0xffffffffu, d);
+        uint32_t before = d < 256 ? wcnt[w][d] : 0;
+        rank[r] = before + __popc(peers & lt);
+        __syncwarp();
+        if (d < 256 && lane == __ffs(peers) - 1) wcnt[w][d] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    // exclusive prefix over warps for each digit, folded into per-warp offsets
+    {
+        int d = threadIdx.x;
+        uint32_t run = base[d];
+#pragma unroll
+        for (int ww = 0; ww < RS_WARPS; ww++) {
+            uint32_t c = wcnt[ww][d];
+            wcnt[ww][d] = run;
+            run += c;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < RS_ITEMS; r++) {
+        int64_t idx = t0 + r * 32 + lane;
+        if (idx < n) {
+            uint32_t d = (uint32_t)((k[r] >> shift) & 255);
+            uint32_t pos = wcnt[w][d] + rank[r];
+            okey[pos] = k[r];
+            if (PAIRS) oval[pos] = v[r];
+        }
+    }
+}
+
+static void rs_run(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_tmp, int64_t n, int bits,
+                   kifmm_plan *P, bool pairs) {
+    if (n <= 1) return;
+    KIFMM_REQUIRE(n < (1ll << 31), KIFMM_ERR_ARG, "radix sort: more than 2^31 keys");
+    int nb = (int)((n + RS_TILE - 1) / RS_TILE);
+    P->sort_hist.alloc((size_t)256 * nb);
+    int passes = (bits + 7) / 8;
+    uint64_t *ka = key, *kb = key_tmp;
+    int32_t *va = val, *vb = val_tmp;
+    for (int p = 0; p < passes; p++) {
+        int shift = 8 * p;
+        k_rs_hist<<<nb, RS_THREADS, 0, P->stream>>>(ka, n, shift, P->sort_hist.p, nb);
+        KIFMM_LAUNCHED();
+        k_rs_scan<<<1, 1024, 0, P->stream>>>(P->sort_hist.p, (int64_t)256 * nb);
+        KIFMM_LAUNCHED();
+        if (pairs)
+            k_rs_scatter<true><<<nb, RS_THREADS, 0, P->stream>>>(ka, va, kb, vb, n, shift, P->sort_hist.p, nb);
+        else
+            k_rs_scatter<false><<<nb, RS_THREADS, 0, P->stream>>>(ka, nullptr, kb, nullptr, n, shift,
+                                                                  P->sort_hist.p, nb);
+        KIFMM_LAUNCHED();
+        uint64_t *tk = ka; ka = kb; kb = tk;
+        int32_t *tv = va; va = vb; vb = tv;
+    }
+    if (ka != key) {
+        KIFMM_CUDA(cudaMemcpyAsync(key, ka, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, P->stream));
+        if (pairs) KIFMM_CUDA(cudaMemcpyAsync(val, va, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, P->stream));
+    }
+}
+
+void radix_sort_pairs(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_tmp, int64_t n, int bits,
+                      kifmm_plan *P) {
+    rs_run(key, val, key_tmp, val_tmp, n, bits, P, true);
+}
+
+void radix_sort_keys(uint64_t *key, uint64_t *key_tmp, int64_t n, int bits, kifmm_plan *P) {
+    rs_run(key, nullptr, key_tmp, nullptr, n, bits, P, false);
+}
+
+}  // namespace kifmm

@@ -1,0 +1,581 @@
+// tree.cu -- level-restricted adaptive quadtree on the GPU.
+//
+// Reference: Tree (pykifmm2d/tree.py:460-590).  The reference splits level by
+// level with in-place partitions; here the same tree is derived from sorted
+// Morton keys:
+//   * root box [m, M] as in tree.py:475-484 (including its ymax = y.min()
+//     quirk unless fix_bbox), all midpoints exact dyadic numbers, so the
+//     reference's strict 'x > xmid' descent equals the key prefix;
+//   * a cell is split in the unrestricted tree iff it holds > Ncutoff points
+//     (tree.py:242): found from the sorted keys in one pass -- point i reports
+//     the cells it opens whose window [i, i+Ncutoff] stays inside them;
+//   * level restriction (tree.py:533-545, numba_get_bads :432-444) is the
+//     closure Split_l = Split0_l U N9(parent(Split_{l+1})), computed level by
+//     level from the deepest one (N9 = the 3x3 block of cells in the domain);
+//   * X-list (tree.py:546-576, numba_get_Xlist :446-458): a real leaf with a
+//     split colleague gets four fake children;
+//   * nodes of level l+1 are the four children of every split or X-list cell
+//     of level l, in Morton order; colleagues (tree.py:260-294) are the
+//     existing same-level cells of the 3x3 block, stored by direction.
+// Split and X-list cells live in a device hash set while they are collected,
+// then in one sorted list that every lookup binary-searches.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "kifmm_internal.cuh"
+
+namespace kifmm {
+
+constexpr uint64_t KEY56 = (1ull << 56) - 1;
+
+__device__ __forceinline__ uint64_t ordered_bits(double v) {
+    uint64_t u = (uint64_t)__double_as_longlong(v);
+    return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
+}
+static double from_ordered(uint64_t o) {
+    uint64_t u = (o >> 63) ? (o & 0x7fffffffffffffffull) : ~o;
+    double d;
+    memcpy(&d, &u, 8);
+    return d;
+}
+
+// scal[0..3]: ordered min x, max x, min y, max y; scal[4]: non-finite count
+__global__ void k_bbox(const double *__restrict__ x, const double *__restrict__ y, int64_t n,
+                       unsigned long long *scal) {
+    uint64_t mnx = ~0ull, mxx = 0, mny = ~0ull, mxy = 0;
+    unsigned long long bad = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double a = x[i], b = y[i];
+        if (!isfinite(a) || !isfinite(b)) { bad++; continue; }
+        uint64_t oa = ordered_bits(a), ob = ordered_bits(b);
+        mnx = min(mnx, oa); mxx = max(mxx, oa);
+        mny = min(mny, ob); mxy = max(mxy, ob);
+    }
+    for (int o = 16; o; o >>= 1) {
+        mnx = min(mnx, (uint64_t)__shfl_xor_sync(0xffffffffu, mnx, o));
+        mxx = max(mxx, (uint64_t)__shfl_xor_sync(0xffffffffu, mxx, o));
+        mny = min(mny, (uint64_t)__shfl_xor_sync(0xffffffffu, mny, o));
+        mxy = max(mxy, (uint64_t)__shfl_xor_sync(0xffffffffu, mxy, o));
+        bad += __shfl_xor_sync(0xffffffffu, bad, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&scal[0], mnx); atomicMax(&scal[1], mxx);
+        atomicMin(&scal[2], mny); atomicMax(&scal[3], mxy);
+        if (bad) atomicAdd(&scal[4], bad);
+    }
+}
+
+// Exact grid cell: j = #{k in [1, 2^D-1] : v > m + k h}.  The gridlines are
+// the midpoints of every level (m + odd * W / 2^(l+1)), exact in FP64 for the
+// coordinate range checked on the host.
+__device__ __forceinline__ uint64_t grid_cell(double v, double m, double h) {
+    const int64_t top = (1ll << KEY_DEPTH) - 1;
+    double t = ceil((v - m) / h) - 1.0;
+    int64_t j = t < 0 ? 0 : (t > (double)top ? top : (int64_t)t);
+    for (int it = 0; it < 8 && j < top && v > m + (double)(j + 1) * h; it++) j++;
+    for (int it = 0; it < 8 && j > 0 && !(v > m + (double)j * h); it++) j--;
+    return (uint64_t)j;
+}
+
+__global__ void k_keys(const double *__restrict__ x, const double *__restrict__ y, int64_t n, double m, double M,
+                       double h, uint64_t *__restrict__ key, int32_t *__restrict__ perm, unsigned long long *outside) {
+    unsigned long long out = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double a = x[i], b = y[i];
+        uint64_t k = 0;
+        if (h > 0) k = morton(grid_cell(a, m, h), grid_cell(b, m, h));
+        key[i] = k;
+        perm[i] = (int32_t)i;
+        out += (a < m || a > M || b < m || b > M);
+    }
+    for (int o = 16; o; o >>= 1) out += __shfl_xor_sync(0xffffffffu, out, o);
+    if ((threadIdx.x & 31) == 0 && out) atomicAdd(outside, out);
+}
+
+__global__ void k_gather2(const double *__restrict__ x, const double *__restrict__ y, const int32_t *__restrict__ perm,
+                          int64_t n, double *__restrict__ xs, double *__restrict__ ys) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int32_t p = perm[i];
+        xs[i] = x[p];
+        ys[i] = y[p];
+    }
+}
+
+// deepest level whose cell contains both keys
+__device__ __forceinline__ int common_level(uint64_t a, uint64_t b) {
+    if (a == b) return KEY_DEPTH;
+    return (__clzll((long long)(a ^ b)) - (64 - 2 * KEY_DEPTH)) >> 1;
+}
+
+// ------------------------------------------------------------ hash set
+__device__ __forceinline__ uint64_t hmix(uint64_t v) {
+    v ^= v >> 33; v *= 0xff51afd7ed558ccdull;
+    v ^= v >> 33; v *= 0xc4ceb9fe1a85ec53ull;
+    v ^= v >> 33;
+    return v;
+}
+
+struct HashSet {
+    unsigned long long *tab;
+    uint64_t mask;
+    uint64_t *list;
+    unsigned long long *count;  // entries appended to list
+    unsigned long long *ovf;
+    uint64_t cap;               // list capacity
+};
+
+__device__ __forceinline__ uint64_t ent_make(int l, uint64_t k, int x) {
+    return ((uint64_t)l << ENT_LEVEL_SHIFT) | (k << 1) | (uint64_t)x;
+}
+
+__device__ void hs_insert(const HashSet &H, uint64_t e) {
+    uint64_t s = hmix(e) & H.mask;
+    for (uint64_t p = 0; p <= H.mask; p++) {
+        unsigned long long prev = atomicCAS(&H.tab[s], (unsigned long long)ENT_EMPTY, (unsigned long long)e);
+        if (prev == ENT_EMPTY) {
+            unsigned long long idx = atomicAdd(H.count, 1ull);
+            if (idx < H.cap) H.list[idx] = e;
+            else atomicOr(H.ovf, 1ull);
+            return;
+        }
+        if (prev == e) return;
+        s = (s + 1) & H.mask;
+    }
+    atomicOr(H.ovf, 2ull);
+}
+
+__device__ bool hs_has(const HashSet &H, uint64_t e) {
+    uint64_t s = hmix(e) & H.mask;
+    for (uint64_t p = 0; p <= H.mask; p++) {
+        uint64_t v = ((volatile unsigned long long *)H.tab)[s];
+        if (v == e) return true;
+        if (v == ENT_EMPTY) return false;
+        s = (s + 1) & H.mask;
+    }
+    return false;
+}
+
+// Split cells of the unrestricted tree.  Point i (sorted) is the first point
+// of its level-l cell for l > common_level(key[i-1], key[i]); that cell holds
+// more than ppl points iff l <= common_level(key[i], key[i+ppl]).
+// mode 0: count + deepest level; mode 1: insert.
+// scal[5]: count, scal[6]: deepest split level + 1, scal[7]: depth overflow
+__global__ void k_t0(const uint64_t *__restrict__ key, int64_t n, int64_t ppl, int mode, HashSet H,
+                     unsigned long long *scal) {
+    unsigned long long cnt = 0;
+    int deepest = 0;
+    bool over = false;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        if (i + ppl >= n) continue;
+        uint64_t k = key[i];
+        int hi = common_level(k, key[i + ppl]);
+        if (hi >= KEY_DEPTH) { over = true; hi = KEY_DEPTH - 1; }
+        int lo = i == 0 ? -1 : common_level(key[i - 1], k);
+        if (hi <= lo) continue;
+        if (mode == 0) {
+            cnt += (unsigned long long)(hi - lo);
+            deepest = max(deepest, hi + 1);
+        } else {
+            for (int l = lo + 1; l <= hi; l++) hs_insert(H, ent_make(l, k >> (2 * (KEY_DEPTH - l)), 0));
+        }
+    }
+    if (mode == 0) {
+        for (int o = 16; o; o >>= 1) {
+            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+            deepest = max(deepest, __shfl_xor_sync(0xffffffffu, deepest, o));
+        }
+        over = __any_sync(0xffffffffu, over);
+        if ((threadIdx.x & 31) == 0) {
+            if (cnt) atomicAdd(&scal[5], cnt);
+            atomicMax(&scal[6], (unsigned long long)deepest);
+            if (over) atomicOr(&scal[7], 1ull);
+        }
+    }
+}
+
+// Restriction step for level l: every split cell s of level l+1 forces the
+// 3x3 block around parent(s) to be split.
+__global__ void k_restrict(HashSet H, int l) {
+    unsigned long long n = *((volatile unsigned long long *)H.count);
+    if (n > H.cap) n = H.cap;
+    const int64_t side = 1ll << l;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < (int64_t)n; j += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t e = H.list[j];
+        if ((int)(e >> ENT_LEVEL_SHIFT) != l + 1 || (e & 1)) continue;
+        uint64_t p = ((e >> 1) & KEY56) >> 2;
+        int64_t px = (int64_t)compact2(p >> 1), py = (int64_t)compact2(p);
+        for (int dx = -1; dx <= 1; dx++)
+            for (int dy = -1; dy <= 1; dy++) {
+                int64_t qx = px + dx, qy = py + dy;
+                if (qx < 0 || qy < 0 || qx >= side || qy >= side) continue;
+                hs_insert(H, ent_make(l, morton((uint64_t)qx, (uint64_t)qy), 0));
+            }
+    }
+}
+
+// X-list: for levels 1..L-2, a real leaf (cell not split, parent split) next
+// to a split cell becomes an X-list cell.
+__global__ void k_xlist(HashSet H, int L) {
+    unsigned long long n = *((volatile unsigned long long *)H.count);
+    if (n > H.cap) n = H.cap;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < (int64_t)n; j += (int64_t)gridDim.x * blockDim.x) {
+        uint64_t e = H.list[j];
+        int l = (int)(e >> ENT_LEVEL_SHIFT);
+        if ((e & 1) || l < 1 || l > L - 2) continue;
+        uint64_t k = (e >> 1) & KEY56;
+        int64_t sx = (int64_t)compact2(k >> 1), sy = (int64_t)compact2(k);
+        const int64_t side = 1ll << l;
+        for (int dx = -1; dx <= 1; dx++)
+            for (int dy = -1; dy <= 1; dy++) {
+                if (!dx && !dy) continue;
+                int64_t cx = sx + dx, cy = sy + dy;
+                if (cx < 0 || cy < 0 || cx >= side || cy >= side) continue;
+                uint64_t c = morton((uint64_t)cx, (uint64_t)cy);
+                if (hs_has(H, ent_make(l, c, 0))) continue;
+                if (!hs_has(H, ent_make(l - 1, c >> 2, 0))) continue;
+                hs_insert(H, ent_make(l, c, 1));
+            }
+    }
+}
+
+__global__ void k_level_counts(const uint64_t *__restrict__ ent, int64_t n, unsigned long long *cnt) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        atomicAdd(&cnt[ent[i] >> ENT_LEVEL_SHIFT], 1ull);
+}
+
+// ----------------------------------------------------------- node arrays
+__device__ __forceinline__ int64_t find_entry(const uint64_t *__restrict__ ent, const LevelTable &T, int l,
+                                              uint64_t k) {
+    if (l < 0 || l >= T.L) return -1;
+    int64_t lo = T.eoff[l], end = lo + T.ne[l], hi = end;
+    uint64_t target = ((uint64_t)l << (ENT_LEVEL_SHIFT - 1)) | k;
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if ((ent[mid] >> 1) < target) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < end && (ent[lo] >> 1) == target) ? lo : -1;
+}
+
+__device__ __forceinline__ int64_t node_index(const uint64_t *__restrict__ ent, const LevelTable &T, int l,
+                                              uint64_t k) {
+    if (l == 0) return k == 0 ? 0 : -1;
+    int64_t j = find_entry(ent, T, l - 1, k >> 2);
+    if (j < 0) return -1;
+    return T.off[l] + 4 * (j - T.eoff[l - 1]) + (int64_t)(k & 3);
+}
+
+__device__ __forceinline__ int64_t lower_bound_u64(const uint64_t *__restrict__ a, int64_t n, uint64_t v) {
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        int64_t mid = (lo + hi) >> 1;
+        if (a[mid] < v) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_nodes(LevelTable T, int64_t n_nodes, const uint64_t *__restrict__ ent,
+                        const uint64_t *__restrict__ pkey, int64_t npts, uint64_t *__restrict__ nkey,
+                        int8_t *__restrict__ nlev, uint8_t *__restrict__ nflag, int32_t *__restrict__ nbot,
+                        int32_t *__restrict__ ntop, int32_t *__restrict__ nparent, int32_t *__restrict__ nchild,
+                        int32_t *__restrict__ nent, int32_t *__restrict__ ncoll, int32_t *__restrict__ ent_node) {
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_nodes; g += (int64_t)gridDim.x * blockDim.x) {
+        int l = 0;
+        while (l + 1 < T.L && T.off[l + 1] <= g) l++;
+        int64_t i = g - T.off[l];
+        uint64_t k = 0;
+        uint8_t f = 0;
+        int64_t parent = -1;
+        if (l > 0) {
+            uint64_t pe = ent[T.eoff[l - 1] + i / 4];
+            uint64_t pk = (pe >> 1) & KEY56;
+            k = (pk << 2) | (uint64_t)(i & 3);
+            if (pe & 1) f |= NF_FAKE;
+            parent = node_index(ent, T, l - 1, pk);
+        }
+        int64_t j = find_entry(ent, T, l, k);
+        int64_t child = -1;
+        if (j >= 0) {
+            f |= (ent[j] & 1) ? NF_XLIST : NF_SPLIT;
+            child = T.off[l + 1] + 4 * (j - T.eoff[l]);
+            ent_node[j] = (int32_t)g;
+        }
+        int sh = 2 * (KEY_DEPTH - l);
+        uint64_t lo = k << sh;
+        int64_t b = l == 0 ? 0 : lower_bound_u64(pkey, npts, lo);
+        int64_t e = (l == 0) ? npts : lower_bound_u64(pkey, npts, lo + (1ull << sh));
+        nkey[g] = k;
+        nlev[g] = (int8_t)l;
+        nflag[g] = f;
+        nbot[g] = (int32_t)b;
+        ntop[g] = (int32_t)e;
+        nparent[g] = (int32_t)parent;
+        nchild[g] = (int32_t)child;
+        nent[g] = (int32_t)j;
+        int64_t ix = (int64_t)compact2(k >> 1), iy = (int64_t)compact2(k), side = 1ll << l;
+        for (int dx = -1; dx <= 1; dx++)
+            for (int dy = -1; dy <= 1; dy++) {
+                int64_t cx = ix + dx, cy = iy + dy, c = -1;
+                if (cx >= 0 && cy >= 0 && cx < side && cy < side)
+                    c = (dx == 0 && dy == 0) ? g : node_index(ent, T, l, morton((uint64_t)cx, (uint64_t)cy));
+                ncoll[9 * g + (dx + 1) * 3 + (dy + 1)] = (int32_t)c;
+            }
+    }
+}
+
+// work lists + counts: misc[0] leaf_list, misc[1] p2m_list, misc[2] leaves,
+// misc[3] fake, misc[4] xlist
+__global__ void k_lists(int64_t n_nodes, const int8_t *__restrict__ nlev, const uint8_t *__restrict__ nflag,
+                        const int32_t *__restrict__ nbot, const int32_t *__restrict__ ntop, int32_t *leaf_list,
+                        int32_t *p2m_list, unsigned long long *cnt) {
+    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_nodes; g += (int64_t)gridDim.x * blockDim.x) {
+        uint8_t f = nflag[g];
+        bool fake = f & NF_FAKE, split = f & NF_SPLIT, xl = f & NF_XLIST;
+        bool real_leaf = !fake && !split;
+        int64_t ns = ntop[g] - nbot[g];
+        if (real_leaf) atomicAdd(&cnt[2], 1ull);
+        if (fake) atomicAdd(&cnt[3], 1ull);
+        if (xl) atomicAdd(&cnt[4], 1ull);
+        if (real_leaf && ns > 0) leaf_list[atomicAdd(&cnt[0], 1ull)] = (int32_t)g;
+        if (nlev[g] >= 2 && ns > 0 && ((real_leaf && !xl) || fake)) p2m_list[atomicAdd(&cnt[1], 1ull)] = (int32_t)g;
+    }
+}
+
+// Work counts: cnt[0] P2P pairs, cnt[1] P2M points, cnt[2] V-list pairs,
+// cnt[3] (target group, direction) M2L blocks.
+__global__ void k_stats(LevelTable T, const uint64_t *__restrict__ ent, const int32_t *__restrict__ ent_node,
+                        const int32_t *__restrict__ leaf_list, int64_t nleaf, const int32_t *__restrict__ p2m_list,
+                        int64_t np2m, const int32_t *__restrict__ nbot, const int32_t *__restrict__ ntop,
+                        const int32_t *__restrict__ ncoll, const int32_t *__restrict__ nent, int64_t n_ent,
+                        unsigned long long *cnt) {
+    int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+    unsigned long long a = 0, b = 0, c = 0, d = 0;
+    for (int64_t i = tid; i < nleaf; i += stride) {
+        int g = leaf_list[i];
+        int64_t s = 0;
+        for (int k = 0; k < 9; k++) {
+            int q = ncoll[9 * (int64_t)g + k];
+            if (q >= 0) s += ntop[q] - nbot[q];
+        }
+        a += (unsigned long long)((ntop[g] - nbot[g]) * s);
+    }
+    for (int64_t i = tid; i < np2m; i += stride) b += ntop[p2m_list[i]] - nbot[p2m_list[i]];
+    for (int64_t j = tid; j < n_ent; j += stride) {
+        if (ent[j] & 1) continue;
+        int l = (int)(ent[j] >> ENT_LEVEL_SHIFT);
+        if (l < 1) continue;
+        int p = ent_node[j];
+        for (int dd = 0; dd < 9; dd++) {
+            if (dd == 4) continue;
+            int nb = ncoll[9 * (int64_t)p + dd];
+            if (nb < 0 || nent[nb] < 0) continue;
+            d++;
+            int dx = dd / 3 - 1, dy = dd % 3 - 1;
+            for (int ta = 0; ta < 4; ta++)
+                for (int sb = 0; sb < 4; sb++) {
+                    int ox = 2 * dx - (ta >> 1) + (sb >> 1), oy = 2 * dy - (ta & 1) + (sb & 1);
+                    if (ox < -1 || ox > 1 || oy < -1 || oy > 1) c++;
+                }
+        }
+    }
+    atomicAdd(&cnt[0], a); atomicAdd(&cnt[1], b); atomicAdd(&cnt[2], c); atomicAdd(&cnt[3], d);
+}
+
+void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int mem) {
+    KIFMM_REQUIRE(n > 0 && n < (1ll << 31) - 1, KIFMM_ERR_ARG, "build_tree: need 0 < n < 2^31-1 points");
+    KIFMM_REQUIRE(x && y, KIFMM_ERR_ARG, "build_tree: null coordinate pointer");
+    cudaStream_t s = P->stream;
+    P->have_tree = P->have_ops = P->have_expansions = false;
+    P->N = n;
+    P->x.alloc(n); P->y.alloc(n);
+    cudaMemcpyKind kind = mem == KIFMM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    KIFMM_CUDA(cudaMemcpyAsync(P->x.p, x, n * sizeof(double), kind, s));
+    KIFMM_CUDA(cudaMemcpyAsync(P->y.p, y, n * sizeof(double), kind, s));
+    P->scal.alloc(16);
+    unsigned long long init[16];
+    for (int i = 0; i < 16; i++) init[i] = 0;
+    init[0] = init[2] = ~0ull;
+    KIFMM_CUDA(cudaMemcpyAsync(P->scal.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    const int TB = 256;
+    unsigned gs = grid_for(n, TB, P->num_sms * 8);
+    k_bbox<<<gs, TB, 0, s>>>(P->x.p, P->y.p, n, P->scal.p);
+    KIFMM_LAUNCHED();
+    unsigned long long sc[5];
+    KIFMM_CUDA(cudaMemcpyAsync(sc, P->scal.p, sizeof(sc), cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaStreamSynchronize(s));
+    KIFMM_REQUIRE(sc[4] == 0, KIFMM_ERR_ARG, "build_tree: non-finite coordinates");
+    double xmn = from_ordered(sc[0]), xmx = from_ordered(sc[1]), ymn = from_ordered(sc[2]), ymx = from_ordered(sc[3]);
+    double ytop = P->opt.fix_bbox ? ymx : ymn;
+    double m = std::floor(std::min(xmn, ymn)), M = std::ceil(std::max(xmx, ytop));
+    KIFMM_REQUIRE(std::fabs(m) < 8388608.0 && std::fabs(M) < 8388608.0, KIFMM_ERR_RANGE,
+                  "build_tree: |coordinates| must stay below 2^23 for exact dyadic midpoints");
+    P->root_min = m; P->root_max = M; P->W = M - m;
+    KIFMM_REQUIRE(P->W > 0 || n <= P->ppl, KIFMM_ERR_DEPTH,
+                  "build_tree: more than Ncutoff points on one integer point (zero-width root box)");
+    double h = P->W > 0 ? std::ldexp(P->W, -KEY_DEPTH) : 0.0;
+
+    P->pkey.alloc(n); P->perm.alloc(n); P->key2.alloc(n); P->perm2.alloc(n);
+    k_keys<<<gs, TB, 0, s>>>(P->x.p, P->y.p, n, m, M, h, P->pkey.p, P->perm.p, P->scal.p + 8);
+    KIFMM_LAUNCHED();
+    {
+        PhaseScope ph(P, KIFMM_PHASE_SORT);
+        radix_sort_pairs(P->pkey.p, P->perm.p, P->key2.p, P->perm2.p, n, 2 * KEY_DEPTH, P);
+    }
+    P->xs.alloc(n); P->ys.alloc(n);
+    k_gather2<<<gs, TB, 0, s>>>(P->x.p, P->y.p, P->perm.p, n, P->xs.p, P->ys.p);
+    KIFMM_LAUNCHED();
+
+    // unrestricted split cells: count, then size the set and insert
+    HashSet H{};
+    H.count = P->scal.p + 9;
+    H.ovf = P->scal.p + 10;
+    k_t0<<<gs, TB, 0, s>>>(P->pkey.p, n, P->ppl, 0, H, P->scal.p);
+    KIFMM_LAUNCHED();
+    unsigned long long st[4];
+    KIFMM_CUDA(cudaMemcpyAsync(st, P->scal.p + 5, sizeof(st), cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaStreamSynchronize(s));
+    P->n_outside = (int64_t)st[3];
+    KIFMM_REQUIRE(st[2] == 0, KIFMM_ERR_DEPTH,
+                  "build_tree: more than Ncutoff points share one cell of the finest grid (2^29 per side); "
+                  "the tree would need more than 30 levels");
+    int L = n > P->ppl ? (int)st[1] + 1 : 1;
+    KIFMM_REQUIRE(L <= MAX_LEVELS, KIFMM_ERR_DEPTH, "build_tree: too many levels");
+    P->L = L;
+    uint64_t t0count = st[0];
+
+    int64_t n_ent = 0;
+    if (L > 1) {
+        for (int attempt = 0;; attempt++) {
+            uint64_t cap = (t0count * 16 + 4096) << (2 * attempt);
+            uint64_t hcap = 1;
+            while (hcap < 2 * cap) hcap <<= 1;
+            P->hash.alloc(hcap);
+            P->list.alloc(cap);
+            KIFMM_CUDA(cudaMemsetAsync(P->hash.p, 0xFF, hcap * sizeof(uint64_t), s));
+            KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 9, 0, 2 * sizeof(unsigned long long), s));
+            H.tab = (unsigned long long *)P->hash.p;
+            H.mask = hcap - 1;
+            H.list = P->list.p;
+            H.cap = cap;
+            k_t0<<<gs, TB, 0, s>>>(P->pkey.p, n, P->ppl, 1, H, P->scal.p);
+            KIFMM_LAUNCHED();
+            unsigned rg = (unsigned)(P->num_sms * 4);
+            for (int l = L - 3; l >= 0; l--) {
+                k_restrict<<<rg, TB, 0, s>>>(H, l);
+                KIFMM_LAUNCHED();
+            }
+            k_xlist<<<rg, TB, 0, s>>>(H, L);
+            KIFMM_LAUNCHED();
+            unsigned long long cv[2];
+            KIFMM_CUDA(cudaMemcpyAsync(cv, P->scal.p + 9, sizeof(cv), cudaMemcpyDeviceToHost, s));
+            KIFMM_CUDA(cudaStreamSynchronize(s));
+            if (cv[1] == 0 && cv[0] <= cap) {
+                n_ent = (int64_t)cv[0];
+                break;
+            }
+            KIFMM_REQUIRE(attempt < 4, KIFMM_ERR_NOMEM, "build_tree: split-cell set overflow");
+        }
+    }
+    P->n_ent = n_ent;
+    P->ent.alloc(n_ent);
+    P->key2.alloc(std::max<int64_t>(n, n_ent));
+    if (n_ent) {
+        KIFMM_CUDA(cudaMemcpyAsync(P->ent.p, P->list.p, n_ent * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+        radix_sort_keys(P->ent.p, P->key2.p, n_ent, ENT_LEVEL_SHIFT + 5, P);
+    }
+    // per-level entry counts -> level table
+    P->misc.alloc(64);
+    unsigned long long *lc = (unsigned long long *)P->misc.p;
+    KIFMM_CUDA(cudaMemsetAsync(lc, 0, 32 * sizeof(unsigned long long), s));
+    if (n_ent) {
+        k_level_counts<<<grid_for(n_ent, TB, 1024), TB, 0, s>>>(P->ent.p, n_ent, lc);
+        KIFMM_LAUNCHED();
+    }
+    unsigned long long lcount[32];
+    KIFMM_CUDA(cudaMemcpyAsync(lcount, lc, sizeof(lcount), cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaStreamSynchronize(s));
+    LevelTable &T = P->lt;
+    memset(&T, 0, sizeof(T));
+    T.L = L;
+    int64_t off = 0, eoff = 0;
+    for (int l = 0; l < L; l++) {
+        int64_t nl = l == 0 ? 1 : 4 * (int64_t)lcount[l - 1];
+        T.off[l] = off; T.eoff[l] = eoff; T.ne[l] = (int64_t)lcount[l];
+        P->lv[l].off = off; P->lv[l].n = nl; P->lv[l].eoff = eoff; P->lv[l].ne = (int64_t)lcount[l];
+        P->lv[l].width = std::ldexp(P->W, -l);
+        off += nl;
+        eoff += (int64_t)lcount[l];
+    }
+    T.off[L] = off; T.eoff[L] = eoff;
+    KIFMM_REQUIRE(lcount[L - 1] == 0 && eoff == n_ent, KIFMM_ERR_CUDA, "build_tree: inconsistent level table");
+    int64_t NN = off;
+    KIFMM_REQUIRE(NN < (1ll << 31), KIFMM_ERR_ARG, "build_tree: too many nodes");
+    P->n_nodes = NN;
+    P->nkey.alloc(NN); P->nlev.alloc(NN); P->nflag.alloc(NN); P->nbot.alloc(NN); P->ntop.alloc(NN);
+    P->nparent.alloc(NN); P->nchild.alloc(NN); P->nent.alloc(NN); P->ncoll.alloc(9 * NN);
+    P->ent_node.alloc(std::max<int64_t>(n_ent, 1));
+    P->leaf_list.alloc(NN); P->p2m_list.alloc(NN);
+    unsigned ng = grid_for(NN, TB, P->num_sms * 16);
+    k_nodes<<<ng, TB, 0, s>>>(T, NN, P->ent.p, P->pkey.p, n, P->nkey.p, P->nlev.p, P->nflag.p, P->nbot.p, P->ntop.p,
+                              P->nparent.p, P->nchild.p, P->nent.p, P->ncoll.p, P->ent_node.p);
+    KIFMM_LAUNCHED();
+    unsigned long long *cnt = (unsigned long long *)P->misc.p + 32;
+    KIFMM_CUDA(cudaMemsetAsync(cnt, 0, 8 * sizeof(unsigned long long), s));
+    k_lists<<<ng, TB, 0, s>>>(NN, P->nlev.p, P->nflag.p, P->nbot.p, P->ntop.p, P->leaf_list.p, P->p2m_list.p, cnt);
+    KIFMM_LAUNCHED();
+    unsigned long long c5[5];
+    KIFMM_CUDA(cudaMemcpyAsync(c5, cnt, sizeof(c5), cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaStreamSynchronize(s));
+    P->n_leaf_list = (int64_t)c5[0];
+    P->n_p2m_list = (int64_t)c5[1];
+    P->n_leaves = (int64_t)c5[2];
+    P->n_fake = (int64_t)c5[3];
+    P->n_xlist = (int64_t)c5[4];
+    KIFMM_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(unsigned long long), s));
+    k_stats<<<P->num_sms * 2, TB, 0, s>>>(T, P->ent.p, P->ent_node.p, P->leaf_list.p, P->n_leaf_list, P->p2m_list.p,
+                                          P->n_p2m_list, P->nbot.p, P->ntop.p, P->ncoll.p, P->nent.p, n_ent, cnt);
+    KIFMM_LAUNCHED();
+    KIFMM_CUDA(cudaMemcpyAsync(c5, cnt, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaStreamSynchronize(s));
+    P->n_p2p_pairs = (int64_t)c5[0];
+    P->n_p2m_points = (int64_t)c5[1];
+    P->n_m2l_pairs = (int64_t)c5[2];
+    P->n_m2l_groups = (int64_t)c5[3];
+    P->have_tree = true;
+}
+
+void export_tree(kifmm_plan *P, int64_t *nodes, int64_t *point_leaf) {
+    KIFMM_REQUIRE(P->have_tree, KIFMM_ERR_STATE, "export_tree: no tree");
+    int64_t NN = P->n_nodes, n = P->N;
+    std::vector<uint64_t> key(NN);
+    std::vector<int8_t> lev(NN);
+    std::vector<uint8_t> fl(NN);
+    std::vector<int32_t> bot(NN), top(NN), perm(n);
+    cudaStream_t s = P->stream;
+    KIFMM_CUDA(cudaMemcpyAsync(key.data(), P->nkey.p, NN * 8, cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaMemcpyAsync(lev.data(), P->nlev.p, NN, cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaMemcpyAsync(fl.data(), P->nflag.p, NN, cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaMemcpyAsync(bot.data(), P->nbot.p, NN * 4, cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaMemcpyAsync(top.data(), P->ntop.p, NN * 4, cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaMemcpyAsync(perm.data(), P->perm.p, n * 4, cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaStreamSynchronize(s));
+    for (int64_t g = 0; g < NN; g++) {
+        uint64_t k = key[g];
+        int64_t ix = (int64_t)compact2(k >> 1), iy = (int64_t)compact2(k);
+        bool fake = fl[g] & NF_FAKE, split = fl[g] & NF_SPLIT, xl = fl[g] & NF_XLIST;
+        bool leaf = !fake && !split;
+        if (nodes) {
+            int64_t *r = nodes + 7 * g;
+            r[0] = lev[g]; r[1] = ix; r[2] = iy; r[3] = leaf; r[4] = fake; r[5] = xl; r[6] = top[g] - bot[g];
+        }
+        if (point_leaf && leaf)
+            for (int32_t p = bot[g]; p < top[g]; p++) {
+                int64_t *q = point_leaf + 3 * (int64_t)perm[p];
+                q[0] = lev[g]; q[1] = ix; q[2] = iy;
+            }
+    }
+}
+
+}  // namespace kifmm
