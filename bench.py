@@ -155,7 +155,7 @@ def time_full_steps(torch, cfg, xd, yd, td, precision, steps, warmup, flush, pro
     """Full pipeline on device-resident inputs; returns per-step ms (CUDA events)."""
     from pykifmm2d_b200 import _lib as B
     stream = torch.cuda.current_stream()
-    f = make_fmm(cfg, xd, yd, precision, stream=stream.cuda_stream)
+    f = make_fmm(cfg, xd, yd, precision, stream=stream.cuda_stream or 1)
     out = torch.empty_like(xd)
     lib = B.load()
     times = []

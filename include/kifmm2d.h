@@ -78,7 +78,8 @@ typedef struct kifmm_options {
                            r2=(4-sqrt2-0.02)w/2 (class_fmm.py:35-45); 1: 1.5 and 2.5 half-widths */
     int32_t device;     /* CUDA device ordinal */
     int32_t reserved;
-    void *stream;       /* cudaStream_t to order work on; NULL: the plan creates its own */
+    void *stream;       /* cudaStream_t to order work on (cudaStreamLegacy, i.e. 0x1, for the
+                           legacy default stream); NULL: the plan creates its own stream */
 } kifmm_options;
 
 #define KIFMM_MAX_LEVELS 30

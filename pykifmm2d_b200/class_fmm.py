@@ -235,6 +235,8 @@ class FMM(object):
         if stream is None and self._on_device:
             import torch
             stream = torch.cuda.current_stream(x.device).cuda_stream
+            if stream == 0:
+                stream = 1  # torch's default stream is the legacy stream (cudaStreamLegacy)
         opts.stream = stream
         h = B.ctypes.c_void_p()
         B.check(lib.kifmm_plan_create(kern.desc(), self.Nequiv, self.Ncutoff, ctypes_byref(opts), ctypes_byref(h)))

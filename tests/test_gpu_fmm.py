@@ -164,3 +164,27 @@ def test_errors_are_reported():
     with pytest.raises(B.KifmmError) as e:
         f.build_expansions(np.ones(100))
     assert e.value.code == B.ERR_ARG
+
+
+MIXED_CASES = ["c1_uniform20k", "uniform3k_cut16", "annulus6k_k0", "cluster_dup", "mix2k_cut8"]
+
+
+@pytest.mark.parametrize("name", MIXED_CASES)
+def test_mixed_accuracy_vs_fp64_direct(golden_cases, name):
+    """Mixed form (FP32 near field / P2M / L2P, FP32 M2L) against the FP64
+    direct sum (the reference's KAS output stored in the golden file).  Bound:
+    the reference's own FMM error on the case plus 1e-6."""
+    g = golden_cases[name]
+    f = make(g, precision="mixed")
+    f.build_expansions(g["tau"])
+    pot = f.evaluate_to_points(f.x, f.y, True)
+    fin = np.isfinite(g["direct"])
+    e_mixed = np.abs(pot - g["direct"])[fin].max() / np.abs(g["direct"][fin]).max()
+    e_ref = np.abs(g["pot"] - g["direct"])[fin].max() / np.abs(g["direct"][fin]).max()
+    print(f"{name}: mixed vs direct {e_mixed:.2e} (reference FMM {e_ref:.2e})")
+    assert e_mixed <= e_ref + 1e-6
+    if "xt" in g:
+        pt = f.evaluate_to_points(g["xt"], g["yt"], False)
+        et = rel(pt, g["pot_targets"])
+        print(f"{name}: mixed targets vs reference {et:.2e}")
+        assert et <= 1e-5
