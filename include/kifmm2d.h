@@ -195,6 +195,26 @@ int kifmm_get_phase_times(kifmm_plan *plan, double *ms, int64_t *launches, int32
 /* Number of kernels this library has launched in the process so far. */
 int64_t kifmm_launch_count(void);
 
+/* No counterpart in the reference (it has no device memory at all).
+ * For callers that cannot call cudaMalloc -- code running where another
+ * component owns all device memory, or a loop that must not enter the
+ * allocator: the first stage of the tree build, allocating nothing.
+ * keys[i] = 58-bit Morton key (x bit above y bit) of the i-th point in
+ * sorted order on the 2^29 x 2^29 grid of the root box [root_min, root_max]
+ * (integer corners, as kifmm_get_tree_info reports; points outside the box
+ * clamp to its edge cells), perm[i] = index of that point in x, y.  The sort
+ * is stable.  x, y, keys, perm are device pointers on the current device;
+ * work is queued on `stream` (NULL: the legacy default stream) and the call
+ * returns before it finishes.  Scratch is one fixed device array of the
+ * library (about 12.3 MB, held by every GPU that loads the library until the
+ * process exits), so n may not exceed KIFMM_NOALLOC_MAX_POINTS.  The first
+ * call on a device looks the array's address up (cudaGetSymbolAddress); make
+ * that first call before any stream capture.  All calls share the array:
+ * calls whose work overlaps on the GPU (other streams, other threads) race. */
+#define KIFMM_NOALLOC_MAX_POINTS 1048576
+int kifmm_morton_sort_noalloc(const double *x, const double *y, int64_t n, double root_min, double root_max,
+                              uint64_t *keys, int32_t *perm, void *stream);
+
 /* Library version (major*10000 + minor*100 + patch). */
 int kifmm_version(void);
 

@@ -17,6 +17,7 @@ KERNEL_LAPLACE, KERNEL_MOD_HELMHOLTZ = 0, 1
 PREC_FP64, PREC_MIXED = 0, 1
 M2L_AUTO, M2L_FP32, M2L_BF16X3, M2L_FP16X3, M2L_FP64 = 0, 1, 2, 3, 4
 MAX_LEVELS = 30
+NOALLOC_MAX_POINTS = 1048576
 PHASES = ["tree", "sort", "precompute", "p2m", "m2m", "m2l", "leaf", "targets"]
 
 
@@ -67,6 +68,7 @@ _SIGS = {
     "kifmm_set_profiling": (_i32, [_vp, _i32]),
     "kifmm_get_phase_times": (_i32, [_vp, _vp, _vp, _i32]),
     "kifmm_launch_count": (_i64, []),
+    "kifmm_morton_sort_noalloc": (_i32, [_vp, _vp, _i64, ctypes.c_double, ctypes.c_double, _vp, _vp, _vp]),
     "kifmm_version": (_i32, []),
 }
 

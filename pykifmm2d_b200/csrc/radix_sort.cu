@@ -148,4 +148,30 @@ void radix_sort_keys(uint64_t *key, uint64_t *key_tmp, int64_t n, int bits, kifm
     rs_run(key, nullptr, key_tmp, nullptr, n, bits, P, false);
 }
 
+int64_t radix_sort_hist_words(int64_t n) { return (int64_t)256 * ((n + RS_TILE - 1) / RS_TILE); }
+
+// Same passes as rs_run, on caller-provided scratch (histogram table of
+// radix_sort_hist_words(n) words, ping-pong buffers of n entries); launches
+// only, no allocation.  `bits` must give an even number of passes so the
+// result ends in key/val.
+void radix_sort_pairs_scratch(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_tmp, uint32_t *hist,
+                              int64_t n, int bits, cudaStream_t stream) {
+    if (n <= 1) return;
+    int nb = (int)((n + RS_TILE - 1) / RS_TILE);
+    int passes = (bits + 7) / 8;
+    uint64_t *ka = key, *kb = key_tmp;
+    int32_t *va = val, *vb = val_tmp;
+    for (int p = 0; p < passes; p++) {
+        int shift = 8 * p;
+        k_rs_hist<<<nb, RS_THREADS, 0, stream>>>(ka, n, shift, hist, nb);
+        KIFMM_LAUNCHED();
+        k_rs_scan<<<1, 1024, 0, stream>>>(hist, (int64_t)256 * nb);
+        KIFMM_LAUNCHED();
+        k_rs_scatter<true><<<nb, RS_THREADS, 0, stream>>>(ka, va, kb, vb, n, shift, hist, nb);
+        KIFMM_LAUNCHED();
+        uint64_t *tk = ka; ka = kb; kb = tk;
+        int32_t *tv = va; va = vb; vb = tv;
+    }
+}
+
 }  // namespace kifmm

@@ -383,6 +383,14 @@ __global__ void k_stats(LevelTable T, const uint64_t *__restrict__ ent, const in
     atomicAdd(&cnt[0], a); atomicAdd(&cnt[1], b); atomicAdd(&cnt[2], c); atomicAdd(&cnt[3], d);
 }
 
+// Morton keys of n points on the root box [m, M] (k_keys), launch only.
+void launch_morton_keys(const double *x, const double *y, int64_t n, double m, double M, uint64_t *key,
+                        int32_t *perm, unsigned long long *outside, int num_sms, cudaStream_t stream) {
+    double h = M > m ? std::ldexp(M - m, -KEY_DEPTH) : 0.0;
+    k_keys<<<grid_for(n, 256, num_sms * 8), 256, 0, stream>>>(x, y, n, m, M, h, key, perm, outside);
+    KIFMM_LAUNCHED();
+}
+
 void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int mem) {
     KIFMM_REQUIRE(n > 0 && n < (1ll << 31) - 1, KIFMM_ERR_ARG, "build_tree: need 0 < n < 2^31-1 points");
     KIFMM_REQUIRE(x && y, KIFMM_ERR_ARG, "build_tree: null coordinate pointer");
