@@ -61,11 +61,13 @@ enum {
 };
 /* M2L form used with KIFMM_PREC_MIXED. */
 enum {
-    KIFMM_M2L_AUTO = 0,
+    KIFMM_M2L_AUTO = 0,       /* = KIFMM_M2L_INT8 */
     KIFMM_M2L_FP32 = 1,       /* FP32 FFMA tiles on the CUDA cores */
     KIFMM_M2L_BF16X3 = 2,     /* tcgen05 kind::f16, bf16 hi/lo, 3 products, FP32 accumulate */
     KIFMM_M2L_FP16X3 = 3,     /* tcgen05 kind::f16, fp16 hi/lo with scaling, 3 products */
-    KIFMM_M2L_FP64 = 4        /* FP64 tiles (as in KIFMM_PREC_FP64) */
+    KIFMM_M2L_FP64 = 4,       /* FP64 tiles (the KIFMM_PREC_FP64 form) */
+    KIFMM_M2L_INT8 = 5        /* tcgen05 kind::i8: operator and vectors as five signed 7-bit
+                                 slices, exact int32 accumulation, FP64 reconstruction */
 };
 
 typedef struct kifmm_options {
@@ -77,7 +79,8 @@ typedef struct kifmm_options {
     int32_t radii;      /* 0 (default): the reference's circles r1=(sqrt2+0.01)w/2,
                            r2=(4-sqrt2-0.02)w/2 (class_fmm.py:35-45); 1: 1.5 and 2.5 half-widths */
     int32_t device;     /* CUDA device ordinal */
-    int32_t reserved;
+    int32_t near_fp64;  /* with KIFMM_PREC_MIXED: 1 keeps P2M, L2P and P2P in FP64 (only M2L
+                           takes the mixed form); 0 (default): FP32 near field */
     void *stream;       /* cudaStream_t to order work on (cudaStreamLegacy, i.e. 0x1, for the
                            legacy default stream); NULL: the plan creates its own stream */
 } kifmm_options;

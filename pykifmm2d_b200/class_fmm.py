@@ -178,7 +178,7 @@ def get_level_information(node_width, theta, radii="reference"):
 
 _PREC = {"fp64": B.PREC_FP64, "plain": B.PREC_FP64, "mixed": B.PREC_MIXED}
 _M2L = {"auto": B.M2L_AUTO, "fp32": B.M2L_FP32, "bf16x3": B.M2L_BF16X3, "fp16x3": B.M2L_FP16X3,
-        "fp64": B.M2L_FP64}
+        "fp64": B.M2L_FP64, "int8": B.M2L_INT8}
 
 
 class FMM(object):
@@ -190,6 +190,7 @@ class FMM(object):
                  compensated M2L); m2l selects the mixed M2L form;
       fix_bbox   False keeps the reference's root box (tree.py:475-484);
       radii      'reference' or '1.5/2.5';
+      near_fp64  with precision='mixed', keep P2M/L2P/P2P in FP64;
       device, stream   CUDA device ordinal and stream handle.
     Unlike the reference, repeated ``build_expansions`` calls on one object
     are exact (workspaces are zeroed on every apply).
@@ -197,7 +198,7 @@ class FMM(object):
 
     def __init__(self, x, y, kernel_functions, numba_functions, Nequiv=48, Ncutoff=50, iscomplex=False,
                  verbose=False, precision="fp64", m2l="auto", fix_bbox=False, radii="reference", device=None,
-                 stream=None):
+                 stream=None, near_fp64=False):
         if iscomplex:
             raise NotImplementedError("complex kernels are not part of this build")
         kern = None
@@ -229,6 +230,7 @@ class FMM(object):
         opts.m2l = _M2L[m2l]
         opts.fix_bbox = int(bool(fix_bbox))
         opts.radii = 0 if radii == "reference" else 1
+        opts.near_fp64 = int(bool(near_fp64))
         if device is None:
             device = x.device.index if self._on_device and x.device.index is not None else 0
         opts.device = int(device)

@@ -90,13 +90,26 @@ static void copy_in(kifmm_plan *P, DBuf<double> &dst, const double *src, int64_t
                                    P->stream));
 }
 
+// Device-side failures reported through a flag (a tensor-core M2L wait that
+// ran out of its poll budget); read after the stream has drained.
+static void check_device_flags(kifmm_plan *P) {
+    if (!uses_tensor_m2l(P) || !P->scal.p) return;
+    unsigned long long f = 0;
+    KIFMM_CUDA(cudaMemcpyAsync(&f, P->scal.p + 15, sizeof(f), cudaMemcpyDeviceToHost, P->stream));
+    KIFMM_CUDA(cudaStreamSynchronize(P->stream));
+    KIFMM_REQUIRE(f == 0, KIFMM_ERR_CUDA, "tensor-core M2L: an MMA completion wait timed out");
+}
+
 static void copy_out(kifmm_plan *P, double *dst, const double *src, int64_t n, int mem) {
     KIFMM_REQUIRE(dst || n == 0, KIFMM_ERR_ARG, "null output pointer");
     if (n)
         KIFMM_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(double),
                                    mem == KIFMM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
                                    P->stream));
-    if (mem == KIFMM_MEM_HOST) KIFMM_CUDA(cudaStreamSynchronize(P->stream));
+    if (mem == KIFMM_MEM_HOST) {
+        KIFMM_CUDA(cudaStreamSynchronize(P->stream));
+        check_device_flags(P);
+    }
 }
 
 static void check_kernel(const kifmm_kernel *k) {
@@ -148,7 +161,8 @@ int kifmm_plan_create(const kifmm_kernel *kernel, int32_t nequiv, int32_t ncutof
         if (opts) o = *opts;
         KIFMM_REQUIRE(o.precision == KIFMM_PREC_FP64 || o.precision == KIFMM_PREC_MIXED, KIFMM_ERR_ARG,
                       "unknown precision");
-        KIFMM_REQUIRE(o.m2l >= KIFMM_M2L_AUTO && o.m2l <= KIFMM_M2L_FP64, KIFMM_ERR_ARG, "unknown M2L form");
+        KIFMM_REQUIRE(o.m2l >= KIFMM_M2L_AUTO && o.m2l <= KIFMM_M2L_INT8, KIFMM_ERR_ARG, "unknown M2L form");
+        if (o.precision == KIFMM_PREC_MIXED && o.m2l == KIFMM_M2L_AUTO) o.m2l = KIFMM_M2L_INT8;
         KIFMM_REQUIRE(o.radii == 0 || o.radii == 1, KIFMM_ERR_ARG, "unknown radii preset");
         KIFMM_REQUIRE(!(o.precision == KIFMM_PREC_MIXED && o.m2l == KIFMM_M2L_FP64), KIFMM_ERR_ARG,
                       "an FP64 M2L belongs to the FP64 precision form");
@@ -244,6 +258,7 @@ int kifmm_synchronize(kifmm_plan *P) {
         KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
         use_device(P);
         KIFMM_CUDA(cudaStreamSynchronize(P->stream));
+        check_device_flags(P);
     });
 }
 

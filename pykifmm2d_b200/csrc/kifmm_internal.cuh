@@ -7,7 +7,7 @@
 #include <string>
 #include <vector>
 
-#include "../../include/kifmm2d.h"
+#include "kifmm2d.h"  // include/ (on the include path)
 
 // ----------------------------------------------------------------- errors
 namespace kifmm {
@@ -175,11 +175,14 @@ struct kifmm_plan {
     kifmm::DBuf<float> ops_f;        // FP32 copies for the mixed passes
     kifmm::DBuf<uint16_t> ops_h;     // split half-precision M2L operators
     size_t ops_stride = 0;           // doubles per level block
+    kifmm::DBuf<unsigned char> tc_a; // tensor-core M2L operator slices
+    kifmm::DBuf<double> tc_rowscale;
+    kifmm::DBuf<unsigned char> tc_pre;  // per-apply slices of the source groups
+    kifmm::DBuf<int> tc_gexp;
 
     // workspaces
     kifmm::DBuf<double> tau, taus, pots, pot_out, tx, ty, tpot;
     kifmm::DBuf<double> uup, udown;
-    kifmm::DBuf<float> uup_f, udown_f;
     bool have_expansions = false;
 
     // scratch for the tree build
@@ -311,6 +314,9 @@ void kernel_matrix_device(const kifmm_kernel &k, const double *sx, const double 
 void kernel_apply_device(const kifmm_kernel &k, const double *sx, const double *sy, int64_t ns,
                          const double *tx, const double *ty, int64_t nt, const double *tau, double *out,
                          cudaStream_t s);
+// m2l_tc.cu
+void build_tc_operators(kifmm_plan *P);
+bool uses_tensor_m2l(const kifmm_plan *P);
 // radix_sort.cu
 void radix_sort_pairs(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_tmp, int64_t n, int bits,
                       kifmm_plan *P);

@@ -257,6 +257,7 @@ void build_operators(kifmm_plan *P) {
         P->ops_f.alloc(A.stride * (size_t)L);
         k_to_float<<<grid_for(A.stride * L, 256, 4096), 256, 0, s>>>(P->ops.p, P->ops_f.p, A.stride * (size_t)L);
         KIFMM_LAUNCHED();
+        if (uses_tensor_m2l(P) && L >= 3) build_tc_operators(P);
     }
     P->have_ops = true;
 }

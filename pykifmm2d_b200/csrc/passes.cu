@@ -204,6 +204,29 @@ __global__ void k_leaf_eval_d(PassArgs A, const int32_t *__restrict__ list, int 
     }
 }
 
+// L2L alone, added onto the M2L result: u_down(children of a split entry) +=
+// L2L_l u_down(parent).  One warp per entry.
+__global__ void k_l2l_d(PassArgs A, int l) {
+    extern __shared__ double svl[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    int64_t e = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int Q = A.Q, Q4 = 4 * Q;
+    double *v = svl + (size_t)wib * Q;
+    bool active = e < A.T.ne[l] && !(A.ent[A.T.eoff[l] + e] & 1);
+    int p = active ? A.ent_node[A.T.eoff[l] + e] : 0;
+    if (active)
+        for (int c = lane; c < Q; c += 32) v[c] = A.udown[(size_t)p * Q + c];
+    __syncwarp();
+    if (!active) return;
+    int64_t c0 = A.T.off[l + 1] + 4 * e;
+    const double *op = A.ops + (size_t)l * A.stride + A.off_l2l;
+    for (int r = lane; r < Q4; r += 32) {
+        double acc = 0.0;
+        for (int c = 0; c < Q; c++) acc = fma(op[(size_t)c * Q4 + r], v[c], acc);
+        A.udown[(size_t)c0 * Q + r] += acc;
+    }
+}
+
 // Evaluation at arbitrary targets: locate by strict '>' descent
 // (numba_locate_points, tree.py:712-727), then L2P and P2P.
 __global__ void k_eval_targets_d(PassArgs A, const double *__restrict__ tx, const double *__restrict__ ty, int64_t n,
@@ -276,9 +299,38 @@ PassArgs make_pass_args(kifmm_plan *P) {
     A.pots = P->pots.p;
     A.uup = P->uup.p;
     A.udown = P->udown.p;
-    A.uup_f = P->uup_f.p;
-    A.udown_f = P->udown_f.p;
     return A;
+}
+
+void launch_p2m_d(kifmm_plan *P, const PassArgs &A) {
+    k_p2m_d<<<grid_for(P->n_p2m_list * 32, 256), 256, 0, P->stream>>>(A, P->p2m_list.p, P->n_p2m_list);
+    KIFMM_LAUNCHED();
+}
+
+void launch_leaf_eval_d(kifmm_plan *P, const PassArgs &A, int check_self) {
+    int thr = P->ppl <= 64 ? 64 : 128;
+    size_t smem = (size_t)(P->Q + 3 * thr) * sizeof(double);
+    k_leaf_eval_d<<<(unsigned)P->n_leaf_list, thr, smem, P->stream>>>(A, P->leaf_list.p, check_self);
+    KIFMM_LAUNCHED();
+}
+
+void launch_eval_targets_d(kifmm_plan *P, const PassArgs &A, const double *tx, const double *ty, int64_t n,
+                           int check_self, double *pot) {
+    k_eval_targets_d<<<grid_for(n, 128, P->num_sms * 16), 128, 0, P->stream>>>(A, tx, ty, n, check_self, pot);
+    KIFMM_LAUNCHED();
+}
+
+void launch_m2m_d(kifmm_plan *P, const PassArgs &A, int l) {
+    int64_t ne = P->lt.ne[l];
+    size_t smem = (size_t)8 * 4 * P->Q * sizeof(double);
+    k_m2m_d<<<grid_for(ne * 32, 256), 256, smem, P->stream>>>(A, l);
+    KIFMM_LAUNCHED();
+}
+
+void launch_l2l_d(kifmm_plan *P, const PassArgs &A, int l) {
+    int64_t ne = P->lt.ne[l];
+    k_l2l_d<<<grid_for(ne * 32, 256), 256, (size_t)8 * P->Q * sizeof(double), P->stream>>>(A, l);
+    KIFMM_LAUNCHED();
 }
 
 void run_upward_downward(kifmm_plan *P) {
@@ -301,8 +353,7 @@ void run_upward_downward(kifmm_plan *P) {
     PassArgs A = make_pass_args(P);
     if (P->n_p2m_list) {
         PhaseScope ph(P, KIFMM_PHASE_P2M);
-        k_p2m_d<<<grid_for(P->n_p2m_list * 32, 256), 256, 0, s>>>(A, P->p2m_list.p, P->n_p2m_list);
-        KIFMM_LAUNCHED();
+        launch_p2m_d(P, A);
     }
     {
     PhaseScope ph_m2m(P, KIFMM_PHASE_M2M);
@@ -334,12 +385,9 @@ void run_eval_sources(kifmm_plan *P, int check_self) {
         run_eval_sources_mixed(P, check_self);
     } else {
         PassArgs A = make_pass_args(P);
-        int thr = P->ppl <= 64 ? 64 : 128;
-        size_t smem = (size_t)(P->Q + 3 * thr) * sizeof(double);
         if (P->n_leaf_list) {
             PhaseScope ph(P, KIFMM_PHASE_LEAF);
-            k_leaf_eval_d<<<(unsigned)P->n_leaf_list, thr, smem, s>>>(A, P->leaf_list.p, check_self);
-            KIFMM_LAUNCHED();
+            launch_leaf_eval_d(P, A, check_self);
         }
     }
     k_scatter_pot<<<grid_for(n, 256, P->num_sms * 8), 256, 0, s>>>(P->pots.p, P->perm.p, n, P->pot_out.p);
@@ -352,8 +400,7 @@ void run_eval_targets(kifmm_plan *P, const double *tx, const double *ty, int64_t
         run_eval_targets_mixed(P, tx, ty, n, check_self, pot);
         return;
     }
-    k_eval_targets_d<<<grid_for(n, 128, P->num_sms * 16), 128, 0, P->stream>>>(A, tx, ty, n, check_self, pot);
-    KIFMM_LAUNCHED();
+    launch_eval_targets_d(P, A, tx, ty, n, check_self, pot);
 }
 
 // ------------------------------------------------ kernel-function utilities

@@ -21,7 +21,6 @@ struct PassArgs {
     const double *xs, *ys, *taus;
     double *pots;
     double *uup, *udown;
-    float *uup_f, *udown_f;
 };
 
 // Node centre, exactly the reference's xmid = xmin + w/2 (tree.py:339-346):

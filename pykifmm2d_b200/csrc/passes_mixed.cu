@@ -1,14 +1,18 @@
 // passes_mixed.cu -- mixed-precision passes.
 //
 // Same algorithm as passes.cu (reference class_fmm.py:299-399) with
-//   * P2M, L2P and P2P in FP32 on coordinates relative to the box centre
-//     (FP64 subtraction, then rounding: nearby points keep their relative
-//     precision wherever the box sits, as the reference's L2P does with
-//     tx = x - xmid, class_fmm.py:81-82);
-//   * check potentials u_up / u_down stored in FP32;
-//   * M2M, L2L and M2L applied with FP32 operators (the FP64 operators of
-//     operators.cu rounded once), M2L either on the CUDA cores (this file) or
-//     on the tensor cores with compensated half-precision splits (m2l_tc.cu);
+//   * P2P in FP32 on coordinates relative to the box centre (FP64
+//     subtraction, then rounding: nearby points keep their relative precision
+//     wherever the box sits, as the reference's L2P does with tx = x - xmid,
+//     class_fmm.py:81-82);
+//   * P2M and L2P in FP64: their terms are weighted by equivalent densities
+//     of alternating sign, and FP32 logs there cost ~1.6e-7 each at 1M points
+//     (measured), while they are only Q evaluations per point;
+//   * check potentials u_up / u_down kept in FP64, M2M and L2L in FP64 (a few
+//     percent of the work);
+//   * M2L on the tensor cores (m2l_tc.cu): int8 slices with exact int32
+//     accumulation (default), or bf16 / fp16 hi-lo splits with FP32
+//     accumulation; or FP32 tiles on the CUDA cores (this file);
 //   * the local expansion's equivalent density Inv_l u_down formed in FP64.
 // Coincident source/target pairs (r^2 == 0 after rounding) contribute zero.
 #include "passes.cuh"
@@ -49,62 +53,8 @@ struct Kahan {
     __device__ __forceinline__ double value() const { return (double)s - (double)c; }
 };
 
-template <int KIND>
-__global__ void k_p2m_f(PassArgs A, const int32_t *__restrict__ list, int64_t nlist) {
-    const int lane = threadIdx.x & 31;
-    int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (w >= nlist) return;
-    int g = list[w];
-    int l = A.nlev[g];
-    double cx, cy;
-    node_center(A, g, l, cx, cy);
-    const bool lap = KIND == KIFMM_KERNEL_LAPLACE;
-    const double sc = lap ? 1.0 / ldexp(A.W, -l) : 1.0;
-    const double lw = lap ? -2.0 * log2(sc) : 0.0;
-    const float fsc = (float)sc;
-    const float *lg = A.ops_f + (size_t)l * A.stride + A.off_large;
-    const float kk = (float)A.k;
-    const int b = A.nbot[g], e = A.ntop[g];
-    for (int q0 = 0; q0 < A.Q; q0 += 32) {
-        int q = q0 + lane;
-        bool ok = q < A.Q;
-        float tx = ok ? lg[q] * fsc : 0.f, ty = ok ? lg[A.Q + q] * fsc : 0.f;
-        Kahan acc;
-        double tsum = 0.0;
-        for (int s = b; s < e; s++) {
-            float dx = tx - (float)((A.xs[s] - cx) * sc), dy = ty - (float)((A.ys[s] - cy) * sc);
-            float r2 = fmaf(dx, dx, dy * dy);
-            acc.fma_add((float)A.taus[s], gsum_term<KIND>(r2, kk));
-            tsum += A.taus[s];
-        }
-        double v = acc.value() + (lap ? lw * tsum : 0.0);
-        if (ok) A.uup_f[(size_t)g * A.Q + q] = (float)(v * (double)gsum_scale<KIND>());
-    }
-}
-
-__global__ void k_m2m_f(PassArgs A, int l) {
-    extern __shared__ float svf[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    int64_t e = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int Q = A.Q, Q4 = 4 * Q;
-    float *v = svf + (size_t)wib * Q4;
-    bool active = e < A.T.ne[l];
-    int64_t j = A.T.eoff[l] + e;
-    int64_t c0 = active ? A.T.off[l + 1] + 4 * e : 0;
-    if (active)
-        for (int c = lane; c < Q4; c += 32) v[c] = A.uup_f[(size_t)c0 * Q + c];
-    __syncwarp();
-    if (!active) return;
-    int g = A.ent_node[j];
-    const float *op = A.ops_f + (size_t)l * A.stride + A.off_m2m;
-    for (int r = lane; r < Q; r += 32) {
-        float acc = 0.f;
-        for (int c = 0; c < Q4; c++) acc = fmaf(op[(size_t)c * Q + r], v[c], acc);
-        A.uup_f[(size_t)g * Q + r] = acc;
-    }
-}
-
-// FP32 M2L + L2L on the CUDA cores: block = 4Q rows x TE target groups.
+// FP32 M2L + L2L on the CUDA cores (FP64 state in and out): block = 4Q rows x
+// TE target groups.
 constexpr int M2LF_TE = 32;
 __global__ void k_m2l_f(PassArgs A, int l) {
     extern __shared__ float smf[];
@@ -144,7 +94,7 @@ __global__ void k_m2l_f(PassArgs A, int l) {
         for (int idx = threadIdx.x; idx < M2LF_TE * Q4; idx += blockDim.x) {
             int t = idx / Q4, c = idx % Q4;
             int64_t grp = sgrp[t];
-            src[idx] = grp >= 0 ? A.uup_f[(size_t)grp * Q + c] : 0.f;
+            src[idx] = grp >= 0 ? (float)A.uup[(size_t)grp * Q + c] : 0.f;
         }
         __syncthreads();
         const float *op = opl + (size_t)d * Q4 * Q4;
@@ -160,7 +110,7 @@ __global__ void k_m2l_f(PassArgs A, int l) {
         for (int idx = threadIdx.x; idx < M2LF_TE * Q; idx += blockDim.x) {
             int t = idx / Q, c = idx % Q;
             int p = spar[t];
-            src[idx] = p >= 0 ? A.udown_f[(size_t)p * Q + c] : 0.f;
+            src[idx] = p >= 0 ? (float)A.udown[(size_t)p * Q + c] : 0.f;
         }
         __syncthreads();
         const float *op = A.ops_f + (size_t)l * A.stride + A.off_l2l;
@@ -174,40 +124,18 @@ __global__ void k_m2l_f(PassArgs A, int l) {
     if (r < Q4)
 #pragma unroll
         for (int t = 0; t < M2LF_TE; t++)
-            if (schild[t] >= 0) A.udown_f[(size_t)schild[t] * Q + r] = acc[t];
+            if (schild[t] >= 0) A.udown[(size_t)schild[t] * Q + r] = (double)acc[t];
 }
 
-// L2L alone (used next to the tensor-core M2L): u_down(children) += L2L u_down(parent).
-__global__ void k_l2l_f(PassArgs A, int l) {
-    extern __shared__ float svl[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    int64_t e = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int Q = A.Q, Q4 = 4 * Q;
-    float *v = svl + (size_t)wib * Q;
-    bool active = e < A.T.ne[l] && !(A.ent[A.T.eoff[l] + e] & 1);
-    int p = active ? A.ent_node[A.T.eoff[l] + e] : 0;
-    if (active)
-        for (int c = lane; c < Q; c += 32) v[c] = A.udown_f[(size_t)p * Q + c];
-    __syncwarp();
-    if (!active) return;
-    int64_t c0 = A.T.off[l + 1] + 4 * e;
-    const float *op = A.ops_f + (size_t)l * A.stride + A.off_l2l;
-    for (int r = lane; r < Q4; r += 32) {
-        float acc = 0.f;
-        for (int c = 0; c < Q; c++) acc = fmaf(op[(size_t)c * Q4 + r], v[c], acc);
-        A.udown_f[(size_t)c0 * Q + r] += acc;
-    }
-}
-
-// Equivalent density of the local expansion, FP64 product of the FP32 check
-// potential, for the leaves a warp evaluates.
-__device__ __forceinline__ void local_density(const PassArgs &A, int g, int l, float *qd, int lane) {
+// Equivalent density of the local expansion (FP64), for the leaves a warp
+// evaluates.
+__device__ __forceinline__ void local_density(const PassArgs &A, int g, int l, double *qd, int lane) {
     const double *inv = A.ops + (size_t)l * A.stride + A.off_inv;
     for (int r = lane; r < A.Q; r += 32) {
         double s = 0.0;
         if (l >= 2)
-            for (int c = 0; c < A.Q; c++) s = fma(inv[r * A.Q + c], (double)A.udown_f[(size_t)g * A.Q + c], s);
-        qd[r] = (float)s;
+            for (int c = 0; c < A.Q; c++) s = fma(inv[r * A.Q + c], A.udown[(size_t)g * A.Q + c], s);
+        qd[r] = s;
     }
 }
 
@@ -221,7 +149,7 @@ template <int KIND>
 __global__ void __launch_bounds__(32 * LEAF_WARPS) k_leaf_eval_f(PassArgs A, const int32_t *__restrict__ list,
                                                                  int64_t nlist) {
     __shared__ float4 tile[LEAF_WARPS][32];
-    __shared__ float qds[LEAF_WARPS][64];
+    __shared__ double qds[LEAF_WARPS][64];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     int64_t w = (int64_t)blockIdx.x * LEAF_WARPS + wib;
     if (w >= nlist) return;
@@ -229,7 +157,7 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS) k_leaf_eval_f(PassArgs A, con
     const int l = A.nlev[g];
     double cx, cy;
     node_center(A, g, l, cx, cy);
-    float *qd = qds[wib];
+    double *qd = qds[wib];
     local_density(A, g, l, qd, lane);
     __syncwarp();
     const bool lap = KIND == KIFMM_KERNEL_LAPLACE;
@@ -237,8 +165,6 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS) k_leaf_eval_f(PassArgs A, con
     const double sc = lap ? 1.0 / width : 1.0;     // coordinate scale
     const double lw = lap ? -2.0 * log2(sc) : 0.0; // log2 of the squared length unit
     const float kk = (float)A.k;
-    const float fsc = (float)sc;
-    const float *lg = A.ops_f + (size_t)l * A.stride + A.off_large;
     const int b = A.nbot[g], e = A.ntop[g];
     int coll[9];
 #pragma unroll
@@ -247,14 +173,14 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS) k_leaf_eval_f(PassArgs A, con
         const int t = t0 + lane;
         const bool act = t < e;
         const float tx = act ? (float)((A.xs[t] - cx) * sc) : 0.f, ty = act ? (float)((A.ys[t] - cy) * sc) : 0.f;
-        // far field: equivalent density on the (scaled) check circle
-        Kahan far;
-        double qsum = 0.0;
-        if (l >= 2) {
+        // far field (L2P) in FP64: equivalent density on the check circle
+        double far = 0.0;
+        if (l >= 2 && act) {
+            const double *lgd = A.ops + (size_t)l * A.stride + A.off_large;
+            const double px = A.xs[t] - cx, py = A.ys[t] - cy;
             for (int q = 0; q < A.Q; q++) {
-                float dx = tx - lg[q] * fsc, dy = ty - lg[A.Q + q] * fsc;
-                far.fma_add(qd[q], gsum_term<KIND>(fmaf(dx, dx, dy * dy), kk));
-                qsum += (double)qd[q];
+                double dx = px - lgd[q], dy = py - lgd[A.Q + q];
+                far = fma(green_d(A.kind, A.k, dx * dx + dy * dy), qd[q], far);
             }
         }
         Kahan near;
@@ -293,9 +219,9 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS) k_leaf_eval_f(PassArgs A, con
             }
         }
         if (act) {
-            double v = far.value() + near.value();
-            if (lap) v += lw * (qsum + tsum - (double)excl);
-            A.pots[t] = v * (double)gsum_scale<KIND>();
+            double v = near.value();
+            if (lap) v += lw * (tsum - (double)excl);
+            A.pots[t] = v * (double)gsum_scale<KIND>() + far;
         }
     }
 }
@@ -317,17 +243,18 @@ __global__ void k_eval_targets_f(PassArgs A, const double *__restrict__ tx, cons
         double cx, cy;
         node_center(A, g, l, cx, cy);
         const float rx = (float)(px - cx), ry = (float)(py - cy);
-        float acc = 0.f;
+        double far = 0.0;  // L2P in FP64
         if (l >= 2) {
             const double *inv = A.ops + (size_t)l * A.stride + A.off_inv;
-            const float *lg = A.ops_f + (size_t)l * A.stride + A.off_large;
+            const double *lgd = A.ops + (size_t)l * A.stride + A.off_large;
             for (int q = 0; q < A.Q; q++) {
                 double qd = 0.0;
-                for (int c = 0; c < A.Q; c++) qd = fma(inv[q * A.Q + c], (double)A.udown_f[(size_t)g * A.Q + c], qd);
-                float dx = rx - lg[q], dy = ry - lg[A.Q + q];
-                acc = fmaf((float)qd, gsum_term<KIND>(fmaf(dx, dx, dy * dy), kk), acc);
+                for (int c = 0; c < A.Q; c++) qd = fma(inv[q * A.Q + c], A.udown[(size_t)g * A.Q + c], qd);
+                double dx = (px - cx) - lgd[q], dy = (py - cy) - lgd[A.Q + q];
+                far = fma(green_d(A.kind, A.k, dx * dx + dy * dy), qd, far);
             }
         }
+        float acc = 0.f;
         for (int d = 0; d < 9; d++) {
             int c = A.ncoll[9 * (size_t)g + d];
             if (c < 0) continue;
@@ -337,64 +264,66 @@ __global__ void k_eval_targets_f(PassArgs A, const double *__restrict__ tx, cons
                 if (r2 > 0.f) acc = fmaf((float)A.taus[s], gsum_term<KIND>(r2, kk), acc);
             }
         }
-        pot[i] = (double)(acc * gsum_scale<KIND>());
+        pot[i] = (double)(acc * gsum_scale<KIND>()) + far;
     }
 }
 
-// tensor-core M2L (m2l_tc.cu); returns false when the form is unavailable
-bool run_m2l_tensor(kifmm_plan *P, const PassArgs &A, int l);
+// m2l_tc.cu / passes.cu
+void run_m2l_tensor(kifmm_plan *P, const PassArgs &A);
+void launch_p2m_d(kifmm_plan *P, const PassArgs &A);
+void launch_leaf_eval_d(kifmm_plan *P, const PassArgs &A, int check_self);
+void launch_eval_targets_d(kifmm_plan *P, const PassArgs &A, const double *tx, const double *ty, int64_t n,
+                           int check_self, double *pot);
+void launch_m2m_d(kifmm_plan *P, const PassArgs &A, int l);
+void launch_l2l_d(kifmm_plan *P, const PassArgs &A, int l);
 
 void run_passes_mixed(kifmm_plan *P) {
     cudaStream_t s = P->stream;
     const int Q = P->Q, L = P->L;
     int64_t NN = P->n_nodes;
-    P->uup_f.alloc((size_t)NN * Q);
-    P->udown_f.alloc((size_t)NN * Q);
-    KIFMM_CUDA(cudaMemsetAsync(P->uup_f.p, 0, (size_t)NN * Q * sizeof(float), s));
-    KIFMM_CUDA(cudaMemsetAsync(P->udown_f.p, 0, (size_t)NN * Q * sizeof(float), s));
+    KIFMM_CUDA(cudaMemsetAsync(P->uup.p, 0, (size_t)NN * Q * sizeof(double), s));
+    KIFMM_CUDA(cudaMemsetAsync(P->udown.p, 0, (size_t)NN * Q * sizeof(double), s));
     if (L < 3) return;
     PassArgs A = make_pass_args(P);
     if (P->n_p2m_list) {
         PhaseScope ph(P, KIFMM_PHASE_P2M);
-        unsigned gr = grid_for(P->n_p2m_list * 32, 256);
-        if (P->kern.kind == KIFMM_KERNEL_LAPLACE) k_p2m_f<KIFMM_KERNEL_LAPLACE><<<gr, 256, 0, s>>>(A, P->p2m_list.p, P->n_p2m_list);
-        else k_p2m_f<KIFMM_KERNEL_MOD_HELMHOLTZ><<<gr, 256, 0, s>>>(A, P->p2m_list.p, P->n_p2m_list);
-        KIFMM_LAUNCHED();
+        launch_p2m_d(P, A);
     }
     {
         PhaseScope ph(P, KIFMM_PHASE_M2M);
-        for (int l = L - 2; l >= 2; l--) {
-            int64_t ne = P->lt.ne[l];
-            if (!ne) continue;
-            k_m2m_f<<<grid_for(ne * 32, 256), 256, (size_t)8 * 4 * Q * sizeof(float), s>>>(A, l);
-            KIFMM_LAUNCHED();
-        }
+        for (int l = L - 2; l >= 2; l--)
+            if (P->lt.ne[l]) launch_m2m_d(P, A, l);
     }
     PhaseScope ph(P, KIFMM_PHASE_M2L);
+    const bool simt = P->opt.m2l == KIFMM_M2L_FP32;
     int thr = ((4 * Q + 31) / 32) * 32;
     size_t smem = (size_t)M2LF_TE * 4 * Q * sizeof(float);
-    KIFMM_CUDA(cudaFuncSetAttribute(k_m2l_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (simt) {
+        KIFMM_CUDA(cudaFuncSetAttribute(k_m2l_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    } else {
+        KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 15, 0, sizeof(unsigned long long), s));
+        run_m2l_tensor(P, A);  // all levels at once
+    }
     for (int l = 1; l <= L - 2; l++) {
         int64_t ne = P->lt.ne[l];
         if (!ne) continue;
-        bool tc = (P->opt.m2l == KIFMM_M2L_BF16X3 || P->opt.m2l == KIFMM_M2L_FP16X3) && run_m2l_tensor(P, A, l);
-        if (tc) {
-            if (l >= 2) {
-                k_l2l_f<<<grid_for(ne * 32, 256), 256, (size_t)8 * Q * sizeof(float), s>>>(A, l);
-                KIFMM_LAUNCHED();
-            }
-        } else {
+        if (simt) {
             k_m2l_f<<<(unsigned)((ne + M2LF_TE - 1) / M2LF_TE), thr, smem, s>>>(A, l);
             KIFMM_LAUNCHED();
+        } else if (l >= 2) {
+            launch_l2l_d(P, A, l);
         }
     }
 }
 
 void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
-    (void)check_self;  // coincident pairs always contribute zero in this form
     if (!P->n_leaf_list) return;
     PhaseScope ph(P, KIFMM_PHASE_LEAF);
     PassArgs A = make_pass_args(P);
+    if (P->opt.near_fp64) {
+        launch_leaf_eval_d(P, A, check_self);
+        return;
+    }  // FP32 form: coincident pairs always contribute zero
     unsigned gr = (unsigned)((P->n_leaf_list + LEAF_WARPS - 1) / LEAF_WARPS);
     if (P->kern.kind == KIFMM_KERNEL_LAPLACE)
         k_leaf_eval_f<KIFMM_KERNEL_LAPLACE><<<gr, 32 * LEAF_WARPS, 0, P->stream>>>(A, P->leaf_list.p, P->n_leaf_list);
@@ -406,8 +335,11 @@ void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
 
 void run_eval_targets_mixed(kifmm_plan *P, const double *tx, const double *ty, int64_t n, int check_self,
                             double *pot) {
-    (void)check_self;
     PassArgs A = make_pass_args(P);
+    if (P->opt.near_fp64) {
+        launch_eval_targets_d(P, A, tx, ty, n, check_self, pot);
+        return;
+    }
     unsigned gr = grid_for(n, 128, P->num_sms * 16);
     if (P->kern.kind == KIFMM_KERNEL_LAPLACE)
         k_eval_targets_f<KIFMM_KERNEL_LAPLACE><<<gr, 128, 0, P->stream>>>(A, tx, ty, n, pot);

@@ -188,3 +188,42 @@ def test_mixed_accuracy_vs_fp64_direct(golden_cases, name):
         et = rel(pt, g["pot_targets"])
         print(f"{name}: mixed targets vs reference {et:.2e}")
         assert et <= 1e-5
+
+
+# bound on (mixed form - reference FP64 output) / max|reference|, per M2L form.
+# On these small clouds (max|u| 14-34) the FP32 near field alone sits near
+# 1.5e-7; the FP32-accumulated M2L forms add their own error on top.
+M2L_FORMS = {"int8": 5e-7, "fp32": 1e-5, "bf16x3": 1e-4, "fp16x3": 1e-5}
+
+
+@pytest.mark.parametrize("form", sorted(M2L_FORMS))
+@pytest.mark.parametrize("name", ["uniform3k_cut16", "c1_uniform20k", "mix2k_cut8", "annulus6k_k0"])
+def test_mixed_m2l_forms_vs_reference(golden_cases, name, form):
+    """Each mixed M2L form against the reference's FP64 output: int8 slices
+    (exact int32 accumulation) hold the plain form's accuracy; the FP32-
+    accumulated forms stay within their stated bounds."""
+    g = golden_cases[name]
+    f = make(g, precision="mixed", m2l=form)
+    f.build_expansions(g["tau"])
+    pot = f.evaluate_to_points(f.x, f.y, True)
+    e = rel(pot, g["pot"])
+    fin = np.isfinite(g["direct"])
+    e_ref = np.abs(g["pot"] - g["direct"])[fin].max() / np.abs(g["direct"][fin]).max()
+    print(f"{name} m2l={form}: mixed vs reference {e:.2e} (reference FMM vs direct {e_ref:.2e})")
+    # never more than a fifth of the reference's own discretisation error on coarse cases
+    assert e <= max(M2L_FORMS[form], 0.2 * e_ref)
+
+
+@pytest.mark.parametrize("name", ["uniform3k_cut16", "c1_uniform20k", "mix2k_cut8", "annulus6k_k0", "cluster_dup"])
+def test_int8_tensor_m2l_is_fp64_accurate(golden_cases, name):
+    """Tensor-core M2L on int8 slices (exact int32 accumulation) with the
+    near field kept in FP64: must reproduce the reference's FP64 output to
+    <= 1e-8 (measured 2e-9, from the 7-bit quantised group exponents), below
+    the FP64 form's own error against the direct sum on these cases."""
+    g = golden_cases[name]
+    f = make(g, precision="mixed", m2l="int8", near_fp64=True)
+    f.build_expansions(g["tau"])
+    pot = f.evaluate_to_points(f.x, f.y, True)
+    e = rel(pot, g["pot"])
+    print(f"{name}: int8 tensor M2L + FP64 near field vs reference {e:.2e}")
+    assert e <= 1e-8
