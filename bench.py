@@ -434,9 +434,26 @@ def main():
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-run", action="store_true",
+                    help="only the timed pipeline steps (for ncu launch lists); prints phase times")
+    ap.add_argument("--n", type=int, default=0, help="override the number of points (profiling small cases)")
     args = ap.parse_args()
-    cfg = CONFIGS[args.config]
+    cfg = dict(CONFIGS[args.config])
+    if args.n:
+        cfg["n"] = args.n
+        cfg["desc"] += f" (N overridden to {args.n})"
     world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.profile_run:
+        import torch
+        from pykifmm2d_b200 import _lib as B
+        x, y, tau = cfg["gen"](cfg["n"], 0)
+        xd, yd, td = (torch.from_numpy(v).cuda() for v in (x, y, tau))
+        flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+        times, launches, phase, _, _ = time_full_steps(torch, cfg, xd, yd, td, args.precision, args.steps,
+                                                       args.warmup, flush, profile=True)
+        print(json.dumps({"ms_per_step": statistics.mean(times), "launches_per_step": launches / args.steps,
+                          "phases_ms": {nm: float(v) for nm, v in zip(B.PHASES, phase)}}))
+        return 0
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
         if rank == 0:

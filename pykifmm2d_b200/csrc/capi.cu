@@ -266,6 +266,8 @@ int kifmm_get_tree_info(kifmm_plan *P, kifmm_tree_info *info) {
     return guarded([&] {
         KIFMM_REQUIRE(P && info, KIFMM_ERR_ARG, "null argument");
         KIFMM_REQUIRE(P->have_tree, KIFMM_ERR_STATE, "tree_info: no tree");
+        use_device(P);
+        tree_stats(P);
         memset(info, 0, sizeof(*info));
         info->n_points = P->N;
         info->levels = P->L;

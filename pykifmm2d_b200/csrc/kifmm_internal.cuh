@@ -167,6 +167,7 @@ struct kifmm_plan {
     int64_t n_leaf_list = 0, n_p2m_list = 0;
     int64_t n_leaves = 0, n_fake = 0, n_xlist = 0;
     int64_t n_p2p_pairs = 0, n_p2m_points = 0, n_m2l_pairs = 0, n_m2l_groups = 0;
+    bool have_stats = false;
 
     // operators
     bool have_ops = false;
@@ -301,6 +302,7 @@ inline unsigned grid_for(int64_t n, int block, int cap = 1 << 20) {
 // tree.cu
 void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int mem);
 void export_tree(kifmm_plan *P, int64_t *nodes, int64_t *point_leaf);
+void tree_stats(kifmm_plan *P);
 // operators.cu
 void build_operators(kifmm_plan *P);
 // passes.cu
@@ -321,5 +323,7 @@ bool uses_tensor_m2l(const kifmm_plan *P);
 void radix_sort_pairs(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_tmp, int64_t n, int bits,
                       kifmm_plan *P);
 void radix_sort_keys(uint64_t *key, uint64_t *key_tmp, int64_t n, int bits, kifmm_plan *P);
+void radix_sort_pairs_bits(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_tmp, int64_t n, int lo_bit,
+                           int bits, kifmm_plan *P);
 
 }  // namespace kifmm

@@ -182,17 +182,21 @@ struct TcOpsArgs {
     double *rowscale;        // [L][MP]
 };
 
-__global__ void k_tc_rowscale(TcOpsArgs T) {
-    const int l = blockIdx.x;
+// row scales: block (level, 32 rows), thread (row, direction)
+__global__ void __launch_bounds__(256) k_tc_rowscale(TcOpsArgs T) {
+    __shared__ double part[8][32];
+    const int l = blockIdx.x, r = blockIdx.y * 32 + threadIdx.x % 32, dg = threadIdx.x / 32;
+    const int d = dg < 4 ? dg : dg + 1;  // the eight parent directions
     const int Q4 = T.g.Q4;
-    for (int r = threadIdx.x; r < T.g.MP; r += blockDim.x) {
-        double m = 0.0;
-        if (r < Q4 && l >= 2)
-            for (int d = 0; d < 9; d++) {
-                if (d == 4) continue;
-                const double *C = T.ops + (size_t)l * T.stride + T.off_m2l + (size_t)d * Q4 * Q4;
-                for (int c = 0; c < Q4; c++) m = fmax(m, fabs(C[(size_t)c * Q4 + r]));
-            }
+    double m = 0.0;
+    if (r < Q4 && l >= 2) {
+        const double *C = T.ops + (size_t)l * T.stride + T.off_m2l + (size_t)d * Q4 * Q4;
+        for (int c = 0; c < Q4; c++) m = fmax(m, fabs(C[(size_t)c * Q4 + r]));
+    }
+    part[dg][threadIdx.x % 32] = m;
+    __syncthreads();
+    if (threadIdx.x < 32 && r < T.g.MP) {
+        for (int i = 1; i < 8; i++) m = fmax(m, part[i][threadIdx.x]);
         T.rowscale[(size_t)l * T.g.MP + r] = pow2_scale(m);
     }
 }
@@ -495,7 +499,7 @@ static void build_tc_ops_t(kifmm_plan *P) {
     T.g = g;
     T.aslices = P->tc_a.p;
     T.rowscale = P->tc_rowscale.p;
-    k_tc_rowscale<<<P->L, 256, 0, P->stream>>>(T);
+    k_tc_rowscale<<<dim3(P->L, g.MP / 32), 256, 0, P->stream>>>(T);
     KIFMM_LAUNCHED();
     k_tc_slices<F><<<dim3(P->L, 9), 256, 0, P->stream>>>(T);
     KIFMM_LAUNCHED();

@@ -21,12 +21,12 @@ void radix_sort_pairs_scratch(uint64_t *key, int32_t *val, uint64_t *key_tmp, in
                               int64_t n, int bits, cudaStream_t stream);
 
 // Scratch layout: key ping-pong [NMAX] u64 | index ping-pong [NMAX] i32 |
-// digit histograms [256 * NMAX/4096] u32 | one u64 counter.  About 12.3 MB.
+// digit histograms [256 * NMAX/4096 + 256] u32 | one u64 counter.  About 12.3 MB.
 constexpr int64_t NA_MAX = KIFMM_NOALLOC_MAX_POINTS;
 constexpr size_t NA_KEY_OFF = 0;
 constexpr size_t NA_IDX_OFF = NA_KEY_OFF + (size_t)NA_MAX * 8;
 constexpr size_t NA_HIST_OFF = NA_IDX_OFF + (size_t)NA_MAX * 4;
-constexpr size_t NA_CNT_OFF = NA_HIST_OFF + (size_t)256 * (NA_MAX / 4096) * 4;
+constexpr size_t NA_CNT_OFF = NA_HIST_OFF + ((size_t)256 * (NA_MAX / 4096) + 256) * 4;
 constexpr size_t NA_BYTES = NA_CNT_OFF + 256;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];

@@ -47,29 +47,6 @@ __global__ void k_p2m_d(PassArgs A, const int32_t *__restrict__ list, int64_t nl
     }
 }
 
-// M2M for the entries (split or X-list cells) of level l: one warp each.
-__global__ void k_m2m_d(PassArgs A, int l) {
-    extern __shared__ double sv[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    int64_t e = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int Q = A.Q, Q4 = 4 * Q;
-    double *v = sv + (size_t)wib * Q4;
-    bool active = e < A.T.ne[l];
-    int64_t j = A.T.eoff[l] + e;
-    int64_t c0 = active ? A.T.off[l + 1] + 4 * e : 0;
-    if (active)
-        for (int c = lane; c < Q4; c += 32) v[c] = A.uup[(size_t)c0 * Q + c];
-    __syncwarp();
-    if (!active) return;
-    int g = A.ent_node[j];
-    const double *op = A.ops + (size_t)l * A.stride + A.off_m2m;  // [4Q][Q]
-    for (int r = lane; r < Q; r += 32) {
-        double acc = 0.0;
-        for (int c = 0; c < Q4; c++) acc = fma(op[(size_t)c * Q + r], v[c], acc);
-        A.uup[(size_t)g * Q + r] = acc;
-    }
-}
-
 // M2L + L2L into the children of the split entries of level l (targets on
 // level l+1): class_fmm.py:324-343.  A block owns M2L_TE entries and 4Q rows;
 // for each parent direction the source groups are staged in shared memory
@@ -204,29 +181,6 @@ __global__ void k_leaf_eval_d(PassArgs A, const int32_t *__restrict__ list, int 
     }
 }
 
-// L2L alone, added onto the M2L result: u_down(children of a split entry) +=
-// L2L_l u_down(parent).  One warp per entry.
-__global__ void k_l2l_d(PassArgs A, int l) {
-    extern __shared__ double svl[];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    int64_t e = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int Q = A.Q, Q4 = 4 * Q;
-    double *v = svl + (size_t)wib * Q;
-    bool active = e < A.T.ne[l] && !(A.ent[A.T.eoff[l] + e] & 1);
-    int p = active ? A.ent_node[A.T.eoff[l] + e] : 0;
-    if (active)
-        for (int c = lane; c < Q; c += 32) v[c] = A.udown[(size_t)p * Q + c];
-    __syncwarp();
-    if (!active) return;
-    int64_t c0 = A.T.off[l + 1] + 4 * e;
-    const double *op = A.ops + (size_t)l * A.stride + A.off_l2l;
-    for (int r = lane; r < Q4; r += 32) {
-        double acc = 0.0;
-        for (int c = 0; c < Q; c++) acc = fma(op[(size_t)c * Q4 + r], v[c], acc);
-        A.udown[(size_t)c0 * Q + r] += acc;
-    }
-}
-
 // Evaluation at arbitrary targets: locate by strict '>' descent
 // (numba_locate_points, tree.py:712-727), then L2P and P2P.
 __global__ void k_eval_targets_d(PassArgs A, const double *__restrict__ tx, const double *__restrict__ ty, int64_t n,
@@ -320,18 +274,115 @@ void launch_eval_targets_d(kifmm_plan *P, const PassArgs &A, const double *tx, c
     KIFMM_LAUNCHED();
 }
 
-void launch_m2m_d(kifmm_plan *P, const PassArgs &A, int l) {
+// M2M and L2L as small FP64 GEMMs per level, C[M x n] = Op[M x K] X[K x n]:
+//   M2M: M = Q, K = 4Q, X = the entries' children groups (contiguous), C -> the
+//        entries' own rows of u_up;
+//   L2L: M = 4Q, K = Q, X = the split entries' u_down (gathered), C added to
+//        their children groups.
+// A block stages the whole operator and NT columns of X in shared memory and
+// each thread accumulates a 4 x 4 register tile.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_lvl_gemm_d(PassArgs A, int l, int M, int K, int NT) {
+    extern __shared__ double sm_g[];
+    double *opS = sm_g;                       // [K][M]
+    double *xS = sm_g + (size_t)K * M;        // [NT][K + 1]
+    const int ldx = K + 1;
+    const int Q = A.Q;
+    const int64_t ne = A.T.ne[l], eoff = A.T.eoff[l], e0 = (int64_t)blockIdx.x * NT;
+    const double *op = A.ops + (size_t)l * A.stride + (MODE == 0 ? A.off_m2m : A.off_l2l);
+    // operator: 16-byte loads when aligned (odd Nequiv gives odd offsets)
+    if ((((uintptr_t)op) & 15) == 0 && (K * M) % 2 == 0)
+        for (int i = threadIdx.x; i < K * M / 2; i += blockDim.x) ((double2 *)opS)[i] = ((const double2 *)op)[i];
+    else
+        for (int i = threadIdx.x; i < K * M; i += blockDim.x) opS[i] = op[i];
+    const double *src0 = A.uup + (size_t)(A.T.off[l + 1] + 4 * e0) * Q;
+    if (MODE == 0 && (((uintptr_t)src0) & 15) == 0) {  // children groups of consecutive entries: one block
+        const int64_t nt = min((int64_t)NT, ne - e0);
+        const double2 *src = (const double2 *)src0;
+        for (int i = threadIdx.x; i < NT * K / 2; i += blockDim.x) {
+            int t = (2 * i) / K, c = (2 * i) % K;
+            double2 v = t < nt ? src[i] : make_double2(0.0, 0.0);
+            xS[t * ldx + c] = v.x;
+            xS[t * ldx + c + 1] = v.y;
+        }
+    } else {
+        for (int i = threadIdx.x; i < NT * K; i += blockDim.x) {
+            int t = i / K, c = i % K;
+            int64_t e = e0 + t;
+            double v = 0.0;
+            if (e < ne) {
+                if (MODE == 0) v = src0[(size_t)t * K + c];
+                else if (!(A.ent[eoff + e] & 1)) v = A.udown[(size_t)A.ent_node[eoff + e] * Q + c];
+            }
+            xS[t * ldx + c] = v;
+        }
+    }
+    __syncthreads();
+    const int TMr = (M + 3) / 4;
+    const int tx = threadIdx.x % TMr, ty = threadIdx.x / TMr;
+    if (ty * 4 >= NT) return;
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; i++)
+#pragma unroll
+        for (int j = 0; j < 4; j++) acc[i][j] = 0.0;
+    const int r0 = tx * 4;
+    for (int c = 0; c < K; c++) {
+        double a[4], bb[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) a[i] = r0 + i < M ? opS[c * M + r0 + i] : 0.0;
+#pragma unroll
+        for (int j = 0; j < 4; j++) bb[j] = xS[(ty * 4 + j) * ldx + c];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[i][j] = fma(a[i], bb[j], acc[i][j]);
+    }
+#pragma unroll
+    for (int j = 0; j < 4; j++) {
+        int64_t e = e0 + ty * 4 + j;
+        if (e >= ne) continue;
+        if (MODE == 0) {
+            double *dst = A.uup + (size_t)A.ent_node[eoff + e] * Q;
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                if (r0 + i < M) dst[r0 + i] = acc[i][j];
+        } else {
+            if (A.ent[eoff + e] & 1) continue;
+            double *dst = A.udown + (size_t)(A.T.off[l + 1] + 4 * e) * Q;
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                if (r0 + i < M) dst[r0 + i] += acc[i][j];
+        }
+    }
+}
+
+// NT columns per block: (ceil(M/4)) x (NT/4) threads <= 256 and at most
+// 200 KB of shared memory
+static int lvl_gemm_nt(int M, int K) {
+    int tm = (M + 3) / 4;
+    int nt = (256 / tm) * 4;
+    if (nt > 32) nt = 32;  // more blocks per level: the levels are small
+    int cap = (int)(((200 << 10) / 8 - (int64_t)K * M) / (K + 1)) / 4 * 4;
+    if (nt > cap) nt = cap;
+    return nt < 4 ? 4 : nt;
+}
+
+template <int MODE>
+static void launch_lvl_gemm(kifmm_plan *P, const PassArgs &A, int l) {
+    const int Q = P->Q;
+    const int M = MODE == 0 ? Q : 4 * Q, K = MODE == 0 ? 4 * Q : Q;
+    int nt = lvl_gemm_nt(M, K);
+    int threads = ((M + 3) / 4) * (nt / 4);
+    size_t smem = ((size_t)K * M + (size_t)nt * (K + 1)) * sizeof(double);
+    KIFMM_CUDA(cudaFuncSetAttribute(k_lvl_gemm_d<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int64_t ne = P->lt.ne[l];
-    size_t smem = (size_t)8 * 4 * P->Q * sizeof(double);
-    k_m2m_d<<<grid_for(ne * 32, 256), 256, smem, P->stream>>>(A, l);
+    k_lvl_gemm_d<MODE><<<(unsigned)((ne + nt - 1) / nt), threads, smem, P->stream>>>(A, l, M, K, nt);
     KIFMM_LAUNCHED();
 }
 
-void launch_l2l_d(kifmm_plan *P, const PassArgs &A, int l) {
-    int64_t ne = P->lt.ne[l];
-    k_l2l_d<<<grid_for(ne * 32, 256), 256, (size_t)8 * P->Q * sizeof(double), P->stream>>>(A, l);
-    KIFMM_LAUNCHED();
-}
+void launch_m2m_d(kifmm_plan *P, const PassArgs &A, int l) { launch_lvl_gemm<0>(P, A, l); }
+void launch_l2l_d(kifmm_plan *P, const PassArgs &A, int l) { launch_lvl_gemm<1>(P, A, l); }
 
 void run_upward_downward(kifmm_plan *P) {
     cudaStream_t s = P->stream;
@@ -356,14 +407,9 @@ void run_upward_downward(kifmm_plan *P) {
         launch_p2m_d(P, A);
     }
     {
-    PhaseScope ph_m2m(P, KIFMM_PHASE_M2M);
-    for (int l = L - 2; l >= 2; l--) {
-        int64_t ne = P->lt.ne[l];
-        if (!ne) continue;
-        size_t smem = (size_t)8 * 4 * Q * sizeof(double);
-        k_m2m_d<<<grid_for(ne * 32, 256), 256, smem, s>>>(A, l);
-        KIFMM_LAUNCHED();
-    }
+        PhaseScope ph_m2m(P, KIFMM_PHASE_M2M);
+        for (int l = L - 2; l >= 2; l--)
+            if (P->lt.ne[l]) launch_m2m_d(P, A, l);
     }
     PhaseScope ph(P, KIFMM_PHASE_M2L);
     int thr = ((4 * Q + 31) / 32) * 32;

@@ -3,10 +3,12 @@
 //
 // Each pass sorts one 8-bit digit in three kernels:
 //   1. per-tile digit histograms (tile = 256 threads x 16 keys),
-//   2. one exclusive scan over the digit-major histogram table,
+//   2. a per-digit exclusive scan over the tiles (one block per digit), which
+//      also leaves the 256 digit totals behind the table,
 //   3. a stable scatter: inside a tile, each warp ranks its 512 keys in order
 //      with __match_any_sync, warps are combined by a per-digit prefix in
-//      shared memory, and the tile's base comes from the scanned table.
+//      shared memory, and the tile's base is the digit's start (a scan of the
+//      digit totals) plus the digit's scanned tile prefix.
 #include "kifmm_internal.cuh"
 
 namespace kifmm {
@@ -31,27 +33,30 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const uint64_t *__restri
     hist[(size_t)threadIdx.x * nblocks + blockIdx.x] = h[threadIdx.x];
 }
 
-// exclusive scan of `total` counters by one block of 1024 threads
-__global__ void __launch_bounds__(1024) k_rs_scan(uint32_t *__restrict__ hist, int64_t total) {
-    __shared__ uint32_t part[1024];
-    int64_t chunk = (total + 1023) / 1024;
-    int64_t b = threadIdx.x * chunk, e = b + chunk < total ? b + chunk : total;
-    uint32_t s = 0;
-    for (int64_t i = b; i < e; i++) s += hist[i];
-    part[threadIdx.x] = s;
+// Per-digit scan: block d turns hist[d][0..nb) into exclusive prefixes over
+// the tiles and writes the digit's total to dtot[d] (dtot = hist + 256 * nb).
+__global__ void __launch_bounds__(256) k_rs_scan(uint32_t *__restrict__ hist, int nblocks) {
+    __shared__ uint32_t part[256];
+    uint32_t *h = hist + (size_t)blockIdx.x * nblocks;
+    const int chunk = (nblocks + 255) / 256;
+    const int b = threadIdx.x * chunk, e = min(b + chunk, nblocks);
+    uint32_t sum = 0;
+    for (int i = b; i < e; i++) sum += h[i];
+    part[threadIdx.x] = sum;
     __syncthreads();
-    for (int off = 1; off < 1024; off <<= 1) {
+    for (int off = 1; off < 256; off <<= 1) {
         uint32_t v = threadIdx.x >= off ? part[threadIdx.x - off] : 0;
         __syncthreads();
         part[threadIdx.x] += v;
         __syncthreads();
     }
-    uint32_t run = part[threadIdx.x] - s;
-    for (int64_t i = b; i < e; i++) {
-        uint32_t v = hist[i];
-        hist[i] = run;
+    uint32_t run = part[threadIdx.x] - sum;
+    for (int i = b; i < e; i++) {
+        uint32_t v = h[i];
+        h[i] = run;
         run += v;
     }
+    if (threadIdx.x == 255) hist[(size_t)256 * nblocks + blockIdx.x] = part[255];
 }
 
 template <bool PAIRS>
@@ -61,9 +66,21 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t *__res
                                                             int nblocks) {
     __shared__ uint32_t wcnt[RS_WARPS][256];
     __shared__ uint32_t base[256];
+    __shared__ uint32_t wsum[RS_WARPS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int d = threadIdx.x; d < 256 * RS_WARPS; d += RS_THREADS) (&wcnt[0][0])[d] = 0;
-    base[threadIdx.x] = hist[(size_t)threadIdx.x * nblocks + blockIdx.x];
+    {  // digit bases: exclusive scan of the 256 digit totals
+        uint32_t t = hist[(size_t)256 * nblocks + threadIdx.x], x = t;
+        for (int o = 1; o < 32; o <<= 1) {
+            uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
+        __syncthreads();
+        uint32_t woff = 0;
+        for (int i = 0; i < w; i++) woff += wsum[i];
+        base[threadIdx.x] = woff + x - t + hist[(size_t)threadIdx.x * nblocks + blockIdx.x];
+    }
     __syncthreads();
     const int64_t t0 = (int64_t)blockIdx.x * RS_TILE + (int64_t)w * (RS_ITEMS * 32);
     uint64_t k[RS_ITEMS];
@@ -110,19 +127,19 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t *__res
 }
 
 static void rs_run(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_tmp, int64_t n, int bits,
-                   kifmm_plan *P, bool pairs) {
+                   kifmm_plan *P, bool pairs, int lo_bit = 0) {
     if (n <= 1) return;
     KIFMM_REQUIRE(n < (1ll << 31), KIFMM_ERR_ARG, "radix sort: more than 2^31 keys");
     int nb = (int)((n + RS_TILE - 1) / RS_TILE);
-    P->sort_hist.alloc((size_t)256 * nb);
+    P->sort_hist.alloc((size_t)256 * nb + 256);
     int passes = (bits + 7) / 8;
     uint64_t *ka = key, *kb = key_tmp;
     int32_t *va = val, *vb = val_tmp;
     for (int p = 0; p < passes; p++) {
-        int shift = 8 * p;
+        int shift = lo_bit + 8 * p;
         k_rs_hist<<<nb, RS_THREADS, 0, P->stream>>>(ka, n, shift, P->sort_hist.p, nb);
         KIFMM_LAUNCHED();
-        k_rs_scan<<<1, 1024, 0, P->stream>>>(P->sort_hist.p, (int64_t)256 * nb);
+        k_rs_scan<<<256, 256, 0, P->stream>>>(P->sort_hist.p, nb);
         KIFMM_LAUNCHED();
         if (pairs)
             k_rs_scatter<true><<<nb, RS_THREADS, 0, P->stream>>>(ka, va, kb, vb, n, shift, P->sort_hist.p, nb);
@@ -144,11 +161,17 @@ void radix_sort_pairs(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *v
     rs_run(key, val, key_tmp, val_tmp, n, bits, P, true);
 }
 
+// sorts by bits [lo_bit, lo_bit + bits) only (stable)
+void radix_sort_pairs_bits(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_tmp, int64_t n, int lo_bit,
+                           int bits, kifmm_plan *P) {
+    rs_run(key, val, key_tmp, val_tmp, n, bits, P, true, lo_bit);
+}
+
 void radix_sort_keys(uint64_t *key, uint64_t *key_tmp, int64_t n, int bits, kifmm_plan *P) {
     rs_run(key, nullptr, key_tmp, nullptr, n, bits, P, false);
 }
 
-int64_t radix_sort_hist_words(int64_t n) { return (int64_t)256 * ((n + RS_TILE - 1) / RS_TILE); }
+int64_t radix_sort_hist_words(int64_t n) { return (int64_t)256 * ((n + RS_TILE - 1) / RS_TILE) + 256; }
 
 // Same passes as rs_run, on caller-provided scratch (histogram table of
 // radix_sort_hist_words(n) words, ping-pong buffers of n entries); launches
@@ -165,7 +188,7 @@ void radix_sort_pairs_scratch(uint64_t *key, int32_t *val, uint64_t *key_tmp, in
         int shift = 8 * p;
         k_rs_hist<<<nb, RS_THREADS, 0, stream>>>(ka, n, shift, hist, nb);
         KIFMM_LAUNCHED();
-        k_rs_scan<<<1, 1024, 0, stream>>>(hist, (int64_t)256 * nb);
+        k_rs_scan<<<256, 256, 0, stream>>>(hist, nb);
         KIFMM_LAUNCHED();
         k_rs_scatter<true><<<nb, RS_THREADS, 0, stream>>>(ka, va, kb, vb, n, shift, hist, nb);
         KIFMM_LAUNCHED();

@@ -427,23 +427,31 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     P->pkey.alloc(n); P->perm.alloc(n); P->key2.alloc(n); P->perm2.alloc(n);
     k_keys<<<gs, TB, 0, s>>>(P->x.p, P->y.p, n, m, M, h, P->pkey.p, P->perm.p, P->scal.p + 8);
     KIFMM_LAUNCHED();
+    // Sort by the top 32 key bits first (levels 1..16, four 8-bit passes): that
+    // orders every cell of level <= 16, enough whenever no split lies deeper
+    // than level 15.  Otherwise sort all 58 bits and count again.
+    constexpr int FAST_BITS = 32, FAST_LEVELS = FAST_BITS / 2;
     {
+        PhaseScope ph(P, KIFMM_PHASE_SORT);
+        radix_sort_pairs_bits(P->pkey.p, P->perm.p, P->key2.p, P->perm2.p, n, 2 * KEY_DEPTH - FAST_BITS, FAST_BITS, P);
+    }
+    HashSet H{};
+    H.count = P->scal.p + 9;
+    H.ovf = P->scal.p + 10;
+    unsigned long long st[4];
+    for (int full = 0; full < 2; full++) {
+        KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 5, 0, 3 * sizeof(unsigned long long), s));
+        k_t0<<<gs, TB, 0, s>>>(P->pkey.p, n, P->ppl, 0, H, P->scal.p);
+        KIFMM_LAUNCHED();
+        KIFMM_CUDA(cudaMemcpyAsync(st, P->scal.p + 5, sizeof(st), cudaMemcpyDeviceToHost, s));
+        KIFMM_CUDA(cudaStreamSynchronize(s));
+        if (full || (st[1] <= (unsigned long long)FAST_LEVELS && st[2] == 0)) break;
         PhaseScope ph(P, KIFMM_PHASE_SORT);
         radix_sort_pairs(P->pkey.p, P->perm.p, P->key2.p, P->perm2.p, n, 2 * KEY_DEPTH, P);
     }
     P->xs.alloc(n); P->ys.alloc(n);
     k_gather2<<<gs, TB, 0, s>>>(P->x.p, P->y.p, P->perm.p, n, P->xs.p, P->ys.p);
     KIFMM_LAUNCHED();
-
-    // unrestricted split cells: count, then size the set and insert
-    HashSet H{};
-    H.count = P->scal.p + 9;
-    H.ovf = P->scal.p + 10;
-    k_t0<<<gs, TB, 0, s>>>(P->pkey.p, n, P->ppl, 0, H, P->scal.p);
-    KIFMM_LAUNCHED();
-    unsigned long long st[4];
-    KIFMM_CUDA(cudaMemcpyAsync(st, P->scal.p + 5, sizeof(st), cudaMemcpyDeviceToHost, s));
-    KIFMM_CUDA(cudaStreamSynchronize(s));
     P->n_outside = (int64_t)st[3];
     KIFMM_REQUIRE(st[2] == 0, KIFMM_ERR_DEPTH,
                   "build_tree: more than Ncutoff points share one cell of the finest grid (2^29 per side); "
@@ -541,17 +549,28 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     P->n_leaves = (int64_t)c5[2];
     P->n_fake = (int64_t)c5[3];
     P->n_xlist = (int64_t)c5[4];
-    KIFMM_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(unsigned long long), s));
-    k_stats<<<P->num_sms * 2, TB, 0, s>>>(T, P->ent.p, P->ent_node.p, P->leaf_list.p, P->n_leaf_list, P->p2m_list.p,
-                                          P->n_p2m_list, P->nbot.p, P->ntop.p, P->ncoll.p, P->nent.p, n_ent, cnt);
-    KIFMM_LAUNCHED();
-    KIFMM_CUDA(cudaMemcpyAsync(c5, cnt, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
-    KIFMM_CUDA(cudaStreamSynchronize(s));
-    P->n_p2p_pairs = (int64_t)c5[0];
-    P->n_p2m_points = (int64_t)c5[1];
-    P->n_m2l_pairs = (int64_t)c5[2];
-    P->n_m2l_groups = (int64_t)c5[3];
+    P->have_stats = false;
     P->have_tree = true;
+}
+
+// Work counts for reporting (kifmm_get_tree_info), computed on request.
+void tree_stats(kifmm_plan *P) {
+    if (P->have_stats) return;
+    cudaStream_t s = P->stream;
+    unsigned long long *cnt = (unsigned long long *)P->misc.p + 40;
+    KIFMM_CUDA(cudaMemsetAsync(cnt, 0, 4 * sizeof(unsigned long long), s));
+    k_stats<<<P->num_sms * 2, 256, 0, s>>>(P->lt, P->ent.p, P->ent_node.p, P->leaf_list.p, P->n_leaf_list,
+                                             P->p2m_list.p, P->n_p2m_list, P->nbot.p, P->ntop.p, P->ncoll.p,
+                                             P->nent.p, P->n_ent, cnt);
+    KIFMM_LAUNCHED();
+    unsigned long long c4[4];
+    KIFMM_CUDA(cudaMemcpyAsync(c4, cnt, sizeof(c4), cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaStreamSynchronize(s));
+    P->n_p2p_pairs = (int64_t)c4[0];
+    P->n_p2m_points = (int64_t)c4[1];
+    P->n_m2l_pairs = (int64_t)c4[2];
+    P->n_m2l_groups = (int64_t)c4[3];
+    P->have_stats = true;
 }
 
 void export_tree(kifmm_plan *P, int64_t *nodes, int64_t *point_leaf) {
