@@ -83,6 +83,8 @@ struct DBuf {
 // is the top 2l bits of the 2D-bit Morton key (child order (hx, hy) -> 2hx+hy,
 // the reference's (lo-x,lo-y), (lo-x,hi-y), (hi-x,lo-y), (hi-x,hi-y), tree.py:170-185).
 constexpr int KEY_DEPTH = 29;
+// Taylor order of the Laplace L2P fast path (|z|/r2 <= 0.585 inside 0.75 w)
+#define KIFMM_TAYLOR_P 48
 constexpr int MAX_LEVELS = KIFMM_MAX_LEVELS;  // levels 0..29
 // Split/X-list cell entries: (level << 57) | (cell key << 1) | is_xlist
 constexpr int ENT_LEVEL_SHIFT = 57;
@@ -178,6 +180,7 @@ struct kifmm_plan {
     size_t ops_stride = 0;           // doubles per level block
     kifmm::DBuf<unsigned char> tc_a; // tensor-core M2L operator slices
     kifmm::DBuf<double> tc_rowscale;
+    kifmm::DBuf<double> l2p_taylor;  // Laplace: [L][Q][2p+1] check potential -> Taylor coefficients
     kifmm::DBuf<unsigned char> tc_pre;  // per-apply slices of the source groups
     kifmm::DBuf<int> tc_gexp;
 

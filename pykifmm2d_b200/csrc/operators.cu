@@ -144,42 +144,52 @@ __global__ void k_ops_kmats(OpsArgs A) {
     }
 }
 
-// P_o = M2LS_o . Inv_l (far offsets), M2M and L2L compositions
+// P_o = M2LS_o . Inv_l (far offsets), M2M and L2L compositions; the inverse
+// and the kernel-matrix block are staged in shared memory.
 __global__ void k_ops_compose(OpsArgs A) {
+    extern __shared__ double sm_c[];
     const int Q = A.Q, l = blockIdx.x, slot = blockIdx.y;  // 0..48 offsets, 49 M2M, 50 L2L
     if (l < 1 || l >= A.L) return;
-    double *b = A.ops + (size_t)l * A.stride;
-    const double *inv = b + off_inv(Q);
     if (slot < 49) {
         int ox = slot / 7 - 3, oy = slot % 7 - 3;
         if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1) return;
+    }
+    if (slot >= 49 && l + 1 >= A.L) return;
+    double *b = A.ops + (size_t)l * A.stride;
+    const double *inv = slot == 49 ? A.ops + (size_t)(l + 1) * A.stride + off_inv(Q) : b + off_inv(Q);
+    double *iv = sm_c;              // [Q][Q]
+    double *mm = sm_c + Q * Q;      // M2LS block [Q][Q] or M2MC [Q][4Q]
+    for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) iv[e] = inv[e];
+    if (slot < 49) {
         const double *m = A.m2ls + ((size_t)l * 49 + slot) * Q * Q;
+        for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) mm[e] = m[e];
+    } else {
+        const double *m = A.m2mc + (size_t)l * Q * 4 * Q;
+        for (int e = threadIdx.x; e < 4 * Q * Q; e += blockDim.x) mm[e] = m[e];
+    }
+    __syncthreads();
+    if (slot < 49) {
         double *p = A.poff + ((size_t)l * 49 + slot) * Q * Q;
         for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) {
             int r = e / Q, c = e % Q;
             double s = 0;
-            for (int t = 0; t < Q; t++) s = fma(m[r * Q + t], inv[t * Q + c], s);
+            for (int t = 0; t < Q; t++) s = fma(mm[r * Q + t], iv[t * Q + c], s);
             p[e] = s;
         }
     } else if (slot == 49) {
-        if (l + 1 >= A.L) return;
-        const double *inv1 = A.ops + (size_t)(l + 1) * A.stride + off_inv(Q);
-        const double *m = A.m2mc + (size_t)l * Q * 4 * Q;
         double *o = b + off_m2m(Q);  // [4Q cols][Q rows]
         for (int e = threadIdx.x; e < Q * 4 * Q; e += blockDim.x) {
             int r = e / (4 * Q), c = e % (4 * Q), qc = c / Q, cc = c % Q;
             double s = 0;
-            for (int t = 0; t < Q; t++) s = fma(m[r * 4 * Q + qc * Q + t], inv1[t * Q + cc], s);
+            for (int t = 0; t < Q; t++) s = fma(mm[r * 4 * Q + qc * Q + t], iv[t * Q + cc], s);
             o[(size_t)c * Q + r] = s;
         }
     } else {
-        if (l + 1 >= A.L) return;
-        const double *m = A.m2mc + (size_t)l * Q * 4 * Q;
         double *o = b + off_l2l(Q);  // [Q cols][4Q rows]
         for (int e = threadIdx.x; e < 4 * Q * Q; e += blockDim.x) {
             int r = e / Q, c = e % Q;  // r in 4Q (child block q = r / Q), c in Q
             double s = 0;
-            for (int t = 0; t < Q; t++) s = fma(m[t * 4 * Q + r], inv[t * Q + c], s);
+            for (int t = 0; t < Q; t++) s = fma(mm[t * 4 * Q + r], iv[t * Q + c], s);
             o[(size_t)c * 4 * Q + r] = s;
         }
     }
@@ -203,6 +213,44 @@ __global__ void k_ops_assemble(OpsArgs A) {
             v = A.poff[((size_t)l * 49 + slot) * Q * Q + rr * Q + cc];
         }
         o[e] = v;
+    }
+}
+
+// Laplace local expansion as a Taylor series about the box centre.  With
+// L_k = r2 e^(i theta_k) the equivalent points, z~ = z / w and rho = r2 / w:
+//   -(1/2pi) sum_k q_k log|z - L_k| = a0 + Re sum_{j=1..p} c_j z~^j,
+//   a0 = -(log r2 / 2pi) sum_k q_k,  c_j = (rho^-j / (2 pi j)) sum_k q_k e^(-i j theta_k),
+// valid for |z~| < rho.  taylor_l [(2p+1) rows][Q cols] (column-major) maps the
+// downward check potential to (a0, Re c_1, Im c_1, ...) through q = Inv_l u.
+__global__ void k_ops_taylor(OpsArgs A, double *taylor, int p) {
+    extern __shared__ double sm_t[];
+    const int Q = A.Q, l = blockIdx.x, R = 2 * p + 1;
+    if (l < 1 || l >= A.L) return;
+    double *C = sm_t;            // [R][Q]
+    double *iv = sm_t + R * Q;   // [Q][Q]
+    const double *inv = A.ops + (size_t)l * A.stride + off_inv(Q);
+    const double w = lvl_width(A, l), r2 = 0.5 * w * A.rf2, rho = r2 / w;
+    const double twopi = 2.0 * 3.141592653589793;
+    for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) iv[e] = inv[e];
+    for (int e = threadIdx.x; e < R * Q; e += blockDim.x) {
+        int row = e / Q, k = e % Q;
+        double v;
+        if (row == 0) {
+            v = -log(r2) / twopi;
+        } else {
+            int j = (row + 1) / 2;
+            double th = (double)((j * k) % Q) * (twopi / Q);  // j theta_k reduced mod 2 pi
+            double f = pow(rho, -(double)j) / (twopi * j);
+            v = (row & 1) ? f * cos(th) : -f * sin(th);
+        }
+        C[e] = v;
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < R * Q; e += blockDim.x) {
+        int row = e % R, c = e / R;
+        double acc = 0.0;
+        for (int k = 0; k < Q; k++) acc = fma(C[row * Q + k], iv[k * Q + c], acc);
+        taylor[((size_t)l * Q + c) * R + row] = acc;
     }
 }
 
@@ -248,7 +296,9 @@ void build_operators(kifmm_plan *P) {
         KIFMM_LAUNCHED();
         k_ops_kmats<<<dim3(L, 50), 256, 0, s>>>(A);
         KIFMM_LAUNCHED();
-        k_ops_compose<<<dim3(L, 51), 256, 0, s>>>(A);
+        size_t csm = (size_t)5 * Q * Q * sizeof(double);
+        KIFMM_CUDA(cudaFuncSetAttribute(k_ops_compose, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+        k_ops_compose<<<dim3(L, 51), 256, csm, s>>>(A);
         KIFMM_LAUNCHED();
         k_ops_assemble<<<dim3(L, 9), 256, 0, s>>>(A);
         KIFMM_LAUNCHED();
@@ -258,6 +308,14 @@ void build_operators(kifmm_plan *P) {
         k_to_float<<<grid_for(A.stride * L, 256, 4096), 256, 0, s>>>(P->ops.p, P->ops_f.p, A.stride * (size_t)L);
         KIFMM_LAUNCHED();
         if (uses_tensor_m2l(P) && L >= 3) build_tc_operators(P);
+        if (P->kern.kind == KIFMM_KERNEL_LAPLACE && L >= 3) {
+            const int R = 2 * KIFMM_TAYLOR_P + 1;
+            P->l2p_taylor.alloc((size_t)L * Q * R);
+            size_t tsm = ((size_t)R * Q + (size_t)Q * Q) * sizeof(double);
+            KIFMM_CUDA(cudaFuncSetAttribute(k_ops_taylor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
+            k_ops_taylor<<<L, 256, tsm, s>>>(A, P->l2p_taylor.p, KIFMM_TAYLOR_P);
+            KIFMM_LAUNCHED();
+        }
     }
     P->have_ops = true;
 }

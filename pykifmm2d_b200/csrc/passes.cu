@@ -24,9 +24,13 @@ __global__ void k_scatter_pot(const double *__restrict__ pots, const int32_t *__
 }
 
 // P2M (numba_upwards_pass, class_fmm.py:57-71): one warp per node; lane q
-// accumulates over the node's sources in order.
-__global__ void k_p2m_d(PassArgs A, const int32_t *__restrict__ list, int64_t nlist) {
-    const int lane = threadIdx.x & 31;
+// accumulates over the node's sources, which the warp stages 32 at a time
+// in shared memory.
+constexpr int P2M_WARPS = 8;
+__global__ void __launch_bounds__(32 * P2M_WARPS) k_p2m_d(PassArgs A, const int32_t *__restrict__ list,
+                                                           int64_t nlist) {
+    __shared__ double sx[P2M_WARPS][32], sy[P2M_WARPS][32], st[P2M_WARPS][32];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (w >= nlist) return;
     int g = list[w];
@@ -34,16 +38,34 @@ __global__ void k_p2m_d(PassArgs A, const int32_t *__restrict__ list, int64_t nl
     double cx, cy;
     node_center(A, g, l, cx, cy);
     const double *lg = A.ops + (size_t)l * A.stride + A.off_large;
+    const int b = A.nbot[g], e = A.ntop[g];
     for (int q0 = 0; q0 < A.Q; q0 += 32) {
         int q = q0 + lane;
         bool ok = q < A.Q;
         double tx = ok ? lg[q] + cx : 0.0, ty = ok ? lg[A.Q + q] + cy : 0.0;
-        double acc = 0.0;
-        for (int s = A.nbot[g]; s < A.ntop[g]; s++) {
-            double dx = tx - A.xs[s], dy = ty - A.ys[s];
-            acc += green_d(A.kind, A.k, dx * dx + dy * dy) * A.taus[s];
+        double acc0 = 0.0, acc1 = 0.0;
+        for (int s0 = b; s0 < e; s0 += 32) {
+            __syncwarp();
+            if (s0 + lane < e) {
+                sx[wib][lane] = A.xs[s0 + lane];
+                sy[wib][lane] = A.ys[s0 + lane];
+                st[wib][lane] = A.taus[s0 + lane];
+            }
+            __syncwarp();
+            const int ns = min(32, e - s0);
+            int u = 0;
+            for (; u + 1 < ns; u += 2) {
+                double dx0 = tx - sx[wib][u], dy0 = ty - sy[wib][u];
+                double dx1 = tx - sx[wib][u + 1], dy1 = ty - sy[wib][u + 1];
+                acc0 += green_d(A.kind, A.k, dx0 * dx0 + dy0 * dy0) * st[wib][u];
+                acc1 += green_d(A.kind, A.k, dx1 * dx1 + dy1 * dy1) * st[wib][u + 1];
+            }
+            if (u < ns) {
+                double dx = tx - sx[wib][u], dy = ty - sy[wib][u];
+                acc0 += green_d(A.kind, A.k, dx * dx + dy * dy) * st[wib][u];
+            }
         }
-        if (ok) A.uup[(size_t)g * A.Q + q] = acc;
+        if (ok) A.uup[(size_t)g * A.Q + q] = acc0 + acc1;
     }
 }
 
@@ -253,11 +275,13 @@ PassArgs make_pass_args(kifmm_plan *P) {
     A.pots = P->pots.p;
     A.uup = P->uup.p;
     A.udown = P->udown.p;
+    A.taylor = P->l2p_taylor.p;
     return A;
 }
 
 void launch_p2m_d(kifmm_plan *P, const PassArgs &A) {
-    k_p2m_d<<<grid_for(P->n_p2m_list * 32, 256), 256, 0, P->stream>>>(A, P->p2m_list.p, P->n_p2m_list);
+    k_p2m_d<<<grid_for(P->n_p2m_list * 32, 32 * P2M_WARPS), 32 * P2M_WARPS, 0, P->stream>>>(A, P->p2m_list.p,
+                                                                                         P->n_p2m_list);
     KIFMM_LAUNCHED();
 }
 

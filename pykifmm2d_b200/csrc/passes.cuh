@@ -21,6 +21,7 @@ struct PassArgs {
     const double *xs, *ys, *taus;
     double *pots;
     double *uup, *udown;
+    const double *taylor;  // Laplace L2P coefficients map, or null
 };
 
 // Node centre, exactly the reference's xmid = xmin + w/2 (tree.py:339-346):

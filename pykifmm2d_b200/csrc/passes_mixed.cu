@@ -148,8 +148,9 @@ constexpr int LEAF_WARPS = 4;
 template <int KIND>
 __global__ void __launch_bounds__(32 * LEAF_WARPS) k_leaf_eval_f(PassArgs A, const int32_t *__restrict__ list,
                                                                  int64_t nlist) {
+    constexpr int R = 2 * KIFMM_TAYLOR_P + 1;
     __shared__ float4 tile[LEAF_WARPS][32];
-    __shared__ double qds[LEAF_WARPS][64];
+    __shared__ double qds[LEAF_WARPS][R > 64 ? R : 64];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     int64_t w = (int64_t)blockIdx.x * LEAF_WARPS + wib;
     if (w >= nlist) return;
@@ -157,38 +158,64 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS) k_leaf_eval_f(PassArgs A, con
     const int l = A.nlev[g];
     double cx, cy;
     node_center(A, g, l, cx, cy);
-    double *qd = qds[wib];
-    local_density(A, g, l, qd, lane);
-    __syncwarp();
     const bool lap = KIND == KIFMM_KERNEL_LAPLACE;
+    const bool taylor = lap && A.taylor != nullptr && l >= 2;
+    double *qd = qds[wib];
     const double width = ldexp(A.W, -l);
     const double sc = lap ? 1.0 / width : 1.0;     // coordinate scale
     const double lw = lap ? -2.0 * log2(sc) : 0.0; // log2 of the squared length unit
+    if (taylor) {  // Taylor coefficients of the local expansion (FP64)
+        const double *T = A.taylor + (size_t)l * A.Q * R;
+        const double *u = A.udown + (size_t)g * A.Q;
+        for (int r = lane; r < R; r += 32) {
+            double s = 0.0;
+            for (int c = 0; c < A.Q; c++) s = fma(T[(size_t)c * R + r], u[c], s);
+            qd[r] = s;
+        }
+    } else {
+        local_density(A, g, l, qd, lane);
+    }
+    __syncwarp();
     const float kk = (float)A.k;
     const int b = A.nbot[g], e = A.ntop[g];
-    int coll[9];
-#pragma unroll
-    for (int d = 0; d < 9; d++) coll[d] = A.ncoll[9 * (size_t)g + d];
     for (int t0 = b; t0 < e; t0 += 32) {
         const int t = t0 + lane;
         const bool act = t < e;
-        const float tx = act ? (float)((A.xs[t] - cx) * sc) : 0.f, ty = act ? (float)((A.ys[t] - cy) * sc) : 0.f;
-        // far field (L2P) in FP64: equivalent density on the check circle
+        const double pxd = act ? A.xs[t] - cx : 0.0, pyd = act ? A.ys[t] - cy : 0.0;
+        const float tx = (float)(pxd * sc), ty = (float)(pyd * sc);
+        // far field (L2P) in FP64
         double far = 0.0;
         if (l >= 2 && act) {
-            const double *lgd = A.ops + (size_t)l * A.stride + A.off_large;
-            const double px = A.xs[t] - cx, py = A.ys[t] - cy;
-            for (int q = 0; q < A.Q; q++) {
-                double dx = px - lgd[q], dy = py - lgd[A.Q + q];
-                far = fma(green_d(A.kind, A.k, dx * dx + dy * dy), qd[q], far);
+            const double zx = pxd * sc, zy = pyd * sc;
+            if (taylor && zx * zx + zy * zy <= 0.5625) {
+                double sr = qd[R - 2], si = qd[R - 1];
+                for (int j = KIFMM_TAYLOR_P - 1; j >= 1; j--) {
+                    double nr = fma(sr, zx, fma(-si, zy, qd[2 * j - 1]));
+                    double ni = fma(sr, zy, fma(si, zx, qd[2 * j]));
+                    sr = nr;
+                    si = ni;
+                }
+                far = qd[0] + (sr * zx - si * zy);
+            } else {
+                // direct FP64 sum over the equivalent points (out-of-box targets, K0)
+                const double *lgd = A.ops + (size_t)l * A.stride + A.off_large;
+                const double *inv = A.ops + (size_t)l * A.stride + A.off_inv;
+                const double *u = A.udown + (size_t)g * A.Q;
+                for (int q = 0; q < A.Q; q++) {
+                    double qq = taylor ? 0.0 : qd[q];
+                    if (taylor)
+                        for (int c = 0; c < A.Q; c++) qq = fma(inv[q * A.Q + c], u[c], qq);
+                    double dx = pxd - lgd[q], dy = pyd - lgd[A.Q + q];
+                    far = fma(green_d(A.kind, A.k, dx * dx + dy * dy), qq, far);
+                }
             }
         }
-        Kahan near;
+        Kahan near0, near1;
         double tsum = 0.0;  // FP64 sum of the sources' charges
         float excl = 0.f;   // charges of the skipped coincident pairs
 #pragma unroll 1
         for (int d = 0; d < 9; d++) {
-            const int c = coll[d];
+            const int c = A.ncoll[9 * (size_t)g + d];
             if (c < 0) continue;
             const int cb = A.nbot[c], ce = A.ntop[c];
             for (int s0 = cb; s0 < ce; s0 += 32) {
@@ -206,20 +233,32 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS) k_leaf_eval_f(PassArgs A, con
                 }
                 __syncwarp();
                 const int ns = min(32, ce - s0);
-#pragma unroll 8
-                for (int u = 0; u < ns; u++) {
+                int u = 0;
+                if (KIND == KIFMM_KERNEL_LAPLACE)
+#pragma unroll 4
+                for (; u + 1 < ns; u += 2) {
+                    const float4 s0v = tile[wib][u], s1v = tile[wib][u + 1];
+                    const float dx0 = tx - s0v.x, dy0 = ty - s0v.y, dx1 = tx - s1v.x, dy1 = ty - s1v.y;
+                    const float r20 = fmaf(dx0, dx0, dy0 * dy0), r21 = fmaf(dx1, dx1, dy1 * dy1);
+                    float g0 = 0.f, g1 = 0.f;
+                    if (r20 > 0.f) g0 = gsum_term<KIND>(r20, kk); else excl += s0v.z;
+                    if (r21 > 0.f) g1 = gsum_term<KIND>(r21, kk); else excl += s1v.z;
+                    near0.fma_add(s0v.z, g0);
+                    near1.fma_add(s1v.z, g1);
+                }
+#pragma unroll 1
+                for (; u < ns; u++) {
                     const float4 sv = tile[wib][u];
                     const float dx = tx - sv.x, dy = ty - sv.y;
                     const float r2 = fmaf(dx, dx, dy * dy);
                     float gv = 0.f;
-                    if (r2 > 0.f) gv = gsum_term<KIND>(r2, kk);
-                    else excl += sv.z;
-                    near.fma_add(sv.z, gv);
+                    if (r2 > 0.f) gv = gsum_term<KIND>(r2, kk); else excl += sv.z;
+                    near0.fma_add(sv.z, gv);
                 }
             }
         }
         if (act) {
-            double v = near.value();
+            double v = near0.value() + near1.value();
             if (lap) v += lw * (tsum - (double)excl);
             A.pots[t] = v * (double)gsum_scale<KIND>() + far;
         }
