@@ -241,8 +241,73 @@ def peaks():
 
 
 def p2p_flops_per_pair(kernel):
-    # Laplace: 2 sub, 2 mul/fma for r^2, 1 lg2, 1 fma = 8 flops per pair (SURVEY-style count)
+    # Laplace: 2 sub, mul + fma for r^2, 1 lg2, 1 fma = 8 flops per pair;
+    # modified Helmholtz: ~40 (sqrt + K0 series)
     return 8.0 if kernel == 0 else 40.0
+
+
+def measured_traffic():
+    """DRAM bytes per launch of the profiled kernels, from the committed ncu
+    summary profiles/traffic_c2.txt (lines: kernel_name bytes)."""
+    out = {}
+    try:
+        for line in open(os.path.join(ROOT, "profiles", "traffic_c2.txt")):
+            p = line.split()
+            if len(p) == 2 and not line.startswith("#"):
+                out[p[0]] = float(p[1])
+    except OSError:
+        pass
+    return out
+
+
+def build_rooflines(cfg, info, phase, precision, pk, pk_src, n):
+    """Rooflines of the dominant kernel (the leaf L2P+P2P kernel), of the
+    tensor-core M2L and of the Morton radix sort, from the phase timers
+    (CUDA events on the plan's stream, averaged over the timed steps)."""
+    from pykifmm2d_b200 import _lib as B
+    ph = dict(zip(B.PHASES, phase))
+    clk = pk.get("sm_max_mhz", 1965.0) * 1e6
+    traffic = measured_traffic()
+    out = {}
+    fp32_peak = 148 * 128 * 2 * clk / 1e12          # TFLOP/s, FFMA = 2 flops
+    fp64_peak = fp32_peak / 2
+    pairs = float(info.n_p2p_pairs)
+    fl = pairs * p2p_flops_per_pair(cfg["kernel"])
+    t = ph["leaf"] * 1e-3
+    if t > 0:
+        peak = fp32_peak if precision == "mixed" else fp64_peak
+        ach = fl / t / 1e12
+        name = "k_leaf_eval_f" if precision == "mixed" else "k_leaf_eval_d"
+        out["dominant"] = {
+            "kernel": name + " (P2P + L2P, one launch per step)", "bound": "fp32" if precision == "mixed" else "fp64",
+            "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+            "traffic": traffic.get(name),
+            "work": f"{pairs:.4g} P2P pairs x {p2p_flops_per_pair(cfg['kernel']):.0f} flops per launch",
+            "sfu_frac": (pairs / t) / (148 * 16 * clk),
+            "peak_source": f"SIMT peak 148 SMs x 128 lanes x 2 flops at sm_max_mhz ({pk_src}); "
+                           "sfu_frac = pairs/s over 16 lg2/clk/SM"}
+    tm = ph["m2l"] * 1e-3
+    if precision == "mixed" and tm > 0:
+        Q = cfg["neq"]
+        useful = 2.0 * Q * Q * float(info.n_m2l_pairs)
+        int8_peak = 2 * pk["bf16_tflops"]
+        ach = useful / tm / 1e12
+        out["m2l"] = {"kernel": "k_m2l_tc<int8> (+ source slicing)", "bound": "tensor", "achieved": ach,
+                      "peak": int8_peak, "unit": "TFLOP/s", "frac": ach / int8_peak,
+                      "traffic": traffic.get("k_m2l_tc"),
+                      "work": f"useful M2L flops 2 Q^2 x {info.n_m2l_pairs} V-list pairs; the int8 form "
+                              "executes 15 slice products of the dense 4Qx4Q direction blocks",
+                      "peak_source": f"dense int8 = 2 x measured bf16 {pk['bf16_tflops']} TFLOP/s ({pk_src})"}
+    ts = ph["sort"] * 1e-3
+    if ts > 0:
+        byts = 4 * 36.0 * n  # four 8-bit passes: histogram read + scatter read + write of 12 B per key
+        ach = byts / ts / 1e9
+        out["sort"] = {"kernel": "radix sort (k_rs_hist/scan/scatter, 4 passes)", "bound": "hbm",
+                       "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": ach / pk["hbm_gbs"],
+                       "traffic": traffic.get("k_rs_scatter"),
+                       "work": "4 passes x 36 B per key (12 B key+index read twice, written once)",
+                       "peak_source": pk_src}
+    return out
 
 
 def run_ours(args, cfg, rank, world, dist):
@@ -306,30 +371,8 @@ def run_ours(args, cfg, rank, world, dist):
     if rank != 0:
         return None
     pk, pk_src = peaks()
-    # roofline of the dominant phase
     names = B.PHASES
-    dom = int(np.argmax(phase[[0, 2, 3, 4, 5, 6]]))
-    dom = [0, 2, 3, 4, 5, 6][dom]
-    roof = None
-    if names[dom] == "leaf":
-        pairs = info.n_p2p_pairs
-        flops = pairs * p2p_flops_per_pair(cfg["kernel"]) + n * cfg["neq"] * (p2p_flops_per_pair(cfg["kernel"]) + 2)
-        fp32_peak = 148 * 128 * 2 * pk.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
-        fp64_peak = fp32_peak / 2
-        peak = fp32_peak if precision == "mixed" else fp64_peak
-        ach = flops / (phase[dom] * 1e-3) / 1e12
-        roof = {"kernel": "k_leaf_eval (L2P+P2P)", "bound": "fp32" if precision == "mixed" else "fp64",
-                "achieved": ach, "peak": peak, "unit": "TFLOP/s", "frac": ach / peak, "traffic": None,
-                "peak_source": f"nominal SIMT peak at sm_max_mhz of MEASURED_PEAKS.json ({pk_src})",
-                "work": f"{pairs:.4g} P2P pairs x {p2p_flops_per_pair(cfg['kernel'])} flops + L2P"}
-    elif names[dom] == "tree":
-        byts = 52.0 * n
-        ach = byts / (phase[1] * 1e-3) / 1e9 if phase[1] > 0 else 0.0
-        roof = {"kernel": "radix sort (Morton keys)", "bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"],
-                "unit": "GB/s", "frac": ach / pk["hbm_gbs"], "traffic": None, "peak_source": pk_src}
-    else:
-        roof = {"kernel": names[dom], "bound": "tensor" if names[dom] == "m2l" else "hbm", "achieved": None,
-                "peak": None, "unit": None, "frac": None, "traffic": None}
+    rooflines = build_rooflines(cfg, info, phase, precision, pk, pk_src, n)
     line = {
         "metric": METRIC,
         "value": value,
@@ -355,7 +398,9 @@ def run_ours(args, cfg, rank, world, dist):
         "phases_ms": {nm: float(v) for nm, v in zip(names, phase)},
         "tree": {"levels": info.levels, "nodes": info.n_nodes, "leaves": info.n_leaves, "outside_root": info.n_outside,
                  "p2p_pairs": info.n_p2p_pairs},
-        "roofline": roof,
+        "roofline": rooflines["dominant"],
+        "roofline_tensor_m2l": rooflines.get("m2l"),
+        "roofline_hbm_sort": rooflines.get("sort"),
         "e2e": {"value": n / (res["e2e_ms"] * 1e-3) / 1e6, "unit": "Mpts/s",
                 "h2d_bytes_per_step": 3 * 8 * n, "d2h_bytes_per_step": 8 * n, "ms_per_step": res["e2e_ms"],
                 "rel_err": res["e2e_err"]},

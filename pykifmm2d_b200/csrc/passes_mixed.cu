@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS) k_leaf_eval_f(PassArgs A, con
                 }
             }
         }
-        Kahan near0, near1;
+        double near = 0.0;  // FP64 sum of per-tile FP32 partial sums
         double tsum = 0.0;  // FP64 sum of the sources' charges
         float excl = 0.f;   // charges of the skipped coincident pairs
 #pragma unroll 1
@@ -222,44 +222,49 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS) k_leaf_eval_f(PassArgs A, con
                 const int s = s0 + lane;
                 __syncwarp();
                 double ts = 0.0;
+                // a short tile is padded with far, uncharged sources: fixed 32-wide loop
+                float4 v = make_float4(1e18f, 1e18f, 0.f, 0.f);
                 if (s < ce) {
                     ts = A.taus[s];
-                    tile[wib][lane] = make_float4((float)((A.xs[s] - cx) * sc), (float)((A.ys[s] - cy) * sc),
-                                                  (float)ts, 0.f);
+                    v = make_float4((float)((A.xs[s] - cx) * sc), (float)((A.ys[s] - cy) * sc), (float)ts, 0.f);
                 }
+                tile[wib][lane] = v;
                 if (lap) {
                     for (int o = 16; o; o >>= 1) ts += __shfl_xor_sync(0xffffffffu, ts, o);
                     tsum += ts;
                 }
                 __syncwarp();
-                const int ns = min(32, ce - s0);
-                int u = 0;
-                if (KIND == KIFMM_KERNEL_LAPLACE)
-#pragma unroll 4
-                for (; u + 1 < ns; u += 2) {
-                    const float4 s0v = tile[wib][u], s1v = tile[wib][u + 1];
-                    const float dx0 = tx - s0v.x, dy0 = ty - s0v.y, dx1 = tx - s1v.x, dy1 = ty - s1v.y;
-                    const float r20 = fmaf(dx0, dx0, dy0 * dy0), r21 = fmaf(dx1, dx1, dy1 * dy1);
-                    float g0 = 0.f, g1 = 0.f;
-                    if (r20 > 0.f) g0 = gsum_term<KIND>(r20, kk); else excl += s0v.z;
-                    if (r21 > 0.f) g1 = gsum_term<KIND>(r21, kk); else excl += s1v.z;
-                    near0.fma_add(s0v.z, g0);
-                    near1.fma_add(s1v.z, g1);
-                }
+                float acc = 0.f;
+                if (KIND == KIFMM_KERNEL_LAPLACE) {
+#pragma unroll 8
+                    for (int u = 0; u < 32; u++) {
+                        const float4 sv = tile[wib][u];
+                        const float dx = tx - sv.x, dy = ty - sv.y;
+                        const float r2 = fmaf(dx, dx, dy * dy);
+                        const bool z = r2 == 0.f;  // coincident pair: skipped (class_fmm.py:107)
+                        acc = fmaf(sv.z, __log2f(z ? 1.f : r2), acc);
+                        excl += z ? sv.z : 0.f;
+                    }
+                } else {
+                    const int ns = min(32, ce - s0);
 #pragma unroll 1
-                for (; u < ns; u++) {
-                    const float4 sv = tile[wib][u];
-                    const float dx = tx - sv.x, dy = ty - sv.y;
-                    const float r2 = fmaf(dx, dx, dy * dy);
-                    float gv = 0.f;
-                    if (r2 > 0.f) gv = gsum_term<KIND>(r2, kk); else excl += sv.z;
-                    near0.fma_add(sv.z, gv);
+                    for (int u = 0; u < ns; u++) {
+                        const float4 sv = tile[wib][u];
+                        const float dx = tx - sv.x, dy = ty - sv.y;
+                        const float r2 = fmaf(dx, dx, dy * dy);
+                        if (r2 > 0.f) acc = fmaf(sv.z, gsum_term<KIND>(r2, kk), acc);
+                    }
                 }
+                near += (double)acc;
             }
         }
         if (act) {
-            double v = near0.value() + near1.value();
-            if (lap) v += lw * (tsum - (double)excl);
+            double v = near;
+            // the skipped pair is almost always the target itself: take its
+            // charge in FP64 so that log2(w^2) * (tsum - excl) cancels exactly
+            const double tau_t = A.taus[t];
+            const double ex = (excl == (float)tau_t) ? tau_t : (double)excl;
+            if (lap) v += lw * (tsum - ex);
             A.pots[t] = v * (double)gsum_scale<KIND>() + far;
         }
     }
@@ -333,26 +338,28 @@ void run_passes_mixed(kifmm_plan *P) {
         for (int l = L - 2; l >= 2; l--)
             if (P->lt.ne[l]) launch_m2m_d(P, A, l);
     }
-    PhaseScope ph(P, KIFMM_PHASE_M2L);
     const bool simt = P->opt.m2l == KIFMM_M2L_FP32;
     int thr = ((4 * Q + 31) / 32) * 32;
     size_t smem = (size_t)M2LF_TE * 4 * Q * sizeof(float);
     if (simt) {
+        PhaseScope ph(P, KIFMM_PHASE_M2L);
         KIFMM_CUDA(cudaFuncSetAttribute(k_m2l_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    } else {
+        for (int l = 1; l <= L - 2; l++) {
+            int64_t ne = P->lt.ne[l];
+            if (!ne) continue;
+            k_m2l_f<<<(unsigned)((ne + M2LF_TE - 1) / M2LF_TE), thr, smem, s>>>(A, l);
+            KIFMM_LAUNCHED();
+        }
+        return;
+    }
+    {
+        PhaseScope ph(P, KIFMM_PHASE_M2L);
         KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 15, 0, sizeof(unsigned long long), s));
         run_m2l_tensor(P, A);  // all levels at once
     }
-    for (int l = 1; l <= L - 2; l++) {
-        int64_t ne = P->lt.ne[l];
-        if (!ne) continue;
-        if (simt) {
-            k_m2l_f<<<(unsigned)((ne + M2LF_TE - 1) / M2LF_TE), thr, smem, s>>>(A, l);
-            KIFMM_LAUNCHED();
-        } else if (l >= 2) {
-            launch_l2l_d(P, A, l);
-        }
-    }
+    PhaseScope ph(P, KIFMM_PHASE_L2L);
+    for (int l = 2; l <= L - 2; l++)
+        if (P->lt.ne[l]) launch_l2l_d(P, A, l);
 }
 
 void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
