@@ -166,6 +166,7 @@ struct kifmm_plan {
     kifmm::DBuf<int32_t> nparent, nchild, nent;  // parent, first child, own entry
     kifmm::DBuf<int32_t> ncoll;      // [n_nodes][9] colleagues by direction (dx+1)*3+(dy+1)
     kifmm::DBuf<int32_t> leaf_list, p2m_list;
+    kifmm::DBuf<uint32_t> list_tiles;  // per-tile counts/offsets while the lists are built
     int64_t n_leaf_list = 0, n_p2m_list = 0;
     int64_t n_leaves = 0, n_fake = 0, n_xlist = 0;
     int64_t n_p2p_pairs = 0, n_p2m_points = 0, n_m2l_pairs = 0, n_m2l_groups = 0;

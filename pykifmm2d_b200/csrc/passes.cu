@@ -381,6 +381,139 @@ __global__ void __launch_bounds__(256) k_lvl_gemm_d(PassArgs A, int l, int M, in
     }
 }
 
+// The same products with the operator held once per block and one entry per
+// lane: warp w of a block takes 32 entries and RPT rows of the operator, so
+// every operator read is a shared-memory broadcast (two rows per 16-byte
+// load) and each thread's RPT accumulators are FP64-pipe bound.  Rows are
+// padded to Mp = RG * RPT with zeros.  Blocks hold NT = 32 * S entries, S
+// sets of wps = min(RG, 8) warps; with RG > 8 a warp loops over row groups.
+constexpr int LG_THREADS = 256;
+
+// Copy n doubles from global memory through store(i, v), i in [0, n), with
+// eight independent loads per thread in flight (16-byte loads when src is
+// 16-byte aligned and n even).  Small staging loops are otherwise bound by
+// one load latency per iteration.
+template <class F>
+__device__ __forceinline__ void stage_f64(const double *__restrict__ src, int n, F store) {
+    if ((((uintptr_t)src) & 15) == 0 && (n & 1) == 0) {
+        const double2 *s2 = (const double2 *)src;
+        const int n2 = n >> 1;
+        for (int i0 = threadIdx.x; i0 < n2; i0 += 8 * LG_THREADS) {
+            double2 v[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int i = i0 + k * LG_THREADS;
+                v[k] = i < n2 ? s2[i] : make_double2(0.0, 0.0);
+            }
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int i = i0 + k * LG_THREADS;
+                if (i < n2) {
+                    store(2 * i, v[k].x);
+                    store(2 * i + 1, v[k].y);
+                }
+            }
+        }
+    } else {
+        for (int i0 = threadIdx.x; i0 < n; i0 += 8 * LG_THREADS) {
+            double v[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int i = i0 + k * LG_THREADS;
+                v[k] = i < n ? src[i] : 0.0;
+            }
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int i = i0 + k * LG_THREADS;
+                if (i < n) store(i, v[k]);
+            }
+        }
+    }
+}
+template <int MODE, int RPT>
+__global__ void __launch_bounds__(LG_THREADS) k_lvl_gemm_b(PassArgs A, int l, int M, int K, int Mp, int NT) {
+    extern __shared__ __align__(16) double sm_b[];
+    double *opS = sm_b;                    // [K][Mp]
+    double *xS = sm_b + (size_t)K * Mp;    // [NT][K + 1]
+    const int ldx = K + 1, Q = A.Q;
+    const int64_t ne = A.T.ne[l], eoff = A.T.eoff[l], e0 = (int64_t)blockIdx.x * NT;
+    const int nt = (int)min((int64_t)NT, ne - e0);
+    const double *op = A.ops + (size_t)l * A.stride + (MODE == 0 ? A.off_m2m : A.off_l2l);  // [K][M]
+    // staging: eight independent loads per thread in flight
+    if (Mp != M)
+        for (int i = threadIdx.x; i < K * Mp; i += LG_THREADS) opS[i] = 0.0;
+    stage_f64(op, K * M, [&](int i, double v) {
+        const int c = i / M;
+        opS[c * Mp + (i - c * M)] = v;
+    });
+    if (MODE == 0) {  // children groups of consecutive entries are contiguous
+        const double *src0 = A.uup + (size_t)(A.T.off[l + 1] + 4 * e0) * Q;
+        for (int i = nt * K + threadIdx.x; i < NT * K; i += LG_THREADS) {
+            const int t = i / K;
+            xS[t * ldx + (i - t * K)] = 0.0;
+        }
+        stage_f64(src0, nt * K, [&](int i, double v) {
+            const int t = i / K;
+            xS[t * ldx + (i - t * K)] = v;
+        });
+    } else {
+        for (int i0 = threadIdx.x; i0 < NT * K; i0 += 8 * LG_THREADS) {
+            double v[8];
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int i = i0 + k * LG_THREADS, t = i / K;
+                v[k] = 0.0;
+                if (i < NT * K && t < nt && !(A.ent[eoff + e0 + t] & 1))
+                    v[k] = A.udown[(size_t)A.ent_node[eoff + e0 + t] * Q + (i - t * K)];
+            }
+#pragma unroll
+            for (int k = 0; k < 8; k++) {
+                const int i = i0 + k * LG_THREADS, t = i / K;
+                if (i < NT * K) xS[t * ldx + (i - t * K)] = v[k];
+            }
+        }
+    }
+    __syncthreads();
+    const int RG = Mp / RPT, wps = RG < 8 ? RG : 8, S = 8 / wps;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int set = warp / wps;
+    if (set >= S) return;
+    const int t = set * 32 + lane;
+    const double *xp = xS + (size_t)t * ldx;
+    for (int rg = warp % wps; rg < RG; rg += wps) {
+        double acc[RPT];
+#pragma unroll
+        for (int i = 0; i < RPT; i++) acc[i] = 0.0;
+        const double *ap = opS + rg * RPT;
+#pragma unroll 2
+        for (int c = 0; c < K; c++) {
+            const double xv = xp[c];
+            const double2 *a2 = (const double2 *)(ap + (size_t)c * Mp);
+#pragma unroll
+            for (int i = 0; i < RPT / 2; i++) {
+                const double2 a = a2[i];
+                acc[2 * i] = fma(a.x, xv, acc[2 * i]);
+                acc[2 * i + 1] = fma(a.y, xv, acc[2 * i + 1]);
+            }
+        }
+        if (t < nt) {
+            const int64_t e = e0 + t;
+            const int r0 = rg * RPT;
+            if (MODE == 0) {
+                double *dst = A.uup + (size_t)A.ent_node[eoff + e] * Q + r0;
+#pragma unroll
+                for (int i = 0; i < RPT; i++)
+                    if (r0 + i < M) dst[i] = acc[i];
+            } else if (!(A.ent[eoff + e] & 1)) {
+                double *dst = A.udown + (size_t)(A.T.off[l + 1] + 4 * e) * Q + r0;
+#pragma unroll
+                for (int i = 0; i < RPT; i++)
+                    if (r0 + i < M) dst[i] += acc[i];
+            }
+        }
+    }
+}
+
 // NT columns per block: (ceil(M/4)) x (NT/4) threads <= 256 and at most
 // 200 KB of shared memory
 static int lvl_gemm_nt(int M, int K) {
@@ -396,11 +529,25 @@ template <int MODE>
 static void launch_lvl_gemm(kifmm_plan *P, const PassArgs &A, int l) {
     const int Q = P->Q;
     const int M = MODE == 0 ? Q : 4 * Q, K = MODE == 0 ? 4 * Q : Q;
+    const int64_t ne = P->lt.ne[l];
+    {  // broadcast form when the operator and the entry tile fit in shared memory
+        constexpr int RPT = MODE == 0 ? 8 : 16;
+        const int RG = (M + RPT - 1) / RPT, Mp = RG * RPT;
+        const int wps = RG < 8 ? RG : 8, NT = 32 * (8 / wps);
+        const size_t smem = ((size_t)K * Mp + (size_t)NT * (K + 1)) * sizeof(double);
+        if (smem <= (size_t)(220 << 10)) {
+            KIFMM_CUDA(cudaFuncSetAttribute(k_lvl_gemm_b<MODE, RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)smem));
+            k_lvl_gemm_b<MODE, RPT><<<(unsigned)((ne + NT - 1) / NT), LG_THREADS, smem, P->stream>>>(A, l, M, K, Mp,
+                                                                                                     NT);
+            KIFMM_LAUNCHED();
+            return;
+        }
+    }
     int nt = lvl_gemm_nt(M, K);
     int threads = ((M + 3) / 4) * (nt / 4);
     size_t smem = ((size_t)K * M + (size_t)nt * (K + 1)) * sizeof(double);
     KIFMM_CUDA(cudaFuncSetAttribute(k_lvl_gemm_d<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int64_t ne = P->lt.ne[l];
     k_lvl_gemm_d<MODE><<<(unsigned)((ne + nt - 1) / nt), threads, smem, P->stream>>>(A, l, M, K, nt);
     KIFMM_LAUNCHED();
 }

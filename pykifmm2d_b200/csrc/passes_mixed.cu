@@ -14,7 +14,7 @@
 //     accumulation (default), or bf16 / fp16 hi-lo splits with FP32
 //     accumulation; or FP32 tiles on the CUDA cores (this file);
 //   * the local expansion's equivalent density Inv_l u_down formed in FP64.
-// Coincident source/target pairs (r^2 == 0 after rounding) contribute zero.
+// Coincident source/target pairs contribute zero, as in the reference.
 #include "passes.cuh"
 
 namespace kifmm {
@@ -33,25 +33,6 @@ template <int KIND>
 __device__ __forceinline__ float gsum_scale() {
     return KIND == KIFMM_KERNEL_LAPLACE ? -LN2_OVER_4PI : INV_2PI_F;
 }
-
-// Compensated FP32 accumulation (Kahan): sum += term with the lost low part
-// carried in c.
-struct Kahan {
-    float s = 0.f, c = 0.f;
-    __device__ __forceinline__ void add(float term) {
-        float y = term - c;
-        float t = s + y;
-        c = (t - s) - y;
-        s = t;
-    }
-    __device__ __forceinline__ void fma_add(float a, float b) {
-        float y = fmaf(a, b, -c);
-        float t = s + y;
-        c = (t - s) - y;
-        s = t;
-    }
-    __device__ __forceinline__ double value() const { return (double)s - (double)c; }
-};
 
 // FP32 M2L + L2L on the CUDA cores (FP64 state in and out): block = 4Q rows x
 // TE target groups.
@@ -139,18 +120,45 @@ __device__ __forceinline__ void local_density(const PassArgs &A, int g, int l, d
     }
 }
 
-// L2P + P2P: one warp per target leaf, lane per target, 32-source tiles in
-// shared memory.  For the Laplace kernel the offsets are scaled by 1/w (w the
-// leaf width) so every log2 term is O(1); the remainder log2(w^2) * sum(tau)
-// is added in FP64 from per-tile FP64 charge sums (coincident pairs, skipped,
-// are taken back out).  Sums are Kahan-compensated.
+// L2P + P2P: one warp per target leaf.  The sources of the leaf and its eight
+// colleagues are staged in shared memory as one list (the leaf's own points
+// first), in chunks of LEAF_CHUNK.  A tile of nt <= 32 targets is spread over
+// the warp with sp = 32 / nt lanes per target, each lane taking every sp-th
+// source, so a leaf of 15 points keeps 30 lanes busy instead of 15 and no lane
+// idles on a short colleague.  For the Laplace kernel the offsets are scaled
+// by 1/w (w the leaf width) so every log2 term is O(1); the remainder
+// log2(w^2) * sum(tau) is added in FP64.  The inner loop is branch-free: r^2
+// is clamped below at FLT_MIN and short chunks are padded with far, uncharged
+// sources.  The pairs inside the leaf itself that meet the clamp (the target's
+// own point and exact duplicates, which the reference skips, class_fmm.py:107)
+// are counted by a short second loop over the leaf's own points and taken back
+// out.  Distinct points of different leaves closer than about 2^-24 leaf widths
+// round to the same FP32 offsets and keep log2(FLT_MIN) for their pair; the
+// FP64 near field (near_fp64) resolves such pairs.  FP32 partial sums of at
+// most 32 terms are accumulated in FP64.
 constexpr int LEAF_WARPS = 4;
+constexpr int LEAF_CHUNK = 256;
+
+__device__ __forceinline__ float lg2_ftz(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float pair_r2(float tx, float ty, const float4 &sv) {
+    const float dx = tx - sv.x, dy = ty - sv.y;
+    return fmaf(dx, dx, dy * dy);
+}
+
 template <int KIND>
-__global__ void __launch_bounds__(32 * LEAF_WARPS) k_leaf_eval_f(PassArgs A, const int32_t *__restrict__ list,
+__global__ void __launch_bounds__(32 * LEAF_WARPS, 6) k_leaf_eval_f(PassArgs A, const int32_t *__restrict__ list,
                                                                  int64_t nlist) {
     constexpr int R = 2 * KIFMM_TAYLOR_P + 1;
-    __shared__ float4 tile[LEAF_WARPS][32];
+    constexpr float CLAMP = 1.17549435e-38f;  // FLT_MIN
+    __shared__ float4 srcs[LEAF_WARPS][LEAF_CHUNK + 32];
     __shared__ double qds[LEAF_WARPS][R > 64 ? R : 64];
+    __shared__ double red[LEAF_WARPS][32];
+    __shared__ float redf[LEAF_WARPS][32];
+    __shared__ int rngs[LEAF_WARPS][18];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     int64_t w = (int64_t)blockIdx.x * LEAF_WARPS + wib;
     if (w >= nlist) return;
@@ -161,112 +169,207 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS) k_leaf_eval_f(PassArgs A, con
     const bool lap = KIND == KIFMM_KERNEL_LAPLACE;
     const bool taylor = lap && A.taylor != nullptr && l >= 2;
     double *qd = qds[wib];
+    float4 *src = srcs[wib];
     const double width = ldexp(A.W, -l);
     const double sc = lap ? 1.0 / width : 1.0;     // coordinate scale
     const double lw = lap ? -2.0 * log2(sc) : 0.0; // log2 of the squared length unit
-    if (taylor) {  // Taylor coefficients of the local expansion (FP64)
-        const double *T = A.taylor + (size_t)l * A.Q * R;
+    if (taylor) {  // Taylor coefficients of the local expansion (FP64), NR independent rows per lane
+        constexpr int NR = (R + 31) / 32;
+        const double *T = A.taylor + (size_t)l * A.Q * R + lane;
         const double *u = A.udown + (size_t)g * A.Q;
-        for (int r = lane; r < R; r += 32) {
-            double s = 0.0;
-            for (int c = 0; c < A.Q; c++) s = fma(T[(size_t)c * R + r], u[c], s);
-            qd[r] = s;
+        double cs[NR];
+#pragma unroll
+        for (int i = 0; i < NR; i++) cs[i] = 0.0;
+#pragma unroll 2
+        for (int c = 0; c < A.Q; c++) {
+            const double uc = u[c];
+#pragma unroll
+            for (int i = 0; i < NR; i++)
+                if (lane + 32 * i < R) cs[i] = fma(T[(size_t)c * R + 32 * i], uc, cs[i]);
         }
+#pragma unroll
+        for (int i = 0; i < NR; i++)
+            if (lane + 32 * i < R) qd[lane + 32 * i] = cs[i];
     } else {
         local_density(A, g, l, qd, lane);
     }
-    __syncwarp();
     const float kk = (float)A.k;
+    const float lclamp = lg2_ftz(CLAMP);
     const int b = A.nbot[g], e = A.ntop[g];
-    for (int t0 = b; t0 < e; t0 += 32) {
-        const int t = t0 + lane;
-        const bool act = t < e;
-        const double pxd = act ? A.xs[t] - cx : 0.0, pyd = act ? A.ys[t] - cy : 0.0;
-        const float tx = (float)(pxd * sc), ty = (float)(pyd * sc);
-        // far field (L2P) in FP64
-        double far = 0.0;
-        if (l >= 2 && act) {
-            const double zx = pxd * sc, zy = pyd * sc;
-            if (taylor && zx * zx + zy * zy <= 0.5625) {
-                double sr = qd[R - 2], si = qd[R - 1];
-                for (int j = KIFMM_TAYLOR_P - 1; j >= 1; j--) {
-                    double nr = fma(sr, zx, fma(-si, zy, qd[2 * j - 1]));
-                    double ni = fma(sr, zy, fma(si, zx, qd[2 * j]));
-                    sr = nr;
-                    si = ni;
-                }
-                far = qd[0] + (sr * zx - si * zy);
-            } else {
-                // direct FP64 sum over the equivalent points (out-of-box targets, K0)
-                const double *lgd = A.ops + (size_t)l * A.stride + A.off_large;
-                const double *inv = A.ops + (size_t)l * A.stride + A.off_inv;
-                const double *u = A.udown + (size_t)g * A.Q;
-                for (int q = 0; q < A.Q; q++) {
-                    double qq = taylor ? 0.0 : qd[q];
-                    if (taylor)
-                        for (int c = 0; c < A.Q; c++) qq = fma(inv[q * A.Q + c], u[c], qq);
-                    double dx = pxd - lgd[q], dy = pyd - lgd[A.Q + q];
-                    far = fma(green_d(A.kind, A.k, dx * dx + dy * dy), qq, far);
-                }
-            }
+    // source ranges: the leaf itself, then its colleagues in direction order;
+    // list element p lies in the last range i with pre[i] <= p, at p + off[i]
+    // (kept in shared memory: registers are scarce in the pair loop)
+    int *rng = rngs[wib];
+    int ns = 0;
+    if (lane < 9) {
+        const int d = lane <= 4 ? lane - 1 : lane;
+        const int c = lane == 0 ? g : A.ncoll[9 * (size_t)g + d];
+        const int rb = c >= 0 ? A.nbot[c] : 0, rn = c >= 0 ? A.ntop[c] - rb : 0;
+        int x = rn;  // inclusive prefix over lanes 0..8
+        for (int o = 1; o < 16; o <<= 1) {
+            const int y = __shfl_up_sync(0x1ffu, x, o);
+            if (lane >= o) x += y;
         }
-        double near = 0.0;  // FP64 sum of per-tile FP32 partial sums
-        double tsum = 0.0;  // FP64 sum of the sources' charges
-        float excl = 0.f;   // charges of the skipped coincident pairs
-#pragma unroll 1
-        for (int d = 0; d < 9; d++) {
-            const int c = A.ncoll[9 * (size_t)g + d];
-            if (c < 0) continue;
-            const int cb = A.nbot[c], ce = A.ntop[c];
-            for (int s0 = cb; s0 < ce; s0 += 32) {
-                const int s = s0 + lane;
-                __syncwarp();
-                double ts = 0.0;
-                // a short tile is padded with far, uncharged sources: fixed 32-wide loop
-                float4 v = make_float4(1e18f, 1e18f, 0.f, 0.f);
-                if (s < ce) {
-                    ts = A.taus[s];
-                    v = make_float4((float)((A.xs[s] - cx) * sc), (float)((A.ys[s] - cy) * sc), (float)ts, 0.f);
+        rng[lane] = x - rn;
+        rng[9 + lane] = rb - (x - rn);
+        ns = x;
+    }
+    ns = __shfl_sync(0xffffffffu, ns, 8);
+    double tsum = 0.0;  // FP64 sum of the near sources' charges (Laplace)
+    // stage sources [c0, c0 + cn) of the list, padded with 32 far, uncharged
+    // ones; four elements per lane per pass, loads issued before any is used
+    auto gather = [&](int c0, int cn, bool sum) {
+        __syncwarp();
+        int pre[9], off[9];
+#pragma unroll
+        for (int i = 0; i < 9; i++) {
+            pre[i] = rng[i];
+            off[i] = rng[9 + i];
+        }
+        for (int q0 = 0; q0 < cn; q0 += 128) {
+            int si[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                const int q = q0 + lane + 32 * k, p = c0 + q;
+                int sv = p + off[0];
+#pragma unroll
+                for (int i = 1; i < 9; i++) sv = p >= pre[i] ? p + off[i] : sv;
+                si[k] = q < cn ? sv : -1;
+            }
+            double vx[4], vy[4], vt[4];
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (si[k] >= 0) {
+                    vx[k] = A.xs[si[k]];
+                    vy[k] = A.ys[si[k]];
+                    vt[k] = A.taus[si[k]];
                 }
-                tile[wib][lane] = v;
-                if (lap) {
-                    for (int o = 16; o; o >>= 1) ts += __shfl_xor_sync(0xffffffffu, ts, o);
-                    tsum += ts;
+#pragma unroll
+            for (int k = 0; k < 4; k++)
+                if (si[k] >= 0) {
+                    src[q0 + lane + 32 * k] =
+                        make_float4((float)((vx[k] - cx) * sc), (float)((vy[k] - cy) * sc), (float)vt[k], 0.f);
+                    if (sum) tsum += vt[k];
                 }
-                __syncwarp();
-                float acc = 0.f;
-                if (KIND == KIFMM_KERNEL_LAPLACE) {
-#pragma unroll 8
-                    for (int u = 0; u < 32; u++) {
-                        const float4 sv = tile[wib][u];
-                        const float dx = tx - sv.x, dy = ty - sv.y;
-                        const float r2 = fmaf(dx, dx, dy * dy);
-                        const bool z = r2 == 0.f;  // coincident pair: skipped (class_fmm.py:107)
-                        acc = fmaf(sv.z, __log2f(z ? 1.f : r2), acc);
-                        excl += z ? sv.z : 0.f;
+        }
+        src[cn + lane] = make_float4(1e18f, 1e18f, 0.f, 0.f);
+        __syncwarp();
+    };
+    __syncwarp();
+    for (int t0 = b; t0 < e; t0 += 32) {
+        const int nt = min(32, e - t0);
+        const int sp = 32 / nt;  // lanes per target
+        const int ti = lane % nt, j = lane / nt;
+        const int t = t0 + ti;
+        const double pxd = A.xs[t] - cx, pyd = A.ys[t] - cy;
+        const float tx = (float)(pxd * sc), ty = (float)(pyd * sc);
+        double near = 0.0;
+        float exf = 0.f;  // charges of the leaf's own points met at the clamp
+        for (int c0 = 0; c0 < ns; c0 += LEAF_CHUNK) {
+            const int cn = min(LEAF_CHUNK, ns - c0);
+            if (t0 == b || ns > LEAF_CHUNK) gather(c0, cn, lap && t0 == b);
+            // lane (ti, j) takes sources j, j + sp, ...; j + (it - 1) sp < cn + 32
+            const int it = (cn + sp - 1) / sp;
+            const float4 *sv0 = src + j;
+            if (KIND == KIFMM_KERNEL_LAPLACE) {
+                // the list starts with the leaf's own points, local [0, en): the
+                // first kown passes count the pairs there that meet the clamp
+                const int en = min(e - b - c0, cn);
+                const int kown = en > 0 ? (en + sp - 1) / sp : 0;
+                for (int k0 = 0; k0 < kown; k0 += 32) {
+                    const int k1 = min(kown, k0 + 32);
+                    float acc = 0.f;
+                    for (int k = k0; k < k1; k++) {
+                        const int u = j + k * sp;
+                        const float4 sv = src[u];
+                        const float r2 = pair_r2(tx, ty, sv);
+                        acc = fmaf(sv.z, lg2_ftz(fmaxf(r2, CLAMP)), acc);
+                        exf += (r2 < CLAMP && u < en) ? sv.z : 0.f;
                     }
-                } else {
-                    const int ns = min(32, ce - s0);
+                    near += (double)acc;
+                }
+                for (int k0 = kown; k0 < it; k0 += 32) {
+                    const int k1 = min(it, k0 + 32);
+                    float acc = 0.f, acc1 = 0.f;  // two chains: even and odd passes
+                    const float4 *pp = sv0 + (size_t)k0 * sp;
+                    int k = k0;
+#pragma unroll 2
+                    for (; k + 1 < k1; k += 2) {
+                        const float4 sa = pp[0], sb = pp[sp];
+                        pp += 2 * sp;
+                        acc = fmaf(sa.z, lg2_ftz(fmaxf(pair_r2(tx, ty, sa), CLAMP)), acc);
+                        acc1 = fmaf(sb.z, lg2_ftz(fmaxf(pair_r2(tx, ty, sb), CLAMP)), acc1);
+                    }
+                    if (k < k1) {
+                        const float4 sa = pp[0];
+                        acc = fmaf(sa.z, lg2_ftz(fmaxf(pair_r2(tx, ty, sa), CLAMP)), acc);
+                    }
+                    near += (double)(acc + acc1);
+                }
+            } else {
+                for (int k0 = 0; k0 < it; k0 += 32) {
+                    const int k1 = min(it, k0 + 32);
+                    float acc = 0.f;
 #pragma unroll 1
-                    for (int u = 0; u < ns; u++) {
-                        const float4 sv = tile[wib][u];
-                        const float dx = tx - sv.x, dy = ty - sv.y;
-                        const float r2 = fmaf(dx, dx, dy * dy);
+                    for (int k = k0; k < k1; k++) {
+                        const float4 sv = sv0[k * sp];
+                        const float r2 = pair_r2(tx, ty, sv);
                         if (r2 > 0.f) acc = fmaf(sv.z, gsum_term<KIND>(r2, kk), acc);
                     }
+                    near += (double)acc;
                 }
-                near += (double)acc;
             }
         }
-        if (act) {
-            double v = near;
-            // the skipped pair is almost always the target itself: take its
-            // charge in FP64 so that log2(w^2) * (tsum - excl) cancels exactly
-            const double tau_t = A.taus[t];
-            const double ex = (excl == (float)tau_t) ? tau_t : (double)excl;
-            if (lap) v += lw * (tsum - ex);
+        if (lap && t0 == b)
+            for (int o = 16; o; o >>= 1) tsum += __shfl_xor_sync(0xffffffffu, tsum, o);
+        // per-lane share with the clamped own pairs taken out
+        red[wib][lane] = lap ? near - (double)exf * (double)lclamp : near;
+        redf[wib][lane] = exf;
+        __syncwarp();
+        if (lane < nt) {
+            double v = 0.0;
+            float ex = 0.f;
+            for (int m = 0; m < sp; m++) {
+                v += red[wib][lane + m * nt];
+                ex += redf[wib][lane + m * nt];
+            }
+            if (lap) {
+                // the skipped charges leave log2(w^2) * sum(tau); the one skipped
+                // pair is almost always the target itself: take its FP64 charge
+                const double tau_t = A.taus[t];
+                const double exd = ex == (float)tau_t ? tau_t : (double)ex;
+                v += lw * (tsum - exd);
+            }
+            // far field (L2P) in FP64
+            double far = 0.0;
+            if (l >= 2) {
+                const double zx = pxd * sc, zy = pyd * sc;
+                if (taylor && zx * zx + zy * zy <= 0.5625) {
+                    double sr = qd[R - 2], si = qd[R - 1];
+                    for (int jj = KIFMM_TAYLOR_P - 1; jj >= 1; jj--) {
+                        double nr = fma(sr, zx, fma(-si, zy, qd[2 * jj - 1]));
+                        double ni = fma(sr, zy, fma(si, zx, qd[2 * jj]));
+                        sr = nr;
+                        si = ni;
+                    }
+                    far = qd[0] + (sr * zx - si * zy);
+                } else {
+                    // direct FP64 sum over the equivalent points (out-of-box targets, K0)
+                    const double *lgd = A.ops + (size_t)l * A.stride + A.off_large;
+                    const double *inv = A.ops + (size_t)l * A.stride + A.off_inv;
+                    const double *u = A.udown + (size_t)g * A.Q;
+                    for (int q = 0; q < A.Q; q++) {
+                        double qq = taylor ? 0.0 : qd[q];
+                        if (taylor)
+                            for (int c = 0; c < A.Q; c++) qq = fma(inv[q * A.Q + c], u[c], qq);
+                        double dx = pxd - lgd[q], dy = pyd - lgd[A.Q + q];
+                        far = fma(green_d(A.kind, A.k, dx * dx + dy * dy), qq, far);
+                    }
+                }
+            }
             A.pots[t] = v * (double)gsum_scale<KIND>() + far;
         }
+        __syncwarp();
     }
 }
 

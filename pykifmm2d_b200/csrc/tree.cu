@@ -195,47 +195,46 @@ __global__ void k_t0(const uint64_t *__restrict__ key, int64_t n, int64_t ppl, i
 }
 
 // Restriction step for level l: every split cell s of level l+1 forces the
-// 3x3 block around parent(s) to be split.
+// 3x3 block around parent(s) to be split.  One thread per (cell, neighbour):
+// the inserts are independent, so none waits on another's atomic.
 __global__ void k_restrict(HashSet H, int l) {
     unsigned long long n = *((volatile unsigned long long *)H.count);
     if (n > H.cap) n = H.cap;
     const int64_t side = 1ll << l;
-    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < (int64_t)n; j += (int64_t)gridDim.x * blockDim.x) {
-        uint64_t e = H.list[j];
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < 9 * (int64_t)n;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = j / 9;
+        const int d = (int)(j - 9 * i);
+        const uint64_t e = H.list[i];
         if ((int)(e >> ENT_LEVEL_SHIFT) != l + 1 || (e & 1)) continue;
-        uint64_t p = ((e >> 1) & KEY56) >> 2;
-        int64_t px = (int64_t)compact2(p >> 1), py = (int64_t)compact2(p);
-        for (int dx = -1; dx <= 1; dx++)
-            for (int dy = -1; dy <= 1; dy++) {
-                int64_t qx = px + dx, qy = py + dy;
-                if (qx < 0 || qy < 0 || qx >= side || qy >= side) continue;
-                hs_insert(H, ent_make(l, morton((uint64_t)qx, (uint64_t)qy), 0));
-            }
+        const uint64_t p = ((e >> 1) & KEY56) >> 2;
+        const int64_t qx = (int64_t)compact2(p >> 1) + d / 3 - 1, qy = (int64_t)compact2(p) + d % 3 - 1;
+        if (qx < 0 || qy < 0 || qx >= side || qy >= side) continue;
+        hs_insert(H, ent_make(l, morton((uint64_t)qx, (uint64_t)qy), 0));
     }
 }
 
 // X-list: for levels 1..L-2, a real leaf (cell not split, parent split) next
-// to a split cell becomes an X-list cell.
+// to a split cell becomes an X-list cell.  One thread per (cell, neighbour).
 __global__ void k_xlist(HashSet H, int L) {
     unsigned long long n = *((volatile unsigned long long *)H.count);
     if (n > H.cap) n = H.cap;
-    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < (int64_t)n; j += (int64_t)gridDim.x * blockDim.x) {
-        uint64_t e = H.list[j];
-        int l = (int)(e >> ENT_LEVEL_SHIFT);
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < 9 * (int64_t)n;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = j / 9;
+        const int d = (int)(j - 9 * i);
+        if (d == 4) continue;
+        const uint64_t e = H.list[i];
+        const int l = (int)(e >> ENT_LEVEL_SHIFT);
         if ((e & 1) || l < 1 || l > L - 2) continue;
-        uint64_t k = (e >> 1) & KEY56;
-        int64_t sx = (int64_t)compact2(k >> 1), sy = (int64_t)compact2(k);
+        const uint64_t k = (e >> 1) & KEY56;
+        const int64_t cx = (int64_t)compact2(k >> 1) + d / 3 - 1, cy = (int64_t)compact2(k) + d % 3 - 1;
         const int64_t side = 1ll << l;
-        for (int dx = -1; dx <= 1; dx++)
-            for (int dy = -1; dy <= 1; dy++) {
-                if (!dx && !dy) continue;
-                int64_t cx = sx + dx, cy = sy + dy;
-                if (cx < 0 || cy < 0 || cx >= side || cy >= side) continue;
-                uint64_t c = morton((uint64_t)cx, (uint64_t)cy);
-                if (hs_has(H, ent_make(l, c, 0))) continue;
-                if (!hs_has(H, ent_make(l - 1, c >> 2, 0))) continue;
-                hs_insert(H, ent_make(l, c, 1));
-            }
+        if (cx < 0 || cy < 0 || cx >= side || cy >= side) continue;
+        const uint64_t c = morton((uint64_t)cx, (uint64_t)cy);
+        if (hs_has(H, ent_make(l, c, 0))) continue;
+        if (!hs_has(H, ent_make(l - 1, c >> 2, 0))) continue;
+        hs_insert(H, ent_make(l, c, 1));
     }
 }
 
@@ -325,21 +324,123 @@ __global__ void k_nodes(LevelTable T, int64_t n_nodes, const uint64_t *__restric
     }
 }
 
-// work lists + counts: misc[0] leaf_list, misc[1] p2m_list, misc[2] leaves,
-// misc[3] fake, misc[4] xlist
-__global__ void k_lists(int64_t n_nodes, const int8_t *__restrict__ nlev, const uint8_t *__restrict__ nflag,
-                        const int32_t *__restrict__ nbot, const int32_t *__restrict__ ntop, int32_t *leaf_list,
-                        int32_t *p2m_list, unsigned long long *cnt) {
-    for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_nodes; g += (int64_t)gridDim.x * blockDim.x) {
-        uint8_t f = nflag[g];
-        bool fake = f & NF_FAKE, split = f & NF_SPLIT, xl = f & NF_XLIST;
-        bool real_leaf = !fake && !split;
-        int64_t ns = ntop[g] - nbot[g];
-        if (real_leaf) atomicAdd(&cnt[2], 1ull);
-        if (fake) atomicAdd(&cnt[3], 1ull);
-        if (xl) atomicAdd(&cnt[4], 1ull);
-        if (real_leaf && ns > 0) leaf_list[atomicAdd(&cnt[0], 1ull)] = (int32_t)g;
-        if (nlev[g] >= 2 && ns > 0 && ((real_leaf && !xl) || fake)) p2m_list[atomicAdd(&cnt[1], 1ull)] = (int32_t)g;
+// Work lists in node order (level-major, Morton order within a level), so
+// that consecutive entries share a level and a neighbourhood.  The nodes are
+// cut into tiles of LT_TILE: k_lists_count counts each tile's entries,
+// k_lists_scan turns the counts into offsets, k_lists_write compacts each
+// tile in order.  cnt: [0] leaf_list, [1] p2m_list, [2] leaves, [3] fake,
+// [4] xlist.
+constexpr int LT_THREADS = 256, LT_TILE = LT_THREADS * 8;
+struct ListFlags {
+    bool leaf = false, p2m = false, real_leaf = false, fake = false, xl = false;
+};
+__device__ __forceinline__ ListFlags list_flags(int64_t g, const int8_t *nlev, const uint8_t *nflag,
+                                                const int32_t *nbot, const int32_t *ntop) {
+    ListFlags r;
+    const uint8_t f = nflag[g];
+    r.fake = f & NF_FAKE;
+    r.xl = f & NF_XLIST;
+    r.real_leaf = !r.fake && !(f & NF_SPLIT);
+    const bool pts = ntop[g] > nbot[g];
+    r.leaf = r.real_leaf && pts;
+    r.p2m = nlev[g] >= 2 && pts && ((r.real_leaf && !r.xl) || r.fake);
+    return r;
+}
+// Exclusive scan over the block (blockDim.x a multiple of 32); total = block sum.
+__device__ __forceinline__ unsigned block_excl_scan(unsigned v, unsigned *sm, unsigned &total) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    unsigned x = v;
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) sm[wid] = x;
+    __syncthreads();
+    if (wid == 0) {
+        unsigned z = lane < nw ? sm[lane] : 0u;
+        for (int o = 1; o < 32; o <<= 1) {
+            const unsigned y = __shfl_up_sync(0xffffffffu, z, o);
+            if (lane >= o) z += y;
+        }
+        sm[lane] = z;  // inclusive prefix of the warp sums
+    }
+    __syncthreads();
+    const unsigned r = (wid ? sm[wid - 1] : 0u) + x - v;
+    total = sm[nw - 1];
+    __syncthreads();
+    return r;
+}
+__global__ void __launch_bounds__(LT_THREADS) k_lists_count(int64_t n_nodes, const int8_t *__restrict__ nlev,
+                                                            const uint8_t *__restrict__ nflag,
+                                                            const int32_t *__restrict__ nbot,
+                                                            const int32_t *__restrict__ ntop, uint32_t *tcnt,
+                                                            unsigned long long *cnt) {
+    __shared__ unsigned sm[32];
+    const int64_t g0 = (int64_t)blockIdx.x * LT_TILE;
+    unsigned c[5] = {0, 0, 0, 0, 0};
+    for (int i = threadIdx.x; i < LT_TILE; i += LT_THREADS) {
+        const int64_t g = g0 + i;
+        if (g >= n_nodes) break;
+        const ListFlags f = list_flags(g, nlev, nflag, nbot, ntop);
+        c[0] += f.leaf;
+        c[1] += f.p2m;
+        c[2] += f.real_leaf;
+        c[3] += f.fake;
+        c[4] += f.xl;
+    }
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        unsigned t;
+        block_excl_scan(c[k], sm, t);
+        if (threadIdx.x == 0) {
+            if (k < 2) tcnt[2 * blockIdx.x + k] = t;
+            else if (t) atomicAdd(&cnt[k], (unsigned long long)t);
+        }
+    }
+}
+// one block: tile counts -> exclusive tile offsets (both lists); totals to cnt[0..1]
+__global__ void __launch_bounds__(1024) k_lists_scan(int64_t ntiles, uint32_t *tcnt, unsigned long long *cnt) {
+    __shared__ unsigned sm[32];
+    unsigned carry0 = 0, carry1 = 0;
+    for (int64_t base = 0; base < ntiles; base += blockDim.x) {
+        const int64_t i = base + threadIdx.x;
+        const unsigned a = i < ntiles ? tcnt[2 * i] : 0u, b = i < ntiles ? tcnt[2 * i + 1] : 0u;
+        unsigned ta, tb;
+        const unsigned ea = block_excl_scan(a, sm, ta);
+        const unsigned eb = block_excl_scan(b, sm, tb);
+        if (i < ntiles) {
+            tcnt[2 * i] = carry0 + ea;
+            tcnt[2 * i + 1] = carry1 + eb;
+        }
+        carry0 += ta;
+        carry1 += tb;
+    }
+    if (threadIdx.x == 0) {
+        cnt[0] = carry0;
+        cnt[1] = carry1;
+    }
+}
+__global__ void __launch_bounds__(LT_THREADS) k_lists_write(int64_t n_nodes, const int8_t *__restrict__ nlev,
+                                                            const uint8_t *__restrict__ nflag,
+                                                            const int32_t *__restrict__ nbot,
+                                                            const int32_t *__restrict__ ntop,
+                                                            const uint32_t *__restrict__ tcnt, int32_t *leaf_list,
+                                                            int32_t *p2m_list) {
+    __shared__ unsigned sm[32];
+    unsigned oa = tcnt[2 * blockIdx.x], ob = tcnt[2 * blockIdx.x + 1];
+    const int64_t g0 = (int64_t)blockIdx.x * LT_TILE;
+    for (int k = 0; k < LT_TILE; k += LT_THREADS) {
+        if (g0 + k >= n_nodes) break;  // uniform over the block
+        const int64_t g = g0 + k + threadIdx.x;
+        ListFlags f;
+        if (g < n_nodes) f = list_flags(g, nlev, nflag, nbot, ntop);
+        unsigned ta, tb;
+        const unsigned ea = block_excl_scan(f.leaf, sm, ta);
+        const unsigned eb = block_excl_scan(f.p2m, sm, tb);
+        if (f.leaf) leaf_list[oa + ea] = (int32_t)g;
+        if (f.p2m) p2m_list[ob + eb] = (int32_t)g;
+        oa += ta;
+        ob += tb;
     }
 }
 
@@ -539,8 +640,18 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     KIFMM_LAUNCHED();
     unsigned long long *cnt = (unsigned long long *)P->misc.p + 32;
     KIFMM_CUDA(cudaMemsetAsync(cnt, 0, 8 * sizeof(unsigned long long), s));
-    k_lists<<<ng, TB, 0, s>>>(NN, P->nlev.p, P->nflag.p, P->nbot.p, P->ntop.p, P->leaf_list.p, P->p2m_list.p, cnt);
-    KIFMM_LAUNCHED();
+    {
+        const int64_t ntiles = (NN + LT_TILE - 1) / LT_TILE;
+        P->list_tiles.alloc(2 * ntiles);
+        k_lists_count<<<(unsigned)ntiles, LT_THREADS, 0, s>>>(NN, P->nlev.p, P->nflag.p, P->nbot.p, P->ntop.p,
+                                                              P->list_tiles.p, cnt);
+        KIFMM_LAUNCHED();
+        k_lists_scan<<<1, 1024, 0, s>>>(ntiles, P->list_tiles.p, cnt);
+        KIFMM_LAUNCHED();
+        k_lists_write<<<(unsigned)ntiles, LT_THREADS, 0, s>>>(NN, P->nlev.p, P->nflag.p, P->nbot.p, P->ntop.p,
+                                                              P->list_tiles.p, P->leaf_list.p, P->p2m_list.p);
+        KIFMM_LAUNCHED();
+    }
     unsigned long long c5[5];
     KIFMM_CUDA(cudaMemcpyAsync(c5, cnt, sizeof(c5), cudaMemcpyDeviceToHost, s));
     KIFMM_CUDA(cudaStreamSynchronize(s));
