@@ -1,5 +1,7 @@
 // capi.cu -- the extern "C" entry points declared in include/kifmm2d.h.
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 
 #include "kifmm_internal.cuh"
@@ -56,6 +58,18 @@ static void resolve_phases(kifmm_plan *P) {
     P->pending.clear();
 }
 
+void ensure_dyn_smem(const void *fn, size_t bytes) {
+    static std::mutex mu;
+    static std::map<std::pair<int, const void *>, size_t> done;
+    int dev = 0;
+    KIFMM_CUDA(cudaGetDevice(&dev));
+    std::lock_guard<std::mutex> lock(mu);
+    size_t &cur = done[{dev, fn}];
+    if (bytes <= cur) return;
+    KIFMM_CUDA(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+    cur = bytes;
+}
+
 void set_error(const std::string &msg) { g_last_error = msg; }
 
 template <class F>
@@ -93,11 +107,12 @@ static void copy_in(kifmm_plan *P, DBuf<double> &dst, const double *src, int64_t
 // Device-side failures reported through a flag (a tensor-core M2L wait that
 // ran out of its poll budget); read after the stream has drained.
 static void check_device_flags(kifmm_plan *P) {
-    if (!uses_tensor_m2l(P) || !P->scal.p) return;
-    unsigned long long f = 0;
-    KIFMM_CUDA(cudaMemcpyAsync(&f, P->scal.p + 15, sizeof(f), cudaMemcpyDeviceToHost, P->stream));
+    if (!P->scal.p) return;
+    unsigned long long f[2] = {0, 0};
+    KIFMM_CUDA(cudaMemcpyAsync(f, P->scal.p + KIFMM_SCAL_PASS_ERR, sizeof(f), cudaMemcpyDeviceToHost, P->stream));
     KIFMM_CUDA(cudaStreamSynchronize(P->stream));
-    KIFMM_REQUIRE(f == 0, KIFMM_ERR_CUDA, "tensor-core M2L: an MMA completion wait timed out");
+    KIFMM_REQUIRE(f[0] == 0, KIFMM_ERR_CUDA, "M2M/L2L pass: a bulk-copy wait timed out");
+    KIFMM_REQUIRE(f[1] == 0, KIFMM_ERR_CUDA, "tensor-core M2L: an MMA completion wait timed out");
 }
 
 static void copy_out(kifmm_plan *P, double *dst, const double *src, int64_t n, int mem) {

@@ -206,6 +206,21 @@ struct kifmm_plan {
 
 namespace kifmm {
 // Brackets one phase with CUDA events on the plan's stream when profiling.
+// Raise a kernel's dynamic shared-memory limit to at least `bytes` on the
+// current device; the driver call is made once per (device, kernel, larger
+// size), not before every launch.
+void ensure_dyn_smem(const void *fn, size_t bytes);
+template <class K>
+inline void ensure_dyn_smem(K *fn, size_t bytes) {
+    ensure_dyn_smem((const void *)fn, bytes);
+}
+
+// device scalar slots (plan->scal) holding error flags that the host reads
+// after an apply: a bulk-copy wait in the level passes that ran out, and an
+// MMA completion wait in the tensor-core M2L that ran out
+constexpr int KIFMM_SCAL_PASS_ERR = 14;
+constexpr int KIFMM_SCAL_TC_ERR = 15;
+
 struct PhaseScope {
     kifmm_plan *P;
     int id;

@@ -31,6 +31,7 @@
 #include <cmath>
 
 #include "passes.cuh"
+#include "async_copy.cuh"
 
 namespace kifmm {
 
@@ -73,9 +74,6 @@ __host__ __device__ __forceinline__ uint32_t core_off(int row, int k, int rows, 
 }
 
 // ------------------------------------------------------------- PTX helpers
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
 __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
     return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);  // version 1, no swizzle
@@ -109,25 +107,6 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
 }
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void mbar_init(uint32_t bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
-    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-}
-// bounded wait on the mbarrier phase; false after `limit` polls
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
-    for (long long it = 0; it < limit; it++) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.b32 %0, 1, 0, p;\n\t}\n"
-            : "=r"(done)
-            : "r"(bar), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
@@ -280,14 +259,6 @@ __global__ void k_tc_preslice(PassArgs A, int64_t n_ent, TcPre T) {
     }
 }
 
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
 
 // ------------------------------------------------------------- the kernel
 struct TcArgs {
@@ -533,7 +504,7 @@ static void run_m2l_tensor_t(kifmm_plan *P, const PassArgs &A) {
     T.aslices = P->tc_a.p;
     T.rowscale = P->tc_rowscale.p;
     T.pre = pre;
-    T.err = P->scal.p + 15;
+    T.err = P->scal.p + KIFMM_SCAL_TC_ERR;
     T.wait_limit = 1ll << 26;
     T.lmin = 1;
     T.lmax = L - 2;
@@ -544,7 +515,7 @@ static void run_m2l_tensor_t(kifmm_plan *P, const PassArgs &A) {
     }
     if (!tiles) return;
     size_t smem = tc_smem_bytes<F>();
-    KIFMM_CUDA(cudaFuncSetAttribute(k_m2l_tc<F>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ensure_dyn_smem(k_m2l_tc<F>, smem);
     k_m2l_tc<F><<<(unsigned)tiles, TC_THREADS, smem, P->stream>>>(T);
     KIFMM_LAUNCHED();
 }

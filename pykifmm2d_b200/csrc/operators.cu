@@ -291,13 +291,13 @@ void build_operators(kifmm_plan *P) {
         k_ops_surfaces<<<L, Q, 0, s>>>(A);
         KIFMM_LAUNCHED();
         size_t smem = (size_t)Q * 2 * Q * sizeof(double) + Q * sizeof(double);
-        KIFMM_CUDA(cudaFuncSetAttribute(k_ops_inverse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ensure_dyn_smem(k_ops_inverse, smem);
         k_ops_inverse<<<L, 256, smem, s>>>(A);
         KIFMM_LAUNCHED();
         k_ops_kmats<<<dim3(L, 50), 256, 0, s>>>(A);
         KIFMM_LAUNCHED();
         size_t csm = (size_t)5 * Q * Q * sizeof(double);
-        KIFMM_CUDA(cudaFuncSetAttribute(k_ops_compose, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)csm));
+        ensure_dyn_smem(k_ops_compose, csm);
         k_ops_compose<<<dim3(L, 51), 256, csm, s>>>(A);
         KIFMM_LAUNCHED();
         k_ops_assemble<<<dim3(L, 9), 256, 0, s>>>(A);
@@ -312,7 +312,7 @@ void build_operators(kifmm_plan *P) {
             const int R = 2 * KIFMM_TAYLOR_P + 1;
             P->l2p_taylor.alloc((size_t)L * Q * R);
             size_t tsm = ((size_t)R * Q + (size_t)Q * Q) * sizeof(double);
-            KIFMM_CUDA(cudaFuncSetAttribute(k_ops_taylor, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tsm));
+            ensure_dyn_smem(k_ops_taylor, tsm);
             k_ops_taylor<<<L, 256, tsm, s>>>(A, P->l2p_taylor.p, KIFMM_TAYLOR_P);
             KIFMM_LAUNCHED();
         }

@@ -8,6 +8,7 @@
 // of an entry (split or X-list cell) form one 4Q vector.
 #include "kifmm_internal.cuh"
 #include "passes.cuh"
+#include "async_copy.cuh"
 
 namespace kifmm {
 
@@ -393,21 +394,21 @@ constexpr int LG_THREADS = 256;
 // eight independent loads per thread in flight (16-byte loads when src is
 // 16-byte aligned and n even).  Small staging loops are otherwise bound by
 // one load latency per iteration.
-template <class F>
+template <int NTHR, class F>
 __device__ __forceinline__ void stage_f64(const double *__restrict__ src, int n, F store) {
     if ((((uintptr_t)src) & 15) == 0 && (n & 1) == 0) {
         const double2 *s2 = (const double2 *)src;
         const int n2 = n >> 1;
-        for (int i0 = threadIdx.x; i0 < n2; i0 += 8 * LG_THREADS) {
+        for (int i0 = threadIdx.x; i0 < n2; i0 += 8 * NTHR) {
             double2 v[8];
 #pragma unroll
             for (int k = 0; k < 8; k++) {
-                const int i = i0 + k * LG_THREADS;
+                const int i = i0 + k * NTHR;
                 v[k] = i < n2 ? s2[i] : make_double2(0.0, 0.0);
             }
 #pragma unroll
             for (int k = 0; k < 8; k++) {
-                const int i = i0 + k * LG_THREADS;
+                const int i = i0 + k * NTHR;
                 if (i < n2) {
                     store(2 * i, v[k].x);
                     store(2 * i + 1, v[k].y);
@@ -415,16 +416,16 @@ __device__ __forceinline__ void stage_f64(const double *__restrict__ src, int n,
             }
         }
     } else {
-        for (int i0 = threadIdx.x; i0 < n; i0 += 8 * LG_THREADS) {
+        for (int i0 = threadIdx.x; i0 < n; i0 += 8 * NTHR) {
             double v[8];
 #pragma unroll
             for (int k = 0; k < 8; k++) {
-                const int i = i0 + k * LG_THREADS;
+                const int i = i0 + k * NTHR;
                 v[k] = i < n ? src[i] : 0.0;
             }
 #pragma unroll
             for (int k = 0; k < 8; k++) {
-                const int i = i0 + k * LG_THREADS;
+                const int i = i0 + k * NTHR;
                 if (i < n) store(i, v[k]);
             }
         }
@@ -442,7 +443,7 @@ __global__ void __launch_bounds__(LG_THREADS) k_lvl_gemm_b(PassArgs A, int l, in
     // staging: eight independent loads per thread in flight
     if (Mp != M)
         for (int i = threadIdx.x; i < K * Mp; i += LG_THREADS) opS[i] = 0.0;
-    stage_f64(op, K * M, [&](int i, double v) {
+    stage_f64<LG_THREADS>(op, K * M, [&](int i, double v) {
         const int c = i / M;
         opS[c * Mp + (i - c * M)] = v;
     });
@@ -452,7 +453,7 @@ __global__ void __launch_bounds__(LG_THREADS) k_lvl_gemm_b(PassArgs A, int l, in
             const int t = i / K;
             xS[t * ldx + (i - t * K)] = 0.0;
         }
-        stage_f64(src0, nt * K, [&](int i, double v) {
+        stage_f64<LG_THREADS>(src0, nt * K, [&](int i, double v) {
             const int t = i / K;
             xS[t * ldx + (i - t * K)] = v;
         });
@@ -514,6 +515,128 @@ __global__ void __launch_bounds__(LG_THREADS) k_lvl_gemm_b(PassArgs A, int l, in
     }
 }
 
+// The same products on the FP64 tensor path (mma.sync m8n8k4 .f64; the FP64
+// vector pipe sustains a quarter of its rate).  A block takes 32 entries.  It
+// stages by bulk asynchronous copies on one mbarrier: the operator [K][M] row
+// by row into a row stride ldo = 4 mod 16 doubles (conflict-free fragment
+// loads), the entries' columns X into rows of stride ldx, and for L2L the
+// children groups' current u_down (M = 4Q contiguous doubles per entry) into
+// C.  Warp w computes all M rows for entries 8w..8w+7 in chunks of 8*MT rows
+// (MT 8x8 accumulator tiles); results are written (M2M) or added (L2L) into C
+// in shared memory and leave by bulk stores, one row per entry.  Fragments:
+// A[row = lane/4][k = lane%4], B[k = lane%4][n = lane/4],
+// C[row = lane/4][n = 2*(lane%4) + {0,1}].  Needs M % 8 == 0, K % 4 == 0 and
+// 16-byte aligned operator rows.  A copy wait that runs out sets *err and the
+// block leaves without writing.
+constexpr int LM_THREADS = 128;
+__device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+__host__ __device__ constexpr int pad4mod16(int m) { return m + (20 - m % 16) % 16; }
+static size_t lvl_mma_smem(int M, int K) {
+    return ((size_t)K * pad4mod16(M) + 32 * (size_t)pad4mod16(K) + 32 * (size_t)M) * sizeof(double);
+}
+
+template <int MODE, int MT>
+__global__ void __launch_bounds__(LM_THREADS) k_lvl_mma(PassArgs A, int l, int M, int K, long long wait_limit,
+                                                       unsigned long long *err) {
+    extern __shared__ __align__(128) double sm_m[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ int snode[32];  // node of the entry (M2M), or of a split entry (L2L); -1 otherwise
+    const int ldo = pad4mod16(M), ldx = pad4mod16(K), Q = A.Q, tid = threadIdx.x;
+    double *opS = sm_m;                  // [K][ldo]
+    double *xS = opS + (size_t)K * ldo;  // [32][ldx]
+    double *cS = xS + (size_t)32 * ldx;  // [32][M]
+    const int64_t ne = A.T.ne[l], eoff = A.T.eoff[l], e0 = (int64_t)blockIdx.x * 32;
+    const int nt = (int)min((int64_t)32, ne - e0);
+    const double *op = A.ops + (size_t)l * A.stride + (MODE == 0 ? A.off_m2m : A.off_l2l);  // [K][M]
+    const size_t child0 = (size_t)A.T.off[l + 1] + 4 * (size_t)e0;  // first child of the block's first entry
+    int has = 0;
+    if (tid < 32) {
+        int node = -1;
+        if (tid < nt) {
+            const int64_t e = eoff + e0 + tid;
+            if (MODE == 0 || !(A.ent[e] & 1)) node = A.ent_node[e];
+        }
+        snode[tid] = node;
+        has = node >= 0;
+    }
+    const uint32_t mb = smem_u32(&bar);
+    if (tid == 0) mbar_init(mb);
+    const int nact = __syncthreads_count(has);
+    if (tid == 0) mbar_expect_tx(mb, (uint32_t)(K * M + nact * K + (MODE == 1 ? nact * M : 0)) * 8u);
+    __syncthreads();
+    for (int c = tid; c < K + 64; c += LM_THREADS) {
+        if (c < K) {
+            bulk_g2s(smem_u32(opS + (size_t)c * ldo), op + (size_t)c * M, (uint32_t)M * 8u, mb);
+        } else if (c < K + 32) {
+            const int n = c - K;
+            if (n < nt && snode[n] >= 0) {
+                const double *src = MODE == 0 ? A.uup + (child0 + 4 * (size_t)n) * Q : A.udown + (size_t)snode[n] * Q;
+                bulk_g2s(smem_u32(xS + (size_t)n * ldx), src, (uint32_t)K * 8u, mb);
+            }
+        } else if (MODE == 1) {
+            const int n = c - K - 32;
+            if (n < nt && snode[n] >= 0)
+                bulk_g2s(smem_u32(cS + (size_t)n * M), A.udown + (child0 + 4 * (size_t)n) * Q, (uint32_t)M * 8u, mb);
+        }
+    }
+    const bool ok = __syncthreads_and(mbar_wait(mb, 0, wait_limit));
+    if (!ok) {
+        if (tid == 0) atomicOr(err, 1ull);
+        mbar_wait(mb, 0, wait_limit);  // let copies in flight land before the block leaves
+        return;
+    }
+    const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
+    const int n0 = warp * 8;
+    if (n0 < nt) {
+        const double *xb = xS + (size_t)(n0 + g) * ldx + t;
+        for (int rc = 0; rc < M; rc += 8 * MT) {
+            double acc[MT][2];
+#pragma unroll
+            for (int i = 0; i < MT; i++) acc[i][0] = acc[i][1] = 0.0;
+            const double *ab = opS + (size_t)t * ldo + rc + g;
+#pragma unroll 2
+            for (int k0 = 0; k0 < K; k0 += 4) {
+                const double b = xb[k0];
+#pragma unroll
+                for (int i = 0; i < MT; i++)
+                    if (rc + 8 * i < M) dmma_8x8x4(acc[i][0], acc[i][1], ab[(size_t)k0 * ldo + 8 * i], b);
+            }
+#pragma unroll
+            for (int i = 0; i < MT; i++) {
+                const int r = rc + 8 * i + g;
+                if (r >= M) continue;
+#pragma unroll
+                for (int j = 0; j < 2; j++) {
+                    const int n = n0 + 2 * t + j;
+                    if (n >= nt || snode[n] < 0) continue;
+                    if (MODE == 0) cS[(size_t)n * M + r] = acc[i][j];
+                    else cS[(size_t)n * M + r] += acc[i][j];
+                }
+            }
+        }
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (tid < nt && snode[tid] >= 0) {
+        double *dst = MODE == 0 ? A.uup + (size_t)snode[tid] * Q : A.udown + (child0 + 4 * (size_t)tid) * Q;
+        bulk_s2g(dst, smem_u32(cS + (size_t)tid * M), (uint32_t)M * 8u);
+        bulk_commit();
+        bulk_wait_read();
+    }
+}
+
+template <int MODE, int MT>
+static void launch_lvl_mma(kifmm_plan *P, const PassArgs &A, int l, int M, int K, size_t smem) {
+    ensure_dyn_smem(k_lvl_mma<MODE, MT>, smem);
+    k_lvl_mma<MODE, MT><<<(unsigned)((P->lt.ne[l] + 31) / 32), LM_THREADS, smem, P->stream>>>(
+        A, l, M, K, 1ll << 26, P->scal.p + KIFMM_SCAL_PASS_ERR);
+    KIFMM_LAUNCHED();
+}
+
 // NT columns per block: (ceil(M/4)) x (NT/4) threads <= 256 and at most
 // 200 KB of shared memory
 static int lvl_gemm_nt(int M, int K) {
@@ -530,14 +653,25 @@ static void launch_lvl_gemm(kifmm_plan *P, const PassArgs &A, int l) {
     const int Q = P->Q;
     const int M = MODE == 0 ? Q : 4 * Q, K = MODE == 0 ? 4 * Q : Q;
     const int64_t ne = P->lt.ne[l];
+    if (M % 8 == 0 && K % 4 == 0 && A.stride % 2 == 0 && A.off_m2m % 2 == 0 && A.off_l2l % 2 == 0) {
+        // FP64 tensor path with bulk-copy staging (16-byte aligned rows)
+        const size_t smem = lvl_mma_smem(M, K);
+        if (smem <= (size_t)(220 << 10)) {
+            const int mt = M / 8;
+            if (mt <= 2) launch_lvl_mma<MODE, 2>(P, A, l, M, K, smem);
+            else if (mt <= 4) launch_lvl_mma<MODE, 4>(P, A, l, M, K, smem);
+            else if (mt <= 8) launch_lvl_mma<MODE, 8>(P, A, l, M, K, smem);
+            else launch_lvl_mma<MODE, 16>(P, A, l, M, K, smem);
+            return;
+        }
+    }
     {  // broadcast form when the operator and the entry tile fit in shared memory
         constexpr int RPT = MODE == 0 ? 8 : 16;
         const int RG = (M + RPT - 1) / RPT, Mp = RG * RPT;
         const int wps = RG < 8 ? RG : 8, NT = 32 * (8 / wps);
         const size_t smem = ((size_t)K * Mp + (size_t)NT * (K + 1)) * sizeof(double);
         if (smem <= (size_t)(220 << 10)) {
-            KIFMM_CUDA(cudaFuncSetAttribute(k_lvl_gemm_b<MODE, RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)smem));
+            ensure_dyn_smem(k_lvl_gemm_b<MODE, RPT>, smem);
             k_lvl_gemm_b<MODE, RPT><<<(unsigned)((ne + NT - 1) / NT), LG_THREADS, smem, P->stream>>>(A, l, M, K, Mp,
                                                                                                      NT);
             KIFMM_LAUNCHED();
@@ -547,7 +681,7 @@ static void launch_lvl_gemm(kifmm_plan *P, const PassArgs &A, int l) {
     int nt = lvl_gemm_nt(M, K);
     int threads = ((M + 3) / 4) * (nt / 4);
     size_t smem = ((size_t)K * M + (size_t)nt * (K + 1)) * sizeof(double);
-    KIFMM_CUDA(cudaFuncSetAttribute(k_lvl_gemm_d<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ensure_dyn_smem(k_lvl_gemm_d<MODE>, smem);
     k_lvl_gemm_d<MODE><<<(unsigned)((ne + nt - 1) / nt), threads, smem, P->stream>>>(A, l, M, K, nt);
     KIFMM_LAUNCHED();
 }
@@ -565,6 +699,8 @@ void run_upward_downward(kifmm_plan *P) {
     P->udown.alloc((size_t)NN * Q);
     k_gather_tau<<<grid_for(n, 256, P->num_sms * 8), 256, 0, s>>>(P->tau.p, P->perm.p, n, P->taus.p);
     KIFMM_LAUNCHED();
+    // error flags of the level passes and the tensor-core M2L
+    KIFMM_CUDA(cudaMemsetAsync(P->scal.p + KIFMM_SCAL_PASS_ERR, 0, 2 * sizeof(unsigned long long), s));
     if (P->opt.precision == KIFMM_PREC_MIXED) {
         run_passes_mixed(P);
         return;
@@ -585,7 +721,7 @@ void run_upward_downward(kifmm_plan *P) {
     PhaseScope ph(P, KIFMM_PHASE_M2L);
     int thr = ((4 * Q + 31) / 32) * 32;
     size_t smem = (size_t)M2L_TE * 4 * Q * sizeof(double);
-    KIFMM_CUDA(cudaFuncSetAttribute(k_m2l_d, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    ensure_dyn_smem(k_m2l_d, smem);
     for (int l = 1; l <= L - 2; l++) {
         int64_t ne = P->lt.ne[l];
         if (!ne) continue;

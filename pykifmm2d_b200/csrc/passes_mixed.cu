@@ -446,7 +446,7 @@ void run_passes_mixed(kifmm_plan *P) {
     size_t smem = (size_t)M2LF_TE * 4 * Q * sizeof(float);
     if (simt) {
         PhaseScope ph(P, KIFMM_PHASE_M2L);
-        KIFMM_CUDA(cudaFuncSetAttribute(k_m2l_f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ensure_dyn_smem(k_m2l_f, smem);
         for (int l = 1; l <= L - 2; l++) {
             int64_t ne = P->lt.ne[l];
             if (!ne) continue;
@@ -457,7 +457,6 @@ void run_passes_mixed(kifmm_plan *P) {
     }
     {
         PhaseScope ph(P, KIFMM_PHASE_M2L);
-        KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 15, 0, sizeof(unsigned long long), s));
         run_m2l_tensor(P, A);  // all levels at once
     }
     PhaseScope ph(P, KIFMM_PHASE_L2L);
