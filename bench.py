@@ -248,10 +248,10 @@ def p2p_flops_per_pair(kernel):
 
 def measured_traffic():
     """DRAM bytes per launch of the profiled kernels, from the committed ncu
-    summary profiles/traffic_c2.txt (lines: kernel_name bytes)."""
+    summary profiles/traffic_laplace_mixture_1m.txt (lines: kernel_name bytes)."""
     out = {}
     try:
-        for line in open(os.path.join(ROOT, "profiles", "traffic_c2.txt")):
+        for line in open(os.path.join(ROOT, "profiles", "traffic_laplace_mixture_1m.txt")):
             p = line.split()
             if len(p) == 2 and not line.startswith("#"):
                 out[p[0]] = float(p[1])
