@@ -194,6 +194,7 @@ struct kifmm_plan {
     kifmm::DBuf<uint64_t> key2, hash, list;
     kifmm::DBuf<int32_t> perm2;
     kifmm::DBuf<uint32_t> sort_hist;
+    kifmm::DBuf<unsigned long long> sort_status;  // radix sort look-back words
     kifmm::DBuf<unsigned long long> scal;  // small device scalars
     kifmm::DBuf<int64_t> misc;
 
@@ -218,6 +219,7 @@ inline void ensure_dyn_smem(K *fn, size_t bytes) {
 // device scalar slots (plan->scal) holding error flags that the host reads
 // after an apply: a bulk-copy wait in the level passes that ran out, and an
 // MMA completion wait in the tensor-core M2L that ran out
+constexpr int KIFMM_SCAL_SORT_ERR = 13;  // a radix-sort look-back wait that ran out
 constexpr int KIFMM_SCAL_PASS_ERR = 14;
 constexpr int KIFMM_SCAL_TC_ERR = 15;
 
@@ -342,6 +344,8 @@ bool uses_tensor_m2l(const kifmm_plan *P);
 void radix_sort_pairs(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_tmp, int64_t n, int bits,
                       kifmm_plan *P);
 void radix_sort_keys(uint64_t *key, uint64_t *key_tmp, int64_t n, int bits, kifmm_plan *P);
+void radix_sort_keys_shifts(uint64_t *key, uint64_t *key_tmp, int64_t n, const int *shifts, int npass,
+                            kifmm_plan *P);
 void radix_sort_pairs_bits(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_tmp, int64_t n, int lo_bit,
                            int bits, kifmm_plan *P);
 

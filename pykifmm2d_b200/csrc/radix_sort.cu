@@ -1,7 +1,10 @@
 // radix_sort.cu -- stable LSD radix sort of 64-bit keys (optionally with int32
 // payloads) for the Morton-key tree build.
 //
-// Each pass sorts one 8-bit digit in three kernels:
+// The plan's sorts use the onesweep form further down (one histogram kernel,
+// then one kernel per 8-bit digit).  The no-allocation entry point keeps the
+// three-kernel form, whose scratch is a fixed histogram table: each pass
+// sorts one 8-bit digit in three kernels:
 //   1. per-tile digit histograms (tile = 256 threads x 16 keys),
 //   2. a per-digit exclusive scan over the tiles (one block per digit), which
 //      also leaves the 256 digit totals behind the table,
@@ -9,6 +12,8 @@
 //      with __match_any_sync, warps are combined by a per-digit prefix in
 //      shared memory, and the tile's base is the digit's start (a scan of the
 //      digit totals) plus the digit's scanned tile prefix.
+#include <algorithm>
+
 #include "kifmm_internal.cuh"
 
 namespace kifmm {
@@ -126,34 +131,252 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t *__res
     }
 }
 
-static void rs_run(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_tmp, int64_t n, int bits,
-                   kifmm_plan *P, bool pairs, int lo_bit = 0) {
-    if (n <= 1) return;
+// ---------------------------------------------------------------- onesweep
+// The plan's sorts: one read of the keys counts the digits of every pass
+// (k_os_hist), then each pass is ONE kernel (k_os_pass) that ranks a tile's
+// keys as k_rs_scatter does and finds the tile's offset for each digit by a
+// decoupled look-back over the tiles before it: every tile publishes its digit
+// counts (AGG) as soon as it has ranked its keys and then its inclusive prefix
+// (PREFIX), and a tile sums its predecessors' values back to the first PREFIX.
+// Tiles take their index from a counter in the order they start, so every
+// tile waited on is already running and publishes without waiting itself.
+// Waits are bounded; one that runs out sets *err (the tree build then fails).
+constexpr int OS_MAX_PASSES = 8;
+struct OsShifts {
+    int n;
+    int s[OS_MAX_PASSES];
+};
+constexpr unsigned long long OS_AGG = 1ull << 62, OS_PREFIX = 2ull << 62, OS_VAL = (1ull << 62) - 1;
+
+__device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long long *p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+
+__global__ void __launch_bounds__(RS_THREADS) k_os_hist(const uint64_t *__restrict__ key, int64_t n, OsShifts sh,
+                                                         uint32_t *__restrict__ hist) {
+    __shared__ uint32_t h[OS_MAX_PASSES][256];
+    for (int i = threadIdx.x; i < OS_MAX_PASSES * 256; i += RS_THREADS) (&h[0][0])[i] = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    for (int64_t base = (int64_t)blockIdx.x * RS_TILE; base < n; base += (int64_t)gridDim.x * RS_TILE) {
+        uint64_t k[RS_ITEMS];
+#pragma unroll
+        for (int r = 0; r < RS_ITEMS; r++) {
+            const int64_t idx = base + r * RS_THREADS + threadIdx.x;
+            k[r] = idx < n ? key[idx] : 0;
+        }
+#pragma unroll
+        for (int r = 0; r < RS_ITEMS; r++) {
+            const bool ok = base + r * RS_THREADS + threadIdx.x < n;
+            for (int p = 0; p < sh.n; p++) {
+                const uint32_t d = ok ? (uint32_t)((k[r] >> sh.s[p]) & 255) : 256u;
+                const unsigned peers = __match_any_sync(0xffffffffu, d);  // one add per distinct digit
+                if (d < 256 && lane == __ffs(peers) - 1) atomicAdd(&h[p][d], (uint32_t)__popc(peers));
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < sh.n * 256; i += RS_THREADS) {
+        const uint32_t c = (&h[0][0])[i];
+        if (c) atomicAdd(&hist[i], c);
+    }
+}
+
+// One pass.  The tile's keys are ranked per warp, ordered by digit in shared
+// memory (tile-local digit starts tstart[]), and written out in that order so
+// that consecutive threads store consecutive positions of one digit's run.
+// The look-back reads eight predecessors' words per step.
+constexpr size_t OS_PASS_SMEM = (size_t)RS_TILE * (sizeof(uint64_t) + sizeof(int32_t));
+template <bool PAIRS>
+__global__ void __launch_bounds__(RS_THREADS) k_os_pass(const uint64_t *__restrict__ key, const int32_t *__restrict__ val,
+                                                         uint64_t *__restrict__ okey, int32_t *__restrict__ oval,
+                                                         int64_t n, int shift, const uint32_t *__restrict__ ghist,
+                                                         unsigned long long *status, unsigned *tile_ctr,
+                                                         unsigned long long *err, long long limit) {
+    extern __shared__ __align__(16) unsigned char os_sm[];
+    uint64_t *skey = (uint64_t *)os_sm;                        // [RS_TILE]
+    int32_t *sval = (int32_t *)(os_sm + RS_TILE * sizeof(uint64_t));
+    __shared__ uint32_t wcnt[RS_WARPS][256];
+    __shared__ uint32_t tstart[256];
+    __shared__ uint32_t dbase[256];
+    __shared__ uint32_t wsum[2][RS_WARPS];
+    __shared__ unsigned tile_s;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (threadIdx.x == 0) tile_s = atomicAdd(tile_ctr, 1u);
+    for (int d = threadIdx.x; d < 256 * RS_WARPS; d += RS_THREADS) (&wcnt[0][0])[d] = 0;
+    __syncthreads();
+    const unsigned tile = tile_s;
+    const int64_t tbase = (int64_t)tile * RS_TILE;
+    const int tn = (int)min((int64_t)RS_TILE, n - tbase);
+    const int64_t t0 = tbase + (int64_t)w * (RS_ITEMS * 32);
+    uint64_t k[RS_ITEMS];
+    int32_t v[RS_ITEMS];
+    uint32_t rank[RS_ITEMS];
+    const unsigned lt = (1u << lane) - 1u;
+#pragma unroll
+    for (int r = 0; r < RS_ITEMS; r++) {
+        const int64_t idx = t0 + r * 32 + lane;
+        const bool ok = idx < n;
+        k[r] = ok ? key[idx] : 0;
+        if (PAIRS) v[r] = ok ? val[idx] : 0;
+    }
+#pragma unroll
+    for (int r = 0; r < RS_ITEMS; r++) {
+        const bool ok = t0 + r * 32 + lane < n;
+        const uint32_t d = ok ? (uint32_t)((k[r] >> shift) & 255) : 256u;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t before = d < 256 ? wcnt[w][d] : 0;
+        rank[r] = before + __popc(peers & lt);
+        __syncwarp();
+        if (d < 256 && lane == __ffs(peers) - 1) wcnt[w][d] = before + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+    const int d = threadIdx.x;
+    uint32_t tot = 0;
+#pragma unroll
+    for (int ww = 0; ww < RS_WARPS; ww++) {
+        const uint32_t c = wcnt[ww][d];
+        wcnt[ww][d] = tot;
+        tot += c;
+    }
+    unsigned long long *st = status + (size_t)tile * 256;
+    st_relaxed_u64(st + d, (tile == 0 ? OS_PREFIX : OS_AGG) | tot);
+    // block scans over the digits: tile-local starts, and the pass's global starts
+    const uint32_t g = ghist[d];
+    uint32_t xt = tot, xg = g;
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t yt = __shfl_up_sync(0xffffffffu, xt, o), yg = __shfl_up_sync(0xffffffffu, xg, o);
+        if (lane >= o) {
+            xt += yt;
+            xg += yg;
+        }
+    }
+    if (lane == 31) {
+        wsum[0][w] = xt;
+        wsum[1][w] = xg;
+    }
+    uint32_t excl = 0;
+    if (tile > 0) {  // decoupled look-back, eight predecessors per step
+        long long j = (long long)tile - 1, polls = 0;
+        bool found = false;
+        while (!found) {
+            unsigned long long sv[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                sv[q] = j - q >= 0 ? ld_relaxed_u64(status + (size_t)(j - q) * 256 + d) : OS_PREFIX;
+            int stop = 8;
+#pragma unroll
+            for (int q = 0; q < 8; q++) {
+                if (found || q >= stop) continue;
+                const unsigned long long f = sv[q] & ~OS_VAL;
+                if (f == 0) {
+                    stop = q;  // not yet published: read again from there
+                } else {
+                    excl += (uint32_t)(sv[q] & OS_VAL);
+                    found = f == OS_PREFIX;
+                }
+            }
+            if (found) break;
+            j -= stop;
+            if (stop < 8 && ++polls > limit) {
+                atomicOr(err, 1ull);
+                break;
+            }
+        }
+        st_relaxed_u64(st + d, OS_PREFIX | (excl + tot));
+    }
+    __syncthreads();
+    uint32_t wt = 0, wg = 0;
+    for (int i = 0; i < w; i++) {
+        wt += wsum[0][i];
+        wg += wsum[1][i];
+    }
+    const uint32_t ts = wt + xt - tot;
+    tstart[d] = ts;
+    dbase[d] = wg + xg - g + excl - ts;  // global position = dbase[digit] + tile-local index
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < RS_ITEMS; r++) {
+        if (t0 + r * 32 + lane < n) {
+            const uint32_t dd = (uint32_t)((k[r] >> shift) & 255);
+            const uint32_t li = tstart[dd] + wcnt[w][dd] + rank[r];
+            skey[li] = k[r];
+            if (PAIRS) sval[li] = v[r];
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < tn; i += RS_THREADS) {
+        const uint64_t kk = skey[i];
+        const uint32_t pos = dbase[(uint32_t)((kk >> shift) & 255)] + (uint32_t)i;
+        okey[pos] = kk;
+        if (PAIRS) oval[pos] = sval[i];
+    }
+}
+
+// Sort by the 8-bit digits at the given shifts (ascending), stable.
+static void os_run(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_tmp, int64_t n, const int *shifts,
+                   int npass, kifmm_plan *P, bool pairs) {
+    if (n <= 1 || npass == 0) return;
     KIFMM_REQUIRE(n < (1ll << 31), KIFMM_ERR_ARG, "radix sort: more than 2^31 keys");
-    int nb = (int)((n + RS_TILE - 1) / RS_TILE);
-    P->sort_hist.alloc((size_t)256 * nb + 256);
-    int passes = (bits + 7) / 8;
+    KIFMM_REQUIRE(npass <= OS_MAX_PASSES, KIFMM_ERR_ARG, "radix sort: too many passes");
+    cudaStream_t s = P->stream;
+    const int64_t ntiles = (n + RS_TILE - 1) / RS_TILE;
+    OsShifts sh{};
+    sh.n = npass;
+    for (int p = 0; p < npass; p++) sh.s[p] = shifts[p];
+    // scratch: digit counts [npass][256], tile counters [npass], look-back status
+    // [npass][ntiles][256] (one pass's worth, cleared before each pass, when large)
+    const size_t per_pass = (size_t)ntiles * 256;
+    const bool all_at_once = (size_t)npass * per_pass * 8 <= ((size_t)64 << 20);
+    const size_t nstat = all_at_once ? (size_t)npass * per_pass : per_pass;
+    P->sort_hist.alloc((size_t)npass * 256 + npass);
+    P->sort_status.alloc(nstat);
+    uint32_t *hist = P->sort_hist.p;
+    unsigned *ctr = P->sort_hist.p + (size_t)npass * 256;
+    KIFMM_CUDA(cudaMemsetAsync(hist, 0, ((size_t)npass * 256 + npass) * sizeof(uint32_t), s));
+    KIFMM_CUDA(cudaMemsetAsync(P->sort_status.p, 0, nstat * sizeof(unsigned long long), s));
+    const unsigned hg = (unsigned)std::min<int64_t>(ntiles, (int64_t)P->num_sms * 4);
+    k_os_hist<<<hg, RS_THREADS, 0, s>>>(key, n, sh, hist);
+    KIFMM_LAUNCHED();
     uint64_t *ka = key, *kb = key_tmp;
     int32_t *va = val, *vb = val_tmp;
-    for (int p = 0; p < passes; p++) {
-        int shift = lo_bit + 8 * p;
-        k_rs_hist<<<nb, RS_THREADS, 0, P->stream>>>(ka, n, shift, P->sort_hist.p, nb);
+    unsigned long long *err = P->scal.p + KIFMM_SCAL_SORT_ERR;
+    for (int p = 0; p < npass; p++) {
+        unsigned long long *stat = P->sort_status.p + (all_at_once ? (size_t)p * per_pass : 0);
+        if (!all_at_once && p > 0)
+            KIFMM_CUDA(cudaMemsetAsync(stat, 0, per_pass * sizeof(unsigned long long), s));
+        if (pairs) {
+            ensure_dyn_smem(k_os_pass<true>, OS_PASS_SMEM);
+            k_os_pass<true><<<(unsigned)ntiles, RS_THREADS, OS_PASS_SMEM, s>>>(ka, va, kb, vb, n, sh.s[p], hist + 256 * p,
+                                                                               stat, ctr + p, err, 1ll << 20);
+        } else {
+            ensure_dyn_smem(k_os_pass<false>, OS_PASS_SMEM);
+            k_os_pass<false><<<(unsigned)ntiles, RS_THREADS, OS_PASS_SMEM, s>>>(ka, nullptr, kb, nullptr, n, sh.s[p],
+                                                                                hist + 256 * p, stat, ctr + p, err,
+                                                                                1ll << 20);
+        }
         KIFMM_LAUNCHED();
-        k_rs_scan<<<256, 256, 0, P->stream>>>(P->sort_hist.p, nb);
-        KIFMM_LAUNCHED();
-        if (pairs)
-            k_rs_scatter<true><<<nb, RS_THREADS, 0, P->stream>>>(ka, va, kb, vb, n, shift, P->sort_hist.p, nb);
-        else
-            k_rs_scatter<false><<<nb, RS_THREADS, 0, P->stream>>>(ka, nullptr, kb, nullptr, n, shift,
-                                                                  P->sort_hist.p, nb);
-        KIFMM_LAUNCHED();
-        uint64_t *tk = ka; ka = kb; kb = tk;
-        int32_t *tv = va; va = vb; vb = tv;
+        std::swap(ka, kb);
+        std::swap(va, vb);
     }
     if (ka != key) {
-        KIFMM_CUDA(cudaMemcpyAsync(key, ka, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, P->stream));
-        if (pairs) KIFMM_CUDA(cudaMemcpyAsync(val, va, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, P->stream));
+        KIFMM_CUDA(cudaMemcpyAsync(key, ka, n * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+        if (pairs) KIFMM_CUDA(cudaMemcpyAsync(val, va, n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s));
     }
+}
+
+static void rs_run(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_tmp, int64_t n, int bits,
+                   kifmm_plan *P, bool pairs, int lo_bit = 0) {
+    int shifts[OS_MAX_PASSES];
+    const int passes = (bits + 7) / 8;
+    for (int p = 0; p < passes; p++) shifts[p] = lo_bit + 8 * p;
+    os_run(key, val, key_tmp, val_tmp, n, shifts, passes, P, pairs);
 }
 
 void radix_sort_pairs(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_tmp, int64_t n, int bits,
@@ -169,6 +392,13 @@ void radix_sort_pairs_bits(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32
 
 void radix_sort_keys(uint64_t *key, uint64_t *key_tmp, int64_t n, int bits, kifmm_plan *P) {
     rs_run(key, nullptr, key_tmp, nullptr, n, bits, P, false);
+}
+
+// keys sorted by the digits at `shifts` only: the caller knows the other
+// digits are equal for every key
+void radix_sort_keys_shifts(uint64_t *key, uint64_t *key_tmp, int64_t n, const int *shifts, int npass,
+                            kifmm_plan *P) {
+    os_run(key, nullptr, key_tmp, nullptr, n, shifts, npass, P, false);
 }
 
 int64_t radix_sort_hist_words(int64_t n) { return (int64_t)256 * ((n + RS_TILE - 1) / RS_TILE) + 256; }

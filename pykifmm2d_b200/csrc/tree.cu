@@ -600,7 +600,17 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     P->key2.alloc(std::max<int64_t>(n, n_ent));
     if (n_ent) {
         KIFMM_CUDA(cudaMemcpyAsync(P->ent.p, P->list.p, n_ent * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
-        radix_sort_keys(P->ent.p, P->key2.p, n_ent, ENT_LEVEL_SHIFT + 5, P);
+        // entry = (level << 57) | (key << 1) | xlist with keys of at most 2(L-1)
+        // bits: sort the digits holding key bits, then the level digit
+        int shifts[8], np = 0;
+        for (int sh = 0; sh <= 2 * (L - 1); sh += 8) shifts[np++] = sh;
+        if (8 * np > 56) {
+            np = 0;
+            for (int sh = 0; sh < 64; sh += 8) shifts[np++] = sh;
+        } else {
+            shifts[np++] = 56;
+        }
+        radix_sort_keys_shifts(P->ent.p, P->key2.p, n_ent, shifts, np, P);
     }
     // per-level entry counts -> level table
     P->misc.alloc(64);
@@ -652,9 +662,11 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
                                                               P->list_tiles.p, P->leaf_list.p, P->p2m_list.p);
         KIFMM_LAUNCHED();
     }
-    unsigned long long c5[5];
+    unsigned long long c5[5], sort_err = 0;
     KIFMM_CUDA(cudaMemcpyAsync(c5, cnt, sizeof(c5), cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaMemcpyAsync(&sort_err, P->scal.p + KIFMM_SCAL_SORT_ERR, sizeof(sort_err), cudaMemcpyDeviceToHost, s));
     KIFMM_CUDA(cudaStreamSynchronize(s));
+    KIFMM_REQUIRE(sort_err == 0, KIFMM_ERR_CUDA, "build_tree: a radix-sort look-back wait timed out");
     P->n_leaf_list = (int64_t)c5[0];
     P->n_p2m_list = (int64_t)c5[1];
     P->n_leaves = (int64_t)c5[2];
