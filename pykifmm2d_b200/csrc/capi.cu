@@ -70,6 +70,15 @@ void ensure_dyn_smem(const void *fn, size_t bytes) {
     cur = bytes;
 }
 
+cudaStream_t device_side_stream(int device) {
+    static std::mutex mu;
+    static cudaStream_t side[64] = {};
+    KIFMM_REQUIRE(device >= 0 && device < 64, KIFMM_ERR_ARG, "device index out of range");
+    std::lock_guard<std::mutex> lock(mu);
+    if (!side[device]) KIFMM_CUDA(cudaStreamCreateWithFlags(&side[device], cudaStreamNonBlocking));
+    return side[device];
+}
+
 void set_error(const std::string &msg) { g_last_error = msg; }
 
 template <class F>
@@ -222,7 +231,9 @@ int kifmm_precompute(kifmm_plan *P) {
         KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
         use_device(P);
         PhaseScope ph(P, KIFMM_PHASE_PRECOMPUTE);
-        build_operators(P);
+        KIFMM_REQUIRE(P->have_tree, KIFMM_ERR_STATE, "precompute: build_tree first");
+        if (P->ops_pending) join_operators(P);  // started by build_tree
+        else build_operators(P);
     });
 }
 
@@ -316,10 +327,16 @@ int kifmm_plan_destroy(kifmm_plan *P) {
         g_stream = P->stream;
         for (auto &ph : P->pending) { cudaEventDestroy(ph.a); cudaEventDestroy(ph.b); }
         P->pending.clear();
-        cudaStream_t s = P->stream;
+        cudaStream_t s = P->stream, side = P->side;
+        cudaEvent_t e0 = P->ops_fork, e1 = P->ops_done;
         bool own = P->own_stream;
-        delete P;  // buffers are freed stream-ordered on s
+        delete P;  // buffers are freed stream-ordered on s and on the side stream
         if (s) cudaStreamSynchronize(s);
+        if (side) {  // the device's shared side stream stays
+            cudaStreamSynchronize(side);
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+        }
         if (own && s) cudaStreamDestroy(s);
     });
 }

@@ -139,6 +139,12 @@ struct kifmm_plan {
     kifmm_options opt{};
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    // operator construction runs on a side stream of the plan while the tree
+    // build continues (it needs only the root width and the depth); the main
+    // stream waits on ops_done before the operators are used
+    cudaStream_t side = nullptr;
+    cudaEvent_t ops_fork = nullptr, ops_done = nullptr;
+    bool ops_pending = false;
     int device = 0;
     int num_sms = 148;
 
@@ -326,6 +332,9 @@ void export_tree(kifmm_plan *P, int64_t *nodes, int64_t *point_leaf);
 void tree_stats(kifmm_plan *P);
 // operators.cu
 void build_operators(kifmm_plan *P);
+void start_operators(kifmm_plan *P);  // build_operators on the side stream
+cudaStream_t device_side_stream(int device);  // one per device, created on first use
+void join_operators(kifmm_plan *P);   // main stream waits for it
 // passes.cu
 void run_upward_downward(kifmm_plan *P);
 void run_eval_sources(kifmm_plan *P, int check_self);

@@ -260,7 +260,7 @@ __global__ void k_to_float(const double *__restrict__ a, float *__restrict__ b, 
 }
 
 void build_operators(kifmm_plan *P) {
-    KIFMM_REQUIRE(P->have_tree, KIFMM_ERR_STATE, "precompute: build_tree first");
+    KIFMM_REQUIRE(P->L >= 1 && P->W >= 0, KIFMM_ERR_STATE, "precompute: build_tree first");
     const int L = P->L, Q = P->Q;
     cudaStream_t s = P->stream;
     OpsArgs A{};
@@ -317,6 +317,47 @@ void build_operators(kifmm_plan *P) {
             KIFMM_LAUNCHED();
         }
     }
+    P->have_ops = true;
+}
+
+// The operators depend on the kernel, Nequiv, the radii, the root width and the
+// number of levels only, so build_tree starts them as soon as the depth is
+// known, on the plan's side stream; the rest of the tree build (restriction,
+// X-list, entry sort, node tables, with their host round trips) runs meanwhile.
+// Buffers allocated here belong to the side stream, which is ordered after all
+// earlier work of the main stream, the earlier users of those buffers.  The
+// side stream is one per device, shared by all plans (kept until exit), so that
+// operator memory freed by one plan is reused by the next in stream order.
+void start_operators(kifmm_plan *P) {
+    if (!P->side) {
+        P->side = device_side_stream(P->device);
+        KIFMM_CUDA(cudaEventCreateWithFlags(&P->ops_fork, cudaEventDisableTiming));
+        KIFMM_CUDA(cudaEventCreateWithFlags(&P->ops_done, cudaEventDisableTiming));
+    }
+    KIFMM_CUDA(cudaEventRecord(P->ops_fork, P->stream));
+    KIFMM_CUDA(cudaStreamWaitEvent(P->side, P->ops_fork, 0));
+    struct Swap {  // launches and allocations go to the side stream meanwhile
+        kifmm_plan *P;
+        cudaStream_t main, g;
+        Swap(kifmm_plan *p) : P(p), main(p->stream), g(g_stream) {
+            P->stream = P->side;
+            g_stream = P->side;
+        }
+        ~Swap() {
+            P->stream = main;
+            g_stream = g;
+        }
+    } sw(P);
+    build_operators(P);
+    P->have_ops = false;  // usable once joined
+    KIFMM_CUDA(cudaEventRecord(P->ops_done, P->side));
+    P->ops_pending = true;
+}
+
+void join_operators(kifmm_plan *P) {
+    if (!P->ops_pending) return;
+    KIFMM_CUDA(cudaStreamWaitEvent(P->stream, P->ops_done, 0));
+    P->ops_pending = false;
     P->have_ops = true;
 }
 

@@ -561,6 +561,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     KIFMM_REQUIRE(L <= MAX_LEVELS, KIFMM_ERR_DEPTH, "build_tree: too many levels");
     P->L = L;
     uint64_t t0count = st[0];
+    start_operators(P);  // overlaps the rest of the tree build
 
     int64_t n_ent = 0;
     if (L > 1) {
