@@ -407,9 +407,35 @@ def run_ours(args, cfg, rank, world, dist):
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
+    if args.serve_requests > 0:
+        line["serving"] = run_serving(args, dev)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, x, y, tau, repeats=3)
     return line
+
+
+# ------------------------------------------------------- serving stream
+def run_serving(args, device):
+    """Mixed-size request stream through pykifmm2d_b200.serving: first all
+    requests at once (closed system) to measure capacity, then the same
+    requests with Poisson arrivals at 70% of that rate; latency per request =
+    completion - arrival (tree build, operators, every density's host->device
+    copy, graph replay and device->host copy)."""
+    from pykifmm2d_b200 import serving as S
+    srv = S.Server(device=device, slots=args.serve_slots, keep_pots=False)
+    srv.run(S.make_stream(4, 0.0, seed=99, nmax=20_000, applies=(2, 2)), realtime=False)  # warm-up
+    _, cap = srv.run(S.make_stream(args.serve_requests, 0.0, seed=0), realtime=False)
+    rate = 0.7 * cap["requests_per_s"]
+    _, st = srv.run(S.make_stream(args.serve_requests, rate, seed=0), realtime=True)
+    return {
+        "requests": st["requests"], "failed": st["failed"] + cap["failed"],
+        "mix": "70% Laplace / 30% K0 (k in {1,10,50}), N log-uniform in [1e3, 3e5] (mixture + circle points), "
+               "8-32 densities per request, Nequiv 32, Ncutoff 64, mixed precision",
+        "capacity_requests_per_s": cap["requests_per_s"], "offered_requests_per_s": rate, "offered_load": 0.7,
+        "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+        "point_applies_per_s": st["point_applies_per_s"], "wall_s": st["wall_s"],
+        "slots": st["slots"], "hbm_budget_bytes": st["hbm_budget_bytes"],
+    }
 
 
 # ------------------------------------------------------- CPU baseline
@@ -482,6 +508,9 @@ def main():
     ap.add_argument("--profile-run", action="store_true",
                     help="only the timed pipeline steps (for ncu launch lists); prints phase times")
     ap.add_argument("--n", type=int, default=0, help="override the number of points (profiling small cases)")
+    ap.add_argument("--serve-requests", type=int, default=1024,
+                    help="requests in the serving stream (0 skips it)")
+    ap.add_argument("--serve-slots", type=int, default=8, help="concurrent requests in the serving stream")
     args = ap.parse_args()
     cfg = dict(CONFIGS[args.config])
     if args.n:

@@ -137,8 +137,23 @@ int kifmm_evaluate_to_sources(kifmm_plan *plan, double *pot, int32_t check_self,
 int kifmm_evaluate_to_points(kifmm_plan *plan, const double *x, const double *y, int64_t n,
                              int32_t check_self, double *pot, int32_t mem);
 
-/* Wait for all work queued on the plan's stream. */
+/* Wait for all work queued on the plan's stream, then report device-side
+ * failures (a bounded wait in a kernel that ran out) as KIFMM_ERR_CUDA. */
 int kifmm_synchronize(kifmm_plan *plan);
+
+/* Repeated densities on one tree as one CUDA graph: the reference applies a
+ * planned FMM to a new density with FMM.build_expansions(tau) followed by
+ * FMM.evaluate_to_points(x, y, check_self) at the sources (class_fmm.py:299-352,
+ * 379-399).  kifmm_graph_capture runs that pair once on the device pointers
+ * tau_dev -> pot_dev (a normal apply, which allocates the plan's apply buffers),
+ * then captures the same pair into a graph owned by the plan.
+ * kifmm_graph_launch replays it on the plan's stream: it reads tau_dev as it is
+ * when the replay runs and writes pot_dev; no host synchronisation, no
+ * allocation.  The plan's stream must be a created stream (capture is not
+ * possible on the legacy default stream).  build_tree or precompute on the plan
+ * drops the graph.  Check results with kifmm_synchronize. */
+int kifmm_graph_capture(kifmm_plan *plan, const double *tau_dev, double *pot_dev, int32_t check_self);
+int kifmm_graph_launch(kifmm_plan *plan);
 
 /* Tree statistics (reference Tree.levels, Level.n_node, ...). */
 int kifmm_get_tree_info(kifmm_plan *plan, kifmm_tree_info *info);

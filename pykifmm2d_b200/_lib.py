@@ -58,6 +58,8 @@ _SIGS = {
     "kifmm_evaluate_to_sources": (_i32, [_vp, _vp, _i32, _i32]),
     "kifmm_evaluate_to_points": (_i32, [_vp, _vp, _vp, _i64, _i32, _vp, _i32]),
     "kifmm_synchronize": (_i32, [_vp]),
+    "kifmm_graph_capture": (_i32, [_vp, _vp, _vp, _i32]),
+    "kifmm_graph_launch": (_i32, [_vp]),
     "kifmm_get_tree_info": (_i32, [_vp, ctypes.POINTER(TreeInfo)]),
     "kifmm_export_tree": (_i32, [_vp, _vp, _vp]),
     "kifmm_plan_destroy": (_i32, [_vp]),

@@ -328,6 +328,27 @@ class FMM(object):
     def synchronize(self):
         B.check(self._lib.kifmm_synchronize(self._plan))
 
+    def capture_apply(self, tau_dev, pot_dev, check_self=True):
+        """Planned repeated evaluation at the sources (the reference's
+        build_expansions(tau) + evaluate_to_points(x, y, check_self) per density,
+        class_fmm.py:299-399) as a CUDA graph: runs the pair once from the CUDA
+        tensor tau_dev into pot_dev, then keeps it captured; ``replay`` runs it
+        again on whatever tau_dev holds.  Needs a plan on a created stream."""
+        if not self._have_ops:
+            self.precompute()
+        import torch
+        for t in (tau_dev, pot_dev):
+            if not (_is_torch(t) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+                raise ValueError("capture_apply needs contiguous float64 CUDA tensors (the graph keeps their addresses)")
+        p_t, p_o = tau_dev.data_ptr(), pot_dev.data_ptr()
+        if _numel(tau_dev) != self.N or _numel(pot_dev) != self.N:
+            raise ValueError("tau_dev and pot_dev must have one value per source point")
+        B.check(self._lib.kifmm_graph_capture(self._plan, p_t, p_o, int(bool(check_self))))
+
+    def replay(self):
+        """One graph launch of the captured apply (asynchronous on the plan's stream)."""
+        B.check(self._lib.kifmm_graph_launch(self._plan))
+
     def __del__(self):
         h = getattr(self, "_plan", None)
         if h is not None and h.value:

@@ -216,8 +216,14 @@ int kifmm_plan_create(const kifmm_kernel *kernel, int32_t nequiv, int32_t ncutof
     });
 }
 
+static void drop_graph(kifmm_plan *P) {
+    if (P->graph) cudaGraphExecDestroy(P->graph);
+    P->graph = nullptr;
+}
+
 int kifmm_build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int32_t mem) {
     return guarded([&] {
+        if (P) drop_graph(P);
         KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
         KIFMM_REQUIRE(mem == KIFMM_MEM_HOST || mem == KIFMM_MEM_DEVICE, KIFMM_ERR_ARG, "bad mem flag");
         use_device(P);
@@ -232,6 +238,7 @@ int kifmm_precompute(kifmm_plan *P) {
         use_device(P);
         PhaseScope ph(P, KIFMM_PHASE_PRECOMPUTE);
         KIFMM_REQUIRE(P->have_tree, KIFMM_ERR_STATE, "precompute: build_tree first");
+        drop_graph(P);
         if (P->ops_pending) join_operators(P);  // started by build_tree
         else build_operators(P);
     });
@@ -288,6 +295,63 @@ int kifmm_synchronize(kifmm_plan *P) {
     });
 }
 
+// One apply on device pointers, no host synchronisation: what the graph holds.
+static void apply_device(kifmm_plan *P, const double *tau, double *pot, bool check_self) {
+    P->tau.alloc(P->N);
+    KIFMM_CUDA(cudaMemcpyAsync(P->tau.p, tau, P->N * sizeof(double), cudaMemcpyDeviceToDevice, P->stream));
+    run_upward_downward(P);
+    run_eval_sources(P, check_self);
+    KIFMM_CUDA(cudaMemcpyAsync(pot, P->pot_out.p, P->N * sizeof(double), cudaMemcpyDeviceToDevice, P->stream));
+}
+
+int kifmm_graph_capture(kifmm_plan *P, const double *tau, double *pot, int32_t check_self) {
+    return guarded([&] {
+        KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
+        KIFMM_REQUIRE(tau && pot, KIFMM_ERR_ARG, "null device pointer");
+        KIFMM_REQUIRE(P->have_ops, KIFMM_ERR_STATE, "graph capture: call precompute first");
+        KIFMM_REQUIRE(P->stream && P->stream != cudaStreamLegacy && P->stream != cudaStreamPerThread,
+                      KIFMM_ERR_ARG, "graph capture: the plan needs a created stream, not a default stream");
+        use_device(P);
+        drop_graph(P);
+        const bool prof = P->profiling;
+        P->profiling = false;  // no timer events inside the graph
+        struct Restore {
+            kifmm_plan *P;
+            bool prof;
+            ~Restore() { P->profiling = prof; }
+        } restore{P, prof};
+        apply_device(P, tau, pot, check_self != 0);  // allocates; sets kernel attributes
+        P->have_expansions = true;
+        KIFMM_CUDA(cudaStreamSynchronize(P->stream));
+        check_device_flags(P);
+        KIFMM_CUDA(cudaStreamBeginCapture(P->stream, cudaStreamCaptureModeThreadLocal));
+        cudaGraph_t g = nullptr;
+        try {
+            apply_device(P, tau, pot, check_self != 0);
+        } catch (...) {
+            cudaStreamEndCapture(P->stream, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        KIFMM_CUDA(cudaStreamEndCapture(P->stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&P->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            P->graph = nullptr;
+            KIFMM_CUDA(e);
+        }
+    });
+}
+
+int kifmm_graph_launch(kifmm_plan *P) {
+    return guarded([&] {
+        KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
+        KIFMM_REQUIRE(P->graph, KIFMM_ERR_STATE, "graph launch: call kifmm_graph_capture first");
+        use_device(P);
+        KIFMM_CUDA(cudaGraphLaunch(P->graph, P->stream));
+    });
+}
+
 int kifmm_get_tree_info(kifmm_plan *P, kifmm_tree_info *info) {
     return guarded([&] {
         KIFMM_REQUIRE(P && info, KIFMM_ERR_ARG, "null argument");
@@ -325,6 +389,7 @@ int kifmm_plan_destroy(kifmm_plan *P) {
         if (!P) return;
         cudaSetDevice(P->device);
         g_stream = P->stream;
+        drop_graph(P);
         for (auto &ph : P->pending) { cudaEventDestroy(ph.a); cudaEventDestroy(ph.b); }
         P->pending.clear();
         cudaStream_t s = P->stream, side = P->side;

@@ -145,6 +145,7 @@ struct kifmm_plan {
     cudaStream_t side = nullptr;
     cudaEvent_t ops_fork = nullptr, ops_done = nullptr;
     bool ops_pending = false;
+    cudaGraphExec_t graph = nullptr;  // captured apply (kifmm_graph_capture)
     int device = 0;
     int num_sms = 148;
 
