@@ -9,7 +9,9 @@
 // with C_d = CM2LS_d . blockdiag(Inv) (4Q x 4Q, FP64, operators.cu).  As a
 // GEMM: D[rows, targets] = A[rows, 8 x 4Q] . B[targets, 8 x 4Q]^T where B's
 // columns are gathered per target from its eight neighbour groups.  A CTA
-// owns TC_N = 64 targets and one 128-row M tile; per direction (and per
+// owns TC_N = 32 targets and one 128-row M tile (its five int8 accumulators
+// fit a 256-column TMEM allocation and its tiles 101 KB of shared memory, so
+// two CTAs share an SM and one's copies overlap the other's MMAs); per direction (and per
 // K chunk of 128) it stages A and B in shared memory in the UMMA K-major,
 // no-swizzle layout, one thread issues the MMA chain, tcgen05.commit signals
 // an mbarrier, and the epilogue reads TMEM with tcgen05.ld.
@@ -37,14 +39,18 @@ namespace kifmm {
 
 enum TcForm { TC_INT8 = 0, TC_BF16 = 1, TC_FP16 = 2 };
 template <int F> struct TcTraits;
-template <> struct TcTraits<TC_INT8> { static constexpr int NS = 5, EB = 1, KSTEP = 32, NACC = 5, NCOLS = 512; };
-template <> struct TcTraits<TC_BF16> { static constexpr int NS = 2, EB = 2, KSTEP = 16, NACC = 1, NCOLS = 64; };
-template <> struct TcTraits<TC_FP16> { static constexpr int NS = 2, EB = 2, KSTEP = 16, NACC = 1, NCOLS = 64; };
+template <> struct TcTraits<TC_INT8> { static constexpr int NS = 5, EB = 1, KSTEP = 32, NACC = 5, NCOLS = 256; };
+template <> struct TcTraits<TC_BF16> { static constexpr int NS = 2, EB = 2, KSTEP = 16, NACC = 1, NCOLS = 32; };
+template <> struct TcTraits<TC_FP16> { static constexpr int NS = 2, EB = 2, KSTEP = 16, NACC = 1, NCOLS = 32; };
 
 constexpr int TC_M = 128;      // MMA M: operator rows per tile (TMEM lanes)
-constexpr int TC_N = 64;       // MMA N: target groups per CTA
+constexpr int TC_N = 32;       // MMA N: target groups per CTA
 constexpr int TC_KC = 128;     // K elements staged per step
 constexpr int TC_THREADS = 128;
+static_assert(TC_N % 16 == 0 && TC_N >= 16 && TC_N <= 256, "MMA N for M = 128");
+static_assert(TcTraits<TC_INT8>::NACC * TC_N <= TcTraits<TC_INT8>::NCOLS, "int8 accumulators exceed the TMEM allocation");
+static_assert(TcTraits<TC_BF16>::NACC * TC_N <= TcTraits<TC_BF16>::NCOLS, "accumulator exceeds the TMEM allocation");
+static_assert(2 * TcTraits<TC_INT8>::NCOLS <= 512, "two CTAs per SM must fit the 512 TMEM columns");
 constexpr double FP16_PRESCALE = 4096.0;
 
 struct TcGeom {
@@ -274,14 +280,14 @@ struct TcArgs {
 };
 
 template <int F>
-__global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(TcArgs T) {
+__global__ void __launch_bounds__(TC_THREADS, 2) k_m2l_tc(TcArgs T) {
     using TR = TcTraits<F>;
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const PassArgs &A = T.A;
     const int Q = A.Q, Q4 = T.g.Q4, KP = T.pre.KP;
     const size_t a_sb = T.g.slice_bytes;                       // A slice (128 x KC)
-    const size_t b_sb = (size_t)TC_N * TC_KC * TR::EB;         // B slice (64 x KC)
+    const size_t b_sb = (size_t)TC_N * TC_KC * TR::EB;         // B slice (TC_N x KC)
     unsigned char *sA = tc_smem;
     unsigned char *sB = sA + TR::NS * a_sb;
     int *sgrp = (int *)(sB + TR::NS * b_sb);                   // [TC_N][9]
