@@ -315,6 +315,10 @@ void build_operators(kifmm_plan *P) {
             ensure_dyn_smem(k_ops_taylor, tsm);
             k_ops_taylor<<<L, 256, tsm, s>>>(A, P->l2p_taylor.p, KIFMM_TAYLOR_P);
             KIFMM_LAUNCHED();
+            P->l2p_taylor_f.alloc((size_t)L * Q * R);
+            k_to_float<<<grid_for((size_t)L * Q * R, 256, 1024), 256, 0, s>>>(P->l2p_taylor.p, P->l2p_taylor_f.p,
+                                                                             (size_t)L * Q * R);
+            KIFMM_LAUNCHED();
         }
     }
     P->have_ops = true;

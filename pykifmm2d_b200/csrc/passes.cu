@@ -277,6 +277,7 @@ PassArgs make_pass_args(kifmm_plan *P) {
     A.uup = P->uup.p;
     A.udown = P->udown.p;
     A.taylor = P->l2p_taylor.p;
+    A.taylor_f = P->l2p_taylor_f.p;
     return A;
 }
 

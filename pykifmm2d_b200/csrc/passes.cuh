@@ -22,6 +22,7 @@ struct PassArgs {
     double *pots;
     double *uup, *udown;
     const double *taylor;  // Laplace L2P coefficients map, or null
+    const float *taylor_f;  // FP32 copy of it (the orders computed in FP32)
 };
 
 // Node centre, exactly the reference's xmid = xmin + w/2 (tree.py:339-346):

@@ -156,6 +156,7 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, 6) k_leaf_eval_f(PassArgs A, 
     constexpr float CLAMP = 1.17549435e-38f;  // FLT_MIN
     __shared__ float4 srcs[LEAF_WARPS][LEAF_CHUNK + 32];
     __shared__ double qds[LEAF_WARPS][R > 64 ? R : 64];
+    __shared__ float qfs[LEAF_WARPS][R > 64 ? R : 64];
     __shared__ double red[LEAF_WARPS][32];
     __shared__ float redf[LEAF_WARPS][32];
     __shared__ int rngs[LEAF_WARPS][18];
@@ -169,27 +170,36 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, 6) k_leaf_eval_f(PassArgs A, 
     const bool lap = KIND == KIFMM_KERNEL_LAPLACE;
     const bool taylor = lap && A.taylor != nullptr && l >= 2;
     double *qd = qds[wib];
+    float *qf = qfs[wib];
     float4 *src = srcs[wib];
     const double width = ldexp(A.W, -l);
     const double sc = lap ? 1.0 / width : 1.0;     // coordinate scale
     const double lw = lap ? -2.0 * log2(sc) : 0.0; // log2 of the squared length unit
-    if (taylor) {  // Taylor coefficients of the local expansion (FP64), NR independent rows per lane
-        constexpr int NR = (R + 31) / 32;
+    if (taylor) {
+        // Taylor coefficients of the local expansion: rows 0..31 (orders j <= 16)
+        // in FP64, rows 32.. (j >= 16, weighted by at most (|z|/rho)^16 ~ 2e-4
+        // where they are used) in FP32, each lane four independent rows
+        static_assert(R > 96 && R <= 128, "row groups below assume 96 < 2p+1 <= 128");
         const double *T = A.taylor + (size_t)l * A.Q * R + lane;
+        const float *Tf = A.taylor_f + (size_t)l * A.Q * R + lane;
         const double *u = A.udown + (size_t)g * A.Q;
-        double cs[NR];
-#pragma unroll
-        for (int i = 0; i < NR; i++) cs[i] = 0.0;
-#pragma unroll 2
+        double c0 = 0.0;
+        float c1 = 0.f, c2 = 0.f, c3 = 0.f;
+        const bool r3 = lane + 96 < R;
+#pragma unroll 4
         for (int c = 0; c < A.Q; c++) {
             const double uc = u[c];
-#pragma unroll
-            for (int i = 0; i < NR; i++)
-                if (lane + 32 * i < R) cs[i] = fma(T[(size_t)c * R + 32 * i], uc, cs[i]);
+            const float ucf = (float)uc;
+            c0 = fma(T[(size_t)c * R], uc, c0);
+            c1 = fmaf(Tf[(size_t)c * R + 32], ucf, c1);
+            c2 = fmaf(Tf[(size_t)c * R + 64], ucf, c2);
+            if (r3) c3 = fmaf(Tf[(size_t)c * R + 96], ucf, c3);
         }
-#pragma unroll
-        for (int i = 0; i < NR; i++)
-            if (lane + 32 * i < R) qd[lane + 32 * i] = cs[i];
+        qd[lane] = c0;
+        qf[lane + 32] = c1;
+        qf[lane + 64] = c2;
+        if (r3) qf[lane + 96] = c3;
+        if (lane == 0) qd[32] = (double)c1;  // Im c_16, used by the FP64 part of the Horner sum
     } else {
         local_density(A, g, l, qd, lane);
     }
@@ -345,8 +355,17 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, 6) k_leaf_eval_f(PassArgs A, 
             if (l >= 2) {
                 const double zx = pxd * sc, zy = pyd * sc;
                 if (taylor && zx * zx + zy * zy <= 0.5625) {
-                    double sr = qd[R - 2], si = qd[R - 1];
-                    for (int jj = KIFMM_TAYLOR_P - 1; jj >= 1; jj--) {
+                    // Horner: orders P..17 in FP32, then 16..1 in FP64
+                    const float zxf = (float)zx, zyf = (float)zy;
+                    float fr = qf[R - 2], fi = qf[R - 1];
+                    for (int jj = KIFMM_TAYLOR_P - 1; jj >= 17; jj--) {
+                        const float nr = fmaf(fr, zxf, fmaf(-fi, zyf, qf[2 * jj - 1]));
+                        const float ni = fmaf(fr, zyf, fmaf(fi, zxf, qf[2 * jj]));
+                        fr = nr;
+                        fi = ni;
+                    }
+                    double sr = fr, si = fi;
+                    for (int jj = 16; jj >= 1; jj--) {
                         double nr = fma(sr, zx, fma(-si, zy, qd[2 * jj - 1]));
                         double ni = fma(sr, zy, fma(si, zx, qd[2 * jj]));
                         sr = nr;
