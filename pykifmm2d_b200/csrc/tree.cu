@@ -33,11 +33,23 @@ __device__ __forceinline__ uint64_t ordered_bits(double v) {
     uint64_t u = (uint64_t)__double_as_longlong(v);
     return (u >> 63) ? ~u : (u | 0x8000000000000000ull);
 }
-static double from_ordered(uint64_t o) {
+__host__ __device__ inline double from_ordered(uint64_t o) {
     uint64_t u = (o >> 63) ? (o & 0x7fffffffffffffffull) : ~o;
     double d;
     memcpy(&d, &u, 8);
     return d;
+}
+
+// Root box from the ordered extremes in scal[0..3] (tree.py:475-484, with the
+// reference's ymax = y.min() unless fix_bbox): m = floor(min(xmin, ymin)),
+// M = ceil(max(xmax, ytop)).  Computed the same way on the device (k_keys_dev)
+// and on the host once the counts come back.
+__host__ __device__ inline void root_box(const unsigned long long *sc, int fix_bbox, double &m, double &M) {
+    const double xmn = from_ordered(sc[0]), xmx = from_ordered(sc[1]), ymn = from_ordered(sc[2]),
+                 ymx = from_ordered(sc[3]);
+    const double ytop = fix_bbox ? ymx : ymn;
+    m = floor(fmin(xmn, ymn));
+    M = ceil(fmax(xmx, ytop));
 }
 
 // scal[0..3]: ordered min x, max x, min y, max y; scal[4]: non-finite count
@@ -93,6 +105,29 @@ __global__ void k_keys(const double *__restrict__ x, const double *__restrict__ 
     if ((threadIdx.x & 31) == 0 && out) atomicAdd(outside, out);
 }
 
+// k_keys with the root box read from the device (no host round trip after
+// k_bbox).  Inputs that the host will reject (non-finite coordinates, |m| or
+// |M| >= 2^23) get key 0 here; the host reports them at its next read-back.
+__global__ void k_keys_dev(const double *__restrict__ x, const double *__restrict__ y, int64_t n, int fix_bbox,
+                           const unsigned long long *__restrict__ scal, uint64_t *__restrict__ key,
+                           int32_t *__restrict__ perm, unsigned long long *outside) {
+    double m, M;
+    root_box(scal, fix_bbox, m, M);
+    const bool valid = scal[4] == 0 && fabs(m) < 8388608.0 && fabs(M) < 8388608.0;
+    const double h = (valid && M > m) ? ldexp(M - m, -KEY_DEPTH) : 0.0;
+    unsigned long long out = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double a = x[i], b = y[i];
+        uint64_t k = 0;
+        if (h > 0 && isfinite(a) && isfinite(b)) k = morton(grid_cell(a, m, h), grid_cell(b, m, h));
+        key[i] = k;
+        perm[i] = (int32_t)i;
+        out += (a < m || a > M || b < m || b > M);
+    }
+    for (int o = 16; o; o >>= 1) out += __shfl_xor_sync(0xffffffffu, out, o);
+    if ((threadIdx.x & 31) == 0 && out) atomicAdd(outside, out);
+}
+
 __global__ void k_gather2(const double *__restrict__ x, const double *__restrict__ y, const int32_t *__restrict__ perm,
                           int64_t n, double *__restrict__ xs, double *__restrict__ ys) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -123,6 +158,7 @@ struct HashSet {
     unsigned long long *count;  // entries appended to list
     unsigned long long *ovf;
     uint64_t cap;               // list capacity
+    unsigned long long *lcount; // [32] entries per level, counted as they are appended
 };
 
 __device__ __forceinline__ uint64_t ent_make(int l, uint64_t k, int x) {
@@ -135,8 +171,12 @@ __device__ void hs_insert(const HashSet &H, uint64_t e) {
         unsigned long long prev = atomicCAS(&H.tab[s], (unsigned long long)ENT_EMPTY, (unsigned long long)e);
         if (prev == ENT_EMPTY) {
             unsigned long long idx = atomicAdd(H.count, 1ull);
-            if (idx < H.cap) H.list[idx] = e;
-            else atomicOr(H.ovf, 1ull);
+            if (idx < H.cap) {
+                H.list[idx] = e;
+                atomicAdd(&H.lcount[(int)(e >> ENT_LEVEL_SHIFT)], 1ull);
+            } else {
+                atomicOr(H.ovf, 1ull);
+            }
             return;
         }
         if (prev == e) return;
@@ -161,6 +201,17 @@ __device__ bool hs_has(const HashSet &H, uint64_t e) {
 // more than ppl points iff l <= common_level(key[i], key[i+ppl]).
 // mode 0: count + deepest level; mode 1: insert.
 // scal[5]: count, scal[6]: deepest split level + 1, scal[7]: depth overflow
+// T0 split cells opened by sorted point i (mode 1 of k_t0)
+__device__ __forceinline__ void t0_insert(const uint64_t *__restrict__ key, int64_t n, int64_t ppl, const HashSet &H,
+                                          int64_t i) {
+    if (i + ppl >= n) return;
+    const uint64_t k = key[i];
+    int hi = common_level(k, key[i + ppl]);
+    if (hi >= KEY_DEPTH) hi = KEY_DEPTH - 1;
+    const int lo = i == 0 ? -1 : common_level(key[i - 1], k);
+    for (int l = lo + 1; l <= hi; l++) hs_insert(H, ent_make(l, k >> (2 * (KEY_DEPTH - l)), 0));
+}
+
 __global__ void k_t0(const uint64_t *__restrict__ key, int64_t n, int64_t ppl, int mode, HashSet H,
                      unsigned long long *scal) {
     unsigned long long cnt = 0;
@@ -195,52 +246,107 @@ __global__ void k_t0(const uint64_t *__restrict__ key, int64_t n, int64_t ppl, i
 }
 
 // Restriction step for level l: every split cell s of level l+1 forces the
-// 3x3 block around parent(s) to be split.  One thread per (cell, neighbour):
+// 3x3 block around parent(s) to be split.  One work item per (cell, neighbour):
 // the inserts are independent, so none waits on another's atomic.
-__global__ void k_restrict(HashSet H, int l) {
-    unsigned long long n = *((volatile unsigned long long *)H.count);
-    if (n > H.cap) n = H.cap;
+__device__ __forceinline__ void restrict_item(const HashSet &H, int l, int64_t j) {
+    const int64_t i = j / 9;
+    const int d = (int)(j - 9 * i);
+    const uint64_t e = H.list[i];
+    if ((int)(e >> ENT_LEVEL_SHIFT) != l + 1 || (e & 1)) return;
     const int64_t side = 1ll << l;
-    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < 9 * (int64_t)n;
-         j += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = j / 9;
-        const int d = (int)(j - 9 * i);
-        const uint64_t e = H.list[i];
-        if ((int)(e >> ENT_LEVEL_SHIFT) != l + 1 || (e & 1)) continue;
-        const uint64_t p = ((e >> 1) & KEY56) >> 2;
-        const int64_t qx = (int64_t)compact2(p >> 1) + d / 3 - 1, qy = (int64_t)compact2(p) + d % 3 - 1;
-        if (qx < 0 || qy < 0 || qx >= side || qy >= side) continue;
-        hs_insert(H, ent_make(l, morton((uint64_t)qx, (uint64_t)qy), 0));
-    }
+    const uint64_t p = ((e >> 1) & KEY56) >> 2;
+    const int64_t qx = (int64_t)compact2(p >> 1) + d / 3 - 1, qy = (int64_t)compact2(p) + d % 3 - 1;
+    if (qx < 0 || qy < 0 || qx >= side || qy >= side) return;
+    hs_insert(H, ent_make(l, morton((uint64_t)qx, (uint64_t)qy), 0));
 }
 
 // X-list: for levels 1..L-2, a real leaf (cell not split, parent split) next
-// to a split cell becomes an X-list cell.  One thread per (cell, neighbour).
-__global__ void k_xlist(HashSet H, int L) {
-    unsigned long long n = *((volatile unsigned long long *)H.count);
-    if (n > H.cap) n = H.cap;
-    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < 9 * (int64_t)n;
-         j += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t i = j / 9;
-        const int d = (int)(j - 9 * i);
-        if (d == 4) continue;
-        const uint64_t e = H.list[i];
-        const int l = (int)(e >> ENT_LEVEL_SHIFT);
-        if ((e & 1) || l < 1 || l > L - 2) continue;
-        const uint64_t k = (e >> 1) & KEY56;
-        const int64_t cx = (int64_t)compact2(k >> 1) + d / 3 - 1, cy = (int64_t)compact2(k) + d % 3 - 1;
-        const int64_t side = 1ll << l;
-        if (cx < 0 || cy < 0 || cx >= side || cy >= side) continue;
-        const uint64_t c = morton((uint64_t)cx, (uint64_t)cy);
-        if (hs_has(H, ent_make(l, c, 0))) continue;
-        if (!hs_has(H, ent_make(l - 1, c >> 2, 0))) continue;
-        hs_insert(H, ent_make(l, c, 1));
-    }
+// to a split cell becomes an X-list cell.  One work item per (cell, neighbour).
+__device__ __forceinline__ void xlist_item(const HashSet &H, int L, int64_t j) {
+    const int64_t i = j / 9;
+    const int d = (int)(j - 9 * i);
+    if (d == 4) return;
+    const uint64_t e = H.list[i];
+    const int l = (int)(e >> ENT_LEVEL_SHIFT);
+    if ((e & 1) || l < 1 || l > L - 2) return;
+    const uint64_t k = (e >> 1) & KEY56;
+    const int64_t cx = (int64_t)compact2(k >> 1) + d / 3 - 1, cy = (int64_t)compact2(k) + d % 3 - 1;
+    const int64_t side = 1ll << l;
+    if (cx < 0 || cy < 0 || cx >= side || cy >= side) return;
+    const uint64_t c = morton((uint64_t)cx, (uint64_t)cy);
+    if (hs_has(H, ent_make(l, c, 0))) return;
+    if (!hs_has(H, ent_make(l - 1, c >> 2, 0))) return;
+    hs_insert(H, ent_make(l, c, 1));
 }
 
-__global__ void k_level_counts(const uint64_t *__restrict__ ent, int64_t n, unsigned long long *cnt) {
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        atomicAdd(&cnt[ent[i] >> ENT_LEVEL_SHIFT], 1ull);
+__device__ __forceinline__ unsigned long long hs_count(const HashSet &H) {
+    unsigned long long n = *((volatile unsigned long long *)H.count);
+    return n > H.cap ? H.cap : n;
+}
+
+__global__ void k_restrict(HashSet H, int l) {
+    const unsigned long long n = hs_count(H);
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < 9 * (int64_t)n;
+         j += (int64_t)gridDim.x * blockDim.x)
+        restrict_item(H, l, j);
+}
+
+__global__ void k_xlist(HashSet H, int L) {
+    const unsigned long long n = hs_count(H);
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < 9 * (int64_t)n;
+         j += (int64_t)gridDim.x * blockDim.x)
+        xlist_item(H, L, j);
+}
+
+// Grid-wide barrier for a cooperative launch: bar[0] arrivals, bar[1]
+// generation.  A wait that runs past `limit` polls returns false.
+__device__ bool grid_barrier(unsigned *bar, long long limit) {
+    __shared__ int ok_s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned *gen = bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        int ok = 1;
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            for (long long it = 0; *gen == g; it++)
+                if (it > limit) {
+                    ok = 0;
+                    break;
+                }
+        }
+        __threadfence();
+        ok_s = ok;
+    }
+    __syncthreads();
+    return ok_s != 0;
+}
+
+// The whole split-cell set in one cooperative launch: T0 inserts, the
+// restriction closure from level L-3 up to 0 (a grid barrier between levels,
+// as each level reads the cells the level below added), then the X-list.
+// Fourteen launches and their gaps become fifteen barriers.
+__global__ void __launch_bounds__(256) k_split_closure(const uint64_t *__restrict__ key, int64_t n, int64_t ppl,
+                                                       HashSet H, int L, unsigned *bar, long long limit,
+                                                       unsigned long long *err) {
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t i = tid; i < n; i += stride) t0_insert(key, n, ppl, H, i);
+    bool ok = grid_barrier(bar, limit);
+    for (int l = L - 3; l >= 0 && ok; l--) {
+        const unsigned long long cnt = hs_count(H);
+        for (int64_t j = tid; j < 9 * (int64_t)cnt; j += stride) restrict_item(H, l, j);
+        ok = grid_barrier(bar, limit);
+    }
+    if (ok) {
+        const unsigned long long cnt = hs_count(H);
+        for (int64_t j = tid; j < 9 * (int64_t)cnt; j += stride) xlist_item(H, L, j);
+    } else if (threadIdx.x == 0) {
+        atomicOr(err, 1ull);
+    }
 }
 
 // ----------------------------------------------------------- node arrays
@@ -511,22 +617,9 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     unsigned gs = grid_for(n, TB, P->num_sms * 8);
     k_bbox<<<gs, TB, 0, s>>>(P->x.p, P->y.p, n, P->scal.p);
     KIFMM_LAUNCHED();
-    unsigned long long sc[5];
-    KIFMM_CUDA(cudaMemcpyAsync(sc, P->scal.p, sizeof(sc), cudaMemcpyDeviceToHost, s));
-    KIFMM_CUDA(cudaStreamSynchronize(s));
-    KIFMM_REQUIRE(sc[4] == 0, KIFMM_ERR_ARG, "build_tree: non-finite coordinates");
-    double xmn = from_ordered(sc[0]), xmx = from_ordered(sc[1]), ymn = from_ordered(sc[2]), ymx = from_ordered(sc[3]);
-    double ytop = P->opt.fix_bbox ? ymx : ymn;
-    double m = std::floor(std::min(xmn, ymn)), M = std::ceil(std::max(xmx, ytop));
-    KIFMM_REQUIRE(std::fabs(m) < 8388608.0 && std::fabs(M) < 8388608.0, KIFMM_ERR_RANGE,
-                  "build_tree: |coordinates| must stay below 2^23 for exact dyadic midpoints");
-    P->root_min = m; P->root_max = M; P->W = M - m;
-    KIFMM_REQUIRE(P->W > 0 || n <= P->ppl, KIFMM_ERR_DEPTH,
-                  "build_tree: more than Ncutoff points on one integer point (zero-width root box)");
-    double h = P->W > 0 ? std::ldexp(P->W, -KEY_DEPTH) : 0.0;
-
     P->pkey.alloc(n); P->perm.alloc(n); P->key2.alloc(n); P->perm2.alloc(n);
-    k_keys<<<gs, TB, 0, s>>>(P->x.p, P->y.p, n, m, M, h, P->pkey.p, P->perm.p, P->scal.p + 8);
+    // the root box stays on the device until the counts below come back
+    k_keys_dev<<<gs, TB, 0, s>>>(P->x.p, P->y.p, n, P->opt.fix_bbox, P->scal.p, P->pkey.p, P->perm.p, P->scal.p + 8);
     KIFMM_LAUNCHED();
     // Sort by the top 32 key bits first (levels 1..16, four 8-bit passes): that
     // orders every cell of level <= 16, enough whenever no split lies deeper
@@ -539,13 +632,24 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     HashSet H{};
     H.count = P->scal.p + 9;
     H.ovf = P->scal.p + 10;
-    unsigned long long st[4];
+    unsigned long long sc[9];  // [0..3] ordered extremes, [4] non-finite, [5..7] T0 count/depth/overflow, [8] outside
+    unsigned long long *st = sc + 5;
     for (int full = 0; full < 2; full++) {
         KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 5, 0, 3 * sizeof(unsigned long long), s));
         k_t0<<<gs, TB, 0, s>>>(P->pkey.p, n, P->ppl, 0, H, P->scal.p);
         KIFMM_LAUNCHED();
-        KIFMM_CUDA(cudaMemcpyAsync(st, P->scal.p + 5, sizeof(st), cudaMemcpyDeviceToHost, s));
+        KIFMM_CUDA(cudaMemcpyAsync(sc, P->scal.p, sizeof(sc), cudaMemcpyDeviceToHost, s));
         KIFMM_CUDA(cudaStreamSynchronize(s));
+        if (full == 0) {
+            KIFMM_REQUIRE(sc[4] == 0, KIFMM_ERR_ARG, "build_tree: non-finite coordinates");
+            double m, M;
+            root_box(sc, P->opt.fix_bbox, m, M);
+            KIFMM_REQUIRE(std::fabs(m) < 8388608.0 && std::fabs(M) < 8388608.0, KIFMM_ERR_RANGE,
+                          "build_tree: |coordinates| must stay below 2^23 for exact dyadic midpoints");
+            P->root_min = m; P->root_max = M; P->W = M - m;
+            KIFMM_REQUIRE(P->W > 0 || n <= P->ppl, KIFMM_ERR_DEPTH,
+                          "build_tree: more than Ncutoff points on one integer point (zero-width root box)");
+        }
         if (full || (st[1] <= (unsigned long long)FAST_LEVELS && st[2] == 0)) break;
         PhaseScope ph(P, KIFMM_PHASE_SORT);
         radix_sort_pairs(P->pkey.p, P->perm.p, P->key2.p, P->perm2.p, n, 2 * KEY_DEPTH, P);
@@ -564,7 +668,18 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     start_operators(P);  // overlaps the rest of the tree build
 
     int64_t n_ent = 0;
+    P->misc.alloc(64);
+    unsigned long long *lc = (unsigned long long *)P->misc.p;  // [32] entries per level
+    unsigned long long lcount[32] = {};
     if (L > 1) {
+        P->grid_bar.alloc(2);
+        static int coop_blocks[64] = {};  // co-resident blocks per SM of k_split_closure, per device
+        if (P->device >= 0 && P->device < 64 && coop_blocks[P->device] == 0) {
+            int nb = 0;
+            KIFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_split_closure, TB, 0));
+            coop_blocks[P->device] = std::max(1, std::min(nb, 4));
+        }
+        const unsigned cg = (unsigned)(coop_blocks[P->device] * P->num_sms);
         for (int attempt = 0;; attempt++) {
             uint64_t cap = (t0count * 16 + 4096) << (2 * attempt);
             uint64_t hcap = 1;
@@ -572,23 +687,31 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
             P->hash.alloc(hcap);
             P->list.alloc(cap);
             KIFMM_CUDA(cudaMemsetAsync(P->hash.p, 0xFF, hcap * sizeof(uint64_t), s));
-            KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 9, 0, 2 * sizeof(unsigned long long), s));
+            KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 9, 0, 3 * sizeof(unsigned long long), s));
+            KIFMM_CUDA(cudaMemsetAsync(lc, 0, 32 * sizeof(unsigned long long), s));
+            KIFMM_CUDA(cudaMemsetAsync(P->grid_bar.p, 0, 2 * sizeof(unsigned), s));
             H.tab = (unsigned long long *)P->hash.p;
             H.mask = hcap - 1;
             H.list = P->list.p;
             H.cap = cap;
-            k_t0<<<gs, TB, 0, s>>>(P->pkey.p, n, P->ppl, 1, H, P->scal.p);
-            KIFMM_LAUNCHED();
-            unsigned rg = (unsigned)(P->num_sms * 4);
-            for (int l = L - 3; l >= 0; l--) {
-                k_restrict<<<rg, TB, 0, s>>>(H, l);
+            H.lcount = lc;
+            {
+                const uint64_t *kp = P->pkey.p;
+                int64_t nn = n, ppl = P->ppl;
+                int LL = L;
+                unsigned *bar = P->grid_bar.p;
+                long long limit = 1ll << 22;
+                unsigned long long *err = P->scal.p + KIFMM_SCAL_TREE_ERR;
+                void *args[] = {(void *)&kp, (void *)&nn, (void *)&ppl, (void *)&H, (void *)&LL, (void *)&bar,
+                                (void *)&limit, (void *)&err};
+                KIFMM_CUDA(cudaLaunchCooperativeKernel((const void *)k_split_closure, cg, TB, args, 0, s));
                 KIFMM_LAUNCHED();
             }
-            k_xlist<<<rg, TB, 0, s>>>(H, L);
-            KIFMM_LAUNCHED();
-            unsigned long long cv[2];
+            unsigned long long cv[3];
             KIFMM_CUDA(cudaMemcpyAsync(cv, P->scal.p + 9, sizeof(cv), cudaMemcpyDeviceToHost, s));
+            KIFMM_CUDA(cudaMemcpyAsync(lcount, lc, sizeof(lcount), cudaMemcpyDeviceToHost, s));
             KIFMM_CUDA(cudaStreamSynchronize(s));
+            KIFMM_REQUIRE(cv[2] == 0, KIFMM_ERR_CUDA, "build_tree: a grid barrier wait timed out");
             if (cv[1] == 0 && cv[0] <= cap) {
                 n_ent = (int64_t)cv[0];
                 break;
@@ -613,17 +736,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
         }
         radix_sort_keys_shifts(P->ent.p, P->key2.p, n_ent, shifts, np, P);
     }
-    // per-level entry counts -> level table
-    P->misc.alloc(64);
-    unsigned long long *lc = (unsigned long long *)P->misc.p;
-    KIFMM_CUDA(cudaMemsetAsync(lc, 0, 32 * sizeof(unsigned long long), s));
-    if (n_ent) {
-        k_level_counts<<<grid_for(n_ent, TB, 1024), TB, 0, s>>>(P->ent.p, n_ent, lc);
-        KIFMM_LAUNCHED();
-    }
-    unsigned long long lcount[32];
-    KIFMM_CUDA(cudaMemcpyAsync(lcount, lc, sizeof(lcount), cudaMemcpyDeviceToHost, s));
-    KIFMM_CUDA(cudaStreamSynchronize(s));
+    // per-level entry counts (counted as the entries were added) -> level table
     LevelTable &T = P->lt;
     memset(&T, 0, sizeof(T));
     T.L = L;
