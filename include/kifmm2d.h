@@ -197,14 +197,15 @@ int kifmm_kernel_apply(const kifmm_kernel *kernel, const double *sx, const doubl
 enum {
     KIFMM_PHASE_TREE = 0,      /* whole build_tree */
     KIFMM_PHASE_SORT = 1,      /* Morton radix sort of the points (inside TREE) */
-    KIFMM_PHASE_PRECOMPUTE = 2,
+    KIFMM_PHASE_PRECOMPUTE = 2, /* wait for the operators (started by build_tree) */
     KIFMM_PHASE_P2M = 3,
     KIFMM_PHASE_M2M = 4,
     KIFMM_PHASE_M2L = 5,       /* M2L, all levels (with L2L where one kernel does both) */
     KIFMM_PHASE_LEAF = 6,      /* L2P + P2P at the sources */
     KIFMM_PHASE_TARGETS = 7,   /* locate + L2P + P2P at separate targets */
     KIFMM_PHASE_L2L = 8,       /* separate L2L chain (after the tensor-core M2L) */
-    KIFMM_PHASE_COUNT = 9
+    KIFMM_PHASE_OPERATORS = 9, /* operator construction on the side stream, overlapping TREE */
+    KIFMM_PHASE_COUNT = 10
 };
 int kifmm_set_profiling(kifmm_plan *plan, int32_t on);
 /* ms[KIFMM_PHASE_COUNT] and launches[KIFMM_PHASE_COUNT] (either may be NULL);

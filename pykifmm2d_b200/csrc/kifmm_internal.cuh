@@ -189,6 +189,7 @@ struct kifmm_plan {
     size_t ops_stride = 0;           // doubles per level block
     kifmm::DBuf<unsigned char> tc_a; // tensor-core M2L operator slices
     kifmm::DBuf<double> tc_rowscale;
+    kifmm::DBuf<unsigned long long> tc_rowmax;  // [L][4Q] largest |value| per M2L operator row
     kifmm::DBuf<double> l2p_taylor;  // Laplace: [L][Q][2p+1] check potential -> Taylor coefficients
     kifmm::DBuf<float> l2p_taylor_f;  // FP32 copy
     kifmm::DBuf<unsigned char> tc_pre;  // per-apply slices of the source groups

@@ -165,26 +165,8 @@ struct TcOpsArgs {
     TcGeom g;
     unsigned char *aslices;  // [L][9][MT][NKC][NS][slice]
     double *rowscale;        // [L][MP]
+    const unsigned long long *rowmax;  // [L][Q4] largest |value| per row (operators.cu, k_ops_assemble)
 };
-
-// row scales: block (level, 32 rows), thread (row, direction)
-__global__ void __launch_bounds__(256) k_tc_rowscale(TcOpsArgs T) {
-    __shared__ double part[8][32];
-    const int l = blockIdx.x, r = blockIdx.y * 32 + threadIdx.x % 32, dg = threadIdx.x / 32;
-    const int d = dg < 4 ? dg : dg + 1;  // the eight parent directions
-    const int Q4 = T.g.Q4;
-    double m = 0.0;
-    if (r < Q4 && l >= 2) {
-        const double *C = T.ops + (size_t)l * T.stride + T.off_m2l + (size_t)d * Q4 * Q4;
-        for (int c = 0; c < Q4; c++) m = fmax(m, fabs(C[(size_t)c * Q4 + r]));
-    }
-    part[dg][threadIdx.x % 32] = m;
-    __syncthreads();
-    if (threadIdx.x < 32 && r < T.g.MP) {
-        for (int i = 1; i < 8; i++) m = fmax(m, part[i][threadIdx.x]);
-        T.rowscale[(size_t)l * T.g.MP + r] = pow2_scale(m);
-    }
-}
 
 template <int F>
 __global__ void k_tc_slices(TcOpsArgs T) {
@@ -192,13 +174,19 @@ __global__ void k_tc_slices(TcOpsArgs T) {
     if (l < 2 || d == 4) return;
     const int Q4 = T.g.Q4;
     const double *C = T.ops + (size_t)l * T.stride + T.off_m2l + (size_t)d * Q4 * Q4;
-    const double *rs = T.rowscale + (size_t)l * T.g.MP;
     unsigned char *base = T.aslices + (size_t)l * T.g.level_bytes;
     const size_t sb = T.g.slice_bytes;
     const int total = T.g.MP * T.g.KP;
-    for (int e = threadIdx.x; e < total; e += blockDim.x) {
-        int r = e / T.g.KP, k = e % T.g.KP;
-        double v = (r < Q4 && k < Q4) ? C[(size_t)k * Q4 + r] / rs[r] : 0.0;
+    // row scale: the power of two above the row's largest |value| over all
+    // directions (1 for padding rows); multiplying by its reciprocal is exact
+    auto scale_of = [&](int r) {
+        return r < Q4 ? pow2_scale(__longlong_as_double((long long)T.rowmax[(size_t)l * Q4 + r])) : 1.0;
+    };
+    if (d == 0 && blockIdx.z == 0)
+        for (int r = threadIdx.x; r < T.g.MP; r += blockDim.x) T.rowscale[(size_t)l * T.g.MP + r] = scale_of(r);
+    for (int e = blockIdx.z * blockDim.x + threadIdx.x; e < total; e += gridDim.z * blockDim.x) {
+        int r = e % T.g.MP, k = e / T.g.MP;
+        double v = (r < Q4 && k < Q4) ? C[(size_t)k * Q4 + r] * (1.0 / scale_of(r)) : 0.0;
         int mt = r / TC_M, kc = k / TC_KC;
         unsigned char *tile = base + (((size_t)d * T.g.MT + mt) * T.g.NKC + kc) * TcTraits<F>::NS * sb;
         put_slices<F>(tile, sb, core_off(r % TC_M, k % TC_KC, TC_M, TcTraits<F>::EB), v);
@@ -476,9 +464,8 @@ static void build_tc_ops_t(kifmm_plan *P) {
     T.g = g;
     T.aslices = P->tc_a.p;
     T.rowscale = P->tc_rowscale.p;
-    k_tc_rowscale<<<dim3(P->L, g.MP / 32), 256, 0, P->stream>>>(T);
-    KIFMM_LAUNCHED();
-    k_tc_slices<F><<<dim3(P->L, 9), 256, 0, P->stream>>>(T);
+    T.rowmax = P->tc_rowmax.p;
+    k_tc_slices<F><<<dim3(P->L, 9, 8), 256, 0, P->stream>>>(T);
     KIFMM_LAUNCHED();
 }
 

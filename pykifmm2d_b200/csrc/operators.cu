@@ -28,8 +28,6 @@ struct OpsArgs {
     double rf1, rf2;
     size_t stride;          // doubles per level block
     double *ops;            // level blocks
-    double *m2ls;           // temp [L][49][Q][Q] (row-major r, t)
-    double *m2mc;           // temp [L][Q][4Q] (row-major)
     double *poff;           // temp [L][49][Q][Q] = M2LS . Inv (row-major)
 };
 
@@ -44,104 +42,72 @@ __host__ __device__ inline size_t ops_stride(int Q) { return ((size_t)153 * Q * 
 
 __device__ __forceinline__ double lvl_width(const OpsArgs &A, int l) { return ldexp(A.W, -l); }
 
-__global__ void k_ops_surfaces(OpsArgs A) {
-    int l = blockIdx.x, q = threadIdx.x;
-    if (l >= A.L || q >= A.Q) return;
-    double w = lvl_width(A, l);
-    double r1 = 0.5 * w * A.rf1, r2 = 0.5 * w * A.rf2;
-    double th = q * (2.0 * 3.141592653589793 / A.Q);
-    double c = cos(th), s = sin(th);
-    double *b = A.ops + (size_t)l * A.stride;
-    b[off_large(A.Q) + q] = r2 * c;
-    b[off_large(A.Q) + A.Q + q] = r2 * s;
-    b[off_small(A.Q) + q] = r1 * c;
-    b[off_small(A.Q) + A.Q + q] = r1 * s;
-}
-
 __device__ __forceinline__ double gval(const OpsArgs &A, double sx, double sy, double tx, double ty) {
     double dx = tx - sx, dy = ty - sy;
     return green_d(A.kind, A.k, dx * dx + dy * dy);
 }
 
-// Gauss-Jordan with partial pivoting on [E2C | I] for one level per block.
+// Gauss-Jordan with partial pivoting on [E2C | I], one warp per level: lane r
+// owns row r of the augmented matrix (rows of 2Q+1 doubles in shared memory,
+// conflict-free), so a pivot step needs warp synchronisation only.  Rows
+// beyond 32 are taken by the same lanes in turn.  Per element the arithmetic
+// is the block-wide form's: a[k][c] /= pivot, a[r][c] -= a[r][k] * a[k][c].
 __global__ void k_ops_inverse(OpsArgs A) {
     extern __shared__ double sm[];
-    const int Q = A.Q, Q2 = 2 * Q, l = blockIdx.x;
-    if (l < 1 || l >= A.L) return;
-    double *a = sm;                 // Q x 2Q
-    double *fac = sm + Q * Q2;      // Q
-    __shared__ int piv;
+    const int Q = A.Q, Q2 = 2 * Q, ld = Q2 + 1, l = blockIdx.x, lane = threadIdx.x;
+    if (l >= A.L) return;
+    {  // the level's circles (get_level_information, class_fmm.py:35-45)
+        const double w = lvl_width(A, l), r1 = 0.5 * w * A.rf1, r2 = 0.5 * w * A.rf2;
+        double *bw = A.ops + (size_t)l * A.stride;
+        for (int q = lane; q < Q; q += 32) {
+            const double th = q * (2.0 * 3.141592653589793 / Q);
+            const double c = cos(th), s = sin(th);
+            bw[off_large(Q) + q] = r2 * c;
+            bw[off_large(Q) + Q + q] = r2 * s;
+            bw[off_small(Q) + q] = r1 * c;
+            bw[off_small(Q) + Q + q] = r1 * s;
+        }
+        __syncwarp();
+    }
+    if (l < 1) return;
+    double *a = sm;  // Q x ld
     const double *b = A.ops + (size_t)l * A.stride;
     const double *lx = b + off_large(Q), *ly = lx + Q, *sx = b + off_small(Q), *sy = sx + Q;
-    for (int e = threadIdx.x; e < Q * Q2; e += blockDim.x) {
+    for (int e = lane; e < Q * Q2; e += 32) {
         int r = e / Q2, c = e % Q2;
-        a[e] = c < Q ? gval(A, sx[c], sy[c], lx[r], ly[r]) : (c - Q == r ? 1.0 : 0.0);
+        a[r * ld + c] = c < Q ? gval(A, sx[c], sy[c], lx[r], ly[r]) : (c - Q == r ? 1.0 : 0.0);
     }
-    __syncthreads();
+    __syncwarp();
     for (int k = 0; k < Q; k++) {
-        if (threadIdx.x < 32) {
-            double best = -1.0;
-            int bi = k;
-            for (int i = k + threadIdx.x; i < Q; i += 32) {
-                double v = fabs(a[i * Q2 + k]);
-                if (v > best) { best = v; bi = i; }
-            }
-            for (int o = 16; o; o >>= 1) {
-                double ob = __shfl_xor_sync(0xffffffffu, best, o);
-                int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-            }
-            if (threadIdx.x == 0) piv = bi;
+        double best = -1.0;
+        int bi = k;
+        for (int i = k + lane; i < Q; i += 32) {
+            double v = fabs(a[i * ld + k]);
+            if (v > best) { best = v; bi = i; }
         }
-        __syncthreads();
-        int p = piv;
+        for (int o = 16; o; o >>= 1) {
+            double ob = __shfl_xor_sync(0xffffffffu, best, o);
+            int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+            if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+        }
+        const int p = bi;
         if (p != k)
-            for (int c = threadIdx.x; c < Q2; c += blockDim.x) {
-                double t = a[k * Q2 + c]; a[k * Q2 + c] = a[p * Q2 + c]; a[p * Q2 + c] = t;
+            for (int c = lane; c < Q2; c += 32) {
+                double t = a[k * ld + c]; a[k * ld + c] = a[p * ld + c]; a[p * ld + c] = t;
             }
-        __syncthreads();
-        double pv = a[k * Q2 + k];
-        for (int i = threadIdx.x; i < Q; i += blockDim.x) fac[i] = a[i * Q2 + k];
-        __syncthreads();
-        for (int c = threadIdx.x; c < Q2; c += blockDim.x) a[k * Q2 + c] /= pv;
-        __syncthreads();
-        for (int e = threadIdx.x; e < Q * Q2; e += blockDim.x) {
-            int r = e / Q2, c = e % Q2;
-            if (r != k) a[e] -= fac[r] * a[k * Q2 + c];
+        __syncwarp();
+        const double pv = a[k * ld + k];
+        for (int c = lane; c < Q2; c += 32) a[k * ld + c] /= pv;
+        __syncwarp();
+        for (int r = lane; r < Q; r += 32) {
+            if (r == k) continue;
+            const double f = a[r * ld + k];
+            for (int c = 0; c < Q2; c++) a[r * ld + c] -= f * a[k * ld + c];
         }
-        __syncthreads();
+        __syncwarp();
     }
     double *inv = A.ops + (size_t)l * A.stride + off_inv(Q);  // row-major
-    for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) inv[e] = a[(e / Q) * Q2 + Q + e % Q];
-}
-
-// kernel matrices: M2LS (far offsets) and M2MC, one block per (level, slot)
-__global__ void k_ops_kmats(OpsArgs A) {
-    const int Q = A.Q, l = blockIdx.x, slot = blockIdx.y;  // slot 0..48: M2LS offset, 49: M2MC
-    if (l < 1 || l >= A.L) return;
-    const double *b = A.ops + (size_t)l * A.stride;
-    const double *sx = b + off_small(Q), *sy = sx + Q, *lx = b + off_large(Q), *ly = lx + Q;
-    double w = lvl_width(A, l);
-    if (slot < 49) {
-        int ox = slot / 7 - 3, oy = slot % 7 - 3;
-        if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1) return;
-        double *m = A.m2ls + ((size_t)l * 49 + slot) * Q * Q;
-        for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) {
-            int r = e / Q, t = e % Q;
-            m[e] = gval(A, sx[t] + ox * w, sy[t] + oy * w, sx[r], sy[r]);
-        }
-    } else {
-        if (l + 1 >= A.L) return;
-        const double *b1 = A.ops + (size_t)(l + 1) * A.stride;
-        const double *cx = b1 + off_small(Q), *cy = cx + Q;
-        double hw = 0.5 * lvl_width(A, l + 1);
-        double *m = A.m2mc + (size_t)l * Q * 4 * Q;
-        for (int e = threadIdx.x; e < Q * 4 * Q; e += blockDim.x) {
-            int r = e / (4 * Q), c = e % (4 * Q), qc = c / Q, t = c % Q;
-            double ox = (qc >= 2) ? hw : -hw, oy = (qc & 1) ? hw : -hw;
-            m[e] = gval(A, cx[t] + ox, cy[t] + oy, lx[r], ly[r]);
-        }
-    }
+    for (int e = lane; e < Q * Q; e += 32) inv[e] = a[(e / Q) * ld + Q + e % Q];
 }
 
 // P_o = M2LS_o . Inv_l (far offsets), M2M and L2L compositions; the inverse
@@ -160,12 +126,24 @@ __global__ void k_ops_compose(OpsArgs A) {
     double *iv = sm_c;              // [Q][Q]
     double *mm = sm_c + Q * Q;      // M2LS block [Q][Q] or M2MC [Q][4Q]
     for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) iv[e] = inv[e];
-    if (slot < 49) {
-        const double *m = A.m2ls + ((size_t)l * 49 + slot) * Q * Q;
-        for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) mm[e] = m[e];
-    } else {
-        const double *m = A.m2mc + (size_t)l * Q * 4 * Q;
-        for (int e = threadIdx.x; e < 4 * Q * Q; e += blockDim.x) mm[e] = m[e];
+    // the kernel-matrix block, evaluated here (class_fmm.py:219-250)
+    const double *sx = b + off_small(Q), *sy = sx + Q, *lx = b + off_large(Q), *ly = lx + Q;
+    if (slot < 49) {  // M2LS_o[r][t] = G(small_t + o w -> small_r)
+        const int ox = slot / 7 - 3, oy = slot % 7 - 3;
+        const double w = lvl_width(A, l);
+        for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) {
+            const int r = e / Q, t = e % Q;
+            mm[e] = gval(A, sx[t] + ox * w, sy[t] + oy * w, sx[r], sy[r]);
+        }
+    } else {  // M2MC_l[r][q Q + t] = G(small_{l+1, t} + child offset q -> large_r)
+        const double *b1 = A.ops + (size_t)(l + 1) * A.stride;
+        const double *cx = b1 + off_small(Q), *cy = cx + Q;
+        const double hw = 0.5 * lvl_width(A, l + 1);
+        for (int e = threadIdx.x; e < Q * 4 * Q; e += blockDim.x) {
+            const int r = e / (4 * Q), c = e % (4 * Q), qc = c / Q, t = c % Q;
+            const double ox = (qc >= 2) ? hw : -hw, oy = (qc & 1) ? hw : -hw;
+            mm[e] = gval(A, cx[t] + ox, cy[t] + oy, lx[r], ly[r]);
+        }
     }
     __syncthreads();
     if (slot < 49) {
@@ -198,11 +176,16 @@ __global__ void k_ops_compose(OpsArgs A) {
 // directional M2L blocks: for parent direction d = (dx+1)*3 + (dy+1), target
 // child a = 2ii+jj and source child b = 2iii+jjj sit at offset
 // 2(dx,dy) - (ii,jj) + (iii,jjj) (class_fmm.py:263-283); near offsets are zero.
-__global__ void k_ops_assemble(OpsArgs A) {
+// rowmax (or null): per (level, row), the largest |value| over all directions
+// and columns (bit pattern of a non-negative double, max by atomicMax), for
+// the tensor-core M2L's row scales.
+__global__ void k_ops_assemble(OpsArgs A, unsigned long long *rowmax) {
     const int Q = A.Q, Q4 = 4 * Q, l = blockIdx.x, d = blockIdx.y;
     if (l < 1 || l >= A.L || d == 4) return;
     int dx = d / 3 - 1, dy = d % 3 - 1;
     double *o = A.ops + (size_t)l * A.stride + off_m2l(Q) + (size_t)d * Q4 * Q4;
+    int cur = -1;
+    double mx = 0.0;
     for (int e = threadIdx.x; e < Q4 * Q4; e += blockDim.x) {
         int c = e / Q4, r = e % Q4;       // column-major element (r, c)
         int ta = r / Q, rr = r % Q, sb = c / Q, cc = c % Q;
@@ -213,7 +196,16 @@ __global__ void k_ops_assemble(OpsArgs A) {
             v = A.poff[((size_t)l * 49 + slot) * Q * Q + rr * Q + cc];
         }
         o[e] = v;
+        if (rowmax) {
+            if (r != cur) {
+                if (cur >= 0) atomicMax(&rowmax[(size_t)l * Q4 + cur], (unsigned long long)__double_as_longlong(mx));
+                cur = r;
+                mx = 0.0;
+            }
+            mx = fmax(mx, fabs(v));
+        }
     }
+    if (rowmax && cur >= 0) atomicMax(&rowmax[(size_t)l * Q4 + cur], (unsigned long long)__double_as_longlong(mx));
 }
 
 // Laplace local expansion as a Taylor series about the box centre.  With
@@ -222,18 +214,15 @@ __global__ void k_ops_assemble(OpsArgs A) {
 //   a0 = -(log r2 / 2pi) sum_k q_k,  c_j = (rho^-j / (2 pi j)) sum_k q_k e^(-i j theta_k),
 // valid for |z~| < rho.  taylor_l [(2p+1) rows][Q cols] (column-major) maps the
 // downward check potential to (a0, Re c_1, Im c_1, ...) through q = Inv_l u.
-__global__ void k_ops_taylor(OpsArgs A, double *taylor, int p) {
-    extern __shared__ double sm_t[];
-    const int Q = A.Q, l = blockIdx.x, R = 2 * p + 1;
-    if (l < 1 || l >= A.L) return;
-    double *C = sm_t;            // [R][Q]
-    double *iv = sm_t + R * Q;   // [Q][Q]
+__global__ void k_ops_taylor(OpsArgs A, double *taylor, float *taylor_f, int p) {
+    // one block per (level, row): thread k forms C[row][k], thread c the output
+    __shared__ double Crow[256];
+    const int Q = A.Q, l = blockIdx.x, row = blockIdx.y, R = 2 * p + 1;
+    if (l < 1 || l >= A.L || row >= R) return;
     const double *inv = A.ops + (size_t)l * A.stride + off_inv(Q);
     const double w = lvl_width(A, l), r2 = 0.5 * w * A.rf2, rho = r2 / w;
     const double twopi = 2.0 * 3.141592653589793;
-    for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) iv[e] = inv[e];
-    for (int e = threadIdx.x; e < R * Q; e += blockDim.x) {
-        int row = e / Q, k = e % Q;
+    for (int k = threadIdx.x; k < Q; k += blockDim.x) {
         double v;
         if (row == 0) {
             v = -log(r2) / twopi;
@@ -243,14 +232,14 @@ __global__ void k_ops_taylor(OpsArgs A, double *taylor, int p) {
             double f = pow(rho, -(double)j) / (twopi * j);
             v = (row & 1) ? f * cos(th) : -f * sin(th);
         }
-        C[e] = v;
+        Crow[k] = v;
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < R * Q; e += blockDim.x) {
-        int row = e % R, c = e / R;
+    for (int c = threadIdx.x; c < Q; c += blockDim.x) {
         double acc = 0.0;
-        for (int k = 0; k < Q; k++) acc = fma(C[row * Q + k], iv[k * Q + c], acc);
+        for (int k = 0; k < Q; k++) acc = fma(Crow[k], inv[k * Q + c], acc);
         taylor[((size_t)l * Q + c) * R + row] = acc;
+        if (taylor_f) taylor_f[((size_t)l * Q + c) * R + row] = (float)acc;
     }
 }
 
@@ -274,10 +263,8 @@ void build_operators(kifmm_plan *P) {
     A.ops = P->ops.p;
     DBuf<double> &tmp = P->ops_tmp;
     size_t n49 = (size_t)L * 49 * Q * Q;
-    tmp.alloc(2 * n49 + (size_t)L * 4 * Q * Q);
-    A.m2ls = tmp.p;
-    A.poff = tmp.p + n49;
-    A.m2mc = tmp.p + 2 * n49;
+    tmp.alloc(n49);
+    A.poff = tmp.p;
     for (int l = 0; l < L; l++) {
         double *b = P->ops.p + (size_t)l * A.stride;
         P->lops[l].inv = b + off_inv(Q);
@@ -287,37 +274,42 @@ void build_operators(kifmm_plan *P) {
         P->lops[l].large = b + off_large(Q);
         P->lops[l].small = b + off_small(Q);
     }
+    const bool mixed = P->opt.precision == KIFMM_PREC_MIXED;
+    const bool tc = mixed && uses_tensor_m2l(P) && L >= 3;
+    unsigned long long *rowmax = nullptr;
+    if (tc) {
+        P->tc_rowmax.alloc((size_t)L * 4 * Q);
+        rowmax = P->tc_rowmax.p;
+        KIFMM_CUDA(cudaMemsetAsync(rowmax, 0, (size_t)L * 4 * Q * sizeof(unsigned long long), s));
+    }
+    // circles + inverse, then kernel matrices composed with the inverses, then
+    // the directional M2L blocks (with the row maxima the tensor-core slices use)
+    size_t smem = (size_t)Q * (2 * Q + 1) * sizeof(double);
+    ensure_dyn_smem(k_ops_inverse, smem);
+    k_ops_inverse<<<L, 32, smem, s>>>(A);
+    KIFMM_LAUNCHED();
     if (L >= 2) {
-        k_ops_surfaces<<<L, Q, 0, s>>>(A);
-        KIFMM_LAUNCHED();
-        size_t smem = (size_t)Q * 2 * Q * sizeof(double) + Q * sizeof(double);
-        ensure_dyn_smem(k_ops_inverse, smem);
-        k_ops_inverse<<<L, 256, smem, s>>>(A);
-        KIFMM_LAUNCHED();
-        k_ops_kmats<<<dim3(L, 50), 256, 0, s>>>(A);
-        KIFMM_LAUNCHED();
         size_t csm = (size_t)5 * Q * Q * sizeof(double);
         ensure_dyn_smem(k_ops_compose, csm);
         k_ops_compose<<<dim3(L, 51), 256, csm, s>>>(A);
         KIFMM_LAUNCHED();
-        k_ops_assemble<<<dim3(L, 9), 256, 0, s>>>(A);
+        k_ops_assemble<<<dim3(L, 9), 256, 0, s>>>(A, rowmax);
         KIFMM_LAUNCHED();
     }
-    if (P->opt.precision == KIFMM_PREC_MIXED) {
-        P->ops_f.alloc(A.stride * (size_t)L);
-        k_to_float<<<grid_for(A.stride * L, 256, 4096), 256, 0, s>>>(P->ops.p, P->ops_f.p, A.stride * (size_t)L);
-        KIFMM_LAUNCHED();
-        if (uses_tensor_m2l(P) && L >= 3) build_tc_operators(P);
+    if (mixed) {
+        if (P->opt.m2l == KIFMM_M2L_FP32) {  // only the FP32 SIMT M2L reads FP32 operators
+            P->ops_f.alloc(A.stride * (size_t)L);
+            k_to_float<<<grid_for(A.stride * L, 256, 4096), 256, 0, s>>>(P->ops.p, P->ops_f.p, A.stride * (size_t)L);
+            KIFMM_LAUNCHED();
+        }
+        if (tc) build_tc_operators(P);
         if (P->kern.kind == KIFMM_KERNEL_LAPLACE && L >= 3) {
             const int R = 2 * KIFMM_TAYLOR_P + 1;
             P->l2p_taylor.alloc((size_t)L * Q * R);
-            size_t tsm = ((size_t)R * Q + (size_t)Q * Q) * sizeof(double);
-            ensure_dyn_smem(k_ops_taylor, tsm);
-            k_ops_taylor<<<L, 256, tsm, s>>>(A, P->l2p_taylor.p, KIFMM_TAYLOR_P);
-            KIFMM_LAUNCHED();
             P->l2p_taylor_f.alloc((size_t)L * Q * R);
-            k_to_float<<<grid_for((size_t)L * Q * R, 256, 1024), 256, 0, s>>>(P->l2p_taylor.p, P->l2p_taylor_f.p,
-                                                                             (size_t)L * Q * R);
+            KIFMM_REQUIRE(Q <= 256, KIFMM_ERR_ARG, "Nequiv above 256");
+            k_ops_taylor<<<dim3(L, R), ((Q + 31) / 32) * 32, 0, s>>>(A, P->l2p_taylor.p, P->l2p_taylor_f.p,
+                                                                    KIFMM_TAYLOR_P);
             KIFMM_LAUNCHED();
         }
     }
@@ -352,7 +344,10 @@ void start_operators(kifmm_plan *P) {
             g_stream = g;
         }
     } sw(P);
-    build_operators(P);
+    {
+        PhaseScope ph(P, KIFMM_PHASE_OPERATORS);  // events on the side stream
+        build_operators(P);
+    }
     P->have_ops = false;  // usable once joined
     KIFMM_CUDA(cudaEventRecord(P->ops_done, P->side));
     P->ops_pending = true;

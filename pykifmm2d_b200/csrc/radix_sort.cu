@@ -261,18 +261,39 @@ __global__ void __launch_bounds__(RS_THREADS) k_os_pass(const uint64_t *__restri
         wsum[0][w] = xt;
         wsum[1][w] = xg;
     }
+    __syncthreads();
+    uint32_t wt = 0, wg = 0;
+    for (int i = 0; i < w; i++) {
+        wt += wsum[0][i];
+        wg += wsum[1][i];
+    }
+    const uint32_t ts = wt + xt - tot;
+    tstart[d] = ts;
+    __syncthreads();
+    // the tile in digit order into shared memory, before the look-back, so
+    // that the look-back has the registers for wide batches
+#pragma unroll
+    for (int r = 0; r < RS_ITEMS; r++) {
+        if (t0 + r * 32 + lane < n) {
+            const uint32_t dd = (uint32_t)((k[r] >> shift) & 255);
+            const uint32_t li = tstart[dd] + wcnt[w][dd] + rank[r];
+            skey[li] = k[r];
+            if (PAIRS) sval[li] = v[r];
+        }
+    }
     uint32_t excl = 0;
-    if (tile > 0) {  // decoupled look-back, eight predecessors per step
+    if (tile > 0) {  // decoupled look-back, 32 predecessors per step
+        constexpr int LB = 32;
         long long j = (long long)tile - 1, polls = 0;
         bool found = false;
         while (!found) {
-            unsigned long long sv[8];
+            unsigned long long sv[LB];
 #pragma unroll
-            for (int q = 0; q < 8; q++)
+            for (int q = 0; q < LB; q++)
                 sv[q] = j - q >= 0 ? ld_relaxed_u64(status + (size_t)(j - q) * 256 + d) : OS_PREFIX;
-            int stop = 8;
+            int stop = LB;
 #pragma unroll
-            for (int q = 0; q < 8; q++) {
+            for (int q = 0; q < LB; q++) {
                 if (found || q >= stop) continue;
                 const unsigned long long f = sv[q] & ~OS_VAL;
                 if (f == 0) {
@@ -284,32 +305,14 @@ __global__ void __launch_bounds__(RS_THREADS) k_os_pass(const uint64_t *__restri
             }
             if (found) break;
             j -= stop;
-            if (stop < 8 && ++polls > limit) {
+            if (stop < LB && ++polls > limit) {
                 atomicOr(err, 1ull);
                 break;
             }
         }
         st_relaxed_u64(st + d, OS_PREFIX | (excl + tot));
     }
-    __syncthreads();
-    uint32_t wt = 0, wg = 0;
-    for (int i = 0; i < w; i++) {
-        wt += wsum[0][i];
-        wg += wsum[1][i];
-    }
-    const uint32_t ts = wt + xt - tot;
-    tstart[d] = ts;
     dbase[d] = wg + xg - g + excl - ts;  // global position = dbase[digit] + tile-local index
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < RS_ITEMS; r++) {
-        if (t0 + r * 32 + lane < n) {
-            const uint32_t dd = (uint32_t)((k[r] >> shift) & 255);
-            const uint32_t li = tstart[dd] + wcnt[w][dd] + rank[r];
-            skey[li] = k[r];
-            if (PAIRS) sval[li] = v[r];
-        }
-    }
     __syncthreads();
     for (int i = threadIdx.x; i < tn; i += RS_THREADS) {
         const uint64_t kk = skey[i];

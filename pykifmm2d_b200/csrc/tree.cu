@@ -665,7 +665,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     KIFMM_REQUIRE(L <= MAX_LEVELS, KIFMM_ERR_DEPTH, "build_tree: too many levels");
     P->L = L;
     uint64_t t0count = st[0];
-    start_operators(P);  // overlaps the rest of the tree build
+    bool ops_started = false;
 
     int64_t n_ent = 0;
     P->misc.alloc(64);
@@ -677,7 +677,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
         if (P->device >= 0 && P->device < 64 && coop_blocks[P->device] == 0) {
             int nb = 0;
             KIFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_split_closure, TB, 0));
-            coop_blocks[P->device] = std::max(1, std::min(nb, 4));
+            coop_blocks[P->device] = std::max(1, std::min(nb, 2));
         }
         const unsigned cg = (unsigned)(coop_blocks[P->device] * P->num_sms);
         for (int attempt = 0;; attempt++) {
@@ -707,6 +707,12 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
                 KIFMM_CUDA(cudaLaunchCooperativeKernel((const void *)k_split_closure, cg, TB, args, 0, s));
                 KIFMM_LAUNCHED();
             }
+            if (!ops_started) {
+                // the operators overlap the rest of the tree build; queued after the
+                // cooperative launch, which needs its blocks resident at once
+                start_operators(P);
+                ops_started = true;
+            }
             unsigned long long cv[3];
             KIFMM_CUDA(cudaMemcpyAsync(cv, P->scal.p + 9, sizeof(cv), cudaMemcpyDeviceToHost, s));
             KIFMM_CUDA(cudaMemcpyAsync(lcount, lc, sizeof(lcount), cudaMemcpyDeviceToHost, s));
@@ -719,6 +725,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
             KIFMM_REQUIRE(attempt < 4, KIFMM_ERR_NOMEM, "build_tree: split-cell set overflow");
         }
     }
+    if (!ops_started) start_operators(P);
     P->n_ent = n_ent;
     P->ent.alloc(n_ent);
     P->key2.alloc(std::max<int64_t>(n, n_ent));
