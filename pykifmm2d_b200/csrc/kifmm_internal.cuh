@@ -5,6 +5,7 @@
 
 #include <atomic>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "kifmm2d.h"  // include/ (on the include path)
@@ -217,6 +218,30 @@ struct kifmm_plan {
 
 namespace kifmm {
 // Brackets one phase with CUDA events on the plan's stream when profiling.
+// Programmatic dependent launch: a kernel launched with launch_pdl may be
+// scheduled while the previous kernel on the stream is still finishing; it
+// calls pdl_wait() before it reads anything that kernel wrote (the wait
+// returns once that grid has completed and its writes are visible), and
+// pdl_trigger() to let the next one be scheduled.  Without the attribute both
+// are no-ops.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    KIFMM_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...));
+    KIFMM_LAUNCHED();
+}
+
 // Raise a kernel's dynamic shared-memory limit to at least `bytes` on the
 // current device; the driver call is made once per (device, kernel, larger
 // size), not before every launch.

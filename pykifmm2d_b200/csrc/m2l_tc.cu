@@ -207,6 +207,8 @@ struct TcPre {
 template <int F>
 __global__ void k_tc_preslice(PassArgs A, int64_t n_ent, TcPre T) {
     using TR = TcTraits<F>;
+    pdl_trigger();
+    pdl_wait();
     const int lane = threadIdx.x & 31;
     int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (j >= n_ent) return;
@@ -271,6 +273,8 @@ template <int F>
 __global__ void __launch_bounds__(TC_THREADS, 2) k_m2l_tc(TcArgs T) {
     using TR = TcTraits<F>;
     extern __shared__ __align__(1024) unsigned char tc_smem[];
+    pdl_trigger();
+    pdl_wait();
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const PassArgs &A = T.A;
     const int Q = A.Q, Q4 = T.g.Q4, KP = T.pre.KP;
@@ -489,8 +493,7 @@ static void run_m2l_tensor_t(kifmm_plan *P, const PassArgs &A) {
     P->tc_gexp.alloc(P->n_ent);
     pre.slices = P->tc_pre.p;
     pre.gexp = P->tc_gexp.p;
-    k_tc_preslice<F><<<grid_for(P->n_ent * 32, 256), 256, 0, P->stream>>>(A, P->n_ent, pre);
-    KIFMM_LAUNCHED();
+    launch_pdl(k_tc_preslice<F>, dim3(grid_for(P->n_ent * 32, 256)), dim3(256), 0, P->stream, A, P->n_ent, pre);
     TcArgs T{};
     T.A = A;
     T.g = g;
@@ -509,8 +512,7 @@ static void run_m2l_tensor_t(kifmm_plan *P, const PassArgs &A) {
     if (!tiles) return;
     size_t smem = tc_smem_bytes<F>();
     ensure_dyn_smem(k_m2l_tc<F>, smem);
-    k_m2l_tc<F><<<(unsigned)tiles, TC_THREADS, smem, P->stream>>>(T);
-    KIFMM_LAUNCHED();
+    launch_pdl(k_m2l_tc<F>, dim3((unsigned)tiles), dim3(TC_THREADS), smem, P->stream, T);
 }
 
 // M2L of every level in one launch (u_down of each split entry's children is

@@ -14,12 +14,16 @@ namespace kifmm {
 
 __global__ void k_gather_tau(const double *__restrict__ tau, const int32_t *__restrict__ perm, int64_t n,
                              double *__restrict__ taus) {
+    pdl_trigger();
+    pdl_wait();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         taus[i] = tau[perm[i]];
 }
 
 __global__ void k_scatter_pot(const double *__restrict__ pots, const int32_t *__restrict__ perm, int64_t n,
                               double *__restrict__ pot) {
+    pdl_trigger();
+    pdl_wait();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         pot[perm[i]] = pots[i];
 }
@@ -31,6 +35,8 @@ constexpr int P2M_WARPS = 8;
 __global__ void __launch_bounds__(32 * P2M_WARPS) k_p2m_d(PassArgs A, const int32_t *__restrict__ list,
                                                            int64_t nlist) {
     __shared__ double sx[P2M_WARPS][32], sy[P2M_WARPS][32], st[P2M_WARPS][32];
+    pdl_trigger();
+    pdl_wait();
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (w >= nlist) return;
@@ -282,9 +288,8 @@ PassArgs make_pass_args(kifmm_plan *P) {
 }
 
 void launch_p2m_d(kifmm_plan *P, const PassArgs &A) {
-    k_p2m_d<<<grid_for(P->n_p2m_list * 32, 32 * P2M_WARPS), 32 * P2M_WARPS, 0, P->stream>>>(A, P->p2m_list.p,
-                                                                                         P->n_p2m_list);
-    KIFMM_LAUNCHED();
+launch_pdl(k_p2m_d, dim3(grid_for(P->n_p2m_list * 32, 32 * P2M_WARPS)), dim3(32 * P2M_WARPS), 0, P->stream, A,
+               (const int32_t *)P->p2m_list.p, P->n_p2m_list);
 }
 
 void launch_leaf_eval_d(kifmm_plan *P, const PassArgs &A, int check_self) {
@@ -569,10 +574,15 @@ __global__ void __launch_bounds__(LM_THREADS) k_lvl_mma(PassArgs A, int l, int M
     const int nact = __syncthreads_count(has);
     if (tid == 0) mbar_expect_tx(mb, (uint32_t)(K * M + nact * K + (MODE == 1 ? nact * M : 0)) * 8u);
     __syncthreads();
-    for (int c = tid; c < K + 64; c += LM_THREADS) {
-        if (c < K) {
-            bulk_g2s(smem_u32(opS + (size_t)c * ldo), op + (size_t)c * M, (uint32_t)M * 8u, mb);
-        } else if (c < K + 32) {
+    // the operator does not depend on the previous level: copy it before waiting
+    for (int c = tid; c < K; c += LM_THREADS)
+        bulk_g2s(smem_u32(opS + (size_t)c * ldo), op + (size_t)c * M, (uint32_t)M * 8u, mb);
+    // launched with programmatic stream serialisation: let the next level's
+    // kernel be scheduled, then wait until the previous kernel has completed
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    for (int c = K + tid; c < K + 64; c += LM_THREADS) {
+        if (c < K + 32) {
             const int n = c - K;
             if (n < nt && snode[n] >= 0) {
                 const double *src = MODE == 0 ? A.uup + (child0 + 4 * (size_t)n) * Q : A.udown + (size_t)snode[n] * Q;
@@ -633,8 +643,18 @@ __global__ void __launch_bounds__(LM_THREADS) k_lvl_mma(PassArgs A, int l, int M
 template <int MODE, int MT>
 static void launch_lvl_mma(kifmm_plan *P, const PassArgs &A, int l, int M, int K, size_t smem) {
     ensure_dyn_smem(k_lvl_mma<MODE, MT>, smem);
-    k_lvl_mma<MODE, MT><<<(unsigned)((P->lt.ne[l] + 31) / 32), LM_THREADS, smem, P->stream>>>(
-        A, l, M, K, 1ll << 26, P->scal.p + KIFMM_SCAL_PASS_ERR);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)((P->lt.ne[l] + 31) / 32));
+    cfg.blockDim = dim3(LM_THREADS);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = P->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;  // overlap with the previous level's tail
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    KIFMM_CUDA(cudaLaunchKernelEx(&cfg, k_lvl_mma<MODE, MT>, A, l, M, K, 1ll << 26,
+                                  P->scal.p + KIFMM_SCAL_PASS_ERR));
     KIFMM_LAUNCHED();
 }
 
@@ -698,16 +718,18 @@ void run_upward_downward(kifmm_plan *P) {
     P->pots.alloc(n);
     P->uup.alloc((size_t)NN * Q);
     P->udown.alloc((size_t)NN * Q);
-    k_gather_tau<<<grid_for(n, 256, P->num_sms * 8), 256, 0, s>>>(P->tau.p, P->perm.p, n, P->taus.p);
-    KIFMM_LAUNCHED();
-    // error flags of the level passes and the tensor-core M2L
+    // error flags of the level passes and the tensor-core M2L, and the
+    // expansions, cleared first so that the kernels below form one chain of
+    // programmatic dependent launches
     KIFMM_CUDA(cudaMemsetAsync(P->scal.p + KIFMM_SCAL_PASS_ERR, 0, 2 * sizeof(unsigned long long), s));
+    KIFMM_CUDA(cudaMemsetAsync(P->uup.p, 0, (size_t)NN * Q * sizeof(double), s));
+    KIFMM_CUDA(cudaMemsetAsync(P->udown.p, 0, (size_t)NN * Q * sizeof(double), s));
+    launch_pdl(k_gather_tau, dim3(grid_for(n, 256, P->num_sms * 8)), dim3(256), 0, s, (const double *)P->tau.p,
+               (const int32_t *)P->perm.p, n, P->taus.p);
     if (P->opt.precision == KIFMM_PREC_MIXED) {
         run_passes_mixed(P);
         return;
     }
-    KIFMM_CUDA(cudaMemsetAsync(P->uup.p, 0, (size_t)NN * Q * sizeof(double), s));
-    KIFMM_CUDA(cudaMemsetAsync(P->udown.p, 0, (size_t)NN * Q * sizeof(double), s));
     if (L < 3) return;  // no level has well-separated boxes
     PassArgs A = make_pass_args(P);
     if (P->n_p2m_list) {
@@ -744,8 +766,8 @@ void run_eval_sources(kifmm_plan *P, int check_self) {
             launch_leaf_eval_d(P, A, check_self);
         }
     }
-    k_scatter_pot<<<grid_for(n, 256, P->num_sms * 8), 256, 0, s>>>(P->pots.p, P->perm.p, n, P->pot_out.p);
-    KIFMM_LAUNCHED();
+    launch_pdl(k_scatter_pot, dim3(grid_for(n, 256, P->num_sms * 8)), dim3(256), 0, s, (const double *)P->pots.p,
+               (const int32_t *)P->perm.p, n, P->pot_out.p);
 }
 
 void run_eval_targets(kifmm_plan *P, const double *tx, const double *ty, int64_t n, int check_self, double *pot) {
