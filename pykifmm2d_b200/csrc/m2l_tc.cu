@@ -45,7 +45,11 @@ template <> struct TcTraits<TC_FP16> { static constexpr int NS = 2, EB = 2, KSTE
 
 constexpr int TC_M = 128;      // MMA M: operator rows per tile (TMEM lanes)
 constexpr int TC_N = 32;       // MMA N: target groups per CTA
-constexpr int TC_KC = 128;     // K elements staged per step
+constexpr int TC_KC = 128;     // K elements staged per stage
+// Stages in flight.  One: at K = 128 a stage is 100 KB, and two CTAs per SM
+// (one's copies under the other's MMAs) measured faster than two 64-K slots in
+// one CTA, whose extra stages cost more synchronisation than they hid.
+constexpr int TC_SLOTS = 1;
 constexpr int TC_THREADS = 128;
 static_assert(TC_N % 16 == 0 && TC_N >= 16 && TC_N <= 256, "MMA N for M = 128");
 static_assert(TcTraits<TC_INT8>::NACC * TC_N <= TcTraits<TC_INT8>::NCOLS, "int8 accumulators exceed the TMEM allocation");
@@ -280,14 +284,15 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_m2l_tc(TcArgs T) {
     const int Q = A.Q, Q4 = T.g.Q4, KP = T.pre.KP;
     const size_t a_sb = T.g.slice_bytes;                       // A slice (128 x KC)
     const size_t b_sb = (size_t)TC_N * TC_KC * TR::EB;         // B slice (TC_N x KC)
-    unsigned char *sA = tc_smem;
-    unsigned char *sB = sA + TR::NS * a_sb;
-    int *sgrp = (int *)(sB + TR::NS * b_sb);                   // [TC_N][9]
+    const size_t a_stage = TR::NS * a_sb, b_stage = TR::NS * b_sb;
+    unsigned char *sA = tc_smem;                               // [TC_SLOTS][NS slices]
+    unsigned char *sB = sA + TC_SLOTS * a_stage;               // [TC_SLOTS][NS slices]
+    int *sgrp = (int *)(sB + TC_SLOTS * b_stage);              // [TC_N][9]
     int *sshift = sgrp + TC_N * 9;                             // [TC_N][9] slice shift (INT8)
     double *stau = (double *)(sshift + TC_N * 9 + 2);          // [TC_N]
     int *sact = (int *)(stau + TC_N);                          // [TC_N]
-    uint64_t *bars = (uint64_t *)(sact + TC_N + 2);            // [0]: A copy, [1]: MMA
-    uint32_t *tslot = (uint32_t *)(bars + 2);
+    uint64_t *bars = (uint64_t *)(sact + TC_N + 2);            // [0..1] A landed, [2..3] MMAs done (per stage slot)
+    uint32_t *tslot = (uint32_t *)(bars + 4);
 
     // which level / column tile / M tile
     const int64_t tile = blockIdx.x;
@@ -331,73 +336,117 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_m2l_tc(TcArgs T) {
         stau[tid] = F == TC_INT8 ? ldexp(1.0, 7 * kcol) : 1.0;
         sact[tid] = act;
     }
-    if (tid == 0) {
-        mbar_init(smem_u32(&bars[0]));
-        mbar_init(smem_u32(&bars[1]));
-    }
+    if (tid == 0)
+        for (int i = 0; i < 4; i++) mbar_init(smem_u32(&bars[i]));
     fence_before();
     __syncthreads();
     fence_after();
     const uint32_t tmem = *tslot;
     const uint32_t idesc = instr_desc<F>();
-    const uint32_t bar_a = smem_u32(&bars[0]), bar_m = smem_u32(&bars[1]);
-    uint32_t phase = 0;
+    const uint32_t bfull[2] = {smem_u32(&bars[0]), smem_u32(&bars[1])};
+    const uint32_t bdone[2] = {smem_u32(&bars[2]), smem_u32(&bars[3])};
+    uint32_t pfull[2] = {0u, 0u}, pdone[2] = {0u, 0u};
+    int nfull[2] = {0, 0}, ndone[2] = {0, 0};  // copies / commits issued and not yet waited for, per slot
     bool failed = false;
-    const uint32_t a_bytes = (uint32_t)(TR::NS * a_sb);
+    const uint32_t a_bytes = (uint32_t)a_stage;
     constexpr int CH = TC_KC * TR::EB / 16;  // 16-byte chunks per slice row
+    const int NKC = T.g.NKC, NST = 8 * NKC;   // stages: (direction != centre, K chunk)
 
-    for (int d = 0; d < 9 && !failed; d++) {
-        if (d == 4) continue;
-        for (int kc = 0; kc < T.g.NKC && !failed; kc++) {
-            if (tid == 0) {  // A: one bulk copy of the NS slices of this (direction, M tile, K chunk)
-                mbar_expect_tx(bar_a, a_bytes);
-                bulk_g2s(smem_u32(sA), alev + (((size_t)d * T.g.MT + mt) * T.g.NKC + kc) * TR::NS * a_sb, a_bytes,
-                         bar_a);
-            }
-            // B: 16-byte copies of the pre-sliced source groups (shifted slices for INT8)
-            for (int idx = tid; idx < TC_N * TR::NS * CH; idx += TC_THREADS) {
-                int c = idx % CH, i = (idx / CH) % TR::NS, j = idx / (CH * TR::NS);
-                int grp = sgrp[j * 9 + d], si = i - sshift[j * 9 + d];
-                uint4 v = make_uint4(0, 0, 0, 0);
+    // stage st into slot: A by one bulk copy (on bfull[slot]), B by 16-byte copies
+    // of the pre-sliced source groups (shifted slices for INT8)
+    auto prepare = [&](int st, int slot) {
+        const int dd = st / NKC, d = dd < 4 ? dd : dd + 1, kc = st % NKC;
+        if (tid == 0) {
+            mbar_expect_tx(bfull[slot], a_bytes);
+            bulk_g2s(smem_u32(sA + slot * a_stage), alev + (((size_t)d * T.g.MT + mt) * NKC + kc) * a_stage, a_bytes,
+                     bfull[slot]);
+        }
+        nfull[slot]++;
+        unsigned char *sBs = sB + slot * b_stage;
+        // all of a thread's loads first, then its stores: one round trip per stage
+        constexpr int NBI = TC_N * TR::NS * CH, NB = (NBI + TC_THREADS - 1) / TC_THREADS;
+        uint4 v[NB];
+#pragma unroll
+        for (int q = 0; q < NB; q++) {
+            const int idx = tid + q * TC_THREADS;
+            v[q] = make_uint4(0, 0, 0, 0);
+            if (idx < NBI) {
+                const int c = idx % CH, i = (idx / CH) % TR::NS, j = idx / (CH * TR::NS);
+                const int grp = sgrp[j * 9 + d], si = i - sshift[j * 9 + d];
                 if (grp >= 0 && si >= 0 && si < TR::NS)
-                    v = *(const uint4 *)(T.pre.slices + ((size_t)grp * TR::NS + si) * KP * TR::EB +
-                                         (size_t)kc * TC_KC * TR::EB + c * 16);
-                *(uint4 *)(sB + i * b_sb + core_off(j, c * 16 / TR::EB, TC_N, TR::EB)) = v;
+                    v[q] = __ldg((const uint4 *)(T.pre.slices + ((size_t)grp * TR::NS + si) * KP * TR::EB +
+                                                 (size_t)kc * TC_KC * TR::EB + c * 16));
             }
-            fence_proxy_async();
-            fence_before();
-            __syncthreads();
-            bool ok = mbar_wait(bar_a, phase, T.wait_limit);
-            failed = __syncthreads_or(!ok) != 0;
-            if (failed) {
-                mbar_wait(bar_a, phase, T.wait_limit);  // let an in-flight copy land before leaving
-                break;
+        }
+#pragma unroll
+        for (int q = 0; q < NB; q++) {
+            const int idx = tid + q * TC_THREADS;
+            if (idx < NBI) {
+                const int c = idx % CH, i = (idx / CH) % TR::NS, j = idx / (CH * TR::NS);
+                *(uint4 *)(sBs + i * b_sb + core_off(j, c * 16 / TR::EB, TC_N, TR::EB)) = v[q];
             }
-            if (tid == 0) {
-                fence_after();
-                const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-                const uint32_t a_lbo = (TC_M / 8) * 128, b_lbo = (TC_N / 8) * 128;
-                for (int ks = 0; ks < TC_KC / TR::KSTEP; ks++) {
-                    for (int i = 0; i < TR::NS; i++) {
-                        const int jmax = F == TC_INT8 ? TR::NS - 1 - i : (i == 0 ? 1 : 0);
-                        for (int jj = 0; jj <= jmax; jj++) {
-                            const int acc = F == TC_INT8 ? i + jj : 0;
-                            const bool first = d == 0 && kc == 0 && ks == 0 && i == 0 && (F == TC_INT8 || jj == 0);
-                            uint64_t ad = umma_desc(a0 + i * (uint32_t)a_sb + ks * 2 * a_lbo, a_lbo, 128);
-                            uint64_t bd = umma_desc(b0 + jj * (uint32_t)b_sb + ks * 2 * b_lbo, b_lbo, 128);
-                            mma_issue<F>(tmem + acc * TC_N, ad, bd, idesc, first ? 0u : 1u);
-                        }
+        }
+        fence_proxy_async();
+        fence_before();
+        __syncthreads();
+    };
+    // bounded wait on a slot barrier, uniform over the block
+    // (a wait that runs out is tried once more, bounded, so that a copy or MMA
+    // still in flight lands before the block frees TMEM and leaves)
+    auto wait_slot = [&](const uint32_t *bar, uint32_t *par, int *cnt, int slot) {
+        bool ok = mbar_wait(bar[slot], par[slot], T.wait_limit);
+        if (!ok) mbar_wait(bar[slot], par[slot], T.wait_limit);
+        par[slot] ^= 1u;
+        cnt[slot]--;
+        return __syncthreads_or(!ok) == 0;
+    };
+
+    // pipeline over TC_SLOTS slots: the MMAs of stage st run on the tensor pipe
+    // while the block stages st + 1 into the next slot
+    prepare(0, 0);
+    for (int st = 0; st < NST && !failed; st++) {
+        const int slot = st % TC_SLOTS;
+        if (!wait_slot(bfull, pfull, nfull, slot)) {
+            failed = true;
+            break;
+        }
+        if (tid == 0) {
+            fence_after();
+            const uint32_t a0 = smem_u32(sA + slot * a_stage), b0 = smem_u32(sB + slot * b_stage);
+            const uint32_t a_lbo = (TC_M / 8) * 128, b_lbo = (TC_N / 8) * 128;
+            for (int ks = 0; ks < TC_KC / TR::KSTEP; ks++) {
+                for (int i = 0; i < TR::NS; i++) {
+                    const int jmax = F == TC_INT8 ? TR::NS - 1 - i : (i == 0 ? 1 : 0);
+                    for (int jj = 0; jj <= jmax; jj++) {
+                        const int acc = F == TC_INT8 ? i + jj : 0;
+                        const bool first = st == 0 && ks == 0 && i == 0 && (F == TC_INT8 || jj == 0);
+                        uint64_t ad = umma_desc(a0 + i * (uint32_t)a_sb + ks * 2 * a_lbo, a_lbo, 128);
+                        uint64_t bd = umma_desc(b0 + jj * (uint32_t)b_sb + ks * 2 * b_lbo, b_lbo, 128);
+                        mma_issue<F>(tmem + acc * TC_N, ad, bd, idesc, first ? 0u : 1u);
                     }
                 }
-                mma_commit(bar_m);
             }
-            ok = mbar_wait(bar_m, phase, T.wait_limit);
-            phase ^= 1u;
-            fence_after();
-            failed = __syncthreads_or(!ok) != 0;
-            if (failed) mbar_wait(bar_m, phase ^ 1u, T.wait_limit);  // MMAs still running: wait before TMEM is freed
+            mma_commit(bdone[slot]);
+        }
+        ndone[slot]++;
+        if (st + 1 < NST) {
+            const int ns = (st + 1) % TC_SLOTS;
+            if (ndone[ns] > 0 && !wait_slot(bdone, pdone, ndone, ns)) {  // the MMAs that last read slot ns
+                failed = true;
+                break;
+            }
+            prepare(st + 1, ns);
         }
     }
+    // drain what is still in flight (on failure too: copies must land and MMAs
+    // finish before the block frees TMEM and leaves)
+    for (int sl = 0; sl < TC_SLOTS; sl++) {
+        while (ndone[sl] > 0)
+            if (!wait_slot(bdone, pdone, ndone, sl)) failed = true;
+        while (nfull[sl] > 0)
+            if (!wait_slot(bfull, pfull, nfull, sl)) failed = true;
+    }
+    fence_after();
 
     if (!failed) {
         const int row = warp * 32 + lane, r = mt * TC_M + row;
@@ -450,8 +499,8 @@ static int form_of(int m2l) {
 template <int F>
 static size_t tc_smem_bytes() {
     using TR = TcTraits<F>;
-    return TR::NS * (size_t)TC_M * TC_KC * TR::EB + TR::NS * (size_t)TC_N * TC_KC * TR::EB + 2 * TC_N * 9 * 4 + 8 +
-           TC_N * 8 + TC_N * 4 + 8 + 16 + 8 + 1024;
+    return TC_SLOTS * (TR::NS * (size_t)TC_M * TC_KC * TR::EB + TR::NS * (size_t)TC_N * TC_KC * TR::EB) + 2 * TC_N * 9 * 4 +
+           8 + TC_N * 8 + TC_N * 4 + 8 + 32 + 8 + 1024;
 }
 
 template <int F>

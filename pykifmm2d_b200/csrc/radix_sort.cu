@@ -157,8 +157,10 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
     return v;
 }
 
-__global__ void __launch_bounds__(RS_THREADS) k_os_hist(const uint64_t *__restrict__ key, int64_t n, OsShifts sh,
-                                                         uint32_t *__restrict__ hist) {
+// digit counts of every pass; shifts packed 8 bits each in `packed` (no
+// per-pass array in local memory), npass <= OS_MAX_PASSES
+__global__ void __launch_bounds__(RS_THREADS) k_os_hist(const uint64_t *__restrict__ key, int64_t n, uint64_t packed,
+                                                         int npass, uint32_t *__restrict__ hist) {
     __shared__ uint32_t h[OS_MAX_PASSES][256];
     for (int i = threadIdx.x; i < OS_MAX_PASSES * 256; i += RS_THREADS) (&h[0][0])[i] = 0;
     __syncthreads();
@@ -171,17 +173,20 @@ __global__ void __launch_bounds__(RS_THREADS) k_os_hist(const uint64_t *__restri
             k[r] = idx < n ? key[idx] : 0;
         }
 #pragma unroll
-        for (int r = 0; r < RS_ITEMS; r++) {
-            const bool ok = base + r * RS_THREADS + threadIdx.x < n;
-            for (int p = 0; p < sh.n; p++) {
-                const uint32_t d = ok ? (uint32_t)((k[r] >> sh.s[p]) & 255) : 256u;
+        for (int p = 0; p < OS_MAX_PASSES; p++) {
+            if (p >= npass) break;
+            const int sh = (int)((packed >> (8 * p)) & 63);
+#pragma unroll
+            for (int r = 0; r < RS_ITEMS; r++) {
+                const bool ok = base + r * RS_THREADS + threadIdx.x < n;
+                const uint32_t d = ok ? (uint32_t)((k[r] >> sh) & 255) : 256u;
                 const unsigned peers = __match_any_sync(0xffffffffu, d);  // one add per distinct digit
                 if (d < 256 && lane == __ffs(peers) - 1) atomicAdd(&h[p][d], (uint32_t)__popc(peers));
             }
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < sh.n * 256; i += RS_THREADS) {
+    for (int i = threadIdx.x; i < npass * 256; i += RS_THREADS) {
         const uint32_t c = (&h[0][0])[i];
         if (c) atomicAdd(&hist[i], c);
     }
@@ -190,7 +195,6 @@ __global__ void __launch_bounds__(RS_THREADS) k_os_hist(const uint64_t *__restri
 // One pass.  The tile's keys are ranked per warp, ordered by digit in shared
 // memory (tile-local digit starts tstart[]), and written out in that order so
 // that consecutive threads store consecutive positions of one digit's run.
-// The look-back reads eight predecessors' words per step.
 constexpr size_t OS_PASS_SMEM = (size_t)RS_TILE * (sizeof(uint64_t) + sizeof(int32_t));
 template <bool PAIRS>
 __global__ void __launch_bounds__(RS_THREADS) k_os_pass(const uint64_t *__restrict__ key, const int32_t *__restrict__ val,
@@ -345,7 +349,9 @@ static void os_run(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_
     KIFMM_CUDA(cudaMemsetAsync(hist, 0, ((size_t)npass * 256 + npass) * sizeof(uint32_t), s));
     KIFMM_CUDA(cudaMemsetAsync(P->sort_status.p, 0, nstat * sizeof(unsigned long long), s));
     const unsigned hg = (unsigned)std::min<int64_t>(ntiles, (int64_t)P->num_sms * 4);
-    k_os_hist<<<hg, RS_THREADS, 0, s>>>(key, n, sh, hist);
+    uint64_t packed = 0;
+    for (int p = 0; p < npass; p++) packed |= (uint64_t)(shifts[p] & 63) << (8 * p);
+    k_os_hist<<<hg, RS_THREADS, 0, s>>>(key, n, packed, npass, hist);
     KIFMM_LAUNCHED();
     uint64_t *ka = key, *kb = key_tmp;
     int32_t *va = val, *vb = val_tmp;
