@@ -177,6 +177,7 @@ struct kifmm_plan {
     kifmm::DBuf<uint32_t> list_tiles;
     kifmm::DBuf<unsigned> grid_bar;  // grid barrier of the split-cell closure  // per-tile counts/offsets while the lists are built
     int64_t n_leaf_list = 0, n_p2m_list = 0;
+    int64_t leaf_loff[KIFMM_MAX_LEVELS + 1] = {};  // leaf_list range of each level
     int64_t n_leaves = 0, n_fake = 0, n_xlist = 0;
     int64_t n_p2p_pairs = 0, n_p2m_points = 0, n_m2l_pairs = 0, n_m2l_groups = 0;
     bool have_stats = false;
@@ -192,7 +193,7 @@ struct kifmm_plan {
     kifmm::DBuf<double> tc_rowscale;
     kifmm::DBuf<unsigned long long> tc_rowmax;  // [L][4Q] largest |value| per M2L operator row
     kifmm::DBuf<double> l2p_taylor;  // Laplace: [L][Q][2p+1] check potential -> Taylor coefficients
-    kifmm::DBuf<float> l2p_taylor_f;  // FP32 copy
+    kifmm::DBuf<double> leaf_coef;   // [n_leaf_list][2p+1] Taylor coefficients per apply
     kifmm::DBuf<unsigned char> tc_pre;  // per-apply slices of the source groups
     kifmm::DBuf<int> tc_gexp;
 

@@ -214,7 +214,7 @@ __global__ void k_ops_assemble(OpsArgs A, unsigned long long *rowmax) {
 //   a0 = -(log r2 / 2pi) sum_k q_k,  c_j = (rho^-j / (2 pi j)) sum_k q_k e^(-i j theta_k),
 // valid for |z~| < rho.  taylor_l [(2p+1) rows][Q cols] (column-major) maps the
 // downward check potential to (a0, Re c_1, Im c_1, ...) through q = Inv_l u.
-__global__ void k_ops_taylor(OpsArgs A, double *taylor, float *taylor_f, int p) {
+__global__ void k_ops_taylor(OpsArgs A, double *taylor, int p) {
     // one block per (level, row): thread k forms C[row][k], thread c the output
     __shared__ double Crow[256];
     const int Q = A.Q, l = blockIdx.x, row = blockIdx.y, R = 2 * p + 1;
@@ -239,7 +239,6 @@ __global__ void k_ops_taylor(OpsArgs A, double *taylor, float *taylor_f, int p) 
         double acc = 0.0;
         for (int k = 0; k < Q; k++) acc = fma(Crow[k], inv[k * Q + c], acc);
         taylor[((size_t)l * Q + c) * R + row] = acc;
-        if (taylor_f) taylor_f[((size_t)l * Q + c) * R + row] = (float)acc;
     }
 }
 
@@ -306,10 +305,8 @@ void build_operators(kifmm_plan *P) {
         if (P->kern.kind == KIFMM_KERNEL_LAPLACE && L >= 3) {
             const int R = 2 * KIFMM_TAYLOR_P + 1;
             P->l2p_taylor.alloc((size_t)L * Q * R);
-            P->l2p_taylor_f.alloc((size_t)L * Q * R);
             KIFMM_REQUIRE(Q <= 256, KIFMM_ERR_ARG, "Nequiv above 256");
-            k_ops_taylor<<<dim3(L, R), ((Q + 31) / 32) * 32, 0, s>>>(A, P->l2p_taylor.p, P->l2p_taylor_f.p,
-                                                                    KIFMM_TAYLOR_P);
+            k_ops_taylor<<<dim3(L, R), ((Q + 31) / 32) * 32, 0, s>>>(A, P->l2p_taylor.p, KIFMM_TAYLOR_P);
             KIFMM_LAUNCHED();
         }
     }

@@ -283,7 +283,7 @@ PassArgs make_pass_args(kifmm_plan *P) {
     A.uup = P->uup.p;
     A.udown = P->udown.p;
     A.taylor = P->l2p_taylor.p;
-    A.taylor_f = P->l2p_taylor_f.p;
+    A.leaf_coef = P->leaf_coef.p;
     return A;
 }
 
@@ -535,12 +535,6 @@ __global__ void __launch_bounds__(LG_THREADS) k_lvl_gemm_b(PassArgs A, int l, in
 // 16-byte aligned operator rows.  A copy wait that runs out sets *err and the
 // block leaves without writing.
 constexpr int LM_THREADS = 128;
-__device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b) {
-    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
-                 : "+d"(c0), "+d"(c1)
-                 : "d"(a), "d"(b));
-}
-__host__ __device__ constexpr int pad4mod16(int m) { return m + (20 - m % 16) % 16; }
 static size_t lvl_mma_smem(int M, int K) {
     return ((size_t)K * pad4mod16(M) + 32 * (size_t)pad4mod16(K) + 32 * (size_t)M) * sizeof(double);
 }

@@ -22,7 +22,7 @@ struct PassArgs {
     double *pots;
     double *uup, *udown;
     const double *taylor;  // Laplace L2P coefficients map, or null
-    const float *taylor_f;  // FP32 copy of it (the orders computed in FP32)
+    const double *leaf_coef;  // [leaf_list index][2p+1] Taylor coefficients of the leaves (mixed form)
 };
 
 // Node centre, exactly the reference's xmid = xmin + w/2 (tree.py:339-346):
@@ -35,6 +35,17 @@ __device__ __forceinline__ void node_center(const PassArgs &A, int g, int l, dou
 }
 
 PassArgs make_pass_args(kifmm_plan *P);
+
+// FP64 tensor-core MMA (mma.sync m8n8k4 .f64): D = A B + D with fragments
+// A[row = lane/4][k = lane%4], B[k = lane%4][n = lane/4],
+// D[row = lane/4][n = 2*(lane%4) + {0,1}].
+__device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+// row stride = 4 mod 16 doubles: conflict-free fragment loads
+__host__ __device__ constexpr int pad4mod16(int m) { return m + (20 - m % 16) % 16; }
 // passes_mixed.cu
 void run_passes_mixed(kifmm_plan *P);
 void run_eval_sources_mixed(kifmm_plan *P, int check_self);

@@ -120,6 +120,91 @@ __device__ __forceinline__ void local_density(const PassArgs &A, int g, int l, d
     }
 }
 
+// Taylor coefficients of every leaf's local expansion (Laplace, levels >= 2),
+// FP64 on the tensor path: C[R x leaves] = Taylor_l[R x Q] . u_down[Q x leaves],
+// one block per 32 consecutive leaves of one level (leaf_list is level-major).
+// Warp w computes all R rows (MTR 8-row tiles) for leaves 8w..8w+7; the block
+// writes its 32 x R coefficients as one contiguous run.
+struct TaylorArgs {
+    PassArgs A;
+    const int32_t *list;
+    double *coef;
+    int lmin, lmax;
+    int64_t loff[MAX_LEVELS + 1];  // leaf_list range of each level
+    int64_t toff[MAX_LEVELS + 1];  // first block of each level
+};
+constexpr int TY_THREADS = 128;
+constexpr int TY_R = 2 * KIFMM_TAYLOR_P + 1, TY_MTR = (TY_R + 7) / 8;
+__global__ void __launch_bounds__(TY_THREADS) k_leaf_taylor(TaylorArgs T) {
+    extern __shared__ __align__(16) double sm_ty[];
+    const PassArgs &A = T.A;
+    const int Q = A.Q, R = TY_R, ldt = pad4mod16(8 * TY_MTR), ldx = pad4mod16(Q);
+    double *tS = sm_ty;                      // [Q][ldt]: element (row r, col k) at k * ldt + r
+    double *xS = tS + (size_t)Q * ldt;       // [32 leaves][ldx]
+    double *cS = xS + 32 * (size_t)ldx;      // [32 leaves][R]
+    pdl_trigger();
+    const int64_t b = blockIdx.x;
+    int l = T.lmin;
+    while (l < T.lmax && T.toff[l + 1] <= b) l++;
+    const int64_t w0 = T.loff[l] + (b - T.toff[l]) * 32;
+    const int nt = (int)min((int64_t)32, T.loff[l + 1] - w0);
+    const int tid = threadIdx.x;
+    // the level's map (precomputed, independent of the previous kernel), rows padded with zeros
+    const double *tl = A.taylor + (size_t)l * Q * R;
+    for (int i0 = tid; i0 < Q * ldt; i0 += 4 * TY_THREADS) {
+        double v[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int i = i0 + q * TY_THREADS, k = i / ldt, r = i - k * ldt;
+            v[q] = (i < Q * ldt && r < R) ? tl[(size_t)k * R + r] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int i = i0 + q * TY_THREADS;
+            if (i < Q * ldt) tS[i] = v[q];
+        }
+    }
+    pdl_wait();  // u_down comes from the L2L chain
+    for (int i0 = tid; i0 < 32 * Q; i0 += 4 * TY_THREADS) {
+        double v[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int i = i0 + q * TY_THREADS, n = i / Q, k = i - n * Q;
+            v[q] = (i < 32 * Q && n < nt) ? A.udown[(size_t)T.list[w0 + n] * Q + k] : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int i = i0 + q * TY_THREADS, n = i / Q, k = i - n * Q;
+            if (i < 32 * Q) xS[n * ldx + k] = v[q];
+        }
+    }
+    __syncthreads();
+    const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3, n0 = warp * 8;
+    if (n0 < nt) {
+        double acc[TY_MTR][2];
+#pragma unroll
+        for (int i = 0; i < TY_MTR; i++) acc[i][0] = acc[i][1] = 0.0;
+        const double *xb = xS + (size_t)(n0 + g) * ldx + t;
+        const double *ab = tS + (size_t)t * ldt + g;
+        for (int k0 = 0; k0 < Q; k0 += 4) {
+            const double bv = xb[k0];
+#pragma unroll
+            for (int i = 0; i < TY_MTR; i++) dmma_8x8x4(acc[i][0], acc[i][1], ab[(size_t)k0 * ldt + 8 * i], bv);
+        }
+#pragma unroll
+        for (int i = 0; i < TY_MTR; i++) {
+            const int r = 8 * i + g;
+            if (r < R) {
+                cS[(n0 + 2 * t) * R + r] = acc[i][0];
+                cS[(n0 + 2 * t + 1) * R + r] = acc[i][1];
+            }
+        }
+    }
+    __syncthreads();
+    double *out = T.coef + (size_t)w0 * R;
+    for (int i = tid; i < nt * R; i += TY_THREADS) out[i] = cS[i];
+}
+
 // L2P + P2P: one warp per target leaf.  The sources of the leaf and its eight
 // colleagues are staged in shared memory as one list (the leaf's own points
 // first), in chunks of LEAF_CHUNK.  A tile of nt <= 32 targets is spread over
@@ -177,31 +262,13 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, 6) k_leaf_eval_f(PassArgs A, 
     const double width = ldexp(A.W, -l);
     const double sc = lap ? 1.0 / width : 1.0;     // coordinate scale
     const double lw = lap ? -2.0 * log2(sc) : 0.0; // log2 of the squared length unit
-    if (taylor) {
-        // Taylor coefficients of the local expansion: rows 0..31 (orders j <= 16)
-        // in FP64, rows 32.. (j >= 16, weighted by at most (|z|/rho)^16 ~ 2e-4
-        // where they are used) in FP32, each lane four independent rows
-        static_assert(R > 96 && R <= 128, "row groups below assume 96 < 2p+1 <= 128");
-        const double *T = A.taylor + (size_t)l * A.Q * R + lane;
-        const float *Tf = A.taylor_f + (size_t)l * A.Q * R + lane;
-        const double *u = A.udown + (size_t)g * A.Q;
-        double c0 = 0.0;
-        float c1 = 0.f, c2 = 0.f, c3 = 0.f;
-        const bool r3 = lane + 96 < R;
-#pragma unroll 4
-        for (int c = 0; c < A.Q; c++) {
-            const double uc = u[c];
-            const float ucf = (float)uc;
-            c0 = fma(T[(size_t)c * R], uc, c0);
-            c1 = fmaf(Tf[(size_t)c * R + 32], ucf, c1);
-            c2 = fmaf(Tf[(size_t)c * R + 64], ucf, c2);
-            if (r3) c3 = fmaf(Tf[(size_t)c * R + 96], ucf, c3);
+    if (taylor) {  // Taylor coefficients of the local expansion (k_leaf_taylor, FP64)
+        const double *cf = A.leaf_coef + (size_t)w * R;
+        for (int r = lane; r < R; r += 32) {
+            const double v = cf[r];
+            qd[r] = v;
+            qf[r] = (float)v;
         }
-        qd[lane] = c0;
-        qf[lane + 32] = c1;
-        qf[lane + 64] = c2;
-        if (r3) qf[lane + 96] = c3;
-        if (lane == 0) qd[32] = (double)c1;  // Im c_16, used by the FP64 part of the Horner sum
     } else {
         local_density(A, g, l, qd, lane);
     }
@@ -357,17 +424,18 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, 6) k_leaf_eval_f(PassArgs A, 
             if (l >= 2) {
                 const double zx = pxd * sc, zy = pyd * sc;
                 if (taylor && zx * zx + zy * zy <= 0.5625) {
-                    // Horner: orders P..17 in FP32, then 16..1 in FP64
+                    // Horner: orders P..9 in FP32 (weighted by |z/rho|^9 < 0.008 where
+                    // used), then 8..1 in FP64
                     const float zxf = (float)zx, zyf = (float)zy;
                     float fr = qf[R - 2], fi = qf[R - 1];
-                    for (int jj = KIFMM_TAYLOR_P - 1; jj >= 17; jj--) {
+                    for (int jj = KIFMM_TAYLOR_P - 1; jj >= 9; jj--) {
                         const float nr = fmaf(fr, zxf, fmaf(-fi, zyf, qf[2 * jj - 1]));
                         const float ni = fmaf(fr, zyf, fmaf(fi, zxf, qf[2 * jj]));
                         fr = nr;
                         fi = ni;
                     }
                     double sr = fr, si = fi;
-                    for (int jj = 16; jj >= 1; jj--) {
+                    for (int jj = 8; jj >= 1; jj--) {
                         double nr = fma(sr, zx, fma(-si, zy, qd[2 * jj - 1]));
                         double ni = fma(sr, zy, fma(si, zx, qd[2 * jj]));
                         sr = nr;
@@ -494,6 +562,31 @@ void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
         launch_leaf_eval_d(P, A, check_self);
         return;
     }  // FP32 form: coincident pairs always contribute zero
+    if (P->kern.kind == KIFMM_KERNEL_LAPLACE && P->l2p_taylor.p && P->L >= 3) {
+        constexpr int R = 2 * KIFMM_TAYLOR_P + 1;
+        KIFMM_REQUIRE(P->Q % 4 == 0, KIFMM_ERR_ARG, "mixed Laplace form: Nequiv must be a multiple of 4");
+        P->leaf_coef.alloc((size_t)P->n_leaf_list * R);
+        A.leaf_coef = P->leaf_coef.p;
+        TaylorArgs T{};
+        T.A = A;
+        T.list = P->leaf_list.p;
+        T.coef = P->leaf_coef.p;
+        T.lmin = 2;
+        T.lmax = P->L - 1;
+        int64_t tiles = 0;
+        for (int l = 0; l <= MAX_LEVELS; l++) {
+            T.loff[l] = P->leaf_loff[l];
+            T.toff[l] = tiles;
+            if (l >= T.lmin && l <= T.lmax && l < MAX_LEVELS)
+                tiles += (P->leaf_loff[l + 1] - P->leaf_loff[l] + 31) / 32;
+        }
+        if (tiles) {
+            const size_t smem = ((size_t)P->Q * pad4mod16(8 * TY_MTR) + 32 * (size_t)pad4mod16(P->Q) + 32 * (size_t)R) *
+                                sizeof(double);
+            ensure_dyn_smem(k_leaf_taylor, smem);
+            launch_pdl(k_leaf_taylor, dim3((unsigned)tiles), dim3(TY_THREADS), smem, P->stream, T);
+        }
+    }
     unsigned gr = (unsigned)((P->n_leaf_list + LEAF_WARPS - 1) / LEAF_WARPS);
     if (P->kern.kind == KIFMM_KERNEL_LAPLACE)
         launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_LAPLACE>, dim3(gr), dim3(32 * LEAF_WARPS), 0, P->stream, A,

@@ -476,12 +476,17 @@ __device__ __forceinline__ unsigned block_excl_scan(unsigned v, unsigned *sm, un
     __syncthreads();
     return r;
 }
+// lcnt[l]: entries of leaf_list on level l (leaf_list is level-major, so they
+// are the contiguous range after those of the levels above)
 __global__ void __launch_bounds__(LT_THREADS) k_lists_count(int64_t n_nodes, const int8_t *__restrict__ nlev,
                                                             const uint8_t *__restrict__ nflag,
                                                             const int32_t *__restrict__ nbot,
                                                             const int32_t *__restrict__ ntop, uint32_t *tcnt,
-                                                            unsigned long long *cnt) {
+                                                            unsigned long long *cnt, unsigned long long *lcnt) {
     __shared__ unsigned sm[32];
+    __shared__ unsigned slv[MAX_LEVELS];
+    if (threadIdx.x < MAX_LEVELS) slv[threadIdx.x] = 0;
+    __syncthreads();
     const int64_t g0 = (int64_t)blockIdx.x * LT_TILE;
     unsigned c[5] = {0, 0, 0, 0, 0};
     for (int i = threadIdx.x; i < LT_TILE; i += LT_THREADS) {
@@ -493,7 +498,10 @@ __global__ void __launch_bounds__(LT_THREADS) k_lists_count(int64_t n_nodes, con
         c[2] += f.real_leaf;
         c[3] += f.fake;
         c[4] += f.xl;
+        if (f.leaf) atomicAdd(&slv[nlev[g]], 1u);
     }
+    __syncthreads();
+    if (threadIdx.x < MAX_LEVELS && slv[threadIdx.x]) atomicAdd(&lcnt[threadIdx.x], (unsigned long long)slv[threadIdx.x]);
 #pragma unroll
     for (int k = 0; k < 5; k++) {
         unsigned t;
@@ -668,7 +676,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     bool ops_started = false;
 
     int64_t n_ent = 0;
-    P->misc.alloc(64);
+    P->misc.alloc(128);
     unsigned long long *lc = (unsigned long long *)P->misc.p;  // [32] entries per level
     unsigned long long lcount[32] = {};
     if (L > 1) {
@@ -770,12 +778,14 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
                               P->nparent.p, P->nchild.p, P->nent.p, P->ncoll.p, P->ent_node.p);
     KIFMM_LAUNCHED();
     unsigned long long *cnt = (unsigned long long *)P->misc.p + 32;
+    unsigned long long *lcnt = (unsigned long long *)P->misc.p + 64;  // [MAX_LEVELS] leaves per level
     KIFMM_CUDA(cudaMemsetAsync(cnt, 0, 8 * sizeof(unsigned long long), s));
+    KIFMM_CUDA(cudaMemsetAsync(lcnt, 0, MAX_LEVELS * sizeof(unsigned long long), s));
     {
         const int64_t ntiles = (NN + LT_TILE - 1) / LT_TILE;
         P->list_tiles.alloc(2 * ntiles);
         k_lists_count<<<(unsigned)ntiles, LT_THREADS, 0, s>>>(NN, P->nlev.p, P->nflag.p, P->nbot.p, P->ntop.p,
-                                                              P->list_tiles.p, cnt);
+                                                              P->list_tiles.p, cnt, lcnt);
         KIFMM_LAUNCHED();
         k_lists_scan<<<1, 1024, 0, s>>>(ntiles, P->list_tiles.p, cnt);
         KIFMM_LAUNCHED();
@@ -783,12 +793,16 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
                                                               P->list_tiles.p, P->leaf_list.p, P->p2m_list.p);
         KIFMM_LAUNCHED();
     }
-    unsigned long long c5[5], sort_err = 0;
+    unsigned long long c5[5], sort_err = 0, lv[MAX_LEVELS];
     KIFMM_CUDA(cudaMemcpyAsync(c5, cnt, sizeof(c5), cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaMemcpyAsync(lv, lcnt, sizeof(lv), cudaMemcpyDeviceToHost, s));
     KIFMM_CUDA(cudaMemcpyAsync(&sort_err, P->scal.p + KIFMM_SCAL_SORT_ERR, sizeof(sort_err), cudaMemcpyDeviceToHost, s));
     KIFMM_CUDA(cudaStreamSynchronize(s));
     KIFMM_REQUIRE(sort_err == 0, KIFMM_ERR_CUDA, "build_tree: a radix-sort look-back wait timed out");
     P->n_leaf_list = (int64_t)c5[0];
+    P->leaf_loff[0] = 0;
+    for (int l = 0; l < MAX_LEVELS; l++) P->leaf_loff[l + 1] = P->leaf_loff[l] + (int64_t)lv[l];
+    KIFMM_REQUIRE(P->leaf_loff[MAX_LEVELS] == P->n_leaf_list, KIFMM_ERR_CUDA, "build_tree: inconsistent leaf counts");
     P->n_p2m_list = (int64_t)c5[1];
     P->n_leaves = (int64_t)c5[2];
     P->n_fake = (int64_t)c5[3];
