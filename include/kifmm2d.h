@@ -205,7 +205,10 @@ enum {
     KIFMM_PHASE_TARGETS = 7,   /* locate + L2P + P2P at separate targets */
     KIFMM_PHASE_L2L = 8,       /* separate L2L chain (after the tensor-core M2L) */
     KIFMM_PHASE_OPERATORS = 9, /* operator construction on the side stream, overlapping TREE */
-    KIFMM_PHASE_COUNT = 10
+    KIFMM_PHASE_CLOSURE = 10,  /* split cells, level restriction, X-list (inside TREE) */
+    KIFMM_PHASE_ENTRIES = 11,  /* sort of the split-cell entries (inside TREE) */
+    KIFMM_PHASE_NODES = 12,    /* node tables and work lists (inside TREE) */
+    KIFMM_PHASE_COUNT = 13
 };
 int kifmm_set_profiling(kifmm_plan *plan, int32_t on);
 /* ms[KIFMM_PHASE_COUNT] and launches[KIFMM_PHASE_COUNT] (either may be NULL);

@@ -161,6 +161,8 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
 // per-pass array in local memory), npass <= OS_MAX_PASSES
 __global__ void __launch_bounds__(RS_THREADS) k_os_hist(const uint64_t *__restrict__ key, int64_t n, uint64_t packed,
                                                          int npass, uint32_t *__restrict__ hist) {
+    pdl_trigger();
+    pdl_wait();
     __shared__ uint32_t h[OS_MAX_PASSES][256];
     for (int i = threadIdx.x; i < OS_MAX_PASSES * 256; i += RS_THREADS) (&h[0][0])[i] = 0;
     __syncthreads();
@@ -202,6 +204,8 @@ __global__ void __launch_bounds__(RS_THREADS) k_os_pass(const uint64_t *__restri
                                                          int64_t n, int shift, const uint32_t *__restrict__ ghist,
                                                          unsigned long long *status, unsigned *tile_ctr,
                                                          unsigned long long *err, long long limit) {
+    pdl_trigger();
+    pdl_wait();
     extern __shared__ __align__(16) unsigned char os_sm[];
     uint64_t *skey = (uint64_t *)os_sm;                        // [RS_TILE]
     int32_t *sval = (int32_t *)(os_sm + RS_TILE * sizeof(uint64_t));
@@ -351,8 +355,7 @@ static void os_run(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_
     const unsigned hg = (unsigned)std::min<int64_t>(ntiles, (int64_t)P->num_sms * 4);
     uint64_t packed = 0;
     for (int p = 0; p < npass; p++) packed |= (uint64_t)(shifts[p] & 63) << (8 * p);
-    k_os_hist<<<hg, RS_THREADS, 0, s>>>(key, n, packed, npass, hist);
-    KIFMM_LAUNCHED();
+    launch_pdl(k_os_hist, dim3(hg), dim3(RS_THREADS), 0, s, (const uint64_t *)key, n, packed, npass, hist);
     uint64_t *ka = key, *kb = key_tmp;
     int32_t *va = val, *vb = val_tmp;
     unsigned long long *err = P->scal.p + KIFMM_SCAL_SORT_ERR;
@@ -362,15 +365,15 @@ static void os_run(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_
             KIFMM_CUDA(cudaMemsetAsync(stat, 0, per_pass * sizeof(unsigned long long), s));
         if (pairs) {
             ensure_dyn_smem(k_os_pass<true>, OS_PASS_SMEM);
-            k_os_pass<true><<<(unsigned)ntiles, RS_THREADS, OS_PASS_SMEM, s>>>(ka, va, kb, vb, n, sh.s[p], hist + 256 * p,
-                                                                               stat, ctr + p, err, 1ll << 20);
+            launch_pdl(k_os_pass<true>, dim3((unsigned)ntiles), dim3(RS_THREADS), OS_PASS_SMEM, s,
+                       (const uint64_t *)ka, (const int32_t *)va, kb, vb, n, sh.s[p], (const uint32_t *)(hist + 256 * p),
+                       stat, ctr + p, err, 1ll << 20);
         } else {
             ensure_dyn_smem(k_os_pass<false>, OS_PASS_SMEM);
-            k_os_pass<false><<<(unsigned)ntiles, RS_THREADS, OS_PASS_SMEM, s>>>(ka, nullptr, kb, nullptr, n, sh.s[p],
-                                                                                hist + 256 * p, stat, ctr + p, err,
-                                                                                1ll << 20);
+            launch_pdl(k_os_pass<false>, dim3((unsigned)ntiles), dim3(RS_THREADS), OS_PASS_SMEM, s,
+                       (const uint64_t *)ka, (const int32_t *)nullptr, kb, (int32_t *)nullptr, n, sh.s[p],
+                       (const uint32_t *)(hist + 256 * p), stat, ctr + p, err, 1ll << 20);
         }
-        KIFMM_LAUNCHED();
         std::swap(ka, kb);
         std::swap(va, vb);
     }

@@ -23,6 +23,8 @@
 #include <cmath>
 #include <cstring>
 
+#include <optional>
+
 #include "kifmm_internal.cuh"
 
 namespace kifmm {
@@ -111,6 +113,8 @@ __global__ void k_keys(const double *__restrict__ x, const double *__restrict__ 
 __global__ void k_keys_dev(const double *__restrict__ x, const double *__restrict__ y, int64_t n, int fix_bbox,
                            const unsigned long long *__restrict__ scal, uint64_t *__restrict__ key,
                            int32_t *__restrict__ perm, unsigned long long *outside) {
+    pdl_trigger();
+    pdl_wait();
     double m, M;
     root_box(scal, fix_bbox, m, M);
     const bool valid = scal[4] == 0 && fabs(m) < 8388608.0 && fabs(M) < 8388608.0;
@@ -130,6 +134,8 @@ __global__ void k_keys_dev(const double *__restrict__ x, const double *__restric
 
 __global__ void k_gather2(const double *__restrict__ x, const double *__restrict__ y, const int32_t *__restrict__ perm,
                           int64_t n, double *__restrict__ xs, double *__restrict__ ys) {
+    pdl_trigger();
+    pdl_wait();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         int32_t p = perm[i];
         xs[i] = x[p];
@@ -214,6 +220,8 @@ __device__ __forceinline__ void t0_insert(const uint64_t *__restrict__ key, int6
 
 __global__ void k_t0(const uint64_t *__restrict__ key, int64_t n, int64_t ppl, int mode, HashSet H,
                      unsigned long long *scal) {
+    pdl_trigger();
+    pdl_wait();
     unsigned long long cnt = 0;
     int deepest = 0;
     bool over = false;
@@ -350,25 +358,49 @@ __global__ void __launch_bounds__(256) k_split_closure(const uint64_t *__restric
 }
 
 // ----------------------------------------------------------- node arrays
-__device__ __forceinline__ int64_t find_entry(const uint64_t *__restrict__ ent, const LevelTable &T, int l,
-                                              uint64_t k) {
-    if (l < 0 || l >= T.L) return -1;
-    int64_t lo = T.eoff[l], end = lo + T.ne[l], hi = end;
-    uint64_t target = ((uint64_t)l << (ENT_LEVEL_SHIFT - 1)) | k;
-    while (lo < hi) {
-        int64_t mid = (lo + hi) >> 1;
-        if ((ent[mid] >> 1) < target) lo = mid + 1;
-        else hi = mid;
+// Entry lookup by hash probe: the split-cell set's table holds every entry
+// (with its X-list bit), and hidx[slot] is the sorted position of the entry in
+// that slot (k_hash_index).  One or two probes instead of a binary search.
+struct EntryIndex {
+    const unsigned long long *tab;
+    const int32_t *hidx;
+    uint64_t mask;
+};
+__device__ __forceinline__ int64_t find_entry_h(const EntryIndex &X, int l, uint64_t k) {
+    if (l < 0 || !X.hidx) return -1;  // no entries (single-leaf tree): no table either
+    for (int x = 0; x < 2; x++) {
+        const uint64_t e = ent_make(l, k, x);
+        uint64_t s = hmix(e) & X.mask;
+        for (uint64_t p = 0; p <= X.mask; p++) {
+            const uint64_t v = X.tab[s];
+            if (v == e) return X.hidx[s];
+            if (v == ENT_EMPTY) break;
+            s = (s + 1) & X.mask;
+        }
     }
-    return (lo < end && (ent[lo] >> 1) == target) ? lo : -1;
+    return -1;
 }
-
-__device__ __forceinline__ int64_t node_index(const uint64_t *__restrict__ ent, const LevelTable &T, int l,
-                                              uint64_t k) {
+__device__ __forceinline__ int64_t node_index_h(const EntryIndex &X, const LevelTable &T, int l, uint64_t k) {
     if (l == 0) return k == 0 ? 0 : -1;
-    int64_t j = find_entry(ent, T, l - 1, k >> 2);
+    int64_t j = find_entry_h(X, l - 1, k >> 2);
     if (j < 0) return -1;
     return T.off[l] + 4 * (j - T.eoff[l - 1]) + (int64_t)(k & 3);
+}
+__global__ void k_hash_index(const uint64_t *__restrict__ ent, int64_t n_ent, const unsigned long long *__restrict__ tab,
+                             uint64_t mask, int32_t *__restrict__ hidx) {
+    pdl_trigger();
+    pdl_wait();
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n_ent; j += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t e = ent[j];
+        uint64_t s = hmix(e) & mask;
+        for (uint64_t p = 0; p <= mask; p++) {
+            if (tab[s] == e) {
+                hidx[s] = (int32_t)j;
+                break;
+            }
+            s = (s + 1) & mask;
+        }
+    }
 }
 
 __device__ __forceinline__ int64_t lower_bound_u64(const uint64_t *__restrict__ a, int64_t n, uint64_t v) {
@@ -381,11 +413,13 @@ __device__ __forceinline__ int64_t lower_bound_u64(const uint64_t *__restrict__ 
     return lo;
 }
 
-__global__ void k_nodes(LevelTable T, int64_t n_nodes, const uint64_t *__restrict__ ent,
+__global__ void k_nodes(LevelTable T, EntryIndex X, int64_t n_nodes, const uint64_t *__restrict__ ent,
                         const uint64_t *__restrict__ pkey, int64_t npts, uint64_t *__restrict__ nkey,
                         int8_t *__restrict__ nlev, uint8_t *__restrict__ nflag, int32_t *__restrict__ nbot,
                         int32_t *__restrict__ ntop, int32_t *__restrict__ nparent, int32_t *__restrict__ nchild,
                         int32_t *__restrict__ nent, int32_t *__restrict__ ncoll, int32_t *__restrict__ ent_node) {
+    pdl_trigger();
+    pdl_wait();
     for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < n_nodes; g += (int64_t)gridDim.x * blockDim.x) {
         int l = 0;
         while (l + 1 < T.L && T.off[l + 1] <= g) l++;
@@ -398,9 +432,9 @@ __global__ void k_nodes(LevelTable T, int64_t n_nodes, const uint64_t *__restric
             uint64_t pk = (pe >> 1) & KEY56;
             k = (pk << 2) | (uint64_t)(i & 3);
             if (pe & 1) f |= NF_FAKE;
-            parent = node_index(ent, T, l - 1, pk);
+            parent = node_index_h(X, T, l - 1, pk);
         }
-        int64_t j = find_entry(ent, T, l, k);
+        int64_t j = find_entry_h(X, l, k);
         int64_t child = -1;
         if (j >= 0) {
             f |= (ent[j] & 1) ? NF_XLIST : NF_SPLIT;
@@ -424,7 +458,7 @@ __global__ void k_nodes(LevelTable T, int64_t n_nodes, const uint64_t *__restric
             for (int dy = -1; dy <= 1; dy++) {
                 int64_t cx = ix + dx, cy = iy + dy, c = -1;
                 if (cx >= 0 && cy >= 0 && cx < side && cy < side)
-                    c = (dx == 0 && dy == 0) ? g : node_index(ent, T, l, morton((uint64_t)cx, (uint64_t)cy));
+                    c = (dx == 0 && dy == 0) ? g : node_index_h(X, T, l, morton((uint64_t)cx, (uint64_t)cy));
                 ncoll[9 * g + (dx + 1) * 3 + (dy + 1)] = (int32_t)c;
             }
     }
@@ -483,6 +517,8 @@ __global__ void __launch_bounds__(LT_THREADS) k_lists_count(int64_t n_nodes, con
                                                             const int32_t *__restrict__ nbot,
                                                             const int32_t *__restrict__ ntop, uint32_t *tcnt,
                                                             unsigned long long *cnt, unsigned long long *lcnt) {
+    pdl_trigger();
+    pdl_wait();
     __shared__ unsigned sm[32];
     __shared__ unsigned slv[MAX_LEVELS];
     if (threadIdx.x < MAX_LEVELS) slv[threadIdx.x] = 0;
@@ -514,6 +550,8 @@ __global__ void __launch_bounds__(LT_THREADS) k_lists_count(int64_t n_nodes, con
 }
 // one block: tile counts -> exclusive tile offsets (both lists); totals to cnt[0..1]
 __global__ void __launch_bounds__(1024) k_lists_scan(int64_t ntiles, uint32_t *tcnt, unsigned long long *cnt) {
+    pdl_trigger();
+    pdl_wait();
     __shared__ unsigned sm[32];
     unsigned carry0 = 0, carry1 = 0;
     for (int64_t base = 0; base < ntiles; base += blockDim.x) {
@@ -540,6 +578,8 @@ __global__ void __launch_bounds__(LT_THREADS) k_lists_write(int64_t n_nodes, con
                                                             const int32_t *__restrict__ ntop,
                                                             const uint32_t *__restrict__ tcnt, int32_t *leaf_list,
                                                             int32_t *p2m_list) {
+    pdl_trigger();
+    pdl_wait();
     __shared__ unsigned sm[32];
     unsigned oa = tcnt[2 * blockIdx.x], ob = tcnt[2 * blockIdx.x + 1];
     const int64_t g0 = (int64_t)blockIdx.x * LT_TILE;
@@ -627,8 +667,8 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     KIFMM_LAUNCHED();
     P->pkey.alloc(n); P->perm.alloc(n); P->key2.alloc(n); P->perm2.alloc(n);
     // the root box stays on the device until the counts below come back
-    k_keys_dev<<<gs, TB, 0, s>>>(P->x.p, P->y.p, n, P->opt.fix_bbox, P->scal.p, P->pkey.p, P->perm.p, P->scal.p + 8);
-    KIFMM_LAUNCHED();
+    launch_pdl(k_keys_dev, dim3(gs), dim3(TB), 0, s, (const double *)P->x.p, (const double *)P->y.p, n,
+               (int)P->opt.fix_bbox, (const unsigned long long *)P->scal.p, P->pkey.p, P->perm.p, P->scal.p + 8);
     // Sort by the top 32 key bits first (levels 1..16, four 8-bit passes): that
     // orders every cell of level <= 16, enough whenever no split lies deeper
     // than level 15.  Otherwise sort all 58 bits and count again.
@@ -644,8 +684,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     unsigned long long *st = sc + 5;
     for (int full = 0; full < 2; full++) {
         KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 5, 0, 3 * sizeof(unsigned long long), s));
-        k_t0<<<gs, TB, 0, s>>>(P->pkey.p, n, P->ppl, 0, H, P->scal.p);
-        KIFMM_LAUNCHED();
+        launch_pdl(k_t0, dim3(gs), dim3(TB), 0, s, (const uint64_t *)P->pkey.p, n, (int64_t)P->ppl, 0, H, P->scal.p);
         KIFMM_CUDA(cudaMemcpyAsync(sc, P->scal.p, sizeof(sc), cudaMemcpyDeviceToHost, s));
         KIFMM_CUDA(cudaStreamSynchronize(s));
         if (full == 0) {
@@ -663,8 +702,8 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
         radix_sort_pairs(P->pkey.p, P->perm.p, P->key2.p, P->perm2.p, n, 2 * KEY_DEPTH, P);
     }
     P->xs.alloc(n); P->ys.alloc(n);
-    k_gather2<<<gs, TB, 0, s>>>(P->x.p, P->y.p, P->perm.p, n, P->xs.p, P->ys.p);
-    KIFMM_LAUNCHED();
+    launch_pdl(k_gather2, dim3(gs), dim3(TB), 0, s, (const double *)P->x.p, (const double *)P->y.p,
+               (const int32_t *)P->perm.p, n, P->xs.p, P->ys.p);
     P->n_outside = (int64_t)st[3];
     KIFMM_REQUIRE(st[2] == 0, KIFMM_ERR_DEPTH,
                   "build_tree: more than Ncutoff points share one cell of the finest grid (2^29 per side); "
@@ -680,6 +719,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     unsigned long long *lc = (unsigned long long *)P->misc.p;  // [32] entries per level
     unsigned long long lcount[32] = {};
     if (L > 1) {
+        PhaseScope ph_c(P, KIFMM_PHASE_CLOSURE);
         P->grid_bar.alloc(2);
         static int coop_blocks[64] = {};  // co-resident blocks per SM of k_split_closure, per device
         if (P->device >= 0 && P->device < 64 && coop_blocks[P->device] == 0) {
@@ -693,6 +733,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
             uint64_t hcap = 1;
             while (hcap < 2 * cap) hcap <<= 1;
             P->hash.alloc(hcap);
+            P->hash_cap = hcap;
             P->list.alloc(cap);
             KIFMM_CUDA(cudaMemsetAsync(P->hash.p, 0xFF, hcap * sizeof(uint64_t), s));
             KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 9, 0, 3 * sizeof(unsigned long long), s));
@@ -738,6 +779,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     P->ent.alloc(n_ent);
     P->key2.alloc(std::max<int64_t>(n, n_ent));
     if (n_ent) {
+        PhaseScope ph_e(P, KIFMM_PHASE_ENTRIES);
         KIFMM_CUDA(cudaMemcpyAsync(P->ent.p, P->list.p, n_ent * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
         // entry = (level << 57) | (key << 1) | xlist with keys of at most 2(L-1)
         // bits: sort the digits holding key bits, then the level digit
@@ -769,12 +811,21 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     int64_t NN = off;
     KIFMM_REQUIRE(NN < (1ll << 31), KIFMM_ERR_ARG, "build_tree: too many nodes");
     P->n_nodes = NN;
+    std::optional<PhaseScope> ph_n;
+    ph_n.emplace(P, KIFMM_PHASE_NODES);
     P->nkey.alloc(NN); P->nlev.alloc(NN); P->nflag.alloc(NN); P->nbot.alloc(NN); P->ntop.alloc(NN);
     P->nparent.alloc(NN); P->nchild.alloc(NN); P->nent.alloc(NN); P->ncoll.alloc(9 * NN);
     P->ent_node.alloc(std::max<int64_t>(n_ent, 1));
     P->leaf_list.alloc(NN); P->p2m_list.alloc(NN);
     unsigned ng = grid_for(NN, TB, P->num_sms * 16);
-    k_nodes<<<ng, TB, 0, s>>>(T, NN, P->ent.p, P->pkey.p, n, P->nkey.p, P->nlev.p, P->nflag.p, P->nbot.p, P->ntop.p,
+    EntryIndex X{(const unsigned long long *)P->hash.p, nullptr, (uint64_t)(P->hash_cap - 1)};
+    if (n_ent) {
+        P->hash_idx.alloc(P->hash_cap);
+        X.hidx = P->hash_idx.p;
+        launch_pdl(k_hash_index, dim3(grid_for(n_ent, TB, P->num_sms * 8)), dim3(TB), 0, s, (const uint64_t *)P->ent.p,
+                   (int64_t)n_ent, X.tab, X.mask, P->hash_idx.p);
+    }
+    launch_pdl(k_nodes, dim3(ng), dim3(TB), 0, s, T, X, NN, P->ent.p, P->pkey.p, n, P->nkey.p, P->nlev.p, P->nflag.p, P->nbot.p, P->ntop.p,
                               P->nparent.p, P->nchild.p, P->nent.p, P->ncoll.p, P->ent_node.p);
     KIFMM_LAUNCHED();
     unsigned long long *cnt = (unsigned long long *)P->misc.p + 32;
@@ -784,12 +835,12 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     {
         const int64_t ntiles = (NN + LT_TILE - 1) / LT_TILE;
         P->list_tiles.alloc(2 * ntiles);
-        k_lists_count<<<(unsigned)ntiles, LT_THREADS, 0, s>>>(NN, P->nlev.p, P->nflag.p, P->nbot.p, P->ntop.p,
+        launch_pdl(k_lists_count, dim3((unsigned)ntiles), dim3(LT_THREADS), 0, s, NN, P->nlev.p, P->nflag.p, P->nbot.p, P->ntop.p,
                                                               P->list_tiles.p, cnt, lcnt);
         KIFMM_LAUNCHED();
-        k_lists_scan<<<1, 1024, 0, s>>>(ntiles, P->list_tiles.p, cnt);
+        launch_pdl(k_lists_scan, dim3(1), dim3(1024), 0, s, ntiles, P->list_tiles.p, cnt);
         KIFMM_LAUNCHED();
-        k_lists_write<<<(unsigned)ntiles, LT_THREADS, 0, s>>>(NN, P->nlev.p, P->nflag.p, P->nbot.p, P->ntop.p,
+        launch_pdl(k_lists_write, dim3((unsigned)ntiles), dim3(LT_THREADS), 0, s, NN, P->nlev.p, P->nflag.p, P->nbot.p, P->ntop.p,
                                                               P->list_tiles.p, P->leaf_list.p, P->p2m_list.p);
         KIFMM_LAUNCHED();
     }
@@ -804,6 +855,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     for (int l = 0; l < MAX_LEVELS; l++) P->leaf_loff[l + 1] = P->leaf_loff[l] + (int64_t)lv[l];
     KIFMM_REQUIRE(P->leaf_loff[MAX_LEVELS] == P->n_leaf_list, KIFMM_ERR_CUDA, "build_tree: inconsistent leaf counts");
     P->n_p2m_list = (int64_t)c5[1];
+    ph_n.reset();
     P->n_leaves = (int64_t)c5[2];
     P->n_fake = (int64_t)c5[3];
     P->n_xlist = (int64_t)c5[4];
