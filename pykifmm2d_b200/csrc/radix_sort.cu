@@ -161,12 +161,14 @@ __device__ __forceinline__ unsigned long long ld_relaxed_u64(const unsigned long
 // per-pass array in local memory), npass <= OS_MAX_PASSES
 __global__ void __launch_bounds__(RS_THREADS) k_os_hist(const uint64_t *__restrict__ key, int64_t n, uint64_t packed,
                                                          int npass, uint32_t *__restrict__ hist) {
+    // warp-private counters per pass (conflicts only among a warp's own lanes):
+    // dynamic shared memory [RS_WARPS][npass][256]
+    extern __shared__ uint32_t h_dyn[];
     pdl_trigger();
     pdl_wait();
-    __shared__ uint32_t h[OS_MAX_PASSES][256];
-    for (int i = threadIdx.x; i < OS_MAX_PASSES * 256; i += RS_THREADS) (&h[0][0])[i] = 0;
+    for (int i = threadIdx.x; i < RS_WARPS * npass * 256; i += RS_THREADS) h_dyn[i] = 0;
     __syncthreads();
-    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
     for (int64_t base = (int64_t)blockIdx.x * RS_TILE; base < n; base += (int64_t)gridDim.x * RS_TILE) {
         uint64_t k[RS_ITEMS];
 #pragma unroll
@@ -179,17 +181,16 @@ __global__ void __launch_bounds__(RS_THREADS) k_os_hist(const uint64_t *__restri
             if (p >= npass) break;
             const int sh = (int)((packed >> (8 * p)) & 63);
 #pragma unroll
-            for (int r = 0; r < RS_ITEMS; r++) {
-                const bool ok = base + r * RS_THREADS + threadIdx.x < n;
-                const uint32_t d = ok ? (uint32_t)((k[r] >> sh) & 255) : 256u;
-                const unsigned peers = __match_any_sync(0xffffffffu, d);  // one add per distinct digit
-                if (d < 256 && lane == __ffs(peers) - 1) atomicAdd(&h[p][d], (uint32_t)__popc(peers));
-            }
+            for (int r = 0; r < RS_ITEMS; r++)
+                if (base + r * RS_THREADS + threadIdx.x < n)
+                    atomicAdd(&h_dyn[(w * npass + p) * 256 + ((k[r] >> sh) & 255)], 1u);
         }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < npass * 256; i += RS_THREADS) {
-        const uint32_t c = (&h[0][0])[i];
+        uint32_t c = 0;
+#pragma unroll
+        for (int ww = 0; ww < RS_WARPS; ww++) c += h_dyn[ww * npass * 256 + i];
         if (c) atomicAdd(&hist[i], c);
     }
 }
@@ -355,7 +356,9 @@ static void os_run(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_
     const unsigned hg = (unsigned)std::min<int64_t>(ntiles, (int64_t)P->num_sms * 4);
     uint64_t packed = 0;
     for (int p = 0; p < npass; p++) packed |= (uint64_t)(shifts[p] & 63) << (8 * p);
-    launch_pdl(k_os_hist, dim3(hg), dim3(RS_THREADS), 0, s, (const uint64_t *)key, n, packed, npass, hist);
+    const size_t hsm = (size_t)RS_WARPS * npass * 256 * sizeof(uint32_t);
+    ensure_dyn_smem(k_os_hist, hsm);
+    launch_pdl(k_os_hist, dim3(hg), dim3(RS_THREADS), hsm, s, (const uint64_t *)key, n, packed, npass, hist);
     uint64_t *ka = key, *kb = key_tmp;
     int32_t *va = val, *vb = val_tmp;
     unsigned long long *err = P->scal.p + KIFMM_SCAL_SORT_ERR;

@@ -73,7 +73,19 @@ __global__ void k_bbox(const double *__restrict__ x, const double *__restrict__ 
         mxy = max(mxy, (uint64_t)__shfl_xor_sync(0xffffffffu, mxy, o));
         bad += __shfl_xor_sync(0xffffffffu, bad, o);
     }
+    // one global atomic per value and block (not per warp: they all hit the same words)
+    __shared__ unsigned long long red[5][32];
+    const int w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     if ((threadIdx.x & 31) == 0) {
+        red[0][w] = mnx; red[1][w] = mxx; red[2][w] = mny; red[3][w] = mxy; red[4][w] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int i = 1; i < nw; i++) {
+            mnx = min(mnx, (uint64_t)red[0][i]); mxx = max(mxx, (uint64_t)red[1][i]);
+            mny = min(mny, (uint64_t)red[2][i]); mxy = max(mxy, (uint64_t)red[3][i]);
+            bad += red[4][i];
+        }
         atomicMin(&scal[0], mnx); atomicMax(&scal[1], mxx);
         atomicMin(&scal[2], mny); atomicMax(&scal[3], mxy);
         if (bad) atomicAdd(&scal[4], bad);
