@@ -205,6 +205,7 @@ struct kifmm_plan {
     // scratch for the tree build
     kifmm::DBuf<uint64_t> key2, hash, list;
     uint64_t hash_cap = 1;            // slots of the split-cell hash table (power of two)
+    bool closure_plain = false;       // build the split-cell set with separate launches
     kifmm::DBuf<int32_t> hash_idx;    // [hash_cap] sorted entry index of the entry in each slot
     kifmm::DBuf<int32_t> perm2;
     kifmm::DBuf<uint32_t> sort_hist;

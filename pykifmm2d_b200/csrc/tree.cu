@@ -756,16 +756,26 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
             H.list = P->list.p;
             H.cap = cap;
             H.lcount = lc;
-            {
+            if (!P->closure_plain) {
                 const uint64_t *kp = P->pkey.p;
                 int64_t nn = n, ppl = P->ppl;
                 int LL = L;
                 unsigned *bar = P->grid_bar.p;
-                long long limit = 1ll << 22;
+                long long limit = 1ll << 20;
                 unsigned long long *err = P->scal.p + KIFMM_SCAL_TREE_ERR;
                 void *args[] = {(void *)&kp, (void *)&nn, (void *)&ppl, (void *)&H, (void *)&LL, (void *)&bar,
                                 (void *)&limit, (void *)&err};
                 KIFMM_CUDA(cudaLaunchCooperativeKernel((const void *)k_split_closure, cg, TB, args, 0, s));
+                KIFMM_LAUNCHED();
+            } else {  // the same steps as separate launches (no grid barrier)
+                k_t0<<<gs, TB, 0, s>>>(P->pkey.p, n, P->ppl, 1, H, P->scal.p);
+                KIFMM_LAUNCHED();
+                const unsigned rg = (unsigned)(P->num_sms * 4);
+                for (int l = L - 3; l >= 0; l--) {
+                    k_restrict<<<rg, TB, 0, s>>>(H, l);
+                    KIFMM_LAUNCHED();
+                }
+                k_xlist<<<rg, TB, 0, s>>>(H, L);
                 KIFMM_LAUNCHED();
             }
             if (!ops_started) {
@@ -778,7 +788,15 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
             KIFMM_CUDA(cudaMemcpyAsync(cv, P->scal.p + 9, sizeof(cv), cudaMemcpyDeviceToHost, s));
             KIFMM_CUDA(cudaMemcpyAsync(lcount, lc, sizeof(lcount), cudaMemcpyDeviceToHost, s));
             KIFMM_CUDA(cudaStreamSynchronize(s));
-            KIFMM_REQUIRE(cv[2] == 0, KIFMM_ERR_CUDA, "build_tree: a grid barrier wait timed out");
+            if (cv[2] != 0) {
+                // a grid-barrier wait of the cooperative closure ran out (its blocks
+                // were not all resident in time): this plan builds the set with
+                // separate launches from now on, starting with this attempt
+                KIFMM_REQUIRE(!P->closure_plain, KIFMM_ERR_CUDA, "build_tree: split-cell closure failed");
+                P->closure_plain = true;
+                attempt--;
+                continue;
+            }
             if (cv[1] == 0 && cv[0] <= cap) {
                 n_ent = (int64_t)cv[0];
                 break;
