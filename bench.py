@@ -303,9 +303,9 @@ def build_rooflines(cfg, info, phase, precision, pk, pk_src, n):
     if ts > 0:
         byts = 4 * 36.0 * n  # four 8-bit passes: histogram read + scatter read + write of 12 B per key
         ach = byts / ts / 1e9
-        out["sort"] = {"kernel": "radix sort (k_rs_hist/scan/scatter, 4 passes)", "bound": "hbm",
+        out["sort"] = {"kernel": "onesweep radix sort (k_os_hist + 4 k_os_pass)", "bound": "hbm",
                        "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": ach / pk["hbm_gbs"],
-                       "traffic": traffic.get("k_rs_scatter"),
+                       "traffic": traffic.get("k_os_pass"),
                        "work": "4 passes x 36 B per key (12 B key+index read twice, written once)",
                        "peak_source": pk_src}
     return out
