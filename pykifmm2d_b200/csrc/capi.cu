@@ -202,6 +202,7 @@ int kifmm_plan_create(const kifmm_kernel *kernel, int32_t nequiv, int32_t ncutof
             KIFMM_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, P->device));
             P->num_sms = sms > 0 ? sms : 148;
             prepare_pool(P->device);
+            init_log_table(P->device);
             if (o.stream) {
                 P->stream = (cudaStream_t)o.stream;
             } else {

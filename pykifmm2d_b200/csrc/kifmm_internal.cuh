@@ -366,6 +366,7 @@ void export_tree(kifmm_plan *P, int64_t *nodes, int64_t *point_leaf);
 void tree_stats(kifmm_plan *P);
 // operators.cu
 void build_operators(kifmm_plan *P);
+void init_log_table(int device);     // table of the Laplace P2M logarithm, once per device
 void start_operators(kifmm_plan *P);  // build_operators on the side stream
 cudaStream_t device_side_stream(int device);  // one per device, created on first use
 void join_operators(kifmm_plan *P);   // main stream waits for it

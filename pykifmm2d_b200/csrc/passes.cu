@@ -28,15 +28,56 @@ __global__ void k_scatter_pot(const double *__restrict__ pots, const int32_t *__
         pot[perm[i]] = pots[i];
 }
 
+// Natural logarithm for the Laplace P2M sums, table-driven (P. T. P. Tang,
+// "Table-driven implementation of the logarithm function in IEEE
+// floating-point arithmetic", ACM TOMS 16, 1990): x = 2^e m with m in [1, 2),
+// c_i = 1 + (i + 1/2)/128 the midpoint of m's subinterval, r = m / c_i - 1
+// (|r| < 2^-8), ln x = e ln2 + ln c_i + log1p(r) with log1p by its series to
+// r^7 (the next term is below 2^-67).  ln c_i and 1/c_i are computed on the
+// host in long double (init_log_table) and staged in shared memory.
+__device__ double g_logtab[256];  // [0..127] ln c_i, [128..255] 1 / c_i
+constexpr double LN2_HI = 6.93147180369123816490e-01, LN2_LO = 1.90821492927058770002e-10;
+__device__ __forceinline__ double ln_tab(double x, const double *lt) {
+    const long long b = __double_as_longlong(x);
+    const int e = (int)((b >> 52) & 0x7ff) - 1023;
+    const int i = (int)((b >> 45) & 127);
+    const double m = __longlong_as_double((b & 0x000fffffffffffffll) | 0x3ff0000000000000ll);
+    const double r = fma(m, lt[128 + i], -1.0);
+    double p = 1.0 / 7.0;
+    p = fma(p, r, -1.0 / 6.0);
+    p = fma(p, r, 1.0 / 5.0);
+    p = fma(p, r, -1.0 / 4.0);
+    p = fma(p, r, 1.0 / 3.0);
+    p = fma(p, r, -0.5);
+    p = fma(p * r, r, r);  // r + r^2 (-1/2 + r (1/3 - ...))
+    return fma((double)e, LN2_HI, lt[i] + fma((double)e, LN2_LO, p));
+}
+void init_log_table(int device) {
+    static bool done[64] = {};
+    if (device < 0 || device >= 64 || done[device]) return;
+    double t[256];
+    for (int i = 0; i < 128; i++) {
+        const long double c = 1.0L + ((long double)i + 0.5L) / 128.0L;
+        t[i] = (double)logl(c);
+        t[128 + i] = (double)(1.0L / c);
+    }
+    KIFMM_CUDA(cudaMemcpyToSymbol(g_logtab, t, sizeof(t)));
+    done[device] = true;
+}
+
 // P2M (numba_upwards_pass, class_fmm.py:57-71): one warp per node; lane q
 // accumulates over the node's sources, which the warp stages 32 at a time
-// in shared memory.
+// in shared memory.  Laplace sums tau log(r^2) with ln_tab and scales once.
 constexpr int P2M_WARPS = 8;
 __global__ void __launch_bounds__(32 * P2M_WARPS) k_p2m_d(PassArgs A, const int32_t *__restrict__ list,
                                                            int64_t nlist) {
     __shared__ double sx[P2M_WARPS][32], sy[P2M_WARPS][32], st[P2M_WARPS][32];
+    __shared__ double lt[256];
+    for (int i = threadIdx.x; i < 256; i += blockDim.x) lt[i] = g_logtab[i];
+    __syncthreads();
     pdl_trigger();
     pdl_wait();
+    const bool lap = A.kind == KIFMM_KERNEL_LAPLACE;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     if (w >= nlist) return;
@@ -61,18 +102,32 @@ __global__ void __launch_bounds__(32 * P2M_WARPS) k_p2m_d(PassArgs A, const int3
             __syncwarp();
             const int ns = min(32, e - s0);
             int u = 0;
-            for (; u + 1 < ns; u += 2) {
-                double dx0 = tx - sx[wib][u], dy0 = ty - sy[wib][u];
-                double dx1 = tx - sx[wib][u + 1], dy1 = ty - sy[wib][u + 1];
-                acc0 += green_d(A.kind, A.k, dx0 * dx0 + dy0 * dy0) * st[wib][u];
-                acc1 += green_d(A.kind, A.k, dx1 * dx1 + dy1 * dy1) * st[wib][u + 1];
-            }
-            if (u < ns) {
-                double dx = tx - sx[wib][u], dy = ty - sy[wib][u];
-                acc0 += green_d(A.kind, A.k, dx * dx + dy * dy) * st[wib][u];
+            if (lap) {
+                for (; u + 1 < ns; u += 2) {
+                    double dx0 = tx - sx[wib][u], dy0 = ty - sy[wib][u];
+                    double dx1 = tx - sx[wib][u + 1], dy1 = ty - sy[wib][u + 1];
+                    acc0 = fma(ln_tab(dx0 * dx0 + dy0 * dy0, lt), st[wib][u], acc0);
+                    acc1 = fma(ln_tab(dx1 * dx1 + dy1 * dy1, lt), st[wib][u + 1], acc1);
+                }
+                if (u < ns) {
+                    double dx = tx - sx[wib][u], dy = ty - sy[wib][u];
+                    acc0 = fma(ln_tab(dx * dx + dy * dy, lt), st[wib][u], acc0);
+                }
+            } else {
+                for (; u + 1 < ns; u += 2) {
+                    double dx0 = tx - sx[wib][u], dy0 = ty - sy[wib][u];
+                    double dx1 = tx - sx[wib][u + 1], dy1 = ty - sy[wib][u + 1];
+                    acc0 += green_d(A.kind, A.k, dx0 * dx0 + dy0 * dy0) * st[wib][u];
+                    acc1 += green_d(A.kind, A.k, dx1 * dx1 + dy1 * dy1) * st[wib][u + 1];
+                }
+                if (u < ns) {
+                    double dx = tx - sx[wib][u], dy = ty - sy[wib][u];
+                    acc0 += green_d(A.kind, A.k, dx * dx + dy * dy) * st[wib][u];
+                }
             }
         }
-        if (ok) A.uup[(size_t)g * A.Q + q] = acc0 + acc1;
+        // Laplace: G = -log(r^2) / (4 pi)
+        if (ok) A.uup[(size_t)g * A.Q + q] = lap ? -0.07957747154594767 * (acc0 + acc1) : acc0 + acc1;
     }
 }
 
