@@ -175,7 +175,6 @@ struct kifmm_plan {
     kifmm::DBuf<int32_t> ncoll;      // [n_nodes][9] colleagues by direction (dx+1)*3+(dy+1)
     kifmm::DBuf<int32_t> leaf_list, p2m_list;
     kifmm::DBuf<uint32_t> list_tiles;
-    kifmm::DBuf<unsigned> grid_bar;  // grid barrier of the split-cell closure  // per-tile counts/offsets while the lists are built
     int64_t n_leaf_list = 0, n_p2m_list = 0;
     int64_t leaf_loff[KIFMM_MAX_LEVELS + 1] = {};  // leaf_list range of each level
     int64_t n_leaves = 0, n_fake = 0, n_xlist = 0;
@@ -205,7 +204,6 @@ struct kifmm_plan {
     // scratch for the tree build
     kifmm::DBuf<uint64_t> key2, hash, list;
     uint64_t hash_cap = 1;            // slots of the split-cell hash table (power of two)
-    bool closure_plain = false;       // build the split-cell set with separate launches
     kifmm::DBuf<int32_t> hash_idx;    // [hash_cap] sorted entry index of the entry in each slot
     kifmm::DBuf<int32_t> perm2;
     kifmm::DBuf<uint32_t> sort_hist;
@@ -258,7 +256,6 @@ inline void ensure_dyn_smem(K *fn, size_t bytes) {
 // device scalar slots (plan->scal) holding error flags that the host reads
 // after an apply: a bulk-copy wait in the level passes that ran out, and an
 // MMA completion wait in the tensor-core M2L that ran out
-constexpr int KIFMM_SCAL_TREE_ERR = 11;  // a grid-barrier wait in the split-cell closure that ran out
 constexpr int KIFMM_SCAL_SORT_ERR = 13;  // a radix-sort look-back wait that ran out
 constexpr int KIFMM_SCAL_PASS_ERR = 14;
 constexpr int KIFMM_SCAL_TC_ERR = 15;

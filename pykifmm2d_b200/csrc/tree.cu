@@ -10,15 +10,17 @@
 //     (tree.py:242): found from the sorted keys in one pass -- point i reports
 //     the cells it opens whose window [i, i+Ncutoff] stays inside them;
 //   * level restriction (tree.py:533-545, numba_get_bads :432-444) is the
-//     closure Split_l = Split0_l U N9(parent(Split_{l+1})), computed level by
-//     level from the deepest one (N9 = the 3x3 block of cells in the domain);
+//     closure Split_l = Split0_l U N9(parent(Split_{l+1})) (N9 = the 3x3
+//     block of cells in the domain), built by chains of rectangles from the
+//     T0 cells in one launch (k_closure);
 //   * X-list (tree.py:546-576, numba_get_Xlist :446-458): a real leaf with a
 //     split colleague gets four fake children;
 //   * nodes of level l+1 are the four children of every split or X-list cell
 //     of level l, in Morton order; colleagues (tree.py:260-294) are the
 //     existing same-level cells of the 3x3 block, stored by direction.
-// Split and X-list cells live in a device hash set while they are collected,
-// then in one sorted list that every lookup binary-searches.
+// Split and X-list cells live in a device hash set; once collected they are
+// sorted into one list, and lookups probe the table, which maps each entry to
+// its sorted position (k_hash_index).
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -183,24 +185,23 @@ __device__ __forceinline__ uint64_t ent_make(int l, uint64_t k, int x) {
     return ((uint64_t)l << ENT_LEVEL_SHIFT) | (k << 1) | (uint64_t)x;
 }
 
-__device__ void hs_insert(const HashSet &H, uint64_t e) {
+// Claim entry e in the table: true iff this call stored it (the caller then
+// appends it to the list).  A plain read comes first, so that the many probes
+// of cells that are already in the set take no atomic.
+__device__ __forceinline__ bool hs_claim(const HashSet &H, uint64_t e) {
     uint64_t s = hmix(e) & H.mask;
     for (uint64_t p = 0; p <= H.mask; p++) {
-        unsigned long long prev = atomicCAS(&H.tab[s], (unsigned long long)ENT_EMPTY, (unsigned long long)e);
-        if (prev == ENT_EMPTY) {
-            unsigned long long idx = atomicAdd(H.count, 1ull);
-            if (idx < H.cap) {
-                H.list[idx] = e;
-                atomicAdd(&H.lcount[(int)(e >> ENT_LEVEL_SHIFT)], 1ull);
-            } else {
-                atomicOr(H.ovf, 1ull);
-            }
-            return;
+        const uint64_t v = ((volatile unsigned long long *)H.tab)[s];
+        if (v == e) return false;
+        if (v == ENT_EMPTY) {
+            const unsigned long long prev = atomicCAS(&H.tab[s], (unsigned long long)ENT_EMPTY, (unsigned long long)e);
+            if (prev == ENT_EMPTY) return true;
+            if (prev == e) return false;
         }
-        if (prev == e) return;
         s = (s + 1) & H.mask;
     }
     atomicOr(H.ovf, 2ull);
+    return false;
 }
 
 __device__ bool hs_has(const HashSet &H, uint64_t e) {
@@ -214,24 +215,30 @@ __device__ bool hs_has(const HashSet &H, uint64_t e) {
     return false;
 }
 
-// Split cells of the unrestricted tree.  Point i (sorted) is the first point
-// of its level-l cell for l > common_level(key[i-1], key[i]); that cell holds
-// more than ppl points iff l <= common_level(key[i], key[i+ppl]).
-// mode 0: count + deepest level; mode 1: insert.
-// scal[5]: count, scal[6]: deepest split level + 1, scal[7]: depth overflow
-// T0 split cells opened by sorted point i (mode 1 of k_t0)
-__device__ __forceinline__ void t0_insert(const uint64_t *__restrict__ key, int64_t n, int64_t ppl, const HashSet &H,
-                                          int64_t i) {
-    if (i + ppl >= n) return;
-    const uint64_t k = key[i];
-    int hi = common_level(k, key[i + ppl]);
-    if (hi >= KEY_DEPTH) hi = KEY_DEPTH - 1;
-    const int lo = i == 0 ? -1 : common_level(key[i - 1], k);
-    for (int l = lo + 1; l <= hi; l++) hs_insert(H, ent_make(l, k >> (2 * (KEY_DEPTH - l)), 0));
+// Append the claimed entries of a warp (lanes in `fm`, all of level l) with
+// one atomic on the list count and one on the level count.
+__device__ __forceinline__ void warp_append(const HashSet &H, unsigned fm, uint64_t e, int l, int lane) {
+    if (!fm) return;
+    const int lead = __ffs(fm) - 1;
+    unsigned long long base = 0;
+    if (lane == lead) {
+        base = atomicAdd(H.count, (unsigned long long)__popc(fm));
+        atomicAdd(&H.lcount[l], (unsigned long long)__popc(fm));
+    }
+    base = __shfl_sync(0xffffffffu, base, lead);
+    if ((fm >> lane) & 1) {
+        const unsigned long long idx = base + __popc(fm & ((1u << lane) - 1));
+        if (idx < H.cap) H.list[idx] = e;
+        else atomicOr(H.ovf, 1ull);
+    }
 }
 
-__global__ void k_t0(const uint64_t *__restrict__ key, int64_t n, int64_t ppl, int mode, HashSet H,
-                     unsigned long long *scal) {
+// Split cells of the unrestricted tree (T0).  Point i (sorted) is the first
+// point of its level-l cell for l > common_level(key[i-1], key[i]); that cell
+// holds more than ppl points iff l <= common_level(key[i], key[i+ppl]).
+// Counting pass: scal[5] cell count, scal[6] deepest split level + 1,
+// scal[7] depth overflow.
+__global__ void k_t0_count(const uint64_t *__restrict__ key, int64_t n, int64_t ppl, unsigned long long *scal) {
     pdl_trigger();
     pdl_wait();
     unsigned long long cnt = 0;
@@ -244,59 +251,83 @@ __global__ void k_t0(const uint64_t *__restrict__ key, int64_t n, int64_t ppl, i
         if (hi >= KEY_DEPTH) { over = true; hi = KEY_DEPTH - 1; }
         int lo = i == 0 ? -1 : common_level(key[i - 1], k);
         if (hi <= lo) continue;
-        if (mode == 0) {
-            cnt += (unsigned long long)(hi - lo);
-            deepest = max(deepest, hi + 1);
-        } else {
-            for (int l = lo + 1; l <= hi; l++) hs_insert(H, ent_make(l, k >> (2 * (KEY_DEPTH - l)), 0));
-        }
+        cnt += (unsigned long long)(hi - lo);
+        deepest = max(deepest, hi + 1);
     }
-    if (mode == 0) {
-        for (int o = 16; o; o >>= 1) {
-            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-            deepest = max(deepest, __shfl_xor_sync(0xffffffffu, deepest, o));
-        }
-        over = __any_sync(0xffffffffu, over);
-        if ((threadIdx.x & 31) == 0) {
-            if (cnt) atomicAdd(&scal[5], cnt);
-            atomicMax(&scal[6], (unsigned long long)deepest);
-            if (over) atomicOr(&scal[7], 1ull);
-        }
+    for (int o = 16; o; o >>= 1) {
+        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        deepest = max(deepest, __shfl_xor_sync(0xffffffffu, deepest, o));
+    }
+    over = __any_sync(0xffffffffu, over);
+    if ((threadIdx.x & 31) == 0) {
+        if (cnt) atomicAdd(&scal[5], cnt);
+        atomicMax(&scal[6], (unsigned long long)deepest);
+        if (over) atomicOr(&scal[7], 1ull);
     }
 }
 
-// Restriction step for level l: every split cell s of level l+1 forces the
-// 3x3 block around parent(s) to be split.  One work item per (cell, neighbour):
-// the inserts are independent, so none waits on another's atomic.
-__device__ __forceinline__ void restrict_item(const HashSet &H, int l, int64_t j) {
-    const int64_t i = j / 9;
-    const int d = (int)(j - 9 * i);
-    const uint64_t e = H.list[i];
-    if ((int)(e >> ENT_LEVEL_SHIFT) != l + 1 || (e & 1)) return;
-    const int64_t side = 1ll << l;
-    const uint64_t p = ((e >> 1) & KEY56) >> 2;
-    const int64_t qx = (int64_t)compact2(p >> 1) + d / 3 - 1, qy = (int64_t)compact2(p) + d % 3 - 1;
-    if (qx < 0 || qy < 0 || qx >= side || qy >= side) return;
-    hs_insert(H, ent_make(l, morton((uint64_t)qx, (uint64_t)qy), 0));
+// Level restriction (tree.py:533-545) as chains instead of a level-by-level
+// sweep.  The restricted set is the smallest S containing T0 with
+// N9(parent(x)) in S for every x in S (N9 = the 3x3 block of cells in the
+// domain).  N9 o parent maps a rectangle of cells to a rectangle (at most
+// 5 x 5: widths w -> w/2 + 2 settle at 4) and distributes over unions, so the
+// set is built by chains: the chain of T0 cell x inserts R = N9(parent(x)),
+// then N9(parent(R)), ..., and stops after a level where it stored nothing new.
+// That is complete: every cell of S was stored first either by T0 (and then
+// has its own chain) or by a chain, which then went on one level with a
+// rectangle containing the cell's N9(parent).  One warp runs a chain, a lane
+// per cell of the rectangle.
+__device__ void t0_chain(const HashSet &H, int l0, uint64_t c0, int lane) {
+    {
+        const uint64_t e = ent_make(l0, c0, 0);
+        const bool fresh = lane == 0 && hs_claim(H, e);
+        warp_append(H, __ballot_sync(0xffffffffu, fresh), e, l0, lane);
+    }
+    int64_t x0 = (int64_t)compact2(c0 >> 1), y0 = (int64_t)compact2(c0), x1 = x0, y1 = y0;
+    for (int l = l0 - 1; l >= 0; l--) {
+        const int64_t top = (1ll << l) - 1;
+        x0 = max((x0 >> 1) - 1, (int64_t)0); x1 = min((x1 >> 1) + 1, top);
+        y0 = max((y0 >> 1) - 1, (int64_t)0); y1 = min((y1 >> 1) + 1, top);
+        const int w = (int)(x1 - x0 + 1), h = (int)(y1 - y0 + 1);
+        uint64_t e = 0;
+        bool fresh = false;
+        if (lane < w * h) {
+            const int64_t cx = x0 + lane % w, cy = y0 + lane / w;
+            e = ent_make(l, morton((uint64_t)cx, (uint64_t)cy), 0);
+            fresh = hs_claim(H, e);
+        }
+        const unsigned fm = __ballot_sync(0xffffffffu, fresh);
+        warp_append(H, fm, e, l, lane);
+        if (!fm) break;
+    }
 }
 
-// X-list: for levels 1..L-2, a real leaf (cell not split, parent split) next
-// to a split cell becomes an X-list cell.  One work item per (cell, neighbour).
-__device__ __forceinline__ void xlist_item(const HashSet &H, int L, int64_t j) {
-    const int64_t i = j / 9;
-    const int d = (int)(j - 9 * i);
-    if (d == 4) return;
-    const uint64_t e = H.list[i];
-    const int l = (int)(e >> ENT_LEVEL_SHIFT);
-    if ((e & 1) || l < 1 || l > L - 2) return;
-    const uint64_t k = (e >> 1) & KEY56;
-    const int64_t cx = (int64_t)compact2(k >> 1) + d / 3 - 1, cy = (int64_t)compact2(k) + d % 3 - 1;
-    const int64_t side = 1ll << l;
-    if (cx < 0 || cy < 0 || cx >= side || cy >= side) return;
-    const uint64_t c = morton((uint64_t)cx, (uint64_t)cy);
-    if (hs_has(H, ent_make(l, c, 0))) return;
-    if (!hs_has(H, ent_make(l - 1, c >> 2, 0))) return;
-    hs_insert(H, ent_make(l, c, 1));
+// T0 cells and their restriction chains: one warp per 32 sorted points; each
+// point that opens split cells (levels lo+1..hi) runs their chains, deepest
+// first, so that the chains of its coarser cells mostly find their cells in
+// the set and stop after one level.
+__global__ void __launch_bounds__(256) k_closure(const uint64_t *__restrict__ key, int64_t n, int64_t ppl,
+                                                 HashSet H) {
+    pdl_trigger();
+    pdl_wait();
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; w * 32 + ppl < n; w += nw) {
+        const int64_t i = w * 32 + lane;
+        int lo = 0, hi = -1;
+        uint64_t k = 0;
+        if (i + ppl < n) {
+            k = key[i];
+            hi = min(common_level(k, key[i + ppl]), KEY_DEPTH - 1);
+            lo = i == 0 ? -1 : common_level(key[i - 1], k);
+        }
+        for (unsigned om = __ballot_sync(0xffffffffu, hi > lo); om; om &= om - 1) {
+            const int src = __ffs(om) - 1;
+            const uint64_t ks = __shfl_sync(0xffffffffu, k, src);
+            const int los = __shfl_sync(0xffffffffu, lo, src), his = __shfl_sync(0xffffffffu, hi, src);
+            for (int l = his; l > los; l--) t0_chain(H, l, ks >> (2 * (KEY_DEPTH - l)), lane);
+        }
+    }
 }
 
 __device__ __forceinline__ unsigned long long hs_count(const HashSet &H) {
@@ -304,68 +335,53 @@ __device__ __forceinline__ unsigned long long hs_count(const HashSet &H) {
     return n > H.cap ? H.cap : n;
 }
 
-__global__ void k_restrict(HashSet H, int l) {
+// X-list (tree.py:546-576, numba_get_Xlist :446-458): for levels 1..L-2, a
+// real leaf (cell not split, parent split) next to a split cell becomes an
+// X-list cell.  One item per (split cell, neighbour); the warp's new cells are
+// appended together (one count atomic per warp, one level atomic per level).
+__global__ void __launch_bounds__(256) k_xlist(HashSet H, int L) {
+    pdl_trigger();
+    pdl_wait();
     const unsigned long long n = hs_count(H);
-    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < 9 * (int64_t)n;
-         j += (int64_t)gridDim.x * blockDim.x)
-        restrict_item(H, l, j);
-}
-
-__global__ void k_xlist(HashSet H, int L) {
-    const unsigned long long n = hs_count(H);
-    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < 9 * (int64_t)n;
-         j += (int64_t)gridDim.x * blockDim.x)
-        xlist_item(H, L, j);
-}
-
-// Grid-wide barrier for a cooperative launch: bar[0] arrivals, bar[1]
-// generation.  A wait that runs past `limit` polls returns false.
-__device__ bool grid_barrier(unsigned *bar, long long limit) {
-    __shared__ int ok_s;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        volatile unsigned *gen = bar + 1;
-        const unsigned g = *gen;
-        __threadfence();
-        int ok = 1;
-        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
-            atomicExch(bar, 0u);
-            __threadfence();
-            atomicAdd(bar + 1, 1u);
-        } else {
-            for (long long it = 0; *gen == g; it++)
-                if (it > limit) {
-                    ok = 0;
-                    break;
+    const int lane = threadIdx.x & 31;
+    const int64_t total = 9 * (int64_t)n, stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t base = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) & ~(int64_t)31; base < total;
+         base += stride) {
+        const int64_t j = base + lane;
+        bool fresh = false;
+        uint64_t e = 0;
+        int l = 0;
+        if (j < total) {
+            const int64_t i = j / 9;
+            const int d = (int)(j - 9 * i);
+            const uint64_t s = H.list[i];
+            l = (int)(s >> ENT_LEVEL_SHIFT);
+            if (d != 4 && !(s & 1) && l >= 1 && l <= L - 2) {
+                const uint64_t k = (s >> 1) & KEY56;
+                const int64_t cx = (int64_t)compact2(k >> 1) + d / 3 - 1, cy = (int64_t)compact2(k) + d % 3 - 1;
+                const int64_t side = 1ll << l;
+                if (cx >= 0 && cy >= 0 && cx < side && cy < side) {
+                    const uint64_t c = morton((uint64_t)cx, (uint64_t)cy);
+                    if (!hs_has(H, ent_make(l, c, 0)) && hs_has(H, ent_make(l - 1, c >> 2, 0))) {
+                        e = ent_make(l, c, 1);
+                        fresh = hs_claim(H, e);
+                    }
                 }
+            }
         }
-        __threadfence();
-        ok_s = ok;
-    }
-    __syncthreads();
-    return ok_s != 0;
-}
-
-// The whole split-cell set in one cooperative launch: T0 inserts, the
-// restriction closure from level L-3 up to 0 (a grid barrier between levels,
-// as each level reads the cells the level below added), then the X-list.
-// Fourteen launches and their gaps become fifteen barriers.
-__global__ void __launch_bounds__(256) k_split_closure(const uint64_t *__restrict__ key, int64_t n, int64_t ppl,
-                                                       HashSet H, int L, unsigned *bar, long long limit,
-                                                       unsigned long long *err) {
-    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x, stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t i = tid; i < n; i += stride) t0_insert(key, n, ppl, H, i);
-    bool ok = grid_barrier(bar, limit);
-    for (int l = L - 3; l >= 0 && ok; l--) {
-        const unsigned long long cnt = hs_count(H);
-        for (int64_t j = tid; j < 9 * (int64_t)cnt; j += stride) restrict_item(H, l, j);
-        ok = grid_barrier(bar, limit);
-    }
-    if (ok) {
-        const unsigned long long cnt = hs_count(H);
-        for (int64_t j = tid; j < 9 * (int64_t)cnt; j += stride) xlist_item(H, L, j);
-    } else if (threadIdx.x == 0) {
-        atomicOr(err, 1ull);
+        const unsigned fm = __ballot_sync(0xffffffffu, fresh);
+        if (!fm) continue;
+        const int lead = __ffs(fm) - 1;
+        unsigned long long b0 = 0;
+        if (lane == lead) b0 = atomicAdd(H.count, (unsigned long long)__popc(fm));
+        b0 = __shfl_sync(0xffffffffu, b0, lead);
+        if (fresh) {
+            const unsigned peers = __match_any_sync(fm, l);
+            if (lane == __ffs(peers) - 1) atomicAdd(&H.lcount[l], (unsigned long long)__popc(peers));
+            const unsigned long long idx = b0 + __popc(fm & ((1u << lane) - 1));
+            if (idx < H.cap) H.list[idx] = e;
+            else atomicOr(H.ovf, 1ull);
+        }
     }
 }
 
@@ -696,7 +712,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     unsigned long long *st = sc + 5;
     for (int full = 0; full < 2; full++) {
         KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 5, 0, 3 * sizeof(unsigned long long), s));
-        launch_pdl(k_t0, dim3(gs), dim3(TB), 0, s, (const uint64_t *)P->pkey.p, n, (int64_t)P->ppl, 0, H, P->scal.p);
+        launch_pdl(k_t0_count, dim3(gs), dim3(TB), 0, s, (const uint64_t *)P->pkey.p, n, (int64_t)P->ppl, P->scal.p);
         KIFMM_CUDA(cudaMemcpyAsync(sc, P->scal.p, sizeof(sc), cudaMemcpyDeviceToHost, s));
         KIFMM_CUDA(cudaStreamSynchronize(s));
         if (full == 0) {
@@ -732,14 +748,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     unsigned long long lcount[32] = {};
     if (L > 1) {
         PhaseScope ph_c(P, KIFMM_PHASE_CLOSURE);
-        P->grid_bar.alloc(2);
-        static int coop_blocks[64] = {};  // co-resident blocks per SM of k_split_closure, per device
-        if (P->device >= 0 && P->device < 64 && coop_blocks[P->device] == 0) {
-            int nb = 0;
-            KIFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_split_closure, TB, 0));
-            coop_blocks[P->device] = std::max(1, std::min(nb, 2));
-        }
-        const unsigned cg = (unsigned)(coop_blocks[P->device] * P->num_sms);
+        const unsigned cgrid = grid_for((n + 31) / 32 * 32, TB, P->num_sms * 64);
         for (int attempt = 0;; attempt++) {
             uint64_t cap = (t0count * 16 + 4096) << (2 * attempt);
             uint64_t hcap = 1;
@@ -748,55 +757,28 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
             P->hash_cap = hcap;
             P->list.alloc(cap);
             KIFMM_CUDA(cudaMemsetAsync(P->hash.p, 0xFF, hcap * sizeof(uint64_t), s));
-            KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 9, 0, 3 * sizeof(unsigned long long), s));
+            KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 9, 0, 2 * sizeof(unsigned long long), s));
             KIFMM_CUDA(cudaMemsetAsync(lc, 0, 32 * sizeof(unsigned long long), s));
-            KIFMM_CUDA(cudaMemsetAsync(P->grid_bar.p, 0, 2 * sizeof(unsigned), s));
             H.tab = (unsigned long long *)P->hash.p;
             H.mask = hcap - 1;
             H.list = P->list.p;
             H.cap = cap;
             H.lcount = lc;
-            if (!P->closure_plain) {
-                const uint64_t *kp = P->pkey.p;
-                int64_t nn = n, ppl = P->ppl;
-                int LL = L;
-                unsigned *bar = P->grid_bar.p;
-                long long limit = 1ll << 20;
-                unsigned long long *err = P->scal.p + KIFMM_SCAL_TREE_ERR;
-                void *args[] = {(void *)&kp, (void *)&nn, (void *)&ppl, (void *)&H, (void *)&LL, (void *)&bar,
-                                (void *)&limit, (void *)&err};
-                KIFMM_CUDA(cudaLaunchCooperativeKernel((const void *)k_split_closure, cg, TB, args, 0, s));
-                KIFMM_LAUNCHED();
-            } else {  // the same steps as separate launches (no grid barrier)
-                k_t0<<<gs, TB, 0, s>>>(P->pkey.p, n, P->ppl, 1, H, P->scal.p);
-                KIFMM_LAUNCHED();
-                const unsigned rg = (unsigned)(P->num_sms * 4);
-                for (int l = L - 3; l >= 0; l--) {
-                    k_restrict<<<rg, TB, 0, s>>>(H, l);
-                    KIFMM_LAUNCHED();
-                }
-                k_xlist<<<rg, TB, 0, s>>>(H, L);
-                KIFMM_LAUNCHED();
-            }
+            launch_pdl(k_closure, dim3(cgrid), dim3(TB), 0, s, (const uint64_t *)P->pkey.p, n, (int64_t)P->ppl, H);
+            // the X-list reads the complete split set: nine items per entry
+            // (at most cap entries), one wave of blocks for the usual sizes
+            launch_pdl(k_xlist, dim3(grid_for(9 * (int64_t)std::min<uint64_t>(cap, 4 * t0count + 4096), TB,
+                                              P->num_sms * 8)),
+                       dim3(TB), 0, s, H, L);
             if (!ops_started) {
-                // the operators overlap the rest of the tree build; queued after the
-                // cooperative launch, which needs its blocks resident at once
+                // the operators overlap the rest of the tree build
                 start_operators(P);
                 ops_started = true;
             }
-            unsigned long long cv[3];
+            unsigned long long cv[2];
             KIFMM_CUDA(cudaMemcpyAsync(cv, P->scal.p + 9, sizeof(cv), cudaMemcpyDeviceToHost, s));
             KIFMM_CUDA(cudaMemcpyAsync(lcount, lc, sizeof(lcount), cudaMemcpyDeviceToHost, s));
             KIFMM_CUDA(cudaStreamSynchronize(s));
-            if (cv[2] != 0) {
-                // a grid-barrier wait of the cooperative closure ran out (its blocks
-                // were not all resident in time): this plan builds the set with
-                // separate launches from now on, starting with this attempt
-                KIFMM_REQUIRE(!P->closure_plain, KIFMM_ERR_CUDA, "build_tree: split-cell closure failed");
-                P->closure_plain = true;
-                attempt--;
-                continue;
-            }
             if (cv[1] == 0 && cv[0] <= cap) {
                 n_ent = (int64_t)cv[0];
                 break;
