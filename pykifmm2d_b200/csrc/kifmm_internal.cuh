@@ -260,6 +260,22 @@ constexpr int KIFMM_SCAL_SORT_ERR = 13;  // a radix-sort look-back wait that ran
 constexpr int KIFMM_SCAL_PASS_ERR = 14;
 constexpr int KIFMM_SCAL_TC_ERR = 15;
 
+// Lanes of the warp holding the same 8-bit digit d (d = 256: no key; such
+// lanes match each other only): nine ballots, one per bit, each lane keeping
+// the lanes that agree with it on every bit.  All 32 lanes must call it.
+// __match_any_sync gives the same mask, but its throughput falls with the
+// number of distinct values in the warp, which for radix digits is high.
+__device__ __forceinline__ unsigned warp_match_digit(uint32_t d) {
+    unsigned m = 0xffffffffu;
+#pragma unroll
+    for (int b = 0; b < 9; b++) {
+        const bool bit = (d >> b) & 1u;
+        const unsigned bb = __ballot_sync(0xffffffffu, bit);
+        m &= bit ? bb : ~bb;
+    }
+    return m;
+}
+
 struct PhaseScope {
     kifmm_plan *P;
     int id;

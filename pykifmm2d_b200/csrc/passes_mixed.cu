@@ -233,17 +233,25 @@ __device__ __forceinline__ float pair_r2(float tx, float ty, const float4 &sv) {
     const float dx = tx - sv.x, dy = ty - sv.y;
     return fmaf(dx, dx, dy * dy);
 }
+// log2 of r^2 + FLT_MIN: the floor rides in the r^2 multiply-add instead of
+// a separate clamp.  Every pair of distinct points has r^2 >= 2^-48 (scaled
+// FP32 offsets of O(1)), where adding 2^-126 changes nothing; coincident
+// points give log2(FLT_MIN) exactly, as the clamp does.
+__device__ __forceinline__ float pair_lg2_floor(float tx, float ty, const float4 &sv) {
+    const float dx = tx - sv.x, dy = ty - sv.y;
+    return lg2_ftz(fmaf(dx, dx, fmaf(dy, dy, 1.17549435e-38f)));
+}
 
 template <int KIND>
-__global__ void __launch_bounds__(32 * LEAF_WARPS, 6) k_leaf_eval_f(PassArgs A, const int32_t *__restrict__ list,
+__global__ void __launch_bounds__(32 * LEAF_WARPS, 5) k_leaf_eval_f(PassArgs A, const int32_t *__restrict__ list,
                                                                  int64_t nlist) {
     constexpr int R = 2 * KIFMM_TAYLOR_P + 1;
     constexpr float CLAMP = 1.17549435e-38f;  // FLT_MIN
     __shared__ float4 srcs[LEAF_WARPS][LEAF_CHUNK + 32];
     __shared__ double qds[LEAF_WARPS][R > 64 ? R : 64];
     __shared__ float qfs[LEAF_WARPS][R > 64 ? R : 64];
-    __shared__ double red[LEAF_WARPS][32];
-    __shared__ float redf[LEAF_WARPS][32];
+    __shared__ double red[LEAF_WARPS][2][32];
+    __shared__ float redf[LEAF_WARPS][2][32];
     __shared__ int rngs[LEAF_WARPS][18];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     pdl_trigger();
@@ -337,17 +345,25 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, 6) k_leaf_eval_f(PassArgs A, 
     __syncwarp();
     for (int t0 = b; t0 < e; t0 += 32) {
         const int nt = min(32, e - t0);
-        const int sp = 32 / nt;  // lanes per target
-        const int ti = lane % nt, j = lane / nt;
-        const int t = t0 + ti;
-        const double pxd = A.xs[t] - cx, pyd = A.ys[t] - cy;
-        const float tx = (float)(pxd * sc), ty = (float)(pyd * sc);
-        double near = 0.0;
-        float exf = 0.f;  // charges of the leaf's own points met at the clamp
+        // Lane layout: the tile's targets form ng groups of tb (1 or 2)
+        // targets; sp = 32 / ng lanes share a group, lane (gi, j) taking
+        // sources j, j + sp, ...  Two targets per lane reuse each source
+        // load and give four independent chains per step; the layout with
+        // fewer pair slots per lane (tb * ceil(ns / sp)) is taken.
+        const int ng2 = (nt + 1) >> 1, sp1 = 32 / nt, sp2 = 32 / ng2;
+        const bool two = KIND == KIFMM_KERNEL_LAPLACE &&
+                         2 * ((ns + sp2 - 1) / sp2) <= (ns + sp1 - 1) / sp1;
+        const int ng = two ? ng2 : nt, sp = two ? sp2 : sp1;
+        const int gi = lane % ng, j = lane / ng;
+        const int ia = gi, ib = two && gi + ng < nt ? gi + ng : gi;  // second slot repeats the first when unused
+        const float txa = (float)((A.xs[t0 + ia] - cx) * sc), tya = (float)((A.ys[t0 + ia] - cy) * sc);
+        const float txb = (float)((A.xs[t0 + ib] - cx) * sc), tyb = (float)((A.ys[t0 + ib] - cy) * sc);
+        double neara = 0.0, nearb = 0.0;
+        float exa = 0.f, exb = 0.f;  // charges of the leaf's own points met at the clamp
         for (int c0 = 0; c0 < ns; c0 += LEAF_CHUNK) {
             const int cn = min(LEAF_CHUNK, ns - c0);
             if (t0 == b || ns > LEAF_CHUNK) gather(c0, cn, lap && t0 == b);
-            // lane (ti, j) takes sources j, j + sp, ...; j + (it - 1) sp < cn + 32
+            // lane (gi, j) takes sources j, j + sp, ...; j + (it - 1) sp < cn + 32
             const int it = (cn + sp - 1) / sp;
             const float4 *sv0 = src + j;
             if (KIND == KIFMM_KERNEL_LAPLACE) {
@@ -357,33 +373,74 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, 6) k_leaf_eval_f(PassArgs A, 
                 const int kown = en > 0 ? (en + sp - 1) / sp : 0;
                 for (int k0 = 0; k0 < kown; k0 += 32) {
                     const int k1 = min(kown, k0 + 32);
-                    float acc = 0.f;
-                    for (int k = k0; k < k1; k++) {
-                        const int u = j + k * sp;
-                        const float4 sv = src[u];
-                        const float r2 = pair_r2(tx, ty, sv);
-                        acc = fmaf(sv.z, lg2_ftz(fmaxf(r2, CLAMP)), acc);
-                        exf += (r2 < CLAMP && u < en) ? sv.z : 0.f;
+                    float acca = 0.f, accb = 0.f;
+                    if (two) {
+                        for (int k = k0; k < k1; k++) {
+                            const int u = j + k * sp;
+                            const float4 sv = src[u];
+                            const float ra = pair_r2(txa, tya, sv), rb = pair_r2(txb, tyb, sv);
+                            acca = fmaf(sv.z, lg2_ftz(fmaxf(ra, CLAMP)), acca);
+                            accb = fmaf(sv.z, lg2_ftz(fmaxf(rb, CLAMP)), accb);
+                            exa += (ra < CLAMP && u < en) ? sv.z : 0.f;
+                            exb += (rb < CLAMP && u < en) ? sv.z : 0.f;
+                        }
+                    } else {
+                        for (int k = k0; k < k1; k++) {
+                            const int u = j + k * sp;
+                            const float4 sv = src[u];
+                            const float ra = pair_r2(txa, tya, sv);
+                            acca = fmaf(sv.z, lg2_ftz(fmaxf(ra, CLAMP)), acca);
+                            exa += (ra < CLAMP && u < en) ? sv.z : 0.f;
+                        }
                     }
-                    near += (double)acc;
+                    neara += (double)acca;
+                    nearb += (double)accb;
                 }
-                for (int k0 = kown; k0 < it; k0 += 32) {
-                    const int k1 = min(it, k0 + 32);
-                    float acc = 0.f, acc1 = 0.f;  // two chains: even and odd passes
-                    const float4 *pp = sv0 + (size_t)k0 * sp;
-                    int k = k0;
+                if (two) {
+                    for (int k0 = kown; k0 < it; k0 += 32) {
+                        const int k1 = min(it, k0 + 32);
+                        float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
+                        const float4 *pp = sv0 + (size_t)k0 * sp;
+                        int k = k0;
 #pragma unroll 2
-                    for (; k + 1 < k1; k += 2) {
-                        const float4 sa = pp[0], sb = pp[sp];
-                        pp += 2 * sp;
-                        acc = fmaf(sa.z, lg2_ftz(fmaxf(pair_r2(tx, ty, sa), CLAMP)), acc);
-                        acc1 = fmaf(sb.z, lg2_ftz(fmaxf(pair_r2(tx, ty, sb), CLAMP)), acc1);
+                        for (; k + 1 < k1; k += 2) {
+                            const float4 s0 = pp[0], s1 = pp[sp];
+                            pp += 2 * sp;
+                            a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
+                            b0 = fmaf(s0.z, pair_lg2_floor(txb, tyb, s0), b0);
+                            a1 = fmaf(s1.z, pair_lg2_floor(txa, tya, s1), a1);
+                            b1 = fmaf(s1.z, pair_lg2_floor(txb, tyb, s1), b1);
+                        }
+                        if (k < k1) {
+                            const float4 s0 = pp[0];
+                            a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
+                            b0 = fmaf(s0.z, pair_lg2_floor(txb, tyb, s0), b0);
+                        }
+                        neara += (double)(a0 + a1);
+                        nearb += (double)(b0 + b1);
                     }
-                    if (k < k1) {
-                        const float4 sa = pp[0];
-                        acc = fmaf(sa.z, lg2_ftz(fmaxf(pair_r2(tx, ty, sa), CLAMP)), acc);
+                } else {
+                    for (int k0 = kown; k0 < it; k0 += 32) {
+                        const int k1 = min(it, k0 + 32);
+                        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;  // four chains
+                        const float4 *pp = sv0 + (size_t)k0 * sp;
+                        int k = k0;
+#pragma unroll 1
+                        for (; k + 3 < k1; k += 4) {
+                            const float4 s0 = pp[0], s1 = pp[sp], s2 = pp[2 * sp], s3 = pp[3 * sp];
+                            pp += 4 * sp;
+                            a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
+                            a1 = fmaf(s1.z, pair_lg2_floor(txa, tya, s1), a1);
+                            a2 = fmaf(s2.z, pair_lg2_floor(txa, tya, s2), a2);
+                            a3 = fmaf(s3.z, pair_lg2_floor(txa, tya, s3), a3);
+                        }
+                        for (; k < k1; k++) {
+                            const float4 s0 = pp[0];
+                            pp += sp;
+                            a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
+                        }
+                        neara += (double)((a0 + a1) + (a2 + a3));
                     }
-                    near += (double)(acc + acc1);
                 }
             } else {
                 for (int k0 = 0; k0 < it; k0 += 32) {
@@ -392,25 +449,29 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, 6) k_leaf_eval_f(PassArgs A, 
 #pragma unroll 1
                     for (int k = k0; k < k1; k++) {
                         const float4 sv = sv0[k * sp];
-                        const float r2 = pair_r2(tx, ty, sv);
+                        const float r2 = pair_r2(txa, tya, sv);
                         if (r2 > 0.f) acc = fmaf(sv.z, gsum_term<KIND>(r2, kk), acc);
                     }
-                    near += (double)acc;
+                    neara += (double)acc;
                 }
             }
         }
         if (lap && t0 == b)
             for (int o = 16; o; o >>= 1) tsum += __shfl_xor_sync(0xffffffffu, tsum, o);
-        // per-lane share with the clamped own pairs taken out
-        red[wib][lane] = lap ? near - (double)exf * (double)lclamp : near;
-        redf[wib][lane] = exf;
+        // per-lane shares with the clamped own pairs taken out
+        red[wib][0][lane] = lap ? neara - (double)exa * (double)lclamp : neara;
+        red[wib][1][lane] = lap ? nearb - (double)exb * (double)lclamp : nearb;
+        redf[wib][0][lane] = exa;
+        redf[wib][1][lane] = exb;
         __syncwarp();
         if (lane < nt) {
+            const int t = t0 + lane;
+            const int slot = lane < ng ? 0 : 1, grp = lane - slot * ng;
             double v = 0.0;
             float ex = 0.f;
             for (int m = 0; m < sp; m++) {
-                v += red[wib][lane + m * nt];
-                ex += redf[wib][lane + m * nt];
+                v += red[wib][slot][grp + m * ng];
+                ex += redf[wib][slot][grp + m * ng];
             }
             if (lap) {
                 // the skipped charges leave log2(w^2) * sum(tau); the one skipped
@@ -419,6 +480,7 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, 6) k_leaf_eval_f(PassArgs A, 
                 const double exd = ex == (float)tau_t ? tau_t : (double)ex;
                 v += lw * (tsum - exd);
             }
+            const double pxd = A.xs[t] - cx, pyd = A.ys[t] - cy;
             // far field (L2P) in FP64
             double far = 0.0;
             if (l >= 2) {

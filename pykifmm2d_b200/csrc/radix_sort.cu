@@ -238,7 +238,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_os_pass(const uint64_t *__restri
     for (int r = 0; r < RS_ITEMS; r++) {
         const bool ok = t0 + r * 32 + lane < n;
         const uint32_t d = ok ? (uint32_t)((k[r] >> shift) & 255) : 256u;
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const unsigned peers = warp_match_digit(d);
         const uint32_t before = d < 256 ? wcnt[w][d] : 0;
         rank[r] = before + __popc(peers & lt);
         __syncwarp();

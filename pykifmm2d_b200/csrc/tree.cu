@@ -626,6 +626,105 @@ __global__ void __launch_bounds__(LT_THREADS) k_lists_write(int64_t n_nodes, con
     }
 }
 
+// Entries sorted by (level, key) with one block per level when every level
+// fits in shared memory: block l picks the level-l entries out of the
+// collected list, sorts them by the 2l key bits with an LSD radix sort in
+// shared memory (8-bit digits; warp w ranks its contiguous chunk in order with
+// warp_match_digit, so the sort is stable and the warps' chunks keep their
+// order), and writes them at the level's offset (the counts of the levels
+// above).  Keys are distinct within a level: a cell is either split or X-list.
+constexpr int ES_THREADS = 1024, ES_WARPS = ES_THREADS / 32, ES_CAP = 12288;
+constexpr size_t ES_SMEM = (size_t)2 * ES_CAP * sizeof(uint64_t) + (size_t)ES_WARPS * 256 * sizeof(uint32_t);
+__global__ void __launch_bounds__(ES_THREADS) k_ent_sort(const uint64_t *__restrict__ list, int64_t n_ent,
+                                                         const unsigned long long *__restrict__ lcount,
+                                                         uint64_t *__restrict__ ent) {
+    extern __shared__ __align__(16) unsigned char es_sm[];
+    uint64_t *A = (uint64_t *)es_sm, *B = A + ES_CAP;
+    uint32_t(*wcnt)[256] = (uint32_t(*)[256])(B + ES_CAP);
+    __shared__ unsigned s_cnt, scan_sm[32];
+    __shared__ long long s_eoff;
+    pdl_trigger();
+    pdl_wait();
+    const int l = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int m = (int)lcount[l];
+    if (m == 0 || m > ES_CAP) return;  // the host sorts globally when a level is larger
+    if (threadIdx.x == 0) {
+        long long o = 0;
+        for (int q = 0; q < l; q++) o += (long long)lcount[q];
+        s_eoff = o;
+        s_cnt = 0;
+    }
+    __syncthreads();
+    constexpr int U = 8;
+    for (int64_t base = 0; base < n_ent; base += (int64_t)U * ES_THREADS) {
+        uint64_t e[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int64_t j = base + (int64_t)u * ES_THREADS + threadIdx.x;
+            e[u] = j < n_ent ? list[j] : ENT_EMPTY;
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const bool mine = e[u] != ENT_EMPTY && (int)(e[u] >> ENT_LEVEL_SHIFT) == l;
+            const unsigned bm = __ballot_sync(0xffffffffu, mine);
+            if (!bm) continue;
+            unsigned b0 = 0;
+            if (lane == __ffs(bm) - 1) b0 = atomicAdd(&s_cnt, (unsigned)__popc(bm));
+            b0 = __shfl_sync(0xffffffffu, b0, __ffs(bm) - 1);
+            const unsigned pos = b0 + __popc(bm & ((1u << lane) - 1));
+            if (mine && pos < ES_CAP) A[pos] = e[u];
+        }
+    }
+    __syncthreads();
+    const unsigned lt = (1u << lane) - 1u;
+    const int chunk = ((m + ES_WARPS - 1) / ES_WARPS + 31) & ~31;
+    const int c0 = min(w * chunk, m), c1 = min(c0 + chunk, m);
+    for (int sh = 1; sh < 1 + 2 * l; sh += 8) {
+        for (int d = lane; d < 256; d += 32) wcnt[w][d] = 0;
+        __syncwarp();
+        for (int i = c0 + lane; i - lane < c1; i += 32) {
+            const bool ok = i < c1;
+            const uint32_t d = ok ? (uint32_t)((A[i] >> sh) & 255) : 256u;
+            const unsigned peers = warp_match_digit(d);
+            if (ok && lane == __ffs(peers) - 1) wcnt[w][d] += __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        uint32_t tot = 0;
+        if (threadIdx.x < 256) {
+            for (int ww = 0; ww < ES_WARPS; ww++) {
+                const uint32_t c = wcnt[ww][threadIdx.x];
+                wcnt[ww][threadIdx.x] = tot;
+                tot += c;
+            }
+        }
+        unsigned total;
+        const unsigned start = block_excl_scan(threadIdx.x < 256 ? tot : 0u, scan_sm, total);
+        if (threadIdx.x < 256)
+            for (int ww = 0; ww < ES_WARPS; ww++) wcnt[ww][threadIdx.x] += start;
+        __syncthreads();
+        for (int i = c0 + lane; i - lane < c1; i += 32) {
+            const bool ok = i < c1;
+            const uint64_t k = ok ? A[i] : 0;
+            const uint32_t d = ok ? (uint32_t)((k >> sh) & 255) : 256u;
+            const unsigned peers = warp_match_digit(d);
+            if (ok) {
+                const uint32_t b = wcnt[w][d];
+                B[b + __popc(peers & lt)] = k;
+            }
+            __syncwarp();
+            if (ok && lane == __ffs(peers) - 1) wcnt[w][d] += __popc(peers);
+            __syncwarp();
+        }
+        __syncthreads();
+        uint64_t *t = A;
+        A = B;
+        B = t;
+    }
+    const long long eoff = s_eoff;
+    for (int i = threadIdx.x; i < m; i += ES_THREADS) ent[eoff + i] = A[i];
+}
+
 // Work counts: cnt[0] P2P pairs, cnt[1] P2M points, cnt[2] V-list pairs,
 // cnt[3] (target group, direction) M2L blocks.
 __global__ void k_stats(LevelTable T, const uint64_t *__restrict__ ent, const int32_t *__restrict__ ent_node,
@@ -792,18 +891,26 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     P->key2.alloc(std::max<int64_t>(n, n_ent));
     if (n_ent) {
         PhaseScope ph_e(P, KIFMM_PHASE_ENTRIES);
-        KIFMM_CUDA(cudaMemcpyAsync(P->ent.p, P->list.p, n_ent * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
-        // entry = (level << 57) | (key << 1) | xlist with keys of at most 2(L-1)
-        // bits: sort the digits holding key bits, then the level digit
-        int shifts[8], np = 0;
-        for (int sh = 0; sh <= 2 * (L - 1); sh += 8) shifts[np++] = sh;
-        if (8 * np > 56) {
-            np = 0;
-            for (int sh = 0; sh < 64; sh += 8) shifts[np++] = sh;
+        unsigned long long lmax = 0;
+        for (int l = 0; l < L; l++) lmax = std::max(lmax, lcount[l]);
+        if (lmax <= (unsigned long long)ES_CAP) {
+            ensure_dyn_smem(k_ent_sort, ES_SMEM);
+            launch_pdl(k_ent_sort, dim3((unsigned)L), dim3(ES_THREADS), ES_SMEM, s, (const uint64_t *)P->list.p,
+                       n_ent, (const unsigned long long *)lc, P->ent.p);
         } else {
-            shifts[np++] = 56;
+            KIFMM_CUDA(cudaMemcpyAsync(P->ent.p, P->list.p, n_ent * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s));
+            // entry = (level << 57) | (key << 1) | xlist with keys of at most 2(L-1)
+            // bits: sort the digits holding key bits, then the level digit
+            int shifts[8], np = 0;
+            for (int sh = 0; sh <= 2 * (L - 1); sh += 8) shifts[np++] = sh;
+            if (8 * np > 56) {
+                np = 0;
+                for (int sh = 0; sh < 64; sh += 8) shifts[np++] = sh;
+            } else {
+                shifts[np++] = 56;
+            }
+            radix_sort_keys_shifts(P->ent.p, P->key2.p, n_ent, shifts, np, P);
         }
-        radix_sort_keys_shifts(P->ent.p, P->key2.p, n_ent, shifts, np, P);
     }
     // per-level entry counts (counted as the entries were added) -> level table
     LevelTable &T = P->lt;

@@ -92,6 +92,25 @@ def test_fp64_vs_oracle_200k_mixture():
     assert rel(pot, po) <= 1e-7
 
 
+def test_tree_wide_levels_vs_oracle():
+    """400k uniform points, Ncutoff 8: level 7 holds 16384 split cells, more
+    than one block sorts in shared memory, so the entries take the global
+    radix sort; the tree must still match the oracle exactly."""
+    import pykifmm2d_b200 as P
+    from oracle import oracle as O
+    rng = np.random.default_rng(5)
+    x, y = rng.uniform(-1, 1, 400_000), rng.uniform(-1, 1, 400_000)
+    kern = P.LaplaceKernel()
+    f = P.FMM(x, y, P.Get_Kernel_Functions(kern), P.prepare_numba_functions_on_the_fly(kern), 16, 8)
+    f.build_tree()
+    nodes_g, pl_g = f.export_tree()
+    o = O.OracleTree(x, y, 8)
+    nodes_o, _ = o.export()
+    assert (nodes_o[:, 0] == 7).sum() == 16384
+    np.testing.assert_array_equal(nodes_g, nodes_o)
+    np.testing.assert_array_equal(pl_g, o.locate(x, y))
+
+
 def test_direct_sum_gpu_vs_oracle(golden_cases):
     import pykifmm2d_b200 as P
     from oracle import oracle as O
