@@ -3,6 +3,7 @@
 #include <map>
 #include <mutex>
 #include <new>
+#include <vector>
 
 #include "kifmm_internal.cuh"
 
@@ -56,6 +57,29 @@ static void resolve_phases(kifmm_plan *P) {
         cudaEventDestroy(ph.b);
     }
     P->pending.clear();
+}
+
+// Pinned host blocks of HP_WORDS words, recycled across plans (a pinned
+// allocation costs far more than a plan's other setup).
+static std::mutex g_pin_mu;
+static std::vector<unsigned long long *> g_pin_free;
+unsigned long long *pinned_acquire() {
+    unsigned long long *p = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_pin_mu);
+        if (!g_pin_free.empty()) {
+            p = g_pin_free.back();
+            g_pin_free.pop_back();
+        }
+    }
+    if (!p) KIFMM_CUDA(cudaHostAlloc((void **)&p, HP_WORDS * sizeof(unsigned long long), cudaHostAllocPortable));
+    for (int i = 0; i < HP_WORDS; i++) p[i] = 0;
+    p[HP_INIT + 0] = p[HP_INIT + 2] = ~0ull;
+    return p;
+}
+void pinned_release(unsigned long long *p) {
+    std::lock_guard<std::mutex> lock(g_pin_mu);
+    g_pin_free.push_back(p);
 }
 
 void ensure_dyn_smem(const void *fn, size_t bytes) {
@@ -116,9 +140,10 @@ static void copy_in(kifmm_plan *P, DBuf<double> &dst, const double *src, int64_t
 // Device-side failures reported through a flag (a tensor-core M2L wait that
 // ran out of its poll budget); read after the stream has drained.
 static void check_device_flags(kifmm_plan *P) {
-    if (!P->scal.p) return;
-    unsigned long long f[2] = {0, 0};
-    KIFMM_CUDA(cudaMemcpyAsync(f, P->scal.p + KIFMM_SCAL_PASS_ERR, sizeof(f), cudaMemcpyDeviceToHost, P->stream));
+    if (!P->scal.p || !P->hpin) return;
+    unsigned long long *f = P->hpin + HP_FLAGS;
+    KIFMM_CUDA(cudaMemcpyAsync(f, P->scal.p + KIFMM_SCAL_PASS_ERR, 2 * sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, P->stream));
     KIFMM_CUDA(cudaStreamSynchronize(P->stream));
     KIFMM_REQUIRE(f[0] == 0, KIFMM_ERR_CUDA, "M2M/L2L pass: a bulk-copy wait timed out");
     KIFMM_REQUIRE(f[1] == 0, KIFMM_ERR_CUDA, "tensor-core M2L: an MMA completion wait timed out");
@@ -203,6 +228,7 @@ int kifmm_plan_create(const kifmm_kernel *kernel, int32_t nequiv, int32_t ncutof
             P->num_sms = sms > 0 ? sms : 148;
             prepare_pool(P->device);
             init_log_table(P->device);
+            P->hpin = pinned_acquire();
             if (o.stream) {
                 P->stream = (cudaStream_t)o.stream;
             } else {
@@ -396,8 +422,10 @@ int kifmm_plan_destroy(kifmm_plan *P) {
         cudaStream_t s = P->stream, side = P->side;
         cudaEvent_t e0 = P->ops_fork, e1 = P->ops_done;
         bool own = P->own_stream;
+        unsigned long long *hp = P->hpin;
         delete P;  // buffers are freed stream-ordered on s and on the side stream
         if (s) cudaStreamSynchronize(s);
+        if (hp) pinned_release(hp);
         if (side) {  // the device's shared side stream stays
             cudaStreamSynchronize(side);
             cudaEventDestroy(e0);

@@ -210,6 +210,10 @@ struct kifmm_plan {
     kifmm::DBuf<unsigned long long> sort_status;  // radix sort look-back words
     kifmm::DBuf<unsigned long long> scal;  // small device scalars
     kifmm::DBuf<int64_t> misc;
+    // pinned host words (kifmm::HP_*): read-backs land here by asynchronous
+    // copies followed by one stream sync (a copy to pageable memory would
+    // block the host on every call), and the constant source of scal's reset
+    unsigned long long *hpin = nullptr;
 
     // phase timers (kifmm_set_profiling)
     bool profiling = false;
@@ -252,6 +256,16 @@ template <class K>
 inline void ensure_dyn_smem(K *fn, size_t bytes) {
     ensure_dyn_smem((const void *)fn, bytes);
 }
+
+// layout of kifmm_plan::hpin (64-bit words)
+constexpr int HP_SCAL = 0;     // [16] snapshot of scal
+constexpr int HP_MISC = 16;    // [128] snapshot of misc
+constexpr int HP_INIT = 160;   // [16] reset values of scal (min trackers at ~0)
+constexpr int HP_FLAGS = 192;  // [2] pass / tensor-core error flags
+constexpr int HP_STATS = 200;  // [4] work counts
+constexpr int HP_WORDS = 256;
+unsigned long long *pinned_acquire();
+void pinned_release(unsigned long long *p);
 
 // device scalar slots (plan->scal) holding error flags that the host reads
 // after an apply: a bulk-copy wait in the level passes that ran out, and an

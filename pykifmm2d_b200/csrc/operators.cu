@@ -52,14 +52,21 @@ __device__ __forceinline__ double gval(const OpsArgs &A, double sx, double sy, d
 // conflict-free), so a pivot step needs warp synchronisation only.  Rows
 // beyond 32 are taken by the same lanes in turn.  Per element the arithmetic
 // is the block-wide form's: a[k][c] /= pivot, a[r][c] -= a[r][k] * a[k][c].
-__global__ void k_ops_inverse(OpsArgs A) {
+// One block per level: the circles, then the inverse of the Q x Q
+// equivalent-to-check matrix by Gauss-Jordan elimination with partial
+// pivoting on [E | I] (Q x 2Q), shared over the block: warp 0 picks the pivot,
+// then every thread produces its elements of the next matrix from the current
+// one (two buffers, so a step needs no separate read and write phases).
+constexpr int INV_THREADS = 256;
+__global__ void __launch_bounds__(INV_THREADS) k_ops_inverse(OpsArgs A) {
     extern __shared__ double sm[];
-    const int Q = A.Q, Q2 = 2 * Q, ld = Q2 + 1, l = blockIdx.x, lane = threadIdx.x;
+    __shared__ int s_piv;
+    const int Q = A.Q, Q2 = 2 * Q, ld = Q2 + 1, l = blockIdx.x, tid = threadIdx.x;
     if (l >= A.L) return;
     {  // the level's circles (get_level_information, class_fmm.py:35-45)
         const double w = lvl_width(A, l), r1 = 0.5 * w * A.rf1, r2 = 0.5 * w * A.rf2;
         double *bw = A.ops + (size_t)l * A.stride;
-        for (int q = lane; q < Q; q += 32) {
+        for (int q = tid; q < Q; q += INV_THREADS) {
             const double th = q * (2.0 * 3.141592653589793 / Q);
             const double c = cos(th), s = sin(th);
             bw[off_large(Q) + q] = r2 * c;
@@ -67,47 +74,56 @@ __global__ void k_ops_inverse(OpsArgs A) {
             bw[off_small(Q) + q] = r1 * c;
             bw[off_small(Q) + Q + q] = r1 * s;
         }
-        __syncwarp();
+        __syncthreads();
     }
     if (l < 1) return;
-    double *a = sm;  // Q x ld
+    double *a = sm, *nb = sm + (size_t)Q * ld;  // current and next matrix, Q x ld each
     const double *b = A.ops + (size_t)l * A.stride;
     const double *lx = b + off_large(Q), *ly = lx + Q, *sx = b + off_small(Q), *sy = sx + Q;
-    for (int e = lane; e < Q * Q2; e += 32) {
-        int r = e / Q2, c = e % Q2;
+    for (int e = tid; e < Q * Q2; e += INV_THREADS) {
+        const int r = e / Q2, c = e % Q2;
         a[r * ld + c] = c < Q ? gval(A, sx[c], sy[c], lx[r], ly[r]) : (c - Q == r ? 1.0 : 0.0);
     }
-    __syncwarp();
+    __syncthreads();
     for (int k = 0; k < Q; k++) {
-        double best = -1.0;
-        int bi = k;
-        for (int i = k + lane; i < Q; i += 32) {
-            double v = fabs(a[i * ld + k]);
-            if (v > best) { best = v; bi = i; }
-        }
-        for (int o = 16; o; o >>= 1) {
-            double ob = __shfl_xor_sync(0xffffffffu, best, o);
-            int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-        }
-        const int p = bi;
-        if (p != k)
-            for (int c = lane; c < Q2; c += 32) {
-                double t = a[k * ld + c]; a[k * ld + c] = a[p * ld + c]; a[p * ld + c] = t;
+        if (tid < 32) {  // pivot: largest |a[i][k]| over rows i >= k (lowest row on ties)
+            double best = -1.0;
+            int bi = k;
+            for (int i = k + tid; i < Q; i += 32) {
+                const double v = fabs(a[i * ld + k]);
+                if (v > best) { best = v; bi = i; }
             }
-        __syncwarp();
-        const double pv = a[k * ld + k];
-        for (int c = lane; c < Q2; c += 32) a[k * ld + c] /= pv;
-        __syncwarp();
-        for (int r = lane; r < Q; r += 32) {
-            if (r == k) continue;
-            const double f = a[r * ld + k];
-            for (int c = 0; c < Q2; c++) a[r * ld + c] -= f * a[k * ld + c];
+            for (int o = 16; o; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+            }
+            if (tid == 0) s_piv = bi;
         }
-        __syncwarp();
+        __syncthreads();
+        // rows k and p swap, row k is divided by the pivot, and the pivot row
+        // is subtracted from every other row to clear column k
+        const int p = s_piv;
+        const double rp = 1.0 / a[p * ld + k];
+        for (int e = tid; e < Q * Q2; e += INV_THREADS) {
+            const int r = e / Q2, c = e % Q2;
+            const double pc = a[p * ld + c] * rp;  // normalised pivot row
+            double v;
+            if (r == k) {
+                v = pc;
+            } else {
+                const int src = r == p ? k : r;
+                v = a[src * ld + c] - a[src * ld + k] * pc;
+            }
+            nb[r * ld + c] = v;
+        }
+        __syncthreads();
+        double *t = a;
+        a = nb;
+        nb = t;
     }
     double *inv = A.ops + (size_t)l * A.stride + off_inv(Q);  // row-major
-    for (int e = lane; e < Q * Q; e += 32) inv[e] = a[(e / Q) * ld + Q + e % Q];
+    for (int e = tid; e < Q * Q; e += INV_THREADS) inv[e] = a[(e / Q) * ld + Q + e % Q];
 }
 
 // P_o = M2LS_o . Inv_l (far offsets), M2M and L2L compositions; the inverse
@@ -283,9 +299,9 @@ void build_operators(kifmm_plan *P) {
     }
     // circles + inverse, then kernel matrices composed with the inverses, then
     // the directional M2L blocks (with the row maxima the tensor-core slices use)
-    size_t smem = (size_t)Q * (2 * Q + 1) * sizeof(double);
+    size_t smem = (size_t)2 * Q * (2 * Q + 1) * sizeof(double);
     ensure_dyn_smem(k_ops_inverse, smem);
-    k_ops_inverse<<<L, 32, smem, s>>>(A);
+    k_ops_inverse<<<L, INV_THREADS, smem, s>>>(A);
     KIFMM_LAUNCHED();
     if (L >= 2) {
         size_t csm = (size_t)5 * Q * Q * sizeof(double);

@@ -221,7 +221,10 @@ __global__ void __launch_bounds__(TY_THREADS) k_leaf_taylor(TaylorArgs T) {
 // round to the same FP32 offsets and keep log2(FLT_MIN) for their pair; the
 // FP64 near field (near_fp64) resolves such pairs.  FP32 partial sums of at
 // most 32 terms are accumulated in FP64.
-constexpr int LEAF_WARPS = 4;
+// one warp per block: leaves differ in work by more than 10x, and a block of
+// several warps would hold its SM slot until its slowest warp is done
+constexpr int LEAF_WARPS = 1;
+constexpr int LEAF_BLOCKS_PER_SM = 20;  // resident blocks per SM at the register bound below
 constexpr int LEAF_CHUNK = 256;
 
 __device__ __forceinline__ float lg2_ftz(float x) {
@@ -243,7 +246,7 @@ __device__ __forceinline__ float pair_lg2_floor(float tx, float ty, const float4
 }
 
 template <int KIND>
-__global__ void __launch_bounds__(32 * LEAF_WARPS, 5) k_leaf_eval_f(PassArgs A, const int32_t *__restrict__ list,
+__global__ void __launch_bounds__(32 * LEAF_WARPS, LEAF_BLOCKS_PER_SM) k_leaf_eval_f(PassArgs A, const int32_t *__restrict__ list,
                                                                  int64_t nlist) {
     constexpr int R = 2 * KIFMM_TAYLOR_P + 1;
     constexpr float CLAMP = 1.17549435e-38f;  // FLT_MIN
@@ -256,271 +259,273 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, 5) k_leaf_eval_f(PassArgs A, 
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     pdl_trigger();
     pdl_wait();
-    int64_t w = (int64_t)blockIdx.x * LEAF_WARPS + wib;
-    if (w >= nlist) return;
-    const int g = list[w];
-    const int l = A.nlev[g];
-    double cx, cy;
-    node_center(A, g, l, cx, cy);
-    const bool lap = KIND == KIFMM_KERNEL_LAPLACE;
-    const bool taylor = lap && A.taylor != nullptr && l >= 2;
-    double *qd = qds[wib];
-    float *qf = qfs[wib];
-    float4 *src = srcs[wib];
-    const double width = ldexp(A.W, -l);
-    const double sc = lap ? 1.0 / width : 1.0;     // coordinate scale
-    const double lw = lap ? -2.0 * log2(sc) : 0.0; // log2 of the squared length unit
-    if (taylor) {  // Taylor coefficients of the local expansion (k_leaf_taylor, FP64)
-        const double *cf = A.leaf_coef + (size_t)w * R;
-        for (int r = lane; r < R; r += 32) {
-            const double v = cf[r];
-            qd[r] = v;
-            qf[r] = (float)v;
-        }
-    } else {
-        local_density(A, g, l, qd, lane);
-    }
-    const float kk = (float)A.k;
-    const float lclamp = lg2_ftz(CLAMP);
-    const int b = A.nbot[g], e = A.ntop[g];
-    // source ranges: the leaf itself, then its colleagues in direction order;
-    // list element p lies in the last range i with pre[i] <= p, at p + off[i]
-    // (kept in shared memory: registers are scarce in the pair loop)
-    int *rng = rngs[wib];
-    int ns = 0;
-    if (lane < 9) {
-        const int d = lane <= 4 ? lane - 1 : lane;
-        const int c = lane == 0 ? g : A.ncoll[9 * (size_t)g + d];
-        const int rb = c >= 0 ? A.nbot[c] : 0, rn = c >= 0 ? A.ntop[c] - rb : 0;
-        int x = rn;  // inclusive prefix over lanes 0..8
-        for (int o = 1; o < 16; o <<= 1) {
-            const int y = __shfl_up_sync(0x1ffu, x, o);
-            if (lane >= o) x += y;
-        }
-        rng[lane] = x - rn;
-        rng[9 + lane] = rb - (x - rn);
-        ns = x;
-    }
-    ns = __shfl_sync(0xffffffffu, ns, 8);
-    double tsum = 0.0;  // FP64 sum of the near sources' charges (Laplace)
-    // stage sources [c0, c0 + cn) of the list, padded with 32 far, uncharged
-    // ones; four elements per lane per pass, loads issued before any is used
-    auto gather = [&](int c0, int cn, bool sum) {
-        __syncwarp();
-        int pre[9], off[9];
-#pragma unroll
-        for (int i = 0; i < 9; i++) {
-            pre[i] = rng[i];
-            off[i] = rng[9 + i];
-        }
-        for (int q0 = 0; q0 < cn; q0 += 128) {
-            int si[4];
-#pragma unroll
-            for (int k = 0; k < 4; k++) {
-                const int q = q0 + lane + 32 * k, p = c0 + q;
-                int sv = p + off[0];
-#pragma unroll
-                for (int i = 1; i < 9; i++) sv = p >= pre[i] ? p + off[i] : sv;
-                si[k] = q < cn ? sv : -1;
+    // one warp per leaf (grid-stride only if the grid were capped)
+    const int64_t wstride = (int64_t)gridDim.x * LEAF_WARPS;
+    for (int64_t w = (int64_t)blockIdx.x * LEAF_WARPS + wib; w < nlist; w += wstride) {
+        const int g = list[w];
+        const int l = A.nlev[g];
+        double cx, cy;
+        node_center(A, g, l, cx, cy);
+        const bool lap = KIND == KIFMM_KERNEL_LAPLACE;
+        const bool taylor = lap && A.taylor != nullptr && l >= 2;
+        double *qd = qds[wib];
+        float *qf = qfs[wib];
+        float4 *src = srcs[wib];
+        const double width = ldexp(A.W, -l);
+        const double sc = lap ? 1.0 / width : 1.0;     // coordinate scale
+        const double lw = lap ? -2.0 * log2(sc) : 0.0; // log2 of the squared length unit
+        if (taylor) {  // Taylor coefficients of the local expansion (k_leaf_taylor, FP64)
+            const double *cf = A.leaf_coef + (size_t)w * R;
+            for (int r = lane; r < R; r += 32) {
+                const double v = cf[r];
+                qd[r] = v;
+                qf[r] = (float)v;
             }
-            double vx[4], vy[4], vt[4];
-#pragma unroll
-            for (int k = 0; k < 4; k++)
-                if (si[k] >= 0) {
-                    vx[k] = A.xs[si[k]];
-                    vy[k] = A.ys[si[k]];
-                    vt[k] = A.taus[si[k]];
-                }
-#pragma unroll
-            for (int k = 0; k < 4; k++)
-                if (si[k] >= 0) {
-                    src[q0 + lane + 32 * k] =
-                        make_float4((float)((vx[k] - cx) * sc), (float)((vy[k] - cy) * sc), (float)vt[k], 0.f);
-                    if (sum) tsum += vt[k];
-                }
+        } else {
+            local_density(A, g, l, qd, lane);
         }
-        src[cn + lane] = make_float4(1e18f, 1e18f, 0.f, 0.f);
+        const float kk = (float)A.k;
+        const float lclamp = lg2_ftz(CLAMP);
+        const int b = A.nbot[g], e = A.ntop[g];
+        // source ranges: the leaf itself, then its colleagues in direction order;
+        // list element p lies in the last range i with pre[i] <= p, at p + off[i]
+        // (kept in shared memory: registers are scarce in the pair loop)
+        int *rng = rngs[wib];
+        int ns = 0;
+        if (lane < 9) {
+            const int d = lane <= 4 ? lane - 1 : lane;
+            const int c = lane == 0 ? g : A.ncoll[9 * (size_t)g + d];
+            const int rb = c >= 0 ? A.nbot[c] : 0, rn = c >= 0 ? A.ntop[c] - rb : 0;
+            int x = rn;  // inclusive prefix over lanes 0..8
+            for (int o = 1; o < 16; o <<= 1) {
+                const int y = __shfl_up_sync(0x1ffu, x, o);
+                if (lane >= o) x += y;
+            }
+            rng[lane] = x - rn;
+            rng[9 + lane] = rb - (x - rn);
+            ns = x;
+        }
+        ns = __shfl_sync(0xffffffffu, ns, 8);
+        double tsum = 0.0;  // FP64 sum of the near sources' charges (Laplace)
+        // stage sources [c0, c0 + cn) of the list, padded with 32 far, uncharged
+        // ones; four elements per lane per pass, loads issued before any is used
+        auto gather = [&](int c0, int cn, bool sum) {
+            __syncwarp();
+            int pre[9], off[9];
+    #pragma unroll
+            for (int i = 0; i < 9; i++) {
+                pre[i] = rng[i];
+                off[i] = rng[9 + i];
+            }
+            for (int q0 = 0; q0 < cn; q0 += 128) {
+                int si[4];
+    #pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int q = q0 + lane + 32 * k, p = c0 + q;
+                    int sv = p + off[0];
+    #pragma unroll
+                    for (int i = 1; i < 9; i++) sv = p >= pre[i] ? p + off[i] : sv;
+                    si[k] = q < cn ? sv : -1;
+                }
+                double vx[4], vy[4], vt[4];
+    #pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (si[k] >= 0) {
+                        vx[k] = A.xs[si[k]];
+                        vy[k] = A.ys[si[k]];
+                        vt[k] = A.taus[si[k]];
+                    }
+    #pragma unroll
+                for (int k = 0; k < 4; k++)
+                    if (si[k] >= 0) {
+                        src[q0 + lane + 32 * k] =
+                            make_float4((float)((vx[k] - cx) * sc), (float)((vy[k] - cy) * sc), (float)vt[k], 0.f);
+                        if (sum) tsum += vt[k];
+                    }
+            }
+            src[cn + lane] = make_float4(1e18f, 1e18f, 0.f, 0.f);
+            __syncwarp();
+        };
         __syncwarp();
-    };
-    __syncwarp();
-    for (int t0 = b; t0 < e; t0 += 32) {
-        const int nt = min(32, e - t0);
-        // Lane layout: the tile's targets form ng groups of tb (1 or 2)
-        // targets; sp = 32 / ng lanes share a group, lane (gi, j) taking
-        // sources j, j + sp, ...  Two targets per lane reuse each source
-        // load and give four independent chains per step; the layout with
-        // fewer pair slots per lane (tb * ceil(ns / sp)) is taken.
-        const int ng2 = (nt + 1) >> 1, sp1 = 32 / nt, sp2 = 32 / ng2;
-        const bool two = KIND == KIFMM_KERNEL_LAPLACE &&
-                         2 * ((ns + sp2 - 1) / sp2) <= (ns + sp1 - 1) / sp1;
-        const int ng = two ? ng2 : nt, sp = two ? sp2 : sp1;
-        const int gi = lane % ng, j = lane / ng;
-        const int ia = gi, ib = two && gi + ng < nt ? gi + ng : gi;  // second slot repeats the first when unused
-        const float txa = (float)((A.xs[t0 + ia] - cx) * sc), tya = (float)((A.ys[t0 + ia] - cy) * sc);
-        const float txb = (float)((A.xs[t0 + ib] - cx) * sc), tyb = (float)((A.ys[t0 + ib] - cy) * sc);
-        double neara = 0.0, nearb = 0.0;
-        float exa = 0.f, exb = 0.f;  // charges of the leaf's own points met at the clamp
-        for (int c0 = 0; c0 < ns; c0 += LEAF_CHUNK) {
-            const int cn = min(LEAF_CHUNK, ns - c0);
-            if (t0 == b || ns > LEAF_CHUNK) gather(c0, cn, lap && t0 == b);
-            // lane (gi, j) takes sources j, j + sp, ...; j + (it - 1) sp < cn + 32
-            const int it = (cn + sp - 1) / sp;
-            const float4 *sv0 = src + j;
-            if (KIND == KIFMM_KERNEL_LAPLACE) {
-                // the list starts with the leaf's own points, local [0, en): the
-                // first kown passes count the pairs there that meet the clamp
-                const int en = min(e - b - c0, cn);
-                const int kown = en > 0 ? (en + sp - 1) / sp : 0;
-                for (int k0 = 0; k0 < kown; k0 += 32) {
-                    const int k1 = min(kown, k0 + 32);
-                    float acca = 0.f, accb = 0.f;
+        for (int t0 = b; t0 < e; t0 += 32) {
+            const int nt = min(32, e - t0);
+            // Lane layout: the tile's targets form ng groups of tb (1 or 2)
+            // targets; sp = 32 / ng lanes share a group, lane (gi, j) taking
+            // sources j, j + sp, ...  Two targets per lane reuse each source
+            // load and give four independent chains per step; the layout with
+            // fewer pair slots per lane (tb * ceil(ns / sp)) is taken.
+            const int ng2 = (nt + 1) >> 1, sp1 = 32 / nt, sp2 = 32 / ng2;
+            const bool two = KIND == KIFMM_KERNEL_LAPLACE &&
+                             2 * ((ns + sp2 - 1) / sp2) <= (ns + sp1 - 1) / sp1;
+            const int ng = two ? ng2 : nt, sp = two ? sp2 : sp1;
+            const int gi = lane % ng, j = lane / ng;
+            const int ia = gi, ib = two && gi + ng < nt ? gi + ng : gi;  // second slot repeats the first when unused
+            const float txa = (float)((A.xs[t0 + ia] - cx) * sc), tya = (float)((A.ys[t0 + ia] - cy) * sc);
+            const float txb = (float)((A.xs[t0 + ib] - cx) * sc), tyb = (float)((A.ys[t0 + ib] - cy) * sc);
+            double neara = 0.0, nearb = 0.0;
+            float exa = 0.f, exb = 0.f;  // charges of the leaf's own points met at the clamp
+            for (int c0 = 0; c0 < ns; c0 += LEAF_CHUNK) {
+                const int cn = min(LEAF_CHUNK, ns - c0);
+                if (t0 == b || ns > LEAF_CHUNK) gather(c0, cn, lap && t0 == b);
+                // lane (gi, j) takes sources j, j + sp, ...; j + (it - 1) sp < cn + 32
+                const int it = (cn + sp - 1) / sp;
+                const float4 *sv0 = src + j;
+                if (KIND == KIFMM_KERNEL_LAPLACE) {
+                    // the list starts with the leaf's own points, local [0, en): the
+                    // first kown passes count the pairs there that meet the clamp
+                    const int en = min(e - b - c0, cn);
+                    const int kown = en > 0 ? (en + sp - 1) / sp : 0;
+                    for (int k0 = 0; k0 < kown; k0 += 32) {
+                        const int k1 = min(kown, k0 + 32);
+                        float acca = 0.f, accb = 0.f;
+                        if (two) {
+                            for (int k = k0; k < k1; k++) {
+                                const int u = j + k * sp;
+                                const float4 sv = src[u];
+                                const float ra = pair_r2(txa, tya, sv), rb = pair_r2(txb, tyb, sv);
+                                acca = fmaf(sv.z, lg2_ftz(fmaxf(ra, CLAMP)), acca);
+                                accb = fmaf(sv.z, lg2_ftz(fmaxf(rb, CLAMP)), accb);
+                                exa += (ra < CLAMP && u < en) ? sv.z : 0.f;
+                                exb += (rb < CLAMP && u < en) ? sv.z : 0.f;
+                            }
+                        } else {
+                            for (int k = k0; k < k1; k++) {
+                                const int u = j + k * sp;
+                                const float4 sv = src[u];
+                                const float ra = pair_r2(txa, tya, sv);
+                                acca = fmaf(sv.z, lg2_ftz(fmaxf(ra, CLAMP)), acca);
+                                exa += (ra < CLAMP && u < en) ? sv.z : 0.f;
+                            }
+                        }
+                        neara += (double)acca;
+                        nearb += (double)accb;
+                    }
                     if (two) {
-                        for (int k = k0; k < k1; k++) {
-                            const int u = j + k * sp;
-                            const float4 sv = src[u];
-                            const float ra = pair_r2(txa, tya, sv), rb = pair_r2(txb, tyb, sv);
-                            acca = fmaf(sv.z, lg2_ftz(fmaxf(ra, CLAMP)), acca);
-                            accb = fmaf(sv.z, lg2_ftz(fmaxf(rb, CLAMP)), accb);
-                            exa += (ra < CLAMP && u < en) ? sv.z : 0.f;
-                            exb += (rb < CLAMP && u < en) ? sv.z : 0.f;
+                        for (int k0 = kown; k0 < it; k0 += 32) {
+                            const int k1 = min(it, k0 + 32);
+                            float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
+                            const float4 *pp = sv0 + (size_t)k0 * sp;
+                            int k = k0;
+    #pragma unroll 2
+                            for (; k + 1 < k1; k += 2) {
+                                const float4 s0 = pp[0], s1 = pp[sp];
+                                pp += 2 * sp;
+                                a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
+                                b0 = fmaf(s0.z, pair_lg2_floor(txb, tyb, s0), b0);
+                                a1 = fmaf(s1.z, pair_lg2_floor(txa, tya, s1), a1);
+                                b1 = fmaf(s1.z, pair_lg2_floor(txb, tyb, s1), b1);
+                            }
+                            if (k < k1) {
+                                const float4 s0 = pp[0];
+                                a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
+                                b0 = fmaf(s0.z, pair_lg2_floor(txb, tyb, s0), b0);
+                            }
+                            neara += (double)(a0 + a1);
+                            nearb += (double)(b0 + b1);
                         }
                     } else {
+                        for (int k0 = kown; k0 < it; k0 += 32) {
+                            const int k1 = min(it, k0 + 32);
+                            float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;  // four chains
+                            const float4 *pp = sv0 + (size_t)k0 * sp;
+                            int k = k0;
+    #pragma unroll 1
+                            for (; k + 3 < k1; k += 4) {
+                                const float4 s0 = pp[0], s1 = pp[sp], s2 = pp[2 * sp], s3 = pp[3 * sp];
+                                pp += 4 * sp;
+                                a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
+                                a1 = fmaf(s1.z, pair_lg2_floor(txa, tya, s1), a1);
+                                a2 = fmaf(s2.z, pair_lg2_floor(txa, tya, s2), a2);
+                                a3 = fmaf(s3.z, pair_lg2_floor(txa, tya, s3), a3);
+                            }
+                            for (; k < k1; k++) {
+                                const float4 s0 = pp[0];
+                                pp += sp;
+                                a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
+                            }
+                            neara += (double)((a0 + a1) + (a2 + a3));
+                        }
+                    }
+                } else {
+                    for (int k0 = 0; k0 < it; k0 += 32) {
+                        const int k1 = min(it, k0 + 32);
+                        float acc = 0.f;
+    #pragma unroll 1
                         for (int k = k0; k < k1; k++) {
-                            const int u = j + k * sp;
-                            const float4 sv = src[u];
-                            const float ra = pair_r2(txa, tya, sv);
-                            acca = fmaf(sv.z, lg2_ftz(fmaxf(ra, CLAMP)), acca);
-                            exa += (ra < CLAMP && u < en) ? sv.z : 0.f;
+                            const float4 sv = sv0[k * sp];
+                            const float r2 = pair_r2(txa, tya, sv);
+                            if (r2 > 0.f) acc = fmaf(sv.z, gsum_term<KIND>(r2, kk), acc);
                         }
+                        neara += (double)acc;
                     }
-                    neara += (double)acca;
-                    nearb += (double)accb;
-                }
-                if (two) {
-                    for (int k0 = kown; k0 < it; k0 += 32) {
-                        const int k1 = min(it, k0 + 32);
-                        float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
-                        const float4 *pp = sv0 + (size_t)k0 * sp;
-                        int k = k0;
-#pragma unroll 2
-                        for (; k + 1 < k1; k += 2) {
-                            const float4 s0 = pp[0], s1 = pp[sp];
-                            pp += 2 * sp;
-                            a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
-                            b0 = fmaf(s0.z, pair_lg2_floor(txb, tyb, s0), b0);
-                            a1 = fmaf(s1.z, pair_lg2_floor(txa, tya, s1), a1);
-                            b1 = fmaf(s1.z, pair_lg2_floor(txb, tyb, s1), b1);
-                        }
-                        if (k < k1) {
-                            const float4 s0 = pp[0];
-                            a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
-                            b0 = fmaf(s0.z, pair_lg2_floor(txb, tyb, s0), b0);
-                        }
-                        neara += (double)(a0 + a1);
-                        nearb += (double)(b0 + b1);
-                    }
-                } else {
-                    for (int k0 = kown; k0 < it; k0 += 32) {
-                        const int k1 = min(it, k0 + 32);
-                        float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;  // four chains
-                        const float4 *pp = sv0 + (size_t)k0 * sp;
-                        int k = k0;
-#pragma unroll 1
-                        for (; k + 3 < k1; k += 4) {
-                            const float4 s0 = pp[0], s1 = pp[sp], s2 = pp[2 * sp], s3 = pp[3 * sp];
-                            pp += 4 * sp;
-                            a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
-                            a1 = fmaf(s1.z, pair_lg2_floor(txa, tya, s1), a1);
-                            a2 = fmaf(s2.z, pair_lg2_floor(txa, tya, s2), a2);
-                            a3 = fmaf(s3.z, pair_lg2_floor(txa, tya, s3), a3);
-                        }
-                        for (; k < k1; k++) {
-                            const float4 s0 = pp[0];
-                            pp += sp;
-                            a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
-                        }
-                        neara += (double)((a0 + a1) + (a2 + a3));
-                    }
-                }
-            } else {
-                for (int k0 = 0; k0 < it; k0 += 32) {
-                    const int k1 = min(it, k0 + 32);
-                    float acc = 0.f;
-#pragma unroll 1
-                    for (int k = k0; k < k1; k++) {
-                        const float4 sv = sv0[k * sp];
-                        const float r2 = pair_r2(txa, tya, sv);
-                        if (r2 > 0.f) acc = fmaf(sv.z, gsum_term<KIND>(r2, kk), acc);
-                    }
-                    neara += (double)acc;
                 }
             }
+            if (lap && t0 == b)
+                for (int o = 16; o; o >>= 1) tsum += __shfl_xor_sync(0xffffffffu, tsum, o);
+            // per-lane shares with the clamped own pairs taken out
+            red[wib][0][lane] = lap ? neara - (double)exa * (double)lclamp : neara;
+            red[wib][1][lane] = lap ? nearb - (double)exb * (double)lclamp : nearb;
+            redf[wib][0][lane] = exa;
+            redf[wib][1][lane] = exb;
+            __syncwarp();
+            if (lane < nt) {
+                const int t = t0 + lane;
+                const int slot = lane < ng ? 0 : 1, grp = lane - slot * ng;
+                double v = 0.0;
+                float ex = 0.f;
+                for (int m = 0; m < sp; m++) {
+                    v += red[wib][slot][grp + m * ng];
+                    ex += redf[wib][slot][grp + m * ng];
+                }
+                if (lap) {
+                    // the skipped charges leave log2(w^2) * sum(tau); the one skipped
+                    // pair is almost always the target itself: take its FP64 charge
+                    const double tau_t = A.taus[t];
+                    const double exd = ex == (float)tau_t ? tau_t : (double)ex;
+                    v += lw * (tsum - exd);
+                }
+                const double pxd = A.xs[t] - cx, pyd = A.ys[t] - cy;
+                // far field (L2P) in FP64
+                double far = 0.0;
+                if (l >= 2) {
+                    const double zx = pxd * sc, zy = pyd * sc;
+                    if (taylor && zx * zx + zy * zy <= 0.5625) {
+                        // Horner: orders P..9 in FP32 (weighted by |z/rho|^9 < 0.008 where
+                        // used), then 8..1 in FP64
+                        const float zxf = (float)zx, zyf = (float)zy;
+                        float fr = qf[R - 2], fi = qf[R - 1];
+                        for (int jj = KIFMM_TAYLOR_P - 1; jj >= 9; jj--) {
+                            const float nr = fmaf(fr, zxf, fmaf(-fi, zyf, qf[2 * jj - 1]));
+                            const float ni = fmaf(fr, zyf, fmaf(fi, zxf, qf[2 * jj]));
+                            fr = nr;
+                            fi = ni;
+                        }
+                        double sr = fr, si = fi;
+                        for (int jj = 8; jj >= 1; jj--) {
+                            double nr = fma(sr, zx, fma(-si, zy, qd[2 * jj - 1]));
+                            double ni = fma(sr, zy, fma(si, zx, qd[2 * jj]));
+                            sr = nr;
+                            si = ni;
+                        }
+                        far = qd[0] + (sr * zx - si * zy);
+                    } else {
+                        // direct FP64 sum over the equivalent points (out-of-box targets, K0)
+                        const double *lgd = A.ops + (size_t)l * A.stride + A.off_large;
+                        const double *inv = A.ops + (size_t)l * A.stride + A.off_inv;
+                        const double *u = A.udown + (size_t)g * A.Q;
+                        for (int q = 0; q < A.Q; q++) {
+                            double qq = taylor ? 0.0 : qd[q];
+                            if (taylor)
+                                for (int c = 0; c < A.Q; c++) qq = fma(inv[q * A.Q + c], u[c], qq);
+                            double dx = pxd - lgd[q], dy = pyd - lgd[A.Q + q];
+                            far = fma(green_d(A.kind, A.k, dx * dx + dy * dy), qq, far);
+                        }
+                    }
+                }
+                A.pots[t] = v * (double)gsum_scale<KIND>() + far;
+            }
+            __syncwarp();
         }
-        if (lap && t0 == b)
-            for (int o = 16; o; o >>= 1) tsum += __shfl_xor_sync(0xffffffffu, tsum, o);
-        // per-lane shares with the clamped own pairs taken out
-        red[wib][0][lane] = lap ? neara - (double)exa * (double)lclamp : neara;
-        red[wib][1][lane] = lap ? nearb - (double)exb * (double)lclamp : nearb;
-        redf[wib][0][lane] = exa;
-        redf[wib][1][lane] = exb;
-        __syncwarp();
-        if (lane < nt) {
-            const int t = t0 + lane;
-            const int slot = lane < ng ? 0 : 1, grp = lane - slot * ng;
-            double v = 0.0;
-            float ex = 0.f;
-            for (int m = 0; m < sp; m++) {
-                v += red[wib][slot][grp + m * ng];
-                ex += redf[wib][slot][grp + m * ng];
-            }
-            if (lap) {
-                // the skipped charges leave log2(w^2) * sum(tau); the one skipped
-                // pair is almost always the target itself: take its FP64 charge
-                const double tau_t = A.taus[t];
-                const double exd = ex == (float)tau_t ? tau_t : (double)ex;
-                v += lw * (tsum - exd);
-            }
-            const double pxd = A.xs[t] - cx, pyd = A.ys[t] - cy;
-            // far field (L2P) in FP64
-            double far = 0.0;
-            if (l >= 2) {
-                const double zx = pxd * sc, zy = pyd * sc;
-                if (taylor && zx * zx + zy * zy <= 0.5625) {
-                    // Horner: orders P..9 in FP32 (weighted by |z/rho|^9 < 0.008 where
-                    // used), then 8..1 in FP64
-                    const float zxf = (float)zx, zyf = (float)zy;
-                    float fr = qf[R - 2], fi = qf[R - 1];
-                    for (int jj = KIFMM_TAYLOR_P - 1; jj >= 9; jj--) {
-                        const float nr = fmaf(fr, zxf, fmaf(-fi, zyf, qf[2 * jj - 1]));
-                        const float ni = fmaf(fr, zyf, fmaf(fi, zxf, qf[2 * jj]));
-                        fr = nr;
-                        fi = ni;
-                    }
-                    double sr = fr, si = fi;
-                    for (int jj = 8; jj >= 1; jj--) {
-                        double nr = fma(sr, zx, fma(-si, zy, qd[2 * jj - 1]));
-                        double ni = fma(sr, zy, fma(si, zx, qd[2 * jj]));
-                        sr = nr;
-                        si = ni;
-                    }
-                    far = qd[0] + (sr * zx - si * zy);
-                } else {
-                    // direct FP64 sum over the equivalent points (out-of-box targets, K0)
-                    const double *lgd = A.ops + (size_t)l * A.stride + A.off_large;
-                    const double *inv = A.ops + (size_t)l * A.stride + A.off_inv;
-                    const double *u = A.udown + (size_t)g * A.Q;
-                    for (int q = 0; q < A.Q; q++) {
-                        double qq = taylor ? 0.0 : qd[q];
-                        if (taylor)
-                            for (int c = 0; c < A.Q; c++) qq = fma(inv[q * A.Q + c], u[c], qq);
-                        double dx = pxd - lgd[q], dy = pyd - lgd[A.Q + q];
-                        far = fma(green_d(A.kind, A.k, dx * dx + dy * dy), qq, far);
-                    }
-                }
-            }
-            A.pots[t] = v * (double)gsum_scale<KIND>() + far;
-        }
-        __syncwarp();
     }
 }
 
@@ -649,7 +654,7 @@ void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
             launch_pdl(k_leaf_taylor, dim3((unsigned)tiles), dim3(TY_THREADS), smem, P->stream, T);
         }
     }
-    unsigned gr = (unsigned)((P->n_leaf_list + LEAF_WARPS - 1) / LEAF_WARPS);
+    unsigned gr = (unsigned)std::min<int64_t>((P->n_leaf_list + LEAF_WARPS - 1) / LEAF_WARPS, 1ll << 30);
     if (P->kern.kind == KIFMM_KERNEL_LAPLACE)
         launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_LAPLACE>, dim3(gr), dim3(32 * LEAF_WARPS), 0, P->stream, A,
                    (const int32_t *)P->leaf_list.p, P->n_leaf_list);

@@ -135,18 +135,20 @@ __global__ void __launch_bounds__(RS_THREADS) k_rs_scatter(const uint64_t *__res
 // The plan's sorts: one read of the keys counts the digits of every pass
 // (k_os_hist), then each pass is ONE kernel (k_os_pass) that ranks a tile's
 // keys as k_rs_scatter does and finds the tile's offset for each digit by a
-// decoupled look-back over the tiles before it: every tile publishes its digit
-// counts (AGG) as soon as it has ranked its keys and then its inclusive prefix
-// (PREFIX), and a tile sums its predecessors' values back to the first PREFIX.
+// look-back over the tiles before it: every tile publishes its digit counts as
+// soon as it has ranked its keys; the tiles of a pass all run at once, so
+// instead of a chain of inclusive prefixes (one round trip per 32 tiles) the
+// look-back has two levels, tiles within a group of 32 and group totals.
 // Tiles take their index from a counter in the order they start, so every
-// tile waited on is already running and publishes without waiting itself.
-// Waits are bounded; one that runs out sets *err (the tree build then fails).
+// tile waited on is already running and publishes without waiting on later
+// tiles.  Waits are bounded; one that runs out sets *err (the build fails).
 constexpr int OS_MAX_PASSES = 8;
 struct OsShifts {
     int n;
     int s[OS_MAX_PASSES];
 };
-constexpr unsigned long long OS_AGG = 1ull << 62, OS_PREFIX = 2ull << 62, OS_VAL = (1ull << 62) - 1;
+constexpr unsigned long long OS_AGG = 1ull << 62, OS_VAL = (1ull << 62) - 1;
+constexpr int OS_GROUP = 32;  // tiles per look-back group
 
 __device__ __forceinline__ void st_relaxed_u64(unsigned long long *p, unsigned long long v) {
     asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
@@ -254,8 +256,8 @@ __global__ void __launch_bounds__(RS_THREADS) k_os_pass(const uint64_t *__restri
         wcnt[ww][d] = tot;
         tot += c;
     }
-    unsigned long long *st = status + (size_t)tile * 256;
-    st_relaxed_u64(st + d, (tile == 0 ? OS_PREFIX : OS_AGG) | tot);
+    // this tile's digit counts, for the look-back of the later tiles
+    st_relaxed_u64(status + (size_t)tile * 256 + d, OS_AGG | tot);
     // block scans over the digits: tile-local starts, and the pass's global starts
     const uint32_t g = ghist[d];
     uint32_t xt = tot, xg = g;
@@ -290,39 +292,45 @@ __global__ void __launch_bounds__(RS_THREADS) k_os_pass(const uint64_t *__restri
             if (PAIRS) sval[li] = v[r];
         }
     }
-    uint32_t excl = 0;
-    if (tile > 0) {  // decoupled look-back, 32 predecessors per step
-        constexpr int LB = 32;
-        long long j = (long long)tile - 1, polls = 0;
-        bool found = false;
-        while (!found) {
-            unsigned long long sv[LB];
+    // Two-level look-back.  Tiles form groups of OS_GROUP: a tile sums the
+    // counts of the earlier tiles of its group (one batch of loads); the last
+    // tile of a group then publishes the group's total; a tile adds the totals
+    // of the earlier groups (one batch per OS_GROUP groups).  Every wait is on a
+    // tile with a smaller index, which started earlier and publishes without
+    // waiting on later tiles.  Polls are bounded; one that runs out sets *err.
+    const unsigned long long *gbase = status + (size_t)gridDim.x * 256;  // [groups][256] group totals
+    const unsigned grp = tile / OS_GROUP, tin = tile % OS_GROUP;
+    uint32_t excl_in = 0, excl = 0;
+    bool ok = true;
+    auto sum_published = [&](const unsigned long long *base, unsigned cnt, uint32_t &acc) {
+        unsigned rem = cnt >= 32 ? 0xffffffffu : ((1u << cnt) - 1u);
+        long long polls = 0;
+        while (rem) {
+            unsigned long long sv[OS_GROUP];
 #pragma unroll
-            for (int q = 0; q < LB; q++)
-                sv[q] = j - q >= 0 ? ld_relaxed_u64(status + (size_t)(j - q) * 256 + d) : OS_PREFIX;
-            int stop = LB;
+            for (int q = 0; q < OS_GROUP; q++) sv[q] = ((rem >> q) & 1u) ? ld_relaxed_u64(base + (size_t)q * 256 + d) : 0ull;
 #pragma unroll
-            for (int q = 0; q < LB; q++) {
-                if (found || q >= stop) continue;
-                const unsigned long long f = sv[q] & ~OS_VAL;
-                if (f == 0) {
-                    stop = q;  // not yet published: read again from there
-                } else {
-                    excl += (uint32_t)(sv[q] & OS_VAL);
-                    found = f == OS_PREFIX;
+            for (int q = 0; q < OS_GROUP; q++)
+                if (((rem >> q) & 1u) && (sv[q] & ~OS_VAL)) {
+                    acc += (uint32_t)(sv[q] & OS_VAL);
+                    rem &= ~(1u << q);
                 }
-            }
-            if (found) break;
-            j -= stop;
-            if (stop < LB && ++polls > limit) {
+            if (rem && ++polls > limit) {
                 atomicOr(err, 1ull);
-                break;
+                return false;
             }
         }
-        st_relaxed_u64(st + d, OS_PREFIX | (excl + tot));
-    }
+        return true;
+    };
+    if (tin > 0) ok = sum_published(status + (size_t)grp * OS_GROUP * 256, tin, excl_in);
+    if (tin == OS_GROUP - 1 || tile == gridDim.x - 1)
+        st_relaxed_u64((unsigned long long *)gbase + (size_t)grp * 256 + d, OS_AGG | (excl_in + tot));
+    for (unsigned g0 = 0; ok && g0 < grp; g0 += OS_GROUP)
+        ok = sum_published(gbase + (size_t)g0 * 256, min((unsigned)OS_GROUP, grp - g0), excl);
+    excl += excl_in;
     dbase[d] = wg + xg - g + excl - ts;  // global position = dbase[digit] + tile-local index
-    __syncthreads();
+    // a look-back that ran out leaves the offsets unknown: write nothing (*err is set)
+    if (__syncthreads_or(!ok)) return;
     for (int i = threadIdx.x; i < tn; i += RS_THREADS) {
         const uint64_t kk = skey[i];
         const uint32_t pos = dbase[(uint32_t)((kk >> shift) & 255)] + (uint32_t)i;
@@ -344,7 +352,8 @@ static void os_run(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_
     for (int p = 0; p < npass; p++) sh.s[p] = shifts[p];
     // scratch: digit counts [npass][256], tile counters [npass], look-back status
     // [npass][ntiles][256] (one pass's worth, cleared before each pass, when large)
-    const size_t per_pass = (size_t)ntiles * 256;
+    // per pass: the tiles' digit counts, then the groups' totals
+    const size_t per_pass = (size_t)(ntiles + (ntiles + OS_GROUP - 1) / OS_GROUP) * 256;
     const bool all_at_once = (size_t)npass * per_pass * 8 <= ((size_t)64 << 20);
     const size_t nstat = all_at_once ? (size_t)npass * per_pass : per_pass;
     P->sort_hist.alloc((size_t)npass * 256 + npass);

@@ -784,10 +784,8 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     KIFMM_CUDA(cudaMemcpyAsync(P->x.p, x, n * sizeof(double), kind, s));
     KIFMM_CUDA(cudaMemcpyAsync(P->y.p, y, n * sizeof(double), kind, s));
     P->scal.alloc(16);
-    unsigned long long init[16];
-    for (int i = 0; i < 16; i++) init[i] = 0;
-    init[0] = init[2] = ~0ull;
-    KIFMM_CUDA(cudaMemcpyAsync(P->scal.p, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    KIFMM_CUDA(cudaMemcpyAsync(P->scal.p, P->hpin + HP_INIT, 16 * sizeof(unsigned long long), cudaMemcpyHostToDevice,
+                               s));
     const int TB = 256;
     unsigned gs = grid_for(n, TB, P->num_sms * 8);
     k_bbox<<<gs, TB, 0, s>>>(P->x.p, P->y.p, n, P->scal.p);
@@ -812,8 +810,9 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     for (int full = 0; full < 2; full++) {
         KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 5, 0, 3 * sizeof(unsigned long long), s));
         launch_pdl(k_t0_count, dim3(gs), dim3(TB), 0, s, (const uint64_t *)P->pkey.p, n, (int64_t)P->ppl, P->scal.p);
-        KIFMM_CUDA(cudaMemcpyAsync(sc, P->scal.p, sizeof(sc), cudaMemcpyDeviceToHost, s));
+        KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_SCAL, P->scal.p, sizeof(sc), cudaMemcpyDeviceToHost, s));
         KIFMM_CUDA(cudaStreamSynchronize(s));
+        memcpy(sc, P->hpin + HP_SCAL, sizeof(sc));
         if (full == 0) {
             KIFMM_REQUIRE(sc[4] == 0, KIFMM_ERR_ARG, "build_tree: non-finite coordinates");
             double m, M;
@@ -875,9 +874,11 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
                 ops_started = true;
             }
             unsigned long long cv[2];
-            KIFMM_CUDA(cudaMemcpyAsync(cv, P->scal.p + 9, sizeof(cv), cudaMemcpyDeviceToHost, s));
-            KIFMM_CUDA(cudaMemcpyAsync(lcount, lc, sizeof(lcount), cudaMemcpyDeviceToHost, s));
+            KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_SCAL + 9, P->scal.p + 9, sizeof(cv), cudaMemcpyDeviceToHost, s));
+            KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_MISC, lc, sizeof(lcount), cudaMemcpyDeviceToHost, s));
             KIFMM_CUDA(cudaStreamSynchronize(s));
+            memcpy(cv, P->hpin + HP_SCAL + 9, sizeof(cv));
+            memcpy(lcount, P->hpin + HP_MISC, sizeof(lcount));
             if (cv[1] == 0 && cv[0] <= cap) {
                 n_ent = (int64_t)cv[0];
                 break;
@@ -964,10 +965,15 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
         KIFMM_LAUNCHED();
     }
     unsigned long long c5[5], sort_err = 0, lv[MAX_LEVELS];
-    KIFMM_CUDA(cudaMemcpyAsync(c5, cnt, sizeof(c5), cudaMemcpyDeviceToHost, s));
-    KIFMM_CUDA(cudaMemcpyAsync(lv, lcnt, sizeof(lv), cudaMemcpyDeviceToHost, s));
-    KIFMM_CUDA(cudaMemcpyAsync(&sort_err, P->scal.p + KIFMM_SCAL_SORT_ERR, sizeof(sort_err), cudaMemcpyDeviceToHost, s));
+    // misc[32..128) holds cnt (at 32) and lcnt (at 64)
+    static_assert(64 + MAX_LEVELS <= 128, "misc layout");
+    KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_MISC + 32, cnt, 96 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_SCAL + KIFMM_SCAL_SORT_ERR, P->scal.p + KIFMM_SCAL_SORT_ERR,
+                               sizeof(sort_err), cudaMemcpyDeviceToHost, s));
     KIFMM_CUDA(cudaStreamSynchronize(s));
+    memcpy(c5, P->hpin + HP_MISC + 32, sizeof(c5));
+    memcpy(lv, P->hpin + HP_MISC + 64, sizeof(lv));
+    sort_err = P->hpin[HP_SCAL + KIFMM_SCAL_SORT_ERR];
     KIFMM_REQUIRE(sort_err == 0, KIFMM_ERR_CUDA, "build_tree: a radix-sort look-back wait timed out");
     P->n_leaf_list = (int64_t)c5[0];
     P->leaf_loff[0] = 0;
@@ -993,8 +999,9 @@ void tree_stats(kifmm_plan *P) {
                                              P->nent.p, P->n_ent, cnt);
     KIFMM_LAUNCHED();
     unsigned long long c4[4];
-    KIFMM_CUDA(cudaMemcpyAsync(c4, cnt, sizeof(c4), cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_STATS, cnt, sizeof(c4), cudaMemcpyDeviceToHost, s));
     KIFMM_CUDA(cudaStreamSynchronize(s));
+    memcpy(c4, P->hpin + HP_STATS, sizeof(c4));
     P->n_p2p_pairs = (int64_t)c4[0];
     P->n_p2m_points = (int64_t)c4[1];
     P->n_m2l_pairs = (int64_t)c4[2];
