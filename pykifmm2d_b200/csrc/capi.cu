@@ -420,7 +420,7 @@ int kifmm_plan_destroy(kifmm_plan *P) {
         for (auto &ph : P->pending) { cudaEventDestroy(ph.a); cudaEventDestroy(ph.b); }
         P->pending.clear();
         cudaStream_t s = P->stream, side = P->side;
-        cudaEvent_t e0 = P->ops_fork, e1 = P->ops_done;
+        cudaEvent_t e0 = P->ops_fork, e1 = P->ops_done, e2 = P->tree_ev;
         bool own = P->own_stream;
         unsigned long long *hp = P->hpin;
         delete P;  // buffers are freed stream-ordered on s and on the side stream
@@ -430,6 +430,7 @@ int kifmm_plan_destroy(kifmm_plan *P) {
             cudaStreamSynchronize(side);
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);
+            cudaEventDestroy(e2);
         }
         if (own && s) cudaStreamDestroy(s);
     });

@@ -145,6 +145,8 @@ struct kifmm_plan {
     // stream waits on ops_done before the operators are used
     cudaStream_t side = nullptr;
     cudaEvent_t ops_fork = nullptr, ops_done = nullptr;
+    cudaEvent_t tree_ev = nullptr;   // build_tree: the split-cell counts are on the host
+    uint64_t spec_cap = 0;           // split-cell capacity for the next build (from the last one)
     bool ops_pending = false;
     cudaGraphExec_t graph = nullptr;  // captured apply (kifmm_graph_capture)
     int device = 0;
@@ -394,7 +396,8 @@ void tree_stats(kifmm_plan *P);
 // operators.cu
 void build_operators(kifmm_plan *P);
 void init_log_table(int device);     // table of the Laplace P2M logarithm, once per device
-void start_operators(kifmm_plan *P);  // build_operators on the side stream
+void ensure_side(kifmm_plan *P);      // side stream and its events
+void start_operators(kifmm_plan *P, bool fork_recorded = false);  // build_operators on the side stream
 cudaStream_t device_side_stream(int device);  // one per device, created on first use
 void join_operators(kifmm_plan *P);   // main stream waits for it
 // passes.cu

@@ -337,13 +337,20 @@ void build_operators(kifmm_plan *P) {
 // earlier work of the main stream, the earlier users of those buffers.  The
 // side stream is one per device, shared by all plans (kept until exit), so that
 // operator memory freed by one plan is reused by the next in stream order.
-void start_operators(kifmm_plan *P) {
-    if (!P->side) {
-        P->side = device_side_stream(P->device);
-        KIFMM_CUDA(cudaEventCreateWithFlags(&P->ops_fork, cudaEventDisableTiming));
-        KIFMM_CUDA(cudaEventCreateWithFlags(&P->ops_done, cudaEventDisableTiming));
-    }
-    KIFMM_CUDA(cudaEventRecord(P->ops_fork, P->stream));
+void ensure_side(kifmm_plan *P) {
+    if (P->side) return;
+    P->side = device_side_stream(P->device);
+    KIFMM_CUDA(cudaEventCreateWithFlags(&P->ops_fork, cudaEventDisableTiming));
+    KIFMM_CUDA(cudaEventCreateWithFlags(&P->ops_done, cudaEventDisableTiming));
+    KIFMM_CUDA(cudaEventCreateWithFlags(&P->tree_ev, cudaEventDisableTiming));
+}
+
+// fork_recorded: the caller has recorded ops_fork on the main stream at the
+// point after which the operators may start (build_tree records it before the
+// split-cell kernels, which the operators do not depend on)
+void start_operators(kifmm_plan *P, bool fork_recorded) {
+    ensure_side(P);
+    if (!fork_recorded) KIFMM_CUDA(cudaEventRecord(P->ops_fork, P->stream));
     KIFMM_CUDA(cudaStreamWaitEvent(P->side, P->ops_fork, 0));
     struct Swap {  // launches and allocations go to the side stream meanwhile
         kifmm_plan *P;

@@ -337,9 +337,10 @@ __device__ __forceinline__ unsigned long long hs_count(const HashSet &H) {
 
 // X-list (tree.py:546-576, numba_get_Xlist :446-458): for levels 1..L-2, a
 // real leaf (cell not split, parent split) next to a split cell becomes an
-// X-list cell.  One item per (split cell, neighbour); the warp's new cells are
+// X-list cell (every split cell lies on a level <= L-2, so the level range
+// follows from the split cells themselves).  One item per (split cell, neighbour); the warp's new cells are
 // appended together (one count atomic per warp, one level atomic per level).
-__global__ void __launch_bounds__(256) k_xlist(HashSet H, int L) {
+__global__ void __launch_bounds__(256) k_xlist(HashSet H) {
     pdl_trigger();
     pdl_wait();
     const unsigned long long n = hs_count(H);
@@ -356,7 +357,7 @@ __global__ void __launch_bounds__(256) k_xlist(HashSet H, int L) {
             const int d = (int)(j - 9 * i);
             const uint64_t s = H.list[i];
             l = (int)(s >> ENT_LEVEL_SHIFT);
-            if (d != 4 && !(s & 1) && l >= 1 && l <= L - 2) {
+            if (d != 4 && !(s & 1) && l >= 1) {  // split cells lie on levels <= L-2
                 const uint64_t k = (s >> 1) & KEY56;
                 const int64_t cx = (int64_t)compact2(k >> 1) + d / 3 - 1, cy = (int64_t)compact2(k) + d % 3 - 1;
                 const int64_t side = 1ll << l;
@@ -805,13 +806,57 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     HashSet H{};
     H.count = P->scal.p + 9;
     H.ovf = P->scal.p + 10;
+    P->misc.alloc(128);
+    unsigned long long *lc = (unsigned long long *)P->misc.p;  // [32] entries per level
+    unsigned long long lcount[32] = {};
+    const unsigned cgrid = grid_for((n + 31) / 32 * 32, TB, P->num_sms * 64);
+    ensure_side(P);
+    // The split-cell set for a list capacity: table and list sized and
+    // cleared, the closure and the X-list, then count, overflow and per-level
+    // counts to the host, marked by tree_ev.
+    auto queue_closure = [&](uint64_t cap) {
+        uint64_t hcap = 1;
+        while (hcap < 2 * cap) hcap <<= 1;
+        P->hash.alloc(hcap);
+        P->hash_cap = hcap;
+        P->list.alloc(cap);
+        KIFMM_CUDA(cudaMemsetAsync(P->hash.p, 0xFF, hcap * sizeof(uint64_t), s));
+        KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 9, 0, 2 * sizeof(unsigned long long), s));
+        KIFMM_CUDA(cudaMemsetAsync(lc, 0, 32 * sizeof(unsigned long long), s));
+        H.tab = (unsigned long long *)P->hash.p;
+        H.mask = hcap - 1;
+        H.list = P->list.p;
+        H.cap = cap;
+        H.lcount = lc;
+        launch_pdl(k_closure, dim3(cgrid), dim3(TB), 0, s, (const uint64_t *)P->pkey.p, n, (int64_t)P->ppl, H);
+        // the X-list reads the complete split set: nine items per entry, grid-stride
+        launch_pdl(k_xlist, dim3(grid_for(9 * (int64_t)cap, TB, P->num_sms * 8)), dim3(TB), 0, s, H);
+        KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_SCAL + 9, P->scal.p + 9, 2 * sizeof(unsigned long long),
+                                   cudaMemcpyDeviceToHost, s));
+        KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_MISC, lc, sizeof(lcount), cudaMemcpyDeviceToHost, s));
+        KIFMM_CUDA(cudaEventRecord(P->tree_ev, s));
+    };
     unsigned long long sc[9];  // [0..3] ordered extremes, [4] non-finite, [5..7] T0 count/depth/overflow, [8] outside
     unsigned long long *st = sc + 5;
+    // T0 counts and the root box go to the host (marked by ops_fork, after
+    // which the operators may start); the split-cell set is queued right
+    // behind them, before the counts are seen, with the capacity of the last
+    // build (or an estimate from n): it is kept if the sort by the top 32 key
+    // bits was enough and the set fitted, and rebuilt otherwise.
+    bool spec = n > P->ppl;
+    uint64_t spec_cap = P->spec_cap;
+    if (!spec_cap)
+        spec_cap = std::min<uint64_t>(16 * (uint64_t)std::max<int64_t>(n / P->ppl, 1), 2 * (uint64_t)n) + 4096;
     for (int full = 0; full < 2; full++) {
         KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 5, 0, 3 * sizeof(unsigned long long), s));
         launch_pdl(k_t0_count, dim3(gs), dim3(TB), 0, s, (const uint64_t *)P->pkey.p, n, (int64_t)P->ppl, P->scal.p);
         KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_SCAL, P->scal.p, sizeof(sc), cudaMemcpyDeviceToHost, s));
-        KIFMM_CUDA(cudaStreamSynchronize(s));
+        KIFMM_CUDA(cudaEventRecord(P->ops_fork, s));
+        if (spec && full == 0) {
+            PhaseScope ph_c(P, KIFMM_PHASE_CLOSURE);
+            queue_closure(spec_cap);
+        }
+        KIFMM_CUDA(cudaEventSynchronize(P->ops_fork));
         memcpy(sc, P->hpin + HP_SCAL, sizeof(sc));
         if (full == 0) {
             KIFMM_REQUIRE(sc[4] == 0, KIFMM_ERR_ARG, "build_tree: non-finite coordinates");
@@ -824,6 +869,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
                           "build_tree: more than Ncutoff points on one integer point (zero-width root box)");
         }
         if (full || (st[1] <= (unsigned long long)FAST_LEVELS && st[2] == 0)) break;
+        spec = false;  // the queued set used the partial order: rebuilt below
         PhaseScope ph(P, KIFMM_PHASE_SORT);
         radix_sort_pairs(P->pkey.p, P->perm.p, P->key2.p, P->perm2.p, n, 2 * KEY_DEPTH, P);
     }
@@ -837,56 +883,33 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     int L = n > P->ppl ? (int)st[1] + 1 : 1;
     KIFMM_REQUIRE(L <= MAX_LEVELS, KIFMM_ERR_DEPTH, "build_tree: too many levels");
     P->L = L;
-    uint64_t t0count = st[0];
-    bool ops_started = false;
+    const uint64_t t0count = st[0];
+    // the operators need only the root width and the depth: they run on the
+    // side stream while the split-cell set and the node tables are built
+    start_operators(P, true);
 
     int64_t n_ent = 0;
-    P->misc.alloc(128);
-    unsigned long long *lc = (unsigned long long *)P->misc.p;  // [32] entries per level
-    unsigned long long lcount[32] = {};
     if (L > 1) {
         PhaseScope ph_c(P, KIFMM_PHASE_CLOSURE);
-        const unsigned cgrid = grid_for((n + 31) / 32 * 32, TB, P->num_sms * 64);
+        const uint64_t exact = t0count * 16 + 4096;
         for (int attempt = 0;; attempt++) {
-            uint64_t cap = (t0count * 16 + 4096) << (2 * attempt);
-            uint64_t hcap = 1;
-            while (hcap < 2 * cap) hcap <<= 1;
-            P->hash.alloc(hcap);
-            P->hash_cap = hcap;
-            P->list.alloc(cap);
-            KIFMM_CUDA(cudaMemsetAsync(P->hash.p, 0xFF, hcap * sizeof(uint64_t), s));
-            KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 9, 0, 2 * sizeof(unsigned long long), s));
-            KIFMM_CUDA(cudaMemsetAsync(lc, 0, 32 * sizeof(unsigned long long), s));
-            H.tab = (unsigned long long *)P->hash.p;
-            H.mask = hcap - 1;
-            H.list = P->list.p;
-            H.cap = cap;
-            H.lcount = lc;
-            launch_pdl(k_closure, dim3(cgrid), dim3(TB), 0, s, (const uint64_t *)P->pkey.p, n, (int64_t)P->ppl, H);
-            // the X-list reads the complete split set: nine items per entry
-            // (at most cap entries), one wave of blocks for the usual sizes
-            launch_pdl(k_xlist, dim3(grid_for(9 * (int64_t)std::min<uint64_t>(cap, 4 * t0count + 4096), TB,
-                                              P->num_sms * 8)),
-                       dim3(TB), 0, s, H, L);
-            if (!ops_started) {
-                // the operators overlap the rest of the tree build
-                start_operators(P);
-                ops_started = true;
+            uint64_t cap = spec_cap;
+            if (!spec || attempt > 0) {
+                cap = exact << (2 * std::max(attempt - (spec ? 1 : 0), 0));
+                queue_closure(cap);
             }
+            KIFMM_CUDA(cudaEventSynchronize(P->tree_ev));
             unsigned long long cv[2];
-            KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_SCAL + 9, P->scal.p + 9, sizeof(cv), cudaMemcpyDeviceToHost, s));
-            KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_MISC, lc, sizeof(lcount), cudaMemcpyDeviceToHost, s));
-            KIFMM_CUDA(cudaStreamSynchronize(s));
             memcpy(cv, P->hpin + HP_SCAL + 9, sizeof(cv));
             memcpy(lcount, P->hpin + HP_MISC, sizeof(lcount));
             if (cv[1] == 0 && cv[0] <= cap) {
                 n_ent = (int64_t)cv[0];
                 break;
             }
-            KIFMM_REQUIRE(attempt < 4, KIFMM_ERR_NOMEM, "build_tree: split-cell set overflow");
+            KIFMM_REQUIRE(attempt < 5, KIFMM_ERR_NOMEM, "build_tree: split-cell set overflow");
         }
+        P->spec_cap = exact;
     }
-    if (!ops_started) start_operators(P);
     P->n_ent = n_ent;
     P->ent.alloc(n_ent);
     P->key2.alloc(std::max<int64_t>(n, n_ent));
