@@ -635,6 +635,9 @@ __global__ void __launch_bounds__(LT_THREADS) k_lists_write(int64_t n_nodes, con
 // order), and writes them at the level's offset (the counts of the levels
 // above).  Keys are distinct within a level: a cell is either split or X-list.
 constexpr int ES_THREADS = 1024, ES_WARPS = ES_THREADS / 32, ES_CAP = 12288;
+// levels <= 10 rank through a bitmap of 4^10 bits (128 KB) plus 4096 group
+// prefixes (16 KB), inside the radix sort's shared memory
+constexpr int ES_BITMAP_LEVELS = 10;
 constexpr size_t ES_SMEM = (size_t)2 * ES_CAP * sizeof(uint64_t) + (size_t)ES_WARPS * 256 * sizeof(uint32_t);
 __global__ void __launch_bounds__(ES_THREADS) k_ent_sort(const uint64_t *__restrict__ list, int64_t n_ent,
                                                          const unsigned long long *__restrict__ lcount,
@@ -648,7 +651,7 @@ __global__ void __launch_bounds__(ES_THREADS) k_ent_sort(const uint64_t *__restr
     pdl_wait();
     const int l = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int m = (int)lcount[l];
-    if (m == 0 || m > ES_CAP) return;  // the host sorts globally when a level is larger
+    if (m == 0 || (l > ES_BITMAP_LEVELS && m > ES_CAP)) return;  // the host sorts globally then
     if (threadIdx.x == 0) {
         long long o = 0;
         for (int q = 0; q < l; q++) o += (long long)lcount[q];
@@ -657,6 +660,59 @@ __global__ void __launch_bounds__(ES_THREADS) k_ent_sort(const uint64_t *__restr
     }
     __syncthreads();
     constexpr int U = 8;
+    if (l <= ES_BITMAP_LEVELS) {
+        // Levels up to ES_BITMAP_LEVELS have at most 4^l cells: one bit per
+        // cell in shared memory, prefix counts over groups of 8 words, and an
+        // entry's rank is the number of set bits below its key.
+        uint32_t *bm = (uint32_t *)es_sm;                 // [4^l / 32] words
+        uint32_t *gp = bm + (1u << (2 * ES_BITMAP_LEVELS - 5));  // group prefixes
+        const int nwords = (int)(((1u << (2 * l)) + 31) >> 5), ngroups = (nwords + 7) >> 3;
+        for (int i = threadIdx.x; i < nwords; i += ES_THREADS) bm[i] = 0;
+        __syncthreads();
+        for (int pass = 0; pass < 2; pass++) {
+            for (int64_t base = 0; base < n_ent; base += (int64_t)U * ES_THREADS) {
+                uint64_t e[U];
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    const int64_t j = base + (int64_t)u * ES_THREADS + threadIdx.x;
+                    e[u] = j < n_ent ? list[j] : ENT_EMPTY;
+                }
+#pragma unroll
+                for (int u = 0; u < U; u++) {
+                    if (e[u] == ENT_EMPTY || (int)(e[u] >> ENT_LEVEL_SHIFT) != l) continue;
+                    const uint32_t k = (uint32_t)((e[u] >> 1) & 0xFFFFFFFFull), wd = k >> 5, bit = k & 31;
+                    if (pass == 0) {
+                        atomicOr(&bm[wd], 1u << bit);
+                    } else {
+                        uint32_t r = gp[wd >> 3] + __popc(bm[wd] & ((1u << bit) - 1u));
+                        for (uint32_t q = wd & ~7u; q < wd; q++) r += __popc(bm[q]);
+                        ent[s_eoff + r] = e[u];
+                    }
+                }
+            }
+            if (pass == 0) {
+                __syncthreads();
+                // groups of 8 words: counts, then an exclusive scan (up to 4 groups per thread)
+                const int per = (ngroups + ES_THREADS - 1) / ES_THREADS, g0 = threadIdx.x * per;
+                uint32_t c[4] = {0, 0, 0, 0}, tsum = 0;
+                for (int q = 0; q < per && q < 4; q++) {
+                    const int g = g0 + q;
+                    if (g < ngroups)
+                        for (int i = 8 * g; i < 8 * g + 8 && i < nwords; i++) c[q] += __popc(bm[i]);
+                    tsum += c[q];
+                }
+                unsigned total;
+                unsigned run = block_excl_scan(tsum, scan_sm, total);
+                for (int q = 0; q < per && q < 4; q++) {
+                    const int g = g0 + q;
+                    if (g < ngroups) gp[g] = run;
+                    run += c[q];
+                }
+                __syncthreads();
+            }
+        }
+        return;
+    }
     for (int64_t base = 0; base < n_ent; base += (int64_t)U * ES_THREADS) {
         uint64_t e[U];
 #pragma unroll
@@ -915,8 +971,8 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     P->key2.alloc(std::max<int64_t>(n, n_ent));
     if (n_ent) {
         PhaseScope ph_e(P, KIFMM_PHASE_ENTRIES);
-        unsigned long long lmax = 0;
-        for (int l = 0; l < L; l++) lmax = std::max(lmax, lcount[l]);
+        unsigned long long lmax = 0;  // the largest level that k_ent_sort radix-sorts
+        for (int l = ES_BITMAP_LEVELS + 1; l < L; l++) lmax = std::max(lmax, lcount[l]);
         if (lmax <= (unsigned long long)ES_CAP) {
             ensure_dyn_smem(k_ent_sort, ES_SMEM);
             launch_pdl(k_ent_sort, dim3((unsigned)L), dim3(ES_THREADS), ES_SMEM, s, (const uint64_t *)P->list.p,

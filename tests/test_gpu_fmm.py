@@ -92,23 +92,43 @@ def test_fp64_vs_oracle_200k_mixture():
     assert rel(pot, po) <= 1e-7
 
 
-def test_tree_wide_levels_vs_oracle():
-    """400k uniform points, Ncutoff 8: level 7 holds 16384 split cells, more
-    than one block sorts in shared memory, so the entries take the global
-    radix sort; the tree must still match the oracle exactly."""
+def _tree_vs_oracle(x, y, ncutoff):
     import pykifmm2d_b200 as P
     from oracle import oracle as O
-    rng = np.random.default_rng(5)
-    x, y = rng.uniform(-1, 1, 400_000), rng.uniform(-1, 1, 400_000)
     kern = P.LaplaceKernel()
-    f = P.FMM(x, y, P.Get_Kernel_Functions(kern), P.prepare_numba_functions_on_the_fly(kern), 16, 8)
+    f = P.FMM(x, y, P.Get_Kernel_Functions(kern), P.prepare_numba_functions_on_the_fly(kern), 16, ncutoff)
     f.build_tree()
     nodes_g, pl_g = f.export_tree()
-    o = O.OracleTree(x, y, 8)
+    o = O.OracleTree(x, y, ncutoff)
     nodes_o, _ = o.export()
-    assert (nodes_o[:, 0] == 7).sum() == 16384
     np.testing.assert_array_equal(nodes_g, nodes_o)
     np.testing.assert_array_equal(pl_g, o.locate(x, y))
+    return nodes_o
+
+
+def test_tree_wide_levels_vs_oracle():
+    """400k uniform points, Ncutoff 8: level 7 holds 16384 split cells (more
+    than the shared-memory radix sort takes; the level is ranked through the
+    bitmap); the tree must match the oracle exactly."""
+    rng = np.random.default_rng(5)
+    x, y = rng.uniform(-1, 1, 400_000), rng.uniform(-1, 1, 400_000)
+    nodes = _tree_vs_oracle(x, y, 8)
+    assert (nodes[:, 0] == 7).sum() == 16384
+
+
+def test_tree_wide_deep_level_vs_oracle():
+    """Two points in each cell of a 128 x 128 block of level-11 cells, Ncutoff
+    1: level 11 holds 16384 split cells, too many for one block's radix sort,
+    so the entries take the global onesweep sort; the tree must match the
+    oracle exactly."""
+    i, j = np.meshgrid(np.arange(128), np.arange(128), indexing="ij")
+    i, j = i.ravel().astype(np.float64), j.ravel().astype(np.float64)
+    h = 1.0 / 2048  # level-11 width of the root box [0, 1]
+    x = np.concatenate([(i + 0.25) * h, (i + 0.75) * h, [1.0]])
+    y = np.concatenate([(j + 0.25) * h, (j + 0.75) * h, [1.0]])
+    nodes = _tree_vs_oracle(x, y, 1)
+    split11 = (nodes[:, 0] == 11) & (nodes[:, 3] == 0) & (nodes[:, 4] == 0)
+    assert split11.sum() == 16384
 
 
 def test_direct_sum_gpu_vs_oracle(golden_cases):
