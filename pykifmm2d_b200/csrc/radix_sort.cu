@@ -200,7 +200,12 @@ __global__ void __launch_bounds__(RS_THREADS) k_os_hist(const uint64_t *__restri
 // One pass.  The tile's keys are ranked per warp, ordered by digit in shared
 // memory (tile-local digit starts tstart[]), and written out in that order so
 // that consecutive threads store consecutive positions of one digit's run.
-constexpr size_t OS_PASS_SMEM = (size_t)RS_TILE * (sizeof(uint64_t) + sizeof(int32_t));
+// keys per thread in a onesweep tile (4096-key tiles, two CTAs per SM, every
+// tile of a 1M-key pass resident at once); 4 and 8 keys per thread measured
+// 2.2x slower on the 1M-point tree build (0.20 against 0.091 ms for the sort)
+constexpr int OS_ITEMS = 16;
+constexpr int OS_TILE = RS_THREADS * OS_ITEMS;
+constexpr size_t OS_PASS_SMEM = (size_t)OS_TILE * (sizeof(uint64_t) + sizeof(int32_t));
 template <bool PAIRS>
 __global__ void __launch_bounds__(RS_THREADS) k_os_pass(const uint64_t *__restrict__ key, const int32_t *__restrict__ val,
                                                          uint64_t *__restrict__ okey, int32_t *__restrict__ oval,
@@ -210,8 +215,8 @@ __global__ void __launch_bounds__(RS_THREADS) k_os_pass(const uint64_t *__restri
     pdl_trigger();
     pdl_wait();
     extern __shared__ __align__(16) unsigned char os_sm[];
-    uint64_t *skey = (uint64_t *)os_sm;                        // [RS_TILE]
-    int32_t *sval = (int32_t *)(os_sm + RS_TILE * sizeof(uint64_t));
+    uint64_t *skey = (uint64_t *)os_sm;                        // [OS_TILE]
+    int32_t *sval = (int32_t *)(os_sm + OS_TILE * sizeof(uint64_t));
     __shared__ uint32_t wcnt[RS_WARPS][256];
     __shared__ uint32_t tstart[256];
     __shared__ uint32_t dbase[256];
@@ -222,22 +227,22 @@ __global__ void __launch_bounds__(RS_THREADS) k_os_pass(const uint64_t *__restri
     for (int d = threadIdx.x; d < 256 * RS_WARPS; d += RS_THREADS) (&wcnt[0][0])[d] = 0;
     __syncthreads();
     const unsigned tile = tile_s;
-    const int64_t tbase = (int64_t)tile * RS_TILE;
-    const int tn = (int)min((int64_t)RS_TILE, n - tbase);
-    const int64_t t0 = tbase + (int64_t)w * (RS_ITEMS * 32);
-    uint64_t k[RS_ITEMS];
-    int32_t v[RS_ITEMS];
-    uint32_t rank[RS_ITEMS];
+    const int64_t tbase = (int64_t)tile * OS_TILE;
+    const int tn = (int)min((int64_t)OS_TILE, n - tbase);
+    const int64_t t0 = tbase + (int64_t)w * (OS_ITEMS * 32);
+    uint64_t k[OS_ITEMS];
+    int32_t v[OS_ITEMS];
+    uint32_t rank[OS_ITEMS];
     const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
-    for (int r = 0; r < RS_ITEMS; r++) {
+    for (int r = 0; r < OS_ITEMS; r++) {
         const int64_t idx = t0 + r * 32 + lane;
         const bool ok = idx < n;
         k[r] = ok ? key[idx] : 0;
         if (PAIRS) v[r] = ok ? val[idx] : 0;
     }
 #pragma unroll
-    for (int r = 0; r < RS_ITEMS; r++) {
+    for (int r = 0; r < OS_ITEMS; r++) {
         const bool ok = t0 + r * 32 + lane < n;
         const uint32_t d = ok ? (uint32_t)((k[r] >> shift) & 255) : 256u;
         const unsigned peers = warp_match_digit(d);
@@ -284,7 +289,7 @@ __global__ void __launch_bounds__(RS_THREADS) k_os_pass(const uint64_t *__restri
     // the tile in digit order into shared memory, before the look-back, so
     // that the look-back has the registers for wide batches
 #pragma unroll
-    for (int r = 0; r < RS_ITEMS; r++) {
+    for (int r = 0; r < OS_ITEMS; r++) {
         if (t0 + r * 32 + lane < n) {
             const uint32_t dd = (uint32_t)((k[r] >> shift) & 255);
             const uint32_t li = tstart[dd] + wcnt[w][dd] + rank[r];
@@ -346,7 +351,7 @@ static void os_run(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_
     KIFMM_REQUIRE(n < (1ll << 31), KIFMM_ERR_ARG, "radix sort: more than 2^31 keys");
     KIFMM_REQUIRE(npass <= OS_MAX_PASSES, KIFMM_ERR_ARG, "radix sort: too many passes");
     cudaStream_t s = P->stream;
-    const int64_t ntiles = (n + RS_TILE - 1) / RS_TILE;
+    const int64_t ntiles = (n + OS_TILE - 1) / OS_TILE;
     OsShifts sh{};
     sh.n = npass;
     for (int p = 0; p < npass; p++) sh.s[p] = shifts[p];
