@@ -58,6 +58,7 @@ __device__ __forceinline__ double gval(const OpsArgs &A, double sx, double sy, d
 // then every thread produces its elements of the next matrix from the current
 // one (two buffers, so a step needs no separate read and write phases).
 constexpr int INV_THREADS = 256;
+static_assert(INV_THREADS % 128 == 0, "the elimination maps 128 columns (2 Nequiv <= 128) per row phase");
 __global__ void __launch_bounds__(INV_THREADS) k_ops_inverse(OpsArgs A) {
     extern __shared__ double sm[];
     __shared__ int s_piv;
@@ -105,17 +106,20 @@ __global__ void __launch_bounds__(INV_THREADS) k_ops_inverse(OpsArgs A) {
         // is subtracted from every other row to clear column k
         const int p = s_piv;
         const double rp = 1.0 / a[p * ld + k];
-        for (int e = tid; e < Q * Q2; e += INV_THREADS) {
-            const int r = e / Q2, c = e % Q2;
+        // thread = column tid % 128 (2Q <= 128) and every second row from tid / 128
+        const int c = tid & 127;
+        if (c < Q2) {
             const double pc = a[p * ld + c] * rp;  // normalised pivot row
-            double v;
-            if (r == k) {
-                v = pc;
-            } else {
-                const int src = r == p ? k : r;
-                v = a[src * ld + c] - a[src * ld + k] * pc;
+            for (int r = tid >> 7; r < Q; r += INV_THREADS / 128) {
+                double v;
+                if (r == k) {
+                    v = pc;
+                } else {
+                    const int src = r == p ? k : r;
+                    v = a[src * ld + c] - a[src * ld + k] * pc;
+                }
+                nb[r * ld + c] = v;
             }
-            nb[r * ld + c] = v;
         }
         __syncthreads();
         double *t = a;
@@ -128,19 +132,26 @@ __global__ void __launch_bounds__(INV_THREADS) k_ops_inverse(OpsArgs A) {
 
 // P_o = M2LS_o . Inv_l (far offsets), M2M and L2L compositions; the inverse
 // and the kernel-matrix block are staged in shared memory.
+// Slots 0..48: M2L offsets (the 3x3 near block skipped); 49..52: M2M of
+// child q = slot - 49; 53..56: L2L of child q = slot - 53.  A child's slot
+// needs only its Q x Q block of M2MC, so the M2M and L2L work is spread over
+// four blocks each, like the offsets.
+constexpr int OPS_COMPOSE_SLOTS = 57;
 __global__ void k_ops_compose(OpsArgs A) {
     extern __shared__ double sm_c[];
-    const int Q = A.Q, l = blockIdx.x, slot = blockIdx.y;  // 0..48 offsets, 49 M2M, 50 L2L
+    const int Q = A.Q, l = blockIdx.x, slot = blockIdx.y;
     if (l < 1 || l >= A.L) return;
     if (slot < 49) {
         int ox = slot / 7 - 3, oy = slot % 7 - 3;
         if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1) return;
     }
     if (slot >= 49 && l + 1 >= A.L) return;
+    const bool m2m = slot >= 49 && slot < 53, l2l = slot >= 53;
+    const int q = m2m ? slot - 49 : slot - 53;  // child (M2M, L2L)
     double *b = A.ops + (size_t)l * A.stride;
-    const double *inv = slot == 49 ? A.ops + (size_t)(l + 1) * A.stride + off_inv(Q) : b + off_inv(Q);
-    double *iv = sm_c;              // [Q][Q]
-    double *mm = sm_c + Q * Q;      // M2LS block [Q][Q] or M2MC [Q][4Q]
+    const double *inv = m2m ? A.ops + (size_t)(l + 1) * A.stride + off_inv(Q) : b + off_inv(Q);
+    double *iv = sm_c;          // [Q][Q]
+    double *mm = sm_c + Q * Q;  // M2LS block, or the child's block of M2MC, [Q][Q]
     for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) iv[e] = inv[e];
     // the kernel-matrix block, evaluated here (class_fmm.py:219-250)
     const double *sx = b + off_small(Q), *sy = sx + Q, *lx = b + off_large(Q), *ly = lx + Q;
@@ -151,13 +162,13 @@ __global__ void k_ops_compose(OpsArgs A) {
             const int r = e / Q, t = e % Q;
             mm[e] = gval(A, sx[t] + ox * w, sy[t] + oy * w, sx[r], sy[r]);
         }
-    } else {  // M2MC_l[r][q Q + t] = G(small_{l+1, t} + child offset q -> large_r)
+    } else {  // M2MC_l[r][q Q + t] = G(small_{l+1, t} + child offset q -> large_r), child q's block
         const double *b1 = A.ops + (size_t)(l + 1) * A.stride;
         const double *cx = b1 + off_small(Q), *cy = cx + Q;
         const double hw = 0.5 * lvl_width(A, l + 1);
-        for (int e = threadIdx.x; e < Q * 4 * Q; e += blockDim.x) {
-            const int r = e / (4 * Q), c = e % (4 * Q), qc = c / Q, t = c % Q;
-            const double ox = (qc >= 2) ? hw : -hw, oy = (qc & 1) ? hw : -hw;
+        const double ox = (q >= 2) ? hw : -hw, oy = (q & 1) ? hw : -hw;
+        for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) {
+            const int r = e / Q, t = e % Q;
             mm[e] = gval(A, cx[t] + ox, cy[t] + oy, lx[r], ly[r]);
         }
     }
@@ -170,21 +181,21 @@ __global__ void k_ops_compose(OpsArgs A) {
             for (int t = 0; t < Q; t++) s = fma(mm[r * Q + t], iv[t * Q + c], s);
             p[e] = s;
         }
-    } else if (slot == 49) {
-        double *o = b + off_m2m(Q);  // [4Q cols][Q rows]
-        for (int e = threadIdx.x; e < Q * 4 * Q; e += blockDim.x) {
-            int r = e / (4 * Q), c = e % (4 * Q), qc = c / Q, cc = c % Q;
+    } else if (m2m) {
+        double *o = b + off_m2m(Q);  // [4Q cols][Q rows]; this child's columns q Q .. q Q + Q - 1
+        for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) {
+            int r = e / Q, cc = e % Q;
             double s = 0;
-            for (int t = 0; t < Q; t++) s = fma(mm[r * 4 * Q + qc * Q + t], iv[t * Q + cc], s);
-            o[(size_t)c * Q + r] = s;
+            for (int t = 0; t < Q; t++) s = fma(mm[r * Q + t], iv[t * Q + cc], s);
+            o[(size_t)(q * Q + cc) * Q + r] = s;
         }
-    } else {
-        double *o = b + off_l2l(Q);  // [Q cols][4Q rows]
-        for (int e = threadIdx.x; e < 4 * Q * Q; e += blockDim.x) {
-            int r = e / Q, c = e % Q;  // r in 4Q (child block q = r / Q), c in Q
+    } else if (l2l) {
+        double *o = b + off_l2l(Q);  // [Q cols][4Q rows]; this child's rows q Q .. q Q + Q - 1
+        for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) {
+            int rr = e / Q, c = e % Q;
             double s = 0;
-            for (int t = 0; t < Q; t++) s = fma(mm[t * 4 * Q + r], iv[t * Q + c], s);
-            o[(size_t)c * 4 * Q + r] = s;
+            for (int t = 0; t < Q; t++) s = fma(mm[t * Q + rr], iv[t * Q + c], s);
+            o[(size_t)c * 4 * Q + q * Q + rr] = s;
         }
     }
 }
@@ -306,7 +317,7 @@ void build_operators(kifmm_plan *P) {
     if (L >= 2) {
         size_t csm = (size_t)5 * Q * Q * sizeof(double);
         ensure_dyn_smem(k_ops_compose, csm);
-        k_ops_compose<<<dim3(L, 51), 256, csm, s>>>(A);
+        k_ops_compose<<<dim3(L, OPS_COMPOSE_SLOTS), 256, csm, s>>>(A);
         KIFMM_LAUNCHED();
         k_ops_assemble<<<dim3(L, 9), 256, 0, s>>>(A, rowmax);
         KIFMM_LAUNCHED();

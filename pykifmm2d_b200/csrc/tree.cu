@@ -499,7 +499,7 @@ __global__ void k_nodes(LevelTable T, EntryIndex X, int64_t n_nodes, const uint6
 // k_lists_scan turns the counts into offsets, k_lists_write compacts each
 // tile in order.  cnt: [0] leaf_list, [1] p2m_list, [2] leaves, [3] fake,
 // [4] xlist.
-constexpr int LT_THREADS = 256, LT_TILE = LT_THREADS * 8;
+constexpr int LT_THREADS = 256, LT_TILE = LT_THREADS * 2;  // ~300 blocks for 150k nodes
 struct ListFlags {
     bool leaf = false, p2m = false, real_leaf = false, fake = false, xl = false;
 };
