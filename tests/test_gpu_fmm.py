@@ -131,6 +131,45 @@ def test_tree_wide_deep_level_vs_oracle():
     assert split11.sum() == 16384
 
 
+def _tight_pairs(sep_level, npairs=1000, seed=3):
+    """npairs point pairs in distinct level-6 cells of the root box [0, 1];
+    the two points of a pair share their level-`sep_level` cell and part at
+    the next level, so with Ncutoff 1 every pair splits down to sep_level."""
+    rng = np.random.default_rng(seed)
+    cells = rng.choice(64 * 64, npairs, replace=False)
+    cx, cy = (cells // 64) / 64.0, (cells % 64) / 64.0
+    h = 2.0 ** -sep_level
+    bx = cx + np.floor(0.37 / 64 / h) * h
+    by = cy + np.floor(0.61 / 64 / h) * h
+    x = np.concatenate([bx + 0.25 * h, bx + 0.75 * h, [1.0]])
+    y = np.concatenate([by + 0.25 * h, by + 0.75 * h, [1.0]])
+    return x, y
+
+
+@pytest.mark.parametrize("sep_level,levels", [(15, 17), (20, 22)])
+def test_tree_split_set_retry_vs_oracle(sep_level, levels):
+    """Split-cell sets far larger than a first build's capacity estimate
+    (162k and 282k split cells from 2,001 points), so the build retries with
+    the exact capacity; at 22 levels the top-32-bit sort is not enough and the
+    keys are sorted in full.  A second build on the same plan starts from the
+    first one's capacity.  Both trees must match the oracle exactly."""
+    import pykifmm2d_b200 as P
+    from oracle import oracle as O
+    x, y = _tight_pairs(sep_level)
+    kern = P.LaplaceKernel()
+    f = P.FMM(x, y, P.Get_Kernel_Functions(kern), P.prepare_numba_functions_on_the_fly(kern), 16, 1)
+    o = O.OracleTree(x, y, 1)
+    assert o.levels == levels
+    nodes_o, _ = o.export()
+    pl_o = o.locate(x, y)
+    for _ in range(2):
+        f.build_tree()
+        assert f.tree_info().levels == levels
+        nodes_g, pl_g = f.export_tree()
+        np.testing.assert_array_equal(nodes_g, nodes_o)
+        np.testing.assert_array_equal(pl_g, pl_o)
+
+
 def test_direct_sum_gpu_vs_oracle(golden_cases):
     import pykifmm2d_b200 as P
     from oracle import oracle as O
