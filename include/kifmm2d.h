@@ -165,6 +165,25 @@ int kifmm_get_tree_info(kifmm_plan *plan, kifmm_tree_info *info);
  * Host buffers; either may be NULL. */
 int kifmm_export_tree(kifmm_plan *plan, int64_t *nodes, int64_t *point_leaf);
 
+/* Interaction lists for parity checks, with node numbers = rows of
+ * kifmm_export_tree's nodes array (host buffers, each may be NULL):
+ *   colleagues[n_nodes][9]: the same-level colleague at cell offset (dx, dy)
+ *     in slot (dx+1)*3 + (dy+1), -1 if none -- the reference's Level.colleagues
+ *     (tree.py:349-375) ordered by direction;
+ *   m2l[*n_m2l][2]: (target, source) node pairs of every M2L translation the
+ *     apply performs: the children of each split cell receive, from each
+ *     colleague's child group that holds points, every well-separated child --
+ *     the reference's numba_add_interactions blocks (class_fmm.py:17-33,
+ *     :323-343) except those into the fake children of X-list leaves, whose
+ *     local expansions the reference computes but never reads;
+ *   p2p[*n_p2p][2]: (leaf, source) node pairs of the near field: each leaf
+ *     holding points reads every colleague holding points
+ *     (numba_target_neighbor_evaluation, class_fmm.py:90-111).
+ * n_m2l / n_p2p receive the pair counts; when m2l / p2p is given, the count
+ * pointer must hold its capacity in pairs on entry (KIFMM_ERR_ARG if short). */
+int kifmm_export_lists(kifmm_plan *plan, int64_t *colleagues, int64_t *m2l, int64_t *n_m2l, int64_t *p2p,
+                       int64_t *n_p2p);
+
 /* Release the plan and its device memory. */
 int kifmm_plan_destroy(kifmm_plan *plan);
 
@@ -225,15 +244,21 @@ int64_t kifmm_launch_count(void);
  * keys[i] = 58-bit Morton key (x bit above y bit) of the i-th point in
  * sorted order on the 2^29 x 2^29 grid of the root box [root_min, root_max]
  * (integer corners, as kifmm_get_tree_info reports; points outside the box
- * clamp to its edge cells), perm[i] = index of that point in x, y.  The sort
- * is stable.  x, y, keys, perm are device pointers on the current device;
- * work is queued on `stream` (NULL: the legacy default stream) and the call
- * returns before it finishes.  Scratch is one fixed device array of the
- * library (about 12.3 MB, held by every GPU that loads the library until the
- * process exits), so n may not exceed KIFMM_NOALLOC_MAX_POINTS.  The first
- * call on a device looks the array's address up (cudaGetSymbolAddress); make
- * that first call before any stream capture.  All calls share the array:
- * calls whose work overlaps on the GPU (other streams, other threads) race. */
+ * clamp to its edge cells; a non-finite coordinate gives key 0 -- this call
+ * does not check its input the way kifmm_build_tree does), perm[i] = index of
+ * that point in x, y.  The sort is stable.  x, y, keys, perm are device
+ * pointers on the current device; work is queued on `stream` (NULL: the
+ * legacy default stream) and the call returns before it finishes.  Scratch is
+ * one fixed device array of the library (about 12.3 MB), so n may not exceed
+ * KIFMM_NOALLOC_MAX_POINTS.  The first call on a device looks the array's
+ * address up (cudaGetSymbolAddress).  CUDA loads modules lazily by default, so
+ * that first call is also when the array is allocated on the device: make it
+ * before the host hands all device memory to its own pool and before any
+ * stream capture (or set CUDA_MODULE_LOADING=EAGER, which reserves the array
+ * on every device when the library loads).  From then on the device holds the
+ * array until the process exits; the cached address does not survive
+ * cudaDeviceReset.  All calls share the array: calls whose work overlaps on
+ * the GPU (other streams, other threads) race. */
 #define KIFMM_NOALLOC_MAX_POINTS 1048576
 int kifmm_morton_sort_noalloc(const double *x, const double *y, int64_t n, double root_min, double root_max,
                               uint64_t *keys, int32_t *perm, void *stream);

@@ -61,6 +61,8 @@ static double ork_k0(double x)
 
 typedef struct { int kind; double k; } OKern;
 
+static int isgn(double v) { return (v > 0) - (v < 0); }
+
 /* G(s -> t): Laplace -log(r^2)/(4 pi); modified Helmholtz K0(k r)/(2 pi).
  * The reference plug-ins: examples/laplace2.py:31-36, modified_helmholtz.py:38-43. */
 static inline double ork_eval(OKern kn, double sx, double sy, double tx, double ty)
@@ -416,6 +418,94 @@ void ork_tree_export(const OTree *t, int64_t *nodes, double *root)
     root[1] = t->rmax;
 }
 
+/* ------------------------------------------------------- interaction lists
+ * Node numbers below are export rows (ork_tree_export order). */
+static int64_t level_offset(const OTree *t, int l)
+{
+    int64_t o = 0;
+    for (int k = 0; k < l; k++) o += t->lv[k].n;
+    return o;
+}
+
+/* Level.colleagues (tree.py:349-375) by direction: coll[r][(dx+1)*3+(dy+1)]
+ * is the colleague at cell offset (dx, dy), -1 if none. */
+void ork_tree_colleagues(const OTree *t, int64_t *coll)
+{
+    for (int l = 0; l < t->L; l++) {
+        const OLevel *v = &t->lv[l];
+        int64_t off = level_offset(t, l);
+        for (int64_t i = 0; i < v->n; i++) {
+            int64_t *row = coll + 9 * (off + i);
+            for (int j = 0; j < 9; j++) row[j] = -1;
+            for (int j = 0; j < 9; j++) {
+                int64_t c = v->coll[9 * i + j];
+                if (c < 0) continue;
+                int64_t dx = llround((v->xmin[c] - v->xmin[i]) / v->width);
+                int64_t dy = llround((v->ymin[c] - v->ymin[i]) / v->width);
+                row[(dx + 1) * 3 + (dy + 1)] = off + c;
+            }
+        }
+    }
+}
+
+/* The (target, source) node pairs of downward pass 1's M2L as
+ * numba_add_interactions adds them (class_fmm.py:17-33, :323-343): for a node
+ * with doit = (!leaf || Xlist) && !fake and a colleague ci != i whose child
+ * group has a density (parent_density_ind[trunc(children[ci] / 4)] >= 0),
+ * child k of i receives child b of that group unless block (k, b) of the
+ * directional CM2LS is zeroed as near.  pairs may be NULL (count only). */
+int64_t ork_m2l_pairs(const OTree *t, int64_t *pairs)
+{
+    int64_t n = 0;
+    for (int l = 1; l < t->L - 1; l++) {
+        const OLevel *v = &t->lv[l], *d = &t->lv[l + 1];
+        int64_t off1 = level_offset(t, l + 1);
+        for (int64_t i = 0; i < v->n; i++) {
+            int doit = (!v->leaf[i] || v->xlist[i]) && !v->fake[i];
+            if (!doit) continue;
+            for (int j = 0; j < 9; j++) {
+                int64_t ci = v->coll[9 * i + j];
+                if (ci < 0 || ci == i) continue;
+                int xd = isgn(v->xmid[ci] - v->xmid[i]), yd = isgn(v->ymid[ci] - v->ymid[i]);
+                if (d->pdi[v->children[ci] / 4] < 0) continue;
+                for (int k = 0; k < 4; k++)
+                    for (int b = 0; b < 4; b++) {
+                        int ox = 2 * xd - (k >> 1) + (b >> 1), oy = 2 * yd - (k & 1) + (b & 1);
+                        if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1) continue;
+                        if (pairs) {
+                            pairs[2 * n] = off1 + 4 * (v->children[i] / 4) + k;
+                            pairs[2 * n + 1] = off1 + 4 * (v->children[ci] / 4) + b;
+                        }
+                        n++;
+                    }
+            }
+        }
+    }
+    return n;
+}
+
+/* The (leaf, source) node pairs of the near field at the sources
+ * (numba_target_neighbor_evaluation, class_fmm.py:90-111): every leaf that
+ * holds a point reads each colleague with points.  pairs may be NULL. */
+int64_t ork_p2p_pairs(const OTree *t, int64_t *pairs)
+{
+    int64_t n = 0;
+    for (int l = 0; l < t->L; l++) {
+        const OLevel *v = &t->lv[l];
+        int64_t off = level_offset(t, l);
+        for (int64_t i = 0; i < v->n; i++) {
+            if (!v->leaf[i] || v->top[i] <= v->bot[i]) continue;
+            for (int j = 0; j < 9; j++) {
+                int64_t c = v->coll[9 * i + j];
+                if (c < 0 || v->top[c] <= v->bot[c]) continue;
+                if (pairs) { pairs[2 * n] = off + i; pairs[2 * n + 1] = off + c; }
+                n++;
+            }
+        }
+    }
+    return n;
+}
+
 /* locate_points (tree.py:703-727): descend with strict '>' until a leaf. */
 static void locate1(const OTree *t, double x, double y, int *ind, int64_t *loc)
 {
@@ -584,8 +674,6 @@ int ork_fmm_create(OTree *t, int kind, double k, int Q, OFMM **out)
     *out = f;
     return 0;
 }
-
-static int isgn(double v) { return (v > 0) - (v < 0); }
 
 /* FMM.build_expansions (class_fmm.py:299-352), on freshly zeroed workspaces */
 int ork_fmm_apply(OFMM *f, const double *tau)

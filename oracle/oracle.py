@@ -43,6 +43,11 @@ def lib():
         L.ork_tree_num_nodes.restype = ctypes.c_int64
         L.ork_tree_export.argtypes = [_vp, _i64, _d]
         L.ork_locate.argtypes = [_vp, _d, _d, ctypes.c_int64, _i64]
+        L.ork_tree_colleagues.argtypes = [_vp, _i64]
+        L.ork_m2l_pairs.argtypes = [_vp, _i64]
+        L.ork_m2l_pairs.restype = ctypes.c_int64
+        L.ork_p2p_pairs.argtypes = [_vp, _i64]
+        L.ork_p2p_pairs.restype = ctypes.c_int64
         L.ork_tree_free.argtypes = [_vp]
         L.ork_fmm_create.argtypes = [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(_vp)]
         L.ork_fmm_create.restype = ctypes.c_int
@@ -98,6 +103,31 @@ class OracleTree:
         lib().ork_tree_export(self.h, _p(nodes, _i64), _p(root))
         order = np.lexsort((nodes[:, 2], nodes[:, 1], nodes[:, 0]))
         return nodes[order], root
+
+    def lists(self):
+        """Interaction lists as canonical rows of ``export()``'s node table:
+        colleagues [n_nodes, 9] by direction (dx+1)*3+(dy+1) (-1: none), and
+        the M2L (target, source) and P2P (leaf, source) pairs, each sorted
+        (tree.py:349-375; class_fmm.py:17-33, :90-111, :323-343)."""
+        n = lib().ork_tree_num_nodes(self.h)
+        nodes = np.zeros((n, 7), dtype=np.int64)
+        lib().ork_tree_export(self.h, _p(nodes, _i64), _p(np.zeros(2)))
+        order = np.lexsort((nodes[:, 2], nodes[:, 1], nodes[:, 0]))
+        rank = np.empty_like(order)
+        rank[order] = np.arange(n)
+        coll = np.zeros((n, 9), dtype=np.int64)
+        lib().ork_tree_colleagues(self.h, _p(coll, _i64))
+        coll = np.where(coll >= 0, rank[np.maximum(coll, 0)], -1)
+        out_coll = np.empty_like(coll)
+        out_coll[rank] = coll
+        res = [out_coll]
+        for f in (lib().ork_m2l_pairs, lib().ork_p2p_pairs):
+            m = f(self.h, ctypes.cast(None, _i64))
+            pr = np.zeros((m, 2), dtype=np.int64)
+            f(self.h, _p(pr, _i64))
+            pr = rank[pr]
+            res.append(pr[np.lexsort((pr[:, 1], pr[:, 0]))])
+        return tuple(res)
 
     def locate(self, x, y):
         x = _f64(x)

@@ -62,6 +62,7 @@ _SIGS = {
     "kifmm_graph_launch": (_i32, [_vp]),
     "kifmm_get_tree_info": (_i32, [_vp, ctypes.POINTER(TreeInfo)]),
     "kifmm_export_tree": (_i32, [_vp, _vp, _vp]),
+    "kifmm_export_lists": (_i32, [_vp, _vp, _vp, _vp, _vp, _vp]),
     "kifmm_plan_destroy": (_i32, [_vp]),
     "kifmm_last_error": (ctypes.c_char_p, []),
     "kifmm_direct_sum": (_i32, [ctypes.POINTER(KernelDesc), _vp, _vp, _vp, _i64, _vp, _i64, _vp, _i32, _i32]),

@@ -276,6 +276,31 @@ class FMM(object):
         order = np.lexsort((nodes[:, 2], nodes[:, 1], nodes[:, 0]))
         return nodes[order], pl
 
+    def export_lists(self):
+        """Interaction lists as canonical rows of ``export_tree()``'s node table
+        (sorted by (level, ix, iy)): colleagues [n_nodes, 9] by direction
+        (dx+1)*3+(dy+1) (-1: none), then the M2L (target, source) and P2P
+        (leaf, source) node pairs of the apply, each sorted."""
+        info = self.tree_info()
+        n = info.n_nodes
+        nodes = np.zeros((n, 7), dtype=np.int64)
+        B.check(self._lib.kifmm_export_tree(self._plan, nodes.ctypes.data, None))
+        order = np.lexsort((nodes[:, 2], nodes[:, 1], nodes[:, 0]))
+        rank = np.empty_like(order)
+        rank[order] = np.arange(n)
+        nm, npp = B.ctypes.c_int64(0), B.ctypes.c_int64(0)
+        B.check(self._lib.kifmm_export_lists(self._plan, None, None, ctypes_byref(nm), None, ctypes_byref(npp)))
+        coll = np.zeros((n, 9), dtype=np.int64)
+        m2l = np.zeros((nm.value, 2), dtype=np.int64)
+        p2p = np.zeros((npp.value, 2), dtype=np.int64)
+        B.check(self._lib.kifmm_export_lists(self._plan, coll.ctypes.data, m2l.ctypes.data, ctypes_byref(nm),
+                                             p2p.ctypes.data, ctypes_byref(npp)))
+        coll = np.where(coll >= 0, rank[np.maximum(coll, 0)], -1)
+        out = np.empty_like(coll)
+        out[rank] = coll
+        m2l, p2p = rank[m2l], rank[p2p]
+        return (out, m2l[np.lexsort((m2l[:, 1], m2l[:, 0]))], p2p[np.lexsort((p2p[:, 1], p2p[:, 0]))])
+
     def precompute(self):
         if not self._have_tree:
             self.build_tree()

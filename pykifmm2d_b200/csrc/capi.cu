@@ -411,6 +411,17 @@ int kifmm_export_tree(kifmm_plan *P, int64_t *nodes, int64_t *point_leaf) {
     });
 }
 
+int kifmm_export_lists(kifmm_plan *P, int64_t *colleagues, int64_t *m2l, int64_t *n_m2l, int64_t *p2p,
+                       int64_t *n_p2p) {
+    return guarded([&] {
+        KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
+        KIFMM_REQUIRE(!m2l || n_m2l, KIFMM_ERR_ARG, "export_lists: m2l needs its capacity in *n_m2l");
+        KIFMM_REQUIRE(!p2p || n_p2p, KIFMM_ERR_ARG, "export_lists: p2p needs its capacity in *n_p2p");
+        use_device(P);
+        export_lists(P, colleagues, m2l, n_m2l, p2p, n_p2p);
+    });
+}
+
 int kifmm_plan_destroy(kifmm_plan *P) {
     return guarded([&] {
         if (!P) return;

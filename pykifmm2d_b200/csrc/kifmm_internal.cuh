@@ -84,6 +84,9 @@ struct DBuf {
 // is the top 2l bits of the 2D-bit Morton key (child order (hx, hy) -> 2hx+hy,
 // the reference's (lo-x,lo-y), (lo-x,hi-y), (hi-x,lo-y), (hi-x,hi-y), tree.py:170-185).
 constexpr int KEY_DEPTH = 29;
+// Keys per tile of the plain LSD radix sort (radix_sort.cu: 256 threads x 16
+// keys); callers that size its histogram table themselves use it.
+constexpr int RADIX_TILE_KEYS = 4096;
 // Taylor order of the Laplace L2P fast path (|z|/r2 <= 0.585 inside 0.75 w)
 #define KIFMM_TAYLOR_P 48
 constexpr int MAX_LEVELS = KIFMM_MAX_LEVELS;  // levels 0..29
@@ -381,6 +384,20 @@ __host__ __device__ __forceinline__ uint64_t morton(uint64_t ix, uint64_t iy) {
     return (spread2(ix) << 1) | spread2(iy);
 }
 
+// Source of the M2L from direction d of parent p: the entry (split or X-list
+// cell) of the colleague in that direction, -1 when there is none, when it has
+// no children, or when its children hold no points (their check potentials
+// are zero; the reference skips such groups through parent_density_ind,
+// class_fmm.py:28-30).
+__host__ __device__ __forceinline__ int m2l_source_entry(const int32_t *__restrict__ ncoll, const int32_t *__restrict__ nent,
+                                                const int32_t *__restrict__ nbot, const int32_t *__restrict__ ntop,
+                                                int p, int d) {
+    const int nb = ncoll[9 * (size_t)p + d];
+    if (nb < 0) return -1;
+    const int je = nent[nb];
+    return (je >= 0 && ntop[nb] > nbot[nb]) ? je : -1;
+}
+
 // ------------------------------------------------------ host-side helpers
 inline unsigned grid_for(int64_t n, int block, int cap = 1 << 20) {
     int64_t g = (n + block - 1) / block;
@@ -392,6 +409,7 @@ inline unsigned grid_for(int64_t n, int block, int cap = 1 << 20) {
 // tree.cu
 void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int mem);
 void export_tree(kifmm_plan *P, int64_t *nodes, int64_t *point_leaf);
+void export_lists(kifmm_plan *P, int64_t *coll, int64_t *m2l, int64_t *n_m2l, int64_t *p2p, int64_t *n_p2p);
 void tree_stats(kifmm_plan *P);
 // operators.cu
 void build_operators(kifmm_plan *P);

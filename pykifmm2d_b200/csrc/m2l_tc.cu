@@ -320,11 +320,8 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_m2l_tc(TcArgs T) {
         for (int d = 0; d < 9; d++) {
             int grp = -1;
             if (act && d != 4) {
-                int nb = A.ncoll[9 * (size_t)p + d];
-                if (nb >= 0 && A.nent[nb] >= 0) {
-                    grp = A.nent[nb];
-                    if (F == TC_INT8) kcol = max(kcol, T.pre.gexp[grp]);
-                }
+                grp = m2l_source_entry(A.ncoll, A.nent, A.nbot, A.ntop, p, d);
+                if (F == TC_INT8 && grp >= 0) kcol = max(kcol, T.pre.gexp[grp]);
             }
             sgrp[tid * 9 + d] = grp;
         }

@@ -21,18 +21,23 @@ void radix_sort_pairs_scratch(uint64_t *key, int32_t *val, uint64_t *key_tmp, in
                               int64_t n, int bits, cudaStream_t stream);
 
 // Scratch layout: key ping-pong [NMAX] u64 | index ping-pong [NMAX] i32 |
-// digit histograms [256 * NMAX/4096 + 256] u32 | one u64 counter.  About 12.3 MB.
+// digit histograms, 256 words per radix tile plus 256 (radix_sort_hist_words).
+// About 12.3 MB.
 constexpr int64_t NA_MAX = KIFMM_NOALLOC_MAX_POINTS;
+constexpr int64_t NA_HIST_WORDS = (int64_t)256 * ((NA_MAX + RADIX_TILE_KEYS - 1) / RADIX_TILE_KEYS) + 256;
 constexpr size_t NA_KEY_OFF = 0;
 constexpr size_t NA_IDX_OFF = NA_KEY_OFF + (size_t)NA_MAX * 8;
 constexpr size_t NA_HIST_OFF = NA_IDX_OFF + (size_t)NA_MAX * 4;
-constexpr size_t NA_CNT_OFF = NA_HIST_OFF + ((size_t)256 * (NA_MAX / 4096) + 256) * 4;
-constexpr size_t NA_BYTES = NA_CNT_OFF + 256;
+constexpr size_t NA_BYTES = NA_HIST_OFF + (size_t)NA_HIST_WORDS * 4;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
 
 // Device address of the scratch array, looked up once per device (with that
-// device current) and cached.
+// device current) and cached for the life of the process.  CUDA loads this
+// file's module lazily by default, so the lookup is also what makes the array
+// resident on the device: the first call on a device allocates its ~12.3 MB
+// (CUDA_MODULE_LOADING=EAGER reserves it when the library loads instead).
+// The cached address does not survive cudaDeviceReset.
 static std::mutex g_na_mutex;
 static void *g_na_ptr[64] = {};
 static int g_na_sms[64] = {};
@@ -81,10 +86,11 @@ extern "C" int kifmm_morton_sort_noalloc(const double *x, const double *y, int64
         uint64_t *ktmp = (uint64_t *)(base + NA_KEY_OFF);
         int32_t *itmp = (int32_t *)(base + NA_IDX_OFF);
         uint32_t *hist = (uint32_t *)(base + NA_HIST_OFF);
-        unsigned long long *cnt = (unsigned long long *)(base + NA_CNT_OFF);
-        // the counter keeps the previous call's value: clear it
-        KIFMM_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s));
-        launch_morton_keys(x, y, n, root_min, root_max, keys, perm, cnt, sms, s);
+        KIFMM_REQUIRE(radix_sort_hist_words(n) <= NA_HIST_WORDS, KIFMM_ERR_CUDA,
+                      "morton_sort_noalloc: histogram table smaller than the sort needs");
+        // every scratch word the sort reads is written by the same call first
+        // (histograms are zeroed per pass), so nothing is cleared here
+        launch_morton_keys(x, y, n, root_min, root_max, keys, perm, nullptr, sms, s);
         radix_sort_pairs_scratch(keys, perm, ktmp, itmp, hist, n, 2 * KEY_DEPTH, s);
         return KIFMM_OK;
     } catch (const Fail &e) {

@@ -310,6 +310,9 @@ void build_operators(kifmm_plan *P) {
     }
     // circles + inverse, then kernel matrices composed with the inverses, then
     // the directional M2L blocks (with the row maxima the tensor-core slices use)
+    // k_ops_inverse's elimination maps the augmented [E2C | I] row (2Q columns)
+    // onto 128 columns per row phase
+    KIFMM_REQUIRE(2 * Q <= 128, KIFMM_ERR_ARG, "operator inverse: Nequiv above 64");
     size_t smem = (size_t)2 * Q * (2 * Q + 1) * sizeof(double);
     ensure_dyn_smem(k_ops_inverse, smem);
     k_ops_inverse<<<L, INV_THREADS, smem, s>>>(A);

@@ -162,11 +162,8 @@ __global__ void k_m2l_d(PassArgs A, int l) {
             int p = spar[r];
             int64_t grp = -1;
             if (p >= 0) {
-                int nb = A.ncoll[9 * (size_t)p + d];
-                if (nb >= 0) {
-                    int je = A.nent[nb];
-                    if (je >= 0) grp = A.T.off[l + 1] + 4 * (je - A.T.eoff[l]);
-                }
+                const int je = m2l_source_entry(A.ncoll, A.nent, A.nbot, A.ntop, p, d);
+                if (je >= 0) grp = A.T.off[l + 1] + 4 * (je - A.T.eoff[l]);
             }
             sgrp[r] = grp;
         }

@@ -21,6 +21,7 @@ namespace kifmm {
 constexpr int RS_THREADS = 256;
 constexpr int RS_ITEMS = 16;
 constexpr int RS_TILE = RS_THREADS * RS_ITEMS;
+static_assert(RS_TILE == RADIX_TILE_KEYS, "histogram tables sized outside this file assume RADIX_TILE_KEYS per tile");
 constexpr int RS_WARPS = RS_THREADS / 32;
 
 __global__ void __launch_bounds__(RS_THREADS) k_rs_hist(const uint64_t *__restrict__ key, int64_t n, int shift,

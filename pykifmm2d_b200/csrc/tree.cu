@@ -112,11 +112,12 @@ __global__ void k_keys(const double *__restrict__ x, const double *__restrict__ 
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         double a = x[i], b = y[i];
         uint64_t k = 0;
-        if (h > 0) k = morton(grid_cell(a, m, h), grid_cell(b, m, h));
+        if (h > 0 && isfinite(a) && isfinite(b)) k = morton(grid_cell(a, m, h), grid_cell(b, m, h));
         key[i] = k;
         perm[i] = (int32_t)i;
         out += (a < m || a > M || b < m || b > M);
     }
+    if (!outside) return;
     for (int o = 16; o; o >>= 1) out += __shfl_xor_sync(0xffffffffu, out, o);
     if ((threadIdx.x & 31) == 0 && out) atomicAdd(outside, out);
 }
@@ -783,7 +784,9 @@ __global__ void __launch_bounds__(ES_THREADS) k_ent_sort(const uint64_t *__restr
 }
 
 // Work counts: cnt[0] P2P pairs, cnt[1] P2M points, cnt[2] V-list pairs,
-// cnt[3] (target group, direction) M2L blocks.
+// cnt[3] (target group, direction) M2L blocks.  The V-list pairs are those of
+// kifmm_export_lists: targets the children of split cells, sources the
+// children of a colleague's non-empty child group, well separated.
 __global__ void k_stats(LevelTable T, const uint64_t *__restrict__ ent, const int32_t *__restrict__ ent_node,
                         const int32_t *__restrict__ leaf_list, int64_t nleaf, const int32_t *__restrict__ p2m_list,
                         int64_t np2m, const int32_t *__restrict__ nbot, const int32_t *__restrict__ ntop,
@@ -808,8 +811,7 @@ __global__ void k_stats(LevelTable T, const uint64_t *__restrict__ ent, const in
         int p = ent_node[j];
         for (int dd = 0; dd < 9; dd++) {
             if (dd == 4) continue;
-            int nb = ncoll[9 * (int64_t)p + dd];
-            if (nb < 0 || nent[nb] < 0) continue;
+            if (m2l_source_entry(ncoll, nent, nbot, ntop, p, dd) < 0) continue;
             d++;
             int dx = dd / 3 - 1, dy = dd % 3 - 1;
             for (int ta = 0; ta < 4; ta++)
@@ -1118,6 +1120,73 @@ void export_tree(kifmm_plan *P, int64_t *nodes, int64_t *point_leaf) {
                 q[0] = lev[g]; q[1] = ix; q[2] = iy;
             }
     }
+}
+
+// Interaction lists as the apply kernels walk them (kifmm_export_lists):
+// colleagues from the node table; M2L pairs from the split entries of levels
+// 1..L-2 and m2l_source_entry (the test k_m2l_d, k_m2l_f and k_m2l_tc make);
+// P2P pairs from the leaf list and its colleagues with points (the leaf
+// kernels).  Node numbers are kifmm_export_tree's rows.
+void export_lists(kifmm_plan *P, int64_t *coll, int64_t *m2l, int64_t *n_m2l, int64_t *p2p, int64_t *n_p2p) {
+    KIFMM_REQUIRE(P->have_tree, KIFMM_ERR_STATE, "export_lists: no tree");
+    const int64_t NN = P->n_nodes, NE = P->n_ent, NL = P->n_leaf_list;
+    std::vector<int32_t> cl(9 * NN), bot(NN), top(NN), nent(NN), en(NE), leaves(NL);
+    std::vector<uint64_t> ent(NE);
+    cudaStream_t s = P->stream;
+    KIFMM_CUDA(cudaMemcpyAsync(cl.data(), P->ncoll.p, 9 * NN * 4, cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaMemcpyAsync(bot.data(), P->nbot.p, NN * 4, cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaMemcpyAsync(top.data(), P->ntop.p, NN * 4, cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaMemcpyAsync(nent.data(), P->nent.p, NN * 4, cudaMemcpyDeviceToHost, s));
+    if (NE) {
+        KIFMM_CUDA(cudaMemcpyAsync(ent.data(), P->ent.p, NE * 8, cudaMemcpyDeviceToHost, s));
+        KIFMM_CUDA(cudaMemcpyAsync(en.data(), P->ent_node.p, NE * 4, cudaMemcpyDeviceToHost, s));
+    }
+    if (NL) KIFMM_CUDA(cudaMemcpyAsync(leaves.data(), P->leaf_list.p, NL * 4, cudaMemcpyDeviceToHost, s));
+    KIFMM_CUDA(cudaStreamSynchronize(s));
+    if (coll)
+        for (int64_t i = 0; i < 9 * NN; i++) coll[i] = cl[i];
+    int64_t nm = 0, cap_m = (m2l && n_m2l) ? *n_m2l : 0;
+    for (int64_t j = 0; j < NE; j++) {
+        if (ent[j] & 1) continue;  // X-list cell: its fake children receive no M2L
+        const int l = (int)(ent[j] >> ENT_LEVEL_SHIFT);
+        if (l < 1 || l > P->L - 2) continue;
+        const int p = en[j];
+        const int64_t t0 = P->lt.off[l + 1] + 4 * (j - P->lt.eoff[l]);
+        for (int dd = 0; dd < 9; dd++) {
+            if (dd == 4) continue;
+            const int je = m2l_source_entry(cl.data(), nent.data(), bot.data(), top.data(), p, dd);
+            if (je < 0) continue;
+            const int64_t s0 = P->lt.off[l + 1] + 4 * (je - P->lt.eoff[l]);
+            const int dx = dd / 3 - 1, dy = dd % 3 - 1;
+            for (int ta = 0; ta < 4; ta++)
+                for (int sb = 0; sb < 4; sb++) {
+                    const int ox = 2 * dx - (ta >> 1) + (sb >> 1), oy = 2 * dy - (ta & 1) + (sb & 1);
+                    if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1) continue;
+                    if (m2l) {
+                        KIFMM_REQUIRE(nm < cap_m, KIFMM_ERR_ARG, "export_lists: m2l buffer smaller than *n_m2l pairs");
+                        m2l[2 * nm] = t0 + ta;
+                        m2l[2 * nm + 1] = s0 + sb;
+                    }
+                    nm++;
+                }
+        }
+    }
+    int64_t np = 0, cap_p = (p2p && n_p2p) ? *n_p2p : 0;
+    for (int64_t i = 0; i < NL; i++) {
+        const int g = leaves[i];
+        for (int dd = 0; dd < 9; dd++) {
+            const int c = cl[9 * (int64_t)g + dd];
+            if (c < 0 || top[c] <= bot[c]) continue;
+            if (p2p) {
+                KIFMM_REQUIRE(np < cap_p, KIFMM_ERR_ARG, "export_lists: p2p buffer smaller than *n_p2p pairs");
+                p2p[2 * np] = g;
+                p2p[2 * np + 1] = c;
+            }
+            np++;
+        }
+    }
+    if (n_m2l) *n_m2l = nm;
+    if (n_p2p) *n_p2p = np;
 }
 
 }  // namespace kifmm

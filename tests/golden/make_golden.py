@@ -20,8 +20,10 @@ script copies the package into a temporary folder and replaces ``i8[4]`` by
 every density because a second ``build_expansions`` on one object accumulates
 into stale check potentials (tree.py:414 with class_fmm.py:71).
 
-Run from the repository root:  python tests/golden/make_golden.py
-It needs the reference checkout at /root/reference (read only) and numba.
+Run from the repository root:
+    python tests/golden/make_golden.py [path/to/pykifmm2d]
+The reference package folder comes from the argument, else from the
+environment variable KIFMM_REFERENCE_PKG; it is only read.  Needs numba.
 """
 import os
 import shutil
@@ -32,13 +34,20 @@ import time
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = "/root/reference/pykifmm2d"
+
+
+def reference_package():
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("KIFMM_REFERENCE_PKG")
+    if not ref or not os.path.isfile(os.path.join(ref, "class_fmm.py")):
+        sys.exit("usage: make_golden.py <reference pykifmm2d package folder> "
+                 "(or set KIFMM_REFERENCE_PKG)")
+    return ref
 
 
 def shimmed_reference():
     tmp = tempfile.mkdtemp(prefix="kifmm_ref_")
     dst = os.path.join(tmp, "pykifmm2d")
-    shutil.copytree(REF, dst, ignore=shutil.ignore_patterns("*.pyc", "__pycache__"))
+    shutil.copytree(reference_package(), dst, ignore=shutil.ignore_patterns("*.pyc", "__pycache__"))
     tp = os.path.join(dst, "tree.py")
     src = open(tp).read()
     assert src.count("i8[4]") >= 4
@@ -101,6 +110,68 @@ CASES = [
 ]
 
 
+def reference_lists(tree, rank, offs):
+    """The reference's interaction lists, read from its own Level arrays and
+    walked the way its passes walk them, as canonical row indices
+    (rank[offs[l] + i] is the canonical row of node i of level l):
+
+    * colleagues[r, (dx+1)*3 + (dy+1)]: the node of Level.colleagues
+      (tree.py:349-375) at cell offset (dx, dy), -1 if none;
+    * m2l[k] = (target, source): every block numba_add_interactions adds in
+      downward pass 1 (class_fmm.py:323-343): for a node i with
+      doit = (not_leaf | Xlist) & ~fake_leaf and a colleague ci != i whose child
+      group has a density (parent_density_ind[trunc(children_ind[ci] / 4)] >= 0),
+      child k of i receives child b of that group unless the CM2LS block for
+      (k, b) is zeroed as near (class_fmm.py:266-291);
+    * p2p[k] = (leaf, source): numba_target_neighbor_evaluation
+      (class_fmm.py:90-111) at the sources: each leaf that holds a point reads
+      every colleague with ns > 0.
+    """
+    root = float(tree.xmin)
+    coll_rows, m2l, p2p = [], [], []
+    for l, L in enumerate(tree.Levels):
+        w = L.width
+        ix = np.rint((L.xmin - root) / w).astype(np.int64)
+        iy = np.rint((L.ymin - root) / w).astype(np.int64)
+        C = -np.ones((L.n_node, 9), dtype=np.int64)
+        for i in range(L.n_node):
+            for c in L.colleagues[i]:
+                if c >= 0:
+                    C[i, (ix[c] - ix[i] + 1) * 3 + (iy[c] - iy[i] + 1)] = rank[offs[l] + c]
+        coll_rows.append(C)
+        ns = L.top_ind - L.bot_ind
+        for i in np.nonzero(L.leaf & (ns > 0))[0]:
+            for c in L.colleagues[i]:
+                if c >= 0 and ns[c] > 0:
+                    p2p.append((rank[offs[l] + i], rank[offs[l] + c]))
+        if l < 1 or l > tree.levels - 2:
+            continue
+        D = tree.Levels[l + 1]
+        doit = (~L.leaf | L.Xlist) & ~L.fake_leaf
+        ci4 = (L.children_ind / 4).astype(int)
+        for i in np.nonzero(doit)[0]:
+            for ci in L.colleagues[i]:
+                if ci < 0 or ci == i:
+                    continue
+                xd = int(np.sign(L.xmid[ci] - L.xmid[i]))
+                yd = int(np.sign(L.ymid[ci] - L.ymid[i]))
+                if D.parent_density_ind[ci4[ci]] < 0:
+                    continue
+                for k in range(4):
+                    for b in range(4):
+                        ox = 2 * xd - (k >> 1) + (b >> 1)
+                        oy = 2 * yd - (k & 1) + (b & 1)
+                        if abs(ox) <= 1 and abs(oy) <= 1:
+                            continue
+                        m2l.append((rank[offs[l + 1] + 4 * ci4[i] + k], rank[offs[l + 1] + 4 * ci4[ci] + b]))
+    coll = np.concatenate(coll_rows, axis=0)
+    out_coll = np.empty_like(coll)
+    out_coll[rank] = coll
+    m2l = np.array(sorted(m2l), dtype=np.int64).reshape(-1, 2)
+    p2p = np.array(sorted(p2p), dtype=np.int64).reshape(-1, 2)
+    return out_coll, m2l, p2p
+
+
 def canonical_tree(tree, x, y):
     root = float(tree.xmin)
     rows = []
@@ -130,7 +201,11 @@ def canonical_tree(tree, x, y):
         pl[m, 1] = np.rint((L.xmin[locs[m]] - root) / w).astype(np.int64)
         pl[m, 2] = np.rint((L.ymin[locs[m]] - root) / w).astype(np.int64)
     order = np.lexsort((nodes[:, 2], nodes[:, 1], nodes[:, 0]))
-    return nodes[order], pl
+    rank = np.empty_like(order)
+    rank[order] = np.arange(order.size)
+    offs = np.concatenate([[0], np.cumsum([L.n_node for L in tree.Levels])])
+    lists = reference_lists(tree, rank, offs)
+    return nodes[order], pl, lists
 
 
 def main():
@@ -159,8 +234,9 @@ def main():
         f.build_expansions(tau)
         pot = f.evaluate_to_points(x, y, True)
         dt = time.time() - t0
-        nodes, pl = canonical_tree(f.tree, x, y)
+        nodes, pl, (coll, m2l, p2p) = canonical_tree(f.tree, x, y)
         out = dict(x=x, y=y, tau=tau, pot=pot, nodes=nodes, point_leaf=pl,
+                   colleagues=coll, m2l_pairs=m2l, p2p_pairs=p2p,
                    kernel=np.array(0 if kern == "laplace" else 1), k=np.array(kk),
                    nequiv=np.array(neq), ncutoff=np.array(cut),
                    root=np.array([f.tree.xmin, f.tree.xmax], dtype=np.float64),
@@ -180,6 +256,7 @@ def main():
         out["direct"] = ref
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
         print(f"{name}: N={n} levels={f.tree.levels} nodes={nodes.shape[0]} "
+              f"m2l_pairs={m2l.shape[0]} p2p_pairs={p2p.shape[0]} "
               f"leaves={int(nodes[:,3].sum())} fake={int(nodes[:,4].sum())} "
               f"xlist={int(nodes[:,5].sum())} ref_time={dt:.2f}s relerr_vs_direct={err:.2e}",
               flush=True)

@@ -55,3 +55,16 @@ def test_repeated_apply_is_fresh(golden_cases):
     f.build_expansions(g["tau"])
     pot = f.evaluate_to_points(g["x"], g["y"], True)
     assert np.abs(pot - g["pot"]).max() / np.abs(g["pot"]).max() < 1e-10
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_lists_match_reference(golden_cases, name):
+    """Colleagues by direction, M2L (target, source) pairs and P2P (leaf,
+    source) pairs read from the reference's own Level arrays
+    (make_golden.reference_lists) equal the oracle's, exactly."""
+    g = golden_cases[name]
+    t = O.OracleTree(g["x"], g["y"], int(g["ncutoff"]))
+    coll, m2l, p2p = t.lists()
+    np.testing.assert_array_equal(coll, g["colleagues"])
+    np.testing.assert_array_equal(m2l, g["m2l_pairs"])
+    np.testing.assert_array_equal(p2p, g["p2p_pairs"])

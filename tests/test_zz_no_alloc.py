@@ -77,3 +77,58 @@ def test_noalloc_sort_rejects_too_many_points():
                                        buf.data_ptr(), None)
     assert rc == B.ERR_ARG
     assert "KIFMM_NOALLOC_MAX_POINTS" in lib.kifmm_last_error().decode()
+
+
+def _host_keys(x, y, m, M):
+    """Exact Morton keys on the host: the cell index is the number of grid
+    lines m + j h (h = (M - m) / 2^29) that the coordinate is strictly above,
+    clamped to the grid (the tree's strict '>' midline rule)."""
+    h = np.ldexp(M - m, -29)
+    top = (1 << 29) - 1
+
+    def cell(v):
+        j = np.clip(np.ceil((v - m) / h) - 1.0, 0, top).astype(np.int64)
+        for _ in range(4):
+            up = (j < top) & (v > m + (j + 1).astype(np.float64) * h)
+            j = j + up
+            dn = (j > 0) & ~(v > m + j.astype(np.float64) * h)
+            j = j - dn
+        return j
+
+    return morton_np(cell(x), cell(y))
+
+
+def test_noalloc_sort_at_capacity_allocates_nothing():
+    """n = KIFMM_NOALLOC_MAX_POINTS exactly (the scratch offsets and the
+    histogram table full): keys equal the host's exact keys in sorted order,
+    perm is a stable permutation, and after a first call the device's free
+    memory is the same before and after a second call."""
+    import torch
+
+    from pykifmm2d_b200 import _lib as B
+    lib = B.load()
+    n = B.NOALLOC_MAX_POINTS
+    rng = np.random.default_rng(11)
+    x, y = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    want = _host_keys(x, y, -1.0, 1.0)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.from_numpy(y).cuda()
+    keys = torch.empty(n, dtype=torch.int64, device="cuda")
+    perm = torch.empty(n, dtype=torch.int32, device="cuda")
+    free = []
+    for call in range(2):
+        torch.cuda.synchronize()
+        free.append(torch.cuda.mem_get_info()[0])
+        rc = lib.kifmm_morton_sort_noalloc(xd.data_ptr(), yd.data_ptr(), n, -1.0, 1.0, keys.data_ptr(),
+                                           perm.data_ptr(), None)
+        torch.cuda.synchronize()
+        B.check(rc)
+        k = keys.cpu().numpy().view(np.uint64)
+        p = perm.cpu().numpy().astype(np.int64)
+        assert np.array_equal(np.sort(p), np.arange(n)), f"call {call}: perm is not a permutation"
+        assert np.array_equal(k, want[p]), f"call {call}: keys differ from the exact host keys"
+        assert np.all(k[1:] >= k[:-1]), f"call {call}: keys not sorted"
+        eq = k[1:] == k[:-1]
+        assert np.all(p[1:][eq] > p[:-1][eq]), f"call {call}: sort not stable"
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free[1], "the second call changed the device's free memory"
