@@ -81,11 +81,11 @@ def kernel_obj(cfg):
     return P.LaplaceKernel() if cfg["kernel"] == 0 else P.ModifiedHelmholtzKernel(cfg["k"])
 
 
-def make_fmm(cfg, x, y, precision, stream=None):
+def make_fmm(cfg, x, y, precision, stream=None, m2l="auto"):
     import pykifmm2d_b200 as P
     kern = kernel_obj(cfg)
     return P.FMM(x, y, P.Get_Kernel_Functions(kern), P.prepare_numba_functions_on_the_fly(kern), cfg["neq"],
-                 cfg["cut"], precision=precision, stream=stream)
+                 cfg["cut"], precision=precision, stream=stream, m2l=m2l)
 
 
 def sample_targets(n):
@@ -151,11 +151,11 @@ def flush_l2(torch, buf):
     buf.zero_()
 
 
-def time_full_steps(torch, cfg, xd, yd, td, precision, steps, warmup, flush, profile=False):
+def time_full_steps(torch, cfg, xd, yd, td, precision, steps, warmup, flush, profile=False, m2l="auto"):
     """Full pipeline on device-resident inputs; returns per-step ms (CUDA events)."""
     from pykifmm2d_b200 import _lib as B
     stream = torch.cuda.Stream()  # the plan's own created stream (not the legacy default stream)
-    f = make_fmm(cfg, xd, yd, precision, stream=stream.cuda_stream)
+    f = make_fmm(cfg, xd, yd, precision, stream=stream.cuda_stream, m2l=m2l)
     f._bench_stream = stream
     out = torch.empty_like(xd)
     lib = B.load()
@@ -301,14 +301,58 @@ def build_rooflines(cfg, info, phase, precision, pk, pk_src, n):
                       "peak_source": f"dense int8 = 2 x measured bf16 {pk['bf16_tflops']} TFLOP/s ({pk_src})"}
     ts = ph["sort"] * 1e-3
     if ts > 0:
-        byts = 4 * 36.0 * n  # four 8-bit passes: histogram read + scatter read + write of 12 B per key
+        byts = 52.0 * n  # algorithmic: read x, y, tau (24 B), write sorted x, y, tau and an i32 index (28 B)
         ach = byts / ts / 1e9
-        out["sort"] = {"kernel": "onesweep radix sort (k_os_hist + 4 k_os_pass)", "bound": "hbm",
-                       "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s", "frac": ach / pk["hbm_gbs"],
-                       "traffic": traffic.get("k_os_pass"),
-                       "work": "4 passes x 36 B per key (12 B key+index read twice, written once)",
+        out["sort"] = {"kernel": "Morton keys + onesweep radix sort (k_keys_dev, k_os_hist, k_os_pass)",
+                       "bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                       "frac": ach / pk["hbm_gbs"], "traffic": traffic.get("k_os_pass"),
+                       "work": "52 B per point: the algorithmic minimum of sorting the points (read x, y, tau; "
+                               "write them sorted with an int32 index)",
+                       "executed_bytes": 4 * 36.0 * n,
                        "peak_source": pk_src}
+    out["composite"] = composite_roofline(cfg, info, ph, precision, pk, pk_src, n)
     return out
+
+
+def composite_roofline(cfg, info, ph, precision, pk, pk_src, n):
+    """t_ideal / t_measured over the phases of one step: each phase's
+    algorithmic work at the peak of the unit that bounds it.
+      P2P    pairs at the lg2 rate (16/clk/SM) for Laplace, 40 flops per pair
+             at the FP32 peak for K0 (FP64 peak in the plain form);
+      P2M    Q kernel evaluations per source point, L2P Q per point, 8 flops
+             each at the FP32 peak (FP64 peak in the plain form);
+      M2L    2 Q^2 per V-list pair at dense int8 (2 x measured bf16) in the
+             mixed form, at the FP64 tensor rate (128 flops/clk/SM) in the plain one;
+      M2M, L2L  2 Q (4Q) per split cell each way at the FP64 tensor rate;
+      sort   52 B per point at the measured HBM bandwidth.
+    t_measured is the sum of the same phases' event times."""
+    clk = pk.get("sm_max_mhz", 1965.0) * 1e6
+    fp32 = 148 * 128 * 2 * clk
+    fp64 = fp32 / 2
+    dmma = 148 * 128 * clk
+    lg2 = 148 * 16 * clk
+    Q = cfg["neq"]
+    mixed = precision == "mixed"
+    pairs = float(info.n_p2p_pairs)
+    if cfg["kernel"] == 0 and mixed:
+        t_p2p = pairs / lg2
+    else:
+        t_p2p = pairs * p2p_flops_per_pair(cfg["kernel"]) / (fp32 if mixed else fp64)
+    evals = Q * float(info.n_p2m_points) + Q * float(n)
+    t_p2m_l2p = evals * 8.0 / (fp32 if mixed else fp64)
+    m2l_fl = 2.0 * Q * Q * float(info.n_m2l_pairs)
+    t_m2l = m2l_fl / (2 * pk["bf16_tflops"] * 1e12) if mixed else m2l_fl / dmma
+    n_split = max(0.0, (float(info.n_nodes) - 1) / 4)
+    t_lvl = 2 * (2.0 * Q * 4 * Q * n_split) / dmma
+    t_sort = 52.0 * n / (pk["hbm_gbs"] * 1e9)
+    t_ideal = t_p2p + t_p2m_l2p + t_m2l + t_lvl + t_sort
+    keys = ["tree", "p2m", "m2m", "m2l", "l2l", "leaf"]
+    t_meas = sum(ph[k] for k in keys) * 1e-3
+    return {"t_ideal_ms": t_ideal * 1e3, "t_measured_ms": t_meas * 1e3,
+            "frac": t_ideal / t_meas if t_meas > 0 else None,
+            "ideal_ms": {"p2p": t_p2p * 1e3, "p2m_l2p": t_p2m_l2p * 1e3, "m2l": t_m2l * 1e3,
+                         "m2m_l2l": t_lvl * 1e3, "sort": t_sort * 1e3},
+            "measured_phases": keys, "peak_source": pk_src}
 
 
 def run_ours(args, cfg, rank, world, dist):
@@ -366,11 +410,22 @@ def run_ours(args, cfg, rank, world, dist):
             res["plain_err"] = rel_err(outp.cpu().numpy(), ref, idx)
             res["plain_apply_ms"] = statistics.mean(time_apply_steps(torch, fp, xd, yd, td, 3, 1, flush))
             del fp
+            _, _, res["plain_phase"], _, _ = time_full_steps(torch, cfg, xd, yd, td, "fp64", 2, 1, flush,
+                                                             profile=True)
+            pe_t, pe_pot = time_e2e(torch, cfg, x, y, tau, "fp64", 3, 1)
+            res["plain_e2e_ms"] = statistics.mean(pe_t)
+            res["plain_e2e_err"] = rel_err(pe_pot, ref, idx)
         else:
             res["plain_ms"], res["plain_err"], res["plain_apply_ms"] = ms_step, res["err"], res["apply_ms"]
+            res["plain_phase"] = phase
         e2e_t, e2e_pot = time_e2e(torch, cfg, x, y, tau, precision, max(3, args.steps // 2), 2)
         res["e2e_ms"] = statistics.mean(e2e_t)
         res["e2e_err"] = rel_err(e2e_pot, ref, idx)
+        if precision == "fp64":
+            res["plain_e2e_ms"], res["plain_e2e_err"] = res["e2e_ms"], res["e2e_err"]
+        if args.extra_configs:
+            res["c3_forms"] = run_c3_forms(torch, flush)
+            res["c4"] = run_c4(torch, flush)
     if rank != 0:
         return None
     pk, pk_src = peaks()
@@ -396,7 +451,13 @@ def run_ours(args, cfg, rank, world, dist):
         "latency_ms": {"p50": float(np.percentile(times, 50)), "p99": float(np.percentile(times, 99))},
         "rel_err": res["err"],
         "plain_fp64": {"ms_per_step": res["plain_ms"], "mpts_s": n / (res["plain_ms"] * 1e-3) / 1e6,
-                       "rel_err": res["plain_err"], "apply_ms": res["plain_apply_ms"]},
+                       "rel_err": res["plain_err"], "apply_ms": res["plain_apply_ms"],
+                       "phases_ms": {nm: float(v) for nm, v in zip(names, res["plain_phase"])},
+                       "e2e": {"value": n / (res["plain_e2e_ms"] * 1e-3) / 1e6, "unit": "Mpts/s",
+                               "ms_per_step": res["plain_e2e_ms"], "rel_err": res["plain_e2e_err"],
+                               "h2d_bytes_per_step": 3 * 8 * n, "d2h_bytes_per_step": 8 * n},
+                       "mixed_over_plain": {"step": res["plain_ms"] / ms_step,
+                                            "e2e": res["plain_e2e_ms"] / res["e2e_ms"]}},
         "apply_only": {"ms": res["apply_ms"], "mpts_s": n / (res["apply_ms"] * 1e-3) / 1e6},
         "phases_ms": {nm: float(v) for nm, v in zip(names, phase)},
         "tree": {"levels": info.levels, "nodes": info.n_nodes, "leaves": info.n_leaves, "outside_root": info.n_outside,
@@ -404,17 +465,96 @@ def run_ours(args, cfg, rank, world, dist):
         "roofline": rooflines["dominant"],
         "roofline_tensor_m2l": rooflines.get("m2l"),
         "roofline_hbm_sort": rooflines.get("sort"),
+        "roofline_composite": rooflines.get("composite"),
         "e2e": {"value": n / (res["e2e_ms"] * 1e-3) / 1e6, "unit": "Mpts/s",
                 "h2d_bytes_per_step": 3 * 8 * n, "d2h_bytes_per_step": 8 * n, "ms_per_step": res["e2e_ms"],
                 "rel_err": res["e2e_err"]},
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
+    for k in ("c3_forms", "c4"):
+        if k in res:
+            line[k] = res[k]
     if args.serve_requests > 0:
         line["serving"] = run_serving(args, dev)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, x, y, tau, repeats=3)
     return line
+
+
+# ------------------------------------------- extra configurations (same run)
+def _direct_ref(cfg, x, y, tau, idx):
+    import pykifmm2d_b200 as P
+    KF, KA, KAS = P.Get_Kernel_Functions(kernel_obj(cfg))
+    ref = np.zeros(idx.size)
+    KAS(x, y, tau, ref, targets=idx)
+    return ref
+
+
+def _form_line(torch, cfg, xd, yd, td, flush, precision, m2l, ref, idx, steps=3, warmup=2):
+    times, launches, _, f, out = time_full_steps(torch, cfg, xd, yd, td, precision, steps, warmup, flush, m2l=m2l)
+    _, _, phase, _, _ = time_full_steps(torch, cfg, xd, yd, td, precision, 2, 1, flush, profile=True, m2l=m2l)
+    from pykifmm2d_b200 import _lib as B
+    ms = statistics.mean(times)
+    err = rel_err(out.cpu().numpy(), ref, idx)
+    return {"precision": precision, "m2l": m2l, "ms_per_step": ms, "mpts_s": xd.numel() / (ms * 1e-3) / 1e6,
+            "rel_err": err, "meets_1e-7": err <= 1e-7, "meets_1e-5": err <= 1e-5,
+            "phases_ms": {nm: float(v) for nm, v in zip(B.PHASES, phase)}}, f
+
+
+def run_c3_forms(torch, flush):
+    """Precision forms on the 4M uniform cloud (Nequiv 32): each M2L form of
+    the mixed precision (FP32 near field) and the plain FP64 form, with the
+    max relative error at 4,096 seeded targets against the FP64 direct sum."""
+    cfg = CONFIGS["c3"]
+    x, y, tau = cfg["gen"](cfg["n"], 0)
+    idx = sample_targets(x.size)
+    ref = _direct_ref(cfg, x, y, tau, idx)
+    xd, yd, td = (torch.from_numpy(v).cuda() for v in (x, y, tau))
+    forms = {}
+    for name, precision, m2l in (("int8", "mixed", "int8"), ("bf16x3", "mixed", "bf16x3"),
+                                 ("fp16x3", "mixed", "fp16x3"), ("fp32", "mixed", "fp32"),
+                                 ("fp64_plain", "fp64", "auto")):
+        forms[name], f = _form_line(torch, cfg, xd, yd, td, flush, precision, m2l, ref, idx)
+        del f
+    return {"workload": cfg["desc"], "n_points": x.size, "targets": int(idx.size),
+            "error": "max |u - u_direct| / max |u_direct| at 4,096 seeded targets, FP64 direct sum on the GPU",
+            "forms": forms,
+            "meet_1e-7": sorted(k for k, v in forms.items() if v["meets_1e-7"]),
+            "meet_1e-5": sorted(k for k, v in forms.items() if v["meets_1e-5"])}
+
+
+def run_c4(torch, flush):
+    """Modified Helmholtz K0 (k = 10) on the 2M annulus (Nequiv 40, Ncutoff
+    48): mixed and plain forms, error at 4,096 targets against the FP64 direct
+    sum, and the K0 near-field kernel against the FP32 peak at 40 flops per
+    pair."""
+    cfg = CONFIGS["c4"]
+    x, y, tau = cfg["gen"](cfg["n"], 0)
+    idx = sample_targets(x.size)
+    ref = _direct_ref(cfg, x, y, tau, idx)
+    xd, yd, td = (torch.from_numpy(v).cuda() for v in (x, y, tau))
+    out = {"workload": cfg["desc"], "n_points": x.size}
+    pk, pk_src = peaks()
+    for name, precision in (("mixed", "mixed"), ("plain_fp64", "fp64")):
+        line, f = _form_line(torch, cfg, xd, yd, td, flush, precision, "auto", ref, idx)
+        info = f.tree_info()
+        out[name] = line
+        if precision == "mixed":
+            clk = pk.get("sm_max_mhz", 1965.0) * 1e6
+            peak = 148 * 128 * 2 * clk / 1e12
+            t = line["phases_ms"]["leaf"] * 1e-3
+            ach = float(info.n_p2p_pairs) * 40.0 / t / 1e12 if t > 0 else None
+            out["roofline_k0_p2p"] = {
+                "kernel": "k_leaf_eval_f<K0> (P2P + L2P)", "bound": "fp32", "achieved": ach, "peak": peak,
+                "unit": "TFLOP/s", "frac": ach / peak if ach else None,
+                "work": f"{info.n_p2p_pairs} P2P pairs x 40 flops (K0 series) per launch",
+                "peak_source": f"SIMT peak at sm_max_mhz ({pk_src})"}
+            out["tree"] = {"levels": info.levels, "nodes": info.n_nodes, "p2p_pairs": info.n_p2p_pairs,
+                           "m2l_pairs": info.n_m2l_pairs}
+        del f
+    out["mixed_over_plain"] = out["plain_fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    return out
 
 
 # ------------------------------------------------------- serving stream
@@ -430,15 +570,28 @@ def run_serving(args, device):
     _, cap = srv.run(S.make_stream(args.serve_requests, 0.0, seed=0), realtime=False)
     rate = 0.7 * cap["requests_per_s"]
     _, st = srv.run(S.make_stream(args.serve_requests, rate, seed=0), realtime=True)
-    return {
+    out = {
         "requests": st["requests"], "failed": st["failed"] + cap["failed"],
         "mix": "70% Laplace / 30% K0 (k in {1,10,50}), N log-uniform in [1e3, 3e5] (mixture + circle points), "
-               "8-32 densities per request, Nequiv 32, Ncutoff 64, mixed precision",
-        "capacity_requests_per_s": cap["requests_per_s"], "offered_requests_per_s": rate, "offered_load": 0.7,
-        "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
-        "point_applies_per_s": st["point_applies_per_s"], "wall_s": st["wall_s"],
-        "slots": st["slots"], "hbm_budget_bytes": st["hbm_budget_bytes"],
+               "8-32 fresh N(0,1) densities per request (drawn on the device), Nequiv 32, Ncutoff 64",
+        "batched_mixed": {"precision": "mixed", "slots": st["slots"], "graphs": True,
+                          "capacity_requests_per_s": cap["requests_per_s"], "offered_requests_per_s": rate,
+                          "offered_load": 0.7, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                          "mean_ms": st["mean_ms"], "point_applies_per_s": st["point_applies_per_s"],
+                          "mpts_s": st["point_applies_per_s"] / 1e6, "wall_s": st["wall_s"]},
+        "hbm_budget_bytes": st["hbm_budget_bytes"],
     }
+    if args.serve_plain:
+        # the same requests and arrival times, one at a time, plain FP64, no graphs
+        plain = S.Server(device=device, slots=1, keep_pots=False, precision="fp64", graphs=False)
+        _, sp = plain.run(S.make_stream(args.serve_requests, rate, seed=0), realtime=True)
+        out["failed"] += sp["failed"]
+        out["one_at_a_time_plain"] = {"precision": "fp64", "slots": 1, "graphs": False,
+                                      "offered_requests_per_s": rate, "p50_ms": sp["p50_ms"],
+                                      "p99_ms": sp["p99_ms"], "mean_ms": sp["mean_ms"],
+                                      "point_applies_per_s": sp["point_applies_per_s"],
+                                      "mpts_s": sp["point_applies_per_s"] / 1e6, "wall_s": sp["wall_s"]}
+    return out
 
 
 # ------------------------------------------------------- CPU baseline
@@ -489,7 +642,9 @@ def run_reference(args, cfg):
         "metric": METRIC, "value": v, "unit": "Mpts/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded generator, seed 0)", "impl": "reference",
-        "config": {"workload": cfg["desc"], "n_points": x.size, "precision": "fp64",
+        "config": {"workload": cfg["desc"], "n_points": x.size, "kernel": "laplace" if cfg["kernel"] == 0 else "k0",
+                   "nequiv": cfg["neq"], "ncutoff": cfg["cut"], "precision": "fp64",
+                   "parallelism": "host threads (rank 0 only)", "l2": "n/a (CPU)",
                    "step": "build_tree + precompute + build_expansions + evaluate_to_points(check_self)"},
         "latency_ms": {"p50": float(np.percentile(ts, 50)) * 1e3, "p99": float(np.percentile(ts, 99)) * 1e3},
         "cpu_baseline": {"value": v, "unit": "Mpts/s", "cores": nthr, "kind": "port",
@@ -514,6 +669,10 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=1024,
                     help="requests in the serving stream (0 skips it)")
     ap.add_argument("--serve-slots", type=int, default=8, help="concurrent requests in the serving stream")
+    ap.add_argument("--no-serve-plain", dest="serve_plain", action="store_false",
+                    help="skip the one-at-a-time plain-FP64 run of the serving stream")
+    ap.add_argument("--no-extra-configs", dest="extra_configs", action="store_false",
+                    help="skip the 4M-point M2L-form comparison and the 2M-point K0 annulus")
     args = ap.parse_args()
     cfg = dict(CONFIGS[args.config])
     if args.n:

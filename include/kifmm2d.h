@@ -83,7 +83,19 @@ typedef struct kifmm_options {
                            takes the mixed form); 0 (default): FP32 near field */
     void *stream;       /* cudaStream_t to order work on (cudaStreamLegacy, i.e. 0x1, for the
                            legacy default stream); NULL: the plan creates its own stream */
+    int32_t e2c;        /* how the check-to-equivalent inverse is formed: KIFMM_E2C_* */
+    int32_t reserved;
 } kifmm_options;
+
+/* Check-to-equivalent solve.  The reference LU-factors the Q x Q E2C matrix
+ * per level (class_fmm.py:213-217); its FFT variant diagonalises the same,
+ * circulant, matrix by the DFT of its first row (svd_fmm.py:239-242,
+ * :281-290): Q kernel evaluations and O(Q^2) work per level instead of Q^2
+ * evaluations and an O(Q^3) factorisation. */
+enum {
+    KIFMM_E2C_DENSE = 0,     /* default: Gauss-Jordan inverse of the dense E2C (partial pivoting) */
+    KIFMM_E2C_CIRCULANT = 1  /* inverse from the DFT eigenvalues of the circulant E2C */
+};
 
 #define KIFMM_MAX_LEVELS 30
 

@@ -191,6 +191,10 @@ class FMM(object):
       fix_bbox   False keeps the reference's root box (tree.py:475-484);
       radii      'reference' or '1.5/2.5';
       near_fp64  with precision='mixed', keep P2M/L2P/P2P in FP64;
+      e2c        'dense' (Gauss-Jordan inverse of E2C, the reference's LU,
+                 class_fmm.py:213-217) or 'circulant' (inverse from the DFT
+                 of E2C's first row, the reference's FFT solve,
+                 svd_fmm.py:239-242, :281-290);
       device, stream   CUDA device ordinal and stream handle.
     Unlike the reference, repeated ``build_expansions`` calls on one object
     are exact (workspaces are zeroed on every apply).
@@ -198,7 +202,7 @@ class FMM(object):
 
     def __init__(self, x, y, kernel_functions, numba_functions, Nequiv=48, Ncutoff=50, iscomplex=False,
                  verbose=False, precision="fp64", m2l="auto", fix_bbox=False, radii="reference", device=None,
-                 stream=None, near_fp64=False):
+                 stream=None, near_fp64=False, e2c="dense"):
         if iscomplex:
             raise NotImplementedError("complex kernels are not part of this build")
         kern = None
@@ -231,6 +235,9 @@ class FMM(object):
         opts.fix_bbox = int(bool(fix_bbox))
         opts.radii = 0 if radii == "reference" else 1
         opts.near_fp64 = int(bool(near_fp64))
+        if e2c not in ("dense", "circulant"):
+            raise ValueError("e2c must be 'dense' or 'circulant'")
+        opts.e2c = B.E2C_CIRCULANT if e2c == "circulant" else B.E2C_DENSE
         if device is None:
             device = x.device.index if self._on_device and x.device.index is not None else 0
         opts.device = int(device)

@@ -213,6 +213,8 @@ int kifmm_plan_create(const kifmm_kernel *kernel, int32_t nequiv, int32_t ncutof
         KIFMM_REQUIRE(o.m2l >= KIFMM_M2L_AUTO && o.m2l <= KIFMM_M2L_INT8, KIFMM_ERR_ARG, "unknown M2L form");
         if (o.precision == KIFMM_PREC_MIXED && o.m2l == KIFMM_M2L_AUTO) o.m2l = KIFMM_M2L_INT8;
         KIFMM_REQUIRE(o.radii == 0 || o.radii == 1, KIFMM_ERR_ARG, "unknown radii preset");
+        KIFMM_REQUIRE(o.e2c == KIFMM_E2C_DENSE || o.e2c == KIFMM_E2C_CIRCULANT, KIFMM_ERR_ARG,
+                      "unknown E2C solve");
         KIFMM_REQUIRE(!(o.precision == KIFMM_PREC_MIXED && o.m2l == KIFMM_M2L_FP64), KIFMM_ERR_ARG,
                       "an FP64 M2L belongs to the FP64 precision form");
         kifmm_plan *P = new kifmm_plan();

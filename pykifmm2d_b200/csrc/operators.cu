@@ -23,6 +23,7 @@ namespace kifmm {
 
 struct OpsArgs {
     int L, Q, kind;
+    int circulant;          // E2C inverse from the DFT of its first row (KIFMM_E2C_CIRCULANT)
     double k;
     double W;
     double rf1, rf2;
@@ -81,6 +82,37 @@ __global__ void __launch_bounds__(INV_THREADS) k_ops_inverse(OpsArgs A) {
     double *a = sm, *nb = sm + (size_t)Q * ld;  // current and next matrix, Q x ld each
     const double *b = A.ops + (size_t)l * A.stride;
     const double *lx = b + off_large(Q), *ly = lx + Q, *sx = b + off_small(Q), *sy = sx + Q;
+    if (A.circulant) {
+        // E2C[t][s] = G(small_s -> large_t) depends on (s - t) mod Q only (both
+        // circles carry the same Q angles and G is radial): E2C = C(a) with
+        // a_j = G(small_j -> large_0), and C(a) C(b) = C(a (*) b) (circular
+        // convolution), so the inverse is C(b) with DFT(b) = 1 / DFT(a).  a is
+        // even (a_j = a_{Q-j}), so DFT(a) is real: lambda_m = sum_j a_j
+        // cos(2 pi j m / Q), b_j = (1/Q) sum_m cos(2 pi j m / Q) / lambda_m.
+        // The reference solves with the same diagonalisation by the FFT
+        // (svd_fmm.py:239-242, :281-290); at Q <= 64 the DFT is formed directly.
+        double *av = sm, *lam = sm + Q, *bv = sm + 2 * Q;
+        for (int j = tid; j < Q; j += INV_THREADS) av[j] = gval(A, sx[j], sy[j], lx[0], ly[0]);
+        __syncthreads();
+        for (int m = tid; m < Q; m += INV_THREADS) {
+            double acc = 0.0;
+            for (int j = 0; j < Q; j++) acc = fma(av[j], cospi(2.0 * (double)((j * m) % Q) / Q), acc);
+            lam[m] = acc;
+        }
+        __syncthreads();
+        for (int j = tid; j < Q; j += INV_THREADS) {
+            double acc = 0.0;
+            for (int m = 0; m < Q; m++) acc += cospi(2.0 * (double)((j * m) % Q) / Q) / lam[m];
+            bv[j] = acc / Q;
+        }
+        __syncthreads();
+        double *inv = A.ops + (size_t)l * A.stride + off_inv(Q);  // row-major, inv[s][t] = b[(t - s) mod Q]
+        for (int e = tid; e < Q * Q; e += INV_THREADS) {
+            const int r = e / Q, c = e % Q;
+            inv[e] = bv[(c - r + Q) % Q];
+        }
+        return;
+    }
     for (int e = tid; e < Q * Q2; e += INV_THREADS) {
         const int r = e / Q2, c = e % Q2;
         a[r * ld + c] = c < Q ? gval(A, sx[c], sy[c], lx[r], ly[r]) : (c - Q == r ? 1.0 : 0.0);
@@ -280,6 +312,7 @@ void build_operators(kifmm_plan *P) {
     cudaStream_t s = P->stream;
     OpsArgs A{};
     A.L = L; A.Q = Q; A.kind = P->kern.kind; A.k = P->kern.k; A.W = P->W;
+    A.circulant = P->opt.e2c == KIFMM_E2C_CIRCULANT;
     if (P->opt.radii == 1) { A.rf1 = 1.5; A.rf2 = 2.5; }
     else { A.rf1 = std::sqrt(2.0) + 0.01; A.rf2 = 4.0 - std::sqrt(2.0) - 2 * 0.01; }
     A.stride = ops_stride(Q);

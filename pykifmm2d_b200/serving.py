@@ -14,9 +14,11 @@ The server:
   that arrives while others run starts as soon as a slot and memory free up;
 * keeps the request's tree, plan and translation operators on the device
   across its densities.  The first density runs the apply and captures it as a
-  CUDA graph (``FMM.capture_apply``); each further density is one
-  host-to-device copy of tau, one graph launch and one device-to-host copy of
-  the potentials;
+  CUDA graph (``FMM.capture_apply``); each further density is one graph
+  launch and one device-to-host copy of the potentials, after the density is
+  in place on the device (a host-to-device copy of a given density, or a fresh
+  N(0,1) draw made on the device, as the iterates of an iterative solve on the
+  GPU would be);
 * records arrival, admission and completion times.  Latency is completion
   minus arrival.
 
@@ -34,14 +36,19 @@ import numpy as np
 from . import class_fmm as C
 
 
+# admission budget of the serving stream: 80 GB of device memory for plans
+DEFAULT_HBM_BUDGET = 80_000_000_000
+
+
 @dataclass
 class Request:
     """One FMM job: points (x, y), kernel ('laplace' or 'k0' with wavenumber
     k), Nequiv, Ncutoff and the densities to apply: either ``taus`` (float64
-    arrays of len(x)) or ``napply`` densities made on demand from ``tau_seed``
-    (one N(0,1) draw, then density i = (-1)^i * roll(draw, 7 i), so that a long
-    stream does not hold all its densities in host memory).  ``arrival`` is in
-    seconds from the start of the run."""
+    host arrays of len(x), copied to the device per density) or ``napply``
+    fresh N(0,1) densities drawn on the device, density i from the seed
+    (tau_seed, i) (``device_density``), so that a long stream holds no
+    densities in host memory.  ``arrival`` is in seconds from the start of the
+    run."""
     x: np.ndarray
     y: np.ndarray
     taus: list = None
@@ -58,11 +65,21 @@ class Request:
         return len(self.taus) if self.taus is not None else self.napply
 
     def density(self, i):
+        """Host copy of density i (for checks; the server draws it on the device)."""
         if self.taus is not None:
             return self.taus[i]
-        base = np.random.default_rng(self.tau_seed).standard_normal(len(self.x)) if i == 0 else self._base
-        self._base = base
-        return (-1.0) ** i * np.roll(base, 7 * i)
+        import torch
+        out = torch.empty(len(self.x), dtype=torch.float64, device="cuda")
+        device_density(torch, self.tau_seed, i, out)
+        return out.cpu().numpy()
+
+
+def device_density(torch, seed, i, out):
+    """Fresh N(0,1) density i of a request, drawn into the CUDA tensor ``out``
+    by a generator seeded with (seed, i): the same numbers alone and in any mix."""
+    g = torch.Generator(device=out.device)
+    g.manual_seed(int(seed) * 4096 + int(i))
+    out.normal_(0.0, 1.0, generator=g)
 
 
 @dataclass
@@ -136,7 +153,8 @@ class Scheduler:
 class Server:
     """Continuous-batching FMM server on one GPU (see the module docstring)."""
 
-    def __init__(self, device=0, slots=8, hbm_budget=None, precision="mixed", check_self=True, keep_pots=True):
+    def __init__(self, device=0, slots=8, hbm_budget=None, precision="mixed", check_self=True, keep_pots=True,
+                 graphs=True):
         import torch
         self.keep_pots = bool(keep_pots)
         self.torch = torch
@@ -144,9 +162,10 @@ class Server:
         self.slots = int(slots)
         self.precision = precision
         self.check_self = bool(check_self)
+        self.graphs = bool(graphs)
         if hbm_budget is None:
             free, _ = torch.cuda.mem_get_info(self.device)
-            hbm_budget = int(0.5 * free)
+            hbm_budget = min(DEFAULT_HBM_BUDGET, int(0.9 * free))
         self.hbm_budget = int(hbm_budget)
         dev = torch.device("cuda", self.device)
         self._streams = [torch.cuda.Stream(dev) for _ in range(self.slots)]
@@ -180,9 +199,14 @@ class Server:
                 tau_d = torch.empty(n, dtype=torch.float64, device=dev)
                 pot_d = torch.empty(n, dtype=torch.float64, device=dev)
                 for i in range(req.count()):
-                    tau = req.density(i)
-                    tau_d.copy_(torch.as_tensor(np.ascontiguousarray(tau, dtype=np.float64)))
-                    if i == 0:
+                    if req.taus is not None:
+                        tau_d.copy_(torch.as_tensor(np.ascontiguousarray(req.taus[i], dtype=np.float64)))
+                    else:
+                        device_density(torch, req.tau_seed, i, tau_d)
+                    if not self.graphs:
+                        f.build_expansions(tau_d)
+                        f.evaluate_to_points(xd, yd, self.check_self, out=pot_d)
+                    elif i == 0:
                         f.capture_apply(tau_d, pot_d, self.check_self)
                     else:
                         f.replay()

@@ -305,3 +305,18 @@ def test_int8_tensor_m2l_is_fp64_accurate(golden_cases, name):
     e = rel(pot, g["pot"])
     print(f"{name}: int8 tensor M2L + FP64 near field vs reference {e:.2e}")
     assert e <= 1e-8
+
+
+@pytest.mark.parametrize("name", ["c1_uniform20k", "uniform3k_cut16", "annulus6k_k0", "mix2k_cut8"])
+def test_circulant_e2c_vs_reference(golden_cases, name):
+    """The check-to-equivalent inverse from the DFT eigenvalues of the
+    circulant E2C (the reference's FFT solve, svd_fmm.py:239-242, :281-290)
+    gives the reference's FP64 output, in the plain and the mixed form."""
+    g = golden_cases[name]
+    for precision, tol in (("fp64", 1e-9), ("mixed", 5e-7)):
+        f = make(g, e2c="circulant", precision=precision)
+        f.build_expansions(g["tau"])
+        pot = f.evaluate_to_points(f.x, f.y, True)
+        e = rel(pot, g["pot"])
+        print(f"{name}: circulant E2C, {precision} vs reference {e:.2e}")
+        assert e <= tol

@@ -52,8 +52,20 @@ def test_make_stream_shapes():
     for r in reqs:
         assert 1000 <= len(r.x) <= 5000 and 2 <= r.count() <= 3
         assert r.kernel in ("laplace", "k0")
-        d0, d1 = r.density(0), r.density(1)
-        assert d0.shape == r.x.shape and np.array_equal(d1, -np.roll(d0, 7))
+        assert r.taus is None and r.tau_seed == 1000 + r.rid
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA GPU")
+def test_device_densities_are_fresh_normals():
+    """Each density of a request is its own N(0,1) draw on the device, the same
+    on every call (seeded by request and density index)."""
+    r = S.make_stream(1, rate_per_s=0.0, seed=3, nmin=20000, nmax=20000, applies=(3, 3))[0]
+    d = [r.density(i) for i in range(3)]
+    assert np.array_equal(d[1], r.density(1))
+    for i in range(3):
+        assert abs(d[i].mean()) < 0.05 and abs(d[i].std() - 1.0) < 0.05
+    assert abs(np.corrcoef(d[0], d[1])[0, 1]) < 0.05 and abs(np.corrcoef(d[1], d[2])[0, 1]) < 0.05
 
 
 gpu = [pytest.mark.gpu, pytest.mark.skipif(not has_gpu(), reason="needs a CUDA GPU")]
