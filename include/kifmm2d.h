@@ -246,6 +246,17 @@ int kifmm_set_profiling(kifmm_plan *plan, int32_t on);
  * reset != 0 clears the accumulators after reading. */
 int kifmm_get_phase_times(kifmm_plan *plan, double *ms, int64_t *launches, int32_t reset);
 
+/* Poll budget of the bounded waits inside the apply kernels (no counterpart
+ * in the reference, which has no device code): the bulk-copy waits of the
+ * M2M/L2L level kernels and the copy/MMA completion waits of the tensor-core
+ * M2L.  A wait that runs out sets a device error flag; the kernel then waits
+ * for its own copies and MMAs in flight (with a fixed budget), frees what it
+ * holds and returns, and the next kifmm_synchronize (or host-buffer
+ * evaluation) on the plan reports KIFMM_ERR_CUDA.  polls >= 0 sets the budget
+ * (0: every first wait runs out at once, which tests that path); polls < 0
+ * restores the default.  Drops a captured graph. */
+int kifmm_set_wait_limit(kifmm_plan *plan, int64_t polls);
+
 /* Number of kernels this library has launched in the process so far. */
 int64_t kifmm_launch_count(void);
 

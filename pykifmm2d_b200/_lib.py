@@ -72,6 +72,7 @@ _SIGS = {
     "kifmm_set_profiling": (_i32, [_vp, _i32]),
     "kifmm_get_phase_times": (_i32, [_vp, _vp, _vp, _i32]),
     "kifmm_launch_count": (_i64, []),
+    "kifmm_set_wait_limit": (_i32, [_vp, _i64]),
     "kifmm_morton_sort_noalloc": (_i32, [_vp, _vp, _i64, ctypes.c_double, ctypes.c_double, _vp, _vp, _vp]),
     "kifmm_version": (_i32, []),
 }

@@ -544,6 +544,14 @@ int kifmm_get_phase_times(kifmm_plan *P, double *ms, int64_t *launches, int32_t 
     });
 }
 
+int kifmm_set_wait_limit(kifmm_plan *P, int64_t polls) {
+    return guarded([&] {
+        KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
+        drop_graph(P);  // a captured graph holds the old budget
+        P->wait_limit = polls >= 0 ? (long long)polls : -1;
+    });
+}
+
 int64_t kifmm_launch_count(void) { return g_launch_count.load(); }
 
 int kifmm_version(void) { return 100; }

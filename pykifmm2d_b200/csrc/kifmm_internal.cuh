@@ -152,6 +152,7 @@ struct kifmm_plan {
     uint64_t spec_cap = 0;           // split-cell capacity for the next build (from the last one)
     bool ops_pending = false;
     cudaGraphExec_t graph = nullptr;  // captured apply (kifmm_graph_capture)
+    long long wait_limit = -1;        // poll budget of the apply kernels' first waits (-1: kDefaultWaitPolls)
     int device = 0;
     int num_sms = 148;
 
@@ -271,6 +272,17 @@ constexpr int HP_STATS = 200;  // [4] work counts
 constexpr int HP_WORDS = 256;
 unsigned long long *pinned_acquire();
 void pinned_release(unsigned long long *p);
+
+// Poll budgets of the bounded waits in the apply kernels: a first wait gets
+// the plan's budget (kifmm_set_wait_limit, default kDefaultWaitPolls); if it
+// runs out, the kernel flags the error and waits once more with
+// kDrainWaitPolls so that its copies and MMAs in flight land before it frees
+// its resources and returns.
+constexpr long long kDefaultWaitPolls = 1ll << 26;
+constexpr long long kDrainWaitPolls = 1ll << 26;
+inline long long plan_wait_polls(const kifmm_plan *P) {
+    return P->wait_limit >= 0 ? P->wait_limit : kDefaultWaitPolls;
+}
 
 // device scalar slots (plan->scal) holding error flags that the host reads
 // after an apply: a bulk-copy wait in the level passes that ran out, and an

@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_m2l_tc(TcArgs T) {
     // still in flight lands before the block frees TMEM and leaves)
     auto wait_slot = [&](const uint32_t *bar, uint32_t *par, int *cnt, int slot) {
         bool ok = mbar_wait(bar[slot], par[slot], T.wait_limit);
-        if (!ok) mbar_wait(bar[slot], par[slot], T.wait_limit);
+        if (!ok) mbar_wait(bar[slot], par[slot], kDrainWaitPolls);
         par[slot] ^= 1u;
         cnt[slot]--;
         return __syncthreads_or(!ok) == 0;
@@ -547,7 +547,7 @@ static void run_m2l_tensor_t(kifmm_plan *P, const PassArgs &A) {
     T.rowscale = P->tc_rowscale.p;
     T.pre = pre;
     T.err = P->scal.p + KIFMM_SCAL_TC_ERR;
-    T.wait_limit = 1ll << 26;
+    T.wait_limit = plan_wait_polls(P);
     T.lmin = 1;
     T.lmax = L - 2;
     int64_t tiles = 0;

@@ -643,7 +643,7 @@ __global__ void __launch_bounds__(LM_THREADS) k_lvl_mma(PassArgs A, int l, int M
     const bool ok = __syncthreads_and(mbar_wait(mb, 0, wait_limit));
     if (!ok) {
         if (tid == 0) atomicOr(err, 1ull);
-        mbar_wait(mb, 0, wait_limit);  // let copies in flight land before the block leaves
+        mbar_wait(mb, 0, kDrainWaitPolls);  // let copies in flight land before the block leaves
         return;
     }
     const int warp = tid >> 5, lane = tid & 31, g = lane >> 2, t = lane & 3;
@@ -699,7 +699,7 @@ static void launch_lvl_mma(kifmm_plan *P, const PassArgs &A, int l, int M, int K
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    KIFMM_CUDA(cudaLaunchKernelEx(&cfg, k_lvl_mma<MODE, MT>, A, l, M, K, 1ll << 26,
+    KIFMM_CUDA(cudaLaunchKernelEx(&cfg, k_lvl_mma<MODE, MT>, A, l, M, K, plan_wait_polls(P),
                                   P->scal.p + KIFMM_SCAL_PASS_ERR));
     KIFMM_LAUNCHED();
 }

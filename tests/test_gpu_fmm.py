@@ -320,3 +320,31 @@ def test_circulant_e2c_vs_reference(golden_cases, name):
         e = rel(pot, g["pot"])
         print(f"{name}: circulant E2C, {precision} vs reference {e:.2e}")
         assert e <= tol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_bounded_wait_that_runs_out_is_reported(golden_cases, precision):
+    """A poll budget of 0 makes the first bounded wait of every M2M/L2L level
+    kernel (and, in the mixed form, of the tensor-core M2L) run out: the
+    kernels flag it, let their copies and MMAs in flight land, free TMEM and
+    return; the evaluation reports KIFMM_ERR_CUDA instead of hanging.  With
+    the default budget restored, the same plan and a fresh one give the
+    reference's output again."""
+    from pykifmm2d_b200 import _lib as B
+    g = golden_cases["uniform3k_cut16"]
+    lib = B.load()
+    f = make(g, precision=precision)
+    f.precompute()
+    B.check(lib.kifmm_set_wait_limit(f._plan, 0))
+    with pytest.raises(B.KifmmError) as e:
+        f.build_expansions(g["tau"])
+        f.evaluate_to_points(f.x, f.y, True)
+    assert e.value.code == B.ERR_CUDA
+    assert "timed out" in str(e.value)
+    B.check(lib.kifmm_set_wait_limit(f._plan, -1))
+    tol = 1e-9 if precision == "fp64" else 5e-7
+    f.build_expansions(g["tau"])
+    assert rel(f.evaluate_to_points(f.x, f.y, True), g["pot"]) <= tol
+    h = make(g, precision=precision)
+    h.build_expansions(g["tau"])
+    assert rel(h.evaluate_to_points(h.x, h.y, True), g["pot"]) <= tol
