@@ -313,7 +313,10 @@ def test_circulant_e2c_vs_reference(golden_cases, name):
     circulant E2C (the reference's FFT solve, svd_fmm.py:239-242, :281-290)
     gives the reference's FP64 output, in the plain and the mixed form."""
     g = golden_cases[name]
-    for precision, tol in (("fp64", 1e-9), ("mixed", 5e-7)):
+    fin = np.isfinite(g["direct"])
+    e_ref = np.abs(g["pot"] - g["direct"])[fin].max() / np.abs(g["direct"][fin]).max()
+    # the mixed bound of test_mixed_m2l_forms_vs_reference for the int8 form
+    for precision, tol in (("fp64", 1e-9), ("mixed", max(5e-7, 0.2 * e_ref))):
         f = make(g, e2c="circulant", precision=precision)
         f.build_expansions(g["tau"])
         pot = f.evaluate_to_points(f.x, f.y, True)
