@@ -10,9 +10,13 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 }
 // order generic-proxy shared-memory writes before later async-proxy (bulk) reads
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void mbar_init(uint32_t bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
+// an mbarrier whose phase completes after `count` arrivals (and its tx bytes)
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count = 1) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 // bounded wait on the mbarrier phase; false after `limit` polls
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit) {
@@ -27,6 +31,11 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long lo
         if (done) return true;
     }
     return false;
+}
+// 16-byte asynchronous copy global -> shared (cp.async, L2 only); src_bytes = 0
+// writes zeros without reading
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void *src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");

@@ -201,10 +201,12 @@ struct kifmm_plan {
     kifmm::DBuf<double> leaf_coef;   // [n_leaf_list][2p+1] Taylor coefficients per apply
     kifmm::DBuf<unsigned char> tc_pre;  // per-apply slices of the source groups
     kifmm::DBuf<int> tc_gexp;
+    kifmm::DBuf<int> tc_src8;        // [n_ent][8] M2L source entry per direction (per apply)
 
     // workspaces
     kifmm::DBuf<double> tau, taus, pots, pot_out, tx, ty, tpot;
     kifmm::DBuf<double> uup, udown;
+    kifmm::DBuf<double> zero4q;      // 4Q zeros: the source of an absent M2L direction
     bool have_expansions = false;
 
     // scratch for the tree build

@@ -9,12 +9,19 @@
 // with C_d = CM2LS_d . blockdiag(Inv) (4Q x 4Q, FP64, operators.cu).  As a
 // GEMM: D[rows, targets] = A[rows, 8 x 4Q] . B[targets, 8 x 4Q]^T where B's
 // columns are gathered per target from its eight neighbour groups.  A CTA
-// owns TC_N = 32 targets and one 128-row M tile (its five int8 accumulators
-// fit a 256-column TMEM allocation and its tiles 101 KB of shared memory, so
-// two CTAs share an SM and one's copies overlap the other's MMAs); per direction (and per
-// K chunk of 128) it stages A and B in shared memory in the UMMA K-major,
-// no-swizzle layout, one thread issues the MMA chain, tcgen05.commit signals
-// an mbarrier, and the epilogue reads TMEM with tcgen05.ld.
+// owns TN target groups (96 for int8: five accumulators of 96 columns fill
+// the 512 TMEM columns of an SM) and one 128-row M tile.  Its work is a list
+// of stages (direction with a source in the tile, 64-byte K chunk) that runs
+// through a ring of TC_STAGES shared-memory slots, warp-specialised:
+//   * warps 0-3 gather the sources' pre-sliced K chunks into a slot (16-byte
+//     cp.async copies) and arrive on its B-full barrier once they landed;
+//   * one thread of warp 4 copies the operator chunk into the slot with one
+//     bulk copy (A-full barrier, transaction bytes), waits for both, issues the
+//     stage's MMA chain and commits it to the slot's empty barrier, which
+//     frees the slot for the gather warps and for its own next operator copy;
+//   * after the last stage, warps 0-3 read TMEM (each its 32 lanes) and
+//     write the FP64 results.
+// Operands sit in the UMMA K-major, no-swizzle core-matrix layout.
 //
 // Forms:
 //   INT8 (default): A row-scaled and B column-scaled by powers of two into
@@ -38,40 +45,43 @@
 namespace kifmm {
 
 enum TcForm { TC_INT8 = 0, TC_BF16 = 1, TC_FP16 = 2 };
+// NS slices per operand, EB bytes per element, KSTEP elements per MMA, NACC
+// accumulators, TN target groups per CTA (MMA N), NCOLS TMEM columns allocated
 template <int F> struct TcTraits;
-template <> struct TcTraits<TC_INT8> { static constexpr int NS = 5, EB = 1, KSTEP = 32, NACC = 5, NCOLS = 256; };
-template <> struct TcTraits<TC_BF16> { static constexpr int NS = 2, EB = 2, KSTEP = 16, NACC = 1, NCOLS = 32; };
-template <> struct TcTraits<TC_FP16> { static constexpr int NS = 2, EB = 2, KSTEP = 16, NACC = 1, NCOLS = 32; };
+template <> struct TcTraits<TC_INT8> { static constexpr int NS = 5, EB = 1, KSTEP = 32, NACC = 5, TN = 96, NCOLS = 512; };
+template <> struct TcTraits<TC_BF16> { static constexpr int NS = 2, EB = 2, KSTEP = 16, NACC = 1, TN = 64, NCOLS = 64; };
+template <> struct TcTraits<TC_FP16> { static constexpr int NS = 2, EB = 2, KSTEP = 16, NACC = 1, TN = 64, NCOLS = 64; };
 
-constexpr int TC_M = 128;      // MMA M: operator rows per tile (TMEM lanes)
-constexpr int TC_N = 32;       // MMA N: target groups per CTA
-constexpr int TC_KC = 128;     // K elements staged per stage
-// Stages in flight.  One: at K = 128 a stage is 100 KB, and two CTAs per SM
-// (one's copies under the other's MMAs) measured faster than two 64-K slots in
-// one CTA, whose extra stages cost more synchronisation than they hid.
-constexpr int TC_SLOTS = 1;
-constexpr int TC_THREADS = 128;
-static_assert(TC_N % 16 == 0 && TC_N >= 16 && TC_N <= 256, "MMA N for M = 128");
-static_assert(TcTraits<TC_INT8>::NACC * TC_N <= TcTraits<TC_INT8>::NCOLS, "int8 accumulators exceed the TMEM allocation");
-static_assert(TcTraits<TC_BF16>::NACC * TC_N <= TcTraits<TC_BF16>::NCOLS, "accumulator exceeds the TMEM allocation");
-static_assert(2 * TcTraits<TC_INT8>::NCOLS <= 512, "two CTAs per SM must fit the 512 TMEM columns");
+constexpr int TC_M = 128;        // MMA M: operator rows per tile (TMEM lanes)
+constexpr int TC_KCB = 64;       // bytes of K per slice row and stage (2 MMA K steps)
+constexpr int TC_STAGES = 3;     // shared-memory ring slots
+constexpr int TC_GWARPS = 4;     // gather / epilogue warps (TMEM lanes 32 w .. 32 w + 31)
+constexpr int TC_THREADS = 32 * (TC_GWARPS + 1);
+template <int F>
+constexpr bool tc_traits_ok() {
+    using TR = TcTraits<F>;
+    return TR::TN % 16 == 0 && TR::TN >= 16 && TR::TN <= 256 && TR::NACC * TR::TN <= TR::NCOLS &&
+           TR::TN <= 32 * TC_GWARPS && TR::TN % 32 == 0 && (TC_KCB / TR::EB) % TR::KSTEP == 0;
+}
+static_assert(tc_traits_ok<TC_INT8>() && tc_traits_ok<TC_BF16>() && tc_traits_ok<TC_FP16>(), "tile shapes");
 constexpr double FP16_PRESCALE = 4096.0;
 
 struct TcGeom {
     int Q4, MP, MT, KP, NKC;   // rows, padded rows, M tiles, padded K per direction, K chunks
-    size_t slice_bytes;        // one slice of one A tile chunk: 128 x TC_KC x EB
+    size_t slice_bytes;        // one slice of one A tile chunk: 128 x TC_KCB bytes
     size_t level_bytes;        // all A slices of one level
 };
 
 template <int F>
 static TcGeom tc_geom(int Q) {
+    constexpr int KCE = TC_KCB / TcTraits<F>::EB;
     TcGeom g;
     g.Q4 = 4 * Q;
     g.MP = (g.Q4 + TC_M - 1) / TC_M * TC_M;
     g.MT = g.MP / TC_M;
-    g.KP = (g.Q4 + TC_KC - 1) / TC_KC * TC_KC;
-    g.NKC = g.KP / TC_KC;
-    g.slice_bytes = (size_t)TC_M * TC_KC * TcTraits<F>::EB;
+    g.KP = (g.Q4 + KCE - 1) / KCE * KCE;
+    g.NKC = g.KP / KCE;
+    g.slice_bytes = (size_t)TC_M * TC_KCB;
     g.level_bytes = (size_t)9 * g.MT * g.NKC * TcTraits<F>::NS * g.slice_bytes;
     return g;
 }
@@ -94,7 +104,7 @@ __device__ __forceinline__ uint32_t instr_desc() {
     uint32_t fmt = F == TC_INT8 ? ((2u << 4) | (1u << 7) | (1u << 10))    // s32 <- s8 x s8
                  : F == TC_BF16 ? ((1u << 4) | (1u << 7) | (1u << 10))    // f32 <- bf16 x bf16
                                 : (1u << 4);                              // f32 <- f16 x f16
-    return fmt | ((uint32_t)(TC_N >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
+    return fmt | ((uint32_t)(TcTraits<F>::TN >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
 }
 template <int F>
 __device__ __forceinline__ void mma_issue(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
@@ -117,6 +127,15 @@ __device__ __forceinline__ void mma_commit(uint32_t bar) {
 }
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t (&v)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15}, [%16];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+        : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
@@ -191,9 +210,10 @@ __global__ void k_tc_slices(TcOpsArgs T) {
     for (int e = blockIdx.z * blockDim.x + threadIdx.x; e < total; e += gridDim.z * blockDim.x) {
         int r = e % T.g.MP, k = e / T.g.MP;
         double v = (r < Q4 && k < Q4) ? C[(size_t)k * Q4 + r] * (1.0 / scale_of(r)) : 0.0;
-        int mt = r / TC_M, kc = k / TC_KC;
+        constexpr int KCE = TC_KCB / TcTraits<F>::EB;
+        int mt = r / TC_M, kc = k / KCE;
         unsigned char *tile = base + (((size_t)d * T.g.MT + mt) * T.g.NKC + kc) * TcTraits<F>::NS * sb;
-        put_slices<F>(tile, sb, core_off(r % TC_M, k % TC_KC, TC_M, TcTraits<F>::EB), v);
+        put_slices<F>(tile, sb, core_off(r % TC_M, k % KCE, TC_M, TcTraits<F>::EB), v);
     }
 }
 
@@ -205,6 +225,7 @@ __global__ void k_tc_slices(TcOpsArgs T) {
 struct TcPre {
     unsigned char *slices;   // [n_ent][NS][KP] elements
     int *gexp;               // [n_ent] (INT8)
+    int *src8;               // [n_ent][8] source entry of a split entry per direction (-1: none)
     int KP;
 };
 
@@ -218,6 +239,10 @@ __global__ void k_tc_preslice(PassArgs A, int64_t n_ent, TcPre T) {
     if (j >= n_ent) return;
     const int Q4 = 4 * A.Q;
     int l = (int)(A.ent[j] >> ENT_LEVEL_SHIFT);
+    if (lane < 8) {  // the entry's M2L sources by direction (split entries only)
+        const int d = lane < 4 ? lane : lane + 1;
+        T.src8[j * 8 + lane] = (A.ent[j] & 1) ? -1 : m2l_source_entry(A.ncoll, A.nent, A.nbot, A.ntop, A.ent_node[j], d);
+    }
     int64_t cg = A.T.off[l + 1] + 4 * (j - A.T.eoff[l]);
     const double *u = A.uup + (size_t)cg * A.Q;
     unsigned char *out = T.slices + (size_t)j * TR::NS * T.KP * TR::EB;
@@ -274,25 +299,47 @@ struct TcArgs {
 };
 
 template <int F>
-__global__ void __launch_bounds__(TC_THREADS, 2) k_m2l_tc(TcArgs T) {
+static constexpr size_t tc_stage_a() { return (size_t)TcTraits<F>::NS * TC_M * TC_KCB; }
+template <int F>
+static constexpr size_t tc_stage_b() { return (size_t)TcTraits<F>::NS * TcTraits<F>::TN * TC_KCB; }
+// shared memory: ring (A then B per slot), then per-target tables, then barriers
+template <int F>
+static constexpr size_t tc_table_off() { return TC_STAGES * (tc_stage_a<F>() + tc_stage_b<F>()); }
+template <int F>
+static constexpr size_t tc_smem_bytes() {
+    constexpr int TN = TcTraits<F>::TN;
+    return tc_table_off<F>() + (size_t)TN * 8 * 4 * 2 + (size_t)TN * 8 + (size_t)TN * 4 + 16 * 4 +
+           (3 * TC_STAGES + 2) * 8 + 16;
+}
+
+// warp-uniform bounded wait: true once the phase with this parity has completed
+__device__ __forceinline__ bool warp_wait(uint32_t bar, uint32_t parity, long long limit) {
+    return __any_sync(0xffffffffu, mbar_wait(bar, parity, limit));
+}
+
+template <int F>
+__global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(TcArgs T) {
     using TR = TcTraits<F>;
+    constexpr int TN = TR::TN, NS = TR::NS, EB = TR::EB, S = TC_STAGES;
+    constexpr int KSTEPS = TC_KCB / EB / TR::KSTEP;
+    constexpr uint32_t A_SLICE = TC_M * TC_KCB, B_SLICE = TN * TC_KCB;
+    constexpr uint32_t A_STAGE = NS * A_SLICE, B_STAGE = NS * B_SLICE;
     extern __shared__ __align__(1024) unsigned char tc_smem[];
+    unsigned char *sA = tc_smem;                                  // [S][NS][128 x 64 B]
+    unsigned char *sB = sA + S * A_STAGE;                         // [S][NS][TN x 64 B]
+    int *sgrp = (int *)(tc_smem + tc_table_off<F>());             // [TN][8] source entry per direction
+    int *sshift = sgrp + TN * 8;                                  // [TN][8] slice shift (INT8)
+    double *stau = (double *)(sshift + TN * 8);                   // [TN] column scale
+    int *sact = (int *)(stau + TN);                               // [TN]
+    int *sdir = sact + TN;                                        // [8] directions with a source; [8] count; [9] abort
+    uint64_t *bars = (uint64_t *)(((uintptr_t)(sdir + 16) + 7) & ~(uintptr_t)7);
+    uint32_t *tslot = (uint32_t *)(bars + 3 * S + 1);
+    volatile int *abort_flag = sdir + 9;
     pdl_trigger();
     pdl_wait();
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const PassArgs &A = T.A;
-    const int Q = A.Q, Q4 = T.g.Q4, KP = T.pre.KP;
-    const size_t a_sb = T.g.slice_bytes;                       // A slice (128 x KC)
-    const size_t b_sb = (size_t)TC_N * TC_KC * TR::EB;         // B slice (TC_N x KC)
-    const size_t a_stage = TR::NS * a_sb, b_stage = TR::NS * b_sb;
-    unsigned char *sA = tc_smem;                               // [TC_SLOTS][NS slices]
-    unsigned char *sB = sA + TC_SLOTS * a_stage;               // [TC_SLOTS][NS slices]
-    int *sgrp = (int *)(sB + TC_SLOTS * b_stage);              // [TC_N][9]
-    int *sshift = sgrp + TC_N * 9;                             // [TC_N][9] slice shift (INT8)
-    double *stau = (double *)(sshift + TC_N * 9 + 2);          // [TC_N]
-    int *sact = (int *)(stau + TC_N);                          // [TC_N]
-    uint64_t *bars = (uint64_t *)(sact + TC_N + 2);            // [0..1] A landed, [2..3] MMAs done (per stage slot)
-    uint32_t *tslot = (uint32_t *)(bars + 4);
+    const int Q = A.Q, Q4 = T.g.Q4, KP = T.pre.KP, NKC = T.g.NKC;
 
     // which level / column tile / M tile
     const int64_t tile = blockIdx.x;
@@ -300,175 +347,212 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_m2l_tc(TcArgs T) {
     while (l < T.lmax && T.tile_off[l + 1] <= tile) l++;
     const int64_t lt = tile - T.tile_off[l];
     const int mt = (int)(lt % T.g.MT);
-    const int64_t ct = lt / T.g.MT;
-    const int64_t ne = A.T.ne[l], eoff = A.T.eoff[l];
-    const int64_t e0 = ct * TC_N;
+    const int64_t e0 = (lt / T.g.MT) * TN, ne = A.T.ne[l], eoff = A.T.eoff[l];
     const int lt1 = l + 1;  // target level: its operators
     const unsigned char *alev = T.aslices + (size_t)lt1 * T.g.level_bytes;
     const double *rsl = T.rowscale + (size_t)lt1 * T.g.MP;
 
-    if (warp == 0) {
+    if (warp == TC_GWARPS) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tslot)),
                      "r"(TR::NCOLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
-    if (tid < TC_N) {
-        int64_t e = e0 + tid;
-        bool act = e < ne && !(A.ent[eoff + e] & 1);
-        int p = act ? A.ent_node[eoff + e] : -1;
+    if (tid == 0) sdir[10] = 0;
+    __syncthreads();
+    if (tid < TN) {
+        const int64_t e = e0 + tid;
+        const bool act = e < ne && !(A.ent[eoff + e] & 1);
         int kcol = -1000000;
-        for (int d = 0; d < 9; d++) {
-            int grp = -1;
-            if (act && d != 4) {
-                grp = m2l_source_entry(A.ncoll, A.nent, A.nbot, A.ntop, p, d);
-                if (F == TC_INT8 && grp >= 0) kcol = max(kcol, T.pre.gexp[grp]);
-            }
-            sgrp[tid * 9 + d] = grp;
+        int gs[8];
+#pragma unroll
+        for (int dd = 0; dd < 8; dd++) gs[dd] = act ? T.pre.src8[(eoff + e) * 8 + dd] : -1;
+#pragma unroll
+        for (int dd = 0; dd < 8; dd++) {
+            const int grp = gs[dd];
+            if (F == TC_INT8 && grp >= 0) kcol = max(kcol, T.pre.gexp[grp]);
+            sgrp[tid * 8 + dd] = grp;
         }
         if (kcol == -1000000) kcol = 0;
-        for (int d = 0; d < 9; d++) {
-            int grp = sgrp[tid * 9 + d];
-            sshift[tid * 9 + d] = (F == TC_INT8 && grp >= 0) ? kcol - T.pre.gexp[grp] : 0;
+        for (int dd = 0; dd < 8; dd++) {
+            const int grp = sgrp[tid * 8 + dd];
+            sshift[tid * 8 + dd] = (F == TC_INT8 && grp >= 0) ? kcol - T.pre.gexp[grp] : 0;
         }
         stau[tid] = F == TC_INT8 ? ldexp(1.0, 7 * kcol) : 1.0;
         sact[tid] = act;
     }
-    if (tid == 0)
-        for (int i = 0; i < 4; i++) mbar_init(smem_u32(&bars[i]));
+    if (tid == 0) {
+        for (int i = 0; i < S; i++) {
+            mbar_init(smem_u32(&bars[i]), 1);                  // A full: the copy's bytes
+            mbar_init(smem_u32(&bars[S + i]), 32 * TC_GWARPS); // B full: each gather thread's copies
+            mbar_init(smem_u32(&bars[2 * S + i]), 1);          // empty: the stage's MMA commit
+        }
+        mbar_init(smem_u32(&bars[3 * S]), 1);                  // accumulators complete
+        sdir[9] = 0;
+    }
+    if (tid < TN) {  // directions with a source somewhere in the tile: OR of the targets' masks
+        unsigned m = 0;
+        for (int dd = 0; dd < 8; dd++) m |= (sgrp[tid * 8 + dd] >= 0 ? 1u : 0u) << dd;
+        for (int o = 16; o; o >>= 1) m |= __shfl_xor_sync(0xffffffffu, m, o);
+        if (lane == 0 && m) atomicOr(&sdir[10], (int)m);
+    }
     fence_before();
     __syncthreads();
     fence_after();
+    if (tid == 0) {
+        const unsigned m = (unsigned)sdir[10];
+        int n = 0;
+        for (int dd = 0; dd < 8; dd++)
+            if (m >> dd & 1u) sdir[n++] = dd;
+        sdir[8] = n;
+    }
+    __syncthreads();
     const uint32_t tmem = *tslot;
-    const uint32_t idesc = instr_desc<F>();
-    const uint32_t bfull[2] = {smem_u32(&bars[0]), smem_u32(&bars[1])};
-    const uint32_t bdone[2] = {smem_u32(&bars[2]), smem_u32(&bars[3])};
-    uint32_t pfull[2] = {0u, 0u}, pdone[2] = {0u, 0u};
-    int nfull[2] = {0, 0}, ndone[2] = {0, 0};  // copies / commits issued and not yet waited for, per slot
-    bool failed = false;
-    const uint32_t a_bytes = (uint32_t)a_stage;
-    constexpr int CH = TC_KC * TR::EB / 16;  // 16-byte chunks per slice row
-    const int NKC = T.g.NKC, NST = 8 * NKC;   // stages: (direction != centre, K chunk)
+    const int nst = sdir[8] * NKC;
+    const uint32_t afull0 = smem_u32(&bars[0]), bfull0 = smem_u32(&bars[S]), empty0 = smem_u32(&bars[2 * S]);
+    const uint32_t accbar = smem_u32(&bars[3 * S]);
 
-    // stage st into slot: A by one bulk copy (on bfull[slot]), B by 16-byte copies
-    // of the pre-sliced source groups (shifted slices for INT8)
-    auto prepare = [&](int st, int slot) {
-        const int dd = st / NKC, d = dd < 4 ? dd : dd + 1, kc = st % NKC;
-        if (tid == 0) {
-            mbar_expect_tx(bfull[slot], a_bytes);
-            bulk_g2s(smem_u32(sA + slot * a_stage), alev + (((size_t)d * T.g.MT + mt) * NKC + kc) * a_stage, a_bytes,
-                     bfull[slot]);
-        }
-        nfull[slot]++;
-        unsigned char *sBs = sB + slot * b_stage;
-        // all of a thread's loads first, then its stores: one round trip per stage
-        constexpr int NBI = TC_N * TR::NS * CH, NB = (NBI + TC_THREADS - 1) / TC_THREADS;
-        uint4 v[NB];
+    if (warp == TC_GWARPS) {
+        if (lane == 0) {
+            // operator chunk of stage st into slot st % S
+            auto issue_a = [&](int st) {
+                const int d0 = sdir[st / NKC], d = d0 < 4 ? d0 : d0 + 1, kc = st % NKC, slot = st % S;
+                const uint32_t bar = afull0 + 8u * slot;
+                mbar_expect_tx(bar, A_STAGE);
+                bulk_g2s(smem_u32(sA + slot * A_STAGE), alev + (((size_t)d * T.g.MT + mt) * NKC + kc) * A_STAGE, A_STAGE,
+                         bar);
+            };
+            int issued = 0, consumed = 0;
+            for (; issued < S && issued < nst; issued++) issue_a(issued);
+            const uint32_t idesc = instr_desc<F>();
+            const uint32_t a_lbo = (TC_M / 8) * 128, b_lbo = (TN / 8) * 128;
+            bool ok = true;
+            for (int st = 0; st < nst; st++) {
+                const int slot = st % S;
+                const uint32_t ph = (uint32_t)(st / S) & 1u;
+                if (!mbar_wait(afull0 + 8u * slot, ph, T.wait_limit) || !mbar_wait(bfull0 + 8u * slot, ph, T.wait_limit)) {
+                    ok = false;
+                    break;
+                }
+                consumed++;
+                fence_after();
+                const uint32_t a0 = smem_u32(sA + slot * A_STAGE), b0 = smem_u32(sB + slot * B_STAGE);
 #pragma unroll
-        for (int q = 0; q < NB; q++) {
-            const int idx = tid + q * TC_THREADS;
-            v[q] = make_uint4(0, 0, 0, 0);
-            if (idx < NBI) {
-                const int c = idx % CH, i = (idx / CH) % TR::NS, j = idx / (CH * TR::NS);
-                const int grp = sgrp[j * 9 + d], si = i - sshift[j * 9 + d];
-                if (grp >= 0 && si >= 0 && si < TR::NS)
-                    v[q] = __ldg((const uint4 *)(T.pre.slices + ((size_t)grp * TR::NS + si) * KP * TR::EB +
-                                                 (size_t)kc * TC_KC * TR::EB + c * 16));
-            }
-        }
+                for (int ks = 0; ks < KSTEPS; ks++) {
 #pragma unroll
-        for (int q = 0; q < NB; q++) {
-            const int idx = tid + q * TC_THREADS;
-            if (idx < NBI) {
-                const int c = idx % CH, i = (idx / CH) % TR::NS, j = idx / (CH * TR::NS);
-                *(uint4 *)(sBs + i * b_sb + core_off(j, c * 16 / TR::EB, TC_N, TR::EB)) = v[q];
-            }
-        }
-        fence_proxy_async();
-        fence_before();
-        __syncthreads();
-    };
-    // bounded wait on a slot barrier, uniform over the block
-    // (a wait that runs out is tried once more, bounded, so that a copy or MMA
-    // still in flight lands before the block frees TMEM and leaves)
-    auto wait_slot = [&](const uint32_t *bar, uint32_t *par, int *cnt, int slot) {
-        bool ok = mbar_wait(bar[slot], par[slot], T.wait_limit);
-        if (!ok) mbar_wait(bar[slot], par[slot], kDrainWaitPolls);
-        par[slot] ^= 1u;
-        cnt[slot]--;
-        return __syncthreads_or(!ok) == 0;
-    };
-
-    // pipeline over TC_SLOTS slots: the MMAs of stage st run on the tensor pipe
-    // while the block stages st + 1 into the next slot
-    prepare(0, 0);
-    for (int st = 0; st < NST && !failed; st++) {
-        const int slot = st % TC_SLOTS;
-        if (!wait_slot(bfull, pfull, nfull, slot)) {
-            failed = true;
-            break;
-        }
-        if (tid == 0) {
-            fence_after();
-            const uint32_t a0 = smem_u32(sA + slot * a_stage), b0 = smem_u32(sB + slot * b_stage);
-            const uint32_t a_lbo = (TC_M / 8) * 128, b_lbo = (TC_N / 8) * 128;
-            for (int ks = 0; ks < TC_KC / TR::KSTEP; ks++) {
-                for (int i = 0; i < TR::NS; i++) {
-                    const int jmax = F == TC_INT8 ? TR::NS - 1 - i : (i == 0 ? 1 : 0);
-                    for (int jj = 0; jj <= jmax; jj++) {
-                        const int acc = F == TC_INT8 ? i + jj : 0;
-                        const bool first = st == 0 && ks == 0 && i == 0 && (F == TC_INT8 || jj == 0);
-                        uint64_t ad = umma_desc(a0 + i * (uint32_t)a_sb + ks * 2 * a_lbo, a_lbo, 128);
-                        uint64_t bd = umma_desc(b0 + jj * (uint32_t)b_sb + ks * 2 * b_lbo, b_lbo, 128);
-                        mma_issue<F>(tmem + acc * TC_N, ad, bd, idesc, first ? 0u : 1u);
+                    for (int i = 0; i < NS; i++) {
+                        const int jmax = F == TC_INT8 ? NS - 1 - i : (i == 0 ? 1 : 0);
+                        for (int jj = 0; jj <= jmax; jj++) {
+                            const int acc = F == TC_INT8 ? i + jj : 0;
+                            const bool first = st == 0 && ks == 0 && i == 0 && (F == TC_INT8 || jj == 0);
+                            const uint64_t ad = umma_desc(a0 + i * A_SLICE + ks * 2 * a_lbo, a_lbo, 128);
+                            const uint64_t bd = umma_desc(b0 + jj * B_SLICE + ks * 2 * b_lbo, b_lbo, 128);
+                            mma_issue<F>(tmem + acc * TN, ad, bd, idesc, first ? 0u : 1u);
+                        }
                     }
                 }
+                mma_commit(empty0 + 8u * slot);
+                // the operator copy of stage st - 1 + S goes into the slot of stage
+                // st - 1 once that stage's MMAs (issued before these) are done
+                if (st >= 1 && issued < nst) {
+                    const int ps = (st - 1) % S;
+                    if (!mbar_wait(empty0 + 8u * ps, (uint32_t)((st - 1) / S) & 1u, T.wait_limit)) {
+                        ok = false;
+                        break;
+                    }
+                    issue_a(issued++);
+                }
             }
-            mma_commit(bdone[slot]);
+            if (!ok) {
+                *abort_flag = 1;
+                atomicOr(T.err, 1ull);
+            }
+            mma_commit(accbar);  // completes once every MMA issued above is done
+            // operator copies issued but never waited for land before the block leaves
+            for (int st = consumed; st < issued; st++) mbar_wait(afull0 + 8u * (st % S), (uint32_t)(st / S) & 1u, kDrainWaitPolls);
         }
-        ndone[slot]++;
-        if (st + 1 < NST) {
-            const int ns = (st + 1) % TC_SLOTS;
-            if (ndone[ns] > 0 && !wait_slot(bdone, pdone, ndone, ns)) {  // the MMAs that last read slot ns
-                failed = true;
+        __syncwarp();
+    } else {
+        // gather warps: the sources' slices of stage st into slot st % S by
+        // 16-byte cp.async copies, one commit group per stage; a thread arrives
+        // on a slot's B-full barrier once its copies of that stage have landed,
+        // checked one stage later so that two stages' copies are in flight
+        constexpr int CH = TC_KCB / 16, NP = TN * NS * CH, PER = (NP + 32 * TC_GWARPS - 1) / (32 * TC_GWARPS);
+        int gdone = 0;  // stages whose copies this thread issued
+        for (int st = 0; st < nst; st++) {
+            if (*abort_flag) break;
+            const int slot = st % S, dd = sdir[st / NKC], kc = st % NKC;
+            if (st >= S && !warp_wait(empty0 + 8u * slot, (uint32_t)(st / S - 1) & 1u, T.wait_limit)) {
+                if (lane == 0) {
+                    *abort_flag = 1;
+                    atomicOr(T.err, 1ull);
+                }
                 break;
             }
-            prepare(st + 1, ns);
+            const uint32_t sBs = smem_u32(sB + slot * B_STAGE);
+            // element idx: row j = 8 jb + t8, 16-byte chunk c, slice i with t8
+            // fastest, so the 8 lanes of a wavefront fill one 128-byte core
+            // matrix (no bank conflicts); absent sources and slices shifted out
+            // are copied as zeros
+#pragma unroll
+            for (int q = 0; q < PER; q++) {
+                const int idx = tid + q * 32 * TC_GWARPS;
+                if (idx < NP) {
+                    const int t8 = idx & 7, c = (idx >> 3) % CH, jb = (idx / (8 * CH)) % (TN / 8),
+                              i = idx / (8 * CH * (TN / 8)), j = 8 * jb + t8;
+                    const int grp = sgrp[j * 8 + dd], si = i - sshift[j * 8 + dd];
+                    const bool has = grp >= 0 && si >= 0 && si < NS;
+                    const unsigned char *src = T.pre.slices + (has ? ((size_t)grp * NS + si) * KP * EB +
+                                                                         (size_t)kc * TC_KCB + c * 16
+                                                                   : 0);
+                    cp_async16(sBs + i * B_SLICE + (c * (TN / 8) + jb) * 128 + t8 * 16, src, has ? 16u : 0u);
+                }
+            }
+            asm volatile("cp.async.commit_group;" ::: "memory");
+            if (st >= 1) {  // stage st - 1 has landed: make it visible to the tensor core, arrive
+                asm volatile("cp.async.wait_group 1;" ::: "memory");
+                fence_proxy_async();
+                mbar_arrive(bfull0 + 8u * ((st - 1) % S));
+            }
+            gdone = st + 1;
+        }
+        // the last stage issued (also after an abort): every copy lands before going on
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        if (gdone >= 1) {
+            fence_proxy_async();
+            mbar_arrive(bfull0 + 8u * ((gdone - 1) % S));
         }
     }
-    // drain what is still in flight (on failure too: copies must land and MMAs
-    // finish before the block frees TMEM and leaves)
-    for (int sl = 0; sl < TC_SLOTS; sl++) {
-        while (ndone[sl] > 0)
-            if (!wait_slot(bdone, pdone, ndone, sl)) failed = true;
-        while (nfull[sl] > 0)
-            if (!wait_slot(bfull, pfull, nfull, sl)) failed = true;
-    }
+    // every thread: the MMAs are complete (or the block gave up) before TMEM is read or freed
+    mbar_wait(accbar, 0, kDrainWaitPolls);
     fence_after();
-
-    if (!failed) {
+    if (warp < TC_GWARPS && !*abort_flag) {
         const int row = warp * 32 + lane, r = mt * TC_M + row;
         const double sig = rsl[r];
 #pragma unroll 1
-        for (int cc = 0; cc < TC_N / 16; cc++) {
+        for (int cc = 0; cc < TN / 16; cc++) {
             double y[16];
 #pragma unroll
             for (int c = 0; c < 16; c++) y[c] = 0.0;
-#pragma unroll 1
-            for (int s = 0; s < TR::NACC; s++) {
-                uint32_t v[16];
-                tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * TC_N + cc * 16), v);
-                const double w = F == TC_INT8 ? ldexp(1.0, -7 * (s + 2))
-                               : F == TC_FP16 ? 1.0 / FP16_PRESCALE : 1.0;
+            if (nst > 0) {
+                uint32_t v[TR::NACC][16];
 #pragma unroll
-                for (int c = 0; c < 16; c++)
-                    y[c] += (F == TC_INT8 ? (double)(int32_t)v[c] : (double)__uint_as_float(v[c])) * w;
+                for (int s = 0; s < TR::NACC; s++)
+                    tmem_ld16_nowait(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * TN + cc * 16), v[s]);
+                tmem_wait_ld();
+#pragma unroll
+                for (int s = 0; s < TR::NACC; s++) {
+                    const double w = F == TC_INT8 ? ldexp(1.0, -7 * (s + 2)) : F == TC_FP16 ? 1.0 / FP16_PRESCALE : 1.0;
+#pragma unroll
+                    for (int c = 0; c < 16; c++)
+                        y[c] += (F == TC_INT8 ? (double)(int32_t)v[s][c] : (double)__uint_as_float(v[s][c])) * w;
+                }
             }
             if (r < Q4)
 #pragma unroll
                 for (int c = 0; c < 16; c++) {
                     const int j = cc * 16 + c;
                     if (sact[j]) {
-                        int64_t cg = A.T.off[lt1] + 4 * (e0 + j);
+                        const int64_t cg = A.T.off[lt1] + 4 * (e0 + j);
                         A.udown[(size_t)cg * Q + r] = y[c] * sig * stau[j];
                     }
                 }
@@ -476,11 +560,10 @@ __global__ void __launch_bounds__(TC_THREADS, 2) k_m2l_tc(TcArgs T) {
     }
     fence_before();
     __syncthreads();
-    if (warp == 0) {
+    if (warp == TC_GWARPS) {
         fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TR::NCOLS));
     }
-    if (failed && tid == 0) atomicOr(T.err, 1ull);
 }
 
 // ------------------------------------------------------------ host side
@@ -491,13 +574,6 @@ bool uses_tensor_m2l(const kifmm_plan *P) {
 
 static int form_of(int m2l) {
     return m2l == KIFMM_M2L_BF16X3 ? TC_BF16 : m2l == KIFMM_M2L_FP16X3 ? TC_FP16 : TC_INT8;
-}
-
-template <int F>
-static size_t tc_smem_bytes() {
-    using TR = TcTraits<F>;
-    return TC_SLOTS * (TR::NS * (size_t)TC_M * TC_KC * TR::EB + TR::NS * (size_t)TC_N * TC_KC * TR::EB) + 2 * TC_N * 9 * 4 +
-           8 + TC_N * 8 + TC_N * 4 + 8 + 32 + 8 + 1024;
 }
 
 template <int F>
@@ -537,8 +613,10 @@ static void run_m2l_tensor_t(kifmm_plan *P, const PassArgs &A) {
     pre.KP = g.KP;
     P->tc_pre.alloc((size_t)P->n_ent * TR::NS * g.KP * TR::EB);
     P->tc_gexp.alloc(P->n_ent);
+    P->tc_src8.alloc((size_t)8 * P->n_ent);
     pre.slices = P->tc_pre.p;
     pre.gexp = P->tc_gexp.p;
+    pre.src8 = P->tc_src8.p;
     launch_pdl(k_tc_preslice<F>, dim3(grid_for(P->n_ent * 32, 256)), dim3(256), 0, P->stream, A, P->n_ent, pre);
     TcArgs T{};
     T.A = A;
@@ -553,7 +631,7 @@ static void run_m2l_tensor_t(kifmm_plan *P, const PassArgs &A) {
     int64_t tiles = 0;
     for (int l = 0; l <= MAX_LEVELS; l++) {
         T.tile_off[l] = tiles;
-        if (l >= T.lmin && l <= T.lmax) tiles += (P->lt.ne[l] + TC_N - 1) / TC_N * g.MT;
+        if (l >= T.lmin && l <= T.lmax) tiles += (P->lt.ne[l] + TR::TN - 1) / TR::TN * g.MT;
     }
     if (!tiles) return;
     size_t smem = tc_smem_bytes<F>();

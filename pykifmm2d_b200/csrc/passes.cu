@@ -204,6 +204,153 @@ __global__ void k_m2l_d(PassArgs A, int l) {
             if (schild[t] >= 0) A.udown[(size_t)schild[t] * Q + r] = acc[t];
 }
 
+// M2L of every level in one launch on the FP64 tensor path (mma.sync
+// m8n8k4 .f64), class_fmm.py:336-343 recast target-centric:
+//   u_down(children of p) = sum_{d != centre} C_d . u_up(children of p + d),
+// C_d = CM2LS_d . blockdiag(Inv) (4Q x 4Q, column-major).  A block owns 32
+// consecutive split entries of one level (its target groups) and all 4Q rows:
+// D[4Q x 32] = sum over (direction, K chunk of 32) of C_d[:, chunk] .
+// B_d[chunk, 32], B_d's columns the targets' source groups in direction d
+// (a zero vector where a target has none).  Stages run through a ring of two
+// shared-memory buffers filled by bulk copies on an mbarrier each: the
+// operator chunk as 32 columns of 4Q doubles, the sources as 32 rows of 32
+// doubles; one thread issues a stage's copies as soon as the buffer is free,
+// so the copies of stage s + 1 land while stage s computes.  Warp w owns row
+// tiles w, w + 8, ... (8 rows each) for all 32 targets.  D is assigned to the
+// children's u_down (the L2L chain adds afterwards).  Needs Q even.
+constexpr int MD_THREADS = 256, MD_TE = 32, MD_KC = 32, MD_MT = 4;  // Q4 <= 8 warps x MD_MT x 8 rows
+struct M2lDmmaArgs {
+    PassArgs A;
+    const double *zero;                 // 4Q zeros
+    int lmin, lmax;
+    int64_t tile_off[MAX_LEVELS + 1];   // first block of each parent level
+    long long wait_limit;
+    unsigned long long *err;
+};
+static size_t m2l_dmma_smem(int Q4) {
+    const size_t ldo = pad4mod16(Q4), ldx = pad4mod16(MD_KC);
+    const size_t stage = (size_t)MD_KC * ldo + (size_t)MD_TE * ldx;
+    const size_t out = (size_t)MD_TE * (Q4 + 1);
+    return (2 * stage > out ? 2 * stage : out) * sizeof(double) + MD_TE * 8 * sizeof(int) + 64;
+}
+__global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
+    extern __shared__ __align__(128) double sm_md[];
+    const PassArgs &A = M.A;
+    const int Q = A.Q, Q4 = 4 * Q, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int ldo = pad4mod16(Q4), ldx = pad4mod16(MD_KC);
+    const size_t stage_d = (size_t)MD_KC * ldo + (size_t)MD_TE * ldx;
+    double *buf[2] = {sm_md, sm_md + stage_d};
+    int *ssrc = (int *)(sm_md + (2 * stage_d > (size_t)MD_TE * (Q4 + 1) ? 2 * stage_d : (size_t)MD_TE * (Q4 + 1)));
+    __shared__ __align__(8) uint64_t bars[2];
+    __shared__ int sact[MD_TE];
+    pdl_trigger();
+    const int64_t b = blockIdx.x;
+    int l = M.lmin;
+    while (l < M.lmax && M.tile_off[l + 1] <= b) l++;
+    const int64_t e0 = (b - M.tile_off[l]) * MD_TE, ne = A.T.ne[l], eoff = A.T.eoff[l];
+    const double *opl = A.ops + (size_t)(l + 1) * A.stride + A.off_m2l;  // target level's operators
+    pdl_wait();  // u_up comes from the M2M chain
+    if (tid < MD_TE) {
+        const int64_t e = e0 + tid;
+        const bool act = e < ne && !(A.ent[eoff + e] & 1);
+        const int p = act ? A.ent_node[eoff + e] : -1;
+        sact[tid] = act;
+        for (int dd = 0; dd < 8; dd++) {
+            const int d = dd < 4 ? dd : dd + 1;
+            ssrc[tid * 8 + dd] = act ? m2l_source_entry(A.ncoll, A.nent, A.nbot, A.ntop, p, d) : -1;
+        }
+    }
+    if (tid == 0) {
+        mbar_init(smem_u32(&bars[0]));
+        mbar_init(smem_u32(&bars[1]));
+    }
+    __syncthreads();
+    const int nkc = (Q4 + MD_KC - 1) / MD_KC, nst = 8 * nkc;
+    // one thread issues all copies of stage st into buffer st % 2
+    auto issue = [&](int st) {
+        const int dd = st / nkc, d = dd < 4 ? dd : dd + 1, kc = st % nkc, k0 = kc * MD_KC;
+        const int kn = min(MD_KC, Q4 - k0);
+        double *bs = buf[st & 1];
+        const uint32_t bar = smem_u32(&bars[st & 1]);
+        mbar_expect_tx(bar, (uint32_t)(kn * Q4 + MD_TE * kn) * 8u);
+        const double *op = opl + (size_t)d * Q4 * Q4 + (size_t)k0 * Q4;
+        for (int c = 0; c < kn; c++) bulk_g2s(smem_u32(bs + (size_t)c * ldo), op + (size_t)c * Q4, (uint32_t)Q4 * 8u, bar);
+        double *xs = bs + (size_t)MD_KC * ldo;
+        for (int n = 0; n < MD_TE; n++) {
+            const int je = ssrc[n * 8 + dd];
+            const double *src = je >= 0 ? A.uup + (size_t)(A.T.off[l + 1] + 4 * (je - eoff)) * Q + k0 : M.zero + k0;
+            bulk_g2s(smem_u32(xs + (size_t)n * ldx), src, (uint32_t)kn * 8u, bar);
+        }
+    };
+    if (tid == 0) {
+        issue(0);
+        if (nst > 1) issue(1);
+    }
+    const int g = lane >> 2, t = lane & 3, nrt = Q4 / 8;
+    double acc[MD_MT][4][2];
+#pragma unroll
+    for (int i = 0; i < MD_MT; i++)
+#pragma unroll
+        for (int c = 0; c < 4; c++) acc[i][c][0] = acc[i][c][1] = 0.0;
+    uint32_t par[2] = {0u, 0u};
+    bool ok = true;
+    int landed = 0;  // stages waited for (issued stages: min(nst, landed + 2))
+    for (int st = 0; st < nst; st++) {
+        const int bi = st & 1;
+        ok = __syncthreads_and(mbar_wait(smem_u32(&bars[bi]), par[bi], M.wait_limit));
+        if (!ok) break;
+        par[bi] ^= 1u;
+        landed++;
+        const int kn = min(MD_KC, Q4 - (st % nkc) * MD_KC);
+        const double *os = buf[bi], *xs = buf[bi] + (size_t)MD_KC * ldo;
+        for (int k0 = 0; k0 < kn; k0 += 4) {
+            double bv[4];
+#pragma unroll
+            for (int c = 0; c < 4; c++) bv[c] = xs[(size_t)(8 * c + g) * ldx + k0 + t];
+#pragma unroll
+            for (int i = 0; i < MD_MT; i++) {
+                const int rt = warp + 8 * i;
+                if (rt < nrt) {
+                    const double av = os[(size_t)(k0 + t) * ldo + 8 * rt + g];
+#pragma unroll
+                    for (int c = 0; c < 4; c++) dmma_8x8x4(acc[i][c][0], acc[i][c][1], av, bv[c]);
+                }
+            }
+        }
+        __syncthreads();  // buffer bi is free
+        if (tid == 0 && st + 2 < nst) issue(st + 2);
+    }
+    if (!ok) {
+        if (tid == 0) atomicOr(M.err, 1ull);
+        // let every issued copy land before the block leaves
+        const int issued = min(nst, landed + 2);
+        for (int st = landed; st < issued; st++) {
+            mbar_wait(smem_u32(&bars[st & 1]), par[st & 1], kDrainWaitPolls);
+            par[st & 1] ^= 1u;
+        }
+        return;
+    }
+    // D through shared memory (the stage buffers are free), then coalesced stores
+    double *cs = sm_md;  // [32 targets][Q4 + 1]
+#pragma unroll
+    for (int i = 0; i < MD_MT; i++) {
+        const int rt = warp + 8 * i;
+        if (rt < nrt)
+#pragma unroll
+            for (int c = 0; c < 4; c++) {
+                cs[(size_t)(8 * c + 2 * t) * (Q4 + 1) + 8 * rt + g] = acc[i][c][0];
+                cs[(size_t)(8 * c + 2 * t + 1) * (Q4 + 1) + 8 * rt + g] = acc[i][c][1];
+            }
+    }
+    __syncthreads();
+    const size_t child0 = (size_t)A.T.off[l + 1] + 4 * (size_t)e0;
+    for (int n = warp; n < MD_TE; n += MD_THREADS / 32) {
+        if (!sact[n]) continue;
+        double *dst = A.udown + (child0 + 4 * (size_t)n) * Q;
+        for (int r = lane; r < Q4; r += 32) dst[r] = cs[(size_t)n * (Q4 + 1) + r];
+    }
+}
+
 // L2P + P2P for one target leaf per block (class_fmm.py:73-111).
 __global__ void k_leaf_eval_d(PassArgs A, const int32_t *__restrict__ list, int check_self) {
     extern __shared__ double sm[];
@@ -786,6 +933,37 @@ void run_upward_downward(kifmm_plan *P) {
         PhaseScope ph_m2m(P, KIFMM_PHASE_M2M);
         for (int l = L - 2; l >= 2; l--)
             if (P->lt.ne[l]) launch_m2m_d(P, A, l);
+    }
+    if (Q % 2 == 0 && 4 * Q <= 8 * MD_MT * 8) {
+        // FP64 tensor path: all levels' M2L in one launch, then the L2L chain
+        M2lDmmaArgs M{};
+        M.A = A;
+        if (!P->zero4q.p) {
+            P->zero4q.alloc((size_t)4 * Q);
+            KIFMM_CUDA(cudaMemsetAsync(P->zero4q.p, 0, (size_t)4 * Q * sizeof(double), s));
+        }
+        M.zero = P->zero4q.p;
+        M.lmin = 1;
+        M.lmax = L - 2;
+        M.wait_limit = plan_wait_polls(P);
+        M.err = P->scal.p + KIFMM_SCAL_PASS_ERR;
+        int64_t tiles = 0;
+        for (int l = 0; l <= MAX_LEVELS; l++) {
+            M.tile_off[l] = tiles;
+            if (l >= M.lmin && l <= M.lmax) tiles += (P->lt.ne[l] + MD_TE - 1) / MD_TE;
+        }
+        {
+            PhaseScope ph(P, KIFMM_PHASE_M2L);
+            if (tiles) {
+                const size_t smem = m2l_dmma_smem(4 * Q);
+                ensure_dyn_smem(k_m2l_dmma, smem);
+                launch_pdl(k_m2l_dmma, dim3((unsigned)tiles), dim3(MD_THREADS), smem, s, M);
+            }
+        }
+        PhaseScope ph(P, KIFMM_PHASE_L2L);
+        for (int l = 2; l <= L - 2; l++)
+            if (P->lt.ne[l]) launch_l2l_d(P, A, l);
+        return;
     }
     PhaseScope ph(P, KIFMM_PHASE_M2L);
     int thr = ((4 * Q + 31) / 32) * 32;
