@@ -44,14 +44,20 @@ enum { KIFMM_MEM_HOST = 0, KIFMM_MEM_DEVICE = 1 };
 typedef struct kifmm_plan kifmm_plan;
 
 /* Kernel plug-ins.  The reference takes a numba scalar function
- * Kernel_Eval(sx, sy, tx, ty) (class_fmm.py:55, :115); the two it ships and
- * benchmarks are the Laplace log kernel (examples/laplace2.py:31-36) and the
- * modified Helmholtz kernel K0(k r)/(2 pi) (examples/modified_helmholtz.py:38-43). */
-enum { KIFMM_KERNEL_LAPLACE = 0, KIFMM_KERNEL_MOD_HELMHOLTZ = 1 };
+ * Kernel_Eval(sx, sy, tx, ty) (class_fmm.py:55, :115); the ones it ships and
+ * benchmarks are the Laplace log kernel (examples/laplace2.py:31-36), the
+ * modified Helmholtz kernel K0(k r)/(2 pi) (examples/modified_helmholtz.py:38-43)
+ * and, with FMM(..., iscomplex=True) (class_fmm.py:174), the Helmholtz kernel
+ * (i/4) H0^(1)(k r) (examples/hankel.py:37-39).
+ * Complex kernel: every density, potential and kernel value the ABI passes is
+ * complex, stored as interleaved (real, imaginary) doubles (C99 double
+ * complex / numpy complex128 layout), so a buffer of n values holds 2n
+ * doubles; the plan needs KIFMM_PREC_FP64 and Nequiv <= 32. */
+enum { KIFMM_KERNEL_LAPLACE = 0, KIFMM_KERNEL_MOD_HELMHOLTZ = 1, KIFMM_KERNEL_HELMHOLTZ = 2 };
 typedef struct kifmm_kernel {
     int32_t kind;     /* KIFMM_KERNEL_* */
     int32_t reserved;
-    double k;         /* modified Helmholtz parameter (unused for Laplace) */
+    double k;         /* wavenumber of the (modified) Helmholtz kernels (unused for Laplace) */
 } kifmm_kernel;
 
 /* Arithmetic of the evaluation passes. */
@@ -84,7 +90,9 @@ typedef struct kifmm_options {
     void *stream;       /* cudaStream_t to order work on (cudaStreamLegacy, i.e. 0x1, for the
                            legacy default stream); NULL: the plan creates its own stream */
     int32_t e2c;        /* how the check-to-equivalent inverse is formed: KIFMM_E2C_* */
-    int32_t reserved;
+    int32_t iscomplex;  /* FMM(..., iscomplex=True) (class_fmm.py:174): 1 makes densities and
+                           potentials complex (interleaved doubles) for any kernel; the
+                           Helmholtz kernel sets it by itself.  0 (default): real values */
 } kifmm_options;
 
 /* Check-to-equivalent solve.  The reference LU-factors the Q x Q E2C matrix

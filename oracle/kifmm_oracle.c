@@ -17,7 +17,13 @@
  * The modified-Helmholtz K0 used here is computed independently of any
  * table: the power series of K0 for x < 2 and the trapezoidal rule on the
  * integral K0(x) = int_0^inf exp(-x cosh t) dt (DLMF 10.32.9) for x >= 2.
+ * The complex mode (the reference's FMM(..., iscomplex=True)) runs the same
+ * FMM on complex values (kifmm_oracle_fmm.inc, entry points orkc_*), with
+ * the Helmholtz kernel (i/4) H0(k r) = (i/4) (J0(k r) + i Y0(k r)) from the C
+ * library's Bessel functions.
  */
+#define _DEFAULT_SOURCE  /* j0, y0 (POSIX Bessel functions) */
+#include <complex.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -535,302 +541,42 @@ void ork_locate(const OTree *t, const double *x, const double *y, int64_t n, int
     }
 }
 
-/* ---------------------------------------------------------------- dense LA */
-/* LU with partial pivoting (the getrf step of scipy.linalg.lu_factor) */
-static void lu_factor(double *a, int n, int *piv)
+/* ------------------------------------------------- the FMM, real and complex */
+/* Helmholtz G(s -> t) = (i/4) H0^(1)(k |t - s|) (examples/hankel.py:37-39);
+ * the real kernels promoted to complex values otherwise. */
+#define ORK_KERNEL_HELMHOLTZ 2
+static inline double complex orkc_eval(OKern kn, double sx, double sy, double tx, double ty)
 {
-    for (int k = 0; k < n; k++) {
-        int p = k;
-        double mx = fabs(a[k * n + k]);
-        for (int i = k + 1; i < n; i++) if (fabs(a[i * n + k]) > mx) { mx = fabs(a[i * n + k]); p = i; }
-        piv[k] = p;
-        if (p != k) for (int j = 0; j < n; j++) { double tmp = a[k * n + j]; a[k * n + j] = a[p * n + j]; a[p * n + j] = tmp; }
-        double d = a[k * n + k];
-        for (int i = k + 1; i < n; i++) {
-            double f = a[i * n + k] / d;
-            a[i * n + k] = f;
-            for (int j = k + 1; j < n; j++) a[i * n + j] -= f * a[k * n + j];
-        }
+    if (kn.kind == ORK_KERNEL_HELMHOLTZ) {
+        double dx = tx - sx, dy = ty - sy, z = kn.k * sqrt(dx * dx + dy * dy);
+        return 0.25 * I * (j0(z) + I * y0(z));
     }
+    return ork_eval(kn, sx, sy, tx, ty);
 }
 
-/* getrs for one right-hand side, in place */
-static void lu_solve(const double *lu, const int *piv, int n, double *b)
-{
-    for (int k = 0; k < n; k++) if (piv[k] != k) { double tmp = b[k]; b[k] = b[piv[k]]; b[piv[k]] = tmp; }
-    for (int i = 0; i < n; i++) { double s = b[i]; for (int j = 0; j < i; j++) s -= lu[i * n + j] * b[j]; b[i] = s; }
-    for (int i = n - 1; i >= 0; i--) { double s = b[i]; for (int j = i + 1; j < n; j++) s -= lu[i * n + j] * b[j]; b[i] = s / lu[i * n + i]; }
-}
+#define OV double
+#define OP(name) ork_##name
+#define OABS(v) fabs(v)
+#define OEVAL ork_eval
+#define OFMM_T ork_fmm_t
+#include "kifmm_oracle_fmm.inc"
+#undef OV
+#undef OP
+#undef OABS
+#undef OEVAL
+#undef OFMM_T
 
-/* ----------------------------------------------------------------- the FMM */
-typedef struct {
-    OTree *t;
-    OKern kn;
-    int Q;                   /* Nequiv */
-    double *sx[ORK_MAXLEV], *sy[ORK_MAXLEV], *lx[ORK_MAXLEV], *ly[ORK_MAXLEV];
-    double *e2c[ORK_MAXLEV]; int *piv[ORK_MAXLEV];
-    double *m2mc[ORK_MAXLEV];            /* Q x 4Q */
-    double *cm2l[ORK_MAXLEV];            /* 9 blocks of 4Q x 4Q (centre unused) */
-    double *chk[ORK_MAXLEV], *eqd[ORK_MAXLEV], *ls[ORK_MAXLEV], *le[ORK_MAXLEV];
-    double *tau_o;
-} OFMM;
-
-/* out[j, i] = G(s_i -> t_j)  (Get_Kernel_Functions.KF, class_fmm.py:116-122) */
-static void kf(OKern kn, const double *sx, const double *sy, int ns, const double *tx, const double *ty, int nt, double *out)
-{
-    for (int j = 0; j < nt; j++)
-        for (int i = 0; i < ns; i++) out[j * ns + i] = ork_eval(kn, sx[i], sy[i], tx[j], ty[j]);
-}
-
-void ork_fmm_free(OFMM *f)
-{
-    if (!f) return;
-    for (int l = 0; l < ORK_MAXLEV; l++) {
-        free(f->sx[l]); free(f->sy[l]); free(f->lx[l]); free(f->ly[l]);
-        free(f->e2c[l]); free(f->piv[l]); free(f->m2mc[l]); free(f->cm2l[l]);
-        free(f->chk[l]); free(f->eqd[l]); free(f->ls[l]); free(f->le[l]);
-    }
-    free(f->tau_o);
-    free(f);
-}
-
-/* FMM.precompute (class_fmm.py:182-298) */
-int ork_fmm_create(OTree *t, int kind, double k, int Q, OFMM **out)
-{
-    if (Q <= 0 || Q > 256) return 1;
-    OFMM *f = calloc(1, sizeof(OFMM));
-    f->t = t; f->kn.kind = kind; f->kn.k = k; f->Q = Q;
-    int L = t->L;
-    double dd = 0.01;
-    for (int l = 0; l < L; l++) {
-        double w = t->lv[l].width;
-        double r1 = 0.5 * w * (sqrt(2.0) + dd), r2 = 0.5 * w * (4.0 - sqrt(2.0) - 2 * dd);
-        f->sx[l] = malloc(Q * sizeof(double)); f->sy[l] = malloc(Q * sizeof(double));
-        f->lx[l] = malloc(Q * sizeof(double)); f->ly[l] = malloc(Q * sizeof(double));
-        double step = 2.0 * M_PI / Q;
-        for (int q = 0; q < Q; q++) {
-            double th = q * step;
-            f->sx[l][q] = r1 * cos(th); f->sy[l][q] = r1 * sin(th);
-            f->lx[l][q] = r2 * cos(th); f->ly[l][q] = r2 * sin(th);
-        }
-        f->e2c[l] = malloc((size_t)Q * Q * sizeof(double));
-        f->piv[l] = malloc(Q * sizeof(int));
-        kf(f->kn, f->sx[l], f->sy[l], Q, f->lx[l], f->ly[l], Q, f->e2c[l]);
-        lu_factor(f->e2c[l], Q, f->piv[l]);
-    }
-    double *cx = malloc(4 * Q * sizeof(double)), *cy = malloc(4 * Q * sizeof(double));
-    for (int l = 0; l + 1 < L; l++) {
-        double hw = 0.5 * t->lv[l + 1].width;
-        for (int q = 0; q < Q; q++) {
-            cx[q] = f->sx[l + 1][q] - hw;         cy[q] = f->sy[l + 1][q] - hw;
-            cx[Q + q] = f->sx[l + 1][q] - hw;     cy[Q + q] = f->sy[l + 1][q] + hw;
-            cx[2 * Q + q] = f->sx[l + 1][q] + hw; cy[2 * Q + q] = f->sy[l + 1][q] - hw;
-            cx[3 * Q + q] = f->sx[l + 1][q] + hw; cy[3 * Q + q] = f->sy[l + 1][q] + hw;
-        }
-        f->m2mc[l] = malloc((size_t)Q * 4 * Q * sizeof(double));
-        kf(f->kn, cx, cy, 4 * Q, f->lx[l], f->ly[l], Q, f->m2mc[l]);
-    }
-    free(cx); free(cy);
-    double *m2l = malloc((size_t)49 * Q * Q * sizeof(double));
-    double *shx = malloc(Q * sizeof(double)), *shy = malloc(Q * sizeof(double));
-    for (int l = 1; l < L; l++) {
-        double w = t->lv[l].width;
-        for (int ix = 0; ix < 7; ix++)
-            for (int iy = 0; iy < 7; iy++) {
-                if (ix >= 2 && ix <= 4 && iy >= 2 && iy <= 4) continue;
-                for (int q = 0; q < Q; q++) { shx[q] = f->sx[l][q] + (ix - 3) * w; shy[q] = f->sy[l][q] + (iy - 3) * w; }
-                kf(f->kn, shx, shy, Q, f->sx[l], f->sy[l], Q, m2l + (size_t)(ix * 7 + iy) * Q * Q);
-            }
-        int Q4 = 4 * Q;
-        f->cm2l[l] = calloc((size_t)9 * Q4 * Q4, sizeof(double));
-        for (int kx = 0; kx < 3; kx++)
-            for (int ky = 0; ky < 3; ky++) {
-                if (kx == 1 && ky == 1) continue;
-                double *C = f->cm2l[l] + (size_t)(kx * 3 + ky) * Q4 * Q4;
-                for (int ii = 0; ii < 2; ii++)
-                    for (int jj = 0; jj < 2; jj++) {
-                        int shx0 = 2 * (kx - 1) - ii + 3, shy0 = 2 * (ky - 1) - jj + 3, base = 2 * ii + jj;
-                        for (int iii = 0; iii < 2; iii++)
-                            for (int jjj = 0; jjj < 2; jjj++) {
-                                int fx = shx0 + iii, fy = shy0 + jjj, bb = 2 * iii + jjj;
-                                int near = fx >= 2 && fx <= 4 && fy >= 2 && fy <= 4;
-                                for (int a = 0; a < Q; a++)
-                                    for (int c = 0; c < Q; c++)
-                                        C[(size_t)(base * Q + a) * Q4 + bb * Q + c] =
-                                            near ? 0.0 : m2l[(size_t)(fx * 7 + fy) * Q * Q + a * Q + c];
-                            }
-                    }
-            }
-    }
-    free(m2l); free(shx); free(shy);
-    for (int l = 1; l < L; l++) {
-        OLevel *v = &t->lv[l];
-        f->chk[l] = calloc((size_t)(v->n_alloc ? v->n_alloc : 1) * Q, sizeof(double));
-        f->eqd[l] = calloc((size_t)(v->n_alloc ? v->n_alloc : 1) * Q, sizeof(double));
-        f->ls[l] = calloc((size_t)(v->n ? v->n : 1) * Q, sizeof(double));
-        f->le[l] = calloc((size_t)(v->n ? v->n : 1) * Q, sizeof(double));
-    }
-    f->tau_o = malloc(t->N * sizeof(double));
-    *out = f;
-    return 0;
-}
-
-/* FMM.build_expansions (class_fmm.py:299-352), on freshly zeroed workspaces */
-int ork_fmm_apply(OFMM *f, const double *tau)
-{
-    OTree *t = f->t;
-    int L = t->L, Q = f->Q, Q4 = 4 * Q;
-    for (int64_t i = 0; i < t->N; i++) f->tau_o[i] = tau[t->ordv[i]];
-    for (int l = 1; l < L; l++) {
-        memset(f->chk[l], 0, (size_t)t->lv[l].n_alloc * Q * sizeof(double));
-        memset(f->ls[l], 0, (size_t)t->lv[l].n * Q * sizeof(double));
-    }
-    /* upward pass */
-    for (int l = L - 1; l >= 1; l--) {
-        OLevel *v = &t->lv[l];
-        double *ucs = f->chk[l];
-        if (l != L - 1) {
-            OLevel *a = &t->lv[l + 1];
-            const double *M = f->m2mc[l];
-            /* temp1 = (M2MC @ RSEQD.T).T, then numba_distribute (:11-15) */
-#pragma omp parallel for
-            for (int64_t g = 0; g < a->n / 4; g++) {
-                int64_t di = a->pdi[g];
-                if (di < 0) continue;
-                const double *rs = f->eqd[l + 1] + (size_t)di * Q4;
-                double *dst = ucs + (size_t)v->tdi[a->parent[4 * g]] * Q;
-                for (int r = 0; r < Q; r++) {
-                    double s = 0;
-                    for (int c = 0; c < Q4; c++) s += M[r * Q4 + c] * rs[c];
-                    dst[r] = s;
-                }
-            }
-        }
-        /* numba_upwards_pass (class_fmm.py:57-71) */
-#pragma omp parallel for schedule(dynamic, 8)
-        for (int64_t i = 0; i < v->n; i++) {
-            if (!v->cu[i] || v->tdi[i] < 0) continue;
-            double *u = ucs + (size_t)v->tdi[i] * Q;
-            for (int64_t s = v->bot[i]; s < v->top[i]; s++)
-                for (int q = 0; q < Q; q++)
-                    u[q] += ork_eval(f->kn, t->x[s], t->y[s], f->lx[l][q] + v->xmid[i], f->ly[l][q] + v->ymid[i]) * f->tau_o[s];
-        }
-#pragma omp parallel for
-        for (int64_t i = 0; i < v->n_alloc; i++) {
-            memcpy(f->eqd[l] + (size_t)i * Q, ucs + (size_t)i * Q, Q * sizeof(double));
-            lu_solve(f->e2c[l], f->piv[l], Q, f->eqd[l] + (size_t)i * Q);
-        }
-    }
-    /* downward pass 1 */
-    for (int l = 1; l < L - 1; l++) {
-        OLevel *v = &t->lv[l], *d = &t->lv[l + 1];
-        const double *M = f->m2mc[l];
-#pragma omp parallel for
-        for (int64_t i = 0; i < v->n; i++) {
-            int doit = (!v->leaf[i] || v->xlist[i]) && !v->fake[i];
-            if (!doit) continue;
-            double le[256], o;
-            memcpy(le, f->ls[l] + (size_t)i * Q, Q * sizeof(double));
-            lu_solve(f->e2c[l], f->piv[l], Q, le);
-            for (int c = 0; c < Q4; c++) {
-                o = 0;
-                for (int r = 0; r < Q; r++) o += M[r * Q4 + c] * le[r];
-                f->ls[l + 1][(size_t)v->children[i] * Q + c] = o;
-            }
-        }
-        /* M2Ms[d] = CM2L[l+1][d] @ RSEQD.T (class_fmm.py:336-341) */
-        int64_t G = d->n_sib;
-        double *M2Ms = malloc((size_t)9 * Q4 * (G ? G : 1) * sizeof(double));
-        const double *CM = f->cm2l[l + 1];
-#pragma omp parallel for collapse(2)
-        for (int dir = 0; dir < 9; dir++)
-            for (int64_t g = 0; g < G; g++) {
-                if (dir == 4) continue;
-                const double *C = CM + (size_t)dir * Q4 * Q4;
-                const double *rs = f->eqd[l + 1] + (size_t)g * Q4;
-                double *o = M2Ms + ((size_t)dir * G + g) * Q4;
-                for (int r = 0; r < Q4; r++) {
-                    double s = 0;
-                    for (int c = 0; c < Q4; c++) s += C[(size_t)r * Q4 + c] * rs[c];
-                    o[r] = s;
-                }
-            }
-        /* numba_add_interactions (class_fmm.py:17-33); ci4 = trunc(children/4) */
-#pragma omp parallel for
-        for (int64_t i = 0; i < v->n; i++) {
-            int doit = (!v->leaf[i] || v->xlist[i]) && !v->fake[i];
-            if (!doit) continue;
-            int64_t dii = v->children[i] / 4;
-            for (int j = 0; j < 9; j++) {
-                int64_t ci = v->coll[9 * i + j];
-                if (ci < 0 || ci == i) continue;
-                int xd = isgn(v->xmid[ci] - v->xmid[i]), yd = isgn(v->ymid[ci] - v->ymid[i]);
-                int64_t di = d->pdi[v->children[ci] / 4];
-                if (di < 0) continue;
-                const double *src = M2Ms + ((size_t)((xd + 1) * 3 + (yd + 1)) * G + di) * Q4;
-                for (int k = 0; k < 4; k++)
-                    for (int q = 0; q < Q; q++) f->ls[l + 1][(size_t)(4 * dii + k) * Q + q] += src[k * Q + q];
-            }
-        }
-        free(M2Ms);
-    }
-    /* downward pass 2a */
-    for (int l = 1; l < L; l++) {
-        OLevel *v = &t->lv[l];
-#pragma omp parallel for
-        for (int64_t i = 0; i < v->n; i++) {
-            memcpy(f->le[l] + (size_t)i * Q, f->ls[l] + (size_t)i * Q, Q * sizeof(double));
-            lu_solve(f->e2c[l], f->piv[l], Q, f->le[l] + (size_t)i * Q);
-        }
-    }
-    return 0;
-}
-
-/* FMM.evaluate_to_points (class_fmm.py:379-399): L2P (:73-88) then P2P (:90-111) */
-int ork_fmm_eval(const OFMM *f, const double *x, const double *y, int64_t n, int check, double *pot)
-{
-    const OTree *t = f->t;
-    int Q = f->Q;
-#pragma omp parallel for schedule(dynamic, 64)
-    for (int64_t p = 0; p < n; p++) {
-        int l; int64_t i;
-        double px = x[p], py = y[p];
-        locate1(t, px, py, &l, &i);
-        const OLevel *v = &t->lv[l];
-        double acc = 0.0;
-        if (l > 0) {
-            double tx = px - v->xmid[i], ty = py - v->ymid[i];
-            const double *e = f->le[l] + (size_t)i * Q;
-            for (int q = 0; q < Q; q++) acc += ork_eval(f->kn, f->lx[l][q], f->ly[l][q], tx, ty) * e[q];
-        }
-        for (int j = 0; j < 9; j++) {
-            int64_t ci = v->coll[9 * i + j];
-            if (ci < 0) continue;
-            for (int64_t s = v->bot[ci]; s < v->top[ci]; s++) {
-                if (check && px - t->x[s] == 0 && py - t->y[s] == 0) continue;
-                acc += ork_eval(f->kn, t->x[s], t->y[s], px, py) * f->tau_o[s];
-            }
-        }
-        pot[p] = acc;
-    }
-    return 0;
-}
-
-/* The reference's KAS (class_fmm.py:134-143) for selected targets: FP64
- * direct sum over all sources, skipping only the pair i == j. */
-void ork_direct(int kind, double k, const double *x, const double *y, const double *tau, int64_t n,
-                const int64_t *tgt, int64_t nt, double *out)
-{
-    OKern kn = {kind, k};
-#pragma omp parallel for schedule(dynamic, 4)
-    for (int64_t a = 0; a < nt; a++) {
-        int64_t j = tgt[a];
-        double s = 0.0;
-        for (int64_t i = 0; i < n; i++)
-            if (i != j) s += ork_eval(kn, x[i], y[i], x[j], y[j]) * tau[i];
-        out[a] = s;
-    }
-}
+#define OV double complex
+#define OP(name) orkc_##name
+#define OABS(v) cabs(v)
+#define OEVAL orkc_eval
+#define OFMM_T orkc_fmm_t
+#include "kifmm_oracle_fmm.inc"
+#undef OV
+#undef OP
+#undef OABS
+#undef OEVAL
+#undef OFMM_T
 
 double ork_k0_value(double x) { return ork_k0(x); }
 void ork_set_threads(int n) { if (n > 0) omp_set_num_threads(n); }

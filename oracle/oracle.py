@@ -31,8 +31,8 @@ def build():
 def lib():
     global _lib
     if _lib is None:
-        src = os.path.join(_HERE, "kifmm_oracle.c")
-        if not os.path.exists(_LIB) or os.path.getmtime(_LIB) < os.path.getmtime(src):
+        srcs = [os.path.join(_HERE, f) for f in ("kifmm_oracle.c", "kifmm_oracle_fmm.inc")]
+        if not os.path.exists(_LIB) or any(os.path.getmtime(_LIB) < os.path.getmtime(f) for f in srcs):
             build()
         L = ctypes.CDLL(_LIB)
         L.ork_tree_build.argtypes = [_d, _d, ctypes.c_int64, ctypes.c_int64, ctypes.c_int, ctypes.POINTER(_vp)]
@@ -49,12 +49,15 @@ def lib():
         L.ork_p2p_pairs.argtypes = [_vp, _i64]
         L.ork_p2p_pairs.restype = ctypes.c_int64
         L.ork_tree_free.argtypes = [_vp]
-        L.ork_fmm_create.argtypes = [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(_vp)]
-        L.ork_fmm_create.restype = ctypes.c_int
-        L.ork_fmm_apply.argtypes = [_vp, _d]
-        L.ork_fmm_eval.argtypes = [_vp, _d, _d, ctypes.c_int64, ctypes.c_int, _d]
-        L.ork_fmm_free.argtypes = [_vp]
-        L.ork_direct.argtypes = [ctypes.c_int, ctypes.c_double, _d, _d, _d, ctypes.c_int64, _i64, ctypes.c_int64, _d]
+        for pre in ("ork", "orkc"):  # real and complex values (complex: pointers to complex128)
+            getattr(L, pre + "_fmm_create").argtypes = [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                                         ctypes.POINTER(_vp)]
+            getattr(L, pre + "_fmm_create").restype = ctypes.c_int
+            getattr(L, pre + "_fmm_apply").argtypes = [_vp, _vp]
+            getattr(L, pre + "_fmm_eval").argtypes = [_vp, _d, _d, ctypes.c_int64, ctypes.c_int, _vp]
+            getattr(L, pre + "_fmm_free").argtypes = [_vp]
+            getattr(L, pre + "_direct").argtypes = [ctypes.c_int, ctypes.c_double, _d, _d, _vp, ctypes.c_int64,
+                                                    _i64, ctypes.c_int64, _vp]
         L.ork_k0_value.argtypes = [ctypes.c_double]
         L.ork_k0_value.restype = ctypes.c_double
         L.ork_set_threads.argtypes = [ctypes.c_int]
@@ -144,41 +147,51 @@ class OracleTree:
 
 KERNEL_LAPLACE = 0
 KERNEL_K0 = 1
+KERNEL_HELMHOLTZ = 2  # (i/4) H0(k r), complex
 
 
 class OracleFMM:
-    """Mirror of the reference's FMM (class_fmm.py:166-402) on the C oracle."""
+    """Mirror of the reference's FMM (class_fmm.py:166-402) on the C oracle.
+    iscomplex (class_fmm.py:174) runs it on complex values, as the Helmholtz
+    kernel requires."""
 
-    def __init__(self, x, y, kernel=KERNEL_LAPLACE, k=0.0, Nequiv=48, Ncutoff=50, fix_bbox=False):
+    def __init__(self, x, y, kernel=KERNEL_LAPLACE, k=0.0, Nequiv=48, Ncutoff=50, fix_bbox=False, iscomplex=False):
         self.tree = OracleTree(x, y, Ncutoff, fix_bbox)
+        self.iscomplex = bool(iscomplex) or kernel == KERNEL_HELMHOLTZ
+        self.dtype = np.complex128 if self.iscomplex else np.float64
+        self._pre = "orkc" if self.iscomplex else "ork"
         h = _vp()
-        rc = lib().ork_fmm_create(self.tree.h, int(kernel), float(k), int(Nequiv), ctypes.byref(h))
+        rc = getattr(lib(), self._pre + "_fmm_create")(self.tree.h, int(kernel), float(k), int(Nequiv),
+                                                       ctypes.byref(h))
         if rc:
             raise ValueError(f"oracle precompute failed (code {rc})")
         self.h = h
 
     def build_expansions(self, tau):
-        self.tau = _f64(tau)
-        lib().ork_fmm_apply(self.h, _p(self.tau))
+        self.tau = np.ascontiguousarray(tau, dtype=self.dtype)
+        getattr(lib(), self._pre + "_fmm_apply")(self.h, self.tau.ctypes.data)
 
     def evaluate_to_points(self, x, y, check_self=False):
         x = _f64(x)
         y = _f64(y)
-        pot = np.zeros(x.size)
-        lib().ork_fmm_eval(self.h, _p(x), _p(y), x.size, int(bool(check_self)), _p(pot))
+        pot = np.zeros(x.size, dtype=self.dtype)
+        getattr(lib(), self._pre + "_fmm_eval")(self.h, _p(x), _p(y), x.size, int(bool(check_self)), pot.ctypes.data)
         return pot
 
     def __del__(self):
         if getattr(self, "h", None):
-            lib().ork_fmm_free(self.h)
+            getattr(lib(), self._pre + "_fmm_free")(self.h)
             self.h = None
 
 
 def direct(x, y, tau, targets, kernel=KERNEL_LAPLACE, k=0.0):
     """FP64 direct sum at selected targets, skipping only i == j (the KAS of
-    class_fmm.py:134-143)."""
-    x, y, tau = _f64(x), _f64(y), _f64(tau)
+    class_fmm.py:134-143); complex for complex charges or the Helmholtz kernel."""
+    x, y = _f64(x), _f64(y)
+    cplx = np.iscomplexobj(tau) or kernel == KERNEL_HELMHOLTZ
+    tau = np.ascontiguousarray(tau, dtype=np.complex128 if cplx else np.float64)
     t = np.ascontiguousarray(targets, dtype=np.int64)
-    out = np.zeros(t.size)
-    lib().ork_direct(int(kernel), float(k), _p(x), _p(y), _p(tau), x.size, _p(t, _i64), t.size, _p(out))
+    out = np.zeros(t.size, dtype=tau.dtype)
+    getattr(lib(), "orkc_direct" if cplx else "ork_direct")(int(kernel), float(k), _p(x), _p(y), tau.ctypes.data,
+                                                            x.size, _p(t, _i64), t.size, out.ctypes.data)
     return out

@@ -12,8 +12,8 @@ The work runs in libkifmm2d.so (hand-written sm_100a CUDA, C ABI in
 include/kifmm2d.h); this package is the Python host layer.
 """
 from . import class_fmm
-from .class_fmm import (FMM, Get_Kernel_Functions, Kernel_Form, LaplaceKernel, ModifiedHelmholtzKernel,
-                        get_level_information, prepare_numba_functions_on_the_fly)
+from .class_fmm import (FMM, Get_Kernel_Functions, HelmholtzKernel, Kernel_Form, LaplaceKernel,
+                        ModifiedHelmholtzKernel, get_level_information, prepare_numba_functions_on_the_fly)
 
 __all__ = ["FMM", "Get_Kernel_Functions", "Kernel_Form", "LaplaceKernel", "ModifiedHelmholtzKernel",
-           "get_level_information", "prepare_numba_functions_on_the_fly", "class_fmm"]
+           "HelmholtzKernel", "get_level_information", "prepare_numba_functions_on_the_fly", "class_fmm"]

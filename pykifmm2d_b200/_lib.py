@@ -13,7 +13,7 @@ LIB_PATH = os.path.join(_HERE, "libkifmm2d.so")
 OK = 0
 ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_DEPTH, ERR_STATE, ERR_RANGE, ERR_UNSUPPORTED = 1, 2, 3, 4, 5, 6, 7
 MEM_HOST, MEM_DEVICE = 0, 1
-KERNEL_LAPLACE, KERNEL_MOD_HELMHOLTZ = 0, 1
+KERNEL_LAPLACE, KERNEL_MOD_HELMHOLTZ, KERNEL_HELMHOLTZ = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 E2C_DENSE, E2C_CIRCULANT = 0, 1
 M2L_AUTO, M2L_FP32, M2L_BF16X3, M2L_FP16X3, M2L_FP64, M2L_INT8 = 0, 1, 2, 3, 4, 5
@@ -29,7 +29,7 @@ class KernelDesc(ctypes.Structure):
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("m2l", ctypes.c_int32), ("fix_bbox", ctypes.c_int32),
                 ("radii", ctypes.c_int32), ("device", ctypes.c_int32), ("near_fp64", ctypes.c_int32),
-                ("stream", ctypes.c_void_p), ("e2c", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+                ("stream", ctypes.c_void_p), ("e2c", ctypes.c_int32), ("iscomplex", ctypes.c_int32)]
 
 
 class TreeInfo(ctypes.Structure):

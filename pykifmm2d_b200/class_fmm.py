@@ -25,7 +25,7 @@ import numpy as np
 
 from . import _lib as B
 
-__all__ = ["LaplaceKernel", "ModifiedHelmholtzKernel", "Get_Kernel_Functions",
+__all__ = ["LaplaceKernel", "ModifiedHelmholtzKernel", "HelmholtzKernel", "Get_Kernel_Functions",
            "prepare_numba_functions_on_the_fly", "Kernel_Form", "FMM", "get_level_information"]
 
 
@@ -70,12 +70,41 @@ class ModifiedHelmholtzKernel:
         return f"ModifiedHelmholtzKernel(k={self.k})"
 
 
+class HelmholtzKernel:
+    """G(s -> t) = (i/4) H0^(1)(k |t - s|), complex (the reference's Helmholtz
+    plug-in, examples/hankel.py:37-39, used with FMM(..., iscomplex=True))."""
+
+    kind = B.KERNEL_HELMHOLTZ
+    complex_valued = True
+
+    def __init__(self, k):
+        if not k > 0:
+            raise ValueError("Helmholtz needs k > 0")
+        self.k = float(k)
+
+    def desc(self):
+        return B.KernelDesc(self.kind, 0, self.k)
+
+    def __call__(self, sx, sy, tx, ty):
+        sx, sy, tx, ty = (np.atleast_1d(np.asarray(v, dtype=np.float64)) for v in (sx, sy, tx, ty))
+        out = np.zeros((tx.size, sx.size), dtype=np.complex128)
+        B.check(_kernel_matrix(self, sx, sy, tx, ty, out))
+        return out if out.size != 1 else complex(out[0, 0])
+
+    def __repr__(self):
+        return f"HelmholtzKernel(k={self.k})"
+
+
 def _as_kernel(kernel):
-    if isinstance(kernel, (LaplaceKernel, ModifiedHelmholtzKernel)):
+    if isinstance(kernel, (LaplaceKernel, ModifiedHelmholtzKernel, HelmholtzKernel)):
         return kernel
     raise TypeError("kernel plug-ins are descriptors of the kernels compiled into the CUDA library: "
-                    "use LaplaceKernel() or ModifiedHelmholtzKernel(k); arbitrary numba scalar "
-                    "kernels are not JIT-compiled by this implementation")
+                    "use LaplaceKernel(), ModifiedHelmholtzKernel(k) or HelmholtzKernel(k); arbitrary numba "
+                    "scalar kernels are not JIT-compiled by this implementation")
+
+
+def _complex_kernel(kern):
+    return getattr(kern, "complex_valued", False)
 
 
 # ------------------------------------------------------------------ arrays
@@ -83,16 +112,18 @@ def _is_torch(a):
     return type(a).__module__.startswith("torch")
 
 
-def _hp(a):
-    """(pointer, mem flag, keep-alive) of a host numpy array or torch tensor."""
+def _hp(a, cplx=False):
+    """(pointer, mem flag, keep-alive) of a host numpy array or torch tensor;
+    cplx: complex128 values (interleaved doubles)."""
     if _is_torch(a):
         import torch
         t = a.detach()
-        if t.dtype != torch.float64:
-            t = t.to(torch.float64)
+        want = torch.complex128 if cplx else torch.float64
+        if t.dtype != want:
+            t = t.to(want)
         t = t.contiguous()
         return t.data_ptr(), (B.MEM_DEVICE if t.is_cuda else B.MEM_HOST), t
-    arr = np.ascontiguousarray(a, dtype=np.float64)
+    arr = np.ascontiguousarray(a, dtype=np.complex128 if cplx else np.float64)
     return arr.ctypes.data, B.MEM_HOST, arr
 
 
@@ -115,24 +146,27 @@ def Get_Kernel_Functions(Kernel_Eval):
     """
     kern = _as_kernel(Kernel_Eval)
     lib = B.load()
+    vt = np.complex128 if _complex_kernel(kern) else np.float64  # value type of the kernel
 
     def KF(sx, sy, tx, ty, out):
         sx, sy, tx, ty = (np.ascontiguousarray(v, dtype=np.float64) for v in (sx, sy, tx, ty))
-        buf = np.empty((tx.size, sx.size))
+        buf = np.empty((tx.size, sx.size), dtype=vt)
         B.check(_kernel_matrix(kern, sx, sy, tx, ty, buf))
         out[...] = buf
 
     def KA(sx, sy, tx, ty, tau, out):
-        sx, sy, tx, ty, tau = (np.ascontiguousarray(v, dtype=np.float64) for v in (sx, sy, tx, ty, tau))
-        buf = np.empty(tx.size)
+        sx, sy, tx, ty = (np.ascontiguousarray(v, dtype=np.float64) for v in (sx, sy, tx, ty))
+        tau = np.ascontiguousarray(tau, dtype=vt)
+        buf = np.empty(tx.size, dtype=vt)
         B.check(lib.kifmm_kernel_apply(kern.desc(), sx.ctypes.data, sy.ctypes.data, sx.size, tx.ctypes.data,
                                        ty.ctypes.data, tx.size, tau.ctypes.data, buf.ctypes.data, B.MEM_HOST, 0))
         out[...] = buf
 
     def KAS(sx, sy, tau, out, targets=None):
-        sx, sy, tau = (np.ascontiguousarray(v, dtype=np.float64) for v in (sx, sy, tau))
+        sx, sy = (np.ascontiguousarray(v, dtype=np.float64) for v in (sx, sy))
+        tau = np.ascontiguousarray(tau, dtype=vt)
         tg = np.arange(sx.size, dtype=np.int64) if targets is None else np.ascontiguousarray(targets, dtype=np.int64)
-        buf = np.empty(tg.size)
+        buf = np.empty(tg.size, dtype=vt)
         B.check(lib.kifmm_direct_sum(kern.desc(), sx.ctypes.data, sy.ctypes.data, tau.ctypes.data, sx.size,
                                      tg.ctypes.data, tg.size, buf.ctypes.data, B.MEM_HOST, 0))
         out[...] = buf
@@ -203,8 +237,6 @@ class FMM(object):
     def __init__(self, x, y, kernel_functions, numba_functions, Nequiv=48, Ncutoff=50, iscomplex=False,
                  verbose=False, precision="fp64", m2l="auto", fix_bbox=False, radii="reference", device=None,
                  stream=None, near_fp64=False, e2c="dense"):
-        if iscomplex:
-            raise NotImplementedError("complex kernels are not part of this build")
         kern = None
         for f in tuple(kernel_functions) + tuple(numba_functions):
             k = getattr(f, "kernel", None) if callable(f) else (f[1] if isinstance(f, tuple) else None)
@@ -223,7 +255,10 @@ class FMM(object):
         self.kernel_functions = kernel_functions
         self.numba_functions = numba_functions
         self.kernel = kern
-        self.dtype = np.float64
+        if _complex_kernel(kern) and not iscomplex:
+            raise ValueError(f"{kern!r} has complex values: construct the FMM with iscomplex=True")
+        self.iscomplex = bool(iscomplex)
+        self.dtype = np.complex128 if self.iscomplex else np.float64
         self.verbose = verbose
         self.precision = precision
         self._on_device = _is_torch(x) and x.is_cuda
@@ -238,6 +273,7 @@ class FMM(object):
         if e2c not in ("dense", "circulant"):
             raise ValueError("e2c must be 'dense' or 'circulant'")
         opts.e2c = B.E2C_CIRCULANT if e2c == "circulant" else B.E2C_DENSE
+        opts.iscomplex = int(self.iscomplex)
         if device is None:
             device = x.device.index if self._on_device and x.device.index is not None else 0
         opts.device = int(device)
@@ -320,7 +356,7 @@ class FMM(object):
         if not self._have_ops:
             self.precompute()
         st = time.time()
-        p, m, keep = _hp(tau)
+        p, m, keep = _hp(tau, self.iscomplex)
         if _numel(keep) != self.N:
             raise ValueError("tau must have one value per source point")
         self.tau = tau
@@ -332,8 +368,8 @@ class FMM(object):
             return out
         if _is_torch(like) and like.is_cuda:
             import torch
-            return torch.empty(n, dtype=torch.float64, device=like.device)
-        return np.empty(n, dtype=np.float64)
+            return torch.empty(n, dtype=torch.complex128 if self.iscomplex else torch.float64, device=like.device)
+        return np.empty(n, dtype=self.dtype)
 
     def evaluate_to_points(self, x, y, check_self=False, out=None):
         """Potential at (x, y): L2P from the leaf's local expansion plus P2P
@@ -343,7 +379,7 @@ class FMM(object):
         py, my, ky = _hp(y)
         n = _numel(kx)
         res = self._out(n, x, out)
-        pr, mr, kr = _hp(res)
+        pr, mr, kr = _hp(res, self.iscomplex)
         same = (x is self.x and y is self.y)
         if same:
             B.check(self._lib.kifmm_evaluate_to_sources(self._plan, pr, int(bool(check_self)), mr))
@@ -369,9 +405,10 @@ class FMM(object):
         if not self._have_ops:
             self.precompute()
         import torch
+        want = torch.complex128 if self.iscomplex else torch.float64
         for t in (tau_dev, pot_dev):
-            if not (_is_torch(t) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
-                raise ValueError("capture_apply needs contiguous float64 CUDA tensors (the graph keeps their addresses)")
+            if not (_is_torch(t) and t.is_cuda and t.dtype == want and t.is_contiguous()):
+                raise ValueError(f"capture_apply needs contiguous {want} CUDA tensors (the graph keeps their addresses)")
         p_t, p_o = tau_dev.data_ptr(), pot_dev.data_ptr()
         if _numel(tau_dev) != self.N or _numel(pot_dev) != self.N:
             raise ValueError("tau_dev and pot_dev must have one value per source point")

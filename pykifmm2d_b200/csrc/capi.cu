@@ -163,11 +163,14 @@ static void copy_out(kifmm_plan *P, double *dst, const double *src, int64_t n, i
 
 static void check_kernel(const kifmm_kernel *k) {
     KIFMM_REQUIRE(k, KIFMM_ERR_ARG, "null kernel descriptor");
-    KIFMM_REQUIRE(k->kind == KIFMM_KERNEL_LAPLACE || k->kind == KIFMM_KERNEL_MOD_HELMHOLTZ, KIFMM_ERR_ARG,
-                  "unknown kernel kind");
-    KIFMM_REQUIRE(k->kind != KIFMM_KERNEL_MOD_HELMHOLTZ || k->k > 0, KIFMM_ERR_ARG,
-                  "modified Helmholtz needs k > 0");
+    KIFMM_REQUIRE(k->kind == KIFMM_KERNEL_LAPLACE || k->kind == KIFMM_KERNEL_MOD_HELMHOLTZ ||
+                      k->kind == KIFMM_KERNEL_HELMHOLTZ,
+                  KIFMM_ERR_ARG, "unknown kernel kind");
+    KIFMM_REQUIRE(k->kind == KIFMM_KERNEL_LAPLACE || k->k > 0, KIFMM_ERR_ARG,
+                  "(modified) Helmholtz needs k > 0");
 }
+// doubles per density / potential value of a kernel called outside a plan
+static int64_t kernel_width(const kifmm_kernel *k) { return k->kind == KIFMM_KERNEL_HELMHOLTZ ? 2 : 1; }
 
 // Stand-alone kernel-function calls (KF/KA/KAS) run on a temporary stream.
 struct TempCtx {
@@ -204,6 +207,14 @@ int kifmm_plan_create(const kifmm_kernel *kernel, int32_t nequiv, int32_t ncutof
         *plan_out = nullptr;
         check_kernel(kernel);
         KIFMM_REQUIRE(nequiv >= 4 && nequiv <= 64, KIFMM_ERR_ARG, "Nequiv must be in [4, 64]");
+        const bool cplx = (opts && opts->iscomplex) || kernel->kind == KIFMM_KERNEL_HELMHOLTZ;
+        if (cplx) {
+            KIFMM_REQUIRE(nequiv <= 32, KIFMM_ERR_ARG, "Nequiv must be in [4, 32] for complex values");
+            KIFMM_REQUIRE(!opts || opts->precision == KIFMM_PREC_FP64, KIFMM_ERR_UNSUPPORTED,
+                          "complex values: only the FP64 precision form is built");
+            KIFMM_REQUIRE(!opts || opts->e2c == KIFMM_E2C_DENSE, KIFMM_ERR_UNSUPPORTED,
+                          "complex values: the circulant E2C solve is for real kernels");
+        }
         KIFMM_REQUIRE(ncutoff >= 1, KIFMM_ERR_ARG, "Ncutoff must be >= 1");
         kifmm_options o;
         kifmm_default_options(&o);
@@ -219,7 +230,10 @@ int kifmm_plan_create(const kifmm_kernel *kernel, int32_t nequiv, int32_t ncutof
                       "an FP64 M2L belongs to the FP64 precision form");
         kifmm_plan *P = new kifmm_plan();
         P->kern = *kernel;
-        P->Q = nequiv;
+        P->cplx = cplx;
+        P->Qc = nequiv;
+        P->Q = cplx ? 2 * nequiv : nequiv;  // complex: node state = [Re, Im] of the check potential
+        o.iscomplex = cplx;
         P->ppl = ncutoff;
         P->opt = o;
         P->device = o.device;
@@ -279,7 +293,7 @@ int kifmm_build_expansions(kifmm_plan *P, const double *tau, int32_t mem) {
         KIFMM_REQUIRE(P->have_ops, KIFMM_ERR_STATE, "build_expansions: call precompute first");
         use_device(P);
         P->have_expansions = false;
-        copy_in(P, P->tau, tau, P->N, mem);
+        copy_in(P, P->tau, tau, P->cplx ? 2 * P->N : P->N, mem);
         run_upward_downward(P);
         P->have_expansions = true;
     });
@@ -292,7 +306,7 @@ int kifmm_evaluate_to_sources(kifmm_plan *P, double *pot, int32_t check_self, in
         KIFMM_REQUIRE(mem == KIFMM_MEM_HOST || mem == KIFMM_MEM_DEVICE, KIFMM_ERR_ARG, "bad mem flag");
         use_device(P);
         run_eval_sources(P, check_self != 0);
-        copy_out(P, pot, P->pot_out.p, P->N, mem);
+        copy_out(P, pot, P->pot_out.p, P->cplx ? 2 * P->N : P->N, mem);
     });
 }
 
@@ -306,12 +320,13 @@ int kifmm_evaluate_to_points(kifmm_plan *P, const double *x, const double *y, in
         if (n == 0) return;
         copy_in(P, P->tx, x, n, mem);
         copy_in(P, P->ty, y, n, mem);
-        P->tpot.alloc(n);
+        const int64_t vw = P->cplx ? 2 : 1;
+        P->tpot.alloc(n * vw);
         {
             PhaseScope ph(P, KIFMM_PHASE_TARGETS);
             run_eval_targets(P, P->tx.p, P->ty.p, n, check_self != 0, P->tpot.p);
         }
-        copy_out(P, pot, P->tpot.p, n, mem);
+        copy_out(P, pot, P->tpot.p, n * vw, mem);
     });
 }
 
@@ -326,11 +341,12 @@ int kifmm_synchronize(kifmm_plan *P) {
 
 // One apply on device pointers, no host synchronisation: what the graph holds.
 static void apply_device(kifmm_plan *P, const double *tau, double *pot, bool check_self) {
-    P->tau.alloc(P->N);
-    KIFMM_CUDA(cudaMemcpyAsync(P->tau.p, tau, P->N * sizeof(double), cudaMemcpyDeviceToDevice, P->stream));
+    const int64_t nv = P->cplx ? 2 * P->N : P->N;
+    P->tau.alloc(nv);
+    KIFMM_CUDA(cudaMemcpyAsync(P->tau.p, tau, nv * sizeof(double), cudaMemcpyDeviceToDevice, P->stream));
     run_upward_downward(P);
     run_eval_sources(P, check_self);
-    KIFMM_CUDA(cudaMemcpyAsync(pot, P->pot_out.p, P->N * sizeof(double), cudaMemcpyDeviceToDevice, P->stream));
+    KIFMM_CUDA(cudaMemcpyAsync(pot, P->pot_out.p, nv * sizeof(double), cudaMemcpyDeviceToDevice, P->stream));
 }
 
 int kifmm_graph_capture(kifmm_plan *P, const double *tau, double *pot, int32_t check_self) {
@@ -467,14 +483,15 @@ int kifmm_direct_sum(const kifmm_kernel *kernel, const double *x, const double *
             KIFMM_REQUIRE(targets || nt == 0, KIFMM_ERR_ARG, "null targets");
             for (int64_t a = 0; a < nt; a++)
                 KIFMM_REQUIRE(targets[a] >= 0 && targets[a] < n, KIFMM_ERR_ARG, "target index out of range");
-            copy_in(P, dx, x, n, mem); copy_in(P, dy, y, n, mem); copy_in(P, dt, tau, n, mem);
+            const int64_t vw = kernel_width(kernel);
+            copy_in(P, dx, x, n, mem); copy_in(P, dy, y, n, mem); copy_in(P, dt, tau, n * vw, mem);
             dtg.alloc(nt);
             KIFMM_CUDA(cudaMemcpyAsync(dtg.p, targets, nt * sizeof(int64_t), cudaMemcpyHostToDevice, P->stream));
-            dout.alloc(nt);
+            dout.alloc(nt * vw);
             px = dx.p; py = dy.p; pt = dt.p; ptg = dtg.p; po = dout.p;
         }
         direct_sum_device(*kernel, px, py, pt, n, ptg, nt, po, P->stream);
-        if (mem == KIFMM_MEM_HOST) copy_out(P, out, dout.p, nt, mem);
+        if (mem == KIFMM_MEM_HOST) copy_out(P, out, dout.p, nt * kernel_width(kernel), mem);
         KIFMM_CUDA(cudaStreamSynchronize(P->stream));
     });
 }
@@ -491,11 +508,11 @@ int kifmm_kernel_matrix(const kifmm_kernel *kernel, const double *sx, const doub
         double *po = out;
         if (mem == KIFMM_MEM_HOST) {
             copy_in(P, a, sx, ns, mem); copy_in(P, b, sy, ns, mem); copy_in(P, c, tx, nt, mem); copy_in(P, d, ty, nt, mem);
-            o.alloc(ns * nt);
+            o.alloc(ns * nt * kernel_width(kernel));
             psx = a.p; psy = b.p; ptx = c.p; pty = d.p; po = o.p;
         }
         kernel_matrix_device(*kernel, psx, psy, ns, ptx, pty, nt, po, P->stream);
-        if (mem == KIFMM_MEM_HOST) copy_out(P, out, o.p, ns * nt, mem);
+        if (mem == KIFMM_MEM_HOST) copy_out(P, out, o.p, ns * nt * kernel_width(kernel), mem);
         KIFMM_CUDA(cudaStreamSynchronize(P->stream));
     });
 }
@@ -512,12 +529,12 @@ int kifmm_kernel_apply(const kifmm_kernel *kernel, const double *sx, const doubl
         double *po = out;
         if (mem == KIFMM_MEM_HOST) {
             copy_in(P, a, sx, ns, mem); copy_in(P, b, sy, ns, mem); copy_in(P, c, tx, nt, mem);
-            copy_in(P, d, ty, nt, mem); copy_in(P, t, tau, ns, mem);
-            o.alloc(nt);
+            copy_in(P, d, ty, nt, mem); copy_in(P, t, tau, ns * kernel_width(kernel), mem);
+            o.alloc(nt * kernel_width(kernel));
             psx = a.p; psy = b.p; ptx = c.p; pty = d.p; pt = t.p; po = o.p;
         }
         kernel_apply_device(*kernel, psx, psy, ns, ptx, pty, nt, pt, po, P->stream);
-        if (mem == KIFMM_MEM_HOST) copy_out(P, out, o.p, nt, mem);
+        if (mem == KIFMM_MEM_HOST) copy_out(P, out, o.p, nt * kernel_width(kernel), mem);
         KIFMM_CUDA(cudaStreamSynchronize(P->stream));
     });
 }

@@ -138,7 +138,9 @@ struct PendingPhase {
 struct kifmm_plan {
     // configuration
     kifmm_kernel kern{};
-    int Q = 0;            // Nequiv
+    int Q = 0;            // state length per node: Nequiv (real kernels), 2 Nequiv (complex: real, imaginary)
+    int Qc = 0;           // points per circle (Nequiv)
+    bool cplx = false;    // complex kernel: densities, potentials and check potentials complex
     int ppl = 0;          // Ncutoff
     kifmm_options opt{};
     cudaStream_t stream = nullptr;
@@ -369,6 +371,17 @@ __device__ __forceinline__ float k0_f(float x) {
 __device__ __forceinline__ double green_d(int kind, double k, double r2) {
     if (kind == KIFMM_KERNEL_LAPLACE) return -0.07957747154594767 * log(r2);
     return 0.15915494309189535 * k0_d(k * sqrt(r2));
+}
+// Helmholtz kernel G = (i/4) H0^(1)(k r) = -Y0(k r)/4 + i J0(k r)/4, FP64
+// (examples/hankel.py:37-39); (re, im).
+__device__ __forceinline__ double2 green_c(double k, double r2) {
+    const double z = k * sqrt(r2);
+    return make_double2(-0.25 * y0(z), 0.25 * j0(z));
+}
+// value of a kernel as a complex number (the real kernels with zero imaginary part)
+__device__ __forceinline__ double2 green_z(int kind, double k, double r2) {
+    if (kind == KIFMM_KERNEL_HELMHOLTZ) return green_c(k, r2);
+    return make_double2(green_d(kind, k, r2), 0.0);
 }
 __device__ __forceinline__ float green_f(int kind, float k, float r2) {
     if (kind == KIFMM_KERNEL_LAPLACE) return -0.0795774715f * __logf(r2);

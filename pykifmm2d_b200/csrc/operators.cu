@@ -22,7 +22,8 @@
 namespace kifmm {
 
 struct OpsArgs {
-    int L, Q, kind;
+    int L, Q, kind;         // Q: state length per node (2 Nequiv for a complex kernel)
+    int Qc, cplx;           // points per circle; complex kernel (realified operators)
     int circulant;          // E2C inverse from the DFT of its first row (KIFMM_E2C_CIRCULANT)
     double k;
     double W;
@@ -47,6 +48,23 @@ __device__ __forceinline__ double gval(const OpsArgs &A, double sx, double sy, d
     double dx = tx - sx, dy = ty - sy;
     return green_d(A.kind, A.k, dx * dx + dy * dy);
 }
+// Entry (rt, cs) of a kernel matrix on the state index space: source point cs
+// of (sx, sy) shifted by (ox, oy), target point rt of (tx, ty).  Real values:
+// G itself.  Complex values act on states [Re (Qc), Im (Qc)], so the matrix
+// is the real image of the complex one: block (bt, bs) of entry
+// (rt mod Qc, cs mod Qc) is Re G, -Im G (bt 0, bs 1), Im G (bt 1, bs 0), Re G.
+// The real image of a transpose is not the transpose of the real image (that
+// is the image of the conjugate transpose): with `tr` the entry is that of
+// the image of the transposed matrix at (cs, rt), i.e. the blocks swap roles.
+__device__ __forceinline__ double gent(const OpsArgs &A, const double *sx, const double *sy, double ox, double oy,
+                                       const double *tx, const double *ty, int rt, int cs, bool tr = false) {
+    if (!A.cplx) return gval(A, sx[cs] + ox, sy[cs] + oy, tx[rt], ty[rt]);
+    const int pr = rt % A.Qc, ps = cs % A.Qc;
+    const int bt = (tr ? cs : rt) / A.Qc, bs = (tr ? rt : cs) / A.Qc;
+    const double dx = tx[pr] - (sx[ps] + ox), dy = ty[pr] - (sy[ps] + oy);
+    const double2 g = green_z(A.kind, A.k, dx * dx + dy * dy);
+    return bt == bs ? g.x : (bt == 0 ? -g.y : g.y);
+}
 
 // Gauss-Jordan with partial pivoting on [E2C | I], one warp per level: lane r
 // owns row r of the augmented matrix (rows of 2Q+1 doubles in shared memory,
@@ -68,20 +86,21 @@ __global__ void __launch_bounds__(INV_THREADS) k_ops_inverse(OpsArgs A) {
     {  // the level's circles (get_level_information, class_fmm.py:35-45)
         const double w = lvl_width(A, l), r1 = 0.5 * w * A.rf1, r2 = 0.5 * w * A.rf2;
         double *bw = A.ops + (size_t)l * A.stride;
-        for (int q = tid; q < Q; q += INV_THREADS) {
-            const double th = q * (2.0 * 3.141592653589793 / Q);
+        const int Qc = A.Qc;  // circle points: x at [0, Qc), y at [Qc, 2 Qc)
+        for (int q = tid; q < Qc; q += INV_THREADS) {
+            const double th = q * (2.0 * 3.141592653589793 / Qc);
             const double c = cos(th), s = sin(th);
             bw[off_large(Q) + q] = r2 * c;
-            bw[off_large(Q) + Q + q] = r2 * s;
+            bw[off_large(Q) + Qc + q] = r2 * s;
             bw[off_small(Q) + q] = r1 * c;
-            bw[off_small(Q) + Q + q] = r1 * s;
+            bw[off_small(Q) + Qc + q] = r1 * s;
         }
         __syncthreads();
     }
     if (l < 1) return;
     double *a = sm, *nb = sm + (size_t)Q * ld;  // current and next matrix, Q x ld each
     const double *b = A.ops + (size_t)l * A.stride;
-    const double *lx = b + off_large(Q), *ly = lx + Q, *sx = b + off_small(Q), *sy = sx + Q;
+    const double *lx = b + off_large(Q), *ly = lx + A.Qc, *sx = b + off_small(Q), *sy = sx + A.Qc;
     if (A.circulant) {
         // E2C[t][s] = G(small_s -> large_t) depends on (s - t) mod Q only (both
         // circles carry the same Q angles and G is radial): E2C = C(a) with
@@ -115,7 +134,7 @@ __global__ void __launch_bounds__(INV_THREADS) k_ops_inverse(OpsArgs A) {
     }
     for (int e = tid; e < Q * Q2; e += INV_THREADS) {
         const int r = e / Q2, c = e % Q2;
-        a[r * ld + c] = c < Q ? gval(A, sx[c], sy[c], lx[r], ly[r]) : (c - Q == r ? 1.0 : 0.0);
+        a[r * ld + c] = c < Q ? gent(A, sx, sy, 0.0, 0.0, lx, ly, r, c) : (c - Q == r ? 1.0 : 0.0);
     }
     __syncthreads();
     for (int k = 0; k < Q; k++) {
@@ -186,22 +205,24 @@ __global__ void k_ops_compose(OpsArgs A) {
     double *mm = sm_c + Q * Q;  // M2LS block, or the child's block of M2MC, [Q][Q]
     for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) iv[e] = inv[e];
     // the kernel-matrix block, evaluated here (class_fmm.py:219-250)
-    const double *sx = b + off_small(Q), *sy = sx + Q, *lx = b + off_large(Q), *ly = lx + Q;
+    const double *sx = b + off_small(Q), *sy = sx + A.Qc, *lx = b + off_large(Q), *ly = lx + A.Qc;
     if (slot < 49) {  // M2LS_o[r][t] = G(small_t + o w -> small_r)
         const int ox = slot / 7 - 3, oy = slot % 7 - 3;
         const double w = lvl_width(A, l);
         for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) {
             const int r = e / Q, t = e % Q;
-            mm[e] = gval(A, sx[t] + ox * w, sy[t] + oy * w, sx[r], sy[r]);
+            mm[e] = gent(A, sx, sy, ox * w, oy * w, sx, sy, r, t);
         }
     } else {  // M2MC_l[r][q Q + t] = G(small_{l+1, t} + child offset q -> large_r), child q's block
         const double *b1 = A.ops + (size_t)(l + 1) * A.stride;
-        const double *cx = b1 + off_small(Q), *cy = cx + Q;
+        const double *cx = b1 + off_small(Q), *cy = cx + A.Qc;
         const double hw = 0.5 * lvl_width(A, l + 1);
         const double ox = (q >= 2) ? hw : -hw, oy = (q & 1) ? hw : -hw;
+        // L2L applies M2MC's transpose (class_fmm.py:329-330): for complex values
+        // its real image is built here, as l2l reads this block transposed
         for (int e = threadIdx.x; e < Q * Q; e += blockDim.x) {
             const int r = e / Q, t = e % Q;
-            mm[e] = gval(A, cx[t] + ox, cy[t] + oy, lx[r], ly[r]);
+            mm[e] = gent(A, cx, cy, ox, oy, lx, ly, r, t, l2l);
         }
     }
     __syncthreads();
@@ -313,6 +334,8 @@ void build_operators(kifmm_plan *P) {
     OpsArgs A{};
     A.L = L; A.Q = Q; A.kind = P->kern.kind; A.k = P->kern.k; A.W = P->W;
     A.circulant = P->opt.e2c == KIFMM_E2C_CIRCULANT;
+    A.Qc = P->Qc;
+    A.cplx = P->cplx;
     if (P->opt.radii == 1) { A.rf1 = 1.5; A.rf2 = 2.5; }
     else { A.rf1 = std::sqrt(2.0) + 0.01; A.rf2 = 4.0 - std::sqrt(2.0) - 2 * 0.01; }
     A.stride = ops_stride(Q);

@@ -453,6 +453,7 @@ PassArgs make_pass_args(kifmm_plan *P) {
     PassArgs A{};
     A.T = P->lt;
     A.Q = P->Q;
+    A.Qc = P->Qc;
     A.kind = P->kern.kind;
     A.k = P->kern.k;
     A.root = P->root_min;
@@ -907,8 +908,9 @@ void run_upward_downward(kifmm_plan *P) {
     cudaStream_t s = P->stream;
     const int Q = P->Q, L = P->L;
     int64_t n = P->N, NN = P->n_nodes;
-    P->taus.alloc(n);
-    P->pots.alloc(n);
+    const int64_t vw = P->cplx ? 2 : 1;  // doubles per density value
+    P->taus.alloc(n * vw);
+    P->pots.alloc(n * vw);
     P->uup.alloc((size_t)NN * Q);
     P->udown.alloc((size_t)NN * Q);
     // error flags of the level passes and the tensor-core M2L, and the
@@ -917,8 +919,11 @@ void run_upward_downward(kifmm_plan *P) {
     KIFMM_CUDA(cudaMemsetAsync(P->scal.p + KIFMM_SCAL_PASS_ERR, 0, 2 * sizeof(unsigned long long), s));
     KIFMM_CUDA(cudaMemsetAsync(P->uup.p, 0, (size_t)NN * Q * sizeof(double), s));
     KIFMM_CUDA(cudaMemsetAsync(P->udown.p, 0, (size_t)NN * Q * sizeof(double), s));
-    launch_pdl(k_gather_tau, dim3(grid_for(n, 256, P->num_sms * 8)), dim3(256), 0, s, (const double *)P->tau.p,
-               (const int32_t *)P->perm.p, n, P->taus.p);
+    if (P->cplx)
+        launch_gather_tau_c(P);
+    else
+        launch_pdl(k_gather_tau, dim3(grid_for(n, 256, P->num_sms * 8)), dim3(256), 0, s, (const double *)P->tau.p,
+                   (const int32_t *)P->perm.p, n, P->taus.p);
     if (P->opt.precision == KIFMM_PREC_MIXED) {
         run_passes_mixed(P);
         return;
@@ -927,7 +932,8 @@ void run_upward_downward(kifmm_plan *P) {
     PassArgs A = make_pass_args(P);
     if (P->n_p2m_list) {
         PhaseScope ph(P, KIFMM_PHASE_P2M);
-        launch_p2m_d(P, A);
+        if (P->cplx) launch_p2m_c(P, A);
+        else launch_p2m_d(P, A);
     }
     {
         PhaseScope ph_m2m(P, KIFMM_PHASE_M2M);
@@ -980,7 +986,11 @@ void run_upward_downward(kifmm_plan *P) {
 void run_eval_sources(kifmm_plan *P, int check_self) {
     cudaStream_t s = P->stream;
     int64_t n = P->N;
-    P->pot_out.alloc(n);
+    P->pot_out.alloc(P->cplx ? 2 * n : n);
+    if (P->cplx) {
+        run_eval_sources_c(P, make_pass_args(P), check_self);
+        return;
+    }
     if (P->opt.precision == KIFMM_PREC_MIXED) {
         run_eval_sources_mixed(P, check_self);
     } else {
@@ -996,6 +1006,10 @@ void run_eval_sources(kifmm_plan *P, int check_self) {
 
 void run_eval_targets(kifmm_plan *P, const double *tx, const double *ty, int64_t n, int check_self, double *pot) {
     PassArgs A = make_pass_args(P);
+    if (P->cplx) {
+        run_eval_targets_c(P, A, tx, ty, n, check_self, pot);
+        return;
+    }
     if (P->opt.precision == KIFMM_PREC_MIXED) {
         run_eval_targets_mixed(P, tx, ty, n, check_self, pot);
         return;
@@ -1051,8 +1065,16 @@ __global__ void k_kapply_d(int kind, double k, const double *sx, const double *s
     }
 }
 
+void direct_sum_device_c(const kifmm_kernel &kn, const double *x, const double *y, const double *tau, int64_t n,
+                         const int64_t *tg, int64_t nt, double *out, cudaStream_t s);
+void kernel_matrix_device_c(const kifmm_kernel &kn, const double *sx, const double *sy, int64_t ns, const double *tx,
+                            const double *ty, int64_t nt, double *out, cudaStream_t s);
+void kernel_apply_device_c(const kifmm_kernel &kn, const double *sx, const double *sy, int64_t ns, const double *tx,
+                           const double *ty, int64_t nt, const double *tau, double *out, cudaStream_t s);
+
 void direct_sum_device(const kifmm_kernel &kn, const double *x, const double *y, const double *tau, int64_t n,
                        const int64_t *tg, int64_t nt, double *out, cudaStream_t s) {
+    if (kn.kind == KIFMM_KERNEL_HELMHOLTZ) return direct_sum_device_c(kn, x, y, tau, n, tg, nt, out, s);
     if (nt <= 0) return;
     KIFMM_REQUIRE(nt < (1ll << 31), KIFMM_ERR_ARG, "direct_sum: too many targets");
     k_direct_d<<<(unsigned)nt, 256, 0, s>>>(kn.kind, kn.k, x, y, tau, n, tg, out);
@@ -1061,6 +1083,7 @@ void direct_sum_device(const kifmm_kernel &kn, const double *x, const double *y,
 
 void kernel_matrix_device(const kifmm_kernel &kn, const double *sx, const double *sy, int64_t ns, const double *tx,
                           const double *ty, int64_t nt, double *out, cudaStream_t s) {
+    if (kn.kind == KIFMM_KERNEL_HELMHOLTZ) return kernel_matrix_device_c(kn, sx, sy, ns, tx, ty, nt, out, s);
     if (ns * nt <= 0) return;
     k_kmatrix_d<<<grid_for(ns * nt, 256, 8192), 256, 0, s>>>(kn.kind, kn.k, sx, sy, ns, tx, ty, nt, out);
     KIFMM_LAUNCHED();
@@ -1068,6 +1091,7 @@ void kernel_matrix_device(const kifmm_kernel &kn, const double *sx, const double
 
 void kernel_apply_device(const kifmm_kernel &kn, const double *sx, const double *sy, int64_t ns, const double *tx,
                          const double *ty, int64_t nt, const double *tau, double *out, cudaStream_t s) {
+    if (kn.kind == KIFMM_KERNEL_HELMHOLTZ) return kernel_apply_device_c(kn, sx, sy, ns, tx, ty, nt, tau, out, s);
     if (nt <= 0) return;
     k_kapply_d<<<grid_for(nt, 128, 8192), 128, 0, s>>>(kn.kind, kn.k, sx, sy, ns, tx, ty, nt, tau, out);
     KIFMM_LAUNCHED();

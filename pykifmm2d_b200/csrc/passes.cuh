@@ -6,7 +6,8 @@ namespace kifmm {
 
 struct PassArgs {
     LevelTable T;
-    int Q, kind;
+    int Q, kind;   // Q: state length per node (2 Nequiv for complex values)
+    int Qc;        // points per circle (Nequiv)
     double k;
     double root, W;
     const double *ops;
@@ -46,6 +47,12 @@ __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, dou
 }
 // row stride = 4 mod 16 doubles: conflict-free fragment loads
 __host__ __device__ constexpr int pad4mod16(int m) { return m + (20 - m % 16) % 16; }
+// passes_complex.cu (complex values: FP64 point passes on double2 densities)
+void launch_gather_tau_c(kifmm_plan *P);
+void launch_p2m_c(kifmm_plan *P, const PassArgs &A);
+void run_eval_sources_c(kifmm_plan *P, const PassArgs &A, int check_self);
+void run_eval_targets_c(kifmm_plan *P, const PassArgs &A, const double *tx, const double *ty, int64_t n,
+                        int check_self, double *pot);
 // passes_mixed.cu
 void run_passes_mixed(kifmm_plan *P);
 void run_eval_sources_mixed(kifmm_plan *P, int check_self);

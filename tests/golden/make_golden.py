@@ -98,6 +98,21 @@ def gen_cluster_dup(n, seed):
     return x, y, rng.standard_normal(n)
 
 
+def gen_uniform_ctau(n, seed):
+    """Uniform points with complex charges N(0,1) + i N(0,1)."""
+    rng = np.random.default_rng(seed)
+    x, y = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    return x, y, rng.standard_normal(n) + 1j * rng.standard_normal(n)
+
+
+def gen_circle(n, seed):
+    """Points on the unit circle with real charges U(0,1), the set-up of the
+    reference's Helmholtz example (examples/hankel.py, test = 'circle')."""
+    rng = np.random.default_rng(seed)
+    th = rng.uniform(0, 2 * np.pi, n)
+    return np.cos(th), np.sin(th), rng.uniform(0, 1, n)
+
+
 CASES = [
     # name, kernel, k, generator, N, seed, Nequiv, Ncutoff, n_targets
     ("c1_uniform20k", "laplace", 0.0, gen_uniform, 20000, 0, 24, 64, 1000),
@@ -107,6 +122,9 @@ CASES = [
     ("annulus6k_k0", "k0", 10.0, gen_annulus, 6000, 3, 24, 48, 300),
     ("cluster_dup", "laplace", 0.0, gen_cluster_dup, 2500, 5, 20, 20, 0),
     ("mix2k_cut8", "laplace", 0.0, gen_mixture, 2000, 4, 16, 8, 0),
+    # complex kernel G = (i/4) H0(k r) with FMM(..., iscomplex=True) (class_fmm.py:174)
+    ("helm_uniform6k_k2", "helmholtz", 2.0, gen_uniform_ctau, 6000, 6, 24, 50, 300),
+    ("helm_circle4k_k10", "helmholtz", 10.0, gen_circle, 4000, 7, 32, 40, 300),
 ]
 
 
@@ -216,6 +234,22 @@ def main():
     def laplace_eval(sx, sy, tx, ty):
         return -0.25 / np.pi * np.log((tx - sx) ** 2 + (ty - sy) ** 2)
 
+    # H0 from the C library's Bessel functions J0, Y0 (the reference's example
+    # interpolates scipy's hankel1 with fast_interp, which is not installed)
+    import ctypes
+    libm = ctypes.CDLL("libm.so.6")
+    j0, y0 = libm.j0, libm.y0
+    for f in (j0, y0):
+        f.restype = ctypes.c_double
+        f.argtypes = [ctypes.c_double]
+
+    def helmholtz_factory(kk):
+        @numba.njit("c16(f8,f8,f8,f8)", fastmath=True)
+        def h_eval(sx, sy, tx, ty):
+            z = kk * np.sqrt((tx - sx) ** 2 + (ty - sy) ** 2)
+            return 0.25j * (j0(z) + 1j * y0(z))
+        return h_eval
+
     def k0_factory(kk):
         @numba.njit("f8(f8,f8,f8,f8)", fastmath=True)
         def k0_eval(sx, sy, tx, ty):
@@ -223,12 +257,17 @@ def main():
         return k0_eval
 
     for name, kern, kk, gen, n, seed, neq, cut, ntarg in CASES:
-        ke = laplace_eval if kern == "laplace" else k0_factory(kk)
+        cplx = kern == "helmholtz"
+        ke = {"laplace": laplace_eval, "k0": None, "helmholtz": None}[kern]
+        if kern == "k0":
+            ke = k0_factory(kk)
+        elif cplx:
+            ke = helmholtz_factory(kk)
         nf = C.prepare_numba_functions_on_the_fly(ke)
         kf = C.Get_Kernel_Functions(ke)
         x, y, tau = gen(n, seed)
         t0 = time.time()
-        f = C.FMM(x, y, kf, nf, neq, cut)
+        f = C.FMM(x, y, kf, nf, neq, cut, cplx)
         f.build_tree()
         f.precompute()
         f.build_expansions(tau)
@@ -237,7 +276,7 @@ def main():
         nodes, pl, (coll, m2l, p2p) = canonical_tree(f.tree, x, y)
         out = dict(x=x, y=y, tau=tau, pot=pot, nodes=nodes, point_leaf=pl,
                    colleagues=coll, m2l_pairs=m2l, p2p_pairs=p2p,
-                   kernel=np.array(0 if kern == "laplace" else 1), k=np.array(kk),
+                   kernel=np.array({"laplace": 0, "k0": 1, "helmholtz": 2}[kern]), k=np.array(kk),
                    nequiv=np.array(neq), ncutoff=np.array(cut),
                    root=np.array([f.tree.xmin, f.tree.xmax], dtype=np.float64),
                    levels=np.array(f.tree.levels))
@@ -249,7 +288,7 @@ def main():
             out.update(xt=xt, yt=yt, pot_targets=f.evaluate_to_points(xt, yt, False))
         # FP64 direct sum (the reference's KAS, class_fmm.py:134-143) for information
         KF, KA, KAS = kf
-        ref = np.zeros(n)
+        ref = np.zeros(n, dtype=complex if cplx else float)
         KAS(x, y, tau, ref)
         fin = np.isfinite(ref)  # coincident points make the i != j direct sum infinite
         err = np.abs(pot - ref)[fin].max() / np.abs(ref[fin]).max()

@@ -6,7 +6,7 @@ import pytest
 from oracle import oracle as O
 
 CASES = ["c1_uniform20k", "mix5k_seed1", "mix20k_seed0", "uniform3k_cut16",
-         "annulus6k_k0", "cluster_dup", "mix2k_cut8"]
+         "annulus6k_k0", "cluster_dup", "mix2k_cut8", "helm_uniform6k_k2", "helm_circle4k_k10"]
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -68,3 +68,11 @@ def test_oracle_lists_match_reference(golden_cases, name):
     np.testing.assert_array_equal(coll, g["colleagues"])
     np.testing.assert_array_equal(m2l, g["m2l_pairs"])
     np.testing.assert_array_equal(p2p, g["p2p_pairs"])
+
+
+@pytest.mark.parametrize("name", ["helm_uniform6k_k2", "helm_circle4k_k10"])
+def test_oracle_complex_direct_matches_reference_kas(golden_cases, name):
+    g = golden_cases[name]
+    idx = np.random.default_rng(5).choice(g["x"].size, 200, replace=False)
+    d = O.direct(g["x"], g["y"], g["tau"], idx, int(g["kernel"]), float(g["k"]))
+    assert np.abs(d - g["direct"][idx]).max() <= 1e-12 * np.abs(g["direct"]).max()
