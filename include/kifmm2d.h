@@ -93,6 +93,13 @@ typedef struct kifmm_options {
     int32_t iscomplex;  /* FMM(..., iscomplex=True) (class_fmm.py:174): 1 makes densities and
                            potentials complex (interleaved doubles) for any kernel; the
                            Helmholtz kernel sets it by itself.  0 (default): real values */
+    int32_t planned;    /* the reference's planned FMM (fmm_planner / planned_fmm, fmm.py:530-814):
+                           1 keeps the P2M, L2P and near-field kernel values of the tree in device
+                           memory (built by the first apply after build_tree / precompute; about
+                           8 B per near-field pair, 4 B in the mixed form, plus 16 Q B per point)
+                           and applies them as matrices; evaluations at the sources with
+                           check_self use them.  Real values only.  0 (default): on the fly */
+    int32_t reserved;
 } kifmm_options;
 
 /* Check-to-equivalent solve.  The reference LU-factors the Q x Q E2C matrix

@@ -29,7 +29,8 @@ class KernelDesc(ctypes.Structure):
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int32), ("m2l", ctypes.c_int32), ("fix_bbox", ctypes.c_int32),
                 ("radii", ctypes.c_int32), ("device", ctypes.c_int32), ("near_fp64", ctypes.c_int32),
-                ("stream", ctypes.c_void_p), ("e2c", ctypes.c_int32), ("iscomplex", ctypes.c_int32)]
+                ("stream", ctypes.c_void_p), ("e2c", ctypes.c_int32), ("iscomplex", ctypes.c_int32),
+                ("planned", ctypes.c_int32), ("reserved", ctypes.c_int32)]
 
 
 class TreeInfo(ctypes.Structure):

@@ -225,6 +225,10 @@ class FMM(object):
       fix_bbox   False keeps the reference's root box (tree.py:475-484);
       radii      'reference' or '1.5/2.5';
       near_fp64  with precision='mixed', keep P2M/L2P/P2P in FP64;
+      planned    keep the P2M, L2P and near-field kernel values in device
+                 memory after the first apply and apply them as matrices (the
+                 reference's fmm_planner / planned_fmm, fmm.py:530-814): for
+                 repeated densities on one tree, evaluated at the sources;
       e2c        'dense' (Gauss-Jordan inverse of E2C, the reference's LU,
                  class_fmm.py:213-217) or 'circulant' (inverse from the DFT
                  of E2C's first row, the reference's FFT solve,
@@ -236,7 +240,7 @@ class FMM(object):
 
     def __init__(self, x, y, kernel_functions, numba_functions, Nequiv=48, Ncutoff=50, iscomplex=False,
                  verbose=False, precision="fp64", m2l="auto", fix_bbox=False, radii="reference", device=None,
-                 stream=None, near_fp64=False, e2c="dense"):
+                 stream=None, near_fp64=False, e2c="dense", planned=False):
         kern = None
         for f in tuple(kernel_functions) + tuple(numba_functions):
             k = getattr(f, "kernel", None) if callable(f) else (f[1] if isinstance(f, tuple) else None)
@@ -274,6 +278,7 @@ class FMM(object):
             raise ValueError("e2c must be 'dense' or 'circulant'")
         opts.e2c = B.E2C_CIRCULANT if e2c == "circulant" else B.E2C_DENSE
         opts.iscomplex = int(self.iscomplex)
+        opts.planned = int(bool(planned))
         if device is None:
             device = x.device.index if self._on_device and x.device.index is not None else 0
         opts.device = int(device)

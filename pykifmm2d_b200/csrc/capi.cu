@@ -214,6 +214,8 @@ int kifmm_plan_create(const kifmm_kernel *kernel, int32_t nequiv, int32_t ncutof
                           "complex values: only the FP64 precision form is built");
             KIFMM_REQUIRE(!opts || opts->e2c == KIFMM_E2C_DENSE, KIFMM_ERR_UNSUPPORTED,
                           "complex values: the circulant E2C solve is for real kernels");
+            KIFMM_REQUIRE(!opts || !opts->planned, KIFMM_ERR_UNSUPPORTED,
+                          "complex values: planned applies are for real values");
         }
         KIFMM_REQUIRE(ncutoff >= 1, KIFMM_ERR_ARG, "Ncutoff must be >= 1");
         kifmm_options o;
@@ -271,6 +273,7 @@ int kifmm_build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n,
         KIFMM_REQUIRE(mem == KIFMM_MEM_HOST || mem == KIFMM_MEM_DEVICE, KIFMM_ERR_ARG, "bad mem flag");
         use_device(P);
         PhaseScope ph(P, KIFMM_PHASE_TREE);
+        P->have_mats = false;
         build_tree(P, x, y, n, mem);
     });
 }
@@ -282,6 +285,7 @@ int kifmm_precompute(kifmm_plan *P) {
         PhaseScope ph(P, KIFMM_PHASE_PRECOMPUTE);
         KIFMM_REQUIRE(P->have_tree, KIFMM_ERR_STATE, "precompute: build_tree first");
         drop_graph(P);
+        P->have_mats = false;
         if (P->ops_pending) join_operators(P);  // started by build_tree
         else build_operators(P);
     });

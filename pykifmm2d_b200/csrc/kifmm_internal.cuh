@@ -204,6 +204,13 @@ struct kifmm_plan {
     kifmm::DBuf<unsigned char> tc_pre;  // per-apply slices of the source groups
     kifmm::DBuf<int> tc_gexp;
     kifmm::DBuf<int> tc_src8;        // [n_ent][8] M2L source entry per direction (per apply)
+    // planned applies (planned.cu): P2M, L2P and near-field blocks, built on
+    // the first apply after build_tree / precompute
+    bool have_mats = false;
+    size_t pm_bytes = 0;
+    kifmm::DBuf<int64_t> pm_near_off, pm_l2p_off, pm_p2m_off;
+    kifmm::DBuf<float> pm_near32;
+    kifmm::DBuf<double> pm_near64, pm_l2p, pm_p2m;
 
     // workspaces
     kifmm::DBuf<double> tau, taus, pots, pot_out, tx, ty, tpot;
@@ -445,6 +452,9 @@ void ensure_side(kifmm_plan *P);      // side stream and its events
 void start_operators(kifmm_plan *P, bool fork_recorded = false);  // build_operators on the side stream
 cudaStream_t device_side_stream(int device);  // one per device, created on first use
 void join_operators(kifmm_plan *P);   // main stream waits for it
+// planned.cu
+bool planned_ready(const kifmm_plan *P);
+void build_plan_matrices(kifmm_plan *P);
 // passes.cu
 void run_upward_downward(kifmm_plan *P);
 void run_eval_sources(kifmm_plan *P, int check_self);

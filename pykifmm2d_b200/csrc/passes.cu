@@ -919,6 +919,7 @@ void run_upward_downward(kifmm_plan *P) {
     KIFMM_CUDA(cudaMemsetAsync(P->scal.p + KIFMM_SCAL_PASS_ERR, 0, 2 * sizeof(unsigned long long), s));
     KIFMM_CUDA(cudaMemsetAsync(P->uup.p, 0, (size_t)NN * Q * sizeof(double), s));
     KIFMM_CUDA(cudaMemsetAsync(P->udown.p, 0, (size_t)NN * Q * sizeof(double), s));
+    if (P->opt.planned) build_plan_matrices(P);  // first apply after build_tree / precompute
     if (P->cplx)
         launch_gather_tau_c(P);
     else
@@ -933,6 +934,7 @@ void run_upward_downward(kifmm_plan *P) {
     if (P->n_p2m_list) {
         PhaseScope ph(P, KIFMM_PHASE_P2M);
         if (P->cplx) launch_p2m_c(P, A);
+        else if (planned_ready(P)) launch_planned_p2m(P, A);
         else launch_p2m_d(P, A);
     }
     {
@@ -991,7 +993,12 @@ void run_eval_sources(kifmm_plan *P, int check_self) {
         run_eval_sources_c(P, make_pass_args(P), check_self);
         return;
     }
-    if (P->opt.precision == KIFMM_PREC_MIXED) {
+    if (check_self && planned_ready(P)) {
+        if (P->n_leaf_list) {
+            PhaseScope ph(P, KIFMM_PHASE_LEAF);
+            launch_planned_leaf(P, make_pass_args(P));
+        }
+    } else if (P->opt.precision == KIFMM_PREC_MIXED) {
         run_eval_sources_mixed(P, check_self);
     } else {
         PassArgs A = make_pass_args(P);

@@ -47,6 +47,9 @@ __device__ __forceinline__ void dmma_8x8x4(double &c0, double &c1, double a, dou
 }
 // row stride = 4 mod 16 doubles: conflict-free fragment loads
 __host__ __device__ constexpr int pad4mod16(int m) { return m + (20 - m % 16) % 16; }
+// planned.cu
+void launch_planned_p2m(kifmm_plan *P, const PassArgs &A);
+void launch_planned_leaf(kifmm_plan *P, const PassArgs &A);
 // passes_complex.cu (complex values: FP64 point passes on double2 densities)
 void launch_gather_tau_c(kifmm_plan *P);
 void launch_p2m_c(kifmm_plan *P, const PassArgs &A);

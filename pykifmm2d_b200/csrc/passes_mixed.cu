@@ -588,7 +588,8 @@ void run_passes_mixed(kifmm_plan *P) {
     PassArgs A = make_pass_args(P);
     if (P->n_p2m_list) {
         PhaseScope ph(P, KIFMM_PHASE_P2M);
-        launch_p2m_d(P, A);
+        if (planned_ready(P)) launch_planned_p2m(P, A);
+        else launch_p2m_d(P, A);
     }
     {
         PhaseScope ph(P, KIFMM_PHASE_M2M);

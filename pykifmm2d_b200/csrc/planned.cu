@@ -1,0 +1,295 @@
+// planned.cu -- planned applies: P2M, L2P and the near field as matrices in HBM.
+//
+// The reference's planner (fmm_planner / planned_fmm, pykifmm2d/fmm.py:530-712,
+// :741-814) trades memory for time on repeated densities: it builds once the
+// sparse matrices of every P2M kernel evaluation ("upwards" matrices, source
+// points -> check circle, build_upwards_pass :472-491), every L2P evaluation
+// ("downwards" matrices, large circle -> points) and every near-field pair
+// (neighbor matrix, build_neighbor_interactions :429-470), and each apply is
+// then sparse matrix products.  Here the same three operators are dense
+// per-node blocks in HBM, built by the GPU on the first apply after the tree
+// and the operators:
+//   P2M   [n_src x Q] per P2M node:   u_up(g)[q]  = sum_s P[s][q] tau_s;
+//   L2P   [Q x n_t] per leaf (l >= 2), with the check-to-equivalent inverse
+//         folded in: far_t = sum_q L[q][t] u_down(g)[q],
+//         L[q][t] = sum_c G(large_c -> t) Inv[c][q];
+//   near  [n_src x n_t] per leaf over the concatenated sources of its 3x3
+//         colleagues: near_t = sum_s N[s][t] tau_s, pairs with equal
+//         coordinates zero (evaluate_to_points(..., check_self=True),
+//         class_fmm.py:105-108).
+// Each apply then streams the blocks once (HBM-bound matrix-vector products,
+// lanes over the contiguous index).  Values are computed in FP64; the near
+// blocks are stored in FP32 for the mixed precision (no FP32 coordinate
+// differences are involved), in FP64 otherwise.
+#include "passes.cuh"
+
+namespace kifmm {
+
+// block sizes of every leaf (near, L2P) and P2M node
+__global__ void k_plan_sizes(PassArgs A, const int32_t *__restrict__ leaves, int64_t nleaf,
+                             const int32_t *__restrict__ p2m, int64_t np2m, int64_t *__restrict__ near_sz,
+                             int64_t *__restrict__ l2p_sz, int64_t *__restrict__ p2m_sz) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nleaf + np2m;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        if (i < nleaf) {
+            const int g = leaves[i];
+            const int64_t nt = A.ntop[g] - A.nbot[g];
+            int64_t ns = 0;
+            for (int d = 0; d < 9; d++) {
+                const int c = A.ncoll[9 * (size_t)g + d];
+                if (c >= 0) ns += A.ntop[c] - A.nbot[c];
+            }
+            near_sz[i] = nt * ns;
+            l2p_sz[i] = A.nlev[g] >= 2 ? (int64_t)A.Q * nt : 0;
+        } else {
+            const int g = p2m[i - nleaf];
+            p2m_sz[i - nleaf] = (int64_t)(A.ntop[g] - A.nbot[g]) * A.Q;
+        }
+    }
+}
+
+// exclusive prefix sums of v[0..n) in place, v[n] = total; one block
+constexpr int PS_THREADS = 1024;
+__global__ void __launch_bounds__(PS_THREADS) k_plan_scan(int64_t *v, int64_t n) {
+    __shared__ int64_t part[PS_THREADS];
+    const int64_t per = (n + PS_THREADS - 1) / PS_THREADS, b = threadIdx.x * per, e = min(n, b + per);
+    int64_t s = 0;
+    for (int64_t i = b; i < e; i++) s += v[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int64_t acc = 0;
+        for (int i = 0; i < PS_THREADS; i++) {
+            const int64_t t = part[i];
+            part[i] = acc;
+            acc += t;
+        }
+        v[n] = acc;
+    }
+    __syncthreads();
+    int64_t acc = part[threadIdx.x];
+    for (int64_t i = b; i < e; i++) {
+        const int64_t t = v[i];
+        v[i] = acc;
+        acc += t;
+    }
+}
+
+// the leaf's source ranges: the leaf itself first, then its colleagues in
+// direction order (rng[0..9): first list position, rng[9..18): point offset)
+__device__ __forceinline__ int leaf_ranges(const PassArgs &A, int g, int *rng) {
+    int ns = 0;
+    for (int i = 0; i < 9; i++) {
+        const int d = i <= 4 ? i - 1 : i;
+        const int c = i == 0 ? g : A.ncoll[9 * (size_t)g + d];
+        const int rb = c >= 0 ? A.nbot[c] : 0, rn = c >= 0 ? A.ntop[c] - rb : 0;
+        rng[i] = ns;
+        rng[9 + i] = rb - ns;
+        ns += rn;
+    }
+    return ns;
+}
+__device__ __forceinline__ int range_point(const int *rng, int p) {
+    int sv = p + rng[9];
+#pragma unroll
+    for (int i = 1; i < 9; i++) sv = p >= rng[i] ? p + rng[9 + i] : sv;
+    return sv;
+}
+
+template <typename T>
+__global__ void k_plan_fill_leaf(PassArgs A, const int32_t *__restrict__ leaves, int64_t nleaf,
+                                 const int64_t *__restrict__ near_off, const int64_t *__restrict__ l2p_off,
+                                 T *__restrict__ near, double *__restrict__ l2p) {
+    __shared__ int rng[18];
+    const int64_t i = blockIdx.x;
+    if (i >= nleaf) return;
+    const int g = leaves[i], l = A.nlev[g], b = A.nbot[g], nt = A.ntop[g] - b, Q = A.Q;
+    if (threadIdx.x == 0) leaf_ranges(A, g, rng);
+    __syncthreads();
+    const int ns = (int)((near_off[i + 1] - near_off[i]) / max(nt, 1));
+    T *nb = near + near_off[i];
+    for (int64_t e = threadIdx.x; e < (int64_t)nt * ns; e += blockDim.x) {
+        const int s = (int)(e / nt), t = (int)(e % nt), sp = range_point(rng, s);
+        const double dx = A.xs[b + t] - A.xs[sp], dy = A.ys[b + t] - A.ys[sp];
+        const double v = (dx == 0.0 && dy == 0.0) ? 0.0 : green_d(A.kind, A.k, dx * dx + dy * dy);
+        nb[e] = (T)v;
+    }
+    if (l < 2) return;
+    double cx, cy;
+    node_center(A, g, l, cx, cy);
+    const double *blk = A.ops + (size_t)l * A.stride;
+    const double *inv = blk + A.off_inv, *lg = blk + A.off_large;
+    double *lb = l2p + l2p_off[i];
+    for (int e = threadIdx.x; e < nt * Q; e += blockDim.x) {
+        const int q = e / nt, t = e % nt;
+        const double px = A.xs[b + t] - cx, py = A.ys[b + t] - cy;
+        double acc = 0.0;
+        for (int c = 0; c < Q; c++) {
+            const double dx = px - lg[c], dy = py - lg[Q + c];
+            acc = fma(green_d(A.kind, A.k, dx * dx + dy * dy), inv[c * Q + q], acc);
+        }
+        lb[e] = acc;
+    }
+}
+
+__global__ void k_plan_fill_p2m(PassArgs A, const int32_t *__restrict__ p2m, int64_t np2m,
+                                const int64_t *__restrict__ p2m_off, double *__restrict__ mat) {
+    const int64_t i = blockIdx.x;
+    if (i >= np2m) return;
+    const int g = p2m[i], l = A.nlev[g], b = A.nbot[g], n = A.ntop[g] - b, Q = A.Q;
+    double cx, cy;
+    node_center(A, g, l, cx, cy);
+    const double *lg = A.ops + (size_t)l * A.stride + A.off_large;
+    double *m = mat + p2m_off[i];
+    for (int e = threadIdx.x; e < n * Q; e += blockDim.x) {
+        const int s = e / Q, q = e % Q;
+        const double dx = lg[q] + cx - A.xs[b + s], dy = lg[Q + q] + cy - A.ys[b + s];
+        m[e] = green_d(A.kind, A.k, dx * dx + dy * dy);
+    }
+}
+
+// planned P2M: one warp per node, lanes over the Q check points
+__global__ void k_planned_p2m(PassArgs A, const int32_t *__restrict__ p2m, int64_t np2m,
+                              const int64_t *__restrict__ p2m_off, const double *__restrict__ mat) {
+    pdl_trigger();
+    pdl_wait();
+    const int lane = threadIdx.x & 31;
+    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (w >= np2m) return;
+    const int g = p2m[w], b = A.nbot[g], n = A.ntop[g] - b, Q = A.Q;
+    const double *m = mat + p2m_off[w];
+    for (int q0 = 0; q0 < Q; q0 += 32) {
+        const int q = q0 + lane;
+        double acc0 = 0.0, acc1 = 0.0;
+        if (q < Q) {
+            int s = 0;
+            for (; s + 1 < n; s += 2) {
+                acc0 = fma(m[(size_t)s * Q + q], A.taus[b + s], acc0);
+                acc1 = fma(m[(size_t)(s + 1) * Q + q], A.taus[b + s + 1], acc1);
+            }
+            if (s < n) acc0 = fma(m[(size_t)s * Q + q], A.taus[b + s], acc0);
+            A.uup[(size_t)g * Q + q] = acc0 + acc1;
+        }
+    }
+}
+
+// planned L2P + near field: one warp per leaf, lanes over its targets; FP32
+// near blocks are summed in FP32 over runs of 32 sources, then in FP64
+template <typename T>
+__global__ void k_planned_leaf(PassArgs A, const int32_t *__restrict__ leaves, int64_t nleaf,
+                               const int64_t *__restrict__ near_off, const int64_t *__restrict__ l2p_off,
+                               const T *__restrict__ near, const double *__restrict__ l2p) {
+    __shared__ int rngs[4][18];
+    pdl_trigger();
+    pdl_wait();
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (w >= nleaf) return;
+    int *rng = rngs[wib];
+    const int g = leaves[w], l = A.nlev[g], b = A.nbot[g], nt = A.ntop[g] - b, Q = A.Q;
+    if (lane == 0) leaf_ranges(A, g, rng);
+    __syncwarp();
+    const int ns = (int)((near_off[w + 1] - near_off[w]) / max(nt, 1));
+    const T *nb = near + near_off[w];
+    const double *lb = l2p + l2p_off[w];
+    const double *u = A.udown + (size_t)g * Q;
+    for (int t0 = 0; t0 < nt; t0 += 32) {
+        const int t = t0 + lane;
+        const bool act = t < nt;
+        double far = 0.0, acc = 0.0;
+        if (act && l >= 2)
+            for (int q = 0; q < Q; q++) far = fma(lb[(size_t)q * nt + t], u[q], far);
+        for (int s0 = 0; s0 < ns; s0 += 32) {
+            const int s1 = min(ns, s0 + 32);
+            // the run's charges: one per lane, then broadcast
+            const int sl = s0 + lane;
+            const double tl = sl < s1 ? A.taus[range_point(rng, sl)] : 0.0;
+            if (sizeof(T) == 4) {
+                float part = 0.f;
+                for (int s = s0; s < s1; s++) {
+                    const float ts = (float)__shfl_sync(0xffffffffu, tl, s - s0);
+                    if (act) part = fmaf((float)nb[(size_t)s * nt + t], ts, part);
+                }
+                acc += (double)part;
+            } else {
+                for (int s = s0; s < s1; s++) {
+                    const double ts = __shfl_sync(0xffffffffu, tl, s - s0);
+                    if (act) acc = fma((double)nb[(size_t)s * nt + t], ts, acc);
+                }
+            }
+        }
+        if (act) A.pots[b + t] = far + acc;
+    }
+}
+
+// ------------------------------------------------------------ host side
+bool planned_ready(const kifmm_plan *P) { return P->opt.planned && P->have_mats; }
+
+void build_plan_matrices(kifmm_plan *P) {
+    if (!P->opt.planned || P->have_mats) return;
+    KIFMM_REQUIRE(!P->cplx, KIFMM_ERR_UNSUPPORTED, "planned applies: real values only");
+    cudaStream_t s = P->stream;
+    const int64_t nl = P->n_leaf_list, np = P->n_p2m_list;
+    PassArgs A = make_pass_args(P);
+    P->pm_near_off.alloc(nl + 1);
+    P->pm_l2p_off.alloc(nl + 1);
+    P->pm_p2m_off.alloc(np + 1);
+    KIFMM_CUDA(cudaMemsetAsync(P->pm_near_off.p, 0, (nl + 1) * 8, s));
+    KIFMM_CUDA(cudaMemsetAsync(P->pm_l2p_off.p, 0, (nl + 1) * 8, s));
+    KIFMM_CUDA(cudaMemsetAsync(P->pm_p2m_off.p, 0, (np + 1) * 8, s));
+    if (nl + np) {
+        k_plan_sizes<<<grid_for(nl + np, 256, P->num_sms * 8), 256, 0, s>>>(
+            A, P->leaf_list.p, nl, P->p2m_list.p, np, P->pm_near_off.p, P->pm_l2p_off.p, P->pm_p2m_off.p);
+        KIFMM_LAUNCHED();
+    }
+    int64_t tot[3];
+    int64_t *offs[3] = {P->pm_near_off.p, P->pm_l2p_off.p, P->pm_p2m_off.p};
+    const int64_t cnt[3] = {nl, nl, np};
+    for (int k = 0; k < 3; k++) {
+        k_plan_scan<<<1, PS_THREADS, 0, s>>>(offs[k], cnt[k]);
+        KIFMM_LAUNCHED();
+        KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_STATS + k, offs[k] + cnt[k], 8, cudaMemcpyDeviceToHost, s));
+    }
+    KIFMM_CUDA(cudaStreamSynchronize(s));
+    for (int k = 0; k < 3; k++) tot[k] = (int64_t)P->hpin[HP_STATS + k];
+    const bool f32 = P->opt.precision == KIFMM_PREC_MIXED;
+    if (f32) P->pm_near32.alloc(tot[0]);
+    else P->pm_near64.alloc(tot[0]);
+    P->pm_l2p.alloc(tot[1]);
+    P->pm_p2m.alloc(tot[2]);
+    if (nl) {
+        if (f32)
+            k_plan_fill_leaf<float><<<(unsigned)nl, 256, 0, s>>>(A, P->leaf_list.p, nl, P->pm_near_off.p,
+                                                                  P->pm_l2p_off.p, P->pm_near32.p, P->pm_l2p.p);
+        else
+            k_plan_fill_leaf<double><<<(unsigned)nl, 256, 0, s>>>(A, P->leaf_list.p, nl, P->pm_near_off.p,
+                                                                   P->pm_l2p_off.p, P->pm_near64.p, P->pm_l2p.p);
+        KIFMM_LAUNCHED();
+    }
+    if (np) {
+        k_plan_fill_p2m<<<(unsigned)np, 256, 0, s>>>(A, P->p2m_list.p, np, P->pm_p2m_off.p, P->pm_p2m.p);
+        KIFMM_LAUNCHED();
+    }
+    P->pm_bytes = (size_t)tot[0] * (f32 ? 4 : 8) + (size_t)(tot[1] + tot[2]) * 8;
+    P->have_mats = true;
+}
+
+void launch_planned_p2m(kifmm_plan *P, const PassArgs &A) {
+    launch_pdl(k_planned_p2m, dim3(grid_for(P->n_p2m_list * 32, 256)), dim3(256), 0, P->stream, A,
+               (const int32_t *)P->p2m_list.p, P->n_p2m_list, (const int64_t *)P->pm_p2m_off.p,
+               (const double *)P->pm_p2m.p);
+}
+
+void launch_planned_leaf(kifmm_plan *P, const PassArgs &A) {
+    const dim3 grid(grid_for(P->n_leaf_list * 32, 128)), block(128);
+    if (P->opt.precision == KIFMM_PREC_MIXED)
+        launch_pdl(k_planned_leaf<float>, grid, block, 0, P->stream, A, (const int32_t *)P->leaf_list.p,
+                   P->n_leaf_list, (const int64_t *)P->pm_near_off.p, (const int64_t *)P->pm_l2p_off.p,
+                   (const float *)P->pm_near32.p, (const double *)P->pm_l2p.p);
+    else
+        launch_pdl(k_planned_leaf<double>, grid, block, 0, P->stream, A, (const int32_t *)P->leaf_list.p,
+                   P->n_leaf_list, (const int64_t *)P->pm_near_off.p, (const int64_t *)P->pm_l2p_off.p,
+                   (const double *)P->pm_near64.p, (const double *)P->pm_l2p.p);
+}
+
+}  // namespace kifmm
