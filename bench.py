@@ -81,11 +81,11 @@ def kernel_obj(cfg):
     return P.LaplaceKernel() if cfg["kernel"] == 0 else P.ModifiedHelmholtzKernel(cfg["k"])
 
 
-def make_fmm(cfg, x, y, precision, stream=None, m2l="auto"):
+def make_fmm(cfg, x, y, precision, stream=None, m2l="auto", planned=False):
     import pykifmm2d_b200 as P
     kern = kernel_obj(cfg)
     return P.FMM(x, y, P.Get_Kernel_Functions(kern), P.prepare_numba_functions_on_the_fly(kern), cfg["neq"],
-                 cfg["cut"], precision=precision, stream=stream, m2l=m2l)
+                 cfg["cut"], precision=precision, stream=stream, m2l=m2l, planned=planned)
 
 
 def sample_targets(n):
@@ -426,6 +426,7 @@ def run_ours(args, cfg, rank, world, dist):
         if args.extra_configs:
             res["c3_forms"] = run_c3_forms(torch, flush)
             res["c4"] = run_c4(torch, flush)
+            res["planned"] = run_planned(torch, flush)
     if rank != 0:
         return None
     pk, pk_src = peaks()
@@ -472,7 +473,7 @@ def run_ours(args, cfg, rank, world, dist):
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
-    for k in ("c3_forms", "c4"):
+    for k in ("c3_forms", "c4", "planned"):
         if k in res:
             line[k] = res[k]
     if args.serve_requests > 0:
@@ -554,6 +555,70 @@ def run_c4(torch, flush):
                            "m2l_pairs": info.n_m2l_pairs}
         del f
     out["mixed_over_plain"] = out["plain_fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"]
+    return out
+
+
+def run_planned(torch, flush, steps=5):
+    """Planned applies (the reference's fmm_planner / planned_fmm): repeated
+    densities on one tree with the P2M, L2P and near-field kernel values kept
+    in HBM, against the same applies on the fly; per workload and precision:
+    the apply (build_expansions + evaluate_to_points at the sources) in ms,
+    the one-time matrix build, the matrices' bytes and the planned leaf
+    kernel's bytes per second against the measured HBM bandwidth."""
+    import pykifmm2d_b200 as P
+    from pykifmm2d_b200 import _lib as B
+    pk, pk_src = peaks()
+    lib = B.load()
+    out = {}
+    for cname in ("c2", "c4"):
+        cfg = CONFIGS[cname]
+        x, y, tau = cfg["gen"](cfg["n"], 0)
+        xd, yd, td = (torch.from_numpy(v).cuda() for v in (x, y, tau))
+        res = {"workload": cfg["desc"]}
+        for precision in ("mixed", "fp64"):
+            line = {}
+            for planned in (False, True):
+                stream = torch.cuda.Stream()
+                f = make_fmm(cfg, xd, yd, precision, stream=stream.cuda_stream, planned=planned)
+                f._bench_stream = stream
+                f.build_tree()
+                f.precompute()
+                o = torch.empty_like(xd)
+                torch.cuda.synchronize()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                f.build_expansions(td)  # planned: builds the matrices
+                f.evaluate_to_points(xd, yd, True, out=o)
+                b.record(stream)
+                torch.cuda.synchronize()
+                first = a.elapsed_time(b)
+                ms = statistics.mean(time_apply_steps(torch, f, xd, yd, td, steps, 2, flush))
+                lib.kifmm_set_profiling(f._plan, 1)
+                f.build_expansions(td)
+                f.evaluate_to_points(xd, yd, True, out=o)
+                ph = np.zeros(len(B.PHASES))
+                lib.kifmm_get_phase_times(f._plan, ph.ctypes.data, None, 1)
+                lib.kifmm_set_profiling(f._plan, 0)
+                ph = dict(zip(B.PHASES, ph))
+                info = f.tree_info()
+                key = "planned" if planned else "on_the_fly"
+                line[key] = {"apply_ms": ms, "mpts_s": x.size / (ms * 1e-3) / 1e6, "first_apply_ms": first,
+                             "leaf_ms": ph["leaf"], "p2m_ms": ph["p2m"]}
+                if planned:
+                    nb = 4 if precision == "mixed" else 8
+                    leaf_bytes = float(info.n_p2p_pairs) * nb + 8.0 * cfg["neq"] * x.size + 24.0 * x.size
+                    ach = leaf_bytes / (ph["leaf"] * 1e-3) / 1e9 if ph["leaf"] > 0 else None
+                    line[key].update({"matrix_bytes": int(info.planned_bytes),
+                                      "roofline_leaf": {"kernel": "k_planned_leaf (L2P + near field as matrices)",
+                                                        "bound": "hbm", "achieved": ach, "peak": pk["hbm_gbs"],
+                                                        "unit": "GB/s", "frac": ach / pk["hbm_gbs"] if ach else None,
+                                                        "work": f"{nb} B per near-field pair + 8 Q B per point "
+                                                                "(L2P block) + charges and potentials",
+                                                        "peak_source": pk_src}})
+                del f
+            line["speedup"] = line["on_the_fly"]["apply_ms"] / line["planned"]["apply_ms"]
+            res[precision] = line
+        out[cname] = res
     return out
 
 

@@ -129,6 +129,7 @@ typedef struct kifmm_tree_info {
     int64_t n_m2l_pairs;     /* V-list (target box, source box) pairs */
     int64_t n_m2l_groups;    /* (target sibling group, parent direction) blocks with a source group */
     int64_t nodes_per_level[KIFMM_MAX_LEVELS];
+    int64_t planned_bytes;   /* device memory of the planned-apply matrices (0 until built) */
 } kifmm_tree_info;
 
 /* Fill *o with the defaults listed above. */

@@ -39,7 +39,7 @@ class TreeInfo(ctypes.Structure):
                 ("n_xlist", ctypes.c_int64), ("n_outside", ctypes.c_int64), ("root_min", ctypes.c_double),
                 ("root_max", ctypes.c_double), ("n_p2p_pairs", ctypes.c_int64), ("n_p2m_points", ctypes.c_int64),
                 ("n_m2l_pairs", ctypes.c_int64), ("n_m2l_groups", ctypes.c_int64),
-                ("nodes_per_level", ctypes.c_int64 * MAX_LEVELS)]
+                ("nodes_per_level", ctypes.c_int64 * MAX_LEVELS), ("planned_bytes", ctypes.c_int64)]
 
 
 class KifmmError(RuntimeError):

@@ -422,6 +422,7 @@ int kifmm_get_tree_info(kifmm_plan *P, kifmm_tree_info *info) {
         info->n_m2l_pairs = P->n_m2l_pairs;
         info->n_m2l_groups = P->n_m2l_groups;
         for (int l = 0; l < P->L && l < KIFMM_MAX_LEVELS; l++) info->nodes_per_level[l] = P->lv[l].n;
+        info->planned_bytes = P->have_mats ? (int64_t)P->pm_bytes : 0;
     });
 }
 

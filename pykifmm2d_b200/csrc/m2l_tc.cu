@@ -424,7 +424,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(TcArgs T) {
             int issued = 0, consumed = 0;
             for (; issued < S && issued < nst; issued++) issue_a(issued);
             const uint32_t idesc = instr_desc<F>();
-            const uint32_t a_lbo = (TC_M / 8) * 128, b_lbo = (TN / 8) * 128;
+            constexpr uint32_t a_lbo = (TC_M / 8) * 128, b_lbo = (TN / 8) * 128;
+            // descriptors of the ring's first slot; an operand's descriptor is that
+            // plus its byte offset / 16 (the start-address field, no carry: smem < 256 KB)
+            const uint64_t adesc0 = umma_desc(smem_u32(sA), a_lbo, 128), bdesc0 = umma_desc(smem_u32(sB), b_lbo, 128);
             bool ok = true;
             for (int st = 0; st < nst; st++) {
                 const int slot = st % S;
@@ -435,18 +438,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(TcArgs T) {
                 }
                 consumed++;
                 fence_after();
-                const uint32_t a0 = smem_u32(sA + slot * A_STAGE), b0 = smem_u32(sB + slot * B_STAGE);
+                const uint64_t as = adesc0 + ((uint64_t)(slot * A_STAGE) >> 4), bs = bdesc0 + ((uint64_t)(slot * B_STAGE) >> 4);
+                const uint32_t later = st != 0;  // the first stage starts every accumulator
 #pragma unroll
                 for (int ks = 0; ks < KSTEPS; ks++) {
 #pragma unroll
                     for (int i = 0; i < NS; i++) {
-                        const int jmax = F == TC_INT8 ? NS - 1 - i : (i == 0 ? 1 : 0);
-                        for (int jj = 0; jj <= jmax; jj++) {
+                        constexpr int JM = F == TC_INT8 ? NS - 1 : 1;
+#pragma unroll
+                        for (int jj = 0; jj <= JM; jj++) {
+                            // int8: the 15 slice pairs with i + j <= 4; f16 forms: hi.hi, hi.lo, lo.hi
+                            if (F == TC_INT8 ? (i + jj > NS - 1) : (i != 0 && jj != 0)) continue;
                             const int acc = F == TC_INT8 ? i + jj : 0;
-                            const bool first = st == 0 && ks == 0 && i == 0 && (F == TC_INT8 || jj == 0);
-                            const uint64_t ad = umma_desc(a0 + i * A_SLICE + ks * 2 * a_lbo, a_lbo, 128);
-                            const uint64_t bd = umma_desc(b0 + jj * B_SLICE + ks * 2 * b_lbo, b_lbo, 128);
-                            mma_issue<F>(tmem + acc * TN, ad, bd, idesc, first ? 0u : 1u);
+                            const bool first_mma = ks == 0 && i == 0 && (F == TC_INT8 || jj == 0);
+                            const uint64_t ad = as + ((uint64_t)(i * A_SLICE + ks * 2 * a_lbo) >> 4);
+                            const uint64_t bd = bs + ((uint64_t)(jj * B_SLICE + ks * 2 * b_lbo) >> 4);
+                            mma_issue<F>(tmem + acc * TN, ad, bd, idesc, first_mma ? later : 1u);
                         }
                     }
                 }
@@ -476,7 +483,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(TcArgs T) {
         // 16-byte cp.async copies, one commit group per stage; a thread arrives
         // on a slot's B-full barrier once its copies of that stage have landed,
         // checked one stage later so that two stages' copies are in flight
-        constexpr int CH = TC_KCB / 16, NP = TN * NS * CH, PER = (NP + 32 * TC_GWARPS - 1) / (32 * TC_GWARPS);
+        // a thread takes (target row j, slice i) pairs and copies the row's CH
+        // 16-byte chunks; j = 8 jb + t8 with t8 the fastest index, so the 8
+        // lanes of a wavefront fill one 128-byte core matrix (no bank conflicts)
+        constexpr int CH = TC_KCB / 16, NP = TN * NS, PER = (NP + 32 * TC_GWARPS - 1) / (32 * TC_GWARPS);
         int gdone = 0;  // stages whose copies this thread issued
         for (int st = 0; st < nst; st++) {
             if (*abort_flag) break;
@@ -489,22 +499,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(TcArgs T) {
                 break;
             }
             const uint32_t sBs = smem_u32(sB + slot * B_STAGE);
-            // element idx: row j = 8 jb + t8, 16-byte chunk c, slice i with t8
-            // fastest, so the 8 lanes of a wavefront fill one 128-byte core
-            // matrix (no bank conflicts); absent sources and slices shifted out
-            // are copied as zeros
+            // absent sources and slices shifted out are copied as zeros
 #pragma unroll
             for (int q = 0; q < PER; q++) {
                 const int idx = tid + q * 32 * TC_GWARPS;
                 if (idx < NP) {
-                    const int t8 = idx & 7, c = (idx >> 3) % CH, jb = (idx / (8 * CH)) % (TN / 8),
-                              i = idx / (8 * CH * (TN / 8)), j = 8 * jb + t8;
+                    const int t8 = idx & 7, jb = (idx >> 3) % (TN / 8), i = idx / TN, j = 8 * jb + t8;
                     const int grp = sgrp[j * 8 + dd], si = i - sshift[j * 8 + dd];
                     const bool has = grp >= 0 && si >= 0 && si < NS;
-                    const unsigned char *src = T.pre.slices + (has ? ((size_t)grp * NS + si) * KP * EB +
-                                                                         (size_t)kc * TC_KCB + c * 16
-                                                                   : 0);
-                    cp_async16(sBs + i * B_SLICE + (c * (TN / 8) + jb) * 128 + t8 * 16, src, has ? 16u : 0u);
+                    const unsigned char *src =
+                        T.pre.slices + (has ? ((size_t)grp * NS + si) * KP * EB + (size_t)kc * TC_KCB : 0);
+                    const uint32_t dst = sBs + i * B_SLICE + jb * 128 + t8 * 16;
+#pragma unroll
+                    for (int c = 0; c < CH; c++)
+                        cp_async16(dst + c * (TN / 8) * 128, src + (has ? c * 16 : 0), has ? 16u : 0u);
                 }
             }
             asm volatile("cp.async.commit_group;" ::: "memory");
@@ -539,12 +547,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(TcArgs T) {
                 for (int s = 0; s < TR::NACC; s++)
                     tmem_ld16_nowait(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * TN + cc * 16), v[s]);
                 tmem_wait_ld();
+                if (F == TC_INT8) {
+                    // accumulator s carries weight 2^-7(s+2): combine exactly in int64
+                    // (|acc| < 2^31, so the sum stays below 2^60), one conversion per column
 #pragma unroll
-                for (int s = 0; s < TR::NACC; s++) {
-                    const double w = F == TC_INT8 ? ldexp(1.0, -7 * (s + 2)) : F == TC_FP16 ? 1.0 / FP16_PRESCALE : 1.0;
+                    for (int c = 0; c < 16; c++) {
+                        long long z = 0;
+#pragma unroll
+                        for (int s = 0; s < TR::NACC; s++) z += (long long)(int32_t)v[s][c] << (7 * (TR::NACC - 1 - s));
+                        y[c] = ldexp((double)z, -7 * (TR::NACC + 1));
+                    }
+                } else {
 #pragma unroll
                     for (int c = 0; c < 16; c++)
-                        y[c] += (F == TC_INT8 ? (double)(int32_t)v[s][c] : (double)__uint_as_float(v[s][c])) * w;
+                        y[c] = (double)__uint_as_float(v[0][c]) * (F == TC_FP16 ? 1.0 / FP16_PRESCALE : 1.0);
                 }
             }
             if (r < Q4)

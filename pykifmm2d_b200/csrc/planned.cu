@@ -10,24 +10,27 @@
 // per-node blocks in HBM, built by the GPU on the first apply after the tree
 // and the operators:
 //   P2M   [n_src x Q] per P2M node:   u_up(g)[q]  = sum_s P[s][q] tau_s;
-//   L2P   [Q x n_t] per leaf (l >= 2), with the check-to-equivalent inverse
-//         folded in: far_t = sum_q L[q][t] u_down(g)[q],
-//         L[q][t] = sum_c G(large_c -> t) Inv[c][q];
-//   near  [n_src x n_t] per leaf over the concatenated sources of its 3x3
-//         colleagues: near_t = sum_s N[s][t] tau_s, pairs with equal
-//         coordinates zero (evaluate_to_points(..., check_self=True),
-//         class_fmm.py:105-108).
-// Each apply then streams the blocks once (HBM-bound matrix-vector products,
-// lanes over the contiguous index).  Values are computed in FP64; the near
-// blocks are stored in FP32 for the mixed precision (no FP32 coordinate
-// differences are involved), in FP64 otherwise.
+//   L2P   [n_t x Q] per leaf (l >= 2), with the check-to-equivalent inverse
+//         folded in: far_t = sum_q L[t][q] u_down(g)[q],
+//         L[t][q] = sum_c G(large_c -> t) Inv[c][q];
+//   near  [n_t x n_s'] per leaf over the concatenated sources of its 3x3
+//         colleagues (rows padded with zeros to 16 bytes):
+//         near_t = sum_s N[t][s] tau_s, pairs with equal coordinates zero
+//         (evaluate_to_points(..., check_self=True), class_fmm.py:105-108).
+// Each apply then streams the blocks once: one CTA per leaf stages the leaf's
+// concatenated charges in shared memory and each warp reduces whole target
+// rows with 16-byte loads (HBM-bound matrix-vector products).  Values are
+// computed in FP64; the near blocks are stored in FP32 for the mixed
+// precision (no FP32 coordinate differences are involved), in FP64 otherwise.
 #include "passes.cuh"
 
 namespace kifmm {
 
 // block sizes of every leaf (near, L2P) and P2M node
+// near rows hold n_s values padded to a multiple of vw (16 bytes)
+__host__ __device__ __forceinline__ int64_t pad_row(int64_t ns, int vw) { return (ns + vw - 1) / vw * vw; }
 __global__ void k_plan_sizes(PassArgs A, const int32_t *__restrict__ leaves, int64_t nleaf,
-                             const int32_t *__restrict__ p2m, int64_t np2m, int64_t *__restrict__ near_sz,
+                             const int32_t *__restrict__ p2m, int64_t np2m, int vw, int64_t *__restrict__ near_sz,
                              int64_t *__restrict__ l2p_sz, int64_t *__restrict__ p2m_sz) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nleaf + np2m;
          i += (int64_t)gridDim.x * blockDim.x) {
@@ -39,7 +42,7 @@ __global__ void k_plan_sizes(PassArgs A, const int32_t *__restrict__ leaves, int
                 const int c = A.ncoll[9 * (size_t)g + d];
                 if (c >= 0) ns += A.ntop[c] - A.nbot[c];
             }
-            near_sz[i] = nt * ns;
+            near_sz[i] = nt * pad_row(ns, vw);
             l2p_sz[i] = A.nlev[g] >= 2 ? (int64_t)A.Q * nt : 0;
         } else {
             const int g = p2m[i - nleaf];
@@ -101,17 +104,22 @@ __global__ void k_plan_fill_leaf(PassArgs A, const int32_t *__restrict__ leaves,
                                  const int64_t *__restrict__ near_off, const int64_t *__restrict__ l2p_off,
                                  T *__restrict__ near, double *__restrict__ l2p) {
     __shared__ int rng[18];
+    __shared__ int s_ns;
     const int64_t i = blockIdx.x;
     if (i >= nleaf) return;
     const int g = leaves[i], l = A.nlev[g], b = A.nbot[g], nt = A.ntop[g] - b, Q = A.Q;
-    if (threadIdx.x == 0) leaf_ranges(A, g, rng);
+    if (threadIdx.x == 0) s_ns = leaf_ranges(A, g, rng);
     __syncthreads();
-    const int ns = (int)((near_off[i + 1] - near_off[i]) / max(nt, 1));
+    const int ns = s_ns, nsp = (int)((near_off[i + 1] - near_off[i]) / max(nt, 1));
     T *nb = near + near_off[i];
-    for (int64_t e = threadIdx.x; e < (int64_t)nt * ns; e += blockDim.x) {
-        const int s = (int)(e / nt), t = (int)(e % nt), sp = range_point(rng, s);
-        const double dx = A.xs[b + t] - A.xs[sp], dy = A.ys[b + t] - A.ys[sp];
-        const double v = (dx == 0.0 && dy == 0.0) ? 0.0 : green_d(A.kind, A.k, dx * dx + dy * dy);
+    for (int64_t e = threadIdx.x; e < (int64_t)nt * nsp; e += blockDim.x) {
+        const int t = (int)(e / nsp), s = (int)(e % nsp);
+        double v = 0.0;
+        if (s < ns) {
+            const int sp = range_point(rng, s);
+            const double dx = A.xs[b + t] - A.xs[sp], dy = A.ys[b + t] - A.ys[sp];
+            v = (dx == 0.0 && dy == 0.0) ? 0.0 : green_d(A.kind, A.k, dx * dx + dy * dy);
+        }
         nb[e] = (T)v;
     }
     if (l < 2) return;
@@ -121,7 +129,7 @@ __global__ void k_plan_fill_leaf(PassArgs A, const int32_t *__restrict__ leaves,
     const double *inv = blk + A.off_inv, *lg = blk + A.off_large;
     double *lb = l2p + l2p_off[i];
     for (int e = threadIdx.x; e < nt * Q; e += blockDim.x) {
-        const int q = e / nt, t = e % nt;
+        const int t = e / Q, q = e % Q;
         const double px = A.xs[b + t] - cx, py = A.ys[b + t] - cy;
         double acc = 0.0;
         for (int c = 0; c < Q; c++) {
@@ -173,53 +181,71 @@ __global__ void k_planned_p2m(PassArgs A, const int32_t *__restrict__ p2m, int64
     }
 }
 
-// planned L2P + near field: one warp per leaf, lanes over its targets; FP32
-// near blocks are summed in FP32 over runs of 32 sources, then in FP64
+// planned L2P + near field: one CTA per leaf.  The leaf's concatenated
+// charges are staged in shared memory (PL_CHUNK at a time), its u_down too;
+// each warp takes whole target rows, lanes over the row with 16-byte loads
+// (FP32 rows: products summed in FP32 per lane, then in FP64 across lanes).
+constexpr int PL_THREADS = 128, PL_CHUNK = 1024;
 template <typename T>
-__global__ void k_planned_leaf(PassArgs A, const int32_t *__restrict__ leaves, int64_t nleaf,
-                               const int64_t *__restrict__ near_off, const int64_t *__restrict__ l2p_off,
-                               const T *__restrict__ near, const double *__restrict__ l2p) {
-    __shared__ int rngs[4][18];
+__global__ void __launch_bounds__(PL_THREADS) k_planned_leaf(PassArgs A, const int32_t *__restrict__ leaves,
+                                                             int64_t nleaf, const int64_t *__restrict__ near_off,
+                                                             const int64_t *__restrict__ l2p_off,
+                                                             const T *__restrict__ near,
+                                                             const double *__restrict__ l2p) {
+    constexpr int VW = 16 / sizeof(T);  // values per 16-byte load
+    extern __shared__ __align__(16) double pl_sm[];
+    T *tch = (T *)pl_sm;                                   // [PL_CHUNK] charges of the chunk
+    double *us = pl_sm + PL_CHUNK;                         // [Q] u_down of the leaf
+    double *acc = us + A.Q;                                // [n_t] per-target sums
+    __shared__ int rng[18];
+    __shared__ int s_ns;
     pdl_trigger();
     pdl_wait();
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int64_t w = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (w >= nleaf) return;
-    int *rng = rngs[wib];
-    const int g = leaves[w], l = A.nlev[g], b = A.nbot[g], nt = A.ntop[g] - b, Q = A.Q;
-    if (lane == 0) leaf_ranges(A, g, rng);
-    __syncwarp();
-    const int ns = (int)((near_off[w + 1] - near_off[w]) / max(nt, 1));
-    const T *nb = near + near_off[w];
-    const double *lb = l2p + l2p_off[w];
-    const double *u = A.udown + (size_t)g * Q;
-    for (int t0 = 0; t0 < nt; t0 += 32) {
-        const int t = t0 + lane;
-        const bool act = t < nt;
-        double far = 0.0, acc = 0.0;
-        if (act && l >= 2)
-            for (int q = 0; q < Q; q++) far = fma(lb[(size_t)q * nt + t], u[q], far);
-        for (int s0 = 0; s0 < ns; s0 += 32) {
-            const int s1 = min(ns, s0 + 32);
-            // the run's charges: one per lane, then broadcast
-            const int sl = s0 + lane;
-            const double tl = sl < s1 ? A.taus[range_point(rng, sl)] : 0.0;
-            if (sizeof(T) == 4) {
-                float part = 0.f;
-                for (int s = s0; s < s1; s++) {
-                    const float ts = (float)__shfl_sync(0xffffffffu, tl, s - s0);
-                    if (act) part = fmaf((float)nb[(size_t)s * nt + t], ts, part);
-                }
-                acc += (double)part;
-            } else {
-                for (int s = s0; s < s1; s++) {
-                    const double ts = __shfl_sync(0xffffffffu, tl, s - s0);
-                    if (act) acc = fma((double)nb[(size_t)s * nt + t], ts, acc);
+    const int64_t i = blockIdx.x;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nw = PL_THREADS / 32;
+    const int g = leaves[i], l = A.nlev[g], b = A.nbot[g], nt = A.ntop[g] - b, Q = A.Q;
+    if (tid == 0) s_ns = leaf_ranges(A, g, rng);
+    for (int q = tid; q < Q; q += PL_THREADS) us[q] = l >= 2 ? A.udown[(size_t)g * Q + q] : 0.0;
+    __syncthreads();
+    const int ns = s_ns, nsp = (int)((near_off[i + 1] - near_off[i]) / max(nt, 1));
+    // far field: L2P rows
+    const double *lb = l2p + l2p_off[i];
+    for (int t = warp; t < nt; t += nw) {
+        double f = 0.0;
+        if (l >= 2)
+            for (int q = lane; q < Q; q += 32) f = fma(lb[(size_t)t * Q + q], us[q], f);
+        for (int o = 16; o; o >>= 1) f += __shfl_xor_sync(0xffffffffu, f, o);
+        if (lane == 0) acc[t] = f;
+    }
+    const T *nb = near + near_off[i];
+    for (int c0 = 0; c0 < nsp; c0 += PL_CHUNK) {
+        const int cn = min(PL_CHUNK, nsp - c0);  // a multiple of VW
+        __syncthreads();
+        for (int s = tid; s < cn; s += PL_THREADS)
+            tch[s] = c0 + s < ns ? (T)A.taus[range_point(rng, c0 + s)] : (T)0;
+        __syncthreads();
+        for (int t = warp; t < nt; t += nw) {
+            const T *row = nb + (size_t)t * nsp + c0;
+            T part = 0;
+#pragma unroll 2
+            for (int s = lane * VW; s < cn; s += 32 * VW) {
+                if (VW == 4) {
+                    const float4 m = *(const float4 *)(row + s);
+                    const float4 v = *(const float4 *)(tch + s);
+                    part = fmaf(m.x, v.x, fmaf(m.y, v.y, fmaf(m.z, v.z, fmaf(m.w, v.w, part))));
+                } else {
+                    const double2 m = *(const double2 *)(row + s);
+                    const double2 v = *(const double2 *)(tch + s);
+                    part = fma(m.x, v.x, fma(m.y, v.y, part));
                 }
             }
+            double d = (double)part;
+            for (int o = 16; o; o >>= 1) d += __shfl_xor_sync(0xffffffffu, d, o);
+            if (lane == 0) acc[t] += d;
         }
-        if (act) A.pots[b + t] = far + acc;
     }
+    __syncthreads();
+    for (int t = tid; t < nt; t += PL_THREADS) A.pots[b + t] = acc[t];
 }
 
 // ------------------------------------------------------------ host side
@@ -239,7 +265,8 @@ void build_plan_matrices(kifmm_plan *P) {
     KIFMM_CUDA(cudaMemsetAsync(P->pm_p2m_off.p, 0, (np + 1) * 8, s));
     if (nl + np) {
         k_plan_sizes<<<grid_for(nl + np, 256, P->num_sms * 8), 256, 0, s>>>(
-            A, P->leaf_list.p, nl, P->p2m_list.p, np, P->pm_near_off.p, P->pm_l2p_off.p, P->pm_p2m_off.p);
+            A, P->leaf_list.p, nl, P->p2m_list.p, np, P->opt.precision == KIFMM_PREC_MIXED ? 4 : 2,
+            P->pm_near_off.p, P->pm_l2p_off.p, P->pm_p2m_off.p);
         KIFMM_LAUNCHED();
     }
     int64_t tot[3];
@@ -281,15 +308,19 @@ void launch_planned_p2m(kifmm_plan *P, const PassArgs &A) {
 }
 
 void launch_planned_leaf(kifmm_plan *P, const PassArgs &A) {
-    const dim3 grid(grid_for(P->n_leaf_list * 32, 128)), block(128);
-    if (P->opt.precision == KIFMM_PREC_MIXED)
-        launch_pdl(k_planned_leaf<float>, grid, block, 0, P->stream, A, (const int32_t *)P->leaf_list.p,
+    const dim3 grid((unsigned)P->n_leaf_list), block(PL_THREADS);
+    const size_t smem = (size_t)(PL_CHUNK + P->Q + P->ppl) * sizeof(double);  // leaves hold <= Ncutoff points
+    if (P->opt.precision == KIFMM_PREC_MIXED) {
+        ensure_dyn_smem(k_planned_leaf<float>, smem);
+        launch_pdl(k_planned_leaf<float>, grid, block, smem, P->stream, A, (const int32_t *)P->leaf_list.p,
                    P->n_leaf_list, (const int64_t *)P->pm_near_off.p, (const int64_t *)P->pm_l2p_off.p,
                    (const float *)P->pm_near32.p, (const double *)P->pm_l2p.p);
-    else
-        launch_pdl(k_planned_leaf<double>, grid, block, 0, P->stream, A, (const int32_t *)P->leaf_list.p,
+    } else {
+        ensure_dyn_smem(k_planned_leaf<double>, smem);
+        launch_pdl(k_planned_leaf<double>, grid, block, smem, P->stream, A, (const int32_t *)P->leaf_list.p,
                    P->n_leaf_list, (const int64_t *)P->pm_near_off.p, (const int64_t *)P->pm_l2p_off.p,
                    (const double *)P->pm_near64.p, (const double *)P->pm_l2p.p);
+    }
 }
 
 }  // namespace kifmm
