@@ -182,6 +182,7 @@ struct kifmm_plan {
     kifmm::DBuf<int32_t> nparent, nchild, nent;  // parent, first child, own entry
     kifmm::DBuf<int32_t> ncoll;      // [n_nodes][9] colleagues by direction (dx+1)*3+(dy+1)
     kifmm::DBuf<int32_t> leaf_list, p2m_list;
+    kifmm::DBuf<int32_t> leaf_rec;   // [n_leaf_list][32] leaf records (passes.cuh, LeafRec)
     kifmm::DBuf<uint32_t> list_tiles;
     int64_t n_leaf_list = 0, n_p2m_list = 0;
     int64_t leaf_loff[KIFMM_MAX_LEVELS + 1] = {};  // leaf_list range of each level

@@ -482,9 +482,38 @@ PassArgs make_pass_args(kifmm_plan *P) {
     A.pots = P->pots.p;
     A.uup = P->uup.p;
     A.udown = P->udown.p;
+    A.leaf_rec = P->leaf_rec.p;
     A.taylor = P->l2p_taylor.p;
     A.leaf_coef = P->leaf_coef.p;
     return A;
+}
+
+__global__ void k_leaf_records(PassArgs A, const int32_t *__restrict__ leaves, int64_t n, int32_t *__restrict__ rec) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const int g = leaves[i];
+        int r[LEAF_REC_WORDS] = {};
+        r[LR_NODE] = g;
+        r[LR_LEVEL] = A.nlev[g];
+        r[LR_BOT] = A.nbot[g];
+        r[LR_TOP] = A.ntop[g];
+        const uint64_t k = A.nkey[g];
+        r[LR_KEY_LO] = (int32_t)(uint32_t)k;
+        r[LR_KEY_HI] = (int32_t)(uint32_t)(k >> 32);
+        r[LR_NSRC] = leaf_ranges(A, g, r + LR_RNG);
+        int4 *o = (int4 *)(rec + i * LEAF_REC_WORDS);
+#pragma unroll
+        for (int q = 0; q < LEAF_REC_WORDS / 4; q++) o[q] = make_int4(r[4 * q], r[4 * q + 1], r[4 * q + 2], r[4 * q + 3]);
+    }
+}
+
+// the leaf records of the plan's leaf list (part of the tree build)
+void build_leaf_records(kifmm_plan *P) {
+    P->leaf_rec.alloc((size_t)(P->n_leaf_list ? P->n_leaf_list : 1) * LEAF_REC_WORDS);
+    if (!P->n_leaf_list) return;
+    PassArgs A = make_pass_args(P);
+    k_leaf_records<<<grid_for(P->n_leaf_list, 128, P->num_sms * 8), 128, 0, P->stream>>>(
+        A, P->leaf_list.p, P->n_leaf_list, P->leaf_rec.p);
+    KIFMM_LAUNCHED();
 }
 
 void launch_p2m_d(kifmm_plan *P, const PassArgs &A) {

@@ -22,6 +22,7 @@ struct PassArgs {
     const double *xs, *ys, *taus;
     double *pots;
     double *uup, *udown;
+    const int32_t *leaf_rec;  // [n_leaf_list][LEAF_REC_WORDS] leaf records (build_leaf_records)
     const double *taylor;  // Laplace L2P coefficients map, or null
     const double *leaf_coef;  // [leaf_list index][2p+1] Taylor coefficients of the leaves (mixed form)
 };
@@ -36,6 +37,38 @@ __device__ __forceinline__ void node_center(const PassArgs &A, int g, int l, dou
 }
 
 PassArgs make_pass_args(kifmm_plan *P);
+
+// The near-field sources of leaf g: the leaf itself first, then its
+// colleagues in direction order, as one list; rng[0..9) is the first list
+// position of each range, rng[9..18) the point index minus the list position.
+__device__ __forceinline__ int leaf_ranges(const PassArgs &A, int g, int *rng) {
+    int ns = 0;
+    for (int i = 0; i < 9; i++) {
+        const int d = i <= 4 ? i - 1 : i;
+        const int c = i == 0 ? g : A.ncoll[9 * (size_t)g + d];
+        const int rb = c >= 0 ? A.nbot[c] : 0, rn = c >= 0 ? A.ntop[c] - rb : 0;
+        rng[i] = ns;
+        rng[9 + i] = rb - ns;
+        ns += rn;
+    }
+    return ns;
+}
+// point index of list position p
+__device__ __forceinline__ int range_point(const int *rng, int p) {
+    int sv = p + rng[9];
+#pragma unroll
+    for (int i = 1; i < 9; i++) sv = p >= rng[i] ? p + rng[9 + i] : sv;
+    return sv;
+}
+// Leaf record (one 128-byte row per entry of the leaf list, built with the
+// tree): everything a leaf kernel needs before it gathers, in one coalesced
+// warp load instead of the chain list -> node -> colleagues -> their ranges.
+enum LeafRec : int {
+    LR_NODE = 0, LR_LEVEL = 1, LR_BOT = 2, LR_TOP = 3, LR_NSRC = 4, LR_KEY_LO = 5, LR_KEY_HI = 6,
+    LR_RNG = 8,  // [LR_RNG, LR_RNG + 18): the leaf_ranges table
+    LEAF_REC_WORDS = 32
+};
+void build_leaf_records(kifmm_plan *P);
 
 // FP64 tensor-core MMA (mma.sync m8n8k4 .f64): D = A B + D with fragments
 // A[row = lane/4][k = lane%4], B[k = lane%4][n = lane/4],

@@ -221,8 +221,17 @@ __global__ void __launch_bounds__(TY_THREADS) k_leaf_taylor(TaylorArgs T) {
 // one warp per block: leaves differ in work by more than 10x, and a block of
 // several warps would hold its SM slot until its slowest warp is done
 constexpr int LEAF_WARPS = 1;
-constexpr int LEAF_BLOCKS_PER_SM = 20;  // resident blocks per SM at the register bound below
-constexpr int LEAF_CHUNK = 256;
+// 28 one-warp blocks per SM (72 registers) with 128-source chunks measured
+// 8% faster than 20 blocks (96 registers) with 256-source chunks on the 1M
+// mixture; shared memory per block sets the ceiling near 32
+#ifndef KIFMM_LEAF_BLOCKS_PER_SM
+#define KIFMM_LEAF_BLOCKS_PER_SM 28
+#endif
+#ifndef KIFMM_LEAF_CHUNK
+#define KIFMM_LEAF_CHUNK 128
+#endif
+constexpr int LEAF_BLOCKS_PER_SM = KIFMM_LEAF_BLOCKS_PER_SM;  // resident blocks per SM at the register bound
+constexpr int LEAF_CHUNK = KIFMM_LEAF_CHUNK;                  // sources staged per pass
 
 __device__ __forceinline__ float lg2_ftz(float x) {
     float y;
@@ -259,10 +268,19 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, LEAF_BLOCKS_PER_SM) k_leaf_ev
     // one warp per leaf (grid-stride only if the grid were capped)
     const int64_t wstride = (int64_t)gridDim.x * LEAF_WARPS;
     for (int64_t w = (int64_t)blockIdx.x * LEAF_WARPS + wib; w < nlist; w += wstride) {
-        const int g = list[w];
-        const int l = A.nlev[g];
+        // the leaf record: node, level, point range, cell key and source ranges
+        // in one coalesced load (list[w] is the record's node)
+        const int rv = A.leaf_rec[w * LEAF_REC_WORDS + lane];
+        const int g = __shfl_sync(0xffffffffu, rv, LR_NODE);
+        const int l = __shfl_sync(0xffffffffu, rv, LR_LEVEL);
+        const uint64_t key = (uint64_t)(uint32_t)__shfl_sync(0xffffffffu, rv, LR_KEY_LO) |
+                             ((uint64_t)(uint32_t)__shfl_sync(0xffffffffu, rv, LR_KEY_HI) << 32);
         double cx, cy;
-        node_center(A, g, l, cx, cy);
+        {
+            const double wl = ldexp(A.W, -l);
+            cx = A.root + ((double)compact2(key >> 1) + 0.5) * wl;
+            cy = A.root + ((double)compact2(key) + 0.5) * wl;
+        }
         const bool lap = KIND == KIFMM_KERNEL_LAPLACE;
         const bool taylor = lap && A.taylor != nullptr && l >= 2;
         double *qd = qds[wib];
@@ -283,26 +301,14 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, LEAF_BLOCKS_PER_SM) k_leaf_ev
         }
         const float kk = (float)A.k;
         const float lclamp = lg2_ftz(CLAMP);
-        const int b = A.nbot[g], e = A.ntop[g];
+        const int b = __shfl_sync(0xffffffffu, rv, LR_BOT), e = __shfl_sync(0xffffffffu, rv, LR_TOP);
+        const int ns = __shfl_sync(0xffffffffu, rv, LR_NSRC);
         // source ranges: the leaf itself, then its colleagues in direction order;
         // list element p lies in the last range i with pre[i] <= p, at p + off[i]
         // (kept in shared memory: registers are scarce in the pair loop)
         int *rng = rngs[wib];
-        int ns = 0;
-        if (lane < 9) {
-            const int d = lane <= 4 ? lane - 1 : lane;
-            const int c = lane == 0 ? g : A.ncoll[9 * (size_t)g + d];
-            const int rb = c >= 0 ? A.nbot[c] : 0, rn = c >= 0 ? A.ntop[c] - rb : 0;
-            int x = rn;  // inclusive prefix over lanes 0..8
-            for (int o = 1; o < 16; o <<= 1) {
-                const int y = __shfl_up_sync(0x1ffu, x, o);
-                if (lane >= o) x += y;
-            }
-            rng[lane] = x - rn;
-            rng[9 + lane] = rb - (x - rn);
-            ns = x;
-        }
-        ns = __shfl_sync(0xffffffffu, ns, 8);
+        if (lane >= LR_RNG && lane < LR_RNG + 18) rng[lane - LR_RNG] = rv;
+        (void)list;
         double tsum = 0.0;  // FP64 sum of the near sources' charges (Laplace)
         // stage sources [c0, c0 + cn) of the list, padded with 32 far, uncharged
         // ones; four elements per lane per pass, loads issued before any is used

@@ -78,27 +78,6 @@ __global__ void __launch_bounds__(PS_THREADS) k_plan_scan(int64_t *v, int64_t n)
     }
 }
 
-// the leaf's source ranges: the leaf itself first, then its colleagues in
-// direction order (rng[0..9): first list position, rng[9..18): point offset)
-__device__ __forceinline__ int leaf_ranges(const PassArgs &A, int g, int *rng) {
-    int ns = 0;
-    for (int i = 0; i < 9; i++) {
-        const int d = i <= 4 ? i - 1 : i;
-        const int c = i == 0 ? g : A.ncoll[9 * (size_t)g + d];
-        const int rb = c >= 0 ? A.nbot[c] : 0, rn = c >= 0 ? A.ntop[c] - rb : 0;
-        rng[i] = ns;
-        rng[9 + i] = rb - ns;
-        ns += rn;
-    }
-    return ns;
-}
-__device__ __forceinline__ int range_point(const int *rng, int p) {
-    int sv = p + rng[9];
-#pragma unroll
-    for (int i = 1; i < 9; i++) sv = p >= rng[i] ? p + rng[9 + i] : sv;
-    return sv;
-}
-
 template <typename T>
 __global__ void k_plan_fill_leaf(PassArgs A, const int32_t *__restrict__ leaves, int64_t nleaf,
                                  const int64_t *__restrict__ near_off, const int64_t *__restrict__ l2p_off,

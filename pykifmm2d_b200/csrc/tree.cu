@@ -30,6 +30,10 @@
 #include "kifmm_internal.cuh"
 
 namespace kifmm {
+void build_leaf_records(kifmm_plan *P);  // passes.cu
+}
+
+namespace kifmm {
 
 constexpr uint64_t KEY56 = (1ull << 56) - 1;
 
@@ -1066,6 +1070,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     P->n_fake = (int64_t)c5[3];
     P->n_xlist = (int64_t)c5[4];
     P->have_stats = false;
+    build_leaf_records(P);
     P->have_tree = true;
 }
 
