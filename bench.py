@@ -480,6 +480,7 @@ def run_ours(args, cfg, rank, world, dist):
         line["serving"] = run_serving(args, dev)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, x, y, tau, repeats=3)
+        line["cpu_baseline_numba_reference"] = numba_reference_baseline(cfg, x, y, tau)
     return line
 
 
@@ -684,6 +685,40 @@ def cpu_baseline(cfg, x, y, tau, repeats=3, threads=None):
         pass
     return {"value": x.size / med / 1e6, "unit": "Mpts/s", "cores": nthr, "kind": "port",
             "sample": f"full workload ({x.size} points), median of {repeats} runs, {med:.2f} s each; CPU: {cpu}"}
+
+
+def numba_reference_baseline(cfg, x, y, tau, repeats=2):
+    """The reference's own numba path (class_fmm.FMM with its i8[4] import
+    shim) from baseline/_ref, timed on all host cores in a subprocess; a second
+    CPU number beside the oracle port (which stays the reference arm)."""
+    ref = os.path.join(ROOT, "baseline", "_ref", "pykifmm2d", "class_fmm.py")
+    if not os.path.exists(ref):
+        return {"unavailable": "baseline/_ref (pip install of the reference) is not present"}
+    if cfg["kernel"] != 0:
+        return {"unavailable": "timed for the Laplace workload only"}
+    try:
+        import numba  # noqa: F401
+    except Exception:
+        return {"unavailable": "numba is not importable on this host"}
+    fd, path = tempfile.mkstemp(suffix=".npz")
+    os.close(fd)
+    try:
+        np.savez(path, x=x, y=y, tau=tau)
+        env = dict(os.environ, NUMBA_NUM_THREADS=str(os.cpu_count()))
+        out = subprocess.run([sys.executable, os.path.join(ROOT, "oracle", "run_reference_numba.py"), path,
+                              str(cfg["neq"]), str(cfg["cut"]), str(repeats)], capture_output=True, text=True,
+                             env=env, timeout=900)
+        line = [l for l in out.stdout.splitlines() if l.startswith("{")]
+        if not line:
+            return {"unavailable": "reference run failed: " + out.stderr.strip()[-300:]}
+        d = json.loads(line[-1])
+    finally:
+        os.unlink(path)
+    return {"value": x.size / d["seconds"] / 1e6, "unit": "Mpts/s", "cores": d["threads"], "kind": "reference",
+            "sample": f"the reference's class_fmm.FMM (numba {d['numba']}, import shim i8[4] -> i8[:]) on the full "
+                      f"workload ({x.size} points), build_tree + precompute + build_expansions + "
+                      f"evaluate_to_points(check_self), JIT warmed on 5,000 points, median of {len(d['runs'])} runs "
+                      f"({d['seconds']:.2f} s each)"}
 
 
 def run_reference(args, cfg):
