@@ -636,21 +636,41 @@ def run_serving(args, device):
     _, cap = srv.run(S.make_stream(args.serve_requests, 0.0, seed=0), realtime=False)
     rate = 0.7 * cap["requests_per_s"]
     _, st = srv.run(S.make_stream(args.serve_requests, rate, seed=0), realtime=True)
+    srv.close()
     out = {
         "requests": st["requests"], "failed": st["failed"] + cap["failed"],
         "mix": "70% Laplace / 30% K0 (k in {1,10,50}), N log-uniform in [1e3, 3e5] (mixture + circle points), "
                "8-32 fresh N(0,1) densities per request (drawn on the device), Nequiv 32, Ncutoff 64",
         "batched_mixed": {"precision": "mixed", "slots": st["slots"], "graphs": True,
-                          "capacity_requests_per_s": cap["requests_per_s"], "offered_requests_per_s": rate,
+                          "capacity_requests_per_s": cap["requests_per_s"],
+                          "capacity_mpts_s": cap["point_applies_per_s"] / 1e6, "offered_requests_per_s": rate,
                           "offered_load": 0.7, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
                           "mean_ms": st["mean_ms"], "point_applies_per_s": st["point_applies_per_s"],
                           "mpts_s": st["point_applies_per_s"] / 1e6, "wall_s": st["wall_s"]},
         "hbm_budget_bytes": st["hbm_budget_bytes"],
     }
+    if args.serve_packed_slots > 0:
+        # the same requests and arrival times through the packed batches: every
+        # step one graph launch over all admitted requests, their M2L in one
+        # tensor-core launch and their near fields in one launch per kernel kind
+        pk = S.Server(device=device, slots=args.serve_packed_slots, keep_pots=False, packed=True)
+        pk.run(S.make_stream(4, 0.0, seed=99, nmax=20_000, applies=(2, 2)), realtime=False)  # warm-up
+        _, pcap = pk.run(S.make_stream(args.serve_requests, 0.0, seed=0), realtime=False)
+        _, ps = pk.run(S.make_stream(args.serve_requests, rate, seed=0), realtime=True)
+        pk.close()
+        out["failed"] += pcap["failed"] + ps["failed"]
+        out["packed_mixed"] = {"precision": "mixed", "slots": ps["slots"], "graphs": True, "packed": True,
+                               "capacity_requests_per_s": pcap["requests_per_s"],
+                               "capacity_mpts_s": pcap["point_applies_per_s"] / 1e6,
+                               "offered_requests_per_s": rate, "p50_ms": ps["p50_ms"], "p99_ms": ps["p99_ms"],
+                               "mean_ms": ps["mean_ms"], "mpts_s": ps["point_applies_per_s"] / 1e6,
+                               "wall_s": ps["wall_s"], "steps": ps["steps"], "captures": ps["captures"],
+                               "mean_batch": ps["mean_batch"]}
     if args.serve_plain:
         # the same requests and arrival times, one at a time, plain FP64, no graphs
         plain = S.Server(device=device, slots=1, keep_pots=False, precision="fp64", graphs=False)
         _, sp = plain.run(S.make_stream(args.serve_requests, rate, seed=0), realtime=True)
+        plain.close()
         out["failed"] += sp["failed"]
         out["one_at_a_time_plain"] = {"precision": "fp64", "slots": 1, "graphs": False,
                                       "offered_requests_per_s": rate, "p50_ms": sp["p50_ms"],
@@ -768,7 +788,10 @@ def main():
     ap.add_argument("--n", type=int, default=0, help="override the number of points (profiling small cases)")
     ap.add_argument("--serve-requests", type=int, default=1024,
                     help="requests in the serving stream (0 skips it)")
-    ap.add_argument("--serve-slots", type=int, default=8, help="concurrent requests in the serving stream")
+    ap.add_argument("--serve-slots", type=int, default=32,
+                    help="concurrent requests in the serving stream (one stream and graph each)")
+    ap.add_argument("--serve-packed-slots", type=int, default=64,
+                    help="requests per packed batch in the packed serving run (0 skips it)")
     ap.add_argument("--no-serve-plain", dest="serve_plain", action="store_false",
                     help="skip the one-at-a-time plain-FP64 run of the serving stream")
     ap.add_argument("--no-extra-configs", dest="extra_configs", action="store_false",

@@ -183,6 +183,55 @@ int kifmm_synchronize(kifmm_plan *plan);
 int kifmm_graph_capture(kifmm_plan *plan, const double *tau_dev, double *pot_dev, int32_t check_self);
 int kifmm_graph_launch(kifmm_plan *plan);
 
+/* Packed applies of several plans (a serving batch): the same pair as
+ * kifmm_graph_capture for plans[0..nplan), with the M2L of all plans in ONE
+ * tensor-core launch and the near field + L2P of all plans in one launch per
+ * kernel kind; the per-plan passes (P2M, M2M, L2L, gathers) run as parallel
+ * branches of the graph.  Each plan's result is the same as its own apply
+ * (the packed kernels run the same per-tile / per-leaf code on that plan's
+ * data).  kifmm_batch_capture first runs one normal apply
+ * (tau_dev[r] -> pot_dev[r]) of every plan that has not evaluated at its
+ * sources since its tree and operators were built (that allocates the apply
+ * buffers), then captures the packed graph without running it; each
+ * kifmm_batch_launch computes every plan's apply from tau_dev[r] as it is
+ * when the launch runs.  stream is the caller's created cudaStream_t on which
+ * the capture and every launch are ordered.  Requirements: every plan precomputed, on
+ * one device, distinct, in the mixed precision form with a tensor-core M2L
+ * (one form for all), no near_fp64, planned or complex option; Laplace and
+ * modified-Helmholtz plans may be mixed.  The plans must outlive the batch and
+ * must not be rebuilt while it exists.  A batch holds the wait budget of its
+ * plans at capture.  kifmm_batch_synchronize waits for the stream and reports
+ * device-side failures of any plan as KIFMM_ERR_CUDA. */
+typedef struct kifmm_batch kifmm_batch;
+int kifmm_batch_capture(kifmm_plan *const *plans, int32_t nplan, const double *const *tau_dev,
+                        double *const *pot_dev, int32_t check_self, void *stream, kifmm_batch **batch_out);
+int kifmm_batch_launch(kifmm_batch *batch);
+int kifmm_batch_synchronize(kifmm_batch *batch);
+/* Densities drawn by the batch itself: before the next kifmm_batch_launch,
+ * lane r gets tau_dev[r] = N(0,1) density number index[r] of seed seed[r]
+ * (the values of kifmm_fill_normal(tau_dev[r], n_r, seed[r], index[r])), drawn
+ * by the graph's first kernel; seed[r] = UINT64_MAX leaves tau_dev[r] as the
+ * caller wrote it.  The setting holds for later launches until changed. */
+int kifmm_batch_set_draws(kifmm_batch *batch, const uint64_t *seed, const uint64_t *index);
+/* After kifmm_batch_synchronize: sums[r] = sum of pot_dev[r] of the last launch
+ * (summed on the device by the graph's last kernel, in a fixed order). */
+int kifmm_batch_sums(kifmm_batch *batch, double *sums);
+/* Tiles of the packed M2L launch and leaves of the packed leaf launches. */
+int kifmm_batch_info(kifmm_batch *batch, int64_t *m2l_tiles, int64_t *leaves);
+int kifmm_batch_destroy(kifmm_batch *batch);
+
+/* A new non-blocking cudaStream_t on `device` (for hosts without a CUDA
+ * runtime binding of their own, e.g. a server that needs streams no other
+ * library hands out), and its release. */
+int kifmm_stream_create(int32_t device, void **stream);
+int kifmm_stream_destroy(void *stream);
+
+/* out[0..n) = N(0,1) density number `index` of stream `seed` (seed != UINT64_MAX),
+ * from a counter-based generator (Philox4x32-10 + Box-Muller): the values
+ * depend only on (seed, index, position), not on the launch that draws them.
+ * out is a device pointer; work is ordered on the cudaStream_t `stream`. */
+int kifmm_fill_normal(double *out, int64_t n, uint64_t seed, uint64_t index, void *stream);
+
 /* Tree statistics (reference Tree.levels, Level.n_node, ...). */
 int kifmm_get_tree_info(kifmm_plan *plan, kifmm_tree_info *info);
 

@@ -62,6 +62,16 @@ _SIGS = {
     "kifmm_synchronize": (_i32, [_vp]),
     "kifmm_graph_capture": (_i32, [_vp, _vp, _vp, _i32]),
     "kifmm_graph_launch": (_i32, [_vp]),
+    "kifmm_batch_capture": (_i32, [_vp, _i32, _vp, _vp, _i32, _vp, ctypes.POINTER(_vp)]),
+    "kifmm_batch_launch": (_i32, [_vp]),
+    "kifmm_batch_synchronize": (_i32, [_vp]),
+    "kifmm_batch_info": (_i32, [_vp, _vp, _vp]),
+    "kifmm_batch_destroy": (_i32, [_vp]),
+    "kifmm_batch_set_draws": (_i32, [_vp, _vp, _vp]),
+    "kifmm_batch_sums": (_i32, [_vp, _vp]),
+    "kifmm_stream_create": (_i32, [_i32, ctypes.POINTER(_vp)]),
+    "kifmm_stream_destroy": (_i32, [_vp]),
+    "kifmm_fill_normal": (_i32, [_vp, _i64, ctypes.c_uint64, ctypes.c_uint64, _vp]),
     "kifmm_get_tree_info": (_i32, [_vp, ctypes.POINTER(TreeInfo)]),
     "kifmm_export_tree": (_i32, [_vp, _vp, _vp]),
     "kifmm_export_lists": (_i32, [_vp, _vp, _vp, _vp, _vp, _vp]),

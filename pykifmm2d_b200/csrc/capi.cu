@@ -1,11 +1,13 @@
 // capi.cu -- the extern "C" entry points declared in include/kifmm2d.h.
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <vector>
 
 #include "kifmm_internal.cuh"
+#include "passes.cuh"
 
 namespace kifmm {
 
@@ -187,9 +189,72 @@ struct TempCtx {
     }
 };
 
+// serving batches: phases of the mixed apply (passes.cu, passes_mixed.cu)
+// and the packed launches (m2l_tc.cu, passes_mixed.cu)
+void apply_prologue(kifmm_plan *P);
+void mixed_upward(kifmm_plan *P, const PassArgs &A);
+void mixed_l2l(kifmm_plan *P, const PassArgs &A);
+PassArgs mixed_leaf_args(kifmm_plan *P);
+void launch_scatter_pot(kifmm_plan *P);
+void launch_leaf_f_batch(int kind, const PassArgs *dargs, const int64_t *doff, int nplan, int64_t nleaf,
+                         cudaStream_t s);
+bool uses_tensor_m2l(const kifmm_plan *P);
+int tc_form(const kifmm_plan *P);
+size_t tc_args_bytes();
+int64_t tc_prepare_batch(kifmm_plan *P, const PassArgs &A, void *args);
+void launch_m2l_tc_batch(int form, const void *dargs, const int64_t *doff, int nplan, int64_t tiles,
+                         cudaStream_t s);
+// draws.cu
+void launch_fill_normal(double *out, int64_t n, uint64_t seed, uint64_t index, cudaStream_t s);
+void launch_fill_lanes(const void *dlanes, int nlanes, int64_t nmax, cudaStream_t s);
+void launch_lane_sums(const void *dlanes, int nlanes, double *sums, cudaStream_t s);
+size_t draw_lane_bytes();
+void set_draw_lane(void *lanes, int r, double *out, int64_t n, uint64_t seed, uint64_t index);
+void set_draw_seed(void *lanes, int r, uint64_t seed, uint64_t index);
+constexpr uint64_t kDrawSkipSeed = ~0ull;
+
 }  // namespace kifmm
 
 using namespace kifmm;
+
+// A packed apply of several plans, captured as one CUDA graph
+// (kifmm_batch_capture).  The device tables hold the per-plan arguments of
+// the two packed launches and the prefix sums of their work items.
+struct kifmm_batch {
+    std::vector<kifmm_plan *> plans;
+    int device = 0;
+    cudaStream_t stream = nullptr;      // the caller's stream
+    std::vector<cudaStream_t> branch;   // one per plan
+    std::vector<cudaEvent_t> ev;        // one per plan, then the fork event
+    unsigned char *d_tc = nullptr;      // [nplan] M2L arguments
+    int64_t *d_tc_off = nullptr;        // [nplan + 1] first tile of each plan
+    PassArgs *d_leaf[2] = {};           // per kernel kind: leaf-pass arguments
+    int64_t *d_leaf_off[2] = {};        // and the first leaf of each plan
+    int64_t tiles = 0, leaves = 0;
+    std::vector<unsigned char> h_draw;  // [nplan] density draws of the next launch (host copy)
+    unsigned char *d_draw = nullptr;    // the same on the device, read by the graph's first kernel
+    unsigned char *d_sumlane = nullptr; // [nplan] (pot_dev, n): the lanes summed by the last kernel
+    double *d_sums = nullptr;           // [nplan] sums of the last launch
+    double *h_sums = nullptr;           // pinned copy (kifmm_batch_synchronize)
+    int64_t nmax = 0;
+    cudaGraphExec_t graph = nullptr;
+    ~kifmm_batch() {
+        cudaSetDevice(device);
+        if (graph) cudaGraphExecDestroy(graph);
+        cudaFree(d_draw);
+        cudaFree(d_sumlane);
+        cudaFree(d_sums);
+        if (h_sums) cudaFreeHost(h_sums);
+        for (auto s : branch) cudaStreamDestroy(s);
+        for (auto e : ev) cudaEventDestroy(e);
+        cudaFree(d_tc);
+        cudaFree(d_tc_off);
+        for (int k = 0; k < 2; k++) {
+            cudaFree(d_leaf[k]);
+            cudaFree(d_leaf_off[k]);
+        }
+    }
+};
 
 extern "C" {
 
@@ -274,6 +339,7 @@ int kifmm_build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n,
         use_device(P);
         PhaseScope ph(P, KIFMM_PHASE_TREE);
         P->have_mats = false;
+        P->applied = false;
         build_tree(P, x, y, n, mem);
     });
 }
@@ -286,6 +352,7 @@ int kifmm_precompute(kifmm_plan *P) {
         KIFMM_REQUIRE(P->have_tree, KIFMM_ERR_STATE, "precompute: build_tree first");
         drop_graph(P);
         P->have_mats = false;
+        P->applied = false;
         if (P->ops_pending) join_operators(P);  // started by build_tree
         else build_operators(P);
     });
@@ -310,6 +377,7 @@ int kifmm_evaluate_to_sources(kifmm_plan *P, double *pot, int32_t check_self, in
         KIFMM_REQUIRE(mem == KIFMM_MEM_HOST || mem == KIFMM_MEM_DEVICE, KIFMM_ERR_ARG, "bad mem flag");
         use_device(P);
         run_eval_sources(P, check_self != 0);
+        P->applied = true;
         copy_out(P, pot, P->pot_out.p, P->cplx ? 2 * P->N : P->N, mem);
     });
 }
@@ -351,6 +419,7 @@ static void apply_device(kifmm_plan *P, const double *tau, double *pot, bool che
     run_upward_downward(P);
     run_eval_sources(P, check_self);
     KIFMM_CUDA(cudaMemcpyAsync(pot, P->pot_out.p, nv * sizeof(double), cudaMemcpyDeviceToDevice, P->stream));
+    P->applied = true;
 }
 
 int kifmm_graph_capture(kifmm_plan *P, const double *tau, double *pot, int32_t check_self) {
@@ -571,6 +640,319 @@ int kifmm_set_wait_limit(kifmm_plan *P, int64_t polls) {
         KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
         drop_graph(P);  // a captured graph holds the old budget
         P->wait_limit = polls >= 0 ? (long long)polls : -1;
+    });
+}
+
+static void check_batch_plan(kifmm_plan *P, int device, int form) {
+    KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "batch: null plan");
+    KIFMM_REQUIRE(P->have_ops, KIFMM_ERR_STATE, "batch: every plan needs precompute first");
+    KIFMM_REQUIRE(P->device == device, KIFMM_ERR_ARG, "batch: all plans must be on one device");
+    KIFMM_REQUIRE(uses_tensor_m2l(P) && !P->opt.near_fp64 && !P->opt.planned && !P->cplx, KIFMM_ERR_ARG,
+                  "batch: plans must use the mixed form with a tensor-core M2L (no near_fp64, planned or "
+                  "complex option)");
+    KIFMM_REQUIRE(tc_form(P) == form, KIFMM_ERR_ARG, "batch: all plans must use one M2L form");
+    KIFMM_REQUIRE(P->kern.kind == KIFMM_KERNEL_LAPLACE || P->kern.kind == KIFMM_KERNEL_MOD_HELMHOLTZ,
+                  KIFMM_ERR_ARG, "batch: Laplace or modified-Helmholtz plans only");
+}
+
+// Every plan's first phase (densities in, P2M, M2M, M2L slices) in its branch,
+// the packed M2L, the L2L and leaf arguments in the branches, the packed leaf
+// passes, then the scatters: fork and join through events, so that the capture
+// holds the branches as parallel paths of one graph.
+static void batch_record(kifmm_batch *B, const double *const *tau, double *const *pot,
+                         std::vector<unsigned char> &htc, std::vector<int64_t> &htoff,
+                         std::vector<PassArgs> (&hleaf)[2], std::vector<int64_t> (&hloff)[2]) {
+    const int n = (int)B->plans.size();
+    cudaEvent_t fork = B->ev[n];
+    const size_t tcb = tc_args_bytes();
+    auto fork_all = [&] {
+        KIFMM_CUDA(cudaEventRecord(fork, B->stream));
+        for (int r = 0; r < n; r++) KIFMM_CUDA(cudaStreamWaitEvent(B->branch[r], fork, 0));
+    };
+    auto join_all = [&] {
+        for (int r = 0; r < n; r++) {
+            KIFMM_CUDA(cudaEventRecord(B->ev[r], B->branch[r]));
+            KIFMM_CUDA(cudaStreamWaitEvent(B->stream, B->ev[r], 0));
+        }
+    };
+    launch_fill_lanes(B->d_draw, n, B->nmax, B->stream);  // lanes whose density the batch draws
+    fork_all();
+    htoff.assign(1, 0);
+    for (int r = 0; r < n; r++) {
+        kifmm_plan *P = B->plans[r];
+        KIFMM_CUDA(cudaMemcpyAsync(P->tau.p, tau[r], P->N * sizeof(double), cudaMemcpyDeviceToDevice, P->stream));
+        apply_prologue(P);
+        int64_t t = 0;
+        if (P->L >= 3) {
+            PassArgs A = make_pass_args(P);
+            mixed_upward(P, A);
+            t = tc_prepare_batch(P, A, htc.data() + (size_t)r * tcb);
+        }
+        htoff.push_back(htoff.back() + t);
+    }
+    join_all();
+    B->tiles = htoff.back();
+    if (B->tiles) launch_m2l_tc_batch(tc_form(B->plans[0]), B->d_tc, B->d_tc_off, n, B->tiles, B->stream);
+    fork_all();
+    for (int k = 0; k < 2; k++) hloff[k].assign(1, 0), hleaf[k].clear();
+    for (int r = 0; r < n; r++) {
+        kifmm_plan *P = B->plans[r];
+        if (P->L >= 3) mixed_l2l(P, make_pass_args(P));
+        if (!P->n_leaf_list) continue;
+        const int k = P->kern.kind == KIFMM_KERNEL_LAPLACE ? 0 : 1;
+        hleaf[k].push_back(mixed_leaf_args(P));
+        hloff[k].push_back(hloff[k].back() + P->n_leaf_list);
+    }
+    join_all();
+    B->leaves = 0;
+    for (int k = 0; k < 2; k++) {
+        const int64_t nl = hloff[k].back();
+        B->leaves += nl;
+        if (nl)
+            launch_leaf_f_batch(k == 0 ? KIFMM_KERNEL_LAPLACE : KIFMM_KERNEL_MOD_HELMHOLTZ, B->d_leaf[k],
+                                B->d_leaf_off[k], (int)hleaf[k].size(), nl, B->stream);
+    }
+    fork_all();
+    for (int r = 0; r < n; r++) {
+        kifmm_plan *P = B->plans[r];
+        launch_scatter_pot(P);
+        KIFMM_CUDA(cudaMemcpyAsync(pot[r], P->pot_out.p, P->N * sizeof(double), cudaMemcpyDeviceToDevice,
+                                   P->stream));
+    }
+    join_all();
+    launch_lane_sums(B->d_sumlane, n, B->d_sums, B->stream);
+}
+
+int kifmm_batch_capture(kifmm_plan *const *plans, int32_t nplan, const double *const *tau, double *const *pot,
+                        int32_t check_self, void *stream, kifmm_batch **batch_out) {
+    return guarded([&] {
+        KIFMM_REQUIRE(batch_out, KIFMM_ERR_ARG, "null output pointer");
+        *batch_out = nullptr;
+        KIFMM_REQUIRE(plans && tau && pot && nplan > 0 && nplan <= 4096, KIFMM_ERR_ARG,
+                      "batch: bad plan list");
+        cudaStream_t cs = (cudaStream_t)stream;
+        KIFMM_REQUIRE(cs && cs != cudaStreamLegacy && cs != cudaStreamPerThread, KIFMM_ERR_ARG,
+                      "batch: needs a created stream, not a default stream");
+        KIFMM_REQUIRE(plans[0], KIFMM_ERR_ARG, "batch: null plan");
+        const int device = plans[0]->device, form = tc_form(plans[0]);
+        for (int r = 0; r < nplan; r++) {
+            check_batch_plan(plans[r], device, form);
+            KIFMM_REQUIRE(tau[r] && pot[r], KIFMM_ERR_ARG, "batch: null device pointer");
+            for (int q = 0; q < r; q++) KIFMM_REQUIRE(plans[q] != plans[r], KIFMM_ERR_ARG, "batch: repeated plan");
+        }
+        KIFMM_CUDA(cudaSetDevice(device));
+        std::unique_ptr<kifmm_batch> B(new kifmm_batch);
+        B->device = device;
+        B->stream = cs;
+        B->plans.assign(plans, plans + nplan);
+        for (int r = 0; r <= nplan; r++) {
+            cudaEvent_t e;
+            KIFMM_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            B->ev.push_back(e);
+        }
+        for (int r = 0; r < nplan; r++) {
+            cudaStream_t st;
+            KIFMM_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+            B->branch.push_back(st);
+        }
+        const size_t tcb = tc_args_bytes();
+        KIFMM_CUDA(cudaMalloc(&B->d_tc, tcb * nplan));
+        KIFMM_CUDA(cudaMalloc(&B->d_tc_off, sizeof(int64_t) * (nplan + 1)));
+        for (int k = 0; k < 2; k++) {
+            KIFMM_CUDA(cudaMalloc(&B->d_leaf[k], sizeof(PassArgs) * nplan));
+            KIFMM_CUDA(cudaMalloc(&B->d_leaf_off[k], sizeof(int64_t) * (nplan + 1)));
+        }
+        const size_t dlb = draw_lane_bytes();
+        B->h_draw.assign(dlb * nplan, 0);
+        std::vector<unsigned char> hsum(dlb * nplan, 0);
+        for (int r = 0; r < nplan; r++) {
+            set_draw_lane(B->h_draw.data(), r, const_cast<double *>(tau[r]), plans[r]->N, kDrawSkipSeed, 0);
+            set_draw_lane(hsum.data(), r, pot[r], plans[r]->N, kDrawSkipSeed, 0);
+            B->nmax = std::max<int64_t>(B->nmax, plans[r]->N);
+        }
+        KIFMM_CUDA(cudaMalloc(&B->d_draw, dlb * nplan));
+        KIFMM_CUDA(cudaMalloc(&B->d_sumlane, dlb * nplan));
+        KIFMM_CUDA(cudaMalloc(&B->d_sums, sizeof(double) * nplan));
+        KIFMM_CUDA(cudaMallocHost(&B->h_sums, sizeof(double) * nplan));
+        KIFMM_CUDA(cudaMemcpy(B->d_draw, B->h_draw.data(), dlb * nplan, cudaMemcpyHostToDevice));
+        KIFMM_CUDA(cudaMemcpy(B->d_sumlane, hsum.data(), dlb * nplan, cudaMemcpyHostToDevice));
+        // a plan without an apply since its tree and operators were built runs
+        // one on its own stream after the caller's work: that allocates every
+        // apply buffer (stream-ordered on the plan's stream)
+        KIFMM_CUDA(cudaEventRecord(B->ev[nplan], cs));
+        for (int r = 0; r < nplan; r++) {
+            kifmm_plan *P = plans[r];
+            use_device(P);
+            if (P->applied) continue;
+            drop_graph(P);
+            KIFMM_CUDA(cudaStreamWaitEvent(P->stream, B->ev[nplan], 0));
+            const bool prof = P->profiling;
+            P->profiling = false;
+            apply_device(P, tau[r], pot[r], check_self != 0);
+            P->profiling = prof;
+            P->have_expansions = true;
+            KIFMM_CUDA(cudaEventRecord(B->ev[r], P->stream));
+            KIFMM_CUDA(cudaStreamWaitEvent(cs, B->ev[r], 0));
+        }
+        KIFMM_CUDA(cudaStreamSynchronize(cs));
+        for (int r = 0; r < nplan; r++) {
+            use_device(plans[r]);
+            KIFMM_CUDA(cudaStreamSynchronize(plans[r]->stream));
+            check_device_flags(plans[r]);
+        }
+        KIFMM_CUDA(cudaSetDevice(device));
+        // capture with each plan's work ordered on its branch stream
+        std::vector<cudaStream_t> own(nplan);
+        std::vector<char> prof(nplan);
+        for (int r = 0; r < nplan; r++) {
+            own[r] = plans[r]->stream;
+            prof[r] = plans[r]->profiling;
+            plans[r]->stream = B->branch[r];
+            plans[r]->profiling = false;
+        }
+        struct Restore {
+            kifmm_plan *const *plans;
+            const std::vector<cudaStream_t> &own;
+            const std::vector<char> &prof;
+            ~Restore() {
+                for (size_t r = 0; r < own.size(); r++) {
+                    plans[r]->stream = own[r];
+                    plans[r]->profiling = prof[r];
+                }
+            }
+        } restore{plans, own, prof};
+        g_stream = own[0];  // no allocation is expected: the apply above made every buffer
+        std::vector<unsigned char> htc(tcb * nplan, 0);
+        std::vector<int64_t> htoff;
+        std::vector<PassArgs> hleaf[2];
+        std::vector<int64_t> hloff[2];
+        // A call made by another host thread meanwhile that synchronises
+        // implicitly with every stream (some allocations do) invalidates a
+        // capture in progress; the capture is then made again.
+        cudaGraph_t g = nullptr;
+        for (int attempt = 0;; attempt++) {
+            KIFMM_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+            bool failed = false;
+            try {
+                batch_record(B.get(), tau, pot, htc, htoff, hleaf, hloff);
+            } catch (...) {
+                failed = true;
+                if (attempt >= 3) {
+                    cudaStreamEndCapture(cs, &g);
+                    if (g) cudaGraphDestroy(g);
+                    throw;
+                }
+            }
+            const cudaError_t ee = cudaStreamEndCapture(cs, &g);
+            if (!failed && ee == cudaSuccess) break;
+            if (g) cudaGraphDestroy(g);
+            g = nullptr;
+            if (attempt >= 3) KIFMM_CUDA(ee != cudaSuccess ? ee : cudaErrorStreamCaptureInvalidated);
+            cudaGetLastError();
+        }
+        cudaError_t e = cudaGraphInstantiate(&B->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            B->graph = nullptr;
+            KIFMM_CUDA(e);
+        }
+        // the tables the packed kernels read, in place before the first launch
+        KIFMM_CUDA(cudaMemcpy(B->d_tc, htc.data(), htc.size(), cudaMemcpyHostToDevice));
+        KIFMM_CUDA(cudaMemcpy(B->d_tc_off, htoff.data(), htoff.size() * sizeof(int64_t), cudaMemcpyHostToDevice));
+        for (int k = 0; k < 2; k++) {
+            if (!hleaf[k].empty())
+                KIFMM_CUDA(cudaMemcpy(B->d_leaf[k], hleaf[k].data(), hleaf[k].size() * sizeof(PassArgs),
+                                      cudaMemcpyHostToDevice));
+            KIFMM_CUDA(cudaMemcpy(B->d_leaf_off[k], hloff[k].data(), hloff[k].size() * sizeof(int64_t),
+                                  cudaMemcpyHostToDevice));
+        }
+        *batch_out = B.release();
+    });
+}
+
+int kifmm_batch_launch(kifmm_batch *B) {
+    return guarded([&] {
+        KIFMM_REQUIRE(B && B->graph, KIFMM_ERR_ARG, "batch launch: no captured batch");
+        KIFMM_CUDA(cudaSetDevice(B->device));
+        KIFMM_CUDA(cudaGraphLaunch(B->graph, B->stream));
+    });
+}
+
+int kifmm_batch_set_draws(kifmm_batch *B, const uint64_t *seed, const uint64_t *index) {
+    return guarded([&] {
+        KIFMM_REQUIRE(B && seed && index, KIFMM_ERR_ARG, "null argument");
+        KIFMM_CUDA(cudaSetDevice(B->device));
+        const int n = (int)B->plans.size();
+        for (int r = 0; r < n; r++)
+            set_draw_seed(B->h_draw.data(), r, seed[r], index[r]);
+        // from pageable memory: the call returns once h_draw has been read
+        KIFMM_CUDA(cudaMemcpyAsync(B->d_draw, B->h_draw.data(), B->h_draw.size(), cudaMemcpyHostToDevice,
+                                   B->stream));
+    });
+}
+
+int kifmm_batch_synchronize(kifmm_batch *B) {
+    return guarded([&] {
+        KIFMM_REQUIRE(B, KIFMM_ERR_ARG, "null batch");
+        KIFMM_CUDA(cudaSetDevice(B->device));
+        // every plan's error flags and the lane sums in one drain of the stream
+        for (auto *P : B->plans)
+            if (P->scal.p && P->hpin)
+                KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_FLAGS, P->scal.p + KIFMM_SCAL_PASS_ERR,
+                                           2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, B->stream));
+        KIFMM_CUDA(cudaMemcpyAsync(B->h_sums, B->d_sums, sizeof(double) * B->plans.size(), cudaMemcpyDeviceToHost,
+                                   B->stream));
+        KIFMM_CUDA(cudaStreamSynchronize(B->stream));
+        for (auto *P : B->plans) {
+            if (!P->scal.p || !P->hpin) continue;
+            const unsigned long long *f = P->hpin + HP_FLAGS;
+            KIFMM_REQUIRE(f[0] == 0, KIFMM_ERR_CUDA, "M2M/L2L pass: a bulk-copy wait timed out");
+            KIFMM_REQUIRE(f[1] == 0, KIFMM_ERR_CUDA, "tensor-core M2L: an MMA completion wait timed out");
+        }
+    });
+}
+
+int kifmm_batch_sums(kifmm_batch *B, double *sums) {
+    return guarded([&] {
+        KIFMM_REQUIRE(B && sums, KIFMM_ERR_ARG, "null argument");
+        memcpy(sums, B->h_sums, sizeof(double) * B->plans.size());
+    });
+}
+
+int kifmm_fill_normal(double *dev, int64_t n, uint64_t seed, uint64_t index, void *stream) {
+    return guarded([&] {
+        KIFMM_REQUIRE(n >= 0 && (dev || n == 0), KIFMM_ERR_ARG, "fill_normal: bad buffer");
+        KIFMM_REQUIRE(seed != kDrawSkipSeed, KIFMM_ERR_ARG, "fill_normal: seed 2^64-1 is reserved");
+        launch_fill_normal(dev, n, seed, index, (cudaStream_t)stream);
+    });
+}
+
+int kifmm_batch_info(kifmm_batch *B, int64_t *m2l_tiles, int64_t *leaves) {
+    return guarded([&] {
+        KIFMM_REQUIRE(B, KIFMM_ERR_ARG, "null batch");
+        if (m2l_tiles) *m2l_tiles = B->tiles;
+        if (leaves) *leaves = B->leaves;
+    });
+}
+
+int kifmm_batch_destroy(kifmm_batch *B) {
+    return guarded([&] { delete B; });
+}
+
+int kifmm_stream_create(int32_t device, void **stream) {
+    return guarded([&] {
+        KIFMM_REQUIRE(stream, KIFMM_ERR_ARG, "null output pointer");
+        KIFMM_REQUIRE(device >= 0 && device < 64, KIFMM_ERR_ARG, "device index out of range");
+        KIFMM_CUDA(cudaSetDevice(device));
+        cudaStream_t s = nullptr;
+        KIFMM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        *stream = (void *)s;
+    });
+}
+
+int kifmm_stream_destroy(void *stream) {
+    return guarded([&] {
+        if (stream) KIFMM_CUDA(cudaStreamDestroy((cudaStream_t)stream));
     });
 }
 

@@ -218,6 +218,7 @@ struct kifmm_plan {
     kifmm::DBuf<double> uup, udown;
     kifmm::DBuf<double> zero4q;      // 4Q zeros: the source of an absent M2L direction
     bool have_expansions = false;
+    bool applied = false;  // an apply at the sources ran since the tree / operators were built
 
     // scratch for the tree build
     kifmm::DBuf<uint64_t> key2, hash, list;

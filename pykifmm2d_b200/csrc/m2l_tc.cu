@@ -317,8 +317,9 @@ __device__ __forceinline__ bool warp_wait(uint32_t bar, uint32_t parity, long lo
     return __any_sync(0xffffffffu, mbar_wait(bar, parity, limit));
 }
 
+// column tile `tile` of the M2L of T's plan, by one CTA
 template <int F>
-__global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(TcArgs T) {
+__device__ __forceinline__ void m2l_tc_tile(const TcArgs &T, const int64_t tile) {
     using TR = TcTraits<F>;
     constexpr int TN = TR::TN, NS = TR::NS, EB = TR::EB, S = TC_STAGES;
     constexpr int KSTEPS = TC_KCB / EB / TR::KSTEP;
@@ -335,14 +336,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(TcArgs T) {
     uint64_t *bars = (uint64_t *)(((uintptr_t)(sdir + 16) + 7) & ~(uintptr_t)7);
     uint32_t *tslot = (uint32_t *)(bars + 3 * S + 1);
     volatile int *abort_flag = sdir + 9;
-    pdl_trigger();
-    pdl_wait();
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const PassArgs &A = T.A;
     const int Q = A.Q, Q4 = T.g.Q4, KP = T.pre.KP, NKC = T.g.NKC;
 
     // which level / column tile / M tile
-    const int64_t tile = blockIdx.x;
     int l = T.lmin;
     while (l < T.lmax && T.tile_off[l + 1] <= tile) l++;
     const int64_t lt = tile - T.tile_off[l];
@@ -582,6 +580,31 @@ __global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(TcArgs T) {
     }
 }
 
+template <int F>
+__global__ void __launch_bounds__(TC_THREADS, 1) k_m2l_tc(TcArgs T) {
+    pdl_trigger();
+    pdl_wait();
+    m2l_tc_tile<F>(T, blockIdx.x);
+}
+
+// The M2L of several plans in one launch (serving batches): CTA b takes tile
+// b - off[r] of plan r, off[r] <= b < off[r + 1].  The plans' arguments are
+// read from global memory.
+template <int F>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_m2l_tc_batch(const TcArgs *__restrict__ args, const int64_t *__restrict__ off, int nplan) {
+    pdl_trigger();
+    pdl_wait();
+    const int64_t b = blockIdx.x;
+    int lo = 0, hi = nplan;  // the last r with off[r] <= b
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= b) lo = mid;
+        else hi = mid;
+    }
+    if (b < off[nplan]) m2l_tc_tile<F>(args[lo], b - off[lo]);
+}
+
 // ------------------------------------------------------------ host side
 bool uses_tensor_m2l(const kifmm_plan *P) {
     return P->opt.precision == KIFMM_PREC_MIXED &&
@@ -619,12 +642,14 @@ void build_tc_operators(kifmm_plan *P) {
     }
 }
 
+// The preslice of P's source expansions (launched on P->stream) and the
+// arguments of P's M2L; returns the number of CTA tiles (0: no M2L).
 template <int F>
-static void run_m2l_tensor_t(kifmm_plan *P, const PassArgs &A) {
+static int64_t tc_prepare_t(kifmm_plan *P, const PassArgs &A, TcArgs &T) {
     using TR = TcTraits<F>;
     TcGeom g = tc_geom<F>(P->Q);
     const int L = P->L;
-    if (L < 3 || !P->n_ent) return;
+    if (L < 3 || !P->n_ent) return 0;
     TcPre pre{};
     pre.KP = g.KP;
     P->tc_pre.alloc((size_t)P->n_ent * TR::NS * g.KP * TR::EB);
@@ -634,7 +659,7 @@ static void run_m2l_tensor_t(kifmm_plan *P, const PassArgs &A) {
     pre.gexp = P->tc_gexp.p;
     pre.src8 = P->tc_src8.p;
     launch_pdl(k_tc_preslice<F>, dim3(grid_for(P->n_ent * 32, 256)), dim3(256), 0, P->stream, A, P->n_ent, pre);
-    TcArgs T{};
+    T = TcArgs{};
     T.A = A;
     T.g = g;
     T.aslices = P->tc_a.p;
@@ -649,6 +674,13 @@ static void run_m2l_tensor_t(kifmm_plan *P, const PassArgs &A) {
         T.tile_off[l] = tiles;
         if (l >= T.lmin && l <= T.lmax) tiles += (P->lt.ne[l] + TR::TN - 1) / TR::TN * g.MT;
     }
+    return tiles;
+}
+
+template <int F>
+static void run_m2l_tensor_t(kifmm_plan *P, const PassArgs &A) {
+    TcArgs T;
+    const int64_t tiles = tc_prepare_t<F>(P, A, T);
     if (!tiles) return;
     size_t smem = tc_smem_bytes<F>();
     ensure_dyn_smem(k_m2l_tc<F>, smem);
@@ -662,6 +694,37 @@ void run_m2l_tensor(kifmm_plan *P, const PassArgs &A) {
         case TC_BF16: run_m2l_tensor_t<TC_BF16>(P, A); break;
         case TC_FP16: run_m2l_tensor_t<TC_FP16>(P, A); break;
         default: run_m2l_tensor_t<TC_INT8>(P, A); break;
+    }
+}
+
+// ---------------------------------------------------- serving batches
+int tc_form(const kifmm_plan *P) { return form_of(P->opt.m2l); }
+size_t tc_args_bytes() { return sizeof(TcArgs); }
+
+int64_t tc_prepare_batch(kifmm_plan *P, const PassArgs &A, void *args) {
+    TcArgs &T = *(TcArgs *)args;
+    switch (form_of(P->opt.m2l)) {
+        case TC_BF16: return tc_prepare_t<TC_BF16>(P, A, T);
+        case TC_FP16: return tc_prepare_t<TC_FP16>(P, A, T);
+        default: return tc_prepare_t<TC_INT8>(P, A, T);
+    }
+}
+
+template <int F>
+static void launch_batch_t(const void *dargs, const int64_t *doff, int nplan, int64_t tiles, cudaStream_t s) {
+    const size_t smem = tc_smem_bytes<F>();
+    ensure_dyn_smem(k_m2l_tc_batch<F>, smem);
+    k_m2l_tc_batch<F><<<(unsigned)tiles, TC_THREADS, smem, s>>>((const TcArgs *)dargs, doff, nplan);
+    KIFMM_LAUNCHED();
+}
+
+void launch_m2l_tc_batch(int form, const void *dargs, const int64_t *doff, int nplan, int64_t tiles,
+                         cudaStream_t s) {
+    KIFMM_REQUIRE(tiles > 0 && tiles < (1ll << 31), KIFMM_ERR_ARG, "batch M2L: bad tile count");
+    switch (form) {
+        case TC_BF16: launch_batch_t<TC_BF16>(dargs, doff, nplan, tiles, s); break;
+        case TC_FP16: launch_batch_t<TC_FP16>(dargs, doff, nplan, tiles, s); break;
+        default: launch_batch_t<TC_INT8>(dargs, doff, nplan, tiles, s); break;
     }
 }
 

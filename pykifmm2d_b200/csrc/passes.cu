@@ -933,9 +933,11 @@ static void launch_lvl_gemm(kifmm_plan *P, const PassArgs &A, int l) {
 void launch_m2m_d(kifmm_plan *P, const PassArgs &A, int l) { launch_lvl_gemm<0>(P, A, l); }
 void launch_l2l_d(kifmm_plan *P, const PassArgs &A, int l) { launch_lvl_gemm<1>(P, A, l); }
 
-void run_upward_downward(kifmm_plan *P) {
+// Buffers of an apply, its cleared flags and expansions, and the densities in
+// tree order.
+void apply_prologue(kifmm_plan *P) {
     cudaStream_t s = P->stream;
-    const int Q = P->Q, L = P->L;
+    const int Q = P->Q;
     int64_t n = P->N, NN = P->n_nodes;
     const int64_t vw = P->cplx ? 2 : 1;  // doubles per density value
     P->taus.alloc(n * vw);
@@ -954,6 +956,12 @@ void run_upward_downward(kifmm_plan *P) {
     else
         launch_pdl(k_gather_tau, dim3(grid_for(n, 256, P->num_sms * 8)), dim3(256), 0, s, (const double *)P->tau.p,
                    (const int32_t *)P->perm.p, n, P->taus.p);
+}
+
+void run_upward_downward(kifmm_plan *P) {
+    cudaStream_t s = P->stream;
+    const int Q = P->Q, L = P->L;
+    apply_prologue(P);
     if (P->opt.precision == KIFMM_PREC_MIXED) {
         run_passes_mixed(P);
         return;
@@ -1014,8 +1022,14 @@ void run_upward_downward(kifmm_plan *P) {
     }
 }
 
+// potentials from tree order to the caller's order
+void launch_scatter_pot(kifmm_plan *P) {
+    const int64_t n = P->N;
+    launch_pdl(k_scatter_pot, dim3(grid_for(n, 256, P->num_sms * 8)), dim3(256), 0, P->stream,
+               (const double *)P->pots.p, (const int32_t *)P->perm.p, n, P->pot_out.p);
+}
+
 void run_eval_sources(kifmm_plan *P, int check_self) {
-    cudaStream_t s = P->stream;
     int64_t n = P->N;
     P->pot_out.alloc(P->cplx ? 2 * n : n);
     if (P->cplx) {
@@ -1036,8 +1050,7 @@ void run_eval_sources(kifmm_plan *P, int check_self) {
             launch_leaf_eval_d(P, A, check_self);
         }
     }
-    launch_pdl(k_scatter_pot, dim3(grid_for(n, 256, P->num_sms * 8)), dim3(256), 0, s, (const double *)P->pots.p,
-               (const int32_t *)P->perm.p, n, P->pot_out.p);
+    launch_scatter_pot(P);
 }
 
 void run_eval_targets(kifmm_plan *P, const double *tx, const double *ty, int64_t n, int check_self, double *pot) {

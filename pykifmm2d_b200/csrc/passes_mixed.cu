@@ -251,9 +251,9 @@ __device__ __forceinline__ float pair_lg2_floor(float tx, float ty, const float4
     return lg2_ftz(fmaf(dx, dx, fmaf(dy, dy, 1.17549435e-38f)));
 }
 
+// the L2P + P2P of leaf w of A's leaf list, by one warp
 template <int KIND>
-__global__ void __launch_bounds__(32 * LEAF_WARPS, LEAF_BLOCKS_PER_SM) k_leaf_eval_f(PassArgs A, const int32_t *__restrict__ list,
-                                                                 int64_t nlist) {
+__device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w) {
     constexpr int R = 2 * KIFMM_TAYLOR_P + 1;
     constexpr float CLAMP = 1.17549435e-38f;  // FLT_MIN
     __shared__ float4 srcs[LEAF_WARPS][LEAF_CHUNK + 32];
@@ -263,11 +263,7 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, LEAF_BLOCKS_PER_SM) k_leaf_ev
     __shared__ float redf[LEAF_WARPS][2][32];
     __shared__ int rngs[LEAF_WARPS][18];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    pdl_trigger();
-    pdl_wait();
-    // one warp per leaf (grid-stride only if the grid were capped)
-    const int64_t wstride = (int64_t)gridDim.x * LEAF_WARPS;
-    for (int64_t w = (int64_t)blockIdx.x * LEAF_WARPS + wib; w < nlist; w += wstride) {
+    {
         // the leaf record: node, level, point range, cell key and source ranges
         // in one coalesced load (list[w] is the record's node)
         const int rv = A.leaf_rec[w * LEAF_REC_WORDS + lane];
@@ -308,7 +304,6 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, LEAF_BLOCKS_PER_SM) k_leaf_ev
         // (kept in shared memory: registers are scarce in the pair loop)
         int *rng = rngs[wib];
         if (lane >= LR_RNG && lane < LR_RNG + 18) rng[lane - LR_RNG] = rv;
-        (void)list;
         double tsum = 0.0;  // FP64 sum of the near sources' charges (Laplace)
         // stage sources [c0, c0 + cn) of the list, padded with 32 far, uncharged
         // ones; four elements per lane per pass, loads issued before any is used
@@ -532,6 +527,33 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, LEAF_BLOCKS_PER_SM) k_leaf_ev
     }
 }
 
+template <int KIND>
+__global__ void __launch_bounds__(32 * LEAF_WARPS, LEAF_BLOCKS_PER_SM) k_leaf_eval_f(PassArgs A, int64_t nlist) {
+    pdl_trigger();
+    pdl_wait();
+    // one warp per leaf (grid-stride only if the grid were capped)
+    const int64_t wstride = (int64_t)gridDim.x * LEAF_WARPS;
+    for (int64_t w = (int64_t)blockIdx.x * LEAF_WARPS + (threadIdx.x >> 5); w < nlist; w += wstride)
+        leaf_eval_f_leaf<KIND>(A, w);
+}
+
+// The leaf pass of several plans in one launch (serving batches): warp w of
+// the grid takes leaf w - off[r] of plan r, off[r] <= w < off[r + 1].
+template <int KIND>
+__global__ void __launch_bounds__(32 * LEAF_WARPS, LEAF_BLOCKS_PER_SM)
+    k_leaf_eval_f_batch(const PassArgs *__restrict__ args, const int64_t *__restrict__ off, int nplan) {
+    pdl_trigger();
+    pdl_wait();
+    const int64_t w = (int64_t)blockIdx.x * LEAF_WARPS + (threadIdx.x >> 5);
+    int lo = 0, hi = nplan;  // the last r with off[r] <= w
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (off[mid] <= w) lo = mid;
+        else hi = mid;
+    }
+    if (w < off[nplan]) leaf_eval_f_leaf<KIND>(args[lo], w - off[lo]);
+}
+
 // separate targets: one thread per target
 template <int KIND>
 __global__ void k_eval_targets_f(PassArgs A, const double *__restrict__ tx, const double *__restrict__ ty, int64_t n,
@@ -583,30 +605,35 @@ void launch_eval_targets_d(kifmm_plan *P, const PassArgs &A, const double *tx, c
 void launch_m2m_d(kifmm_plan *P, const PassArgs &A, int l);
 void launch_l2l_d(kifmm_plan *P, const PassArgs &A, int l);
 
-void run_passes_mixed(kifmm_plan *P) {
-    cudaStream_t s = P->stream;
-    const int Q = P->Q, L = P->L;
-    int64_t NN = P->n_nodes;
-    (void)s;
-    (void)Q;
-    (void)NN;
-    if (L < 3) return;  // expansions cleared by run_upward_downward
-    PassArgs A = make_pass_args(P);
+// P2M and M2M of the mixed apply
+void mixed_upward(kifmm_plan *P, const PassArgs &A) {
     if (P->n_p2m_list) {
         PhaseScope ph(P, KIFMM_PHASE_P2M);
         if (planned_ready(P)) launch_planned_p2m(P, A);
         else launch_p2m_d(P, A);
     }
-    {
-        PhaseScope ph(P, KIFMM_PHASE_M2M);
-        for (int l = L - 2; l >= 2; l--)
-            if (P->lt.ne[l]) launch_m2m_d(P, A, l);
-    }
-    const bool simt = P->opt.m2l == KIFMM_M2L_FP32;
-    int thr = ((4 * Q + 31) / 32) * 32;
-    size_t smem = (size_t)M2LF_TE * 4 * Q * sizeof(float);
-    if (simt) {
+    PhaseScope ph(P, KIFMM_PHASE_M2M);
+    for (int l = P->L - 2; l >= 2; l--)
+        if (P->lt.ne[l]) launch_m2m_d(P, A, l);
+}
+
+// the L2L chain after the M2L
+void mixed_l2l(kifmm_plan *P, const PassArgs &A) {
+    PhaseScope ph(P, KIFMM_PHASE_L2L);
+    for (int l = 2; l <= P->L - 2; l++)
+        if (P->lt.ne[l]) launch_l2l_d(P, A, l);
+}
+
+void run_passes_mixed(kifmm_plan *P) {
+    cudaStream_t s = P->stream;
+    const int Q = P->Q, L = P->L;
+    if (L < 3) return;  // expansions cleared by run_upward_downward
+    PassArgs A = make_pass_args(P);
+    mixed_upward(P, A);
+    if (P->opt.m2l == KIFMM_M2L_FP32) {
         PhaseScope ph(P, KIFMM_PHASE_M2L);
+        const int thr = ((4 * Q + 31) / 32) * 32;
+        const size_t smem = (size_t)M2LF_TE * 4 * Q * sizeof(float);
         ensure_dyn_smem(k_m2l_f, smem);
         for (int l = 1; l <= L - 2; l++) {
             int64_t ne = P->lt.ne[l];
@@ -620,19 +647,13 @@ void run_passes_mixed(kifmm_plan *P) {
         PhaseScope ph(P, KIFMM_PHASE_M2L);
         run_m2l_tensor(P, A);  // all levels at once
     }
-    PhaseScope ph(P, KIFMM_PHASE_L2L);
-    for (int l = 2; l <= L - 2; l++)
-        if (P->lt.ne[l]) launch_l2l_d(P, A, l);
+    mixed_l2l(P, A);
 }
 
-void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
-    if (!P->n_leaf_list) return;
-    PhaseScope ph(P, KIFMM_PHASE_LEAF);
+// The arguments of the FP32 leaf kernel; for the Laplace kernel this first
+// launches the Taylor coefficients of the leaves' local expansions.
+PassArgs mixed_leaf_args(kifmm_plan *P) {
     PassArgs A = make_pass_args(P);
-    if (P->opt.near_fp64) {
-        launch_leaf_eval_d(P, A, check_self);
-        return;
-    }  // FP32 form: coincident pairs always contribute zero
     if (P->kern.kind == KIFMM_KERNEL_LAPLACE && P->l2p_taylor.p && P->L >= 3) {
         constexpr int R = 2 * KIFMM_TAYLOR_P + 1;
         KIFMM_REQUIRE(P->Q % 4 == 0, KIFMM_ERR_ARG, "mixed Laplace form: Nequiv must be a multiple of 4");
@@ -658,13 +679,37 @@ void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
             launch_pdl(k_leaf_taylor, dim3((unsigned)tiles), dim3(TY_THREADS), smem, P->stream, T);
         }
     }
+    return A;
+}
+
+void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
+    if (!P->n_leaf_list) return;
+    PhaseScope ph(P, KIFMM_PHASE_LEAF);
+    if (P->opt.near_fp64) {
+        launch_leaf_eval_d(P, make_pass_args(P), check_self);
+        return;
+    }  // FP32 form: coincident pairs always contribute zero
+    PassArgs A = mixed_leaf_args(P);
     unsigned gr = (unsigned)std::min<int64_t>((P->n_leaf_list + LEAF_WARPS - 1) / LEAF_WARPS, 1ll << 30);
     if (P->kern.kind == KIFMM_KERNEL_LAPLACE)
         launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_LAPLACE>, dim3(gr), dim3(32 * LEAF_WARPS), 0, P->stream, A,
-                   (const int32_t *)P->leaf_list.p, P->n_leaf_list);
+                   P->n_leaf_list);
     else
         launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_MOD_HELMHOLTZ>, dim3(gr), dim3(32 * LEAF_WARPS), 0, P->stream, A,
-                   (const int32_t *)P->leaf_list.p, P->n_leaf_list);
+                   P->n_leaf_list);
+}
+
+// the FP32 leaf pass of several plans of one kernel kind in one launch
+void launch_leaf_f_batch(int kind, const PassArgs *dargs, const int64_t *doff, int nplan, int64_t nleaf,
+                         cudaStream_t s) {
+    const int64_t blocks = (nleaf + LEAF_WARPS - 1) / LEAF_WARPS;
+    KIFMM_REQUIRE(blocks > 0 && blocks < (1ll << 31), KIFMM_ERR_ARG, "batch leaf pass: bad leaf count");
+    if (kind == KIFMM_KERNEL_LAPLACE)
+        k_leaf_eval_f_batch<KIFMM_KERNEL_LAPLACE><<<(unsigned)blocks, 32 * LEAF_WARPS, 0, s>>>(dargs, doff, nplan);
+    else
+        k_leaf_eval_f_batch<KIFMM_KERNEL_MOD_HELMHOLTZ><<<(unsigned)blocks, 32 * LEAF_WARPS, 0, s>>>(dargs, doff,
+                                                                                                      nplan);
+    KIFMM_LAUNCHED();
 }
 
 void run_eval_targets_mixed(kifmm_plan *P, const double *tx, const double *ty, int64_t n, int check_self,

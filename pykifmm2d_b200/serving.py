@@ -22,17 +22,31 @@ The server:
 * records arrival, admission and completion times.  Latency is completion
   minus arrival.
 
+With ``packed=True`` the densities of all admitted requests advance in
+lockstep instead: worker threads build each request's tree and operators and
+apply its first density, then the request joins a ``PackedBatch``
+(``kifmm_batch_capture``), one CUDA graph per set of requests in which the
+M2L of every request is one tensor-core launch and the near field + L2P one
+launch per kernel kind, the per-request passes running as parallel branches;
+the batch draws every request's next density itself and sums its potentials
+on the device.  Each step is one graph launch plus the device-to-host copies.
+
 Results do not depend on what else runs: every request has its own plan and
-buffers, and the kernels are deterministic.  ``tests/test_serving.py`` checks
-that a request gives the same potentials alone and in the mix.
+buffers, the packed kernels run the same per-tile and per-leaf code as a
+request's own launches, and the kernels are deterministic.
+``tests/test_serving.py`` checks that a request gives the same potentials
+alone and in the mix, packed or not.
 """
 import concurrent.futures as cf
 import threading
 import time
 from dataclasses import dataclass, field
 
+import ctypes
+
 import numpy as np
 
+from . import _lib as B
 from . import class_fmm as C
 
 
@@ -74,12 +88,88 @@ class Request:
         return out.cpu().numpy()
 
 
+DRAW_SKIP = (1 << 64) - 1  # lane seed of a packed batch whose density the caller writes
+
+
 def device_density(torch, seed, i, out):
-    """Fresh N(0,1) density i of a request, drawn into the CUDA tensor ``out``
-    by a generator seeded with (seed, i): the same numbers alone and in any mix."""
-    g = torch.Generator(device=out.device)
-    g.manual_seed(int(seed) * 4096 + int(i))
-    out.normal_(0.0, 1.0, generator=g)
+    """Fresh N(0,1) density i of a request, drawn into the contiguous float64
+    CUDA tensor ``out`` on torch's current stream by the library's
+    counter-based generator (``kifmm_fill_normal``, seed ``seed``, density
+    number ``i``): the same numbers alone, in any mix and in a packed batch."""
+    if not (out.is_cuda and out.dtype == torch.float64 and out.is_contiguous()):
+        raise ValueError("device_density needs a contiguous float64 CUDA tensor")
+    st = torch.cuda.current_stream(out.device).cuda_stream
+    B.check(B.load().kifmm_fill_normal(out.data_ptr(), out.numel(), int(seed), int(i),
+                                       ctypes.c_void_p(st if st else 1)))
+
+
+class PackedBatch:
+    """Packed applies of several FMM objects (``kifmm_batch_capture``): one
+    CUDA graph whose M2L of all plans is one tensor-core launch and whose near
+    field + L2P is one launch per kernel kind, with the per-plan passes as
+    parallel branches.  ``fmms`` are mixed-precision FMM objects after
+    precompute; ``taus`` / ``pots`` their float64 CUDA tensors (the graph keeps
+    their addresses); ``stream`` a torch.cuda.Stream that orders the capture
+    and every ``launch``.  Each result equals the plan's own apply."""
+
+    def __init__(self, fmms, taus, pots, stream, check_self=True):
+        import torch
+        n = len(fmms)
+        if not (n == len(taus) == len(pots)) or n == 0:
+            raise ValueError("PackedBatch needs one tau and one pot tensor per FMM")
+        for f, t, q in zip(fmms, taus, pots):
+            for v in (t, q):
+                if not (v.is_cuda and v.dtype == torch.float64 and v.is_contiguous() and v.numel() == f.N):
+                    raise ValueError("PackedBatch needs contiguous float64 CUDA tensors of one value per point")
+        self._lib = B.load()
+        vp = ctypes.c_void_p * n
+        plans = vp(*[f._plan.value for f in fmms])
+        tp = vp(*[t.data_ptr() for t in taus])
+        pp = vp(*[q.data_ptr() for q in pots])
+        h = ctypes.c_void_p()
+        B.check(self._lib.kifmm_batch_capture(plans, n, tp, pp, int(bool(check_self)),
+                                              ctypes.c_void_p(stream.cuda_stream), ctypes.byref(h)))
+        self._h = h
+        self._keep = (list(fmms), list(taus), list(pots), stream)  # the graph uses their memory
+
+    def set_draws(self, seeds, index):
+        """Lane r draws N(0,1) density index[r] of seed seeds[r] into its tau
+        at the start of each later launch (``DRAW_SKIP``: the caller writes it)."""
+        n = len(self._keep[0])
+        sv = (ctypes.c_uint64 * n)(*[int(v) for v in seeds])
+        iv = (ctypes.c_uint64 * n)(*[int(v) for v in index])
+        B.check(self._lib.kifmm_batch_set_draws(self._h, sv, iv))
+
+    def launch(self):
+        B.check(self._lib.kifmm_batch_launch(self._h))
+
+    def synchronize(self):
+        B.check(self._lib.kifmm_batch_synchronize(self._h))
+
+    def sums(self):
+        """Per-lane sums of the potentials of the last launch (after synchronize)."""
+        out = np.empty(len(self._keep[0]))
+        B.check(self._lib.kifmm_batch_sums(self._h, out.ctypes.data))
+        return out
+
+    def info(self):
+        """(tiles of the packed M2L launch, leaves of the packed leaf launches)"""
+        t, l = ctypes.c_int64(), ctypes.c_int64()
+        B.check(self._lib.kifmm_batch_info(self._h, ctypes.byref(t), ctypes.byref(l)))
+        return t.value, l.value
+
+    def close(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            self._lib.kifmm_batch_destroy(h)
+        self._h = None
+        self._keep = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: torch may be gone already
+            pass
 
 
 @dataclass
@@ -154,9 +244,12 @@ class Server:
     """Continuous-batching FMM server on one GPU (see the module docstring)."""
 
     def __init__(self, device=0, slots=8, hbm_budget=None, precision="mixed", check_self=True, keep_pots=True,
-                 graphs=True):
+                 graphs=True, packed=False):
         import torch
         self.keep_pots = bool(keep_pots)
+        self.packed = bool(packed)
+        if self.packed and precision != "mixed":
+            raise ValueError("packed serving runs the mixed-precision form")
         self.torch = torch
         self.device = int(device)
         self.slots = int(slots)
@@ -167,10 +260,32 @@ class Server:
             free, _ = torch.cuda.mem_get_info(self.device)
             hbm_budget = min(DEFAULT_HBM_BUDGET, int(0.9 * free))
         self.hbm_budget = int(hbm_budget)
-        dev = torch.device("cuda", self.device)
-        self._streams = [torch.cuda.Stream(dev) for _ in range(self.slots)]
+        # streams made by the library, one per slot (+ the batch stream): torch's
+        # own stream pool hands the same 32 streams out again, and two slots, or
+        # a slot and a capturing batch, must never share one
+        self._raw_streams = []
+        self._streams = [self._new_stream() for _ in range(self.slots)]
         self._free_streams = list(range(self.slots))
         self._lock = threading.Lock()
+        self._dev_lock = threading.Lock()  # allocations vs graph captures (see _buffers)
+        self._batch_stream = self._new_stream() if self.packed else None
+
+    def _new_stream(self):
+        h = ctypes.c_void_p()
+        B.check(B.load().kifmm_stream_create(self.device, ctypes.byref(h)))
+        self._raw_streams.append(h.value)
+        return self.torch.cuda.ExternalStream(h.value, device=self.torch.device("cuda", self.device))
+
+    def close(self):
+        """Wait for the server's streams and release them."""
+        raw, self._raw_streams = getattr(self, "_raw_streams", []), []
+        if raw:
+            self.torch.cuda.synchronize(self.device)
+        for h in raw:
+            B.load().kifmm_stream_destroy(ctypes.c_void_p(h))
+
+    def __del__(self):
+        self.close()
 
     def _kernel(self, req):
         if req.kernel == "laplace":
@@ -178,6 +293,26 @@ class Server:
         if req.kernel == "k0":
             return C.ModifiedHelmholtzKernel(req.k)
         raise ValueError(f"unknown kernel {req.kernel!r}")
+
+    def _buffers(self, req, s, precision):
+        """A request's device points, plan, density / potential / sum buffers
+        and pinned host potentials.  Made under the server's device lock: an
+        allocation can synchronise with every stream, which must not happen
+        while another thread captures a CUDA graph."""
+        torch = self.torch
+        dev = torch.device("cuda", self.device)
+        n = len(req.x)
+        kern = self._kernel(req)
+        with self._dev_lock:
+            xd = torch.as_tensor(np.ascontiguousarray(req.x, dtype=np.float64), device=dev)
+            yd = torch.as_tensor(np.ascontiguousarray(req.y, dtype=np.float64), device=dev)
+            f = C.FMM(xd, yd, C.Get_Kernel_Functions(kern), C.prepare_numba_functions_on_the_fly(kern),
+                      req.nequiv, req.ncutoff, precision=precision, device=self.device, stream=s.cuda_stream)
+            tau = torch.empty(n, dtype=torch.float64, device=dev)
+            pot = torch.empty(n, dtype=torch.float64, device=dev)
+            tot = torch.empty((), dtype=torch.float64, device=dev)
+            host = torch.empty(n, dtype=torch.float64, pin_memory=True)
+        return xd, yd, f, tau, pot, tot, host
 
     def _run_one(self, req, res, t0):
         torch = self.torch
@@ -187,17 +322,10 @@ class Server:
         try:
             dev = torch.device("cuda", self.device)
             with torch.cuda.device(dev), torch.cuda.stream(s):
-                kern = self._kernel(req)
-                xd = torch.as_tensor(np.ascontiguousarray(req.x, dtype=np.float64), device=dev)
-                yd = torch.as_tensor(np.ascontiguousarray(req.y, dtype=np.float64), device=dev)
-                f = C.FMM(xd, yd, C.Get_Kernel_Functions(kern), C.prepare_numba_functions_on_the_fly(kern),
-                          req.nequiv, req.ncutoff, precision=self.precision, device=self.device,
-                          stream=s.cuda_stream)
+                xd, yd, f, tau_d, pot_d, tot, host = self._buffers(req, s, self.precision)
                 f.build_tree()
                 f.precompute()
                 n = len(req.x)
-                tau_d = torch.empty(n, dtype=torch.float64, device=dev)
-                pot_d = torch.empty(n, dtype=torch.float64, device=dev)
                 for i in range(req.count()):
                     if req.taus is not None:
                         tau_d.copy_(torch.as_tensor(np.ascontiguousarray(req.taus[i], dtype=np.float64)))
@@ -207,13 +335,16 @@ class Server:
                         f.build_expansions(tau_d)
                         f.evaluate_to_points(xd, yd, self.check_self, out=pot_d)
                     elif i == 0:
-                        f.capture_apply(tau_d, pot_d, self.check_self)
+                        with self._dev_lock:
+                            f.capture_apply(tau_d, pot_d, self.check_self)
                     else:
                         f.replay()
-                    pot = pot_d.cpu().numpy()
-                    res.sums.append(float(pot.sum()))
+                    torch.sum(pot_d, dim=0, out=tot)
+                    host.copy_(pot_d, non_blocking=True)
+                    s.synchronize()
+                    res.sums.append(float(tot))
                     if self.keep_pots:
-                        res.pots.append(pot)
+                        res.pots.append(host.numpy().copy())
                 f.synchronize()
                 del f
             res.n, res.napply = n, req.count()
@@ -225,6 +356,143 @@ class Server:
                 self._free_streams.append(si)
         return req, res
 
+    def _setup_packed(self, req, res, t0):
+        """Packed mode, worker thread: plan, tree, operators and the first
+        density of one request on its slot's stream; the request then joins
+        the packed batch for its remaining densities."""
+        torch = self.torch
+        with self._lock:
+            si = self._free_streams.pop()
+        s = self._streams[si]
+        live = _Live(req=req, res=res, si=si)
+        try:
+            dev = torch.device("cuda", self.device)
+            with torch.cuda.device(dev), torch.cuda.stream(s):
+                live.x, live.y, f, live.tau, live.pot, tot, live.host = self._buffers(req, s, "mixed")
+                f.build_tree()
+                f.precompute()
+                n = len(req.x)
+                if req.taus is not None:
+                    live.tau.copy_(torch.as_tensor(np.ascontiguousarray(req.taus[0], dtype=np.float64)))
+                else:
+                    device_density(torch, req.tau_seed, 0, live.tau)
+                f.build_expansions(live.tau)
+                f.evaluate_to_points(live.x, live.y, self.check_self, out=live.pot)
+                torch.sum(live.pot, dim=0, out=tot)
+                live.host.copy_(live.pot, non_blocking=True)
+                f.synchronize()
+                s.synchronize()
+                live.record(self.keep_pots, float(tot))
+                live.f = f
+            res.n, res.napply = n, req.count()
+        except Exception as e:
+            res.error = f"{type(e).__name__}: {e}"
+        return live
+
+    def _run_packed(self, requests, realtime):
+        """The step loop of packed serving.  Every step applies one density of
+        each request in the captured batch (one graph launch), then copies the
+        potentials to pinned host memory.  A request that has had all its
+        densities is done at once (slot and memory released); its lane stays
+        in the graph, computing on its last density, until the next capture.
+        The batch is captured again when the requests that wait to join plus
+        these finished lanes reach half the batch (or nothing live is left),
+        so that captures stay rare against steps."""
+        torch = self.torch
+        sched = Scheduler(requests, self.slots, self.hbm_budget)
+        results = {}
+        t0 = time.perf_counter()
+        setups = {}
+        ready, lanes = [], []
+        batch = None
+        bs = self._batch_stream
+        stats = {"steps": 0, "captures": 0, "member_steps": 0, "idle_lane_steps": 0}
+
+        def complete(live):
+            live.done = True
+            live.res.done = time.perf_counter() - t0
+            with self._lock:
+                self._free_streams.append(live.si)
+            sched.release(live.req)
+
+        with cf.ThreadPoolExecutor(max_workers=self.slots) as pool:
+            while not sched.idle() or ready:
+                now = time.perf_counter() - t0
+                for r in sched.admit(now):
+                    res = Result(rid=r.rid, arrival=r.arrival, admitted=now)
+                    results[r.rid] = res
+                    setups[pool.submit(self._setup_packed, r, res, t0)] = r
+                live = [m for m in lanes if not m.done]
+                if not live and not ready:
+                    # nothing on the GPU from this thread: wait for a setup or an arrival
+                    nxt = sched.next_arrival()
+                    wait = max(nxt - now, 0.0) if nxt is not None else None
+                    if setups:
+                        cf.wait(list(setups), timeout=wait, return_when=cf.FIRST_COMPLETED)
+                    elif wait is not None:
+                        time.sleep(min(wait, 0.05))
+                for fut in [f for f in setups if f.done()]:
+                    lv = fut.result()
+                    del setups[fut]
+                    if lv.res.error or lv.i >= lv.req.count():
+                        complete(lv)
+                    else:
+                        ready.append(lv)
+                idle = len(lanes) - len(live)
+                if ready and (batch is None or not live or len(ready) + idle >= max(1, len(lanes) // 2)):
+                    if batch is not None:
+                        batch.close()
+                        batch = None
+                    for m in lanes:
+                        if m.done:
+                            m.f = None  # the plan goes once no graph uses it
+                    lanes = live + ready
+                    live = list(lanes)
+                    ready = []
+                if not live:
+                    continue
+                with torch.cuda.stream(bs):
+                    if batch is None:
+                        with self._dev_lock:
+                            batch = PackedBatch([m.f for m in lanes], [m.tau for m in lanes],
+                                                [m.pot for m in lanes], bs, self.check_self)
+                        stats["captures"] += 1
+                    seeds, index = [], []
+                    for m in lanes:  # given densities are copied here; fresh ones are drawn by the batch
+                        draw = not m.done and m.req.taus is None
+                        if not m.done and not draw:
+                            m.next_density(torch, bs)
+                        seeds.append(m.req.tau_seed if draw else DRAW_SKIP)
+                        index.append(m.i if draw else 0)
+                    batch.set_draws(seeds, index)
+                    batch.launch()
+                    for m in live:
+                        m.host.copy_(m.pot, non_blocking=True)
+                batch.synchronize()
+                sums = batch.sums()
+                stats["steps"] += 1
+                stats["member_steps"] += len(live)
+                stats["idle_lane_steps"] += len(lanes) - len(live)
+                for r, m in enumerate(lanes):
+                    if m.done:
+                        continue
+                    m.record(self.keep_pots, float(sums[r]))
+                    if m.i >= m.req.count():
+                        complete(m)
+                if all(m.done for m in lanes):
+                    batch.close()
+                    batch = None
+                    for m in lanes:
+                        m.f = None
+                    lanes = []
+            if batch is not None:
+                batch.close()
+        wall = time.perf_counter() - t0
+        out = summarize(results, wall, self.slots, self.hbm_budget)
+        out.update(stats)
+        out["mean_batch"] = stats["member_steps"] / stats["steps"] if stats["steps"] else 0.0
+        return results, out
+
     def run(self, requests, realtime=True):
         """Serve ``requests``; with realtime=True a request is not admitted
         before its arrival time (seconds from the start), otherwise all are
@@ -232,6 +500,8 @@ class Server:
         if not realtime:
             for r in requests:
                 r.arrival = 0.0
+        if self.packed:
+            return self._run_packed(requests, realtime)
         sched = Scheduler(requests, self.slots, self.hbm_budget)
         results = {}
         t0 = time.perf_counter()
@@ -258,6 +528,34 @@ class Server:
                     del running[fut]
         wall = time.perf_counter() - t0
         return results, summarize(results, wall, self.slots, self.hbm_budget)
+
+
+@dataclass
+class _Live:
+    """A request of the packed server between its setup and its last density."""
+    req: Request
+    res: Result
+    si: int
+    f: object = None
+    x: object = None
+    y: object = None
+    tau: object = None
+    pot: object = None
+    host: object = None
+    i: int = 0  # next density index
+    done: bool = False
+
+    def next_density(self, torch, stream):
+        if self.req.taus is not None:
+            self.tau.copy_(torch.as_tensor(np.ascontiguousarray(self.req.taus[self.i], dtype=np.float64)))
+        else:
+            device_density(torch, self.req.tau_seed, self.i, self.tau)
+
+    def record(self, keep, total):
+        self.res.sums.append(total)
+        if keep:
+            self.res.pots.append(self.host.numpy().copy())
+        self.i += 1
 
 
 def summarize(results, wall, slots, budget):

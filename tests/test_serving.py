@@ -129,3 +129,72 @@ def test_each_result_same_alone_and_in_the_mix():
         kinds.add(reqs[rid].kernel)
     assert kinds == {"laplace", "k0"}
     assert st_mix["p99_ms"] >= st_mix["p50_ms"] > 0
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA GPU")
+def test_packed_batch_matches_each_plans_own_apply():
+    """kifmm_batch_capture / kifmm_batch_launch: Laplace and K0 plans of
+    different sizes (one small enough to be a single leaf) in one packed graph,
+    three densities; each plan's potentials against its own unpacked apply."""
+    import torch
+
+    import pykifmm2d_b200 as P
+    rng = np.random.default_rng(21)
+    specs = [(25_000, P.LaplaceKernel()), (7_000, P.ModifiedHelmholtzKernel(10.0)), (50, P.LaplaceKernel()),
+             (60_000, P.ModifiedHelmholtzKernel(1.0)), (12_000, P.LaplaceKernel())]
+    bs = torch.cuda.Stream()
+    fmms, xs, taus, pots, hosts = [], [], [], [], []
+    for n, kern in specs:
+        x, y = S._mixture_points(rng, n)
+        xs.append((x, y, kern))
+        s = torch.cuda.Stream()
+        xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
+        f = P.FMM(xd, yd, P.Get_Kernel_Functions(kern), P.prepare_numba_functions_on_the_fly(kern), 32, 64,
+                  precision="mixed", stream=s.cuda_stream)
+        f.build_tree()
+        f.precompute()
+        fmms.append(f)
+        taus.append(torch.empty(n, dtype=torch.float64, device="cuda"))
+        pots.append(torch.empty(n, dtype=torch.float64, device="cuda"))
+    torch.cuda.synchronize()
+    dens = [[rng.standard_normal(n) for n, _ in specs] for _ in range(3)]
+    with torch.cuda.stream(bs):
+        for t, d in zip(taus, dens[0]):
+            t.copy_(torch.from_numpy(d))
+        b = S.PackedBatch(fmms, taus, pots, bs)
+        tiles, leaves = b.info()
+        assert tiles > 0 and leaves > 0
+        got = []
+        for k in range(3):
+            for t, d in zip(taus, dens[k]):
+                t.copy_(torch.from_numpy(d))
+            b.launch()
+            got.append([p.cpu().numpy() for p in pots])
+        b.synchronize()
+        b.close()
+    for r, (x, y, kern) in enumerate(xs):
+        g = P.FMM(x, y, P.Get_Kernel_Functions(kern), P.prepare_numba_functions_on_the_fly(kern), 32, 64,
+                  precision="mixed")
+        for k in range(3):
+            g.build_expansions(dens[k][r])
+            ref = g.evaluate_to_points(x, y, True)
+            assert _rel(got[k][r], ref) <= TOL, (r, k)
+
+
+@pytest.mark.gpu
+@pytest.mark.skipif(not has_gpu(), reason="needs a CUDA GPU")
+def test_packed_server_same_alone_and_in_the_mix():
+    """Packed serving: each request's potentials in the packed mix against the
+    same request served alone (one at a time, unpacked)."""
+    reqs = S.make_stream(10, rate_per_s=0.0, seed=12, nmin=500, nmax=40_000, k0_frac=0.4, applies=(2, 5))
+    mix, st = S.Server(slots=6, packed=True).run(reqs, realtime=False)
+    assert st["failed"] == 0, [r.error for r in mix.values() if r.error]
+    assert st["captures"] >= 1 and st["mean_batch"] > 1
+    alone, st_alone = S.Server(slots=1).run(reqs, realtime=False)
+    assert st_alone["failed"] == 0
+    for rid, r in mix.items():
+        a = alone[rid]
+        assert len(r.pots) == len(a.pots) == reqs[rid].count()
+        for p, q in zip(r.pots, a.pots):
+            assert _rel(p, q) <= TOL
