@@ -183,6 +183,9 @@ struct kifmm_plan {
     kifmm::DBuf<int32_t> ncoll;      // [n_nodes][9] colleagues by direction (dx+1)*3+(dy+1)
     kifmm::DBuf<int32_t> leaf_list, p2m_list;
     kifmm::DBuf<int32_t> leaf_rec;   // [n_leaf_list][32] leaf records (passes.cuh, LeafRec)
+    kifmm::DBuf<int32_t> m2l_perm;   // [n_ent] M2L target order of the entries (build_m2l_order)
+    kifmm::DBuf<uint16_t> m2l_key;   // [n_ent] direction mask of each entry (256: not split)
+    kifmm::DBuf<unsigned> m2l_hist;  // [MAX_LEVELS + 1][257] counts, then cursors
     kifmm::DBuf<uint32_t> list_tiles;
     int64_t n_leaf_list = 0, n_p2m_list = 0;
     int64_t leaf_loff[KIFMM_MAX_LEVELS + 1] = {};  // leaf_list range of each level
@@ -303,6 +306,7 @@ inline long long plan_wait_polls(const kifmm_plan *P) {
 constexpr int KIFMM_SCAL_SORT_ERR = 13;  // a radix-sort look-back wait that ran out
 constexpr int KIFMM_SCAL_PASS_ERR = 14;
 constexpr int KIFMM_SCAL_TC_ERR = 15;
+constexpr int KIFMM_SCAL_WORDS = 16;
 
 // Lanes of the warp holding the same 8-bit digit d (d = 256: no key; such
 // lanes match each other only): nine ballots, one per bit, each lane keeping

@@ -357,13 +357,13 @@ __device__ __forceinline__ void m2l_tc_tile(const TcArgs &T, const int64_t tile)
     }
     if (tid == 0) sdir[10] = 0;
     __syncthreads();
-    if (tid < TN) {
-        const int64_t e = e0 + tid;
-        const bool act = e < ne && !(A.ent[eoff + e] & 1);
+    if (tid < TN) {  // the tile's targets in M2L target order; sact = 1 + index in the level, 0: none
+        const int64_t e = e0 + tid, ej = e < ne ? (int64_t)A.m2l_perm[eoff + e] : -1;
+        const bool act = ej >= 0 && !(A.ent[ej] & 1);
         int kcol = -1000000;
         int gs[8];
 #pragma unroll
-        for (int dd = 0; dd < 8; dd++) gs[dd] = act ? T.pre.src8[(eoff + e) * 8 + dd] : -1;
+        for (int dd = 0; dd < 8; dd++) gs[dd] = act ? T.pre.src8[ej * 8 + dd] : -1;
 #pragma unroll
         for (int dd = 0; dd < 8; dd++) {
             const int grp = gs[dd];
@@ -376,7 +376,7 @@ __device__ __forceinline__ void m2l_tc_tile(const TcArgs &T, const int64_t tile)
             sshift[tid * 8 + dd] = (F == TC_INT8 && grp >= 0) ? kcol - T.pre.gexp[grp] : 0;
         }
         stau[tid] = F == TC_INT8 ? ldexp(1.0, 7 * kcol) : 1.0;
-        sact[tid] = act;
+        sact[tid] = act ? (int)(ej - eoff) + 1 : 0;
     }
     if (tid == 0) {
         for (int i = 0; i < S; i++) {
@@ -566,7 +566,7 @@ __device__ __forceinline__ void m2l_tc_tile(const TcArgs &T, const int64_t tile)
                 for (int c = 0; c < 16; c++) {
                     const int j = cc * 16 + c;
                     if (sact[j]) {
-                        const int64_t cg = A.T.off[lt1] + 4 * (e0 + j);
+                        const int64_t cg = A.T.off[lt1] + 4 * (int64_t)(sact[j] - 1);
                         A.udown[(size_t)cg * Q + r] = y[c] * sig * stau[j];
                     }
                 }

@@ -243,6 +243,7 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
     int *ssrc = (int *)(sm_md + (2 * stage_d > (size_t)MD_TE * (Q4 + 1) ? 2 * stage_d : (size_t)MD_TE * (Q4 + 1)));
     __shared__ __align__(8) uint64_t bars[2];
     __shared__ int sact[MD_TE];
+    __shared__ int sdir[8], scm[8], snd;  // active directions, their 8-target column tiles with a source
     pdl_trigger();
     const int64_t b = blockIdx.x;
     int l = M.lmin;
@@ -250,11 +251,11 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
     const int64_t e0 = (b - M.tile_off[l]) * MD_TE, ne = A.T.ne[l], eoff = A.T.eoff[l];
     const double *opl = A.ops + (size_t)(l + 1) * A.stride + A.off_m2l;  // target level's operators
     pdl_wait();  // u_up comes from the M2M chain
-    if (tid < MD_TE) {
-        const int64_t e = e0 + tid;
-        const bool act = e < ne && !(A.ent[eoff + e] & 1);
-        const int p = act ? A.ent_node[eoff + e] : -1;
-        sact[tid] = act;
+    if (tid < MD_TE) {  // the tile's targets in M2L target order; sact = 1 + index in the level, 0: none
+        const int64_t e = e0 + tid, ej = e < ne ? (int64_t)A.m2l_perm[eoff + e] : -1;
+        const bool act = ej >= 0 && !(A.ent[ej] & 1);
+        const int p = act ? A.ent_node[ej] : -1;
+        sact[tid] = act ? (int)(ej - eoff) + 1 : 0;
         for (int dd = 0; dd < 8; dd++) {
             const int d = dd < 4 ? dd : dd + 1;
             ssrc[tid * 8 + dd] = act ? m2l_source_entry(A.ncoll, A.nent, A.nbot, A.ntop, p, d) : -1;
@@ -265,24 +266,41 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
         mbar_init(smem_u32(&bars[1]));
     }
     __syncthreads();
-    const int nkc = (Q4 + MD_KC - 1) / MD_KC, nst = 8 * nkc;
+    // Work skipped: a direction no target of the block has a source in, and
+    // within a direction each 8-target column tile without one (a V-list
+    // group is absent where the colleague is missing, a leaf or empty).
+    if (tid < 8) {
+        int m = 0;
+        for (int n = 0; n < MD_TE; n++) m |= (ssrc[n * 8 + tid] >= 0) << (n >> 3);
+        scm[tid] = m;
+    }
+    __syncthreads();
+    if (tid == 0) {
+        int k = 0;
+        for (int dd = 0; dd < 8; dd++)
+            if (scm[dd]) sdir[k++] = dd;
+        snd = k;
+    }
+    __syncthreads();
+    const int nkc = (Q4 + MD_KC - 1) / MD_KC, nst = snd * nkc;
     // one thread issues all copies of stage st into buffer st % 2
     auto issue = [&](int st) {
-        const int dd = st / nkc, d = dd < 4 ? dd : dd + 1, kc = st % nkc, k0 = kc * MD_KC;
-        const int kn = min(MD_KC, Q4 - k0);
+        const int dd = sdir[st / nkc], d = dd < 4 ? dd : dd + 1, kc = st % nkc, k0 = kc * MD_KC;
+        const int kn = min(MD_KC, Q4 - k0), cm = scm[dd];
         double *bs = buf[st & 1];
         const uint32_t bar = smem_u32(&bars[st & 1]);
-        mbar_expect_tx(bar, (uint32_t)(kn * Q4 + MD_TE * kn) * 8u);
+        mbar_expect_tx(bar, (uint32_t)(kn * Q4 + 8 * __popc(cm) * kn) * 8u);
         const double *op = opl + (size_t)d * Q4 * Q4 + (size_t)k0 * Q4;
         for (int c = 0; c < kn; c++) bulk_g2s(smem_u32(bs + (size_t)c * ldo), op + (size_t)c * Q4, (uint32_t)Q4 * 8u, bar);
         double *xs = bs + (size_t)MD_KC * ldo;
         for (int n = 0; n < MD_TE; n++) {
+            if (!((cm >> (n >> 3)) & 1)) continue;
             const int je = ssrc[n * 8 + dd];
             const double *src = je >= 0 ? A.uup + (size_t)(A.T.off[l + 1] + 4 * (je - eoff)) * Q + k0 : M.zero + k0;
             bulk_g2s(smem_u32(xs + (size_t)n * ldx), src, (uint32_t)kn * 8u, bar);
         }
     };
-    if (tid == 0) {
+    if (tid == 0 && nst > 0) {
         issue(0);
         if (nst > 1) issue(1);
     }
@@ -301,7 +319,7 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
         if (!ok) break;
         par[bi] ^= 1u;
         landed++;
-        const int kn = min(MD_KC, Q4 - (st % nkc) * MD_KC);
+        const int kn = min(MD_KC, Q4 - (st % nkc) * MD_KC), cm = scm[sdir[st / nkc]];
         const double *os = buf[bi], *xs = buf[bi] + (size_t)MD_KC * ldo;
         for (int k0 = 0; k0 < kn; k0 += 4) {
             double bv[4];
@@ -313,7 +331,8 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
                 if (rt < nrt) {
                     const double av = os[(size_t)(k0 + t) * ldo + 8 * rt + g];
 #pragma unroll
-                    for (int c = 0; c < 4; c++) dmma_8x8x4(acc[i][c][0], acc[i][c][1], av, bv[c]);
+                    for (int c = 0; c < 4; c++)
+                        if ((cm >> c) & 1) dmma_8x8x4(acc[i][c][0], acc[i][c][1], av, bv[c]);
                 }
             }
         }
@@ -343,10 +362,9 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
             }
     }
     __syncthreads();
-    const size_t child0 = (size_t)A.T.off[l + 1] + 4 * (size_t)e0;
     for (int n = warp; n < MD_TE; n += MD_THREADS / 32) {
         if (!sact[n]) continue;
-        double *dst = A.udown + (child0 + 4 * (size_t)n) * Q;
+        double *dst = A.udown + ((size_t)A.T.off[l + 1] + 4 * (size_t)(sact[n] - 1)) * Q;
         for (int r = lane; r < Q4; r += 32) dst[r] = cs[(size_t)n * (Q4 + 1) + r];
     }
 }
@@ -483,6 +501,7 @@ PassArgs make_pass_args(kifmm_plan *P) {
     A.uup = P->uup.p;
     A.udown = P->udown.p;
     A.leaf_rec = P->leaf_rec.p;
+    A.m2l_perm = P->m2l_perm.p;
     A.taylor = P->l2p_taylor.p;
     A.leaf_coef = P->leaf_coef.p;
     return A;
@@ -513,6 +532,89 @@ void build_leaf_records(kifmm_plan *P) {
     PassArgs A = make_pass_args(P);
     k_leaf_records<<<grid_for(P->n_leaf_list, 128, P->num_sms * 8), 128, 0, P->stream>>>(
         A, P->leaf_list.p, P->n_leaf_list, P->leaf_rec.p);
+    KIFMM_LAUNCHED();
+}
+
+// M2L target order.  The entries of each level are grouped by the set of
+// directions in which they have V-list sources (an 8-bit mask; entries that
+// are not split go last), so that an M2L tile of consecutive targets mostly
+// shares one set and skips every absent direction instead of multiplying
+// zero vectors.  The mask depends on the tree only: the order is built once
+// per tree.  Within a group the order is whatever the atomics give; the M2L
+// result of a target does not depend on which other targets share its tile.
+constexpr int M2L_KEYS = 257;
+__global__ void k_m2l_keys(PassArgs A, int64_t n_ent, uint16_t *__restrict__ key, unsigned *__restrict__ hist) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const bool in = j < n_ent;
+    unsigned bin = 0xffffffffu;
+    if (in) {
+        const uint64_t ej = A.ent[j];
+        const int l = (int)(ej >> ENT_LEVEL_SHIFT);
+        int k = 256;
+        if (!(ej & 1)) {
+            k = 0;
+            for (int dd = 0; dd < 8; dd++) {
+                const int d = dd < 4 ? dd : dd + 1;
+                k |= (m2l_source_entry(A.ncoll, A.nent, A.nbot, A.ntop, A.ent_node[j], d) >= 0) << dd;
+            }
+        }
+        key[j] = (uint16_t)k;
+        bin = (unsigned)(l * M2L_KEYS + k);
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, bin);
+    if (in && (int)(threadIdx.x & 31) == __ffs(peers) - 1) atomicAdd(&hist[bin], (unsigned)__popc(peers));
+}
+
+// counts -> first position of each (level, key) group, from the level's
+// eoff: one block per level, an exclusive scan over the 257 keys
+constexpr int M2L_SCAN_THREADS = 288;  // >= M2L_KEYS, a whole number of warps
+__global__ void __launch_bounds__(M2L_SCAN_THREADS) k_m2l_cursors(LevelTable T, unsigned *__restrict__ hist) {
+    __shared__ unsigned wsum[M2L_SCAN_THREADS / 32];
+    const int l = blockIdx.x, k = threadIdx.x, lane = k & 31, w = k >> 5;
+    const unsigned c = k < M2L_KEYS ? hist[l * M2L_KEYS + k] : 0u;
+    unsigned v = c;  // inclusive scan within the warp
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned u = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += u;
+    }
+    if (lane == 31) wsum[w] = v;
+    __syncthreads();
+    unsigned before = (unsigned)T.eoff[l];
+    for (int i = 0; i < w; i++) before += wsum[i];
+    if (k < M2L_KEYS) hist[l * M2L_KEYS + k] = before + v - c;
+}
+
+__global__ void k_m2l_place(const uint64_t *__restrict__ ent, const uint16_t *__restrict__ key, int64_t n_ent,
+                            unsigned *__restrict__ cursor, int32_t *__restrict__ perm) {
+    const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const bool in = j < n_ent;
+    const int lane = threadIdx.x & 31;
+    const unsigned bin = in ? (unsigned)((int)(ent[j] >> ENT_LEVEL_SHIFT) * M2L_KEYS + key[j]) : 0xffffffffu;
+    const unsigned peers = __match_any_sync(0xffffffffu, bin);
+    const int leader = __ffs(peers) - 1;
+    unsigned base = 0;
+    if (in && lane == leader) base = atomicAdd(&cursor[bin], (unsigned)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (in) perm[base + __popc(peers & ((1u << lane) - 1))] = (int32_t)j;
+}
+
+void build_m2l_order(kifmm_plan *P) {
+    const int64_t n = P->n_ent;
+    P->m2l_perm.alloc(n ? n : 1);
+    if (!n) return;
+    KIFMM_REQUIRE(P->L <= MAX_LEVELS + 1 && n < (1ll << 31), KIFMM_ERR_ARG, "M2L order: tree too large");
+    P->m2l_key.alloc(n);
+    P->m2l_hist.alloc((size_t)(MAX_LEVELS + 1) * M2L_KEYS);
+    KIFMM_CUDA(cudaMemsetAsync(P->m2l_hist.p, 0, (size_t)(MAX_LEVELS + 1) * M2L_KEYS * sizeof(unsigned), P->stream));
+    PassArgs A = make_pass_args(P);
+    const unsigned gr = (unsigned)((n + 255) / 256);
+    k_m2l_keys<<<gr, 256, 0, P->stream>>>(A, n, P->m2l_key.p, P->m2l_hist.p);
+    KIFMM_LAUNCHED();
+    k_m2l_cursors<<<(unsigned)std::min(P->L, MAX_LEVELS + 1), M2L_SCAN_THREADS, 0, P->stream>>>(P->lt, P->m2l_hist.p);
+    KIFMM_LAUNCHED();
+    k_m2l_place<<<gr, 256, 0, P->stream>>>((const uint64_t *)P->ent.p, P->m2l_key.p, n, P->m2l_hist.p,
+                                           P->m2l_perm.p);
     KIFMM_LAUNCHED();
 }
 
@@ -933,6 +1035,16 @@ static void launch_lvl_gemm(kifmm_plan *P, const PassArgs &A, int l) {
 void launch_m2m_d(kifmm_plan *P, const PassArgs &A, int l) { launch_lvl_gemm<0>(P, A, l); }
 void launch_l2l_d(kifmm_plan *P, const PassArgs &A, int l) { launch_lvl_gemm<1>(P, A, l); }
 
+// the upward M2M over levels L-2 .. 2 and the downward L2L over 2 .. L-2
+void run_m2m_levels(kifmm_plan *P, const PassArgs &A) {
+    for (int l = P->L - 2; l >= 2; l--)
+        if (P->lt.ne[l]) launch_m2m_d(P, A, l);
+}
+void run_l2l_levels(kifmm_plan *P, const PassArgs &A) {
+    for (int l = 2; l <= P->L - 2; l++)
+        if (P->lt.ne[l]) launch_l2l_d(P, A, l);
+}
+
 // Buffers of an apply, its cleared flags and expansions, and the densities in
 // tree order.
 void apply_prologue(kifmm_plan *P) {
@@ -947,7 +1059,8 @@ void apply_prologue(kifmm_plan *P) {
     // error flags of the level passes and the tensor-core M2L, and the
     // expansions, cleared first so that the kernels below form one chain of
     // programmatic dependent launches
-    KIFMM_CUDA(cudaMemsetAsync(P->scal.p + KIFMM_SCAL_PASS_ERR, 0, 2 * sizeof(unsigned long long), s));
+    KIFMM_CUDA(cudaMemsetAsync(P->scal.p + KIFMM_SCAL_PASS_ERR, 0,
+                               (KIFMM_SCAL_WORDS - KIFMM_SCAL_PASS_ERR) * sizeof(unsigned long long), s));
     KIFMM_CUDA(cudaMemsetAsync(P->uup.p, 0, (size_t)NN * Q * sizeof(double), s));
     KIFMM_CUDA(cudaMemsetAsync(P->udown.p, 0, (size_t)NN * Q * sizeof(double), s));
     if (P->opt.planned) build_plan_matrices(P);  // first apply after build_tree / precompute
@@ -976,8 +1089,7 @@ void run_upward_downward(kifmm_plan *P) {
     }
     {
         PhaseScope ph_m2m(P, KIFMM_PHASE_M2M);
-        for (int l = L - 2; l >= 2; l--)
-            if (P->lt.ne[l]) launch_m2m_d(P, A, l);
+        run_m2m_levels(P, A);
     }
     if (Q % 2 == 0 && 4 * Q <= 8 * MD_MT * 8) {
         // FP64 tensor path: all levels' M2L in one launch, then the L2L chain
@@ -1006,8 +1118,7 @@ void run_upward_downward(kifmm_plan *P) {
             }
         }
         PhaseScope ph(P, KIFMM_PHASE_L2L);
-        for (int l = 2; l <= L - 2; l++)
-            if (P->lt.ne[l]) launch_l2l_d(P, A, l);
+        run_l2l_levels(P, A);
         return;
     }
     PhaseScope ph(P, KIFMM_PHASE_M2L);

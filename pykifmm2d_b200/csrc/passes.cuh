@@ -23,6 +23,7 @@ struct PassArgs {
     double *pots;
     double *uup, *udown;
     const int32_t *leaf_rec;  // [n_leaf_list][LEAF_REC_WORDS] leaf records (build_leaf_records)
+    const int32_t *m2l_perm;  // [n_ent] entries of each level in M2L target order (build_m2l_order)
     const double *taylor;  // Laplace L2P coefficients map, or null
     const double *leaf_coef;  // [leaf_list index][2p+1] Taylor coefficients of the leaves (mixed form)
 };
@@ -69,6 +70,7 @@ enum LeafRec : int {
     LEAF_REC_WORDS = 32
 };
 void build_leaf_records(kifmm_plan *P);
+void build_m2l_order(kifmm_plan *P);
 
 // FP64 tensor-core MMA (mma.sync m8n8k4 .f64): D = A B + D with fragments
 // A[row = lane/4][k = lane%4], B[k = lane%4][n = lane/4],

@@ -604,6 +604,8 @@ void launch_eval_targets_d(kifmm_plan *P, const PassArgs &A, const double *tx, c
                            int check_self, double *pot);
 void launch_m2m_d(kifmm_plan *P, const PassArgs &A, int l);
 void launch_l2l_d(kifmm_plan *P, const PassArgs &A, int l);
+void run_m2m_levels(kifmm_plan *P, const PassArgs &A);
+void run_l2l_levels(kifmm_plan *P, const PassArgs &A);
 
 // P2M and M2M of the mixed apply
 void mixed_upward(kifmm_plan *P, const PassArgs &A) {
@@ -613,15 +615,13 @@ void mixed_upward(kifmm_plan *P, const PassArgs &A) {
         else launch_p2m_d(P, A);
     }
     PhaseScope ph(P, KIFMM_PHASE_M2M);
-    for (int l = P->L - 2; l >= 2; l--)
-        if (P->lt.ne[l]) launch_m2m_d(P, A, l);
+    run_m2m_levels(P, A);
 }
 
 // the L2L chain after the M2L
 void mixed_l2l(kifmm_plan *P, const PassArgs &A) {
     PhaseScope ph(P, KIFMM_PHASE_L2L);
-    for (int l = 2; l <= P->L - 2; l++)
-        if (P->lt.ne[l]) launch_l2l_d(P, A, l);
+    run_l2l_levels(P, A);
 }
 
 void run_passes_mixed(kifmm_plan *P) {

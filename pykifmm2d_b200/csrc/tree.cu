@@ -31,6 +31,7 @@
 
 namespace kifmm {
 void build_leaf_records(kifmm_plan *P);  // passes.cu
+void build_m2l_order(kifmm_plan *P);     // passes.cu
 }
 
 namespace kifmm {
@@ -846,7 +847,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     cudaMemcpyKind kind = mem == KIFMM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     KIFMM_CUDA(cudaMemcpyAsync(P->x.p, x, n * sizeof(double), kind, s));
     KIFMM_CUDA(cudaMemcpyAsync(P->y.p, y, n * sizeof(double), kind, s));
-    P->scal.alloc(16);
+    P->scal.alloc(KIFMM_SCAL_WORDS);
     KIFMM_CUDA(cudaMemcpyAsync(P->scal.p, P->hpin + HP_INIT, 16 * sizeof(unsigned long long), cudaMemcpyHostToDevice,
                                s));
     const int TB = 256;
@@ -1071,6 +1072,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     P->n_xlist = (int64_t)c5[4];
     P->have_stats = false;
     build_leaf_records(P);
+    build_m2l_order(P);
     P->have_tree = true;
 }
 
