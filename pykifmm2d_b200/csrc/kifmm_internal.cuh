@@ -185,6 +185,7 @@ struct kifmm_plan {
     kifmm::DBuf<int32_t> leaf_rec;   // [n_leaf_list][32] leaf records (passes.cuh, LeafRec)
     kifmm::DBuf<int32_t> m2l_perm;   // [n_ent] M2L target order of the entries (build_m2l_order)
     kifmm::DBuf<uint16_t> m2l_key;   // [n_ent] direction mask of each entry (256: not split)
+    kifmm::DBuf<int32_t> m2l_src8;   // [n_ent][8] source entry per direction (-1: none)
     kifmm::DBuf<unsigned> m2l_hist;  // [MAX_LEVELS + 1][257] counts, then cursors
     kifmm::DBuf<uint32_t> list_tiles;
     int64_t n_leaf_list = 0, n_p2m_list = 0;
@@ -207,7 +208,6 @@ struct kifmm_plan {
     kifmm::DBuf<double> leaf_coef;   // [n_leaf_list][2p+1] Taylor coefficients per apply
     kifmm::DBuf<unsigned char> tc_pre;  // per-apply slices of the source groups
     kifmm::DBuf<int> tc_gexp;
-    kifmm::DBuf<int> tc_src8;        // [n_ent][8] M2L source entry per direction (per apply)
     // planned applies (planned.cu): P2M, L2P and near-field blocks, built on
     // the first apply after build_tree / precompute
     bool have_mats = false;

@@ -225,7 +225,7 @@ __global__ void k_tc_slices(TcOpsArgs T) {
 struct TcPre {
     unsigned char *slices;   // [n_ent][NS][KP] elements
     int *gexp;               // [n_ent] (INT8)
-    int *src8;               // [n_ent][8] source entry of a split entry per direction (-1: none)
+    const int *src8;         // [n_ent][8] source entry of a split entry per direction (-1: none)
     int KP;
 };
 
@@ -239,10 +239,6 @@ __global__ void k_tc_preslice(PassArgs A, int64_t n_ent, TcPre T) {
     if (j >= n_ent) return;
     const int Q4 = 4 * A.Q;
     int l = (int)(A.ent[j] >> ENT_LEVEL_SHIFT);
-    if (lane < 8) {  // the entry's M2L sources by direction (split entries only)
-        const int d = lane < 4 ? lane : lane + 1;
-        T.src8[j * 8 + lane] = (A.ent[j] & 1) ? -1 : m2l_source_entry(A.ncoll, A.nent, A.nbot, A.ntop, A.ent_node[j], d);
-    }
     int64_t cg = A.T.off[l + 1] + 4 * (j - A.T.eoff[l]);
     const double *u = A.uup + (size_t)cg * A.Q;
     unsigned char *out = T.slices + (size_t)j * TR::NS * T.KP * TR::EB;
@@ -256,16 +252,20 @@ __global__ void k_tc_preslice(PassArgs A, int64_t n_ent, TcPre T) {
             frexp(m * (128.0 / 127.0), &e);  // m * 128/127 < 2^e
             kg = (e >= 0) ? (e + 6) / 7 : -((-e) / 7);
         }
-        const double inv = ldexp(1.0, -7 * kg);
+        // X = rint(u 2^(7 NS - 7 kg)), |X| < 2^(7 NS) 127/128 + 1/2, as NS signed
+        // base-128 digits: the NS - 1 low ones balanced in [-64, 63] (taken
+        // from the bottom with carries), the top one in [-127, 127]; exact
+        // integer work after one rounding
+        const double scale = ldexp(1.0, 7 * TR::NS - 7 * kg);
         for (int c = lane; c < T.KP; c += 32) {
-            double r = c < Q4 ? u[c] * inv : 0.0;
+            long long X = c < Q4 ? __double2ll_rn(u[c] * scale) : 0ll;
 #pragma unroll
-            for (int i = 0; i < TR::NS; i++) {
-                r *= 128.0;
-                double q = rint(r);
-                r -= q;
+            for (int i = TR::NS - 1; i > 0; i--) {
+                const long long q = ((X + 64) & 127) - 64;
                 ((int8_t *)out)[(size_t)i * T.KP + c] = (int8_t)q;
+                X = (X - q) >> 7;
             }
+            ((int8_t *)out)[c] = (int8_t)X;
         }
         if (lane == 0) T.gexp[j] = kg;
     } else {
@@ -654,10 +654,9 @@ static int64_t tc_prepare_t(kifmm_plan *P, const PassArgs &A, TcArgs &T) {
     pre.KP = g.KP;
     P->tc_pre.alloc((size_t)P->n_ent * TR::NS * g.KP * TR::EB);
     P->tc_gexp.alloc(P->n_ent);
-    P->tc_src8.alloc((size_t)8 * P->n_ent);
     pre.slices = P->tc_pre.p;
     pre.gexp = P->tc_gexp.p;
-    pre.src8 = P->tc_src8.p;
+    pre.src8 = P->m2l_src8.p;  // built with the tree
     launch_pdl(k_tc_preslice<F>, dim3(grid_for(P->n_ent * 32, 256)), dim3(256), 0, P->stream, A, P->n_ent, pre);
     T = TcArgs{};
     T.A = A;

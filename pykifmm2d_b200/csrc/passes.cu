@@ -254,12 +254,8 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
     if (tid < MD_TE) {  // the tile's targets in M2L target order; sact = 1 + index in the level, 0: none
         const int64_t e = e0 + tid, ej = e < ne ? (int64_t)A.m2l_perm[eoff + e] : -1;
         const bool act = ej >= 0 && !(A.ent[ej] & 1);
-        const int p = act ? A.ent_node[ej] : -1;
         sact[tid] = act ? (int)(ej - eoff) + 1 : 0;
-        for (int dd = 0; dd < 8; dd++) {
-            const int d = dd < 4 ? dd : dd + 1;
-            ssrc[tid * 8 + dd] = act ? m2l_source_entry(A.ncoll, A.nent, A.nbot, A.ntop, p, d) : -1;
-        }
+        for (int dd = 0; dd < 8; dd++) ssrc[tid * 8 + dd] = act ? A.m2l_src8[ej * 8 + dd] : -1;
     }
     if (tid == 0) {
         mbar_init(smem_u32(&bars[0]));
@@ -502,6 +498,7 @@ PassArgs make_pass_args(kifmm_plan *P) {
     A.udown = P->udown.p;
     A.leaf_rec = P->leaf_rec.p;
     A.m2l_perm = P->m2l_perm.p;
+    A.m2l_src8 = P->m2l_src8.p;
     A.taylor = P->l2p_taylor.p;
     A.leaf_coef = P->leaf_coef.p;
     return A;
@@ -543,21 +540,25 @@ void build_leaf_records(kifmm_plan *P) {
 // per tree.  Within a group the order is whatever the atomics give; the M2L
 // result of a target does not depend on which other targets share its tile.
 constexpr int M2L_KEYS = 257;
-__global__ void k_m2l_keys(PassArgs A, int64_t n_ent, uint16_t *__restrict__ key, unsigned *__restrict__ hist) {
+__global__ void k_m2l_keys(PassArgs A, int64_t n_ent, uint16_t *__restrict__ key, int32_t *__restrict__ src8,
+                           unsigned *__restrict__ hist) {
     const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const bool in = j < n_ent;
     unsigned bin = 0xffffffffu;
     if (in) {
         const uint64_t ej = A.ent[j];
         const int l = (int)(ej >> ENT_LEVEL_SHIFT);
-        int k = 256;
-        if (!(ej & 1)) {
-            k = 0;
-            for (int dd = 0; dd < 8; dd++) {
-                const int d = dd < 4 ? dd : dd + 1;
-                k |= (m2l_source_entry(A.ncoll, A.nent, A.nbot, A.ntop, A.ent_node[j], d) >= 0) << dd;
-            }
+        const bool split = !(ej & 1);
+        int k = split ? 0 : 256, sv[8];
+#pragma unroll
+        for (int dd = 0; dd < 8; dd++) {
+            const int d = dd < 4 ? dd : dd + 1;
+            sv[dd] = split ? m2l_source_entry(A.ncoll, A.nent, A.nbot, A.ntop, A.ent_node[j], d) : -1;
+            if (sv[dd] >= 0) k |= 1 << dd;
         }
+        int4 *o = (int4 *)(src8 + 8 * j);
+        o[0] = make_int4(sv[0], sv[1], sv[2], sv[3]);
+        o[1] = make_int4(sv[4], sv[5], sv[6], sv[7]);
         key[j] = (uint16_t)k;
         bin = (unsigned)(l * M2L_KEYS + k);
     }
@@ -605,11 +606,12 @@ void build_m2l_order(kifmm_plan *P) {
     if (!n) return;
     KIFMM_REQUIRE(P->L <= MAX_LEVELS + 1 && n < (1ll << 31), KIFMM_ERR_ARG, "M2L order: tree too large");
     P->m2l_key.alloc(n);
+    P->m2l_src8.alloc((size_t)8 * n);
     P->m2l_hist.alloc((size_t)(MAX_LEVELS + 1) * M2L_KEYS);
     KIFMM_CUDA(cudaMemsetAsync(P->m2l_hist.p, 0, (size_t)(MAX_LEVELS + 1) * M2L_KEYS * sizeof(unsigned), P->stream));
     PassArgs A = make_pass_args(P);
     const unsigned gr = (unsigned)((n + 255) / 256);
-    k_m2l_keys<<<gr, 256, 0, P->stream>>>(A, n, P->m2l_key.p, P->m2l_hist.p);
+    k_m2l_keys<<<gr, 256, 0, P->stream>>>(A, n, P->m2l_key.p, P->m2l_src8.p, P->m2l_hist.p);
     KIFMM_LAUNCHED();
     k_m2l_cursors<<<(unsigned)std::min(P->L, MAX_LEVELS + 1), M2L_SCAN_THREADS, 0, P->stream>>>(P->lt, P->m2l_hist.p);
     KIFMM_LAUNCHED();

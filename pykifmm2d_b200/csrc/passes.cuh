@@ -24,6 +24,7 @@ struct PassArgs {
     double *uup, *udown;
     const int32_t *leaf_rec;  // [n_leaf_list][LEAF_REC_WORDS] leaf records (build_leaf_records)
     const int32_t *m2l_perm;  // [n_ent] entries of each level in M2L target order (build_m2l_order)
+    const int32_t *m2l_src8;  // [n_ent][8] V-list source entry of a split entry per direction, -1: none
     const double *taylor;  // Laplace L2P coefficients map, or null
     const double *leaf_coef;  // [leaf_list index][2p+1] Taylor coefficients of the leaves (mixed form)
 };
