@@ -72,8 +72,10 @@ enum {
     KIFMM_M2L_BF16X3 = 2,     /* tcgen05 kind::f16, bf16 hi/lo, 3 products, FP32 accumulate */
     KIFMM_M2L_FP16X3 = 3,     /* tcgen05 kind::f16, fp16 hi/lo with scaling, 3 products */
     KIFMM_M2L_FP64 = 4,       /* FP64 tiles (the KIFMM_PREC_FP64 form) */
-    KIFMM_M2L_INT8 = 5        /* tcgen05 kind::i8: operator and vectors as five signed 7-bit
+    KIFMM_M2L_INT8 = 5,       /* tcgen05 kind::i8: operator and vectors as five signed 7-bit
                                  slices, exact int32 accumulation, FP64 reconstruction */
+    KIFMM_M2L_INT8X4 = 6      /* the same with four slices (10 slice products, ~2^-28 of the
+                                 row and column scales instead of ~2^-35), 128 targets per tile */
 };
 
 typedef struct kifmm_options {

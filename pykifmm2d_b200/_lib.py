@@ -16,7 +16,7 @@ MEM_HOST, MEM_DEVICE = 0, 1
 KERNEL_LAPLACE, KERNEL_MOD_HELMHOLTZ, KERNEL_HELMHOLTZ = 0, 1, 2
 PREC_FP64, PREC_MIXED = 0, 1
 E2C_DENSE, E2C_CIRCULANT = 0, 1
-M2L_AUTO, M2L_FP32, M2L_BF16X3, M2L_FP16X3, M2L_FP64, M2L_INT8 = 0, 1, 2, 3, 4, 5
+M2L_AUTO, M2L_FP32, M2L_BF16X3, M2L_FP16X3, M2L_FP64, M2L_INT8, M2L_INT8X4 = 0, 1, 2, 3, 4, 5, 6
 MAX_LEVELS = 30
 NOALLOC_MAX_POINTS = 1048576
 PHASES = ["tree", "sort", "precompute", "p2m", "m2m", "m2l", "leaf", "targets", "l2l", "operators", "closure", "entries", "nodes"]

@@ -212,7 +212,7 @@ def get_level_information(node_width, theta, radii="reference"):
 
 _PREC = {"fp64": B.PREC_FP64, "plain": B.PREC_FP64, "mixed": B.PREC_MIXED}
 _M2L = {"auto": B.M2L_AUTO, "fp32": B.M2L_FP32, "bf16x3": B.M2L_BF16X3, "fp16x3": B.M2L_FP16X3,
-        "fp64": B.M2L_FP64, "int8": B.M2L_INT8}
+        "fp64": B.M2L_FP64, "int8": B.M2L_INT8, "int8x4": B.M2L_INT8X4}
 
 
 class FMM(object):

@@ -288,7 +288,7 @@ int kifmm_plan_create(const kifmm_kernel *kernel, int32_t nequiv, int32_t ncutof
         if (opts) o = *opts;
         KIFMM_REQUIRE(o.precision == KIFMM_PREC_FP64 || o.precision == KIFMM_PREC_MIXED, KIFMM_ERR_ARG,
                       "unknown precision");
-        KIFMM_REQUIRE(o.m2l >= KIFMM_M2L_AUTO && o.m2l <= KIFMM_M2L_INT8, KIFMM_ERR_ARG, "unknown M2L form");
+        KIFMM_REQUIRE(o.m2l >= KIFMM_M2L_AUTO && o.m2l <= KIFMM_M2L_INT8X4, KIFMM_ERR_ARG, "unknown M2L form");
         if (o.precision == KIFMM_PREC_MIXED && o.m2l == KIFMM_M2L_AUTO) o.m2l = KIFMM_M2L_INT8;
         KIFMM_REQUIRE(o.radii == 0 || o.radii == 1, KIFMM_ERR_ARG, "unknown radii preset");
         KIFMM_REQUIRE(o.e2c == KIFMM_E2C_DENSE || o.e2c == KIFMM_E2C_CIRCULANT, KIFMM_ERR_ARG,

@@ -44,13 +44,16 @@
 
 namespace kifmm {
 
-enum TcForm { TC_INT8 = 0, TC_BF16 = 1, TC_FP16 = 2 };
+enum TcForm { TC_INT8 = 0, TC_BF16 = 1, TC_FP16 = 2, TC_I8S4 = 3 };
 // NS slices per operand, EB bytes per element, KSTEP elements per MMA, NACC
 // accumulators, TN target groups per CTA (MMA N), NCOLS TMEM columns allocated
 template <int F> struct TcTraits;
 template <> struct TcTraits<TC_INT8> { static constexpr int NS = 5, EB = 1, KSTEP = 32, NACC = 5, TN = 96, NCOLS = 512; };
 template <> struct TcTraits<TC_BF16> { static constexpr int NS = 2, EB = 2, KSTEP = 16, NACC = 1, TN = 64, NCOLS = 64; };
 template <> struct TcTraits<TC_FP16> { static constexpr int NS = 2, EB = 2, KSTEP = 16, NACC = 1, TN = 64, NCOLS = 64; };
+template <> struct TcTraits<TC_I8S4> { static constexpr int NS = 4, EB = 1, KSTEP = 32, NACC = 4, TN = 128, NCOLS = 512; };
+// the integer (kind::i8) forms
+template <int F> __host__ __device__ constexpr bool tc_int() { return F == TC_INT8 || F == TC_I8S4; }
 
 constexpr int TC_M = 128;        // MMA M: operator rows per tile (TMEM lanes)
 constexpr int TC_KCB = 64;       // bytes of K per slice row and stage (2 MMA K steps)
@@ -63,7 +66,8 @@ constexpr bool tc_traits_ok() {
     return TR::TN % 16 == 0 && TR::TN >= 16 && TR::TN <= 256 && TR::NACC * TR::TN <= TR::NCOLS &&
            TR::TN <= 32 * TC_GWARPS && TR::TN % 32 == 0 && (TC_KCB / TR::EB) % TR::KSTEP == 0;
 }
-static_assert(tc_traits_ok<TC_INT8>() && tc_traits_ok<TC_BF16>() && tc_traits_ok<TC_FP16>(), "tile shapes");
+static_assert(tc_traits_ok<TC_INT8>() && tc_traits_ok<TC_BF16>() && tc_traits_ok<TC_FP16>() &&
+                  tc_traits_ok<TC_I8S4>(), "tile shapes");
 constexpr double FP16_PRESCALE = 4096.0;
 
 struct TcGeom {
@@ -101,7 +105,7 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
 template <int F>
 __device__ __forceinline__ uint32_t instr_desc() {
     // c_format [4,6), a_format [7,10), b_format [10,13), N>>3 [17,23), M>>4 [24,29)
-    uint32_t fmt = F == TC_INT8 ? ((2u << 4) | (1u << 7) | (1u << 10))    // s32 <- s8 x s8
+    uint32_t fmt = tc_int<F>() ? ((2u << 4) | (1u << 7) | (1u << 10))    // s32 <- s8 x s8
                  : F == TC_BF16 ? ((1u << 4) | (1u << 7) | (1u << 10))    // f32 <- bf16 x bf16
                                 : (1u << 4);                              // f32 <- f16 x f16
     return fmt | ((uint32_t)(TcTraits<F>::TN >> 3) << 17) | ((uint32_t)(TC_M >> 4) << 24);
@@ -109,7 +113,7 @@ __device__ __forceinline__ uint32_t instr_desc() {
 template <int F>
 __device__ __forceinline__ void mma_issue(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
                                           uint32_t accumulate) {
-    if (F == TC_INT8) {
+    if (tc_int<F>()) {
         asm volatile(
             "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
             "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
@@ -157,7 +161,7 @@ __host__ __device__ __forceinline__ double pow2_scale(double max_abs) {
 // split v in (-1, 1) into the form's slices, writing element (row, k) of each
 template <int F>
 __device__ __forceinline__ void put_slices(unsigned char *tile, size_t slice_bytes, uint32_t off, double v) {
-    if (F == TC_INT8) {
+    if (tc_int<F>()) {
         double r = v;
 #pragma unroll
         for (int s = 0; s < TcTraits<F>::NS; s++) {
@@ -242,7 +246,7 @@ __global__ void k_tc_preslice(PassArgs A, int64_t n_ent, TcPre T) {
     int64_t cg = A.T.off[l + 1] + 4 * (j - A.T.eoff[l]);
     const double *u = A.uup + (size_t)cg * A.Q;
     unsigned char *out = T.slices + (size_t)j * TR::NS * T.KP * TR::EB;
-    if (F == TC_INT8) {
+    if (tc_int<F>()) {
         double m = 0.0;
         for (int c = lane; c < Q4; c += 32) m = fmax(m, fabs(u[c]));
         for (int o = 16; o; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
@@ -367,15 +371,15 @@ __device__ __forceinline__ void m2l_tc_tile(const TcArgs &T, const int64_t tile)
 #pragma unroll
         for (int dd = 0; dd < 8; dd++) {
             const int grp = gs[dd];
-            if (F == TC_INT8 && grp >= 0) kcol = max(kcol, T.pre.gexp[grp]);
+            if (tc_int<F>() && grp >= 0) kcol = max(kcol, T.pre.gexp[grp]);
             sgrp[tid * 8 + dd] = grp;
         }
         if (kcol == -1000000) kcol = 0;
         for (int dd = 0; dd < 8; dd++) {
             const int grp = sgrp[tid * 8 + dd];
-            sshift[tid * 8 + dd] = (F == TC_INT8 && grp >= 0) ? kcol - T.pre.gexp[grp] : 0;
+            sshift[tid * 8 + dd] = (tc_int<F>() && grp >= 0) ? kcol - T.pre.gexp[grp] : 0;
         }
-        stau[tid] = F == TC_INT8 ? ldexp(1.0, 7 * kcol) : 1.0;
+        stau[tid] = tc_int<F>() ? ldexp(1.0, 7 * kcol) : 1.0;
         sact[tid] = act ? (int)(ej - eoff) + 1 : 0;
     }
     if (tid == 0) {
@@ -442,13 +446,13 @@ __device__ __forceinline__ void m2l_tc_tile(const TcArgs &T, const int64_t tile)
                 for (int ks = 0; ks < KSTEPS; ks++) {
 #pragma unroll
                     for (int i = 0; i < NS; i++) {
-                        constexpr int JM = F == TC_INT8 ? NS - 1 : 1;
+                        constexpr int JM = tc_int<F>() ? NS - 1 : 1;
 #pragma unroll
                         for (int jj = 0; jj <= JM; jj++) {
                             // int8: the 15 slice pairs with i + j <= 4; f16 forms: hi.hi, hi.lo, lo.hi
-                            if (F == TC_INT8 ? (i + jj > NS - 1) : (i != 0 && jj != 0)) continue;
-                            const int acc = F == TC_INT8 ? i + jj : 0;
-                            const bool first_mma = ks == 0 && i == 0 && (F == TC_INT8 || jj == 0);
+                            if (tc_int<F>() ? (i + jj > NS - 1) : (i != 0 && jj != 0)) continue;
+                            const int acc = tc_int<F>() ? i + jj : 0;
+                            const bool first_mma = ks == 0 && i == 0 && (tc_int<F>() || jj == 0);
                             const uint64_t ad = as + ((uint64_t)(i * A_SLICE + ks * 2 * a_lbo) >> 4);
                             const uint64_t bd = bs + ((uint64_t)(jj * B_SLICE + ks * 2 * b_lbo) >> 4);
                             mma_issue<F>(tmem + acc * TN, ad, bd, idesc, first_mma ? later : 1u);
@@ -545,7 +549,7 @@ __device__ __forceinline__ void m2l_tc_tile(const TcArgs &T, const int64_t tile)
                 for (int s = 0; s < TR::NACC; s++)
                     tmem_ld16_nowait(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * TN + cc * 16), v[s]);
                 tmem_wait_ld();
-                if (F == TC_INT8) {
+                if (tc_int<F>()) {
                     // accumulator s carries weight 2^-7(s+2): combine exactly in int64
                     // (|acc| < 2^31, so the sum stays below 2^60), one conversion per column
 #pragma unroll
@@ -608,11 +612,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 // ------------------------------------------------------------ host side
 bool uses_tensor_m2l(const kifmm_plan *P) {
     return P->opt.precision == KIFMM_PREC_MIXED &&
-           (P->opt.m2l == KIFMM_M2L_INT8 || P->opt.m2l == KIFMM_M2L_BF16X3 || P->opt.m2l == KIFMM_M2L_FP16X3);
+           (P->opt.m2l == KIFMM_M2L_INT8 || P->opt.m2l == KIFMM_M2L_INT8X4 || P->opt.m2l == KIFMM_M2L_BF16X3 ||
+            P->opt.m2l == KIFMM_M2L_FP16X3);
 }
 
 static int form_of(int m2l) {
-    return m2l == KIFMM_M2L_BF16X3 ? TC_BF16 : m2l == KIFMM_M2L_FP16X3 ? TC_FP16 : TC_INT8;
+    return m2l == KIFMM_M2L_BF16X3 ? TC_BF16 : m2l == KIFMM_M2L_FP16X3 ? TC_FP16 : m2l == KIFMM_M2L_INT8X4 ? TC_I8S4 : TC_INT8;
 }
 
 template <int F>
@@ -638,6 +643,7 @@ void build_tc_operators(kifmm_plan *P) {
     switch (form_of(P->opt.m2l)) {
         case TC_BF16: build_tc_ops_t<TC_BF16>(P); break;
         case TC_FP16: build_tc_ops_t<TC_FP16>(P); break;
+        case TC_I8S4: build_tc_ops_t<TC_I8S4>(P); break;
         default: build_tc_ops_t<TC_INT8>(P); break;
     }
 }
@@ -692,6 +698,7 @@ void run_m2l_tensor(kifmm_plan *P, const PassArgs &A) {
     switch (form_of(P->opt.m2l)) {
         case TC_BF16: run_m2l_tensor_t<TC_BF16>(P, A); break;
         case TC_FP16: run_m2l_tensor_t<TC_FP16>(P, A); break;
+        case TC_I8S4: run_m2l_tensor_t<TC_I8S4>(P, A); break;
         default: run_m2l_tensor_t<TC_INT8>(P, A); break;
     }
 }
@@ -705,6 +712,7 @@ int64_t tc_prepare_batch(kifmm_plan *P, const PassArgs &A, void *args) {
     switch (form_of(P->opt.m2l)) {
         case TC_BF16: return tc_prepare_t<TC_BF16>(P, A, T);
         case TC_FP16: return tc_prepare_t<TC_FP16>(P, A, T);
+        case TC_I8S4: return tc_prepare_t<TC_I8S4>(P, A, T);
         default: return tc_prepare_t<TC_INT8>(P, A, T);
     }
 }
@@ -723,6 +731,7 @@ void launch_m2l_tc_batch(int form, const void *dargs, const int64_t *doff, int n
     switch (form) {
         case TC_BF16: launch_batch_t<TC_BF16>(dargs, doff, nplan, tiles, s); break;
         case TC_FP16: launch_batch_t<TC_FP16>(dargs, doff, nplan, tiles, s); break;
+        case TC_I8S4: launch_batch_t<TC_I8S4>(dargs, doff, nplan, tiles, s); break;
         default: launch_batch_t<TC_INT8>(dargs, doff, nplan, tiles, s); break;
     }
 }
