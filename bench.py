@@ -427,6 +427,7 @@ def run_ours(args, cfg, rank, world, dist):
             res["c3_forms"] = run_c3_forms(torch, flush)
             res["c4"] = run_c4(torch, flush)
             res["planned"] = run_planned(torch, flush)
+            res["next_rows"] = run_next_rows(torch, flush)
     if rank != 0:
         return None
     pk, pk_src = peaks()
@@ -473,7 +474,7 @@ def run_ours(args, cfg, rank, world, dist):
         "gpu_launches": int(launches),
         "clocks": clocks,
     }
-    for k in ("c3_forms", "c4", "planned"):
+    for k in ("c3_forms", "c4", "planned", "next_rows"):
         if k in res:
             line[k] = res[k]
     if args.serve_requests > 0:
@@ -620,6 +621,132 @@ def run_planned(torch, flush, steps=5):
             line["speedup"] = line["on_the_fly"]["apply_ms"] / line["planned"]["apply_ms"]
             res[precision] = line
         out[cname] = res
+    return out
+
+
+def _timed(torch, stream, flush, fn, steps=5, warmup=2):
+    """ms per call of fn() on `stream` (CUDA events, L2 flushed before each)."""
+    ts = []
+    for it in range(warmup + steps):
+        flush_l2(torch, flush)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        if it >= warmup:
+            ts.append(a.elapsed_time(b))
+    return statistics.mean(ts)
+
+
+def run_next_rows(torch, flush):
+    """The rows beside the path, each with its error at 4,096 seeded targets
+    against the FP64 direct sum on the GPU:
+    * separate targets (evaluate_to_points(x, y, check_self=False), the
+      reference's laplace2.py use): 10M uniform targets from the 1M mixture plan;
+    * complex values (FMM(..., iscomplex=True), the reference's hankel.py):
+      Helmholtz (i/4) H0(k r), k = 2, 1M uniform points, Nequiv 24, Ncutoff 50,
+      complex N(0,1) densities, FP64;
+    * circulant E2C (the FFT solve of svd_fmm.py) on the K0 annulus, whose
+      operators differ per level: precompute and full step against the dense
+      inverse."""
+    import pykifmm2d_b200 as P
+    from pykifmm2d_b200 import _lib as B
+    lib = B.load()
+    out = {}
+    # separate targets
+    cfg = CONFIGS["c2"]
+    x, y, tau = cfg["gen"](cfg["n"], 0)
+    xd, yd, td = (torch.from_numpy(v).cuda() for v in (x, y, tau))
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        f = make_fmm(cfg, xd, yd, "mixed", stream=stream.cuda_stream)
+        f.build_tree()
+        f.precompute()
+        f.build_expansions(td)
+        nt = 10_000_000
+        rng = np.random.default_rng(7)
+        tx, ty = rng.uniform(-1, 1, nt), rng.uniform(-1, 1, nt)
+        txd, tyd = torch.from_numpy(tx).cuda(), torch.from_numpy(ty).cuda()
+        o = torch.empty(nt, dtype=torch.float64, device="cuda")
+        ms = _timed(torch, stream, flush, lambda: f.evaluate_to_points(txd, tyd, False, out=o))
+        idx = np.random.default_rng(123).choice(nt, 4096, replace=False)
+        ref = np.zeros(idx.size)
+        P.Get_Kernel_Functions(kernel_obj(cfg))[1](x, y, tx[idx], ty[idx], tau, ref)
+        got = o.cpu().numpy()[idx]
+        out["separate_targets"] = {
+            "workload": f"{cfg['desc']}; {nt} targets uniform in [-1,1]^2, check_self=False",
+            "precision": "mixed", "evaluate_ms": ms, "mtargets_s": nt / (ms * 1e-3) / 1e6,
+            "rel_err": float(np.abs(got - ref).max() / np.abs(ref).max())}
+        del f
+    # complex Helmholtz
+    n = 1_000_000
+    rng = np.random.default_rng(0)
+    x, y = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    tau = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    xd, yd, td = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda(), torch.from_numpy(tau).cuda()
+    H0 = P.HelmholtzKernel(2.0)
+    stream = torch.cuda.Stream()
+    with torch.cuda.stream(stream):
+        oc = torch.empty(n, dtype=torch.complex128, device="cuda")
+
+        def step():
+            g = P.FMM(xd, yd, P.Get_Kernel_Functions(H0), P.prepare_numba_functions_on_the_fly(H0), 24, 50, True,
+                      stream=stream.cuda_stream)
+            g.build_tree()
+            g.precompute()
+            g.build_expansions(td)
+            g.evaluate_to_points(xd, yd, True, out=oc)
+            step.g = g
+        ms = _timed(torch, stream, flush, step, steps=3)
+        g = step.g
+        ams = _timed(torch, stream, flush, lambda: (g.build_expansions(td), g.evaluate_to_points(xd, yd, True, out=oc)),
+                     steps=3)
+        idx = sample_targets(n)
+        ref = np.zeros(idx.size, dtype=np.complex128)
+        P.Get_Kernel_Functions(H0)[2](x, y, tau, ref, targets=idx)
+        got = oc.cpu().numpy()[idx]
+        out["complex_helmholtz"] = {
+            "workload": "Helmholtz (i/4) H0(k r), k = 2, N = 1M uniform in [-1,1]^2, Nequiv 24, Ncutoff 50, "
+                        "complex N(0,1) densities", "precision": "fp64 (complex)", "ms_per_step": ms,
+            "mpts_s": n / (ms * 1e-3) / 1e6, "apply_ms": ams,
+            "rel_err": float(np.abs(got - ref).max() / np.abs(ref).max())}
+        del g, step.g
+    # circulant E2C
+    cfg = CONFIGS["c4"]
+    x, y, tau = cfg["gen"](cfg["n"], 0)
+    xd, yd, td = (torch.from_numpy(v).cuda() for v in (x, y, tau))
+    idx = sample_targets(x.size)
+    ref = _direct_ref(cfg, x, y, tau, idx)
+    kern = kernel_obj(cfg)
+    res = {"workload": cfg["desc"]}
+    for e2c in ("dense", "circulant"):
+        stream = torch.cuda.Stream()
+        with torch.cuda.stream(stream):
+            oo = torch.empty_like(xd)
+
+            def full():
+                h = P.FMM(xd, yd, P.Get_Kernel_Functions(kern), P.prepare_numba_functions_on_the_fly(kern),
+                          cfg["neq"], cfg["cut"], precision="mixed", stream=stream.cuda_stream, e2c=e2c)
+                h.build_tree()
+                h.precompute()
+                h.build_expansions(td)
+                h.evaluate_to_points(xd, yd, True, out=oo)
+                full.h = h
+            ms = _timed(torch, stream, flush, full, steps=3)
+            h = full.h
+            info = np.zeros(len(B.PHASES))
+            lib.kifmm_set_profiling(h._plan, 1)
+            h.precompute()  # the operators again, timed by the plan's phase events
+            lib.kifmm_get_phase_times(h._plan, info.ctypes.data, None, 1)
+            lib.kifmm_set_profiling(h._plan, 0)
+            ph = dict(zip(B.PHASES, info))
+            res[e2c] = {"ms_per_step": ms, "mpts_s": x.size / (ms * 1e-3) / 1e6,
+                        "operators_ms": float(ph["operators"] + ph["precompute"]),
+                        "rel_err": rel_err(oo.cpu().numpy(), ref, idx)}
+            del h, full.h
+    out["circulant_e2c"] = res
     return out
 
 

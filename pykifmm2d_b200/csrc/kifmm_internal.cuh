@@ -218,6 +218,11 @@ struct kifmm_plan {
 
     // workspaces
     kifmm::DBuf<double> tau, taus, pots, pot_out, tx, ty, tpot;
+    // separate targets (evaluate_to_points): Morton-sorted copies, their order, and
+    // the equivalent densities of the leaves' local expansions
+    kifmm::DBuf<uint64_t> tkey, tkey2;
+    kifmm::DBuf<int32_t> tperm, tperm2;
+    kifmm::DBuf<double> txs, tys, node_den;
     kifmm::DBuf<double> uup, udown;
     kifmm::DBuf<double> zero4q;      // 4Q zeros: the source of an absent M2L direction
     bool have_expansions = false;

@@ -554,13 +554,36 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, LEAF_BLOCKS_PER_SM)
     if (w < off[nplan]) leaf_eval_f_leaf<KIND>(args[lo], w - off[lo]);
 }
 
-// separate targets: one thread per target
+// Separate targets (class_fmm.py:379-399 with targets other than the
+// sources), one thread per target in Morton order (sort_targets): descent to
+// the target's leaf, L2P from the leaf's equivalent density (k_leaf_den, in
+// FP64), P2P over the leaf's colleagues in FP32 (pairs at distance 0 skipped),
+// result written to the target's own position.  Neighbouring lanes mostly
+// share a leaf, so node tables and near sources are read once per warp.
+__global__ void k_leaf_den(PassArgs A, int64_t nn, double *__restrict__ den) {
+    const int lane = threadIdx.x & 31;
+    const int64_t w0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5, ws = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int Q = A.Q;
+    for (int64_t g = w0; g < nn; g += ws) {
+        const int l = A.nlev[g];
+        if ((A.nflag[g] & NF_SPLIT) || l < 2) continue;
+        const double *inv = A.ops + (size_t)l * A.stride + A.off_inv;
+        const double *u = A.udown + (size_t)g * Q;
+        for (int q = lane; q < Q; q += 32) {
+            double s = 0.0;
+            for (int c = 0; c < Q; c++) s = fma(inv[q * Q + c], u[c], s);
+            den[(size_t)g * Q + q] = s;
+        }
+    }
+}
+
 template <int KIND>
-__global__ void k_eval_targets_f(PassArgs A, const double *__restrict__ tx, const double *__restrict__ ty, int64_t n,
+__global__ void k_eval_targets_s(PassArgs A, const double *__restrict__ tx, const double *__restrict__ ty,
+                                 const int32_t *__restrict__ order, int64_t n, const double *__restrict__ den,
                                  double *__restrict__ pot) {
     const float kk = (float)A.k;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double px = tx[i], py = ty[i];
+        const double px = tx[i], py = ty[i];
         int g = 0, l = 0;
         while (A.nflag[g] & NF_SPLIT) {
             double cx, cy;
@@ -573,28 +596,28 @@ __global__ void k_eval_targets_f(PassArgs A, const double *__restrict__ tx, cons
         const float rx = (float)(px - cx), ry = (float)(py - cy);
         double far = 0.0;  // L2P in FP64
         if (l >= 2) {
-            const double *inv = A.ops + (size_t)l * A.stride + A.off_inv;
             const double *lgd = A.ops + (size_t)l * A.stride + A.off_large;
+            const double *dg = den + (size_t)g * A.Q;
             for (int q = 0; q < A.Q; q++) {
-                double qd = 0.0;
-                for (int c = 0; c < A.Q; c++) qd = fma(inv[q * A.Q + c], A.udown[(size_t)g * A.Q + c], qd);
-                double dx = (px - cx) - lgd[q], dy = (py - cy) - lgd[A.Q + q];
-                far = fma(green_d(A.kind, A.k, dx * dx + dy * dy), qd, far);
+                const double dx = (px - cx) - lgd[q], dy = (py - cy) - lgd[A.Q + q];
+                far = fma(green_d(A.kind, A.k, dx * dx + dy * dy), dg[q], far);
             }
         }
         float acc = 0.f;
         for (int d = 0; d < 9; d++) {
-            int c = A.ncoll[9 * (size_t)g + d];
+            const int c = A.ncoll[9 * (size_t)g + d];
             if (c < 0) continue;
             for (int s = A.nbot[c]; s < A.ntop[c]; s++) {
-                float dx = rx - (float)(A.xs[s] - cx), dy = ry - (float)(A.ys[s] - cy);
-                float r2 = fmaf(dx, dx, dy * dy);
+                const float dx = rx - (float)(A.xs[s] - cx), dy = ry - (float)(A.ys[s] - cy);
+                const float r2 = fmaf(dx, dx, dy * dy);
                 if (r2 > 0.f) acc = fmaf((float)A.taus[s], gsum_term<KIND>(r2, kk), acc);
             }
         }
-        pot[i] = (double)(acc * gsum_scale<KIND>()) + far;
+        pot[order[i]] = (double)(acc * gsum_scale<KIND>()) + far;
     }
 }
+
+void sort_targets(kifmm_plan *P, const double *tx, const double *ty, int64_t n);  // tree.cu
 
 // m2l_tc.cu / passes.cu
 void run_m2l_tensor(kifmm_plan *P, const PassArgs &A);
@@ -719,11 +742,18 @@ void run_eval_targets_mixed(kifmm_plan *P, const double *tx, const double *ty, i
         launch_eval_targets_d(P, A, tx, ty, n, check_self, pot);
         return;
     }
-    unsigned gr = grid_for(n, 128, P->num_sms * 16);
+    sort_targets(P, tx, ty, n);
+    const int64_t nn = P->n_nodes;
+    P->node_den.alloc((size_t)nn * P->Q);
+    k_leaf_den<<<grid_for(nn * 32, 256, P->num_sms * 16), 256, 0, P->stream>>>(A, nn, P->node_den.p);
+    KIFMM_LAUNCHED();
+    const unsigned gr = grid_for(n, 128, P->num_sms * 16);
     if (P->kern.kind == KIFMM_KERNEL_LAPLACE)
-        k_eval_targets_f<KIFMM_KERNEL_LAPLACE><<<gr, 128, 0, P->stream>>>(A, tx, ty, n, pot);
+        k_eval_targets_s<KIFMM_KERNEL_LAPLACE><<<gr, 128, 0, P->stream>>>(A, P->txs.p, P->tys.p, P->tperm.p, n,
+                                                                          P->node_den.p, pot);
     else
-        k_eval_targets_f<KIFMM_KERNEL_MOD_HELMHOLTZ><<<gr, 128, 0, P->stream>>>(A, tx, ty, n, pot);
+        k_eval_targets_s<KIFMM_KERNEL_MOD_HELMHOLTZ><<<gr, 128, 0, P->stream>>>(A, P->txs.p, P->tys.p, P->tperm.p,
+                                                                                n, P->node_den.p, pot);
     KIFMM_LAUNCHED();
 }
 

@@ -127,6 +127,35 @@ __global__ void k_keys(const double *__restrict__ x, const double *__restrict__ 
     if ((threadIdx.x & 31) == 0 && out) atomicAdd(outside, out);
 }
 
+// Separate targets in the Morton order of the plan's root box, so that the
+// targets of one warp mostly share a leaf (its node tables and near sources
+// are then read once per warp, not once per lane): keys of the coordinates
+// clamped into the box, a sort by the top 32 key bits (16 levels), and the
+// coordinates gathered in that order.  Non-finite coordinates get key 0.
+__global__ void k_target_keys(const double *__restrict__ x, const double *__restrict__ y, int64_t n, double m,
+                              double h, uint64_t *__restrict__ key, int32_t *__restrict__ perm) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double a = x[i], b = y[i];
+        key[i] = (h > 0 && isfinite(a) && isfinite(b)) ? morton(grid_cell(a, m, h), grid_cell(b, m, h)) : 0;
+        perm[i] = (int32_t)i;
+    }
+}
+
+__global__ void k_gather2(const double *__restrict__ x, const double *__restrict__ y, const int32_t *__restrict__ perm,
+                          int64_t n, double *__restrict__ xs, double *__restrict__ ys);
+
+void sort_targets(kifmm_plan *P, const double *tx, const double *ty, int64_t n) {
+    KIFMM_REQUIRE(n < (1ll << 31), KIFMM_ERR_ARG, "evaluate_to_points: more than 2^31 - 1 targets");
+    P->tkey.alloc(n); P->tkey2.alloc(n); P->tperm.alloc(n); P->tperm2.alloc(n);
+    P->txs.alloc(n); P->tys.alloc(n);
+    cudaStream_t s = P->stream;
+    const unsigned gs = grid_for(n, 256, P->num_sms * 8);
+    k_target_keys<<<gs, 256, 0, s>>>(tx, ty, n, P->root_min, std::ldexp(P->W, -KEY_DEPTH), P->tkey.p, P->tperm.p);
+    KIFMM_LAUNCHED();
+    radix_sort_pairs_bits(P->tkey.p, P->tperm.p, P->tkey2.p, P->tperm2.p, n, 2 * KEY_DEPTH - 32, 32, P);
+    launch_pdl(k_gather2, dim3(gs), dim3(256), 0, s, tx, ty, (const int32_t *)P->tperm.p, n, P->txs.p, P->tys.p);
+}
+
 // k_keys with the root box read from the device (no host round trip after
 // k_bbox).  Inputs that the host will reject (non-finite coordinates, |m| or
 // |M| >= 2^23) get key 0 here; the host reports them at its next read-back.
@@ -1056,7 +1085,11 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_MISC + 32, cnt, 96 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
     KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_SCAL + KIFMM_SCAL_SORT_ERR, P->scal.p + KIFMM_SCAL_SORT_ERR,
                                sizeof(sort_err), cudaMemcpyDeviceToHost, s));
-    KIFMM_CUDA(cudaStreamSynchronize(s));
+    KIFMM_CUDA(cudaEventRecord(P->tree_ev, s));
+    // the M2L target order needs only the entries and the node tables: it runs
+    // while the host waits for the counts
+    build_m2l_order(P);
+    KIFMM_CUDA(cudaEventSynchronize(P->tree_ev));
     memcpy(c5, P->hpin + HP_MISC + 32, sizeof(c5));
     memcpy(lv, P->hpin + HP_MISC + 64, sizeof(lv));
     sort_err = P->hpin[HP_SCAL + KIFMM_SCAL_SORT_ERR];
@@ -1072,7 +1105,6 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     P->n_xlist = (int64_t)c5[4];
     P->have_stats = false;
     build_leaf_records(P);
-    build_m2l_order(P);
     P->have_tree = true;
 }
 
