@@ -425,8 +425,11 @@ __global__ void k_leaf_eval_d(PassArgs A, const int32_t *__restrict__ list, int 
 
 // Evaluation at arbitrary targets: locate by strict '>' descent
 // (numba_locate_points, tree.py:712-727), then L2P and P2P.
+// Targets in Morton order (sort_targets) with the leaves' equivalent densities
+// precomputed (k_leaf_den); out[order[i]] is target i's potential.
 __global__ void k_eval_targets_d(PassArgs A, const double *__restrict__ tx, const double *__restrict__ ty, int64_t n,
-                                 int check_self, double *__restrict__ pot) {
+                                 int check_self, const int32_t *__restrict__ order, const double *__restrict__ den,
+                                 double *__restrict__ pot) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         double px = tx[i], py = ty[i];
         int g = 0, l = 0;
@@ -441,13 +444,12 @@ __global__ void k_eval_targets_d(PassArgs A, const double *__restrict__ tx, cons
         double acc = 0.0;
         if (l >= 2) {
             const double *blk = A.ops + (size_t)l * A.stride;
-            const double *inv = blk + A.off_inv, *lg = blk + A.off_large;
+            const double *lg = blk + A.off_large;
             double rx = px - cx, ry = py - cy;
+            const double *dg = den + (size_t)g * A.Q;
             for (int q = 0; q < A.Q; q++) {
-                double qd = 0.0;
-                for (int c = 0; c < A.Q; c++) qd = fma(inv[q * A.Q + c], A.udown[(size_t)g * A.Q + c], qd);
                 double dx = rx - lg[q], dy = ry - lg[A.Q + q];
-                acc += green_d(A.kind, A.k, dx * dx + dy * dy) * qd;
+                acc += green_d(A.kind, A.k, dx * dx + dy * dy) * dg[q];
             }
         }
         for (int d = 0; d < 9; d++) {
@@ -459,7 +461,7 @@ __global__ void k_eval_targets_d(PassArgs A, const double *__restrict__ tx, cons
                 acc += green_d(A.kind, A.k, dx * dx + dy * dy) * A.taus[s];
             }
         }
-        pot[i] = acc;
+        pot[order[i]] = acc;
     }
 }
 
@@ -632,9 +634,15 @@ void launch_leaf_eval_d(kifmm_plan *P, const PassArgs &A, int check_self) {
     KIFMM_LAUNCHED();
 }
 
+void sort_targets(kifmm_plan *P, const double *tx, const double *ty, int64_t n);  // tree.cu
+void launch_leaf_den(kifmm_plan *P, const PassArgs &A);                          // passes_mixed.cu
+
 void launch_eval_targets_d(kifmm_plan *P, const PassArgs &A, const double *tx, const double *ty, int64_t n,
                            int check_self, double *pot) {
-    k_eval_targets_d<<<grid_for(n, 128, P->num_sms * 16), 128, 0, P->stream>>>(A, tx, ty, n, check_self, pot);
+    sort_targets(P, tx, ty, n);
+    launch_leaf_den(P, A);
+    k_eval_targets_d<<<grid_for(n, 128, P->num_sms * 16), 128, 0, P->stream>>>(
+        A, P->txs.p, P->tys.p, n, check_self, P->tperm.p, P->node_den.p, pot);
     KIFMM_LAUNCHED();
 }
 

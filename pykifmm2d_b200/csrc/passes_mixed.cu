@@ -619,6 +619,13 @@ __global__ void k_eval_targets_s(PassArgs A, const double *__restrict__ tx, cons
 
 void sort_targets(kifmm_plan *P, const double *tx, const double *ty, int64_t n);  // tree.cu
 
+void launch_leaf_den(kifmm_plan *P, const PassArgs &A) {
+    const int64_t nn = P->n_nodes;
+    P->node_den.alloc((size_t)nn * P->Q);
+    k_leaf_den<<<grid_for(nn * 32, 256, P->num_sms * 16), 256, 0, P->stream>>>(A, nn, P->node_den.p);
+    KIFMM_LAUNCHED();
+}
+
 // m2l_tc.cu / passes.cu
 void run_m2l_tensor(kifmm_plan *P, const PassArgs &A);
 void launch_p2m_d(kifmm_plan *P, const PassArgs &A);
@@ -743,10 +750,7 @@ void run_eval_targets_mixed(kifmm_plan *P, const double *tx, const double *ty, i
         return;
     }
     sort_targets(P, tx, ty, n);
-    const int64_t nn = P->n_nodes;
-    P->node_den.alloc((size_t)nn * P->Q);
-    k_leaf_den<<<grid_for(nn * 32, 256, P->num_sms * 16), 256, 0, P->stream>>>(A, nn, P->node_den.p);
-    KIFMM_LAUNCHED();
+    launch_leaf_den(P, A);
     const unsigned gr = grid_for(n, 128, P->num_sms * 16);
     if (P->kern.kind == KIFMM_KERNEL_LAPLACE)
         k_eval_targets_s<KIFMM_KERNEL_LAPLACE><<<gr, 128, 0, P->stream>>>(A, P->txs.p, P->tys.p, P->tperm.p, n,
