@@ -184,6 +184,7 @@ struct kifmm_plan {
     kifmm::DBuf<int32_t> leaf_list, p2m_list;
     kifmm::DBuf<int32_t> leaf_rec;   // [n_leaf_list][32] leaf records (passes.cuh, LeafRec)
     kifmm::DBuf<int32_t> m2l_perm;   // [n_ent] M2L target order of the entries (build_m2l_order)
+    kifmm::DBuf<int32_t> leaf_split; // leaves of more than 32 points (split leaf pass)
     kifmm::DBuf<uint16_t> m2l_key;   // [n_ent] direction mask of each entry (256: not split)
     kifmm::DBuf<int32_t> m2l_src8;   // [n_ent][8] source entry per direction (-1: none)
     kifmm::DBuf<unsigned> m2l_hist;  // [MAX_LEVELS + 1][257] counts, then cursors
@@ -311,7 +312,8 @@ inline long long plan_wait_polls(const kifmm_plan *P) {
 constexpr int KIFMM_SCAL_SORT_ERR = 13;  // a radix-sort look-back wait that ran out
 constexpr int KIFMM_SCAL_PASS_ERR = 14;
 constexpr int KIFMM_SCAL_TC_ERR = 15;
-constexpr int KIFMM_SCAL_WORDS = 16;
+constexpr int KIFMM_SCAL_LEAF_SPLIT = 16;  // count of the split leaf list (k_leaf_split_list)
+constexpr int KIFMM_SCAL_WORDS = 17;
 
 // Lanes of the warp holding the same 8-bit digit d (d = 256: no key; such
 // lanes match each other only): nine ballots, one per bit, each lane keeping

@@ -251,9 +251,10 @@ __device__ __forceinline__ float pair_lg2_floor(float tx, float ty, const float4
     return lg2_ftz(fmaf(dx, dx, fmaf(dy, dy, 1.17549435e-38f)));
 }
 
-// the L2P + P2P of leaf w of A's leaf list, by one warp
+// the L2P + P2P of leaf w of A's leaf list, by one warp: its 32-target tiles
+// [tile0, tile1) (all of them by default)
 template <int KIND>
-__device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w) {
+__device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w, int tile0 = 0, int tile1 = 1 << 20) {
     constexpr int R = 2 * KIFMM_TAYLOR_P + 1;
     constexpr float CLAMP = 1.17549435e-38f;  // FLT_MIN
     __shared__ float4 srcs[LEAF_WARPS][LEAF_CHUNK + 32];
@@ -345,7 +346,8 @@ __device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w) {
             __syncwarp();
         };
         __syncwarp();
-        for (int t0 = b; t0 < e; t0 += 32) {
+        const int tfirst = b + 32 * tile0, tend = (int)min((int64_t)e, (int64_t)b + 32 * (int64_t)tile1);
+        for (int t0 = tfirst; t0 < tend; t0 += 32) {
             const int nt = min(32, e - t0);
             // Lane layout: the tile's targets form ng groups of tb (1 or 2)
             // targets; sp = 32 / ng lanes share a group, lane (gi, j) taking
@@ -364,7 +366,7 @@ __device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w) {
             float exa = 0.f, exb = 0.f;  // charges of the leaf's own points met at the clamp
             for (int c0 = 0; c0 < ns; c0 += LEAF_CHUNK) {
                 const int cn = min(LEAF_CHUNK, ns - c0);
-                if (t0 == b || ns > LEAF_CHUNK) gather(c0, cn, lap && t0 == b);
+                if (t0 == tfirst || ns > LEAF_CHUNK) gather(c0, cn, lap && t0 == tfirst);
                 // lane (gi, j) takes sources j, j + sp, ...; j + (it - 1) sp < cn + 32
                 const int it = (cn + sp - 1) / sp;
                 const float4 *sv0 = src + j;
@@ -458,7 +460,7 @@ __device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w) {
                     }
                 }
             }
-            if (lap && t0 == b)
+            if (lap && t0 == tfirst)
                 for (int o = 16; o; o >>= 1) tsum += __shfl_xor_sync(0xffffffffu, tsum, o);
             // per-lane shares with the clamped own pairs taken out
             red[wib][0][lane] = lap ? neara - (double)exa * (double)lclamp : neara;
@@ -527,14 +529,40 @@ __device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w) {
     }
 }
 
-template <int KIND>
-__global__ void __launch_bounds__(32 * LEAF_WARPS, LEAF_BLOCKS_PER_SM) k_leaf_eval_f(PassArgs A, int64_t nlist) {
+// One warp per leaf.  With `split` (a leaf list smaller than one wave of the
+// GPU, where the kernel lasts as long as its heaviest leaf) warps nlist ..
+// nlist + *nsplit - 1 take the tiles after the first of the leaves in
+// split_list, so a leaf of more than 32 points runs on two warps.
+template <int KIND, bool SPLIT>
+__global__ void __launch_bounds__(32 * LEAF_WARPS, LEAF_BLOCKS_PER_SM)
+    k_leaf_eval_f(PassArgs A, int64_t nlist, const int32_t *__restrict__ split_list,
+                  const unsigned *__restrict__ nsplit) {
     pdl_trigger();
     pdl_wait();
-    // one warp per leaf (grid-stride only if the grid were capped)
     const int64_t wstride = (int64_t)gridDim.x * LEAF_WARPS;
-    for (int64_t w = (int64_t)blockIdx.x * LEAF_WARPS + (threadIdx.x >> 5); w < nlist; w += wstride)
-        leaf_eval_f_leaf<KIND>(A, w);
+    if (!SPLIT) {
+        for (int64_t w = (int64_t)blockIdx.x * LEAF_WARPS + (threadIdx.x >> 5); w < nlist; w += wstride)
+            leaf_eval_f_leaf<KIND>(A, w);
+        return;
+    }
+    const int64_t total = nlist + *nsplit;
+    for (int64_t w = (int64_t)blockIdx.x * LEAF_WARPS + (threadIdx.x >> 5); w < total; w += wstride) {
+        const bool first = w < nlist;
+        leaf_eval_f_leaf<KIND>(A, first ? w : (int64_t)split_list[w - nlist], first ? 0 : 1, first ? 1 : 1 << 20);
+    }
+}
+
+// the leaves of more than 32 points (their tiles after the first), for the
+// split form of k_leaf_eval_f
+__global__ void k_leaf_split_list(const int32_t *__restrict__ rec, int64_t nlist, int32_t *__restrict__ out,
+                                  unsigned *__restrict__ count) {
+    const int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const bool big = w < nlist && rec[w * LEAF_REC_WORDS + LR_TOP] - rec[w * LEAF_REC_WORDS + LR_BOT] > 32;
+    const unsigned peers = __ballot_sync(0xffffffffu, big);
+    unsigned base = 0;
+    if ((threadIdx.x & 31) == 0 && peers) base = atomicAdd(count, (unsigned)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (big) out[base + __popc(peers & ((1u << (threadIdx.x & 31)) - 1))] = (int32_t)w;
 }
 
 // The leaf pass of several plans in one launch (serving batches): warp w of
@@ -720,13 +748,34 @@ void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
         return;
     }  // FP32 form: coincident pairs always contribute zero
     PassArgs A = mixed_leaf_args(P);
-    unsigned gr = (unsigned)std::min<int64_t>((P->n_leaf_list + LEAF_WARPS - 1) / LEAF_WARPS, 1ll << 30);
-    if (P->kern.kind == KIFMM_KERNEL_LAPLACE)
-        launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_LAPLACE>, dim3(gr), dim3(32 * LEAF_WARPS), 0, P->stream, A,
-                   P->n_leaf_list);
-    else
-        launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_MOD_HELMHOLTZ>, dim3(gr), dim3(32 * LEAF_WARPS), 0, P->stream, A,
-                   P->n_leaf_list);
+    // fewer leaves than one wave of warps: split the big ones over two warps
+    const int64_t nl = P->n_leaf_list;
+    const bool split = nl < (int64_t)P->num_sms * LEAF_BLOCKS_PER_SM * LEAF_WARPS / 2;
+    const int32_t *slist = nullptr;
+    const unsigned *scount = nullptr;
+    if (split) {
+        P->leaf_split.alloc((size_t)nl);
+        unsigned *cnt = (unsigned *)(P->scal.p + KIFMM_SCAL_LEAF_SPLIT);
+        KIFMM_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), P->stream));
+        k_leaf_split_list<<<(unsigned)((nl + 255) / 256), 256, 0, P->stream>>>(P->leaf_rec.p, nl, P->leaf_split.p,
+                                                                                cnt);
+        KIFMM_LAUNCHED();
+        slist = P->leaf_split.p;
+        scount = cnt;
+    }
+    const int64_t warps = split ? 2 * nl : nl;
+    unsigned gr = (unsigned)std::min<int64_t>((warps + LEAF_WARPS - 1) / LEAF_WARPS, 1ll << 30);
+    const dim3 grid(gr), block(32 * LEAF_WARPS);
+    if (P->kern.kind == KIFMM_KERNEL_LAPLACE) {
+        if (split) launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_LAPLACE, true>, grid, block, 0, P->stream, A, nl, slist, scount);
+        else launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_LAPLACE, false>, grid, block, 0, P->stream, A, nl, slist, scount);
+    } else {
+        if (split)
+            launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_MOD_HELMHOLTZ, true>, grid, block, 0, P->stream, A, nl, slist, scount);
+        else
+            launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_MOD_HELMHOLTZ, false>, grid, block, 0, P->stream, A, nl, slist,
+                       scount);
+    }
 }
 
 // the FP32 leaf pass of several plans of one kernel kind in one launch

@@ -285,7 +285,10 @@ class Server:
             B.load().kifmm_stream_destroy(ctypes.c_void_p(h))
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: torch may be gone already
+            pass
 
     def _kernel(self, req):
         if req.kernel == "laplace":
