@@ -56,8 +56,14 @@ template <> struct TcTraits<TC_I8S4> { static constexpr int NS = 4, EB = 1, KSTE
 template <int F> __host__ __device__ constexpr bool tc_int() { return F == TC_INT8 || F == TC_I8S4; }
 
 constexpr int TC_M = 128;        // MMA M: operator rows per tile (TMEM lanes)
-constexpr int TC_KCB = 64;       // bytes of K per slice row and stage (2 MMA K steps)
-constexpr int TC_STAGES = 3;     // shared-memory ring slots
+#ifndef KIFMM_TC_KCB
+#define KIFMM_TC_KCB 64
+#endif
+#ifndef KIFMM_TC_STAGES
+#define KIFMM_TC_STAGES 3
+#endif
+constexpr int TC_KCB = KIFMM_TC_KCB;        // bytes of K per slice row and stage (64: 2 MMA K steps)
+constexpr int TC_STAGES = KIFMM_TC_STAGES;  // shared-memory ring slots
 constexpr int TC_GWARPS = 4;     // gather / epilogue warps (TMEM lanes 32 w .. 32 w + 31)
 constexpr int TC_THREADS = 32 * (TC_GWARPS + 1);
 template <int F>
