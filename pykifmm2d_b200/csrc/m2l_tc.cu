@@ -318,7 +318,7 @@ static constexpr size_t tc_table_off() { return TC_STAGES * (tc_stage_a<F>() + t
 template <int F>
 static constexpr size_t tc_smem_bytes() {
     constexpr int TN = TcTraits<F>::TN;
-    return tc_table_off<F>() + (size_t)TN * 8 * 4 * 2 + (size_t)TN * 8 + (size_t)TN * 4 + 16 * 4 +
+    return tc_table_off<F>() + (size_t)TN * 8 * 4 * 2 + (size_t)TN * 8 * 2 + (size_t)TN * 4 + 16 * 4 +
            (3 * TC_STAGES + 2) * 8 + 16;
 }
 
@@ -341,7 +341,8 @@ __device__ __forceinline__ void m2l_tc_tile(const TcArgs &T, const int64_t tile)
     int *sgrp = (int *)(tc_smem + tc_table_off<F>());             // [TN][8] source entry per direction
     int *sshift = sgrp + TN * 8;                                  // [TN][8] slice shift (INT8)
     double *stau = (double *)(sshift + TN * 8);                   // [TN] column scale
-    int *sact = (int *)(stau + TN);                               // [TN]
+    long long *sdst = (long long *)(stau + TN);                   // [TN] first u_down element of the target's children
+    int *sact = (int *)(sdst + TN);                               // [TN]
     int *sdir = sact + TN;                                        // [8] directions with a source; [8] count; [9] abort
     uint64_t *bars = (uint64_t *)(((uintptr_t)(sdir + 16) + 7) & ~(uintptr_t)7);
     uint32_t *tslot = (uint32_t *)(bars + 3 * S + 1);
@@ -387,6 +388,7 @@ __device__ __forceinline__ void m2l_tc_tile(const TcArgs &T, const int64_t tile)
         }
         stau[tid] = tc_int<F>() ? ldexp(1.0, 7 * kcol) : 1.0;
         sact[tid] = act ? (int)(ej - eoff) + 1 : 0;
+        sdst[tid] = act ? (A.T.off[l + 1] + 4 * (ej - eoff)) * (long long)Q : 0;
     }
     if (tid == 0) {
         for (int i = 0; i < S; i++) {
@@ -563,7 +565,9 @@ __device__ __forceinline__ void m2l_tc_tile(const TcArgs &T, const int64_t tile)
                         long long z = 0;
 #pragma unroll
                         for (int s = 0; s < TR::NACC; s++) z += (long long)(int32_t)v[s][c] << (7 * (TR::NACC - 1 - s));
-                        y[c] = ldexp((double)z, -7 * (TR::NACC + 1));
+                        // exact: z is an integer below 2^60 and the factor a power of two
+                        constexpr double kWeight = 1.0 / (double)(1ll << (7 * (TR::NACC + 1)));
+                        y[c] = (double)z * kWeight;
                     }
                 } else {
 #pragma unroll
@@ -575,10 +579,7 @@ __device__ __forceinline__ void m2l_tc_tile(const TcArgs &T, const int64_t tile)
 #pragma unroll
                 for (int c = 0; c < 16; c++) {
                     const int j = cc * 16 + c;
-                    if (sact[j]) {
-                        const int64_t cg = A.T.off[lt1] + 4 * (int64_t)(sact[j] - 1);
-                        A.udown[(size_t)cg * Q + r] = y[c] * sig * stau[j];
-                    }
+                    if (sact[j]) A.udown[sdst[j] + r] = y[c] * sig * stau[j];
                 }
         }
     }
