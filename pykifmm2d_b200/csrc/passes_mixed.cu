@@ -232,6 +232,7 @@ constexpr int LEAF_WARPS = 1;
 #endif
 constexpr int LEAF_BLOCKS_PER_SM = KIFMM_LEAF_BLOCKS_PER_SM;  // resident blocks per SM at the register bound
 constexpr int LEAF_CHUNK = KIFMM_LEAF_CHUNK;                  // sources staged per pass
+static_assert(LEAF_CHUNK + 31 <= 200, "the leaf kernel's quotients (small_div) need cn + sp - 1 <= 200");
 
 __device__ __forceinline__ float lg2_ftz(float x) {
     float y;
@@ -251,13 +252,151 @@ __device__ __forceinline__ float pair_lg2_floor(float tx, float ty, const float4
     return lg2_ftz(fmaf(dx, dx, fmaf(dy, dy, 1.17549435e-38f)));
 }
 
+// Packed FP32 pairs (sm_100 .f32x2 arithmetic): one 64-bit register holds a
+// value for each of a lane's two targets.  Sources are staged with their
+// coordinates and charge duplicated, (x, x | y, y) and (z, z), so one
+// instruction forms both targets' offsets, squared distances and products:
+// the same IEEE operations as the scalar form, issued half as often.
+typedef unsigned long long f32x2;
+constexpr f32x2 F2_FLOOR = 0x0080000000800000ull;  // (FLT_MIN, FLT_MIN)
+__device__ __forceinline__ f32x2 f2_pack(float a, float b) {
+    f32x2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(f32x2 v, float &a, float &b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ f32x2 f2_sub(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 f2_add(f32x2 a, f32x2 b) {
+    f32x2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ f32x2 f2_fma(f32x2 a, f32x2 b, f32x2 c) {
+    f32x2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+// r^2 + FLT_MIN of both targets to one source (as pair_lg2_floor)
+__device__ __forceinline__ f32x2 pair2_r2_floor(f32x2 tx, f32x2 ty, const ulonglong2 &s) {
+    const f32x2 dx = f2_sub(tx, s.x), dy = f2_sub(ty, s.y);
+    return f2_fma(dx, dx, f2_fma(dy, dy, F2_FLOOR));
+}
+__device__ __forceinline__ f32x2 lg2_pair(f32x2 r) {
+    float a, b;
+    f2_unpack(r, a, b);
+    return f2_pack(lg2_ftz(a), lg2_ftz(b));
+}
+
+// Laplace pair sums of one lane holding two targets (tx, ty packed): over its
+// sources at list positions j + k SP, k in [k0, k1), of z log2(r^2 + FLT_MIN),
+// in FP32 blocks of at most 32 sources (two chains per target, alternating
+// sources) added to na, nb in FP64.  OWN: the positions are the leaf's own
+// points below en, where coincident pairs (the target itself, duplicates) meet
+// the floor; their charges are summed into exa, exb to be taken out.  SP is a
+// template argument so that the strided shared-memory loads take immediate
+// offsets.
+template <int SP_, bool OWN>
+__device__ __forceinline__ void leaf_pairs2(const ulonglong2 *__restrict__ sxy, const f32x2 *__restrict__ sz, int j,
+                                            int k0, int k1, f32x2 tx, f32x2 ty, int en, double &na, double &nb,
+                                            float &exa, float &exb, int sp_rt = 0) {
+    constexpr float FLOOR2 = 2.0f * 1.17549435e-38f;
+    const int SP = SP_ ? SP_ : sp_rt;
+    for (int kb = k0; kb < k1; kb += 32) {
+        const int ke = min(k1, kb + 32);
+        f32x2 acc0 = 0ull, acc1 = 0ull;
+        const ulonglong2 *p = sxy + j + kb * SP;
+        const f32x2 *q = sz + j + kb * SP;
+        int k = kb;
+        if (OWN) {
+            for (; k < ke; k++, p += SP, q += SP) {
+                const f32x2 r = pair2_r2_floor(tx, ty, *p), z = *q;
+                acc0 = f2_fma(z, lg2_pair(r), acc0);
+                float ra, rb, zs, zu;
+                f2_unpack(r, ra, rb);
+                f2_unpack(z, zs, zu);
+                const bool in = j + k * SP < en;
+                exa += (in && ra < FLOOR2) ? zs : 0.f;
+                exb += (in && rb < FLOOR2) ? zs : 0.f;
+            }
+        } else {
+#pragma unroll 1
+            for (; k + 3 < ke; k += 4, p += 4 * SP, q += 4 * SP) {
+                const ulonglong2 s0 = p[0], s1 = p[SP], s2 = p[2 * SP], s3 = p[3 * SP];
+                const f32x2 z0 = q[0], z1 = q[SP], z2 = q[2 * SP], z3 = q[3 * SP];
+                acc0 = f2_fma(z0, lg2_pair(pair2_r2_floor(tx, ty, s0)), acc0);
+                acc1 = f2_fma(z1, lg2_pair(pair2_r2_floor(tx, ty, s1)), acc1);
+                acc0 = f2_fma(z2, lg2_pair(pair2_r2_floor(tx, ty, s2)), acc0);
+                acc1 = f2_fma(z3, lg2_pair(pair2_r2_floor(tx, ty, s3)), acc1);
+            }
+            for (; k + 1 < ke; k += 2, p += 2 * SP, q += 2 * SP) {
+                acc0 = f2_fma(q[0], lg2_pair(pair2_r2_floor(tx, ty, p[0])), acc0);
+                acc1 = f2_fma(q[SP], lg2_pair(pair2_r2_floor(tx, ty, p[SP])), acc1);
+            }
+            if (k < ke) acc0 = f2_fma(q[0], lg2_pair(pair2_r2_floor(tx, ty, p[0])), acc0);
+        }
+        float sa, sb;
+        f2_unpack(f2_add(acc0, acc1), sa, sb);
+        na += (double)sa;
+        nb += (double)sb;
+    }
+}
+// leaf_pairs2 for a run-time lane stride sp = 32 / groups, groups in 1..16
+template <bool OWN>
+__device__ __forceinline__ void leaf_pairs2_sp(int sp, const ulonglong2 *sxy, const f32x2 *sz, int j, int k0, int k1,
+                                               f32x2 tx, f32x2 ty, int en, double &na, double &nb, float &exa,
+                                               float &exb) {
+#define KIFMM_LEAF_SP(S)                                                          \
+    case S:                                                                       \
+        leaf_pairs2<S, OWN>(sxy, sz, j, k0, k1, tx, ty, en, na, nb, exa, exb); \
+        break;
+#ifndef KIFMM_LEAF_SP_MODE
+#define KIFMM_LEAF_SP_MODE 1
+#endif
+#if KIFMM_LEAF_SP_MODE == 0
+    leaf_pairs2<0, OWN>(sxy, sz, j, k0, k1, tx, ty, en, na, nb, exa, exb, sp);
+#elif KIFMM_LEAF_SP_MODE == 1
+    if (sp == 2) leaf_pairs2<2, OWN>(sxy, sz, j, k0, k1, tx, ty, en, na, nb, exa, exb);
+    else leaf_pairs2<0, OWN>(sxy, sz, j, k0, k1, tx, ty, en, na, nb, exa, exb, sp);
+#else
+    switch (sp) {
+        KIFMM_LEAF_SP(2)
+        KIFMM_LEAF_SP(3)
+        KIFMM_LEAF_SP(4)
+        KIFMM_LEAF_SP(5)
+        KIFMM_LEAF_SP(6)
+        KIFMM_LEAF_SP(8)
+        KIFMM_LEAF_SP(10)
+        KIFMM_LEAF_SP(16)
+        default:
+            leaf_pairs2<32, OWN>(sxy, sz, j, k0, k1, tx, ty, en, na, nb, exa, exb);
+    }
+#endif
+#undef KIFMM_LEAF_SP
+}
+
+// x / d for 0 <= x <= 200 and 1 <= d <= 32 as a multiply and a shift (the
+// lane-layout quotients of the leaf kernel; a division by a run-time value
+// costs a reciprocal and a dozen fix-up instructions): c = ceil(2^16 / d)
+// gives floor(x c / 2^16) = floor(x / d) whenever x < 2^16 / d.
+__constant__ unsigned c_recip16[33] = {
+    0,    65536, 32768, 21846, 16384, 13108, 10923, 9363, 8192, 7282, 6554, 5958, 5462, 5042, 4682, 4370, 4096,
+    3856, 3641,  3450,  3277,  3121,  2979,  2850,  2731, 2622, 2521, 2428, 2341, 2260, 2185, 2115, 2048};
+__device__ __forceinline__ int small_div(int x, int d) { return (int)(((unsigned)x * c_recip16[d]) >> 16); }
+
 // the L2P + P2P of leaf w of A's leaf list, by one warp: its 32-target tiles
 // [tile0, tile1) (all of them by default)
 template <int KIND>
 __device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w, int tile0 = 0, int tile1 = 1 << 20) {
     constexpr int R = 2 * KIFMM_TAYLOR_P + 1;
     constexpr float CLAMP = 1.17549435e-38f;  // FLT_MIN
-    __shared__ float4 srcs[LEAF_WARPS][LEAF_CHUNK + 32];
+    __shared__ ulonglong2 sxys[LEAF_WARPS][LEAF_CHUNK + 32];  // (x, x | y, y) per staged source
+    __shared__ f32x2 szs[LEAF_WARPS][LEAF_CHUNK + 32];        // (z, z)
     __shared__ double qds[LEAF_WARPS][R > 64 ? R : 64];
     __shared__ float qfs[LEAF_WARPS][R > 64 ? R : 64];
     __shared__ double red[LEAF_WARPS][2][32];
@@ -282,7 +421,8 @@ __device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w, i
         const bool taylor = lap && A.taylor != nullptr && l >= 2;
         double *qd = qds[wib];
         float *qf = qfs[wib];
-        float4 *src = srcs[wib];
+        ulonglong2 *sxy = sxys[wib];
+        f32x2 *sz = szs[wib];
         const double width = ldexp(A.W, -l);
         const double sc = lap ? 1.0 / width : 1.0;     // coordinate scale
         const double lw = lap ? -2.0 * log2(sc) : 0.0; // log2 of the squared length unit
@@ -337,122 +477,58 @@ __device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w, i
     #pragma unroll
                 for (int k = 0; k < 4; k++)
                     if (si[k] >= 0) {
-                        src[q0 + lane + 32 * k] =
-                            make_float4((float)((vx[k] - cx) * sc), (float)((vy[k] - cy) * sc), (float)vt[k], 0.f);
+                        const float fx = (float)((vx[k] - cx) * sc), fy = (float)((vy[k] - cy) * sc);
+                        const float fz = (float)vt[k];
+                        sxy[q0 + lane + 32 * k] = make_ulonglong2(f2_pack(fx, fx), f2_pack(fy, fy));
+                        sz[q0 + lane + 32 * k] = f2_pack(fz, fz);
                         if (sum) tsum += vt[k];
                     }
             }
-            src[cn + lane] = make_float4(1e18f, 1e18f, 0.f, 0.f);
+            sxy[cn + lane] = make_ulonglong2(f2_pack(1e18f, 1e18f), f2_pack(1e18f, 1e18f));
+            sz[cn + lane] = 0ull;
             __syncwarp();
         };
         __syncwarp();
         const int tfirst = b + 32 * tile0, tend = (int)min((int64_t)e, (int64_t)b + 32 * (int64_t)tile1);
         for (int t0 = tfirst; t0 < tend; t0 += 32) {
             const int nt = min(32, e - t0);
-            // Lane layout: the tile's targets form ng groups of tb (1 or 2)
-            // targets; sp = 32 / ng lanes share a group, lane (gi, j) taking
-            // sources j, j + sp, ...  Two targets per lane reuse each source
-            // load and give four independent chains per step; the layout with
-            // fewer pair slots per lane (tb * ceil(ns / sp)) is taken.
-            const int ng2 = (nt + 1) >> 1, sp1 = 32 / nt, sp2 = 32 / ng2;
-            const bool two = KIND == KIFMM_KERNEL_LAPLACE &&
-                             2 * ((ns + sp2 - 1) / sp2) <= (ns + sp1 - 1) / sp1;
-            const int ng = two ? ng2 : nt, sp = two ? sp2 : sp1;
-            const int gi = lane % ng, j = lane / ng;
-            const int ia = gi, ib = two && gi + ng < nt ? gi + ng : gi;  // second slot repeats the first when unused
+            // Lane layout: the tile's targets form ng groups of tb targets
+            // (two for the Laplace kernel, one otherwise); sp = 32 / ng lanes
+            // share a group, lane (gi, j) taking sources j, j + sp, ...  Two
+            // targets per lane share each source load and every packed
+            // (f32x2) instruction of the pair loop.
+            const int ng = lap ? (nt + 1) >> 1 : nt, sp = small_div(32, ng);
+            const int j = small_div(lane, ng), gi = lane - j * ng;
+            const int ia = gi, ib = lap && gi + ng < nt ? gi + ng : gi;  // second slot repeats the first when unused
             const float txa = (float)((A.xs[t0 + ia] - cx) * sc), tya = (float)((A.ys[t0 + ia] - cy) * sc);
             const float txb = (float)((A.xs[t0 + ib] - cx) * sc), tyb = (float)((A.ys[t0 + ib] - cy) * sc);
+            const f32x2 tx2 = f2_pack(txa, txb), ty2 = f2_pack(tya, tyb);
             double neara = 0.0, nearb = 0.0;
-            float exa = 0.f, exb = 0.f;  // charges of the leaf's own points met at the clamp
+            float exa = 0.f, exb = 0.f;  // charges of the leaf's own points met at the floor
             for (int c0 = 0; c0 < ns; c0 += LEAF_CHUNK) {
                 const int cn = min(LEAF_CHUNK, ns - c0);
                 if (t0 == tfirst || ns > LEAF_CHUNK) gather(c0, cn, lap && t0 == tfirst);
                 // lane (gi, j) takes sources j, j + sp, ...; j + (it - 1) sp < cn + 32
-                const int it = (cn + sp - 1) / sp;
-                const float4 *sv0 = src + j;
+                const int it = small_div(cn + sp - 1, sp);
                 if (KIND == KIFMM_KERNEL_LAPLACE) {
                     // the list starts with the leaf's own points, local [0, en): the
-                    // first kown passes count the pairs there that meet the clamp
+                    // first kown passes count the pairs there that meet the floor
                     const int en = min(e - b - c0, cn);
-                    const int kown = en > 0 ? (en + sp - 1) / sp : 0;
-                    for (int k0 = 0; k0 < kown; k0 += 32) {
-                        const int k1 = min(kown, k0 + 32);
-                        float acca = 0.f, accb = 0.f;
-                        if (two) {
-                            for (int k = k0; k < k1; k++) {
-                                const int u = j + k * sp;
-                                const float4 sv = src[u];
-                                const float ra = pair_r2(txa, tya, sv), rb = pair_r2(txb, tyb, sv);
-                                acca = fmaf(sv.z, lg2_ftz(fmaxf(ra, CLAMP)), acca);
-                                accb = fmaf(sv.z, lg2_ftz(fmaxf(rb, CLAMP)), accb);
-                                exa += (ra < CLAMP && u < en) ? sv.z : 0.f;
-                                exb += (rb < CLAMP && u < en) ? sv.z : 0.f;
-                            }
-                        } else {
-                            for (int k = k0; k < k1; k++) {
-                                const int u = j + k * sp;
-                                const float4 sv = src[u];
-                                const float ra = pair_r2(txa, tya, sv);
-                                acca = fmaf(sv.z, lg2_ftz(fmaxf(ra, CLAMP)), acca);
-                                exa += (ra < CLAMP && u < en) ? sv.z : 0.f;
-                            }
-                        }
-                        neara += (double)acca;
-                        nearb += (double)accb;
-                    }
-                    if (two) {
-                        for (int k0 = kown; k0 < it; k0 += 32) {
-                            const int k1 = min(it, k0 + 32);
-                            float a0 = 0.f, a1 = 0.f, b0 = 0.f, b1 = 0.f;
-                            const float4 *pp = sv0 + (size_t)k0 * sp;
-                            int k = k0;
-    #pragma unroll 2
-                            for (; k + 1 < k1; k += 2) {
-                                const float4 s0 = pp[0], s1 = pp[sp];
-                                pp += 2 * sp;
-                                a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
-                                b0 = fmaf(s0.z, pair_lg2_floor(txb, tyb, s0), b0);
-                                a1 = fmaf(s1.z, pair_lg2_floor(txa, tya, s1), a1);
-                                b1 = fmaf(s1.z, pair_lg2_floor(txb, tyb, s1), b1);
-                            }
-                            if (k < k1) {
-                                const float4 s0 = pp[0];
-                                a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
-                                b0 = fmaf(s0.z, pair_lg2_floor(txb, tyb, s0), b0);
-                            }
-                            neara += (double)(a0 + a1);
-                            nearb += (double)(b0 + b1);
-                        }
-                    } else {
-                        for (int k0 = kown; k0 < it; k0 += 32) {
-                            const int k1 = min(it, k0 + 32);
-                            float a0 = 0.f, a1 = 0.f, a2 = 0.f, a3 = 0.f;  // four chains
-                            const float4 *pp = sv0 + (size_t)k0 * sp;
-                            int k = k0;
-    #pragma unroll 1
-                            for (; k + 3 < k1; k += 4) {
-                                const float4 s0 = pp[0], s1 = pp[sp], s2 = pp[2 * sp], s3 = pp[3 * sp];
-                                pp += 4 * sp;
-                                a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
-                                a1 = fmaf(s1.z, pair_lg2_floor(txa, tya, s1), a1);
-                                a2 = fmaf(s2.z, pair_lg2_floor(txa, tya, s2), a2);
-                                a3 = fmaf(s3.z, pair_lg2_floor(txa, tya, s3), a3);
-                            }
-                            for (; k < k1; k++) {
-                                const float4 s0 = pp[0];
-                                pp += sp;
-                                a0 = fmaf(s0.z, pair_lg2_floor(txa, tya, s0), a0);
-                            }
-                            neara += (double)((a0 + a1) + (a2 + a3));
-                        }
-                    }
+                    const int kown = en > 0 ? small_div(en + sp - 1, sp) : 0;
+                    leaf_pairs2_sp<true>(sp, sxy, sz, j, 0, kown, tx2, ty2, en, neara, nearb, exa, exb);
+                    leaf_pairs2_sp<false>(sp, sxy, sz, j, kown, it, tx2, ty2, en, neara, nearb, exa, exb);
                 } else {
                     for (int k0 = 0; k0 < it; k0 += 32) {
                         const int k1 = min(it, k0 + 32);
                         float acc = 0.f;
     #pragma unroll 1
                         for (int k = k0; k < k1; k++) {
-                            const float4 sv = sv0[k * sp];
+                            const int u = j + k * sp;
+                            float sx, sy, sw, unused;
+                            f2_unpack(sxy[u].x, sx, unused);
+                            f2_unpack(sxy[u].y, sy, unused);
+                            f2_unpack(sz[u], sw, unused);
+                            const float4 sv = make_float4(sx, sy, sw, 0.f);
                             const float r2 = pair_r2(txa, tya, sv);
                             if (r2 > 0.f) acc = fmaf(sv.z, gsum_term<KIND>(r2, kk), acc);
                         }
