@@ -13,14 +13,14 @@
 // the 512 TMEM columns of an SM) and one 128-row M tile.  Its work is a list
 // of stages (direction with a source in the tile, 64-byte K chunk) that runs
 // through a ring of TC_STAGES shared-memory slots, warp-specialised:
-//   * warps 0-3 gather the sources' pre-sliced K chunks into a slot (16-byte
+//   * warps 0 .. TC_GWARPS-1 gather the sources' pre-sliced K chunks into a slot (16-byte
 //     cp.async copies) and arrive on its B-full barrier once they landed;
 //   * one thread of warp 4 copies the operator chunk into the slot with one
 //     bulk copy (A-full barrier, transaction bytes), waits for both, issues the
 //     stage's MMA chain and commits it to the slot's empty barrier, which
 //     frees the slot for the gather warps and for its own next operator copy;
-//   * after the last stage, warps 0-3 read TMEM (each its 32 lanes) and
-//     write the FP64 results.
+//   * after the last stage, the gather warps read TMEM (warp w its 32 lanes
+//     of quarter w % 4, a share of the columns) and write the FP64 results.
 // Operands sit in the UMMA K-major, no-swizzle core-matrix layout.
 //
 // Forms:
@@ -64,7 +64,13 @@ constexpr int TC_M = 128;        // MMA M: operator rows per tile (TMEM lanes)
 #endif
 constexpr int TC_KCB = KIFMM_TC_KCB;        // bytes of K per slice row and stage (64: 2 MMA K steps)
 constexpr int TC_STAGES = KIFMM_TC_STAGES;  // shared-memory ring slots
-constexpr int TC_GWARPS = 4;     // gather / epilogue warps (TMEM lanes 32 w .. 32 w + 31)
+#ifndef KIFMM_TC_GWARPS
+#define KIFMM_TC_GWARPS 8
+#endif
+// gather / epilogue warps: warp w reads TMEM lanes 32 (w % 4) .. + 31 and every
+// (TC_GWARPS / 4)-th 16-column group of the accumulators from group w / 4
+constexpr int TC_GWARPS = KIFMM_TC_GWARPS;
+static_assert(TC_GWARPS % 4 == 0, "epilogue warps cover the four TMEM lane quarters equally");
 constexpr int TC_THREADS = 32 * (TC_GWARPS + 1);
 template <int F>
 constexpr bool tc_traits_ok() {
@@ -544,10 +550,10 @@ __device__ __forceinline__ void m2l_tc_tile(const TcArgs &T, const int64_t tile)
     mbar_wait(accbar, 0, kDrainWaitPolls);
     fence_after();
     if (warp < TC_GWARPS && !*abort_flag) {
-        const int row = warp * 32 + lane, r = mt * TC_M + row;
+        const int quarter = warp & 3, row = quarter * 32 + lane, r = mt * TC_M + row;
         const double sig = rsl[r];
 #pragma unroll 1
-        for (int cc = 0; cc < TN / 16; cc++) {
+        for (int cc = warp >> 2; cc < TN / 16; cc += TC_GWARPS / 4) {
             double y[16];
 #pragma unroll
             for (int c = 0; c < 16; c++) y[c] = 0.0;
@@ -555,7 +561,7 @@ __device__ __forceinline__ void m2l_tc_tile(const TcArgs &T, const int64_t tile)
                 uint32_t v[TR::NACC][16];
 #pragma unroll
                 for (int s = 0; s < TR::NACC; s++)
-                    tmem_ld16_nowait(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(s * TN + cc * 16), v[s]);
+                    tmem_ld16_nowait(tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(s * TN + cc * 16), v[s]);
                 tmem_wait_ld();
                 if (tc_int<F>()) {
                     // accumulator s carries weight 2^-7(s+2): combine exactly in int64

@@ -205,30 +205,34 @@ __global__ void __launch_bounds__(TY_THREADS) k_leaf_taylor(TaylorArgs T) {
 // L2P + P2P: one warp per target leaf.  The sources of the leaf and its eight
 // colleagues are staged in shared memory as one list (the leaf's own points
 // first), in chunks of LEAF_CHUNK.  A tile of nt <= 32 targets is spread over
-// the warp with sp = 32 / nt lanes per target, each lane taking every sp-th
-// source, so a leaf of 15 points keeps 30 lanes busy instead of 15 and no lane
-// idles on a short colleague.  For the Laplace kernel the offsets are scaled
-// by 1/w (w the leaf width) so every log2 term is O(1); the remainder
-// log2(w^2) * sum(tau) is added in FP64.  The inner loop is branch-free: r^2
-// is clamped below at FLT_MIN and short chunks are padded with far, uncharged
-// sources.  The pairs inside the leaf itself that meet the clamp (the target's
-// own point and exact duplicates, which the reference skips, class_fmm.py:107)
-// are counted by a short second loop over the leaf's own points and taken back
-// out.  Distinct points of different leaves closer than about 2^-24 leaf widths
-// round to the same FP32 offsets and keep log2(FLT_MIN) for their pair; the
-// FP64 near field (near_fp64) resolves such pairs.  FP32 partial sums of at
-// most 32 terms are accumulated in FP64.
+// the warp in ng groups (two targets per lane for the Laplace kernel, one
+// otherwise) with sp = 32 / ng lanes per group, each lane taking every sp-th
+// source, so a leaf of 15 points keeps 32 lanes busy and no lane idles on a
+// short colleague; the Laplace pair loop runs on packed FP32 pairs (f32x2),
+// one instruction for both of a lane's targets.  For the Laplace kernel the
+// offsets are scaled by 1/w (w the leaf width) so every log2 term is O(1); the
+// remainder log2(w^2) * sum(tau) is added in FP64.  The inner loop is
+// branch-free: r^2 is floored at FLT_MIN (r^2 + FLT_MIN) and short chunks are
+// padded with far, uncharged sources.  The pairs inside the leaf itself that
+// meet the floor (the target's own point and exact duplicates, which the
+// reference skips, class_fmm.py:107) are counted in the first passes, over
+// the leaf's own points, and taken back out.  Distinct points of different
+// leaves closer than about 2^-24 leaf widths round to the same FP32 offsets
+// and keep log2(FLT_MIN) for their pair; the FP64 near field (near_fp64)
+// resolves such pairs.  FP32 partial sums of at most 32 terms are accumulated
+// in FP64.
 // one warp per block: leaves differ in work by more than 10x, and a block of
 // several warps would hold its SM slot until its slowest warp is done
 constexpr int LEAF_WARPS = 1;
-// 28 one-warp blocks per SM (72 registers) with 128-source chunks measured
-// 8% faster than 20 blocks (96 registers) with 256-source chunks on the 1M
-// mixture; shared memory per block sets the ceiling near 32
+// 32 one-warp blocks per SM (64 registers) with 96-source chunks measured 2%
+// faster than 28 blocks (72 registers) with 128-source chunks on the 1M
+// mixture (0.240 against 0.244 ms), and those 8% faster than 20 blocks (96
+// registers) with 256-source chunks; shared memory per block sets the ceiling
 #ifndef KIFMM_LEAF_BLOCKS_PER_SM
-#define KIFMM_LEAF_BLOCKS_PER_SM 28
+#define KIFMM_LEAF_BLOCKS_PER_SM 32
 #endif
 #ifndef KIFMM_LEAF_CHUNK
-#define KIFMM_LEAF_CHUNK 128
+#define KIFMM_LEAF_CHUNK 96
 #endif
 constexpr int LEAF_BLOCKS_PER_SM = KIFMM_LEAF_BLOCKS_PER_SM;  // resident blocks per SM at the register bound
 constexpr int LEAF_CHUNK = KIFMM_LEAF_CHUNK;                  // sources staged per pass
