@@ -866,26 +866,33 @@ void launch_morton_keys(const double *x, const double *y, int64_t n, double m, d
     KIFMM_LAUNCHED();
 }
 
-void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int mem) {
+static void build_tree_impl(kifmm_plan *P, const double *x, const double *y, int64_t n, int mem) {
     KIFMM_REQUIRE(n > 0 && n < (1ll << 31) - 1, KIFMM_ERR_ARG, "build_tree: need 0 < n < 2^31-1 points");
     KIFMM_REQUIRE(x && y, KIFMM_ERR_ARG, "build_tree: null coordinate pointer");
     cudaStream_t s = P->stream;
     P->have_tree = P->have_ops = P->have_expansions = false;
     P->N = n;
-    P->x.alloc(n); P->y.alloc(n);
-    cudaMemcpyKind kind = mem == KIFMM_MEM_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-    KIFMM_CUDA(cudaMemcpyAsync(P->x.p, x, n * sizeof(double), kind, s));
-    KIFMM_CUDA(cudaMemcpyAsync(P->y.p, y, n * sizeof(double), kind, s));
+    // The coordinates are read only inside this call (root box, keys, the
+    // gather into Morton order, all complete before it returns): device
+    // arrays are read in place, host arrays are uploaded once.
+    const double *xd = x, *yd = y;
+    if (mem != KIFMM_MEM_DEVICE) {
+        P->x.alloc(n); P->y.alloc(n);
+        KIFMM_CUDA(cudaMemcpyAsync(P->x.p, x, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        KIFMM_CUDA(cudaMemcpyAsync(P->y.p, y, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        xd = P->x.p;
+        yd = P->y.p;
+    }
     P->scal.alloc(KIFMM_SCAL_WORDS);
     KIFMM_CUDA(cudaMemcpyAsync(P->scal.p, P->hpin + HP_INIT, 16 * sizeof(unsigned long long), cudaMemcpyHostToDevice,
                                s));
     const int TB = 256;
     unsigned gs = grid_for(n, TB, P->num_sms * 8);
-    k_bbox<<<gs, TB, 0, s>>>(P->x.p, P->y.p, n, P->scal.p);
+    k_bbox<<<gs, TB, 0, s>>>(xd, yd, n, P->scal.p);
     KIFMM_LAUNCHED();
     P->pkey.alloc(n); P->perm.alloc(n); P->key2.alloc(n); P->perm2.alloc(n);
     // the root box stays on the device until the counts below come back
-    launch_pdl(k_keys_dev, dim3(gs), dim3(TB), 0, s, (const double *)P->x.p, (const double *)P->y.p, n,
+    launch_pdl(k_keys_dev, dim3(gs), dim3(TB), 0, s, xd, yd, n,
                (int)P->opt.fix_bbox, (const unsigned long long *)P->scal.p, P->pkey.p, P->perm.p, P->scal.p + 8);
     // Sort by the top 32 key bits first (levels 1..16, four 8-bit passes): that
     // orders every cell of level <= 16, enough whenever no split lies deeper
@@ -966,7 +973,7 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
         radix_sort_pairs(P->pkey.p, P->perm.p, P->key2.p, P->perm2.p, n, 2 * KEY_DEPTH, P);
     }
     P->xs.alloc(n); P->ys.alloc(n);
-    launch_pdl(k_gather2, dim3(gs), dim3(TB), 0, s, (const double *)P->x.p, (const double *)P->y.p,
+    launch_pdl(k_gather2, dim3(gs), dim3(TB), 0, s, xd, yd,
                (const int32_t *)P->perm.p, n, P->xs.p, P->ys.p);
     P->n_outside = (int64_t)st[3];
     KIFMM_REQUIRE(st[2] == 0, KIFMM_ERR_DEPTH,
@@ -1106,6 +1113,17 @@ void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int 
     P->have_stats = false;
     build_leaf_records(P);
     P->have_tree = true;
+}
+
+void build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n, int mem) {
+    try {
+        build_tree_impl(P, x, y, n, mem);
+    } catch (...) {
+        // device coordinates are read in place: nothing may still read them
+        // once the call has returned, error or not
+        cudaStreamSynchronize(P->stream);
+        throw;
+    }
 }
 
 // Work counts for reporting (kifmm_get_tree_info), computed on request.
