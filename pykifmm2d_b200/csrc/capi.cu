@@ -406,6 +406,7 @@ int kifmm_synchronize(kifmm_plan *P) {
     return guarded([&] {
         KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
         use_device(P);
+        ops_wait_now(P);
         KIFMM_CUDA(cudaStreamSynchronize(P->stream));
         check_device_flags(P);
     });
@@ -523,7 +524,7 @@ int kifmm_plan_destroy(kifmm_plan *P) {
         for (auto &ph : P->pending) { cudaEventDestroy(ph.a); cudaEventDestroy(ph.b); }
         P->pending.clear();
         cudaStream_t s = P->stream, side = P->side;
-        cudaEvent_t e0 = P->ops_fork, e1 = P->ops_done, e2 = P->tree_ev;
+        cudaEvent_t e0 = P->ops_fork, e1 = P->ops_done, e2 = P->tree_ev, e3 = P->ops_circ;
         bool own = P->own_stream;
         unsigned long long *hp = P->hpin;
         delete P;  // buffers are freed stream-ordered on s and on the side stream
@@ -534,6 +535,7 @@ int kifmm_plan_destroy(kifmm_plan *P) {
             cudaEventDestroy(e0);
             cudaEventDestroy(e1);
             cudaEventDestroy(e2);
+            cudaEventDestroy(e3);
         }
         if (own && s) cudaStreamDestroy(s);
     });

@@ -1,5 +1,6 @@
 // kifmm_internal.cuh -- shared definitions of the sm_100a KIFMM library.
 #pragma once
+#include <initializer_list>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -150,9 +151,12 @@ struct kifmm_plan {
     // stream waits on ops_done before the operators are used
     cudaStream_t side = nullptr;
     cudaEvent_t ops_fork = nullptr, ops_done = nullptr;
+    cudaEvent_t ops_circ = nullptr;  // side stream: the check circles are written (the P2M's only operator input)
     cudaEvent_t tree_ev = nullptr;   // build_tree: the split-cell counts are on the host
     uint64_t spec_cap = 0;           // split-cell capacity for the next build (from the last one)
     bool ops_pending = false;
+    bool ops_wait = false;  // operators joined by precompute, the main stream's wait for them not issued yet
+    bool circ_wait = false; // ... and its wait for the check circles (ops_circ) not issued yet
     cudaGraphExec_t graph = nullptr;  // captured apply (kifmm_graph_capture)
     long long wait_limit = -1;        // poll budget of the apply kernels' first waits (-1: kDefaultWaitPolls)
     int device = 0;
@@ -260,6 +264,18 @@ namespace kifmm {
 // are no-ops.
 __device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 __device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+// Fill ranges of 32-bit words with a value in one launch (programmatic
+// dependent launch: it waits for the previous kernel before writing).  Used
+// in place of chains of cudaMemsetAsync, each of which is a launch of its own
+// that the next kernel cannot overlap.
+struct FillRange {
+    void *p;
+    size_t words;
+    uint32_t value;
+};
+void launch_fill(kifmm_plan *P, std::initializer_list<FillRange> ranges);
+constexpr int M2L_KEYS = 257;  // direction-mask groups per level in the M2L target order (256 masks + non-split)
 template <typename... KArgs, typename... Args>
 inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s, Args &&...args) {
     cudaLaunchConfig_t cfg = {};
@@ -465,6 +481,8 @@ void ensure_side(kifmm_plan *P);      // side stream and its events
 void start_operators(kifmm_plan *P, bool fork_recorded = false);  // build_operators on the side stream
 cudaStream_t device_side_stream(int device);  // one per device, created on first use
 void join_operators(kifmm_plan *P);   // main stream waits for it
+void ops_wait_now(kifmm_plan *P);     // issue a deferred join's stream wait (before any operator is read)
+void ops_wait_circles(kifmm_plan *P); // ... for the check circles only (before the P2M)
 // planned.cu
 bool planned_ready(const kifmm_plan *P);
 void build_plan_matrices(kifmm_plan *P);

@@ -373,6 +373,7 @@ void build_operators(kifmm_plan *P) {
     ensure_dyn_smem(k_ops_inverse, smem);
     k_ops_inverse<<<L, INV_THREADS, smem, s>>>(A);
     KIFMM_LAUNCHED();
+    if (P->side && s == P->side) KIFMM_CUDA(cudaEventRecord(P->ops_circ, s));  // circles written
     if (L >= 2) {
         size_t csm = (size_t)5 * Q * Q * sizeof(double);
         ensure_dyn_smem(k_ops_compose, csm);
@@ -413,6 +414,7 @@ void ensure_side(kifmm_plan *P) {
     KIFMM_CUDA(cudaEventCreateWithFlags(&P->ops_fork, cudaEventDisableTiming));
     KIFMM_CUDA(cudaEventCreateWithFlags(&P->ops_done, cudaEventDisableTiming));
     KIFMM_CUDA(cudaEventCreateWithFlags(&P->tree_ev, cudaEventDisableTiming));
+    KIFMM_CUDA(cudaEventCreateWithFlags(&P->ops_circ, cudaEventDisableTiming));
 }
 
 // fork_recorded: the caller has recorded ops_fork on the main stream at the
@@ -443,11 +445,29 @@ void start_operators(kifmm_plan *P, bool fork_recorded) {
     P->ops_pending = true;
 }
 
+// precompute(): the operators count as built; the main stream's wait for the
+// side stream is deferred to the first kernel that reads them (the apply
+// issues it after its P2M, which needs no operator, so that the operator
+// build's tail overlaps the P2M)
 void join_operators(kifmm_plan *P) {
     if (!P->ops_pending) return;
-    KIFMM_CUDA(cudaStreamWaitEvent(P->stream, P->ops_done, 0));
     P->ops_pending = false;
+    P->ops_wait = P->circ_wait = true;
     P->have_ops = true;
+}
+
+void ops_wait_now(kifmm_plan *P) {
+    if (!P->ops_wait) return;
+    KIFMM_CUDA(cudaStreamWaitEvent(P->stream, P->ops_done, 0));
+    P->ops_wait = P->circ_wait = false;
+}
+
+// the check circles (written by the first operator kernel) are all the P2M
+// reads of the operators
+void ops_wait_circles(kifmm_plan *P) {
+    if (!P->circ_wait) return;
+    KIFMM_CUDA(cudaStreamWaitEvent(P->stream, P->ops_circ, 0));
+    P->circ_wait = false;
 }
 
 }  // namespace kifmm

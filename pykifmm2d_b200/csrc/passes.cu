@@ -214,7 +214,7 @@ __global__ void k_m2l_d(PassArgs A, int l) {
 // (a zero vector where a target has none).  Stages run through a ring of two
 // shared-memory buffers filled by bulk copies on an mbarrier each: the
 // operator chunk as 32 columns of 4Q doubles, the sources as 32 rows of 32
-// doubles; one thread issues a stage's copies as soon as the buffer is free,
+// doubles; warp 0 issues a stage's copies as soon as the buffer is free,
 // so the copies of stage s + 1 land while stage s computes.  Warp w owns row
 // tiles w, w + 8, ... (8 rows each) for all 32 targets.  D is assigned to the
 // children's u_down (the L2L chain adds afterwards).  Needs Q even.
@@ -279,24 +279,28 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
     }
     __syncthreads();
     const int nkc = (Q4 + MD_KC - 1) / MD_KC, nst = snd * nkc;
-    // one thread issues all copies of stage st into buffer st % 2
+    // the lanes of warp 0 issue the copies of stage st into buffer st % 2
+    // (one operator column and one source row each: issued by one thread
+    // they kept warp 0, and the whole block at the next barrier, waiting)
     auto issue = [&](int st) {
         const int dd = sdir[st / nkc], d = dd < 4 ? dd : dd + 1, kc = st % nkc, k0 = kc * MD_KC;
         const int kn = min(MD_KC, Q4 - k0), cm = scm[dd];
         double *bs = buf[st & 1];
         const uint32_t bar = smem_u32(&bars[st & 1]);
-        mbar_expect_tx(bar, (uint32_t)(kn * Q4 + 8 * __popc(cm) * kn) * 8u);
+        if (lane == 0) mbar_expect_tx(bar, (uint32_t)(kn * Q4 + 8 * __popc(cm) * kn) * 8u);
+        __syncwarp();
         const double *op = opl + (size_t)d * Q4 * Q4 + (size_t)k0 * Q4;
-        for (int c = 0; c < kn; c++) bulk_g2s(smem_u32(bs + (size_t)c * ldo), op + (size_t)c * Q4, (uint32_t)Q4 * 8u, bar);
+        for (int c = lane; c < kn; c += 32)
+            bulk_g2s(smem_u32(bs + (size_t)c * ldo), op + (size_t)c * Q4, (uint32_t)Q4 * 8u, bar);
         double *xs = bs + (size_t)MD_KC * ldo;
-        for (int n = 0; n < MD_TE; n++) {
+        for (int n = lane; n < MD_TE; n += 32) {
             if (!((cm >> (n >> 3)) & 1)) continue;
             const int je = ssrc[n * 8 + dd];
             const double *src = je >= 0 ? A.uup + (size_t)(A.T.off[l + 1] + 4 * (je - eoff)) * Q + k0 : M.zero + k0;
             bulk_g2s(smem_u32(xs + (size_t)n * ldx), src, (uint32_t)kn * 8u, bar);
         }
     };
-    if (tid == 0 && nst > 0) {
+    if (warp == 0 && nst > 0) {
         issue(0);
         if (nst > 1) issue(1);
     }
@@ -333,7 +337,7 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
             }
         }
         __syncthreads();  // buffer bi is free
-        if (tid == 0 && st + 2 < nst) issue(st + 2);
+        if (warp == 0 && st + 2 < nst) issue(st + 2);
     }
     if (!ok) {
         if (tid == 0) atomicOr(M.err, 1ull);
@@ -541,9 +545,10 @@ void build_leaf_records(kifmm_plan *P) {
 // zero vectors.  The mask depends on the tree only: the order is built once
 // per tree.  Within a group the order is whatever the atomics give; the M2L
 // result of a target does not depend on which other targets share its tile.
-constexpr int M2L_KEYS = 257;
 __global__ void k_m2l_keys(PassArgs A, int64_t n_ent, uint16_t *__restrict__ key, int32_t *__restrict__ src8,
                            unsigned *__restrict__ hist) {
+    pdl_trigger();
+    pdl_wait();
     const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const bool in = j < n_ent;
     unsigned bin = 0xffffffffu;
@@ -573,6 +578,8 @@ __global__ void k_m2l_keys(PassArgs A, int64_t n_ent, uint16_t *__restrict__ key
 constexpr int M2L_SCAN_THREADS = 288;  // >= M2L_KEYS, a whole number of warps
 __global__ void __launch_bounds__(M2L_SCAN_THREADS) k_m2l_cursors(LevelTable T, unsigned *__restrict__ hist) {
     __shared__ unsigned wsum[M2L_SCAN_THREADS / 32];
+    pdl_trigger();
+    pdl_wait();
     const int l = blockIdx.x, k = threadIdx.x, lane = k & 31, w = k >> 5;
     const unsigned c = k < M2L_KEYS ? hist[l * M2L_KEYS + k] : 0u;
     unsigned v = c;  // inclusive scan within the warp
@@ -590,6 +597,8 @@ __global__ void __launch_bounds__(M2L_SCAN_THREADS) k_m2l_cursors(LevelTable T, 
 
 __global__ void k_m2l_place(const uint64_t *__restrict__ ent, const uint16_t *__restrict__ key, int64_t n_ent,
                             unsigned *__restrict__ cursor, int32_t *__restrict__ perm) {
+    pdl_trigger();
+    pdl_wait();
     const int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const bool in = j < n_ent;
     const int lane = threadIdx.x & 31;
@@ -609,16 +618,15 @@ void build_m2l_order(kifmm_plan *P) {
     KIFMM_REQUIRE(P->L <= MAX_LEVELS + 1 && n < (1ll << 31), KIFMM_ERR_ARG, "M2L order: tree too large");
     P->m2l_key.alloc(n);
     P->m2l_src8.alloc((size_t)8 * n);
-    P->m2l_hist.alloc((size_t)(MAX_LEVELS + 1) * M2L_KEYS);
-    KIFMM_CUDA(cudaMemsetAsync(P->m2l_hist.p, 0, (size_t)(MAX_LEVELS + 1) * M2L_KEYS * sizeof(unsigned), P->stream));
+    // m2l_hist ([MAX_LEVELS + 1][M2L_KEYS] counts) is allocated and cleared by
+    // build_tree with the split-cell set
     PassArgs A = make_pass_args(P);
     const unsigned gr = (unsigned)((n + 255) / 256);
-    k_m2l_keys<<<gr, 256, 0, P->stream>>>(A, n, P->m2l_key.p, P->m2l_src8.p, P->m2l_hist.p);
-    KIFMM_LAUNCHED();
-    k_m2l_cursors<<<(unsigned)std::min(P->L, MAX_LEVELS + 1), M2L_SCAN_THREADS, 0, P->stream>>>(P->lt, P->m2l_hist.p);
-    KIFMM_LAUNCHED();
-    k_m2l_place<<<gr, 256, 0, P->stream>>>((const uint64_t *)P->ent.p, P->m2l_key.p, n, P->m2l_hist.p,
-                                           P->m2l_perm.p);
+    launch_pdl(k_m2l_keys, dim3(gr), dim3(256), 0, P->stream, A, n, P->m2l_key.p, P->m2l_src8.p, P->m2l_hist.p);
+    launch_pdl(k_m2l_cursors, dim3((unsigned)std::min(P->L, MAX_LEVELS + 1)), dim3(M2L_SCAN_THREADS), 0, P->stream,
+               P->lt, P->m2l_hist.p);
+    launch_pdl(k_m2l_place, dim3(gr), dim3(256), 0, P->stream, (const uint64_t *)P->ent.p,
+               (const uint16_t *)P->m2l_key.p, n, P->m2l_hist.p, P->m2l_perm.p);
     KIFMM_LAUNCHED();
 }
 
@@ -1073,7 +1081,11 @@ void apply_prologue(kifmm_plan *P) {
                                (KIFMM_SCAL_WORDS - KIFMM_SCAL_PASS_ERR) * sizeof(unsigned long long), s));
     KIFMM_CUDA(cudaMemsetAsync(P->uup.p, 0, (size_t)NN * Q * sizeof(double), s));
     KIFMM_CUDA(cudaMemsetAsync(P->udown.p, 0, (size_t)NN * Q * sizeof(double), s));
-    if (P->opt.planned) build_plan_matrices(P);  // first apply after build_tree / precompute
+    if (P->opt.planned) {
+        ops_wait_now(P);
+        build_plan_matrices(P);  // first apply after build_tree / precompute
+    }
+    ops_wait_circles(P);  // the P2M's check points
     if (P->cplx)
         launch_gather_tau_c(P);
     else
@@ -1087,9 +1099,13 @@ void run_upward_downward(kifmm_plan *P) {
     apply_prologue(P);
     if (P->opt.precision == KIFMM_PREC_MIXED) {
         run_passes_mixed(P);
+        ops_wait_now(P);  // (L < 3: the evaluation reads them)
         return;
     }
-    if (L < 3) return;  // no level has well-separated boxes
+    if (L < 3) {  // no level has well-separated boxes
+        ops_wait_now(P);
+        return;
+    }
     PassArgs A = make_pass_args(P);
     if (P->n_p2m_list) {
         PhaseScope ph(P, KIFMM_PHASE_P2M);
@@ -1097,6 +1113,7 @@ void run_upward_downward(kifmm_plan *P) {
         else if (planned_ready(P)) launch_planned_p2m(P, A);
         else launch_p2m_d(P, A);
     }
+    ops_wait_now(P);  // the P2M reads only the check circles
     {
         PhaseScope ph_m2m(P, KIFMM_PHASE_M2M);
         run_m2m_levels(P, A);

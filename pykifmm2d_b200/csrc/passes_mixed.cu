@@ -752,6 +752,7 @@ void mixed_upward(kifmm_plan *P, const PassArgs &A) {
         if (planned_ready(P)) launch_planned_p2m(P, A);
         else launch_p2m_d(P, A);
     }
+    ops_wait_now(P);  // the P2M reads only the check circles
     PhaseScope ph(P, KIFMM_PHASE_M2M);
     run_m2m_levels(P, A);
 }

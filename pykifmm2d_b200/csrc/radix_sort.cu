@@ -366,8 +366,7 @@ static void os_run(uint64_t *key, int32_t *val, uint64_t *key_tmp, int32_t *val_
     P->sort_status.alloc(nstat);
     uint32_t *hist = P->sort_hist.p;
     unsigned *ctr = P->sort_hist.p + (size_t)npass * 256;
-    KIFMM_CUDA(cudaMemsetAsync(hist, 0, ((size_t)npass * 256 + npass) * sizeof(uint32_t), s));
-    KIFMM_CUDA(cudaMemsetAsync(P->sort_status.p, 0, nstat * sizeof(unsigned long long), s));
+    launch_fill(P, {{hist, (size_t)npass * 256 + npass, 0u}, {P->sort_status.p, 2 * nstat, 0u}});
     const unsigned hg = (unsigned)std::min<int64_t>(ntiles, (int64_t)P->num_sms * 4);
     uint64_t packed = 0;
     for (int p = 0; p < npass; p++) packed |= (uint64_t)(shifts[p] & 63) << (8 * p);

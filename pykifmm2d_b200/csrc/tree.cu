@@ -866,6 +866,47 @@ void launch_morton_keys(const double *x, const double *y, int64_t n, double m, d
     KIFMM_LAUNCHED();
 }
 
+struct FillArgs {
+    uint32_t *p[6];
+    size_t n[6];
+    uint32_t v[6];
+    int k;
+};
+__global__ void k_fill(FillArgs F) {
+    pdl_trigger();
+    pdl_wait();  // the previous kernel may still read what is overwritten here
+    const size_t t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x, ts = (size_t)gridDim.x * blockDim.x;
+    for (int r = 0; r < F.k; r++) {
+        uint32_t *p = F.p[r];
+        const size_t n = F.n[r];
+        const uint32_t v = F.v[r];
+        size_t head = 0;  // words before the first 16-byte boundary
+        while (head < n && (((uintptr_t)(p + head)) & 15)) head++;
+        for (size_t i = t0; i < head; i += ts) p[i] = v;
+        uint4 *q = (uint4 *)(p + head);
+        const size_t nq = (n - head) / 4;
+        for (size_t i = t0; i < nq; i += ts) q[i] = make_uint4(v, v, v, v);
+        for (size_t i = head + 4 * nq + t0; i < n; i += ts) p[i] = v;
+    }
+}
+
+void launch_fill(kifmm_plan *P, std::initializer_list<FillRange> ranges) {
+    FillArgs F{};
+    size_t words = 0;
+    for (const FillRange &r : ranges) {
+        KIFMM_REQUIRE(F.k < 6, KIFMM_ERR_ARG, "launch_fill: at most six ranges");
+        if (!r.words) continue;
+        F.p[F.k] = (uint32_t *)r.p;
+        F.n[F.k] = r.words;
+        F.v[F.k] = r.value;
+        F.k++;
+        words += r.words;
+    }
+    if (!F.k) return;
+    const unsigned grid = grid_for((int64_t)((words + 3) / 4), 256, P->num_sms * 8);
+    launch_pdl(k_fill, dim3(grid), dim3(256), 0, P->stream, F);
+}
+
 static void build_tree_impl(kifmm_plan *P, const double *x, const double *y, int64_t n, int mem) {
     KIFMM_REQUIRE(n > 0 && n < (1ll << 31) - 1, KIFMM_ERR_ARG, "build_tree: need 0 < n < 2^31-1 points");
     KIFMM_REQUIRE(x && y, KIFMM_ERR_ARG, "build_tree: null coordinate pointer");
@@ -906,6 +947,7 @@ static void build_tree_impl(kifmm_plan *P, const double *x, const double *y, int
     H.count = P->scal.p + 9;
     H.ovf = P->scal.p + 10;
     P->misc.alloc(128);
+    P->m2l_hist.alloc((size_t)(MAX_LEVELS + 1) * M2L_KEYS);
     unsigned long long *lc = (unsigned long long *)P->misc.p;  // [32] entries per level
     unsigned long long lcount[32] = {};
     const unsigned cgrid = grid_for((n + 31) / 32 * 32, TB, P->num_sms * 64);
@@ -913,15 +955,21 @@ static void build_tree_impl(kifmm_plan *P, const double *x, const double *y, int
     // The split-cell set for a list capacity: table and list sized and
     // cleared, the closure and the X-list, then count, overflow and per-level
     // counts to the host, marked by tree_ev.
+    bool misc_cleared = false;  // by a queued split-cell set (launch_fill below)
     auto queue_closure = [&](uint64_t cap) {
+        misc_cleared = true;
         uint64_t hcap = 1;
         while (hcap < 2 * cap) hcap <<= 1;
         P->hash.alloc(hcap);
         P->hash_cap = hcap;
         P->list.alloc(cap);
-        KIFMM_CUDA(cudaMemsetAsync(P->hash.p, 0xFF, hcap * sizeof(uint64_t), s));
-        KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 9, 0, 2 * sizeof(unsigned long long), s));
-        KIFMM_CUDA(cudaMemsetAsync(lc, 0, 32 * sizeof(unsigned long long), s));
+        // one launch clears the table (all ones), the set's count and overflow
+        // flag, the per-level entry counts and the later list counters (misc),
+        // and the M2L target order's histogram
+        launch_fill(P, {{P->hash.p, 2 * hcap, 0xFFFFFFFFu},
+                        {P->scal.p + 9, 4, 0u},
+                        {P->misc.p, 2 * 128, 0u},
+                        {P->m2l_hist.p, (size_t)(MAX_LEVELS + 1) * M2L_KEYS, 0u}});
         H.tab = (unsigned long long *)P->hash.p;
         H.mask = hcap - 1;
         H.list = P->list.p;
@@ -947,7 +995,9 @@ static void build_tree_impl(kifmm_plan *P, const double *x, const double *y, int
     if (!spec_cap)
         spec_cap = std::min<uint64_t>(16 * (uint64_t)std::max<int64_t>(n / P->ppl, 1), 2 * (uint64_t)n) + 4096;
     for (int full = 0; full < 2; full++) {
-        KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 5, 0, 3 * sizeof(unsigned long long), s));
+        // T0 count, depth and overflow: still zero from the reset copy at the
+        // start of this call on the first pass
+        if (full) KIFMM_CUDA(cudaMemsetAsync(P->scal.p + 5, 0, 3 * sizeof(unsigned long long), s));
         launch_pdl(k_t0_count, dim3(gs), dim3(TB), 0, s, (const uint64_t *)P->pkey.p, n, (int64_t)P->ppl, P->scal.p);
         KIFMM_CUDA(cudaMemcpyAsync(P->hpin + HP_SCAL, P->scal.p, sizeof(sc), cudaMemcpyDeviceToHost, s));
         KIFMM_CUDA(cudaEventRecord(P->ops_fork, s));
@@ -1072,8 +1122,9 @@ static void build_tree_impl(kifmm_plan *P, const double *x, const double *y, int
     KIFMM_LAUNCHED();
     unsigned long long *cnt = (unsigned long long *)P->misc.p + 32;
     unsigned long long *lcnt = (unsigned long long *)P->misc.p + 64;  // [MAX_LEVELS] leaves per level
-    KIFMM_CUDA(cudaMemsetAsync(cnt, 0, 8 * sizeof(unsigned long long), s));
-    KIFMM_CUDA(cudaMemsetAsync(lcnt, 0, MAX_LEVELS * sizeof(unsigned long long), s));
+    // cnt and lcnt were cleared with the split-cell set (launch_fill above);
+    // a single-leaf tree queued none
+    if (!misc_cleared) launch_fill(P, {{P->misc.p, 2 * 128, 0u}});
     {
         const int64_t ntiles = (NN + LT_TILE - 1) / LT_TILE;
         P->list_tiles.alloc(2 * ntiles);
