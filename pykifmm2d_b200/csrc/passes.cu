@@ -218,7 +218,15 @@ __global__ void k_m2l_d(PassArgs A, int l) {
 // so the copies of stage s + 1 land while stage s computes.  Warp w owns row
 // tiles w, w + 8, ... (8 rows each) for all 32 targets.  D is assigned to the
 // children's u_down (the L2L chain adds afterwards).  Needs Q even.
-constexpr int MD_THREADS = 256, MD_TE = 32, MD_KC = 32, MD_MT = 4;  // Q4 <= 8 warps x MD_MT x 8 rows
+#ifndef KIFMM_MD_KC
+#define KIFMM_MD_KC 32
+#endif
+#ifndef KIFMM_MD_NBUF
+#define KIFMM_MD_NBUF 2
+#endif
+constexpr int MD_THREADS = 256, MD_TE = 32, MD_KC = KIFMM_MD_KC, MD_MT = 4;  // Q4 <= 8 warps x MD_MT x 8 rows
+constexpr int MD_NBUF = KIFMM_MD_NBUF;  // ring slots: copies run MD_NBUF - 1 stages ahead
+static_assert(MD_KC % 4 == 0 && MD_NBUF >= 2 && MD_NBUF <= 8, "DMMA M2L staging shape");
 struct M2lDmmaArgs {
     PassArgs A;
     const double *zero;                 // 4Q zeros
@@ -231,7 +239,7 @@ static size_t m2l_dmma_smem(int Q4) {
     const size_t ldo = pad4mod16(Q4), ldx = pad4mod16(MD_KC);
     const size_t stage = (size_t)MD_KC * ldo + (size_t)MD_TE * ldx;
     const size_t out = (size_t)MD_TE * (Q4 + 1);
-    return (2 * stage > out ? 2 * stage : out) * sizeof(double) + MD_TE * 8 * sizeof(int) + 64;
+    return (MD_NBUF * stage > out ? MD_NBUF * stage : out) * sizeof(double) + MD_TE * 8 * sizeof(int) + 64;
 }
 __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
     extern __shared__ __align__(128) double sm_md[];
@@ -239,9 +247,9 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
     const int Q = A.Q, Q4 = 4 * Q, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int ldo = pad4mod16(Q4), ldx = pad4mod16(MD_KC);
     const size_t stage_d = (size_t)MD_KC * ldo + (size_t)MD_TE * ldx;
-    double *buf[2] = {sm_md, sm_md + stage_d};
-    int *ssrc = (int *)(sm_md + (2 * stage_d > (size_t)MD_TE * (Q4 + 1) ? 2 * stage_d : (size_t)MD_TE * (Q4 + 1)));
-    __shared__ __align__(8) uint64_t bars[2];
+    int *ssrc = (int *)(sm_md + (MD_NBUF * stage_d > (size_t)MD_TE * (Q4 + 1) ? MD_NBUF * stage_d
+                                                                              : (size_t)MD_TE * (Q4 + 1)));
+    __shared__ __align__(8) uint64_t bars[MD_NBUF];
     __shared__ int sact[MD_TE];
     __shared__ int sdir[8], scm[8], snd;  // active directions, their 8-target column tiles with a source
     pdl_trigger();
@@ -257,10 +265,8 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
         sact[tid] = act ? (int)(ej - eoff) + 1 : 0;
         for (int dd = 0; dd < 8; dd++) ssrc[tid * 8 + dd] = act ? A.m2l_src8[ej * 8 + dd] : -1;
     }
-    if (tid == 0) {
-        mbar_init(smem_u32(&bars[0]));
-        mbar_init(smem_u32(&bars[1]));
-    }
+    if (tid == 0)
+        for (int i = 0; i < MD_NBUF; i++) mbar_init(smem_u32(&bars[i]));
     __syncthreads();
     // Work skipped: a direction no target of the block has a source in, and
     // within a direction each 8-target column tile without one (a V-list
@@ -285,8 +291,8 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
     auto issue = [&](int st) {
         const int dd = sdir[st / nkc], d = dd < 4 ? dd : dd + 1, kc = st % nkc, k0 = kc * MD_KC;
         const int kn = min(MD_KC, Q4 - k0), cm = scm[dd];
-        double *bs = buf[st & 1];
-        const uint32_t bar = smem_u32(&bars[st & 1]);
+        double *bs = sm_md + (size_t)(st % MD_NBUF) * stage_d;
+        const uint32_t bar = smem_u32(&bars[st % MD_NBUF]);
         if (lane == 0) mbar_expect_tx(bar, (uint32_t)(kn * Q4 + 8 * __popc(cm) * kn) * 8u);
         __syncwarp();
         const double *op = opl + (size_t)d * Q4 * Q4 + (size_t)k0 * Q4;
@@ -300,27 +306,25 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
             bulk_g2s(smem_u32(xs + (size_t)n * ldx), src, (uint32_t)kn * 8u, bar);
         }
     };
-    if (warp == 0 && nst > 0) {
-        issue(0);
-        if (nst > 1) issue(1);
-    }
+    if (warp == 0)
+        for (int st = 0; st < MD_NBUF && st < nst; st++) issue(st);
     const int g = lane >> 2, t = lane & 3, nrt = Q4 / 8;
     double acc[MD_MT][4][2];
 #pragma unroll
     for (int i = 0; i < MD_MT; i++)
 #pragma unroll
         for (int c = 0; c < 4; c++) acc[i][c][0] = acc[i][c][1] = 0.0;
-    uint32_t par[2] = {0u, 0u};
+    uint32_t par = 0u;  // bit b: parity of slot b's next phase
     bool ok = true;
-    int landed = 0;  // stages waited for (issued stages: min(nst, landed + 2))
+    int landed = 0;  // stages waited for (issued stages: min(nst, landed + MD_NBUF))
     for (int st = 0; st < nst; st++) {
-        const int bi = st & 1;
-        ok = __syncthreads_and(mbar_wait(smem_u32(&bars[bi]), par[bi], M.wait_limit));
+        const int bi = st % MD_NBUF;
+        ok = __syncthreads_and(mbar_wait(smem_u32(&bars[bi]), (par >> bi) & 1u, M.wait_limit));
         if (!ok) break;
-        par[bi] ^= 1u;
+        par ^= 1u << bi;
         landed++;
         const int kn = min(MD_KC, Q4 - (st % nkc) * MD_KC), cm = scm[sdir[st / nkc]];
-        const double *os = buf[bi], *xs = buf[bi] + (size_t)MD_KC * ldo;
+        const double *os = sm_md + (size_t)bi * stage_d, *xs = os + (size_t)MD_KC * ldo;
         for (int k0 = 0; k0 < kn; k0 += 4) {
             double bv[4];
 #pragma unroll
@@ -337,15 +341,15 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
             }
         }
         __syncthreads();  // buffer bi is free
-        if (warp == 0 && st + 2 < nst) issue(st + 2);
+        if (warp == 0 && st + MD_NBUF < nst) issue(st + MD_NBUF);
     }
     if (!ok) {
         if (tid == 0) atomicOr(M.err, 1ull);
         // let every issued copy land before the block leaves
-        const int issued = min(nst, landed + 2);
+        const int issued = min(nst, landed + MD_NBUF);
         for (int st = landed; st < issued; st++) {
-            mbar_wait(smem_u32(&bars[st & 1]), par[st & 1], kDrainWaitPolls);
-            par[st & 1] ^= 1u;
+            mbar_wait(smem_u32(&bars[st % MD_NBUF]), (par >> (st % MD_NBUF)) & 1u, kDrainWaitPolls);
+            par ^= 1u << (st % MD_NBUF);
         }
         return;
     }
