@@ -212,11 +212,13 @@ __global__ void k_m2l_d(PassArgs A, int l) {
 // D[4Q x 32] = sum over (direction, K chunk of 32) of C_d[:, chunk] .
 // B_d[chunk, 32], B_d's columns the targets' source groups in direction d
 // (a zero vector where a target has none).  Stages run through a ring of two
-// shared-memory buffers filled by bulk copies on an mbarrier each: the
-// operator chunk as 32 columns of 4Q doubles, the sources as 32 rows of 32
-// doubles; warp 0 issues a stage's copies as soon as the buffer is free,
-// so the copies of stage s + 1 land while stage s computes.  Warp w owns row
-// tiles w, w + 8, ... (8 rows each) for all 32 targets.  D is assigned to the
+// shared-memory slots, warp-specialised: a copy warp fills a slot by bulk
+// copies (the operator chunk as 32 columns of 4Q doubles, the sources as 32
+// rows of 32 doubles, one copy per lane) on the slot's full barrier as soon
+// as the eight compute warps have arrived on its empty barrier, so the
+// copies of stage s + 1 land while stage s computes and no block-wide
+// barrier stands in the loop.  Compute warp w owns row tiles w, w + 8, ...
+// (8 rows each) for all 32 targets.  D is assigned to the
 // children's u_down (the L2L chain adds afterwards).  Needs Q even.
 #ifndef KIFMM_MD_KC
 #define KIFMM_MD_KC 32
@@ -226,6 +228,7 @@ __global__ void k_m2l_d(PassArgs A, int l) {
 #endif
 constexpr int MD_THREADS = 256, MD_TE = 32, MD_KC = KIFMM_MD_KC, MD_MT = 4;  // Q4 <= 8 warps x MD_MT x 8 rows
 constexpr int MD_NBUF = KIFMM_MD_NBUF;  // ring slots: copies run MD_NBUF - 1 stages ahead
+constexpr int MD_BLOCK = MD_THREADS + 32;  // eight compute warps and one copy warp
 static_assert(MD_KC % 4 == 0 && MD_NBUF >= 2 && MD_NBUF <= 8, "DMMA M2L staging shape");
 struct M2lDmmaArgs {
     PassArgs A;
@@ -235,13 +238,18 @@ struct M2lDmmaArgs {
     long long wait_limit;
     unsigned long long *err;
 };
+// warp-uniform bounded wait on an mbarrier phase (every lane polls; true
+// once the phase has completed, false after `limit` polls)
+__device__ __forceinline__ bool warp_wait_all(uint32_t bar, uint32_t parity, long long limit) {
+    return __any_sync(0xffffffffu, mbar_wait(bar, parity, limit));
+}
 static size_t m2l_dmma_smem(int Q4) {
     const size_t ldo = pad4mod16(Q4), ldx = pad4mod16(MD_KC);
     const size_t stage = (size_t)MD_KC * ldo + (size_t)MD_TE * ldx;
     const size_t out = (size_t)MD_TE * (Q4 + 1);
     return (MD_NBUF * stage > out ? MD_NBUF * stage : out) * sizeof(double) + MD_TE * 8 * sizeof(int) + 64;
 }
-__global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
+__global__ void __launch_bounds__(MD_BLOCK, 2) k_m2l_dmma(M2lDmmaArgs M) {
     extern __shared__ __align__(128) double sm_md[];
     const PassArgs &A = M.A;
     const int Q = A.Q, Q4 = 4 * Q, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -249,7 +257,8 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
     const size_t stage_d = (size_t)MD_KC * ldo + (size_t)MD_TE * ldx;
     int *ssrc = (int *)(sm_md + (MD_NBUF * stage_d > (size_t)MD_TE * (Q4 + 1) ? MD_NBUF * stage_d
                                                                               : (size_t)MD_TE * (Q4 + 1)));
-    __shared__ __align__(8) uint64_t bars[MD_NBUF];
+    __shared__ __align__(8) uint64_t bars[MD_NBUF], empty[MD_NBUF];
+    __shared__ int sabort;
     __shared__ int sact[MD_TE];
     __shared__ int sdir[8], scm[8], snd;  // active directions, their 8-target column tiles with a source
     pdl_trigger();
@@ -265,8 +274,13 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
         sact[tid] = act ? (int)(ej - eoff) + 1 : 0;
         for (int dd = 0; dd < 8; dd++) ssrc[tid * 8 + dd] = act ? A.m2l_src8[ej * 8 + dd] : -1;
     }
-    if (tid == 0)
-        for (int i = 0; i < MD_NBUF; i++) mbar_init(smem_u32(&bars[i]));
+    if (tid == 0) {
+        for (int i = 0; i < MD_NBUF; i++) {
+            mbar_init(smem_u32(&bars[i]));              // full: the stage's copies (transaction bytes)
+            mbar_init(smem_u32(&empty[i]), MD_THREADS / 32);  // empty: each compute warp is done with it
+        }
+        sabort = 0;
+    }
     __syncthreads();
     // Work skipped: a direction no target of the block has a source in, and
     // within a direction each 8-target column tile without one (a V-list
@@ -306,59 +320,74 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
             bulk_g2s(smem_u32(xs + (size_t)n * ldx), src, (uint32_t)kn * 8u, bar);
         }
     };
-    if (warp == 0)
-        for (int st = 0; st < MD_NBUF && st < nst; st++) issue(st);
     const int g = lane >> 2, t = lane & 3, nrt = Q4 / 8;
     double acc[MD_MT][4][2];
 #pragma unroll
     for (int i = 0; i < MD_MT; i++)
 #pragma unroll
         for (int c = 0; c < 4; c++) acc[i][c][0] = acc[i][c][1] = 0.0;
-    uint32_t par = 0u;  // bit b: parity of slot b's next phase
-    bool ok = true;
-    int landed = 0;  // stages waited for (issued stages: min(nst, landed + MD_NBUF))
-    for (int st = 0; st < nst; st++) {
-        const int bi = st % MD_NBUF;
-        ok = __syncthreads_and(mbar_wait(smem_u32(&bars[bi]), (par >> bi) & 1u, M.wait_limit));
-        if (!ok) break;
-        par ^= 1u << bi;
-        landed++;
-        const int kn = min(MD_KC, Q4 - (st % nkc) * MD_KC), cm = scm[sdir[st / nkc]];
-        const double *os = sm_md + (size_t)bi * stage_d, *xs = os + (size_t)MD_KC * ldo;
-        for (int k0 = 0; k0 < kn; k0 += 4) {
-            double bv[4];
+    volatile int *abort_flag = &sabort;
+    if (warp == MD_THREADS / 32) {
+        // producer warp: stage st goes into slot st % MD_NBUF once the compute
+        // warps have released the slot's previous stage
+        int issued = 0;
+        for (int st = 0; st < nst; st++) {
+            const int slot = st % MD_NBUF;
+            if (st >= MD_NBUF && !warp_wait_all(smem_u32(&empty[slot]), (uint32_t)(st / MD_NBUF - 1) & 1u, M.wait_limit)) {
+                if (lane == 0) {
+                    *abort_flag = 1;
+                    atomicOr(M.err, 1ull);
+                }
+                break;
+            }
+            if (*abort_flag) break;
+            issue(st);
+            issued = st + 1;
+        }
+        // every copy issued lands before the block goes on (consumed stages
+        // have landed already; this matters after an abort)
+        for (int st = issued > MD_NBUF ? issued - MD_NBUF : 0; st < issued; st++)
+            mbar_wait(smem_u32(&bars[st % MD_NBUF]), (uint32_t)(st / MD_NBUF) & 1u, kDrainWaitPolls);
+    } else {
+        for (int st = 0; st < nst; st++) {
+            const int bi = st % MD_NBUF;
+            if (!warp_wait_all(smem_u32(&bars[bi]), (uint32_t)(st / MD_NBUF) & 1u, M.wait_limit)) {
+                if (lane == 0) {
+                    *abort_flag = 1;
+                    atomicOr(M.err, 1ull);
+                }
+                break;
+            }
+            if (*abort_flag) break;
+            const int kn = min(MD_KC, Q4 - (st % nkc) * MD_KC), cm = scm[sdir[st / nkc]];
+            const double *os = sm_md + (size_t)bi * stage_d, *xs = os + (size_t)MD_KC * ldo;
+            for (int k0 = 0; k0 < kn; k0 += 4) {
+                double bv[4];
 #pragma unroll
-            for (int c = 0; c < 4; c++) bv[c] = xs[(size_t)(8 * c + g) * ldx + k0 + t];
+                for (int c = 0; c < 4; c++) bv[c] = xs[(size_t)(8 * c + g) * ldx + k0 + t];
 #pragma unroll
-            for (int i = 0; i < MD_MT; i++) {
-                const int rt = warp + 8 * i;
-                if (rt < nrt) {
-                    const double av = os[(size_t)(k0 + t) * ldo + 8 * rt + g];
+                for (int i = 0; i < MD_MT; i++) {
+                    const int rt = warp + 8 * i;
+                    if (rt < nrt) {
+                        const double av = os[(size_t)(k0 + t) * ldo + 8 * rt + g];
 #pragma unroll
-                    for (int c = 0; c < 4; c++)
-                        if ((cm >> c) & 1) dmma_8x8x4(acc[i][c][0], acc[i][c][1], av, bv[c]);
+                        for (int c = 0; c < 4; c++)
+                            if ((cm >> c) & 1) dmma_8x8x4(acc[i][c][0], acc[i][c][1], av, bv[c]);
+                    }
                 }
             }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_u32(&empty[bi]));  // this warp is done with the slot
         }
-        __syncthreads();  // buffer bi is free
-        if (warp == 0 && st + MD_NBUF < nst) issue(st + MD_NBUF);
     }
-    if (!ok) {
-        if (tid == 0) atomicOr(M.err, 1ull);
-        // let every issued copy land before the block leaves
-        const int issued = min(nst, landed + MD_NBUF);
-        for (int st = landed; st < issued; st++) {
-            mbar_wait(smem_u32(&bars[st % MD_NBUF]), (par >> (st % MD_NBUF)) & 1u, kDrainWaitPolls);
-            par ^= 1u << (st % MD_NBUF);
-        }
-        return;
-    }
+    __syncthreads();
+    if (*abort_flag) return;
     // D through shared memory (the stage buffers are free), then coalesced stores
     double *cs = sm_md;  // [32 targets][Q4 + 1]
 #pragma unroll
     for (int i = 0; i < MD_MT; i++) {
         const int rt = warp + 8 * i;
-        if (rt < nrt)
+        if (warp < MD_THREADS / 32 && rt < nrt)
 #pragma unroll
             for (int c = 0; c < 4; c++) {
                 cs[(size_t)(8 * c + 2 * t) * (Q4 + 1) + 8 * rt + g] = acc[i][c][0];
@@ -366,7 +395,7 @@ __global__ void __launch_bounds__(MD_THREADS) k_m2l_dmma(M2lDmmaArgs M) {
             }
     }
     __syncthreads();
-    for (int n = warp; n < MD_TE; n += MD_THREADS / 32) {
+    for (int n = warp; n < MD_TE; n += MD_BLOCK / 32) {
         if (!sact[n]) continue;
         double *dst = A.udown + ((size_t)A.T.off[l + 1] + 4 * (size_t)(sact[n] - 1)) * Q;
         for (int r = lane; r < Q4; r += 32) dst[r] = cs[(size_t)n * (Q4 + 1) + r];
@@ -1145,7 +1174,7 @@ void run_upward_downward(kifmm_plan *P) {
             if (tiles) {
                 const size_t smem = m2l_dmma_smem(4 * Q);
                 ensure_dyn_smem(k_m2l_dmma, smem);
-                launch_pdl(k_m2l_dmma, dim3((unsigned)tiles), dim3(MD_THREADS), smem, s, M);
+                launch_pdl(k_m2l_dmma, dim3((unsigned)tiles), dim3(MD_BLOCK), smem, s, M);
             }
         }
         PhaseScope ph(P, KIFMM_PHASE_L2L);
