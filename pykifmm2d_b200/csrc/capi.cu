@@ -51,6 +51,7 @@ PhaseScope::~PhaseScope() {
 static void resolve_phases(kifmm_plan *P) {
     if (P->pending.empty()) return;
     KIFMM_CUDA(cudaStreamSynchronize(P->stream));
+    if (P->near_stream) KIFMM_CUDA(cudaStreamSynchronize(P->near_stream));
     for (auto &ph : P->pending) {
         float ms = 0.f;
         if (cudaEventElapsedTime(&ms, ph.a, ph.b) == cudaSuccess) P->phase_ms[ph.id] += ms;
@@ -340,6 +341,7 @@ int kifmm_build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n,
         PhaseScope ph(P, KIFMM_PHASE_TREE);
         P->have_mats = false;
         P->applied = false;
+        near_join(P);
         build_tree(P, x, y, n, mem);
     });
 }
@@ -407,6 +409,7 @@ int kifmm_synchronize(kifmm_plan *P) {
         KIFMM_REQUIRE(P, KIFMM_ERR_ARG, "null plan");
         use_device(P);
         ops_wait_now(P);
+        if (P->near_pending) KIFMM_CUDA(cudaStreamWaitEvent(P->stream, P->near_done, 0));  // kept pending
         KIFMM_CUDA(cudaStreamSynchronize(P->stream));
         check_device_flags(P);
     });
@@ -525,6 +528,9 @@ int kifmm_plan_destroy(kifmm_plan *P) {
         P->pending.clear();
         cudaStream_t s = P->stream, side = P->side;
         cudaEvent_t e0 = P->ops_fork, e1 = P->ops_done, e2 = P->tree_ev, e3 = P->ops_circ;
+        cudaStream_t ns = P->near_stream;
+        cudaEvent_t n0 = P->near_fork, n1 = P->near_done;
+        if (ns) cudaStreamSynchronize(ns);  // a near-field pass still reading the plan's buffers
         bool own = P->own_stream;
         unsigned long long *hp = P->hpin;
         delete P;  // buffers are freed stream-ordered on s and on the side stream
@@ -536,6 +542,11 @@ int kifmm_plan_destroy(kifmm_plan *P) {
             cudaEventDestroy(e1);
             cudaEventDestroy(e2);
             cudaEventDestroy(e3);
+        }
+        if (ns) {
+            cudaEventDestroy(n0);
+            cudaEventDestroy(n1);
+            cudaStreamDestroy(ns);
         }
         if (own && s) cudaStreamDestroy(s);
     });

@@ -150,6 +150,11 @@ struct kifmm_plan {
     // build continues (it needs only the root width and the depth); the main
     // stream waits on ops_done before the operators are used
     cudaStream_t side = nullptr;
+    // the near field at the sources, started by build_expansions on a stream
+    // of its own so that it runs under the far-field chain (mixed form)
+    cudaStream_t near_stream = nullptr;
+    cudaEvent_t near_fork = nullptr, near_done = nullptr;
+    bool near_pending = false;  // P->pots holds the near field of the last apply, far field not added yet
     cudaEvent_t ops_fork = nullptr, ops_done = nullptr;
     cudaEvent_t ops_circ = nullptr;  // side stream: the check circles are written (the P2M's only operator input)
     cudaEvent_t tree_ev = nullptr;   // build_tree: the split-cell counts are on the host
@@ -483,6 +488,8 @@ cudaStream_t device_side_stream(int device);  // one per device, created on firs
 void join_operators(kifmm_plan *P);   // main stream waits for it
 void ops_wait_now(kifmm_plan *P);     // issue a deferred join's stream wait (before any operator is read)
 void ops_wait_circles(kifmm_plan *P); // ... for the check circles only (before the P2M)
+void near_join(kifmm_plan *P);        // main stream waits for a near-field pass in flight, which is dropped
+bool near_start(kifmm_plan *P);       // passes_mixed.cu: start the near field on its own stream (mixed form)
 // planned.cu
 bool planned_ready(const kifmm_plan *P);
 void build_plan_matrices(kifmm_plan *P);

@@ -1129,6 +1129,7 @@ void apply_prologue(kifmm_plan *P) {
 void run_upward_downward(kifmm_plan *P) {
     cudaStream_t s = P->stream;
     const int Q = P->Q, L = P->L;
+    near_join(P);  // the previous apply's near-field pass, if never evaluated
     apply_prologue(P);
     if (P->opt.precision == KIFMM_PREC_MIXED) {
         run_passes_mixed(P);

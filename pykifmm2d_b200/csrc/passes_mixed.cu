@@ -394,8 +394,11 @@ __constant__ unsigned c_recip16[33] = {
 __device__ __forceinline__ int small_div(int x, int d) { return (int)(((unsigned)x * c_recip16[d]) >> 16); }
 
 // the L2P + P2P of leaf w of A's leaf list, by one warp: its 32-target tiles
-// [tile0, tile1) (all of them by default)
-template <int KIND>
+// [tile0, tile1) (all of them by default).  PART: LEAF_BOTH writes near + far
+// field, LEAF_NEAR the near field alone (P2P, run under the far-field chain),
+// LEAF_FAR adds the far field (L2P) to what LEAF_NEAR wrote.
+enum LeafPart { LEAF_BOTH = 0, LEAF_NEAR = 1, LEAF_FAR = 2 };
+template <int KIND, int PART = LEAF_BOTH>
 __device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w, int tile0 = 0, int tile1 = 1 << 20) {
     constexpr int R = 2 * KIFMM_TAYLOR_P + 1;
     constexpr float CLAMP = 1.17549435e-38f;  // FLT_MIN
@@ -422,7 +425,7 @@ __device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w, i
             cy = A.root + ((double)compact2(key) + 0.5) * wl;
         }
         const bool lap = KIND == KIFMM_KERNEL_LAPLACE;
-        const bool taylor = lap && A.taylor != nullptr && l >= 2;
+        const bool taylor = lap && A.taylor != nullptr && l >= 2 && PART != LEAF_NEAR;
         double *qd = qds[wib];
         float *qf = qfs[wib];
         ulonglong2 *sxy = sxys[wib];
@@ -437,7 +440,7 @@ __device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w, i
                 qd[r] = v;
                 qf[r] = (float)v;
             }
-        } else {
+        } else if (PART != LEAF_NEAR) {
             local_density(A, g, l, qd, lane);
         }
         const float kk = (float)A.k;
@@ -509,7 +512,7 @@ __device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w, i
             const f32x2 tx2 = f2_pack(txa, txb), ty2 = f2_pack(tya, tyb);
             double neara = 0.0, nearb = 0.0;
             float exa = 0.f, exb = 0.f;  // charges of the leaf's own points met at the floor
-            for (int c0 = 0; c0 < ns; c0 += LEAF_CHUNK) {
+            for (int c0 = 0; PART != LEAF_FAR && c0 < ns; c0 += LEAF_CHUNK) {
                 const int cn = min(LEAF_CHUNK, ns - c0);
                 if (t0 == tfirst || ns > LEAF_CHUNK) gather(c0, cn, lap && t0 == tfirst);
                 // lane (gi, j) takes sources j, j + sp, ...; j + (it - 1) sp < cn + 32
@@ -553,11 +556,11 @@ __device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w, i
                 const int slot = lane < ng ? 0 : 1, grp = lane - slot * ng;
                 double v = 0.0;
                 float ex = 0.f;
-                for (int m = 0; m < sp; m++) {
+                for (int m = 0; PART != LEAF_FAR && m < sp; m++) {
                     v += red[wib][slot][grp + m * ng];
                     ex += redf[wib][slot][grp + m * ng];
                 }
-                if (lap) {
+                if (lap && PART != LEAF_FAR) {
                     // the skipped charges leave log2(w^2) * sum(tau); the one skipped
                     // pair is almost always the target itself: take its FP64 charge
                     const double tau_t = A.taus[t];
@@ -567,7 +570,7 @@ __device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w, i
                 const double pxd = A.xs[t] - cx, pyd = A.ys[t] - cy;
                 // far field (L2P) in FP64
                 double far = 0.0;
-                if (l >= 2) {
+                if (l >= 2 && PART != LEAF_NEAR) {
                     const double zx = pxd * sc, zy = pyd * sc;
                     if (taylor && zx * zx + zy * zy <= 0.5625) {
                         // Horner: orders P..9 in FP32 (weighted by |z/rho|^9 < 0.008 where
@@ -602,7 +605,9 @@ __device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w, i
                         }
                     }
                 }
-                A.pots[t] = v * (double)gsum_scale<KIND>() + far;
+                if (PART == LEAF_BOTH) A.pots[t] = v * (double)gsum_scale<KIND>() + far;
+                else if (PART == LEAF_NEAR) A.pots[t] = v * (double)gsum_scale<KIND>();
+                else A.pots[t] += far;
             }
             __syncwarp();
         }
@@ -613,7 +618,7 @@ __device__ __forceinline__ void leaf_eval_f_leaf(const PassArgs &A, int64_t w, i
 // GPU, where the kernel lasts as long as its heaviest leaf) warps nlist ..
 // nlist + *nsplit - 1 take the tiles after the first of the leaves in
 // split_list, so a leaf of more than 32 points runs on two warps.
-template <int KIND, bool SPLIT>
+template <int KIND, bool SPLIT, int PART = LEAF_BOTH>
 __global__ void __launch_bounds__(32 * LEAF_WARPS, LEAF_BLOCKS_PER_SM)
     k_leaf_eval_f(PassArgs A, int64_t nlist, const int32_t *__restrict__ split_list,
                   const unsigned *__restrict__ nsplit) {
@@ -622,7 +627,7 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, LEAF_BLOCKS_PER_SM)
     const int64_t wstride = (int64_t)gridDim.x * LEAF_WARPS;
     if (!SPLIT) {
         for (int64_t w = (int64_t)blockIdx.x * LEAF_WARPS + (threadIdx.x >> 5); w < nlist; w += wstride)
-            leaf_eval_f_leaf<KIND>(A, w);
+            leaf_eval_f_leaf<KIND, PART>(A, w);
         return;
     }
     const int64_t total = nlist + *nsplit;
@@ -767,6 +772,7 @@ void run_passes_mixed(kifmm_plan *P) {
     cudaStream_t s = P->stream;
     const int Q = P->Q, L = P->L;
     if (L < 3) return;  // expansions cleared by run_upward_downward
+    near_start(P);  // the near field at the sources runs under the far-field chain
     PassArgs A = make_pass_args(P);
     mixed_upward(P, A);
     if (P->opt.m2l == KIFMM_M2L_FP32) {
@@ -829,6 +835,18 @@ void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
         return;
     }  // FP32 form: coincident pairs always contribute zero
     PassArgs A = mixed_leaf_args(P);
+    if (P->near_pending) {  // the near field is in P->pots (near_start): add the far field
+        KIFMM_CUDA(cudaStreamWaitEvent(P->stream, P->near_done, 0));
+        P->near_pending = false;
+        const dim3 grid((unsigned)((P->n_leaf_list + LEAF_WARPS - 1) / LEAF_WARPS)), block(32 * LEAF_WARPS);
+        if (P->kern.kind == KIFMM_KERNEL_LAPLACE)
+            launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_LAPLACE, false, LEAF_FAR>, grid, block, 0, P->stream, A,
+                       P->n_leaf_list, (const int32_t *)nullptr, (const unsigned *)nullptr);
+        else
+            launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_MOD_HELMHOLTZ, false, LEAF_FAR>, grid, block, 0, P->stream, A,
+                       P->n_leaf_list, (const int32_t *)nullptr, (const unsigned *)nullptr);
+        return;
+    }
     // fewer leaves than one wave of warps: split the big ones over two warps
     const int64_t nl = P->n_leaf_list;
     const bool split = nl < (int64_t)P->num_sms * LEAF_BLOCKS_PER_SM * LEAF_WARPS / 2;
@@ -857,6 +875,68 @@ void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
             launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_MOD_HELMHOLTZ, false>, grid, block, 0, P->stream, A, nl, slist,
                        scount);
     }
+}
+
+// The near field at the sources (P2P of every leaf over its colleagues) needs
+// only the sorted points and charges, none of the expansions: build_expansions
+// starts it on a stream of its own right after the charges are in tree order,
+// so that it runs while the far-field chain (P2M, M2M, M2L, L2L: some 30
+// mostly latency-bound launches) leaves SMs idle, and the evaluation at the
+// sources adds only the far field (LEAF_FAR).  Mixed FP32 near field, where
+// the near sum does not depend on check_self (coincident pairs contribute
+// zero); not inside a stream capture and not for leaf lists smaller than one
+// wave (those split big leaves over two warps instead).  A later evaluation
+// at other targets leaves the pass unused.
+// Only for the modified-Helmholtz (K0) kernel: its near field (a K0 series
+// per pair) is several times longer than the far-field chain, which then runs
+// entirely under it (2M-point annulus: 6.02 -> 5.24 ms per step).  The
+// Laplace near pass is about as long as the chain, and its blocks, filling
+// every SM, hold off the chain's small level launches (M2M 0.086 -> 0.21 ms
+// at 1M points, 0.10 -> 0.80 ms at 4M): +0.7% at 1M, -2% at 4M, not kept.
+bool near_start(kifmm_plan *P) {
+    const int64_t nl = P->n_leaf_list;
+    if (P->opt.precision != KIFMM_PREC_MIXED || P->opt.near_fp64 || P->opt.planned || P->cplx || nl <= 0)
+        return false;
+    if (P->kern.kind != KIFMM_KERNEL_MOD_HELMHOLTZ) return false;
+    if (nl < (int64_t)P->num_sms * LEAF_BLOCKS_PER_SM * LEAF_WARPS / 2) return false;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    KIFMM_CUDA(cudaStreamIsCapturing(P->stream, &cap));
+    if (cap != cudaStreamCaptureStatusNone) return false;
+    if (!P->near_stream) {
+        KIFMM_CUDA(cudaStreamCreateWithFlags(&P->near_stream, cudaStreamNonBlocking));
+        KIFMM_CUDA(cudaEventCreateWithFlags(&P->near_fork, cudaEventDisableTiming));
+        KIFMM_CUDA(cudaEventCreateWithFlags(&P->near_done, cudaEventDisableTiming));
+    }
+    KIFMM_CUDA(cudaEventRecord(P->near_fork, P->stream));
+    KIFMM_CUDA(cudaStreamWaitEvent(P->near_stream, P->near_fork, 0));
+    PassArgs A = make_pass_args(P);
+    const dim3 grid((unsigned)((nl + LEAF_WARPS - 1) / LEAF_WARPS)), block(32 * LEAF_WARPS);
+    {
+        struct Swap {  // the phase timer's events go to the near stream
+            kifmm_plan *P;
+            cudaStream_t main;
+            Swap(kifmm_plan *p) : P(p), main(p->stream) { P->stream = P->near_stream; }
+            ~Swap() { P->stream = main; }
+        } sw(P);
+        PhaseScope ph(P, KIFMM_PHASE_LEAF);
+        if (P->kern.kind == KIFMM_KERNEL_LAPLACE)
+            launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_LAPLACE, false, LEAF_NEAR>, grid, block, 0, P->near_stream, A, nl,
+                       (const int32_t *)nullptr, (const unsigned *)nullptr);
+        else
+            launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_MOD_HELMHOLTZ, false, LEAF_NEAR>, grid, block, 0, P->near_stream, A,
+                       nl, (const int32_t *)nullptr, (const unsigned *)nullptr);
+    }
+    KIFMM_CUDA(cudaEventRecord(P->near_done, P->near_stream));
+    P->near_pending = true;
+    return true;
+}
+
+// a near-field pass in flight is waited for and dropped (a new tree or apply
+// replaces the buffers it reads and writes)
+void near_join(kifmm_plan *P) {
+    if (!P->near_pending) return;
+    KIFMM_CUDA(cudaStreamWaitEvent(P->stream, P->near_done, 0));
+    P->near_pending = false;
 }
 
 // the FP32 leaf pass of several plans of one kernel kind in one launch
