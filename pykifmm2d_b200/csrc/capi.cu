@@ -528,8 +528,8 @@ int kifmm_plan_destroy(kifmm_plan *P) {
         P->pending.clear();
         cudaStream_t s = P->stream, side = P->side;
         cudaEvent_t e0 = P->ops_fork, e1 = P->ops_done, e2 = P->tree_ev, e3 = P->ops_circ;
-        cudaStream_t ns = P->near_stream;
-        cudaEvent_t n0 = P->near_fork, n1 = P->near_done;
+        cudaStream_t ns = P->near_stream, fs = P->far_stream;
+        cudaEvent_t n0 = P->near_fork, n1 = P->near_done, f0 = P->far_fork, f1 = P->far_done;
         if (ns) cudaStreamSynchronize(ns);  // a near-field pass still reading the plan's buffers
         bool own = P->own_stream;
         unsigned long long *hp = P->hpin;
@@ -543,10 +543,14 @@ int kifmm_plan_destroy(kifmm_plan *P) {
             cudaEventDestroy(e2);
             cudaEventDestroy(e3);
         }
-        if (ns) {
+        if (ns) {  // buffers allocated on the far stream were freed on it by the plan's destructor
+            cudaStreamSynchronize(fs);
             cudaEventDestroy(n0);
             cudaEventDestroy(n1);
+            cudaEventDestroy(f0);
+            cudaEventDestroy(f1);
             cudaStreamDestroy(ns);
+            cudaStreamDestroy(fs);
         }
         if (own && s) cudaStreamDestroy(s);
     });

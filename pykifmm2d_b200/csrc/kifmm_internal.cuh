@@ -152,8 +152,12 @@ struct kifmm_plan {
     cudaStream_t side = nullptr;
     // the near field at the sources, started by build_expansions on a stream
     // of its own so that it runs under the far-field chain (mixed form)
-    cudaStream_t near_stream = nullptr;
+    cudaStream_t near_stream = nullptr;  // lowest priority
     cudaEvent_t near_fork = nullptr, near_done = nullptr;
+    // ... while the far-field chain runs on a stream of the highest priority,
+    // so that its small launches are scheduled ahead of the near pass's blocks
+    cudaStream_t far_stream = nullptr;
+    cudaEvent_t far_fork = nullptr, far_done = nullptr;
     bool near_pending = false;  // P->pots holds the near field of the last apply, far field not added yet
     cudaEvent_t ops_fork = nullptr, ops_done = nullptr;
     cudaEvent_t ops_circ = nullptr;  // side stream: the check circles are written (the P2M's only operator input)

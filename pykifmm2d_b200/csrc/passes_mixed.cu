@@ -772,7 +772,28 @@ void run_passes_mixed(kifmm_plan *P) {
     cudaStream_t s = P->stream;
     const int Q = P->Q, L = P->L;
     if (L < 3) return;  // expansions cleared by run_upward_downward
-    near_start(P);  // the near field at the sources runs under the far-field chain
+    // the near field at the sources on a low-priority stream, the far-field
+    // chain below on a high-priority one (launches and allocations swapped
+    // there, joined back into the plan's stream at the end)
+    struct FarFork {
+        kifmm_plan *P;
+        bool on;
+        cudaStream_t main, g;
+        FarFork(kifmm_plan *p, bool fork) : P(p), on(fork), main(p->stream), g(g_stream) {
+            if (!on) return;
+            KIFMM_CUDA(cudaEventRecord(P->far_fork, main));
+            KIFMM_CUDA(cudaStreamWaitEvent(P->far_stream, P->far_fork, 0));
+            P->stream = P->far_stream;
+            g_stream = P->far_stream;
+        }
+        ~FarFork() {
+            if (!on) return;
+            cudaEventRecord(P->far_done, P->far_stream);
+            P->stream = main;
+            g_stream = g;
+            cudaStreamWaitEvent(main, P->far_done, 0);
+        }
+    } fork(P, near_start(P));
     PassArgs A = make_pass_args(P);
     mixed_upward(P, A);
     if (P->opt.m2l == KIFMM_M2L_FP32) {
@@ -887,25 +908,31 @@ void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
 // zero); not inside a stream capture and not for leaf lists smaller than one
 // wave (those split big leaves over two warps instead).  A later evaluation
 // at other targets leaves the pass unused.
-// Only for the modified-Helmholtz (K0) kernel: its near field (a K0 series
-// per pair) is several times longer than the far-field chain, which then runs
-// entirely under it (2M-point annulus: 6.02 -> 5.24 ms per step).  The
-// Laplace near pass is about as long as the chain, and its blocks, filling
-// every SM, hold off the chain's small level launches (M2M 0.086 -> 0.21 ms
-// at 1M points, 0.10 -> 0.80 ms at 4M): +0.7% at 1M, -2% at 4M, not kept.
+// The near pass runs on a stream of the lowest priority and the far-field
+// chain on one of the highest (run_passes_mixed), so that the chain's small
+// level launches are scheduled ahead of the near pass's blocks as SMs free up.
+// Measured per step against the single leaf pass after the chain: 2M-point K0
+// annulus 6.02 -> 5.23 ms (the K0 near field is several times longer than the
+// chain, which runs entirely under it); Laplace 1M mixture 1.005 -> 0.991 ms,
+// 4M uniform 2.446 -> 2.423 ms.  With equal priorities the near blocks held
+// off the chain (M2M 0.086 -> 0.21 ms at 1M, 0.10 -> 0.80 ms at 4M: 2% slower
+// at 4M).
 bool near_start(kifmm_plan *P) {
     const int64_t nl = P->n_leaf_list;
     if (P->opt.precision != KIFMM_PREC_MIXED || P->opt.near_fp64 || P->opt.planned || P->cplx || nl <= 0)
         return false;
-    if (P->kern.kind != KIFMM_KERNEL_MOD_HELMHOLTZ) return false;
+    if (P->kern.kind != KIFMM_KERNEL_LAPLACE && P->kern.kind != KIFMM_KERNEL_MOD_HELMHOLTZ) return false;
     if (nl < (int64_t)P->num_sms * LEAF_BLOCKS_PER_SM * LEAF_WARPS / 2) return false;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     KIFMM_CUDA(cudaStreamIsCapturing(P->stream, &cap));
     if (cap != cudaStreamCaptureStatusNone) return false;
     if (!P->near_stream) {
-        KIFMM_CUDA(cudaStreamCreateWithFlags(&P->near_stream, cudaStreamNonBlocking));
-        KIFMM_CUDA(cudaEventCreateWithFlags(&P->near_fork, cudaEventDisableTiming));
-        KIFMM_CUDA(cudaEventCreateWithFlags(&P->near_done, cudaEventDisableTiming));
+        int least = 0, greatest = 0;
+        KIFMM_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        KIFMM_CUDA(cudaStreamCreateWithPriority(&P->near_stream, cudaStreamNonBlocking, least));
+        KIFMM_CUDA(cudaStreamCreateWithPriority(&P->far_stream, cudaStreamNonBlocking, greatest));
+        for (cudaEvent_t *e : {&P->near_fork, &P->near_done, &P->far_fork, &P->far_done})
+            KIFMM_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
     }
     KIFMM_CUDA(cudaEventRecord(P->near_fork, P->stream));
     KIFMM_CUDA(cudaStreamWaitEvent(P->near_stream, P->near_fork, 0));
