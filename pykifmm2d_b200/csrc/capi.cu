@@ -342,6 +342,16 @@ int kifmm_build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n,
         P->have_mats = false;
         P->applied = false;
         near_join(P);
+#ifndef KIFMM_TREE_FORK
+#define KIFMM_TREE_FORK 1
+#endif
+        // the tree build's many small launches on the plan's highest-priority
+        // stream, ahead of the operator build that it starts on the side stream
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        KIFMM_CUDA(cudaStreamIsCapturing(P->stream, &cap));
+        const bool fork = KIFMM_TREE_FORK && cap == cudaStreamCaptureStatusNone;
+        if (fork) ensure_aux_streams(P);
+        HighPriorityFork hp(P, fork);
         build_tree(P, x, y, n, mem);
     });
 }

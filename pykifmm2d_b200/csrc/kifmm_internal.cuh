@@ -494,6 +494,31 @@ void ops_wait_now(kifmm_plan *P);     // issue a deferred join's stream wait (be
 void ops_wait_circles(kifmm_plan *P); // ... for the check circles only (before the P2M)
 void near_join(kifmm_plan *P);        // main stream waits for a near-field pass in flight, which is dropped
 bool near_start(kifmm_plan *P);       // passes_mixed.cu: start the near field on its own stream (mixed form)
+void ensure_aux_streams(kifmm_plan *P); // passes_mixed.cu: the plan's near / far streams
+// Runs what the scope enqueues on the plan's far stream (highest priority):
+// forked from the plan's stream at construction, launches and allocations
+// swapped there, joined back into the plan's stream at destruction.
+struct HighPriorityFork {
+    kifmm_plan *P;
+    bool on;
+    cudaStream_t main, g;
+    HighPriorityFork(kifmm_plan *p, bool fork) : P(p), on(fork), main(p->stream), g(g_stream) {
+        if (!on) return;
+        KIFMM_CUDA(cudaEventRecord(P->far_fork, main));
+        KIFMM_CUDA(cudaStreamWaitEvent(P->far_stream, P->far_fork, 0));
+        P->stream = P->far_stream;
+        g_stream = P->far_stream;
+    }
+    ~HighPriorityFork() {
+        if (!on) return;
+        cudaEventRecord(P->far_done, P->far_stream);
+        P->stream = main;
+        g_stream = g;
+        cudaStreamWaitEvent(main, P->far_done, 0);
+    }
+    HighPriorityFork(const HighPriorityFork &) = delete;
+    HighPriorityFork &operator=(const HighPriorityFork &) = delete;
+};
 // planned.cu
 bool planned_ready(const kifmm_plan *P);
 void build_plan_matrices(kifmm_plan *P);

@@ -775,25 +775,7 @@ void run_passes_mixed(kifmm_plan *P) {
     // the near field at the sources on a low-priority stream, the far-field
     // chain below on a high-priority one (launches and allocations swapped
     // there, joined back into the plan's stream at the end)
-    struct FarFork {
-        kifmm_plan *P;
-        bool on;
-        cudaStream_t main, g;
-        FarFork(kifmm_plan *p, bool fork) : P(p), on(fork), main(p->stream), g(g_stream) {
-            if (!on) return;
-            KIFMM_CUDA(cudaEventRecord(P->far_fork, main));
-            KIFMM_CUDA(cudaStreamWaitEvent(P->far_stream, P->far_fork, 0));
-            P->stream = P->far_stream;
-            g_stream = P->far_stream;
-        }
-        ~FarFork() {
-            if (!on) return;
-            cudaEventRecord(P->far_done, P->far_stream);
-            P->stream = main;
-            g_stream = g;
-            cudaStreamWaitEvent(main, P->far_done, 0);
-        }
-    } fork(P, near_start(P));
+    HighPriorityFork fork(P, near_start(P));
     PassArgs A = make_pass_args(P);
     mixed_upward(P, A);
     if (P->opt.m2l == KIFMM_M2L_FP32) {
@@ -917,6 +899,17 @@ void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
 // 4M uniform 2.446 -> 2.423 ms.  With equal priorities the near blocks held
 // off the chain (M2M 0.086 -> 0.21 ms at 1M, 0.10 -> 0.80 ms at 4M: 2% slower
 // at 4M).
+// the plan's near stream (lowest priority) and far stream (highest), once
+void ensure_aux_streams(kifmm_plan *P) {
+    if (P->near_stream) return;
+    int least = 0, greatest = 0;
+    KIFMM_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    KIFMM_CUDA(cudaStreamCreateWithPriority(&P->near_stream, cudaStreamNonBlocking, least));
+    KIFMM_CUDA(cudaStreamCreateWithPriority(&P->far_stream, cudaStreamNonBlocking, greatest));
+    for (cudaEvent_t *e : {&P->near_fork, &P->near_done, &P->far_fork, &P->far_done})
+        KIFMM_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+}
+
 bool near_start(kifmm_plan *P) {
     const int64_t nl = P->n_leaf_list;
     if (P->opt.precision != KIFMM_PREC_MIXED || P->opt.near_fp64 || P->opt.planned || P->cplx || nl <= 0)
@@ -926,14 +919,7 @@ bool near_start(kifmm_plan *P) {
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     KIFMM_CUDA(cudaStreamIsCapturing(P->stream, &cap));
     if (cap != cudaStreamCaptureStatusNone) return false;
-    if (!P->near_stream) {
-        int least = 0, greatest = 0;
-        KIFMM_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-        KIFMM_CUDA(cudaStreamCreateWithPriority(&P->near_stream, cudaStreamNonBlocking, least));
-        KIFMM_CUDA(cudaStreamCreateWithPriority(&P->far_stream, cudaStreamNonBlocking, greatest));
-        for (cudaEvent_t *e : {&P->near_fork, &P->near_done, &P->far_fork, &P->far_done})
-            KIFMM_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
-    }
+    ensure_aux_streams(P);
     KIFMM_CUDA(cudaEventRecord(P->near_fork, P->stream));
     KIFMM_CUDA(cudaStreamWaitEvent(P->near_stream, P->near_fork, 0));
     PassArgs A = make_pass_args(P);
