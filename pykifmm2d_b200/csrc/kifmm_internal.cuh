@@ -493,7 +493,7 @@ void join_operators(kifmm_plan *P);   // main stream waits for it
 void ops_wait_now(kifmm_plan *P);     // issue a deferred join's stream wait (before any operator is read)
 void ops_wait_circles(kifmm_plan *P); // ... for the check circles only (before the P2M)
 void near_join(kifmm_plan *P);        // main stream waits for a near-field pass in flight, which is dropped
-bool near_start(kifmm_plan *P);       // passes_mixed.cu: start the near field on its own stream (mixed form)
+bool near_possible(kifmm_plan *P);    // passes_mixed.cu: whether the apply runs the near field on its own stream
 void ensure_aux_streams(kifmm_plan *P); // passes_mixed.cu: the plan's near / far streams
 // Runs what the scope enqueues on the plan's far stream (highest priority):
 // forked from the plan's stream at construction, launches and allocations

@@ -751,6 +751,7 @@ void run_m2m_levels(kifmm_plan *P, const PassArgs &A);
 void run_l2l_levels(kifmm_plan *P, const PassArgs &A);
 
 // P2M and M2M of the mixed apply
+void near_launch(kifmm_plan *P);
 void mixed_upward(kifmm_plan *P, const PassArgs &A) {
     if (P->n_p2m_list) {
         PhaseScope ph(P, KIFMM_PHASE_P2M);
@@ -775,9 +776,11 @@ void run_passes_mixed(kifmm_plan *P) {
     // the near field at the sources on a low-priority stream, the far-field
     // chain below on a high-priority one (launches and allocations swapped
     // there, joined back into the plan's stream at the end)
-    HighPriorityFork fork(P, near_start(P));
+    const bool near = near_possible(P);
+    HighPriorityFork fork(P, near);
     PassArgs A = make_pass_args(P);
     mixed_upward(P, A);
+    if (near) near_launch(P);  // after the M2M chain, under the M2L and L2L
     if (P->opt.m2l == KIFMM_M2L_FP32) {
         PhaseScope ph(P, KIFMM_PHASE_M2L);
         const int thr = ((4 * Q + 31) / 32) * 32;
@@ -838,7 +841,7 @@ void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
         return;
     }  // FP32 form: coincident pairs always contribute zero
     PassArgs A = mixed_leaf_args(P);
-    if (P->near_pending) {  // the near field is in P->pots (near_start): add the far field
+    if (P->near_pending) {  // the near field is in P->pots (near_launch): add the far field
         KIFMM_CUDA(cudaStreamWaitEvent(P->stream, P->near_done, 0));
         P->near_pending = false;
         const dim3 grid((unsigned)((P->n_leaf_list + LEAF_WARPS - 1) / LEAF_WARPS)), block(32 * LEAF_WARPS);
@@ -881,24 +884,22 @@ void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
 }
 
 // The near field at the sources (P2P of every leaf over its colleagues) needs
-// only the sorted points and charges, none of the expansions: build_expansions
-// starts it on a stream of its own right after the charges are in tree order,
-// so that it runs while the far-field chain (P2M, M2M, M2L, L2L: some 30
-// mostly latency-bound launches) leaves SMs idle, and the evaluation at the
-// sources adds only the far field (LEAF_FAR).  Mixed FP32 near field, where
-// the near sum does not depend on check_self (coincident pairs contribute
-// zero); not inside a stream capture and not for leaf lists smaller than one
-// wave (those split big leaves over two warps instead).  A later evaluation
-// at other targets leaves the pass unused.
+// only the sorted points and charges, none of the expansions, so the apply
+// runs it on a stream of its own while the far-field chain leaves SMs idle,
+// and the evaluation at the sources adds only the far field (LEAF_FAR).
+// Mixed FP32 near field, where the near sum does not depend on check_self
+// (coincident pairs contribute zero); not inside a stream capture and not for
+// leaf lists smaller than one wave (those split big leaves over two warps
+// instead).  A later evaluation at other targets leaves the pass unused.
 // The near pass runs on a stream of the lowest priority and the far-field
-// chain on one of the highest (run_passes_mixed), so that the chain's small
-// level launches are scheduled ahead of the near pass's blocks as SMs free up.
-// Measured per step against the single leaf pass after the chain: 2M-point K0
-// annulus 6.02 -> 5.23 ms (the K0 near field is several times longer than the
-// chain, which runs entirely under it); Laplace 1M mixture 1.005 -> 0.991 ms,
-// 4M uniform 2.446 -> 2.423 ms.  With equal priorities the near blocks held
-// off the chain (M2M 0.086 -> 0.21 ms at 1M, 0.10 -> 0.80 ms at 4M: 2% slower
-// at 4M).
+// chain on one of the highest, and the pass starts after the M2M chain, under
+// the source slicing, M2L and L2L: started with the apply its blocks, filling
+// every SM, held off the M2M chain's small level launches even with the
+// priorities (M2M 0.086 -> 0.18 ms at 1M points).  Measured per step against
+// the single leaf pass after the chain: 1M mixture 1.005 -> 0.953 ms (0.971-
+// 0.994 when started with the apply), 4M uniform 2.446 -> 2.444 ms, 2M K0
+// annulus 6.02 -> 5.20 ms (the K0 near field is several times longer than the
+// chain, which runs under it).
 // the plan's near stream (lowest priority) and far stream (highest), once
 void ensure_aux_streams(kifmm_plan *P) {
     if (P->near_stream) return;
@@ -910,7 +911,7 @@ void ensure_aux_streams(kifmm_plan *P) {
         KIFMM_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
 }
 
-bool near_start(kifmm_plan *P) {
+bool near_possible(kifmm_plan *P) {
     const int64_t nl = P->n_leaf_list;
     if (P->opt.precision != KIFMM_PREC_MIXED || P->opt.near_fp64 || P->opt.planned || P->cplx || nl <= 0)
         return false;
@@ -920,6 +921,12 @@ bool near_start(kifmm_plan *P) {
     KIFMM_CUDA(cudaStreamIsCapturing(P->stream, &cap));
     if (cap != cudaStreamCaptureStatusNone) return false;
     ensure_aux_streams(P);
+    return true;
+}
+
+// the near pass, forked from the plan's stream at this point
+void near_launch(kifmm_plan *P) {
+    const int64_t nl = P->n_leaf_list;
     KIFMM_CUDA(cudaEventRecord(P->near_fork, P->stream));
     KIFMM_CUDA(cudaStreamWaitEvent(P->near_stream, P->near_fork, 0));
     PassArgs A = make_pass_args(P);
@@ -941,7 +948,6 @@ bool near_start(kifmm_plan *P) {
     }
     KIFMM_CUDA(cudaEventRecord(P->near_done, P->near_stream));
     P->near_pending = true;
-    return true;
 }
 
 // a near-field pass in flight is waited for and dropped (a new tree or apply
