@@ -770,7 +770,6 @@ void mixed_l2l(kifmm_plan *P, const PassArgs &A) {
 }
 
 void run_passes_mixed(kifmm_plan *P) {
-    cudaStream_t s = P->stream;
     const int Q = P->Q, L = P->L;
     if (L < 3) return;  // expansions cleared by run_upward_downward
     // the near field at the sources on a low-priority stream, the far-field
@@ -789,7 +788,7 @@ void run_passes_mixed(kifmm_plan *P) {
         for (int l = 1; l <= L - 2; l++) {
             int64_t ne = P->lt.ne[l];
             if (!ne) continue;
-            k_m2l_f<<<(unsigned)((ne + M2LF_TE - 1) / M2LF_TE), thr, smem, s>>>(A, l);
+            k_m2l_f<<<(unsigned)((ne + M2LF_TE - 1) / M2LF_TE), thr, smem, P->stream>>>(A, l);  // (the far stream)
             KIFMM_LAUNCHED();
         }
         return;

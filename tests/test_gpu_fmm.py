@@ -292,6 +292,38 @@ def test_mixed_m2l_forms_vs_reference(golden_cases, name, form):
     assert e <= max(M2L_FORMS[form], 0.2 * e_ref)
 
 
+@pytest.mark.parametrize("kernel", ["laplace", "k0"])
+@pytest.mark.parametrize("form", ["int8", "int8x4", "fp32", "bf16x3", "fp16x3"])
+def test_near_field_under_far_chain_every_m2l_form(form, kernel):
+    """Trees with more leaves than one wave of the leaf kernel run the near
+    field at the sources on a stream of its own under the far-field chain (the
+    chain on a second stream) and add the far field at the evaluation.  Every
+    M2L form of that path against the plain FP64 form on the same points
+    (bounds as test_mixed_m2l_forms_vs_reference), and the split evaluation
+    against the single-pass one on the same expansions (a second evaluation)."""
+    import pykifmm2d_b200 as P
+    from bench import gen_uniform
+    x, y, tau = gen_uniform(200_000, 5)
+    kern = P.LaplaceKernel() if kernel == "laplace" else P.ModifiedHelmholtzKernel(10.0)
+
+    def run(**kw):
+        f = P.FMM(x, y, P.Get_Kernel_Functions(kern), P.prepare_numba_functions_on_the_fly(kern), 32, 64, **kw)
+        f.build_tree()
+        f.precompute()
+        f.build_expansions(tau)
+        return f, f.evaluate_to_points(f.x, f.y, True)
+
+    _, ref = run(precision="fp64")
+    f, pot = run(precision="mixed", m2l=form)
+    assert f.tree_info().n_leaves > 148 * 32 // 2, "the case must take the split near / far path"
+    e = rel(pot, ref)
+    again = f.evaluate_to_points(f.x, f.y, True)  # single pass on the same expansions
+    d = rel(pot, again)
+    print(f"{kernel} m2l={form}: split path vs FP64 {e:.2e}, vs single pass {d:.2e}")
+    assert e <= M2L_FORMS[form]
+    assert d <= 1e-13
+
+
 @pytest.mark.parametrize("name", ["uniform3k_cut16", "c1_uniform20k", "mix2k_cut8", "annulus6k_k0", "cluster_dup"])
 def test_int8_tensor_m2l_is_fp64_accurate(golden_cases, name):
     """Tensor-core M2L on int8 slices (exact int32 accumulation) with the
