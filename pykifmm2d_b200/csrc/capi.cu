@@ -106,6 +106,33 @@ cudaStream_t device_side_stream(int device) {
     return side[device];
 }
 
+// Pairs of (lowest-priority, highest-priority) streams for the plans' near
+// field and far-field chain, kept per device and handed from a destroyed plan
+// to the next one (creating two streams per plan costs more than a small
+// apply's launches; stream-ordered frees on them stay valid across plans).
+static std::mutex g_aux_mu;
+static std::vector<std::pair<cudaStream_t, cudaStream_t>> g_aux_free[64];
+void aux_streams_acquire(int device, cudaStream_t *near, cudaStream_t *far) {
+    KIFMM_REQUIRE(device >= 0 && device < 64, KIFMM_ERR_ARG, "device index out of range");
+    {
+        std::lock_guard<std::mutex> lock(g_aux_mu);
+        if (!g_aux_free[device].empty()) {
+            *near = g_aux_free[device].back().first;
+            *far = g_aux_free[device].back().second;
+            g_aux_free[device].pop_back();
+            return;
+        }
+    }
+    int least = 0, greatest = 0;
+    KIFMM_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    KIFMM_CUDA(cudaStreamCreateWithPriority(near, cudaStreamNonBlocking, least));
+    KIFMM_CUDA(cudaStreamCreateWithPriority(far, cudaStreamNonBlocking, greatest));
+}
+static void aux_streams_release(int device, cudaStream_t near, cudaStream_t far) {
+    std::lock_guard<std::mutex> lock(g_aux_mu);
+    g_aux_free[device].emplace_back(near, far);
+}
+
 void set_error(const std::string &msg) { g_last_error = msg; }
 
 template <class F>
@@ -540,6 +567,7 @@ int kifmm_plan_destroy(kifmm_plan *P) {
         cudaEvent_t e0 = P->ops_fork, e1 = P->ops_done, e2 = P->tree_ev, e3 = P->ops_circ;
         cudaStream_t ns = P->near_stream, fs = P->far_stream;
         cudaEvent_t n0 = P->near_fork, n1 = P->near_done, f0 = P->far_fork, f1 = P->far_done;
+        const int dev = P->device;
         if (ns) cudaStreamSynchronize(ns);  // a near-field pass still reading the plan's buffers
         bool own = P->own_stream;
         unsigned long long *hp = P->hpin;
@@ -559,8 +587,7 @@ int kifmm_plan_destroy(kifmm_plan *P) {
             cudaEventDestroy(n1);
             cudaEventDestroy(f0);
             cudaEventDestroy(f1);
-            cudaStreamDestroy(ns);
-            cudaStreamDestroy(fs);
+            aux_streams_release(dev, ns, fs);
         }
         if (own && s) cudaStreamDestroy(s);
     });

@@ -900,12 +900,10 @@ void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
 // annulus 6.02 -> 5.20 ms (the K0 near field is several times longer than the
 // chain, which runs under it).
 // the plan's near stream (lowest priority) and far stream (highest), once
+void aux_streams_acquire(int device, cudaStream_t *near, cudaStream_t *far);  // capi.cu: per-device pool
 void ensure_aux_streams(kifmm_plan *P) {
     if (P->near_stream) return;
-    int least = 0, greatest = 0;
-    KIFMM_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
-    KIFMM_CUDA(cudaStreamCreateWithPriority(&P->near_stream, cudaStreamNonBlocking, least));
-    KIFMM_CUDA(cudaStreamCreateWithPriority(&P->far_stream, cudaStreamNonBlocking, greatest));
+    aux_streams_acquire(P->device, &P->near_stream, &P->far_stream);
     for (cudaEvent_t *e : {&P->near_fork, &P->near_done, &P->far_fork, &P->far_done})
         KIFMM_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
 }
