@@ -133,6 +133,27 @@ static void aux_streams_release(int device, cudaStream_t near, cudaStream_t far)
     g_aux_free[device].emplace_back(near, far);
 }
 
+// The plans' own streams (plans created without one), pooled the same way.
+static std::vector<cudaStream_t> g_own_free[64];
+static cudaStream_t own_stream_acquire(int device) {
+    KIFMM_REQUIRE(device >= 0 && device < 64, KIFMM_ERR_ARG, "device index out of range");
+    {
+        std::lock_guard<std::mutex> lock(g_aux_mu);
+        if (!g_own_free[device].empty()) {
+            cudaStream_t s = g_own_free[device].back();
+            g_own_free[device].pop_back();
+            return s;
+        }
+    }
+    cudaStream_t s = nullptr;
+    KIFMM_CUDA(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    return s;
+}
+static void own_stream_release(int device, cudaStream_t s) {
+    std::lock_guard<std::mutex> lock(g_aux_mu);
+    g_own_free[device].push_back(s);
+}
+
 void set_error(const std::string &msg) { g_last_error = msg; }
 
 template <class F>
@@ -343,7 +364,7 @@ int kifmm_plan_create(const kifmm_kernel *kernel, int32_t nequiv, int32_t ncutof
             if (o.stream) {
                 P->stream = (cudaStream_t)o.stream;
             } else {
-                KIFMM_CUDA(cudaStreamCreateWithFlags(&P->stream, cudaStreamNonBlocking));
+                P->stream = own_stream_acquire(P->device);
                 P->own_stream = true;
             }
         } catch (...) {
@@ -589,7 +610,7 @@ int kifmm_plan_destroy(kifmm_plan *P) {
             cudaEventDestroy(f1);
             aux_streams_release(dev, ns, fs);
         }
-        if (own && s) cudaStreamDestroy(s);
+        if (own && s) own_stream_release(dev, s);  // synchronised above
     });
 }
 
