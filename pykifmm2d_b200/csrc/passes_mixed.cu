@@ -637,6 +637,105 @@ __global__ void __launch_bounds__(32 * LEAF_WARPS, LEAF_BLOCKS_PER_SM)
     }
 }
 
+// The far field of the Laplace leaves after a near-only pass (LEAF_NEAR), with
+// every lane busy: one block per 32 consecutive leaves of one level (the
+// k_leaf_taylor tiling), each thread a target of those leaves.  The leaves'
+// Taylor coefficients (written by k_leaf_taylor) are staged in shared memory,
+// orders >= 9 as FP32 and orders <= 8 as FP64, and the Horner L2P is the
+// one of leaf_eval_f_leaf step for step, so the sum added to the near field
+// in pots is the same; targets beyond the series radius take the direct sum
+// over the equivalent points.  Replaces the far-only warp-per-leaf pass,
+// whose Horner ran on about half the lanes.
+constexpr int FT_THREADS = 128;
+__global__ void __launch_bounds__(FT_THREADS) k_leaf_far_taylor(TaylorArgs T) {
+    constexpr int R = 2 * KIFMM_TAYLOR_P + 1;
+    __shared__ float qf[32][R + 1];
+    __shared__ double qd[32][17];  // orders 0..8
+    __shared__ double scx[32], scy[32], ssc[32];
+    __shared__ int sbot[32], spre[33], snode[32], slev[32];
+    const PassArgs &A = T.A;
+    pdl_trigger();
+    const int64_t b = blockIdx.x;
+    int l = T.lmin;
+    while (l < T.lmax && T.toff[l + 1] <= b) l++;
+    const int64_t w0 = T.loff[l] + (b - T.toff[l]) * 32;
+    const int nt = (int)min((int64_t)32, T.loff[l + 1] - w0);
+    const int tid = threadIdx.x;
+    pdl_wait();  // coefficients from k_leaf_taylor; near field in pots
+    if (tid < 32) {
+        int cnt = 0;
+        if (tid < nt) {
+            const int32_t *rec = A.leaf_rec + (w0 + tid) * LEAF_REC_WORDS;
+            const int lv = rec[LR_LEVEL];
+            const uint64_t key = (uint64_t)(uint32_t)rec[LR_KEY_LO] | ((uint64_t)(uint32_t)rec[LR_KEY_HI] << 32);
+            const double wl = ldexp(A.W, -lv);
+            scx[tid] = A.root + ((double)compact2(key >> 1) + 0.5) * wl;
+            scy[tid] = A.root + ((double)compact2(key) + 0.5) * wl;
+            ssc[tid] = 1.0 / wl;
+            sbot[tid] = rec[LR_BOT];
+            snode[tid] = rec[LR_NODE];
+            slev[tid] = lv;
+            cnt = rec[LR_TOP] - rec[LR_BOT];
+        }
+        int v = cnt;  // inclusive scan of the leaves' point counts
+        for (int o = 1; o < 32; o <<= 1) {
+            const int u = __shfl_up_sync(0xffffffffu, v, o);
+            if (tid >= o) v += u;
+        }
+        spre[tid + 1] = v;
+        if (tid == 0) spre[0] = 0;
+    }
+    for (int i = tid; i < nt * R; i += FT_THREADS) {
+        const int n = i / R, r = i - n * R;
+        const double c = T.coef[(w0 + n) * R + r];
+        qf[n][r] = (float)c;
+        if (r < 17) qd[n][r] = c;
+    }
+    __syncthreads();
+    const int total = spre[nt];
+    for (int i = tid; i < total; i += FT_THREADS) {
+        int n = 0;  // the leaf of flat target i: the last n with spre[n] <= i
+        for (int step = 16; step; step >>= 1)
+            if (n + step < nt && spre[n + step] <= i) n += step;
+        const int t = sbot[n] + (i - spre[n]);
+        const double pxd = A.xs[t] - scx[n], pyd = A.ys[t] - scy[n];
+        const double zx = pxd * ssc[n], zy = pyd * ssc[n];
+        double far;
+        if (zx * zx + zy * zy <= 0.5625) {
+            const float zxf = (float)zx, zyf = (float)zy;
+            float fr = qf[n][R - 2], fi = qf[n][R - 1];
+            for (int jj = KIFMM_TAYLOR_P - 1; jj >= 9; jj--) {
+                const float nr = fmaf(fr, zxf, fmaf(-fi, zyf, qf[n][2 * jj - 1]));
+                const float ni = fmaf(fr, zyf, fmaf(fi, zxf, qf[n][2 * jj]));
+                fr = nr;
+                fi = ni;
+            }
+            double sr = fr, si = fi;
+            for (int jj = 8; jj >= 1; jj--) {
+                double nr = fma(sr, zx, fma(-si, zy, qd[n][2 * jj - 1]));
+                double ni = fma(sr, zy, fma(si, zx, qd[n][2 * jj]));
+                sr = nr;
+                si = ni;
+            }
+            far = qd[n][0] + (sr * zx - si * zy);
+        } else {
+            // direct FP64 sum over the equivalent points (targets outside the series radius)
+            const int lv = slev[n], g = snode[n];
+            const double *lgd = A.ops + (size_t)lv * A.stride + A.off_large;
+            const double *inv = A.ops + (size_t)lv * A.stride + A.off_inv;
+            const double *u = A.udown + (size_t)g * A.Q;
+            far = 0.0;
+            for (int q = 0; q < A.Q; q++) {
+                double qq = 0.0;
+                for (int c = 0; c < A.Q; c++) qq = fma(inv[q * A.Q + c], u[c], qq);
+                double dx = pxd - lgd[q], dy = pyd - lgd[A.Q + q];
+                far = fma(green_d(A.kind, A.k, dx * dx + dy * dy), qq, far);
+            }
+        }
+        A.pots[t] += far;
+    }
+}
+
 // the leaves of more than 32 points (their tiles after the first), for the
 // split form of k_leaf_eval_f
 __global__ void k_leaf_split_list(const int32_t *__restrict__ rec, int64_t nlist, int32_t *__restrict__ out,
@@ -802,6 +901,24 @@ void run_passes_mixed(kifmm_plan *P) {
 
 // The arguments of the FP32 leaf kernel; for the Laplace kernel this first
 // launches the Taylor coefficients of the leaves' local expansions.
+// the 32-leaf tiles of the leaves at levels >= 2 (k_leaf_taylor, k_leaf_far_taylor)
+static TaylorArgs taylor_tiling(kifmm_plan *P, const PassArgs &A, int64_t *ntiles) {
+    TaylorArgs T{};
+    T.A = A;
+    T.list = P->leaf_list.p;
+    T.coef = P->leaf_coef.p;
+    T.lmin = 2;
+    T.lmax = P->L - 1;
+    int64_t tiles = 0;
+    for (int l = 0; l <= MAX_LEVELS; l++) {
+        T.loff[l] = P->leaf_loff[l];
+        T.toff[l] = tiles;
+        if (l >= T.lmin && l <= T.lmax && l < MAX_LEVELS) tiles += (P->leaf_loff[l + 1] - P->leaf_loff[l] + 31) / 32;
+    }
+    *ntiles = tiles;
+    return T;
+}
+
 PassArgs mixed_leaf_args(kifmm_plan *P) {
     PassArgs A = make_pass_args(P);
     if (P->kern.kind == KIFMM_KERNEL_LAPLACE && P->l2p_taylor.p && P->L >= 3) {
@@ -809,19 +926,8 @@ PassArgs mixed_leaf_args(kifmm_plan *P) {
         KIFMM_REQUIRE(P->Q % 4 == 0, KIFMM_ERR_ARG, "mixed Laplace form: Nequiv must be a multiple of 4");
         P->leaf_coef.alloc((size_t)P->n_leaf_list * R);
         A.leaf_coef = P->leaf_coef.p;
-        TaylorArgs T{};
-        T.A = A;
-        T.list = P->leaf_list.p;
-        T.coef = P->leaf_coef.p;
-        T.lmin = 2;
-        T.lmax = P->L - 1;
         int64_t tiles = 0;
-        for (int l = 0; l <= MAX_LEVELS; l++) {
-            T.loff[l] = P->leaf_loff[l];
-            T.toff[l] = tiles;
-            if (l >= T.lmin && l <= T.lmax && l < MAX_LEVELS)
-                tiles += (P->leaf_loff[l + 1] - P->leaf_loff[l] + 31) / 32;
-        }
+        TaylorArgs T = taylor_tiling(P, A, &tiles);
         if (tiles) {
             const size_t smem = ((size_t)P->Q * pad4mod16(8 * TY_MTR) + 32 * (size_t)pad4mod16(P->Q) + 32 * (size_t)R) *
                                 sizeof(double);
@@ -843,6 +949,12 @@ void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
     if (P->near_pending) {  // the near field is in P->pots (near_launch): add the far field
         KIFMM_CUDA(cudaStreamWaitEvent(P->stream, P->near_done, 0));
         P->near_pending = false;
+        if (A.leaf_coef) {  // Laplace: every leaf of level >= 2 has its Taylor coefficients
+            int64_t tiles = 0;
+            TaylorArgs T = taylor_tiling(P, A, &tiles);
+            if (tiles) launch_pdl(k_leaf_far_taylor, dim3((unsigned)tiles), dim3(FT_THREADS), 0, P->stream, T);
+            return;
+        }
         const dim3 grid((unsigned)((P->n_leaf_list + LEAF_WARPS - 1) / LEAF_WARPS)), block(32 * LEAF_WARPS);
         if (P->kern.kind == KIFMM_KERNEL_LAPLACE)
             launch_pdl(k_leaf_eval_f<KIFMM_KERNEL_LAPLACE, false, LEAF_FAR>, grid, block, 0, P->stream, A,
