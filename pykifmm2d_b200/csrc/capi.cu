@@ -106,6 +106,11 @@ cudaStream_t device_side_stream(int device) {
     return side[device];
 }
 
+// Build the tree on the plan's highest-priority stream (1) or on its own (0).
+#ifndef KIFMM_TREE_FORK
+#define KIFMM_TREE_FORK 1
+#endif
+
 // Pairs of (lowest-priority, highest-priority) streams for the plans' near
 // field and far-field chain, kept per device and handed from a destroyed plan
 // to the next one (creating two streams per plan costs more than a small
@@ -390,9 +395,6 @@ int kifmm_build_tree(kifmm_plan *P, const double *x, const double *y, int64_t n,
         P->have_mats = false;
         P->applied = false;
         near_join(P);
-#ifndef KIFMM_TREE_FORK
-#define KIFMM_TREE_FORK 1
-#endif
         // the tree build's many small launches on the plan's highest-priority
         // stream, ahead of the operator build that it starts on the side stream
         cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
