@@ -1011,7 +1011,9 @@ void run_eval_sources_mixed(kifmm_plan *P, int check_self) {
 // 0.994 when started with the apply), 4M uniform 2.446 -> 2.444 ms, 2M K0
 // annulus 6.02 -> 5.20 ms (the K0 near field is several times longer than the
 // chain, which runs under it).
-// the plan's near stream (lowest priority) and far stream (highest), once
+
+// the plan's near stream (lowest priority) and far stream (highest), once,
+// from the per-device pool
 void aux_streams_acquire(int device, cudaStream_t *near, cudaStream_t *far);  // capi.cu: per-device pool
 void ensure_aux_streams(kifmm_plan *P) {
     if (P->near_stream) return;
